@@ -1,0 +1,603 @@
+"""numpy front end for the CPU oracle (liboracle.so) and the reference harness.
+
+TEST INFRASTRUCTURE ONLY. Imported by the test suite, the smoke check and the
+benchmark's CPU-baseline leg, as the checker of the CUDA path; the product
+never imports it.
+
+Two libraries are wrapped:
+
+* ``Oracle``: this project's C restatement of the reference algorithm
+  (``oracle/mb2_oracle.c``), built by ``oracle/Makefile``.
+* ``RefHarness``: the reference's own host-compiled functors
+  (``oracle/_ref/libmars_ref.so``, built by ``oracle/ref_harness/Makefile``
+  from the reference checkout). Present only where it was built.
+
+Arrays are numpy, float4 rows for vectors, C-contiguous.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ORACLE_SO = os.path.join(HERE, "liboracle.so")
+REF_SO = os.path.join(HERE, "_ref", "libmars_ref.so")
+
+_f32p = np.ctypeslib.ndpointer(np.float32, flags="C_CONTIGUOUS")
+_f64p = np.ctypeslib.ndpointer(np.float64, flags="C_CONTIGUOUS")
+_u32p = np.ctypeslib.ndpointer(np.uint32, flags="C_CONTIGUOUS")
+_i32p = np.ctypeslib.ndpointer(np.int32, flags="C_CONTIGUOUS")
+
+
+def build_oracle() -> str:
+    """Compile liboracle.so (gcc, seconds). Returns its path."""
+    subprocess.run(["make", "-s", "-C", HERE], check=True)
+    return ORACLE_SO
+
+
+class Box(C.Structure):
+    _fields_ = [("origin", C.c_float * 3), ("size", C.c_float * 3), ("periodic", C.c_int * 3)]
+
+    @classmethod
+    def make(cls, origin, size, periodic=(1, 1, 1)):
+        b = cls()
+        for a in range(3):
+            b.origin[a] = float(origin[a])
+            b.size[a] = float(size[a])
+            b.periodic[a] = int(periodic[a])
+        return b
+
+
+class Table(C.Structure):
+    _fields_ = [("pot", C.c_void_p), ("step_inv", C.c_float), ("size", C.c_uint32),
+                ("start", C.c_float), ("is_periodic", C.c_int)]
+
+
+class Grid(C.Structure):
+    _fields_ = [("data", C.c_void_p), ("origin", C.c_float * 3), ("basis", C.c_float * 9),
+                ("basis_inv", C.c_float * 9), ("dims", C.c_int64 * 3),
+                ("boundary_condition", C.c_int)]
+
+
+class GridTerm(C.Structure):
+    _fields_ = [("grid_id", C.c_int), ("scale", C.c_float), ("scale_slope", C.c_float),
+                ("boundary_condition", C.c_int)]
+
+
+class Types(C.Structure):
+    _fields_ = [("num_types", C.c_int), ("charge", C.c_void_p), ("diffusion4", C.c_void_p),
+                ("pmf_offset", C.c_void_p), ("pmf_count", C.c_void_p), ("terms", C.c_void_p),
+                ("force_grid_id4", C.c_void_p), ("force_grid_scale4", C.c_void_p)]
+
+
+def _ptr(a):
+    return a.ctypes.data_as(C.c_void_p) if a is not None else None
+
+
+class TableSet:
+    """Concatenated float tables plus per-table metadata, kept alive together."""
+
+    def __init__(self, tables, periodic=False):
+        # tables: list of (values float32[size], start, step_inv)
+        vals = [np.ascontiguousarray(t[0], dtype=np.float32) for t in tables]
+        self.values = np.concatenate(vals) if vals else np.zeros(1, np.float32)
+        self.offsets = np.zeros(len(vals), np.uint32)
+        off = 0
+        for k, v in enumerate(vals):
+            self.offsets[k] = off
+            off += len(v)
+        self.sizes = np.array([len(v) for v in vals], np.uint32)
+        self.starts = np.array([t[1] for t in tables], np.float32)
+        self.step_invs = np.array([t[2] for t in tables], np.float32)
+        self.periodic = periodic
+        self.structs = (Table * max(1, len(vals)))()
+        for k in range(len(vals)):
+            self.structs[k].pot = self.values.ctypes.data + 4 * int(self.offsets[k])
+            self.structs[k].step_inv = float(self.step_invs[k])
+            self.structs[k].size = int(self.sizes[k])
+            self.structs[k].start = float(self.starts[k])
+            self.structs[k].is_periodic = int(periodic)
+
+    def __len__(self):
+        return len(self.sizes)
+
+
+class TypeSet:
+    """Per-type BD data (charge, diffusion, PMF terms, force grids)."""
+
+    def __init__(self, charge, diffusion, pmf_terms_per_type=None, force_grid_id=None,
+                 force_grid_scale=None):
+        t = len(charge)
+        self.charge = np.ascontiguousarray(charge, np.float32)
+        d = np.zeros((t, 4), np.float32)
+        d[:, :3] = np.asarray(diffusion, np.float32).reshape(t, 3)
+        self.diffusion4 = d
+        pmf_terms_per_type = pmf_terms_per_type or [[] for _ in range(t)]
+        self.pmf_offset = np.zeros(t, np.int32)
+        self.pmf_count = np.zeros(t, np.int32)
+        flat = []
+        for k, terms in enumerate(pmf_terms_per_type):
+            self.pmf_offset[k] = len(flat)
+            self.pmf_count[k] = len(terms)
+            flat.extend(terms)  # (grid_id, scale, scale_slope, bc)
+        self.terms_flat = np.array(flat, np.float32).reshape(-1, 4) if flat else np.zeros((1, 4), np.float32)
+        self.terms = (GridTerm * max(1, len(flat)))()
+        for k, (gid, s, sl, bc) in enumerate(flat):
+            self.terms[k].grid_id, self.terms[k].scale = int(gid), float(s)
+            self.terms[k].scale_slope, self.terms[k].boundary_condition = float(sl), int(bc)
+        self.n_terms = len(flat)
+        fg = np.full((t, 4), -1, np.int32)
+        if force_grid_id is not None:
+            fg[:, :3] = np.asarray(force_grid_id, np.int32).reshape(t, 3)
+        self.force_grid_id4 = fg
+        fs = np.zeros((t, 4), np.float32)
+        if force_grid_scale is not None:
+            fs[:, :3] = np.asarray(force_grid_scale, np.float32).reshape(t, 3)
+        self.force_grid_scale4 = fs
+        self.struct = Types(t, _ptr(self.charge), _ptr(self.diffusion4), _ptr(self.pmf_offset),
+                            _ptr(self.pmf_count), C.cast(self.terms, C.c_void_p),
+                            _ptr(self.force_grid_id4), _ptr(self.force_grid_scale4))
+
+
+class GridSet:
+    """Dense grids: list of dicts with data (nx,ny,nz float32), origin, basis (3x3, columns
+    are basis vectors), boundary_condition."""
+
+    def __init__(self, grids):
+        self.arrays = []
+        self.structs = (Grid * max(1, len(grids)))()
+        for k, g in enumerate(grids):
+            data = np.ascontiguousarray(g["data"], np.float32)
+            self.arrays.append(data)
+            s = self.structs[k]
+            s.data = data.ctypes.data
+            basis = np.asarray(g["basis"], np.float32)
+            binv = np.asarray(g.get("basis_inv", np.linalg.inv(basis.astype(np.float64))), np.float32)
+            for a in range(3):
+                s.origin[a] = float(g["origin"][a])
+                s.dims[a] = int(data.shape[a])
+            # column-major: element [3*c + r] = M[r, c]
+            for c in range(3):
+                for r in range(3):
+                    s.basis[3 * c + r] = float(basis[r, c])
+                    s.basis_inv[3 * c + r] = float(binv[r, c])
+            s.boundary_condition = int(g.get("boundary_condition", 0))
+        self.n = len(grids)
+
+    def ptr(self):
+        return C.cast(self.structs, C.c_void_p) if self.n else None
+
+
+class Oracle:
+    """C restatement of the reference algorithm."""
+
+    def __init__(self, path: str = ORACLE_SO):
+        if not os.path.exists(path):
+            build_oracle()
+        L = self.lib = C.CDLL(path)
+        vp, sz, f, i, u32, u64 = C.c_void_p, C.c_size_t, C.c_float, C.c_int, C.c_uint32, C.c_uint64
+        L.or_wrap_diff_scalar.restype = f
+        L.or_wrap_diff_scalar.argtypes = [f, f]
+        L.or_wrap_scalar.restype = f
+        L.or_wrap_scalar.argtypes = [f, f, f]
+        L.or_wrap_diff.argtypes = [vp, vp, vp, sz]
+        L.or_wrap.argtypes = [vp, vp, vp, sz]
+        L.or_morton_key.restype = u32
+        L.or_morton_encode.argtypes = [vp, sz, vp, vp, vp, vp]
+        L.or_sort_pairs.argtypes = [vp, vp, sz]
+        L.or_inverse.argtypes = [vp, vp, sz]
+        L.or_gather4.argtypes = [vp, vp, vp, sz]
+        L.or_morton_domain.argtypes = [vp, vp, sz, vp, vp]
+        L.or_select_cell_grid.argtypes = [vp, f, sz, sz, vp, vp, vp]
+        L.or_cell_ranges.argtypes = [vp, sz, i, vp, vp]
+        L.or_cell_neighbors.argtypes = [vp, i, vp, i, vp]
+        L.or_neighbor_walk.restype = u64
+        L.or_neighbor_walk.argtypes = [vp, vp, vp, vp, vp, vp, i, i, f, sz, vp, vp, vp, sz, vp,
+                                       vp, u64]
+        L.or_build_pairlist.restype = u64
+        L.or_build_pairlist.argtypes = [vp, sz, vp, f, vp, vp, sz, vp, vp, u64, vp]
+        L.or_pair_hash.restype = u64
+        L.or_pair_hash.argtypes = [i, i]
+        L.or_exclusion_csr.argtypes = [vp, sz, vp, vp, vp]
+        L.or_max_displacement.restype = f
+        L.or_max_displacement.argtypes = [vp, vp, sz, vp]
+        L.or_table_lookup.argtypes = [vp, f, vp, vp]
+        L.or_resolve_tags.argtypes = [vp, sz, vp, vp, i, vp]
+        L.or_pair_forces.argtypes = [vp, sz, vp, vp, vp, vp, f, i, vp, vp, vp]
+        L.or_bond_forces.argtypes = [vp, vp, sz, vp, vp, vp, i, vp, vp, vp]
+        L.or_angle_forces.argtypes = [vp, vp, sz, vp, vp, vp, i, vp, vp, vp]
+        L.or_pair_energy_f64.restype = C.c_double
+        L.or_pair_energy_f64.argtypes = [vp, sz, vp, vp, vp, vp, f]
+        L.or_grid_value.restype = f
+        L.or_grid_value.argtypes = [vp, vp, i]
+        L.or_grid_gradient.argtypes = [vp, vp, i, vp]
+        L.or_position_force.argtypes = [vp, i, vp, vp, vp, vp]
+        L.or_philox4x32_10.argtypes = [u64, u32, u32, u32, u32, vp]
+        L.or_u01.restype = f
+        L.or_u01.argtypes = [u32]
+        L.or_bd_seed.restype = u64
+        L.or_bd_seed.argtypes = [u64, u64, u64]
+        L.or_bd_integrate.argtypes = [vp, vp, vp, vp, sz, vp, vp, vp, f, f, u64, u64, u32, vp, vp]
+
+    # -- Morton sort ------------------------------------------------------
+    def morton_domain(self, box: Box, pos4):
+        bmin = np.zeros(3, np.float32)
+        bmax = np.zeros(3, np.float32)
+        self.lib.or_morton_domain(C.byref(box), _ptr(pos4), len(pos4), _ptr(bmin), _ptr(bmax))
+        return bmin, bmax
+
+    def morton_encode(self, pos4, bmin, bmax):
+        n = len(pos4)
+        keys = np.zeros(n, np.uint32)
+        idx = np.zeros(n, np.uint32)
+        self.lib.or_morton_encode(_ptr(pos4), n, _ptr(np.asarray(bmin, np.float32)),
+                                  _ptr(np.asarray(bmax, np.float32)), _ptr(keys), _ptr(idx))
+        return keys, idx
+
+    def sort_pairs(self, keys, vals):
+        k = np.array(keys, np.uint32)
+        v = np.array(vals, np.uint32)
+        self.lib.or_sort_pairs(_ptr(k), _ptr(v), len(k))
+        return k, v
+
+    def inverse(self, sorted_idx):
+        inv = np.zeros(len(sorted_idx), np.uint32)
+        self.lib.or_inverse(_ptr(np.ascontiguousarray(sorted_idx, np.uint32)), _ptr(inv), len(inv))
+        return inv
+
+    def gather4(self, pos4, sorted_idx):
+        out = np.zeros_like(pos4)
+        self.lib.or_gather4(_ptr(pos4), _ptr(out), _ptr(np.ascontiguousarray(sorted_idx, np.uint32)),
+                            len(pos4))
+        return out
+
+    def sort_particles(self, box: Box, pos4):
+        """Domain + encode + sort + inverse + gather (ZOrderSort::sort_particles)."""
+        bmin, bmax = self.morton_domain(box, pos4)
+        keys, idx = self.morton_encode(pos4, bmin, bmax)
+        keys, s2o = self.sort_pairs(keys, idx)
+        inv = self.inverse(s2o)
+        return dict(bmin=bmin, bmax=bmax, keys=keys, sorted_to_orig=s2o, inverse=inv,
+                    sorted_pos=self.gather4(pos4, s2o))
+
+    # -- pairlist ---------------------------------------------------------
+    def select_cell_grid(self, extent, cutoff, n, max_pairs):
+        m = C.c_int()
+        radii = np.zeros(3, np.int32)
+        slots = C.c_int()
+        self.lib.or_select_cell_grid(_ptr(np.asarray(extent, np.float32)), C.c_float(cutoff), n,
+                                     max_pairs, C.byref(m), _ptr(radii), C.byref(slots))
+        return m.value, radii, slots.value
+
+    def cell_ranges(self, keys, shift, num_cells):
+        b = np.zeros(num_cells, np.uint32)
+        e = np.zeros(num_cells, np.uint32)
+        self.lib.or_cell_ranges(_ptr(keys), len(keys), shift, _ptr(b), _ptr(e))
+        return b, e
+
+    def cell_neighbors(self, m, radii, npc, box_len):
+        t = np.zeros((1 << (3 * m)) * npc, np.uint32)
+        self.lib.or_cell_neighbors(_ptr(t), m, _ptr(np.asarray(radii, np.int32)), npc,
+                                   _ptr(np.asarray(box_len, np.float32)))
+        return t
+
+    def build_pairlist(self, pos4, box: Box, rc_list, excl=None, rigid_body_id=None,
+                       want_pairs=True, max_pairs=None):
+        """Pair set within rc_list: returns (pairs int32[P,2] sorted lexicographically
+        or None, count, checksum)."""
+        n = len(pos4)
+        off, nb, excl_n = (None, None, 0) if excl is None else excl
+        if want_pairs and max_pairs is None:
+            cnt = self.lib.or_build_pairlist(_ptr(pos4), n, C.byref(box), C.c_float(rc_list),
+                                             _ptr(off), _ptr(nb), excl_n, _ptr(rigid_body_id),
+                                             None, 0, None)
+            max_pairs = int(cnt)
+        buf = np.zeros((max_pairs if want_pairs else 0, 2), np.int32)
+        cs = C.c_uint64()
+        cnt = self.lib.or_build_pairlist(_ptr(pos4), n, C.byref(box), C.c_float(rc_list),
+                                         _ptr(off), _ptr(nb), excl_n, _ptr(rigid_body_id),
+                                         _ptr(buf) if want_pairs else None,
+                                         max_pairs if want_pairs else 0, C.byref(cs))
+        pairs = None
+        if want_pairs:
+            pairs = buf[: min(int(cnt), max_pairs)]
+            order = np.lexsort((pairs[:, 1], pairs[:, 0]))
+            pairs = np.ascontiguousarray(pairs[order])
+        return pairs, int(cnt), int(cs.value)
+
+    def pair_hash_sum(self, pairs):
+        """Order-independent checksum of a pair set (same as build_pairlist's)."""
+        a = np.minimum(pairs[:, 0], pairs[:, 1]).astype(np.uint64)
+        b = np.maximum(pairs[:, 0], pairs[:, 1]).astype(np.uint64)
+        z = (a << np.uint64(32)) | b
+        with np.errstate(over="ignore"):
+            z = z + np.uint64(0x9E3779B97F4A7C15)
+            z = (z ^ (z >> np.uint64(30))) * np.uint64(0xBF58476D1CE4E5B9)
+            z = (z ^ (z >> np.uint64(27))) * np.uint64(0x94D049BB133111EB)
+            z = z ^ (z >> np.uint64(31))
+            return int(np.sum(z, dtype=np.uint64))
+
+    def exclusion_csr(self, pairs):
+        pairs = np.ascontiguousarray(pairs, np.int32).reshape(-1, 2)
+        mx = int(pairs.max()) if len(pairs) else 0
+        off = np.zeros(mx + 2, np.int32)
+        nb = np.zeros(max(1, 2 * len(pairs)), np.int32)
+        npart = C.c_size_t()
+        self.lib.or_exclusion_csr(_ptr(pairs), len(pairs), _ptr(off), _ptr(nb), C.byref(npart))
+        return off, nb, npart.value
+
+    def max_displacement(self, cur4, prev4, box_len):
+        return self.lib.or_max_displacement(_ptr(cur4), _ptr(prev4), len(cur4),
+                                            _ptr(np.asarray(box_len, np.float32)))
+
+    # -- forces -----------------------------------------------------------
+    def table_lookup(self, tables: TableSet, k, x):
+        fo, en = C.c_float(), C.c_float()
+        self.lib.or_table_lookup(C.byref(tables.structs[k]), C.c_float(x), C.byref(fo), C.byref(en))
+        return fo.value, en.value
+
+    def resolve_tags(self, pairs, type_ids, term_matrix, num_types):
+        tags = np.zeros(len(pairs), np.uint32)
+        self.lib.or_resolve_tags(_ptr(pairs), len(pairs), _ptr(type_ids), _ptr(term_matrix),
+                                 num_types, _ptr(tags))
+        return tags
+
+    def pair_forces(self, pairs, pos4, tags, tables: TableSet, box: Box, cutoff_sq,
+                    get_energy=True):
+        n = len(pos4)
+        fe4 = np.zeros((n, 4), np.float32)
+        fe64 = np.zeros((n, 4), np.float64)
+        fabs = np.zeros(n, np.float64)
+        self.lib.or_pair_forces(_ptr(pairs), len(pairs), _ptr(pos4), _ptr(tags),
+                                C.cast(tables.structs, C.c_void_p), C.byref(box),
+                                C.c_float(cutoff_sq), int(get_energy), _ptr(fe4), _ptr(fe64),
+                                _ptr(fabs))
+        return fe4, fe64, fabs
+
+    def pair_energy_f64(self, pairs, pos4, tags, tables: TableSet, box: Box, cutoff_sq):
+        return self.lib.or_pair_energy_f64(_ptr(pairs), len(pairs), _ptr(pos4), _ptr(tags),
+                                           C.cast(tables.structs, C.c_void_p), C.byref(box),
+                                           C.c_float(cutoff_sq))
+
+    def bond_forces(self, bonds, table_idx, pos4, tables: TableSet, box: Box, get_energy=True,
+                    fe4=None, fe64=None, fabs=None):
+        n = len(pos4)
+        fe4 = np.zeros((n, 4), np.float32) if fe4 is None else fe4
+        fe64 = np.zeros((n, 4), np.float64) if fe64 is None else fe64
+        fabs = np.zeros(n, np.float64) if fabs is None else fabs
+        self.lib.or_bond_forces(_ptr(bonds), _ptr(table_idx), len(bonds), _ptr(pos4),
+                                C.cast(tables.structs, C.c_void_p), C.byref(box), int(get_energy),
+                                _ptr(fe4), _ptr(fe64), _ptr(fabs))
+        return fe4, fe64, fabs
+
+    def angle_forces(self, angles4, table_idx, pos4, tables: TableSet, box: Box, get_energy=True,
+                     fe4=None, fe64=None, fabs=None):
+        n = len(pos4)
+        fe4 = np.zeros((n, 4), np.float32) if fe4 is None else fe4
+        fe64 = np.zeros((n, 4), np.float64) if fe64 is None else fe64
+        fabs = np.zeros(n, np.float64) if fabs is None else fabs
+        self.lib.or_angle_forces(_ptr(angles4), _ptr(table_idx), len(angles4), _ptr(pos4),
+                                 C.cast(tables.structs, C.c_void_p), C.byref(box), int(get_energy),
+                                 _ptr(fe4), _ptr(fe64), _ptr(fabs))
+        return fe4, fe64, fabs
+
+    # -- grid, Philox, BD -------------------------------------------------
+    def philox(self, seed, ctr0, ctr1, ctr2, internal=0):
+        out = np.zeros(4, np.uint32)
+        self.lib.or_philox4x32_10(seed, ctr0, ctr1, ctr2, internal, _ptr(out))
+        return out
+
+    def bd_seed(self, seed, patch_id, step):
+        return int(self.lib.or_bd_seed(seed, patch_id, step))
+
+    def position_force(self, pos3, type_id, types: TypeSet, grids: GridSet, efield=(0, 0, 0)):
+        out = np.zeros(4, np.float32)
+        p = np.asarray(pos3, np.float32)
+        self.lib.or_position_force(_ptr(p), int(type_id), C.byref(types.struct), grids.ptr(),
+                                   _ptr(np.asarray(efield, np.float32)), _ptr(out))
+        return out
+
+    def bd_integrate(self, pos4, fe4, type_ids, flags, types: TypeSet, grids, box: Box, dt, kT,
+                     step, base_seed, base_ctr=0, efield=(0, 0, 0), want_noise=False):
+        """In-place on copies; returns (pos4, fe4, noise4 or None)."""
+        pos = np.array(pos4, np.float32)
+        fe = np.array(fe4, np.float32)
+        noise = np.zeros_like(pos) if want_noise else None
+        self.lib.or_bd_integrate(_ptr(pos), _ptr(fe), _ptr(np.ascontiguousarray(type_ids, np.int32)),
+                                 _ptr(flags), len(pos), C.byref(types.struct),
+                                 grids.ptr() if grids is not None else None, C.byref(box),
+                                 C.c_float(dt), C.c_float(kT), step, base_seed, base_ctr,
+                                 _ptr(np.asarray(efield, np.float32)), _ptr(noise))
+        return pos, fe, noise
+
+
+class RefGrid(C.Structure):
+    _fields_ = [("data", C.c_void_p), ("origin", C.c_float * 3), ("basis", C.c_float * 9),
+                ("basis_inv", C.c_float * 9), ("dims", C.c_int64 * 3),
+                ("boundary_condition", C.c_int)]
+
+
+def ref_available(path: str = REF_SO) -> bool:
+    return os.path.exists(path)
+
+
+class RefHarness:
+    """The reference's own functors, host-compiled (see oracle/ref_harness)."""
+
+    def __init__(self, path: str = REF_SO):
+        L = self.lib = C.CDLL(path)
+        vp, sz, f, i, u32, u64 = C.c_void_p, C.c_size_t, C.c_float, C.c_int, C.c_uint32, C.c_uint64
+        L.ref_morton_encode.argtypes = [vp, sz, vp, vp, vp, vp, i]
+        L.ref_sort_pairs.argtypes = [vp, vp, sz]
+        L.ref_inverse.argtypes = [vp, vp, sz]
+        L.ref_reorder_pos.argtypes = [vp, vp, vp, sz]
+        L.ref_cell_ranges.argtypes = [vp, sz, i, vp, vp]
+        L.ref_cell_neighbors.argtypes = [vp, sz, i, vp, i, vp]
+        L.ref_neighbor_walk.restype = u32
+        L.ref_neighbor_walk.argtypes = [vp, vp, vp, vp, vp, vp, vp, sz, f, sz, i, i, i, vp, vp, vp,
+                                        vp, vp, sz, vp]
+        L.ref_resolve_tags.argtypes = [vp, sz, vp, vp, sz, vp, i]
+        L.ref_pair_forces.argtypes = [vp, sz, vp, vp, vp, vp, vp, vp, vp, vp, vp, i, vp, vp, vp,
+                                      i, f, u32]
+        L.ref_bond_forces.argtypes = [vp, vp, vp, sz, vp, vp, vp, vp, vp, vp, vp, i, vp, vp, vp, i]
+        L.ref_angle_forces.argtypes = [vp, vp, vp, sz, vp, vp, vp, vp, vp, vp, vp, i, vp, vp, vp, i]
+        L.ref_bd_integrate.argtypes = [vp, vp, vp, vp, sz, i, vp, vp, vp, vp, vp, i, vp, vp, vp, i,
+                                       vp, vp, vp, f, f, u64, u64, u32, vp, i]
+        L.ref_philox_int4.argtypes = [u64, u32, u32, u32, i, vp]
+        L.ref_philox_float4.argtypes = [u64, u32, u32, u32, i, vp]
+        L.ref_max_displacement.restype = f
+        L.ref_max_displacement.argtypes = [vp, vp, sz, vp]
+        L.ref_wrap_diff.argtypes = [vp, vp, vp, vp, vp, sz]
+        L.ref_wrap.argtypes = [vp, vp, vp, vp, vp, sz]
+        L.ref_table_lookup.argtypes = [f, vp, u32, f, f, i, vp]
+
+    @staticmethod
+    def _box(box: Box):
+        o = np.array(list(box.origin), np.float32)
+        s = np.array(list(box.size), np.float32)
+        p = np.array(list(box.periodic), np.int32)
+        return o, s, p
+
+    def morton_encode(self, pos4, bmin, bmax, nthreads=1):
+        n = len(pos4)
+        keys = np.zeros(n, np.uint32)
+        idx = np.zeros(n, np.uint32)
+        self.lib.ref_morton_encode(_ptr(pos4), n, _ptr(np.asarray(bmin, np.float32)),
+                                   _ptr(np.asarray(bmax, np.float32)), _ptr(keys), _ptr(idx),
+                                   nthreads)
+        return keys, idx
+
+    def sort_pairs(self, keys, vals):
+        k = np.array(keys, np.uint32)
+        v = np.array(vals, np.uint32)
+        self.lib.ref_sort_pairs(_ptr(k), _ptr(v), len(k))
+        return k, v
+
+    def inverse(self, s):
+        inv = np.zeros(len(s), np.uint32)
+        self.lib.ref_inverse(_ptr(s), _ptr(inv), len(s))
+        return inv
+
+    def reorder_pos(self, pos4, s):
+        out = np.zeros_like(pos4)
+        self.lib.ref_reorder_pos(_ptr(pos4), _ptr(out), _ptr(s), len(s))
+        return out
+
+    def cell_ranges(self, keys, shift, num_cells):
+        b = np.zeros(num_cells, np.uint32)
+        e = np.zeros(num_cells, np.uint32)
+        self.lib.ref_cell_ranges(_ptr(keys), len(keys), shift, _ptr(b), _ptr(e))
+        return b, e
+
+    def cell_neighbors(self, m, radii, npc, box_len):
+        t = np.zeros((1 << (3 * m)) * npc, np.uint32)
+        self.lib.ref_cell_neighbors(_ptr(t), 1 << (3 * m), m, _ptr(np.asarray(radii, np.int32)),
+                                    npc, _ptr(np.asarray(box_len, np.float32)))
+        return t
+
+    def neighbor_walk(self, sorted_pos, keys, s2o, begin, end, table, cutoff_sq, npc, shift,
+                      box: Box, excl=None, rigid_body_id=None, tpp=4, max_pairs=None):
+        n = len(keys)
+        o, s, p = self._box(box)
+        off, nb, excl_n = (None, None, 0) if excl is None else excl
+        max_pairs = max_pairs if max_pairs is not None else n * 400
+        buf = np.zeros((max_pairs + 1, 2), np.int32)
+        cnt = self.lib.ref_neighbor_walk(_ptr(sorted_pos), _ptr(keys), _ptr(s2o), _ptr(begin),
+                                         _ptr(end), _ptr(table), _ptr(buf), max_pairs,
+                                         C.c_float(cutoff_sq), n, npc, min(tpp, npc), shift,
+                                         _ptr(o), _ptr(s), _ptr(p), _ptr(off), _ptr(nb), excl_n,
+                                         _ptr(rigid_body_id))
+        return buf[1: cnt + 1], int(cnt)
+
+    def resolve_tags(self, pairs, type_ids, term_matrix, num_types):
+        tags = np.zeros(len(pairs), np.uint32)
+        self.lib.ref_resolve_tags(_ptr(pairs), len(pairs), _ptr(type_ids), _ptr(term_matrix),
+                                  num_types, _ptr(tags), 1)
+        return tags
+
+    def pair_forces(self, pairs, pos4, type_ids, tags, tables: TableSet, box: Box, cutoff_sq,
+                    get_energy=True, enabled_terms=0xFF):
+        fe = np.zeros((len(pos4), 4), np.float32)
+        o, s, p = self._box(box)
+        self.lib.ref_pair_forces(_ptr(pairs), len(pairs), _ptr(pos4), _ptr(type_ids), _ptr(fe),
+                                 _ptr(tags), _ptr(tables.values), _ptr(tables.offsets),
+                                 _ptr(tables.sizes), _ptr(tables.starts), _ptr(tables.step_invs),
+                                 len(tables), _ptr(o), _ptr(s), _ptr(p), int(get_energy),
+                                 C.c_float(cutoff_sq), enabled_terms)
+        return fe
+
+    def bond_forces(self, bonds, table_idx, pos4, tables: TableSet, box: Box, get_energy=True,
+                    fe=None):
+        fe = np.zeros((len(pos4), 4), np.float32) if fe is None else fe
+        forms = np.ones(len(bonds), np.int32)  # InteractionForm::Tabulated (SimParam.h:174)
+        o, s, p = self._box(box)
+        self.lib.ref_bond_forces(_ptr(bonds), _ptr(table_idx), _ptr(forms), len(bonds), _ptr(pos4),
+                                 _ptr(fe), _ptr(tables.values), _ptr(tables.offsets),
+                                 _ptr(tables.sizes), _ptr(tables.starts), _ptr(tables.step_invs),
+                                 len(tables), _ptr(o), _ptr(s), _ptr(p), int(get_energy))
+        return fe
+
+    def angle_forces(self, angles4, table_idx, pos4, tables: TableSet, box: Box, get_energy=True,
+                     fe=None):
+        fe = np.zeros((len(pos4), 4), np.float32) if fe is None else fe
+        forms = np.ones(len(angles4), np.int32)  # InteractionForm::Tabulated
+        o, s, p = self._box(box)
+        self.lib.ref_angle_forces(_ptr(angles4), _ptr(table_idx), _ptr(forms), len(angles4),
+                                  _ptr(pos4), _ptr(fe), _ptr(tables.values), _ptr(tables.offsets),
+                                  _ptr(tables.sizes), _ptr(tables.starts), _ptr(tables.step_invs),
+                                  len(tables), _ptr(o), _ptr(s), _ptr(p), int(get_energy))
+        return fe
+
+    def bd_integrate(self, pos4, fe4, type_ids, flags, types: TypeSet, grids, box: Box, dt, kT,
+                     step, base_seed, base_ctr=0, efield=(0, 0, 0), nthreads=1):
+        pos = np.array(pos4, np.float32)
+        fe = np.array(fe4, np.float32)
+        o, s, p = self._box(box)
+        tid = np.ascontiguousarray(type_ids, np.int32)
+        fl = np.zeros(len(pos), np.uint32) if flags is None else np.ascontiguousarray(flags, np.uint32)
+        rg = None
+        ng = 0
+        if grids is not None and grids.n:
+            rg = (RefGrid * grids.n)()
+            for k in range(grids.n):
+                C.memmove(C.byref(rg[k]), C.byref(grids.structs[k]), C.sizeof(RefGrid))
+            ng = grids.n
+        self.lib.ref_bd_integrate(_ptr(pos), _ptr(fe), _ptr(tid), _ptr(fl), len(pos),
+                                  len(types.charge), _ptr(types.charge), _ptr(types.diffusion4),
+                                  _ptr(types.pmf_offset), _ptr(types.pmf_count),
+                                  _ptr(types.terms_flat), types.n_terms,
+                                  _ptr(types.force_grid_id4), _ptr(types.force_grid_scale4),
+                                  C.cast(rg, C.c_void_p) if rg is not None else None, ng,
+                                  _ptr(o), _ptr(s), _ptr(p), C.c_float(dt), C.c_float(kT), step,
+                                  base_seed, base_ctr, _ptr(np.asarray(efield, np.float32)),
+                                  nthreads)
+        return pos, fe
+
+    def philox_int4(self, seed, ctr, global_seed, ctr1, ndraw=1):
+        out = np.zeros((ndraw, 4), np.uint32)
+        self.lib.ref_philox_int4(seed, ctr, global_seed, ctr1, ndraw, _ptr(out))
+        return out
+
+    def philox_float4(self, seed, ctr, global_seed, ctr1, ndraw=1):
+        out = np.zeros((ndraw, 4), np.float32)
+        self.lib.ref_philox_float4(seed, ctr, global_seed, ctr1, ndraw, _ptr(out))
+        return out
+
+    def max_displacement(self, cur4, prev4, box_len):
+        return self.lib.ref_max_displacement(_ptr(cur4), _ptr(prev4), len(cur4),
+                                             _ptr(np.asarray(box_len, np.float32)))
+
+    def wrap_diff(self, box: Box, v4):
+        o, s, p = self._box(box)
+        out = np.zeros_like(v4)
+        self.lib.ref_wrap_diff(_ptr(o), _ptr(s), _ptr(p), _ptr(v4), _ptr(out), len(v4))
+        return out
+
+    def wrap(self, box: Box, v4):
+        o, s, p = self._box(box)
+        out = np.zeros_like(v4)
+        self.lib.ref_wrap(_ptr(o), _ptr(s), _ptr(p), _ptr(v4), _ptr(out), len(v4))
+        return out
