@@ -1,0 +1,221 @@
+/*
+ * marsb200.h -- C ABI of libmarsb200.so, the B200 (sm_100a) implementation of
+ * the MARS-MD Brownian-dynamics force-and-integrate path.
+ *
+ * Each entry point replaces one reference interface on that path (paths are
+ * relative to the MARS-MD source tree); the reference reaches them through
+ * Backend/Kernels.h launch_kernel -> launch_cuda_kernel<Functor>
+ * (src/Backend/Kernels.h:35-83, src/Backend/CUDA/KernelHelper.cuh:129-183),
+ * which this library replaces on this path only.
+ *
+ * Conventions
+ *   - Every function returns 0 (MB2_OK) or a positive MB2_ERR_* code; the
+ *     message is available from mb2_last_error(ctx). No C++ exception crosses
+ *     this boundary (the reference throws MARS::Exception instead).
+ *   - Particle arrays are caller-owned DEVICE pointers in the reference's
+ *     layouts: positions and ForceEnergy are float4 rows (x, y, z, w), type ids
+ *     int32, flags uint32 (src/Objects/DeviceParticle.h:18-40). Vector3 is
+ *     16 bytes (src/Types/Vector3.h:41). Table values, term matrices and other
+ *     set-up data are HOST pointers, copied in.
+ *   - `stream` is a cudaStream_t (NULL = legacy default stream). Work is
+ *     enqueued asynchronously unless a function returns a host value (noted).
+ *   - Scratch (sort buffers, cell tables, the pair list) belongs to the
+ *     context and grows on demand with cudaMalloc.
+ */
+#ifndef MARSB200_H
+#define MARSB200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#if defined(__GNUC__)
+#define MB2_API __attribute__((visibility("default")))
+#else
+#define MB2_API
+#endif
+
+#define MB2_OK 0
+#define MB2_ERR_ARG 1      /* invalid argument or call order */
+#define MB2_ERR_CUDA 2     /* CUDA runtime error */
+#define MB2_ERR_CAPACITY 3 /* more particles/pairs than the context allows */
+#define MB2_ERR_STATE 4    /* required set-up missing (box, tables, pairlist) */
+
+typedef struct mb2_context mb2_context;
+
+/* Library version (major * 100 + minor). */
+MB2_API int mb2_version(void);
+
+/* Create a context on `device` for up to `max_particles` particles.
+ * Replaces the Pairlist/ZOrderPairlist/ZOrderSort constructors
+ * (src/PatchOperation/Pairlist.h:66-74, PairListKernels/ZOrderPairlist.cpp:83-100,
+ * ZOrderKernels/ZOrderSort.cpp:7-38). */
+MB2_API int mb2_create(int device, uint32_t max_particles, mb2_context** out);
+MB2_API int mb2_destroy(mb2_context* ctx);
+/* Last error message of this context ("" if none). */
+MB2_API const char* mb2_last_error(const mb2_context* ctx);
+
+/* Orthogonal periodic box. Replaces Pairlist::set_periodic_box
+ * (src/PatchOperation/Pairlist.h:118-120) and the PeriodicBox by-value
+ * argument of launch_BD (src/PatchOperation/Integrator.h:26-54). */
+MB2_API int mb2_set_box(mb2_context* ctx, const float origin[3], const float size[3],
+                const int periodic[3]);
+
+/* --- Z-order sort ---------------------------------------------------------
+ * ZOrderSort::sort_particles + reorder_data (ZOrderKernels/ZOrderSort.cpp:40-70,
+ * ZOrderSort.h:316-339): Morton keys against [bmin, bmax], stable sort, inverse
+ * map, gathered positions. Any output pointer may be NULL. Device pointers. */
+MB2_API int mb2_sort_morton(mb2_context* ctx, const float* pos4, uint32_t n, const float bmin[3],
+                    const float bmax[3], uint32_t* keys_out, uint32_t* sorted_to_orig_out,
+                    uint32_t* inverse_out, float* sorted_pos4_out, void* stream);
+
+/* Stable sort of (key, value) pairs by the 32-bit key, in place. Replaces
+ * device_radix_sort_pairs_cub (ZOrderKernels/CUDASort.cu:13-98). */
+MB2_API int mb2_radix_sort_pairs(mb2_context* ctx, uint32_t* keys, uint32_t* vals, uint32_t n,
+                         void* stream);
+
+/* --- pairlist --------------------------------------------------------------
+ * Exclusion CSR (device pointers, borrowed until the next build): replaces
+ * Pairlist::set_exclusions with ExclusionView (Pairlist.h:125-127,
+ * src/Interactions/DeviceExclusions.h:22-75). offsets has num_particles + 1
+ * entries; rigid_body_id may be NULL. Pass offsets = NULL to clear. */
+MB2_API int mb2_set_exclusions(mb2_context* ctx, const int* offsets, const int* neighbors,
+                       uint32_t num_particles, const int* rigid_body_id);
+
+/* Build the half pairlist within `pairlist_cutoff`. Replaces
+ * ZOrderPairlist::build_pairlist (PairListKernels/ZOrderPairlist.cpp:102-178).
+ * Synchronises `stream` once (to size the list); returns the pair count. */
+MB2_API int mb2_build_pairlist(mb2_context* ctx, const float* pos4, const int* type_ids, uint32_t n,
+                       float pairlist_cutoff, void* stream, uint64_t* num_pairs);
+
+/* Pair count of the last build (Pairlist::get_num_pairs, Pairlist.h:139-141). */
+MB2_API int mb2_num_pairs(const mb2_context* ctx, uint64_t* num_pairs);
+
+/* Write the pairs of the last build as int2 (min, max) original indices,
+ * the reference's neighbor_pairs_ format (Pairlist::get_neighbor_pairs,
+ * Pairlist.h:132-134). `capacity` in pairs; fails if smaller than the count. */
+MB2_API int mb2_export_pairs(mb2_context* ctx, int* pairs2, uint64_t capacity, void* stream);
+
+/* Skin check: largest minimum-image displacement since the last build; sets
+ * *needs = (max > skin / 2). Replaces ZOrderPairlist::needs_update
+ * (ZOrderPairlist.cpp:184-190, ZOrderSort.cpp:173-198). Synchronises. */
+MB2_API int mb2_needs_update(mb2_context* ctx, const float* pos4, uint32_t n, float skin, void* stream,
+                     float* max_displacement, int* needs);
+
+/* --- pair forces -----------------------------------------------------------
+ * Type-pair tag matrix and tabulated tables. Replaces
+ * DevicePairNonBondedInteractions::copy_pairwise_from_host and
+ * link_pairwise_tables (src/Interactions/DevicePairNonBondedInteraction.h:97-199).
+ * term_matrix: host uint32 [num_types * num_types], tags as make_pair_tag
+ * (bit 5 = tabulated, table index << 8; src/Interactions/Nonbonded/Pairwise.h:31-35).
+ * values: host float, tables concatenated; sizes/starts/step_invs per table. */
+MB2_API int mb2_set_pair_tables(mb2_context* ctx, int num_types, const uint32_t* term_matrix,
+                        int num_tables, const float* values, const uint32_t* sizes,
+                        const float* starts, const float* step_invs);
+
+/* Tabulated pair forces over the last pairlist, ACCUMULATED into
+ * force_energy (original order; energy halves into .w when get_energy).
+ * Replaces launch_resolve_pair_tables + launch_pairwise_nonbonded
+ * (src/Interactions/NonBondedInteraction.h:205-296) with the tabulated term. */
+MB2_API int mb2_pair_forces(mb2_context* ctx, const float* pos4, const int* type_ids,
+                    float* force_energy4, uint32_t n, float cutoff, int get_energy,
+                    void* stream);
+
+/* FP64 reductions of the last force calls made with get_energy: pair energy,
+ * pair virial (sum of r . f), bond energy, angle energy. Synchronises.
+ * New on this path: the reference sums per-particle floats on the host
+ * (src/SimManager.cpp:1000-1075). */
+MB2_API int mb2_energies(mb2_context* ctx, void* stream, double out[4]);
+MB2_API int mb2_reset_energies(mb2_context* ctx, void* stream);
+
+/* --- bonded forces ---------------------------------------------------------
+ * Tables for bonds (kind 0, non-periodic) or angles (kind 1, periodic, radians).
+ * Replaces DeviceBondedInteractions::link_tables
+ * (src/Interactions/DeviceBondedInteraction.h:205-250). */
+MB2_API int mb2_set_bonded_tables(mb2_context* ctx, int kind, int num_tables, const float* values,
+                          const uint32_t* sizes, const float* starts, const float* step_invs);
+
+/* Tabulated bond forces, accumulated. bonds: device int2 [nb]; table_idx:
+ * device int [nb]. Replaces launch_tabulated_bonds
+ * (DeviceBondedInteraction.h:495-521, Bonded/BondComputer.h:136-192). */
+MB2_API int mb2_bond_forces(mb2_context* ctx, const int* bonds2, const int* table_idx, uint32_t nb,
+                    const float* pos4, float* force_energy4, int get_energy, void* stream);
+
+/* Tabulated angle forces, accumulated. angles: device int4 (i, j, k, pad) [na].
+ * Replaces launch_tabulated_angles (DeviceBondedInteraction.h:523-549,
+ * Bonded/BondComputer.h:204-269). */
+MB2_API int mb2_angle_forces(mb2_context* ctx, const int* angles4, const int* table_idx, uint32_t na,
+                     const float* pos4, float* force_energy4, int get_energy, void* stream);
+
+/* --- integrator ------------------------------------------------------------
+ * Per-type data for the BD step (ParticleTypeView, src/Objects/DeviceParticle.h:49-64).
+ * Host arrays: charge[T], diffusion3[T*3], pmf_offset[T], pmf_count[T],
+ * terms4[n_terms*4] as (grid_id, scale, scale_slope, boundary_condition) in
+ * float, force_grid_id3[T*3] (-1 = none, may be NULL), force_grid_scale3[T*3]. */
+MB2_API int mb2_set_particle_types(mb2_context* ctx, int num_types, const float* charge,
+                           const float* diffusion3, const int* pmf_offset, const int* pmf_count,
+                           int n_terms, const float* terms4, const int* force_grid_id3,
+                           const float* force_grid_scale3);
+
+/* Dense grid `grid_id` (BaseGridView, src/Types/BaseGridDevice.h:22-29):
+ * data is a DEVICE float array [nx][ny][nz] (z fastest), borrowed;
+ * basis_inv column-major; boundary_condition 0 Dirichlet, 1 Neumann, 2 Periodic. */
+MB2_API int mb2_set_grid(mb2_context* ctx, int grid_id, const float* data, const int64_t dims[3],
+                 const float origin[3], const float basis_inv[9], int boundary_condition);
+
+/* One Brownian step in place. Replaces launch_BD<float> / BDIntegrate
+ * (src/PatchOperation/Integrator.h:26-54, Integrator/BD.h:12-93). flags may be
+ * NULL. base_seed as Patch::integrate_motion mixes it (mb2_bd_seed). */
+MB2_API int mb2_bd_integrate(mb2_context* ctx, float* pos4, float* force_energy4, const int* type_ids,
+                     const uint32_t* flags, uint32_t n, float dt, float kT, uint64_t step,
+                     uint64_t base_seed, uint32_t base_ctr, const float efield[3],
+                     void* stream);
+
+/* Patch::integrate_motion seed mixing (src/PatchOperation/Patch.cpp:252-254). */
+MB2_API uint64_t mb2_bd_seed(uint64_t seed, uint64_t patch_id, uint64_t step);
+
+/* Philox4x32-10 draws for counters ctr0 + i (i < n), as the BD step makes them
+ * (philox.h:60-139): out4 gets the raw words, normals4 the Box-Muller normals
+ * (either may be NULL). Device pointers. */
+MB2_API int mb2_philox(mb2_context* ctx, uint64_t seed, uint32_t ctr0, uint32_t ctr1, uint32_t ctr2,
+               uint32_t n, uint32_t* out4, float* normals4, void* stream);
+
+/* --- fused step ------------------------------------------------------------
+ * One whole BD step as SimManager::execute_force_calculation +
+ * execute_integration run it (src/SimManager.cpp:337-504) for one patch:
+ * clear forces, rebuild the pairlist when (step - 1) % rebuild_period == 0
+ * (unless the skin check says the list is still valid), pair forces, bonded
+ * forces (if bonds/angles were given), BD integrate. All device pointers. */
+typedef struct {
+    float pairlist_cutoff;
+    float cutoff;
+    uint32_t rebuild_period;
+    float dt;
+    float kT;
+    uint64_t seed;       /* run seed; mixed per step as Patch::integrate_motion does */
+    uint64_t patch_id;
+    float efield[3];
+    int get_energy;
+    const int* bonds2;   /* may be NULL */
+    const int* bond_table_idx;
+    uint32_t num_bonds;
+    const int* angles4;  /* may be NULL */
+    const int* angle_table_idx;
+    uint32_t num_angles;
+} mb2_step_params;
+
+MB2_API int mb2_step(mb2_context* ctx, float* pos4, float* force_energy4, const int* type_ids,
+             const uint32_t* flags, uint32_t n, uint64_t step, const mb2_step_params* params,
+             void* stream);
+
+/* Rows (particles) served by one group of lanes in the pair kernel: 4, 8, 16
+ * or 32 lanes per row; 0 = choose from the mean row length. */
+MB2_API int mb2_set_lanes_per_row(mb2_context* ctx, int lanes);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,703 @@
+// C ABI of libmarsb200.so: context, set-up, and one entry point per
+// reference interface on the Brownian-dynamics path (see include/marsb200.h).
+#include "../../include/marsb200.h"
+#include "mb2_internal.cuh"
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <limits>
+
+using namespace mb2;
+
+struct mb2_context {
+	int device = 0;
+	uint32_t max_particles = 0;
+	std::string last_error;
+
+	Box box{};
+	bool box_set = false;
+	Scratch scratch;
+
+	// Z-order state of the last build
+	DevBuf<uint32_t> keys, s2o, inv, counts, row_start, nbr, cell_begin, cell_end;
+	DevBuf<float4> sorted_pos, ref_pos, force_sorted;
+	DevBuf<StencilEntry> stencil;
+	DevBuf<float> bbox;  // 6 floats, ordered-int min/max
+	DevBuf<unsigned int> disp;
+	DevBuf<double> energy;  // pair E, pair virial, bond E, angle E
+	uint32_t* pinned_u32 = nullptr;
+	CellGrid grid;
+	bool grid_valid = false;
+	float grid_extent[3] = {0, 0, 0};
+	float grid_rc = 0.0f;
+	uint32_t grid_n = 0;
+	bool built = false;
+	uint32_t built_n = 0;
+	uint64_t num_pairs = 0;
+	Exclusions excl;
+	int lanes_per_row = 0;
+
+	// pair tables
+	PairTables pt;
+	DevBuf<uint32_t> term;
+	DevBuf<Table> tables;
+	DevBuf<float> values;
+
+	// bonded tables
+	DevBuf<Table> bonded_tables[2];
+	DevBuf<float> bonded_values[2];
+	int bonded_count[2] = {0, 0};
+
+	// particle types and grids
+	TypeTable types;
+	bool types_set = false;
+	DevBuf<float> charge;
+	DevBuf<float4> diffusion, fg_scale;
+	DevBuf<int> pmf_off, pmf_cnt;
+	DevBuf<GridTermDev> terms;
+	DevBuf<int4> fg_id;
+	std::vector<GridView> host_grids;
+	DevBuf<GridView> grids;
+};
+
+namespace {
+
+int fail(mb2_context* ctx, int code, const std::string& msg) {
+	if (ctx) ctx->last_error = msg;
+	return code;
+}
+
+template <typename F>
+int guarded(mb2_context* ctx, F&& f) {
+	if (!ctx) return MB2_ERR_ARG;
+	try {
+		MB2_CUDA(cudaSetDevice(ctx->device));
+		f();
+		MB2_CUDA(cudaGetLastError());
+		ctx->last_error.clear();
+		return MB2_OK;
+	} catch (const Error& e) {
+		return fail(ctx, e.code, e.msg);
+	} catch (const std::exception& e) {
+		return fail(ctx, MB2_ERR_CUDA, e.what());
+	}
+}
+
+void require(bool cond, int code, const char* msg) {
+	if (!cond) throw Error{code, msg};
+}
+
+cudaStream_t S(void* stream) { return reinterpret_cast<cudaStream_t>(stream); }
+
+// Ordered-int encoding so atomicMin/Max on int order floats correctly.
+__device__ __forceinline__ int f2o(float f) {
+	const int i = __float_as_int(f);
+	return i >= 0 ? i : i ^ 0x7FFFFFFF;
+}
+__host__ __device__ inline float o2f(int i) {
+	const int b = i >= 0 ? i : i ^ 0x7FFFFFFF;
+	float f;
+	std::memcpy(&f, &b, 4);
+	return f;
+}
+
+__global__ void bbox_kernel(const float4* __restrict__ pos, uint32_t n, int* out) {
+	const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+	int lo[3] = {INT_MAX, INT_MAX, INT_MAX}, hi[3] = {INT_MIN, INT_MIN, INT_MIN};
+	if (i < n) {
+		const float4 p = pos[i];
+		lo[0] = hi[0] = f2o(p.x);
+		lo[1] = hi[1] = f2o(p.y);
+		lo[2] = hi[2] = f2o(p.z);
+	}
+#pragma unroll
+	for (int a = 0; a < 3; ++a) {
+#pragma unroll
+		for (int o = 16; o > 0; o >>= 1) {
+			lo[a] = min(lo[a], __shfl_xor_sync(0xFFFFFFFFu, lo[a], o));
+			hi[a] = max(hi[a], __shfl_xor_sync(0xFFFFFFFFu, hi[a], o));
+		}
+	}
+	if ((threadIdx.x & 31) == 0) {
+		for (int a = 0; a < 3; ++a) {
+			atomicMin(out + a, lo[a]);
+			atomicMax(out + 3 + a, hi[a]);
+		}
+	}
+}
+
+__global__ void bbox_init_kernel(int* out) {
+	if (threadIdx.x < 3) out[threadIdx.x] = INT_MAX;
+	else if (threadIdx.x < 6) out[threadIdx.x] = INT_MIN;
+}
+
+// Morton domain of ZOrderPairlist::build_pairlist (ZOrderPairlist.cpp:130-146)
+// and compute_particle_extent (:368-411): the box on periodic axes, the
+// particle extent + 1 % (at least 1e-4 wide) on open axes.
+void morton_domain(mb2_context* ctx, const float4* pos, uint32_t n, cudaStream_t st, float* bmin,
+				   float* bmax) {
+	const Box& b = ctx->box;
+	const bool any_open = !(b.periodic[0] && b.periodic[1] && b.periodic[2]);
+	float lo[3] = {0, 0, 0}, hi[3] = {0, 0, 0};
+	if (any_open) {
+		ctx->bbox.ensure(6);
+		int* dev = reinterpret_cast<int*>(ctx->bbox.ptr);
+		bbox_init_kernel<<<1, 32, 0, st>>>(dev);
+		if (n) bbox_kernel<<<(n + 255) / 256, 256, 0, st>>>(pos, n, dev);
+		int h[6];
+		MB2_CUDA(cudaMemcpyAsync(h, dev, sizeof(h), cudaMemcpyDeviceToHost, st));
+		MB2_CUDA(cudaStreamSynchronize(st));
+		for (int a = 0; a < 3; ++a) {
+			lo[a] = n ? o2f(h[a]) : std::numeric_limits<float>::max();
+			hi[a] = n ? o2f(h[3 + a]) : std::numeric_limits<float>::lowest();
+		}
+	}
+	for (int a = 0; a < 3; ++a) {
+		if (b.periodic[a]) {
+			bmin[a] = b.origin[a];
+			bmax[a] = b.origin[a] + b.size[a];
+			continue;
+		}
+		volatile float margin = (hi[a] - lo[a]) * 0.01f;
+		float l = lo[a] - margin, h = hi[a] + margin;
+		volatile float range = h - l;
+		if (range < 1e-4f) {
+			const float center = static_cast<float>(static_cast<double>(l) + static_cast<double>(range) * 0.5);
+			l = static_cast<float>(static_cast<double>(center) - static_cast<double>(1e-4f) * 0.5);
+			h = static_cast<float>(static_cast<double>(center) + static_cast<double>(1e-4f) * 0.5);
+		}
+		bmin[a] = l;
+		bmax[a] = h;
+	}
+}
+
+void sort_particles(mb2_context* ctx, const float4* pos, const int* type_ids, uint32_t n,
+					const float* bmin, const float* bmax, cudaStream_t st) {
+	ctx->keys.ensure(n);
+	ctx->s2o.ensure(n);
+	ctx->inv.ensure(n);
+	ctx->sorted_pos.ensure(n);
+	morton_encode(pos, n, bmin, bmax, ctx->keys.ptr, ctx->s2o.ptr, st);
+	radix_sort_pairs(ctx->scratch, ctx->keys.ptr, ctx->s2o.ptr, n, st);
+	inverse_and_gather(ctx->s2o.ptr, n, pos, ctx->inv.ptr, nullptr, st);
+	pack_sorted_positions(pos, type_ids, ctx->s2o.ptr, n, ctx->sorted_pos.ptr, st);
+}
+
+void build(mb2_context* ctx, const float4* pos, const int* type_ids, uint32_t n, float rc_list,
+		   cudaStream_t st) {
+	require(ctx->box_set, MB2_ERR_STATE, "mb2_build_pairlist: call mb2_set_box first");
+	require(n <= ctx->max_particles, MB2_ERR_CAPACITY,
+			"mb2_build_pairlist: more particles than the context was created for");
+	require(rc_list > 0.0f && std::isfinite(rc_list), MB2_ERR_ARG,
+			"mb2_build_pairlist: pairlist cutoff must be positive and finite");
+	float bmin[3], bmax[3], extent[3];
+	morton_domain(ctx, pos, n, st, bmin, bmax);
+	for (int a = 0; a < 3; ++a) extent[a] = bmax[a] - bmin[a];
+	sort_particles(ctx, pos, type_ids, n, bmin, bmax, st);
+
+	const float rc2 = rc_list * rc_list;
+	if (!ctx->grid_valid || ctx->grid_rc != rc_list || ctx->grid_n != n ||
+		std::memcmp(ctx->grid_extent, extent, sizeof(extent)) != 0) {
+		ctx->grid = choose_cell_grid(extent, ctx->box.periodic, std::sqrt(rc2), n);
+		ctx->stencil.ensure(ctx->grid.stencil.size());
+		MB2_CUDA(cudaMemcpyAsync(ctx->stencil.ptr, ctx->grid.stencil.data(),
+								 ctx->grid.stencil.size() * sizeof(StencilEntry),
+								 cudaMemcpyHostToDevice, st));
+		ctx->grid_valid = true;
+		ctx->grid_rc = rc_list;
+		ctx->grid_n = n;
+		std::memcpy(ctx->grid_extent, extent, sizeof(extent));
+	}
+	const CellGrid& g = ctx->grid;
+	const size_t num_cells = static_cast<size_t>(1) << (3 * g.m);
+	ctx->cell_begin.ensure(num_cells);
+	ctx->cell_end.ensure(num_cells);
+	cell_ranges(ctx->keys.ptr, n, g.shift, ctx->cell_begin.ptr, ctx->cell_end.ptr, num_cells, st);
+
+	ctx->counts.ensure(n);
+	ctx->row_start.ensure(static_cast<size_t>(n) + 1);
+	neighbor_count(ctx->sorted_pos.ptr, ctx->keys.ptr, ctx->s2o.ptr, ctx->cell_begin.ptr,
+				   ctx->cell_end.ptr, ctx->stencil.ptr, g.num_stencil, g.m, g.shift, rc2, n,
+				   ctx->box, ctx->excl, ctx->counts.ptr, st);
+	exclusive_scan_u32(ctx->scratch, ctx->counts.ptr, ctx->row_start.ptr, n,
+					   ctx->row_start.ptr + n, st);
+	MB2_CUDA(cudaMemcpyAsync(ctx->pinned_u32, ctx->row_start.ptr + n, sizeof(uint32_t),
+							 cudaMemcpyDeviceToHost, st));
+	MB2_CUDA(cudaStreamSynchronize(st));
+	const uint32_t total = *ctx->pinned_u32;
+	ctx->nbr.ensure(std::max<size_t>(total, 1));
+	neighbor_fill(ctx->sorted_pos.ptr, ctx->keys.ptr, ctx->s2o.ptr, ctx->cell_begin.ptr,
+				  ctx->cell_end.ptr, ctx->stencil.ptr, g.num_stencil, g.m, g.shift, rc2, n,
+				  ctx->box, ctx->excl, ctx->row_start.ptr, ctx->nbr.ptr, st);
+	// Snapshot for the skin check (ZOrderPairlist.cpp:172-173).
+	ctx->ref_pos.ensure(n);
+	MB2_CUDA(cudaMemcpyAsync(ctx->ref_pos.ptr, pos, static_cast<size_t>(n) * sizeof(float4),
+							 cudaMemcpyDeviceToDevice, st));
+	ctx->num_pairs = total;
+	ctx->built = true;
+	ctx->built_n = n;
+}
+
+int pick_lanes(const mb2_context* ctx) {
+	if (ctx->lanes_per_row) return ctx->lanes_per_row;
+	const double mean = ctx->built_n ? static_cast<double>(ctx->num_pairs) / ctx->built_n : 0.0;
+	if (mean >= 48.0) return 32;
+	if (mean >= 20.0) return 16;
+	if (mean >= 8.0) return 8;
+	return 4;
+}
+
+void pair_forces_impl(mb2_context* ctx, const float4* pos, const int* type_ids, float4* fe,
+					  uint32_t n, float cutoff, int get_energy, cudaStream_t st) {
+	require(ctx->built, MB2_ERR_STATE, "mb2_pair_forces: no pairlist; call mb2_build_pairlist");
+	require(n == ctx->built_n, MB2_ERR_ARG,
+			"mb2_pair_forces: particle count differs from the last pairlist build");
+	require(ctx->pt.num_types > 0, MB2_ERR_STATE,
+			"mb2_pair_forces: no pair tables; call mb2_set_pair_tables");
+	if (n == 0) return;
+	pack_sorted_positions(pos, type_ids, ctx->s2o.ptr, n, ctx->sorted_pos.ptr, st);
+	ctx->force_sorted.ensure(n);
+	MB2_CUDA(cudaMemsetAsync(ctx->force_sorted.ptr, 0, static_cast<size_t>(n) * sizeof(float4), st));
+	const float cutoff_sq = cutoff > 0.0f ? cutoff * cutoff : 0.0f;
+	pair_forces(ctx->sorted_pos.ptr, ctx->row_start.ptr, ctx->nbr.ptr, n, ctx->pt, ctx->box,
+				cutoff_sq, get_energy, ctx->force_sorted.ptr, ctx->energy.ptr, pick_lanes(ctx), st);
+	scatter_add_forces(ctx->force_sorted.ptr, ctx->s2o.ptr, n, fe, get_energy, st);
+}
+
+float max_disp(mb2_context* ctx, const float4* pos, uint32_t n, cudaStream_t st) {
+	require(ctx->built && n == ctx->built_n, MB2_ERR_STATE,
+			"mb2_needs_update: no pairlist for this particle count");
+	ctx->disp.ensure(1);
+	max_displacement_sq(pos, ctx->ref_pos.ptr, n, ctx->box, ctx->disp.ptr, st);
+	MB2_CUDA(cudaMemcpyAsync(ctx->pinned_u32, ctx->disp.ptr, sizeof(uint32_t),
+							 cudaMemcpyDeviceToHost, st));
+	MB2_CUDA(cudaStreamSynchronize(st));
+	float d2;
+	std::memcpy(&d2, ctx->pinned_u32, 4);
+	return sqrtf(d2);
+}
+
+void upload_tables(DevBuf<Table>& tbuf, DevBuf<float>& vbuf, int num_tables, const float* values,
+				   const uint32_t* sizes, const float* starts, const float* step_invs,
+				   int periodic, uint32_t* total_out) {
+	size_t total = 0;
+	for (int k = 0; k < num_tables; ++k) {
+		require(sizes[k] >= 2, MB2_ERR_ARG, "table needs at least 2 values");
+		total += sizes[k];
+	}
+	vbuf.ensure(total);
+	MB2_CUDA(cudaMemcpy(vbuf.ptr, values, total * sizeof(float), cudaMemcpyHostToDevice));
+	std::vector<Table> host(num_tables);
+	size_t off = 0;
+	for (int k = 0; k < num_tables; ++k) {
+		host[k] = Table{vbuf.ptr + off, step_invs[k], sizes[k], starts[k], periodic};
+		off += sizes[k];
+	}
+	tbuf.ensure(std::max(num_tables, 1));
+	MB2_CUDA(cudaMemcpy(tbuf.ptr, host.data(), num_tables * sizeof(Table), cudaMemcpyHostToDevice));
+	if (total_out) *total_out = static_cast<uint32_t>(total);
+}
+
+}  // namespace
+
+extern "C" {
+
+int mb2_version(void) { return 100; }
+
+int mb2_create(int device, uint32_t max_particles, mb2_context** out) {
+	if (!out) return MB2_ERR_ARG;
+	*out = nullptr;
+	mb2_context* ctx = new (std::nothrow) mb2_context();
+	if (!ctx) return MB2_ERR_CAPACITY;
+	ctx->device = device;
+	ctx->max_particles = max_particles;
+	const int rc = guarded(ctx, [&] {
+		MB2_CUDA(cudaMallocHost(&ctx->pinned_u32, 64));
+		ctx->energy.ensure(4);
+		MB2_CUDA(cudaMemset(ctx->energy.ptr, 0, 4 * sizeof(double)));
+	});
+	if (rc != MB2_OK) {
+		delete ctx;
+		return rc;
+	}
+	*out = ctx;
+	return MB2_OK;
+}
+
+int mb2_destroy(mb2_context* ctx) {
+	if (!ctx) return MB2_ERR_ARG;
+	cudaSetDevice(ctx->device);
+	cudaDeviceSynchronize();
+	for (auto* b : {&ctx->keys, &ctx->s2o, &ctx->inv, &ctx->counts, &ctx->row_start, &ctx->nbr,
+					&ctx->cell_begin, &ctx->cell_end, &ctx->term})
+		b->release();
+	for (auto* b : {&ctx->sorted_pos, &ctx->ref_pos, &ctx->force_sorted, &ctx->diffusion,
+					&ctx->fg_scale})
+		b->release();
+	ctx->stencil.release();
+	ctx->bbox.release();
+	ctx->disp.release();
+	ctx->energy.release();
+	ctx->tables.release();
+	ctx->values.release();
+	for (int k = 0; k < 2; ++k) {
+		ctx->bonded_tables[k].release();
+		ctx->bonded_values[k].release();
+	}
+	ctx->charge.release();
+	ctx->pmf_off.release();
+	ctx->pmf_cnt.release();
+	ctx->terms.release();
+	ctx->fg_id.release();
+	ctx->grids.release();
+	ctx->scratch.release();
+	if (ctx->pinned_u32) cudaFreeHost(ctx->pinned_u32);
+	delete ctx;
+	return MB2_OK;
+}
+
+const char* mb2_last_error(const mb2_context* ctx) {
+	return ctx ? ctx->last_error.c_str() : "null context";
+}
+
+int mb2_set_box(mb2_context* ctx, const float origin[3], const float size[3],
+				const int periodic[3]) {
+	return guarded(ctx, [&] {
+		require(origin && size && periodic, MB2_ERR_ARG, "mb2_set_box: null argument");
+		for (int a = 0; a < 3; ++a) {
+			require(size[a] > 0.0f && std::isfinite(size[a]), MB2_ERR_ARG,
+					"mb2_set_box: box size must be positive (ZOrderPairlist.cpp:118-126)");
+			ctx->box.origin[a] = origin[a];
+			ctx->box.size[a] = size[a];
+			ctx->box.inv[a] = 1.0f / size[a];
+			ctx->box.half[a] = 0.5f * size[a];
+			ctx->box.periodic[a] = periodic[a] ? 1 : 0;
+		}
+		ctx->box_set = true;
+		ctx->grid_valid = false;
+	});
+}
+
+int mb2_sort_morton(mb2_context* ctx, const float* pos4, uint32_t n, const float bmin[3],
+					const float bmax[3], uint32_t* keys_out, uint32_t* s2o_out,
+					uint32_t* inverse_out, float* sorted_pos4_out, void* stream) {
+	return guarded(ctx, [&] {
+		require(n <= ctx->max_particles, MB2_ERR_CAPACITY, "mb2_sort_morton: n above capacity");
+		require(n == 0 || pos4, MB2_ERR_ARG, "mb2_sort_morton: null positions");
+		const cudaStream_t st = S(stream);
+		const float4* pos = reinterpret_cast<const float4*>(pos4);
+		ctx->keys.ensure(n);
+		ctx->s2o.ensure(n);
+		ctx->inv.ensure(n);
+		morton_encode(pos, n, bmin, bmax, ctx->keys.ptr, ctx->s2o.ptr, st);
+		radix_sort_pairs(ctx->scratch, ctx->keys.ptr, ctx->s2o.ptr, n, st);
+		inverse_and_gather(ctx->s2o.ptr, n, pos, ctx->inv.ptr,
+						   reinterpret_cast<float4*>(sorted_pos4_out), st);
+		const size_t b = static_cast<size_t>(n) * sizeof(uint32_t);
+		if (keys_out) MB2_CUDA(cudaMemcpyAsync(keys_out, ctx->keys.ptr, b, cudaMemcpyDeviceToDevice, st));
+		if (s2o_out) MB2_CUDA(cudaMemcpyAsync(s2o_out, ctx->s2o.ptr, b, cudaMemcpyDeviceToDevice, st));
+		if (inverse_out) MB2_CUDA(cudaMemcpyAsync(inverse_out, ctx->inv.ptr, b, cudaMemcpyDeviceToDevice, st));
+		ctx->built = false;  // the sort state no longer matches a pairlist
+	});
+}
+
+int mb2_radix_sort_pairs(mb2_context* ctx, uint32_t* keys, uint32_t* vals, uint32_t n,
+						 void* stream) {
+	return guarded(ctx, [&] {
+		require(n == 0 || (keys && vals), MB2_ERR_ARG, "mb2_radix_sort_pairs: null argument");
+		radix_sort_pairs(ctx->scratch, keys, vals, n, S(stream));
+	});
+}
+
+int mb2_set_exclusions(mb2_context* ctx, const int* offsets, const int* neighbors,
+					   uint32_t num_particles, const int* rigid_body_id) {
+	return guarded(ctx, [&] {
+		require(!offsets || neighbors || num_particles == 0, MB2_ERR_ARG,
+				"mb2_set_exclusions: offsets without neighbors");
+		ctx->excl.offsets = offsets;
+		ctx->excl.neighbors = neighbors;
+		ctx->excl.num_particles = offsets ? num_particles : 0;
+		ctx->excl.rigid_body_id = rigid_body_id;
+	});
+}
+
+int mb2_build_pairlist(mb2_context* ctx, const float* pos4, const int* type_ids, uint32_t n,
+					   float pairlist_cutoff, void* stream, uint64_t* num_pairs) {
+	return guarded(ctx, [&] {
+		require(n == 0 || pos4, MB2_ERR_ARG, "mb2_build_pairlist: null positions");
+		build(ctx, reinterpret_cast<const float4*>(pos4), type_ids, n, pairlist_cutoff, S(stream));
+		if (num_pairs) *num_pairs = ctx->num_pairs;
+	});
+}
+
+int mb2_num_pairs(const mb2_context* ctx, uint64_t* num_pairs) {
+	if (!ctx || !num_pairs) return MB2_ERR_ARG;
+	*num_pairs = ctx->built ? ctx->num_pairs : 0;
+	return MB2_OK;
+}
+
+int mb2_export_pairs(mb2_context* ctx, int* pairs2, uint64_t capacity, void* stream) {
+	return guarded(ctx, [&] {
+		require(ctx->built, MB2_ERR_STATE, "mb2_export_pairs: no pairlist");
+		require(capacity >= ctx->num_pairs, MB2_ERR_CAPACITY,
+				"mb2_export_pairs: output smaller than the pair count");
+		require(ctx->num_pairs == 0 || pairs2, MB2_ERR_ARG, "mb2_export_pairs: null output");
+		export_pairs(ctx->row_start.ptr, ctx->nbr.ptr, ctx->s2o.ptr, ctx->built_n,
+					 reinterpret_cast<int2*>(pairs2), S(stream));
+	});
+}
+
+int mb2_needs_update(mb2_context* ctx, const float* pos4, uint32_t n, float skin, void* stream,
+					 float* max_displacement, int* needs) {
+	return guarded(ctx, [&] {
+		const float d = max_disp(ctx, reinterpret_cast<const float4*>(pos4), n, S(stream));
+		if (max_displacement) *max_displacement = d;
+		if (needs) *needs = d > skin * 0.5f ? 1 : 0;
+	});
+}
+
+int mb2_set_pair_tables(mb2_context* ctx, int num_types, const uint32_t* term_matrix,
+						int num_tables, const float* values, const uint32_t* sizes,
+						const float* starts, const float* step_invs) {
+	return guarded(ctx, [&] {
+		require(num_types > 0 && num_types <= 64, MB2_ERR_ARG,
+				"mb2_set_pair_tables: 1..64 particle types");
+		require(num_tables >= 0 && term_matrix, MB2_ERR_ARG, "mb2_set_pair_tables: bad tables");
+		for (int k = 0; k < num_types * num_types; ++k) {
+			const uint32_t tag = term_matrix[k];
+			require(!(tag & kTermTabulated) || static_cast<int>(tag >> kTableShift) < num_tables,
+					MB2_ERR_ARG, "mb2_set_pair_tables: tag names a missing table");
+		}
+		uint32_t total = 0;
+		upload_tables(ctx->tables, ctx->values, num_tables, values, sizes, starts, step_invs, 0,
+					  &total);
+		const size_t smem = static_cast<size_t>((num_types * num_types + 3) & ~3) * 4 +
+							static_cast<size_t>(num_tables) * 16 + static_cast<size_t>(total) * 4;
+		require(smem <= 200 * 1024, MB2_ERR_CAPACITY,
+				"mb2_set_pair_tables: tables exceed the 200 KB shared-memory budget");
+		ctx->term.ensure(static_cast<size_t>(num_types) * num_types);
+		MB2_CUDA(cudaMemcpy(ctx->term.ptr, term_matrix, sizeof(uint32_t) * num_types * num_types,
+							cudaMemcpyHostToDevice));
+		ctx->pt.num_types = num_types;
+		ctx->pt.num_tables = num_tables;
+		ctx->pt.term_matrix = ctx->term.ptr;
+		ctx->pt.tables = ctx->tables.ptr;
+		ctx->pt.values = ctx->values.ptr;
+		ctx->pt.total_values = total;
+	});
+}
+
+int mb2_pair_forces(mb2_context* ctx, const float* pos4, const int* type_ids,
+					float* force_energy4, uint32_t n, float cutoff, int get_energy,
+					void* stream) {
+	return guarded(ctx, [&] {
+		require(n == 0 || (pos4 && type_ids && force_energy4), MB2_ERR_ARG,
+				"mb2_pair_forces: null argument");
+		pair_forces_impl(ctx, reinterpret_cast<const float4*>(pos4), type_ids,
+						 reinterpret_cast<float4*>(force_energy4), n, cutoff, get_energy,
+						 S(stream));
+	});
+}
+
+int mb2_energies(mb2_context* ctx, void* stream, double out[4]) {
+	return guarded(ctx, [&] {
+		require(out, MB2_ERR_ARG, "mb2_energies: null output");
+		MB2_CUDA(cudaMemcpyAsync(out, ctx->energy.ptr, 4 * sizeof(double), cudaMemcpyDeviceToHost,
+								 S(stream)));
+		MB2_CUDA(cudaStreamSynchronize(S(stream)));
+	});
+}
+
+int mb2_reset_energies(mb2_context* ctx, void* stream) {
+	return guarded(ctx, [&] {
+		MB2_CUDA(cudaMemsetAsync(ctx->energy.ptr, 0, 4 * sizeof(double), S(stream)));
+	});
+}
+
+int mb2_set_bonded_tables(mb2_context* ctx, int kind, int num_tables, const float* values,
+						  const uint32_t* sizes, const float* starts, const float* step_invs) {
+	return guarded(ctx, [&] {
+		require(kind == 0 || kind == 1, MB2_ERR_ARG, "mb2_set_bonded_tables: kind is 0 or 1");
+		require(num_tables > 0, MB2_ERR_ARG, "mb2_set_bonded_tables: no tables");
+		upload_tables(ctx->bonded_tables[kind], ctx->bonded_values[kind], num_tables, values, sizes,
+					  starts, step_invs, kind == 1 ? 1 : 0, nullptr);
+		ctx->bonded_count[kind] = num_tables;
+	});
+}
+
+int mb2_bond_forces(mb2_context* ctx, const int* bonds2, const int* table_idx, uint32_t nb,
+					const float* pos4, float* force_energy4, int get_energy, void* stream) {
+	return guarded(ctx, [&] {
+		require(ctx->box_set, MB2_ERR_STATE, "mb2_bond_forces: no box");
+		require(nb == 0 || ctx->bonded_count[0] > 0, MB2_ERR_STATE, "mb2_bond_forces: no tables");
+		bond_forces(reinterpret_cast<const int2*>(bonds2), table_idx, nb,
+					reinterpret_cast<const float4*>(pos4), reinterpret_cast<float4*>(force_energy4),
+					ctx->bonded_tables[0].ptr, ctx->box, get_energy, ctx->energy.ptr + 2,
+					S(stream));
+	});
+}
+
+int mb2_angle_forces(mb2_context* ctx, const int* angles4, const int* table_idx, uint32_t na,
+					 const float* pos4, float* force_energy4, int get_energy, void* stream) {
+	return guarded(ctx, [&] {
+		require(ctx->box_set, MB2_ERR_STATE, "mb2_angle_forces: no box");
+		require(na == 0 || ctx->bonded_count[1] > 0, MB2_ERR_STATE, "mb2_angle_forces: no tables");
+		angle_forces(reinterpret_cast<const int4*>(angles4), table_idx, na,
+					 reinterpret_cast<const float4*>(pos4), reinterpret_cast<float4*>(force_energy4),
+					 ctx->bonded_tables[1].ptr, ctx->box, get_energy, ctx->energy.ptr + 3,
+					 S(stream));
+	});
+}
+
+int mb2_set_particle_types(mb2_context* ctx, int num_types, const float* charge,
+						   const float* diffusion3, const int* pmf_offset, const int* pmf_count,
+						   int n_terms, const float* terms4, const int* force_grid_id3,
+						   const float* force_grid_scale3) {
+	return guarded(ctx, [&] {
+		require(num_types > 0 && charge && diffusion3, MB2_ERR_ARG,
+				"mb2_set_particle_types: need charge and diffusion per type");
+		const int T = num_types;
+		std::vector<float4> dif(T), fs(T);
+		std::vector<int4> fg(T);
+		std::vector<int> off(T, 0), cnt(T, 0);
+		for (int t = 0; t < T; ++t) {
+			dif[t] = make_float4(diffusion3[3 * t], diffusion3[3 * t + 1], diffusion3[3 * t + 2], 0.f);
+			fg[t] = force_grid_id3 ? make_int4(force_grid_id3[3 * t], force_grid_id3[3 * t + 1],
+											   force_grid_id3[3 * t + 2], -1)
+								   : make_int4(-1, -1, -1, -1);
+			fs[t] = force_grid_scale3 ? make_float4(force_grid_scale3[3 * t], force_grid_scale3[3 * t + 1],
+													force_grid_scale3[3 * t + 2], 0.f)
+									  : make_float4(0.f, 0.f, 0.f, 0.f);
+			if (pmf_offset && pmf_count) {
+				off[t] = pmf_offset[t];
+				cnt[t] = pmf_count[t];
+				require(off[t] >= 0 && cnt[t] >= 0 && off[t] + cnt[t] <= n_terms, MB2_ERR_ARG,
+						"mb2_set_particle_types: PMF term range out of bounds");
+			}
+		}
+		std::vector<GridTermDev> tm(std::max(n_terms, 1));
+		for (int k = 0; k < n_terms; ++k)
+			tm[k] = GridTermDev{static_cast<int>(terms4[4 * k]), terms4[4 * k + 1],
+								terms4[4 * k + 2], static_cast<int>(terms4[4 * k + 3])};
+		ctx->charge.ensure(T);
+		ctx->diffusion.ensure(T);
+		ctx->fg_scale.ensure(T);
+		ctx->fg_id.ensure(T);
+		ctx->pmf_off.ensure(T);
+		ctx->pmf_cnt.ensure(T);
+		ctx->terms.ensure(tm.size());
+		MB2_CUDA(cudaMemcpy(ctx->charge.ptr, charge, T * sizeof(float), cudaMemcpyHostToDevice));
+		MB2_CUDA(cudaMemcpy(ctx->diffusion.ptr, dif.data(), T * sizeof(float4), cudaMemcpyHostToDevice));
+		MB2_CUDA(cudaMemcpy(ctx->fg_scale.ptr, fs.data(), T * sizeof(float4), cudaMemcpyHostToDevice));
+		MB2_CUDA(cudaMemcpy(ctx->fg_id.ptr, fg.data(), T * sizeof(int4), cudaMemcpyHostToDevice));
+		MB2_CUDA(cudaMemcpy(ctx->pmf_off.ptr, off.data(), T * sizeof(int), cudaMemcpyHostToDevice));
+		MB2_CUDA(cudaMemcpy(ctx->pmf_cnt.ptr, cnt.data(), T * sizeof(int), cudaMemcpyHostToDevice));
+		MB2_CUDA(cudaMemcpy(ctx->terms.ptr, tm.data(), tm.size() * sizeof(GridTermDev),
+							cudaMemcpyHostToDevice));
+		ctx->types.num_types = T;
+		ctx->types.charge = ctx->charge.ptr;
+		ctx->types.diffusion = ctx->diffusion.ptr;
+		ctx->types.pmf_offset = ctx->pmf_off.ptr;
+		ctx->types.pmf_count = ctx->pmf_cnt.ptr;
+		ctx->types.terms = ctx->terms.ptr;
+		ctx->types.force_grid_id = ctx->fg_id.ptr;
+		ctx->types.force_grid_scale = ctx->fg_scale.ptr;
+		ctx->types_set = true;
+	});
+}
+
+int mb2_set_grid(mb2_context* ctx, int grid_id, const float* data, const int64_t dims[3],
+				 const float origin[3], const float basis_inv[9], int boundary_condition) {
+	return guarded(ctx, [&] {
+		require(grid_id >= 0 && grid_id < 1024, MB2_ERR_ARG, "mb2_set_grid: grid id out of range");
+		require(dims && origin && basis_inv, MB2_ERR_ARG, "mb2_set_grid: null argument");
+		if (static_cast<int>(ctx->host_grids.size()) <= grid_id)
+			ctx->host_grids.resize(grid_id + 1, GridView{nullptr, {0, 0, 0}, {0}, {0, 0, 0}, 0});
+		GridView g{};
+		g.data = data;
+		for (int a = 0; a < 3; ++a) {
+			require(dims[a] > 0, MB2_ERR_ARG, "mb2_set_grid: dimensions must be positive");
+			g.origin[a] = origin[a];
+			g.dims[a] = dims[a];
+		}
+		for (int k = 0; k < 9; ++k) g.basis_inv[k] = basis_inv[k];
+		g.boundary_condition = boundary_condition;
+		ctx->host_grids[grid_id] = g;
+		ctx->grids.ensure(ctx->host_grids.size());
+		MB2_CUDA(cudaMemcpy(ctx->grids.ptr, ctx->host_grids.data(),
+							ctx->host_grids.size() * sizeof(GridView), cudaMemcpyHostToDevice));
+		ctx->types.grids = ctx->grids.ptr;
+		ctx->types.num_grids = static_cast<int>(ctx->host_grids.size());
+	});
+}
+
+int mb2_bd_integrate(mb2_context* ctx, float* pos4, float* force_energy4, const int* type_ids,
+					 const uint32_t* flags, uint32_t n, float dt, float kT, uint64_t step,
+					 uint64_t base_seed, uint32_t base_ctr, const float efield[3],
+					 void* stream) {
+	return guarded(ctx, [&] {
+		require(ctx->box_set, MB2_ERR_STATE, "mb2_bd_integrate: no box");
+		require(ctx->types_set, MB2_ERR_STATE, "mb2_bd_integrate: call mb2_set_particle_types");
+		require(n == 0 || (pos4 && force_energy4 && type_ids), MB2_ERR_ARG,
+				"mb2_bd_integrate: null argument");
+		BdParams p{dt, kT, static_cast<uint32_t>(step), base_seed, base_ctr,
+				   {efield ? efield[0] : 0.f, efield ? efield[1] : 0.f, efield ? efield[2] : 0.f}};
+		bd_integrate(reinterpret_cast<float4*>(pos4), reinterpret_cast<float4*>(force_energy4),
+					 type_ids, flags, n, ctx->types, ctx->box, p, S(stream));
+	});
+}
+
+uint64_t mb2_bd_seed(uint64_t seed, uint64_t patch_id, uint64_t step) {
+	return (seed * 0x9E3779B97F4A7C15ULL) ^ (patch_id << 32) ^ (step * 0xBF58476D1CE4E5B9ULL);
+}
+
+int mb2_philox(mb2_context* ctx, uint64_t seed, uint32_t ctr0, uint32_t ctr1, uint32_t ctr2,
+			   uint32_t n, uint32_t* out4, float* normals4, void* stream) {
+	return guarded(ctx, [&] { philox_draws(seed, ctr0, ctr1, ctr2, n, out4, normals4, S(stream)); });
+}
+
+int mb2_step(mb2_context* ctx, float* pos4, float* force_energy4, const int* type_ids,
+			 const uint32_t* flags, uint32_t n, uint64_t step, const mb2_step_params* prm,
+			 void* stream) {
+	return guarded(ctx, [&] {
+		require(prm && (n == 0 || (pos4 && force_energy4 && type_ids)), MB2_ERR_ARG,
+				"mb2_step: null argument");
+		require(ctx->types_set, MB2_ERR_STATE, "mb2_step: call mb2_set_particle_types");
+		const cudaStream_t st = S(stream);
+		float4* pos = reinterpret_cast<float4*>(pos4);
+		float4* fe = reinterpret_cast<float4*>(force_energy4);
+		// DeviceParticle::clear_forces (Patch.cpp:56)
+		MB2_CUDA(cudaMemsetAsync(fe, 0, static_cast<size_t>(n) * sizeof(float4), st));
+		// Rebuild schedule and skin check (Patch.cpp:86-108)
+		const bool at_period = prm->rebuild_period == 0 || (step - 1) % prm->rebuild_period == 0;
+		bool rebuild = at_period || !ctx->built || ctx->built_n != n;
+		const float skin = prm->pairlist_cutoff - prm->cutoff;
+		if (rebuild && prm->rebuild_period != 0 && ctx->built && ctx->built_n == n && skin > 0.0f)
+			rebuild = max_disp(ctx, pos, n, st) > skin * 0.5f;
+		if (rebuild) build(ctx, pos, type_ids, n, prm->pairlist_cutoff, st);
+		pair_forces_impl(ctx, pos, type_ids, fe, n, prm->cutoff, prm->get_energy, st);
+		if (prm->num_bonds)
+			bond_forces(reinterpret_cast<const int2*>(prm->bonds2), prm->bond_table_idx,
+						prm->num_bonds, pos, fe, ctx->bonded_tables[0].ptr, ctx->box,
+						prm->get_energy, ctx->energy.ptr + 2, st);
+		if (prm->num_angles)
+			angle_forces(reinterpret_cast<const int4*>(prm->angles4), prm->angle_table_idx,
+						 prm->num_angles, pos, fe, ctx->bonded_tables[1].ptr, ctx->box,
+						 prm->get_energy, ctx->energy.ptr + 3, st);
+		BdParams p{prm->dt, prm->kT, static_cast<uint32_t>(step),
+				   mb2_bd_seed(prm->seed, prm->patch_id, step), 0u,
+				   {prm->efield[0], prm->efield[1], prm->efield[2]}};
+		bd_integrate(pos, fe, type_ids, flags, n, ctx->types, ctx->box, p, st);
+	});
+}
+
+int mb2_set_lanes_per_row(mb2_context* ctx, int lanes) {
+	return guarded(ctx, [&] {
+		require(lanes == 0 || lanes == 4 || lanes == 8 || lanes == 16 || lanes == 32, MB2_ERR_ARG,
+				"mb2_set_lanes_per_row: 0, 4, 8, 16 or 32");
+		ctx->lanes_per_row = lanes;
+	});
+}
+
+}  // extern "C"

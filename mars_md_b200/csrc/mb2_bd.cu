@@ -1,0 +1,262 @@
+// Brownian-dynamics integrator with the fused position-dependent force.
+//
+// Replaces BDIntegrate<float> (src/PatchOperation/Integrator/BD.h:44-92) with
+// compute_position_dependent_force (src/Interactions/Nonbonded/Pmf.h:68-124)
+// and the trilinear grid sampling of src/Types/BaseGridDevice.h:218-365.
+//
+// Per particle: skip FLAG_RB_ATTACHED; F += q E + sum over the type's PMF
+// terms of -scale * grad U (energy scale * U into .w) + per-axis force grids;
+// Philox4x32-10 with key = base_seed and counter (base_ctr + slot, 0x5324120,
+// step, 0); Box-Muller; x += (D/kT) F dt + sqrt(2 D dt) xi per axis; wrap.
+// The Philox integers are bit-identical to the reference; logf/sinf/cosf are
+// CUDA's (not fast-math), within a few ulp of the host libm the reference's
+// CPU build uses.
+#include "mb2_internal.cuh"
+
+namespace mb2 {
+
+namespace {
+
+// map_grid_index (BaseGridDevice.h:218-232).
+__device__ __forceinline__ bool map_index(int& j, long long n, int bc) {
+	const int ni = static_cast<int>(n);
+	if (j >= 0 && j < ni) return true;
+	if (bc == 2) {
+		j = ((j % ni) + ni) % ni;
+		return true;
+	}
+	if (bc == 1) {
+		j = j < 0 ? 0 : ni - 1;
+		return true;
+	}
+	return false;
+}
+
+__device__ __forceinline__ float fetch(const GridView& g, int jx, int jy, int jz, int bc) {
+	if (!map_index(jx, g.dims[0], bc) || !map_index(jy, g.dims[1], bc) ||
+		!map_index(jz, g.dims[2], bc))
+		return 0.0f;
+	const size_t idx = static_cast<size_t>(jz) + static_cast<size_t>(jy) * g.dims[2] +
+					   static_cast<size_t>(jx) * g.dims[1] * g.dims[2];
+	return __ldg(g.data + idx);
+}
+
+// Trilinear value and analytic gradient (interpolate_grid_point and
+// compute_gradient, BaseGridDevice.h:256-365), same operation order.
+__device__ __forceinline__ void grid_sample(const GridView& g, float px, float py, float pz, int bc,
+											float& value, float3& grad) {
+	const float dx = __fsub_rn(px, g.origin[0]), dy = __fsub_rn(py, g.origin[1]),
+				dz = __fsub_rn(pz, g.origin[2]);
+	const float* m = g.basis_inv;  // column-major
+	float gp[3];
+#pragma unroll
+	for (int r = 0; r < 3; ++r)
+		gp[r] = __fadd_rn(__fadd_rn(__fmul_rn(dx, m[r]), __fmul_rn(dy, m[3 + r])),
+						  __fmul_rn(dz, m[6 + r]));
+	const int i0 = static_cast<int>(floorf(gp[0]));
+	const int j0 = static_cast<int>(floorf(gp[1]));
+	const int k0 = static_cast<int>(floorf(gp[2]));
+	const float fx = __fsub_rn(gp[0], static_cast<float>(i0));
+	const float fy = __fsub_rn(gp[1], static_cast<float>(j0));
+	const float fz = __fsub_rn(gp[2], static_cast<float>(k0));
+	const float v000 = fetch(g, i0, j0, k0, bc), v001 = fetch(g, i0, j0, k0 + 1, bc);
+	const float v010 = fetch(g, i0, j0 + 1, k0, bc), v011 = fetch(g, i0, j0 + 1, k0 + 1, bc);
+	const float v100 = fetch(g, i0 + 1, j0, k0, bc), v101 = fetch(g, i0 + 1, j0, k0 + 1, bc);
+	const float v110 = fetch(g, i0 + 1, j0 + 1, k0, bc),
+				v111 = fetch(g, i0 + 1, j0 + 1, k0 + 1, bc);
+	const float ox = __fsub_rn(1.0f, fx), oy = __fsub_rn(1.0f, fy), oz = __fsub_rn(1.0f, fz);
+	auto lerp = [](float a, float wa, float b, float wb) {
+		return __fadd_rn(__fmul_rn(a, wa), __fmul_rn(b, wb));
+	};
+	const float v00 = lerp(v000, ox, v100, fx), v01 = lerp(v001, ox, v101, fx);
+	const float v10 = lerp(v010, ox, v110, fx), v11 = lerp(v011, ox, v111, fx);
+	const float v0 = lerp(v00, oy, v10, fy), v1 = lerp(v01, oy, v11, fy);
+	value = lerp(v0, oz, v1, fz);
+	auto term = [](float w1, float w2, float d) { return __fmul_rn(__fmul_rn(w1, w2), d); };
+	const float gx = __fadd_rn(__fadd_rn(__fadd_rn(term(oy, oz, __fsub_rn(v100, v000)),
+												   term(fy, oz, __fsub_rn(v110, v010))),
+										 term(oy, fz, __fsub_rn(v101, v001))),
+							   term(fy, fz, __fsub_rn(v111, v011)));
+	const float gy = __fadd_rn(__fadd_rn(__fadd_rn(term(ox, oz, __fsub_rn(v010, v000)),
+												   term(fx, oz, __fsub_rn(v110, v100))),
+										 term(ox, fz, __fsub_rn(v011, v001))),
+							   term(fx, fz, __fsub_rn(v111, v101)));
+	const float gz = __fadd_rn(__fadd_rn(__fadd_rn(term(ox, oy, __fsub_rn(v001, v000)),
+												   term(fx, oy, __fsub_rn(v101, v100))),
+										 term(ox, fy, __fsub_rn(v011, v010))),
+							   term(fx, fy, __fsub_rn(v111, v110)));
+	// transpose(basis_inv).transform(g): row r of basis_inv dotted with g
+	grad.x = __fadd_rn(__fadd_rn(__fmul_rn(gx, m[0]), __fmul_rn(gy, m[1])), __fmul_rn(gz, m[2]));
+	grad.y = __fadd_rn(__fadd_rn(__fmul_rn(gx, m[3]), __fmul_rn(gy, m[4])), __fmul_rn(gz, m[5]));
+	grad.z = __fadd_rn(__fadd_rn(__fmul_rn(gx, m[6]), __fmul_rn(gy, m[7])), __fmul_rn(gz, m[8]));
+}
+
+// compute_position_dependent_force (Pmf.h:68-124).
+__device__ __forceinline__ float4 position_force(const TypeTable& ty, int type, float px, float py,
+												 float pz, const float* efield) {
+	const float q = ty.charge[type];
+	float4 f = make_float4(__fmul_rn(q, efield[0]), __fmul_rn(q, efield[1]),
+						   __fmul_rn(q, efield[2]), 0.0f);
+	if (ty.num_grids == 0) return f;
+	const int begin = ty.pmf_offset[type];
+	const int end = begin + ty.pmf_count[type];
+	for (int k = begin; k < end; ++k) {
+		const GridTermDev term = ty.terms[k];
+		if (term.grid_id < 0) continue;
+		const GridView& g = ty.grids[term.grid_id];
+		if (g.data == nullptr) continue;
+		const int bc = term.boundary_condition >= 0 ? term.boundary_condition : g.boundary_condition;
+		float value;
+		float3 grad;
+		grid_sample(g, px, py, pz, bc, value, grad);
+		const float s = -term.scale;
+		f.x = __fadd_rn(f.x, __fmul_rn(grad.x, s));
+		f.y = __fadd_rn(f.y, __fmul_rn(grad.y, s));
+		f.z = __fadd_rn(f.z, __fmul_rn(grad.z, s));
+		f.w = __fadd_rn(f.w, __fmul_rn(term.scale, value));
+	}
+	const int4 fg = ty.force_grid_id[type];
+	const float4 fs = ty.force_grid_scale[type];
+	const int ids[3] = {fg.x, fg.y, fg.z};
+	const float sc[3] = {fs.x, fs.y, fs.z};
+	float* comp[3] = {&f.x, &f.y, &f.z};
+#pragma unroll
+	for (int a = 0; a < 3; ++a) {
+		if (ids[a] < 0) continue;
+		const GridView& g = ty.grids[ids[a]];
+		if (g.data == nullptr) continue;
+		float value;
+		float3 grad;
+		grid_sample(g, px, py, pz, g.boundary_condition, value, grad);
+		*comp[a] = __fadd_rn(*comp[a], __fmul_rn(sc[a], value));
+	}
+	return f;
+}
+
+// Box-Muller of one Philox draw (BD.h:66-78).
+__device__ __forceinline__ float3 bd_noise(uint64_t seed, uint32_t ctr, uint32_t step) {
+	const uint4 u = philox4x32_10(seed, ctr, kBdStream, step, 0u);
+	const float ux = u01(u.x), uy = u01(u.y), uz = u01(u.z), uw = u01(u.w);
+	const float r1 = __fsqrt_rn(__fmul_rn(-2.0f, logf(ux)));
+	const float t1 = __fmul_rn(6.2831854820251465f, uy);  // 2.0f * 3.1415926535f
+	const float r2 = __fsqrt_rn(__fmul_rn(-2.0f, logf(uz)));
+	const float t2 = __fmul_rn(6.2831854820251465f, uw);
+	float s1, c1;
+	sincosf(t1, &s1, &c1);
+	return make_float3(__fmul_rn(r1, c1), __fmul_rn(r1, s1), __fmul_rn(r2, cosf(t2)));
+}
+
+// x + ((D / kT) F dt + sqrt(2 D dt) xi), as BD.h:80-85 groups it.
+__device__ __forceinline__ float bd_axis(float x, float d, float kT, float f, float dt, float xi) {
+	const float drift = __fmul_rn(__fmul_rn(__fdiv_rn(d, kT), f), dt);
+	const float noise = __fmul_rn(__fsqrt_rn(__fmul_rn(__fmul_rn(2.0f, d), dt)), xi);
+	return __fadd_rn(x, __fadd_rn(drift, noise));
+}
+
+__device__ __forceinline__ float4 bd_update(float4 p, float fx, float fy, float fz, const float4& dif,
+											const float3& xi, const Box& box, const BdParams& bp) {
+	p.x = bd_axis(p.x, dif.x, bp.kT, fx, bp.dt, xi.x);
+	p.y = bd_axis(p.y, dif.y, bp.kT, fy, bp.dt, xi.y);
+	p.z = bd_axis(p.z, dif.z, bp.kT, fz, bp.dt, xi.z);
+	if (box.periodic[0]) p.x = wrap_scalar(p.x, box.origin[0], box.size[0], box.inv[0]);
+	if (box.periodic[1]) p.y = wrap_scalar(p.y, box.origin[1], box.size[1], box.inv[1]);
+	if (box.periodic[2]) p.z = wrap_scalar(p.z, box.origin[2], box.size[2], box.inv[2]);
+	return p;
+}
+
+__global__ void __launch_bounds__(256) bd_kernel(float4* __restrict__ pos, float4* __restrict__ fe,
+												 const int* __restrict__ type_ids,
+												 const uint32_t* __restrict__ flags, uint32_t n,
+												 TypeTable ty, Box box, BdParams bp) {
+	const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+	if (i >= n) return;
+	if (flags && (flags[i] & kFlagRbAttached)) return;
+	float4 p = pos[i];
+	float4 f = fe[i];
+	const int type = type_ids[i];
+	const float4 pmf = position_force(ty, type, p.x, p.y, p.z, bp.efield);
+	f.x = __fadd_rn(f.x, pmf.x);
+	f.y = __fadd_rn(f.y, pmf.y);
+	f.z = __fadd_rn(f.z, pmf.z);
+	if (pmf.w != 0.0f) fe[i].w = __fadd_rn(f.w, pmf.w);
+	const float3 xi = bd_noise(bp.base_seed, bp.base_ctr + i, bp.step);
+	pos[i] = bd_update(p, f.x, f.y, f.z, ty.diffusion[type], xi, box, bp);
+}
+
+// Sorted-order variant used by the fused step: force from the sorted
+// accumulator (zeroed here for the next step) plus the caller's array, noise
+// keyed on the original slot, positions written to both orders.
+__global__ void __launch_bounds__(256) bd_sorted_kernel(
+	float4* __restrict__ sorted_pos, float4* __restrict__ fs, const uint32_t* __restrict__ s2o,
+	float4* __restrict__ pos, float4* __restrict__ fe, const int* __restrict__ type_ids,
+	const uint32_t* __restrict__ flags, uint32_t n, TypeTable ty, Box box, BdParams bp,
+	int write_fe) {
+	const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
+	if (s >= n) return;
+	const uint32_t o = s2o[s];
+	float4 sp = sorted_pos[s];
+	float4 f = fs[s];
+	fs[s] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+	if (fe) {
+		const float4 ext = fe[o];
+		f.x = __fadd_rn(ext.x, f.x);
+		f.y = __fadd_rn(ext.y, f.y);
+		f.z = __fadd_rn(ext.z, f.z);
+		f.w = __fadd_rn(ext.w, f.w);
+	}
+	const int type = type_of(sp);
+	if (!(flags && (flags[o] & kFlagRbAttached))) {
+		const float4 pmf = position_force(ty, type, sp.x, sp.y, sp.z, bp.efield);
+		f.x = __fadd_rn(f.x, pmf.x);
+		f.y = __fadd_rn(f.y, pmf.y);
+		f.z = __fadd_rn(f.z, pmf.z);
+		f.w = __fadd_rn(f.w, pmf.w);
+		const float3 xi = bd_noise(bp.base_seed, bp.base_ctr + o, bp.step);
+		sp = bd_update(sp, f.x, f.y, f.z, ty.diffusion[type], xi, box, bp);
+		sorted_pos[s] = sp;
+		float4 out = pos[o];
+		out.x = sp.x;
+		out.y = sp.y;
+		out.z = sp.z;
+		pos[o] = out;
+	}
+	if (write_fe && fe) fe[o] = f;
+}
+
+__global__ void philox_kernel(uint64_t seed, uint32_t ctr0, uint32_t ctr1, uint32_t ctr2,
+							  uint32_t n, uint4* out4, float4* normals4) {
+	const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+	if (i >= n) return;
+	if (out4) out4[i] = philox4x32_10(seed, ctr0 + i, ctr1, ctr2, 0u);
+	if (normals4) {
+		const float3 xi = bd_noise(seed, ctr0 + i, ctr2);
+		normals4[i] = make_float4(xi.x, xi.y, xi.z, 0.0f);
+	}
+}
+
+}  // namespace
+
+void bd_integrate(float4* pos, float4* fe, const int* type_ids, const uint32_t* flags, uint32_t n,
+				  const TypeTable& types, const Box& box, const BdParams& p, cudaStream_t st) {
+	if (n == 0) return;
+	bd_kernel<<<(n + 255) / 256, 256, 0, st>>>(pos, fe, type_ids, flags, n, types, box, p);
+}
+
+void bd_integrate_sorted(float4* sorted_pos, float4* force_sorted, const uint32_t* s2o,
+						 float4* pos, float4* fe, const int* type_ids, const uint32_t* flags,
+						 uint32_t n, const TypeTable& types, const Box& box, const BdParams& p,
+						 int write_fe, cudaStream_t st) {
+	if (n == 0) return;
+	bd_sorted_kernel<<<(n + 255) / 256, 256, 0, st>>>(sorted_pos, force_sorted, s2o, pos, fe,
+													  type_ids, flags, n, types, box, p, write_fe);
+}
+
+void philox_draws(uint64_t seed, uint32_t ctr0, uint32_t ctr1, uint32_t ctr2, uint32_t n,
+				  uint32_t* out4, float* normals4, cudaStream_t st) {
+	if (n == 0) return;
+	philox_kernel<<<(n + 255) / 256, 256, 0, st>>>(seed, ctr0, ctr1, ctr2, n,
+												   reinterpret_cast<uint4*>(out4),
+												   reinterpret_cast<float4*>(normals4));
+}
+
+}  // namespace mb2

@@ -1,0 +1,186 @@
+// Internal declarations shared by the CUDA translation units of libmarsb200.
+#pragma once
+
+#include <cstddef>
+#include <cstdint>
+#include <cuda_runtime.h>
+#include <string>
+#include <vector>
+
+#include "mb2_common.cuh"
+
+namespace mb2 {
+
+// Thrown inside the library, turned into a status code at the C boundary.
+struct Error {
+	int code;
+	std::string msg;
+};
+
+#define MB2_CUDA(call)                                                                  \
+	do {                                                                                \
+		cudaError_t e_ = (call);                                                        \
+		if (e_ != cudaSuccess)                                                          \
+			throw ::mb2::Error{2, std::string(#call) + ": " + cudaGetErrorString(e_)};   \
+	} while (0)
+
+// Device buffer that only grows; owned by a context.
+template <typename T>
+struct DevBuf {
+	T* ptr = nullptr;
+	size_t cap = 0;
+	void ensure(size_t n) {
+		if (n <= cap) return;
+		if (ptr) cudaFree(ptr);
+		ptr = nullptr;
+		cap = 0;
+		const size_t want = n < 16 ? 16 : n;
+		MB2_CUDA(cudaMalloc(&ptr, want * sizeof(T)));
+		cap = want;
+	}
+	void release() {
+		if (ptr) cudaFree(ptr);
+		ptr = nullptr;
+		cap = 0;
+	}
+};
+
+// Context-owned scratch for sorting and scanning.
+struct Scratch {
+	DevBuf<uint32_t> keys_alt, vals_alt, hist, scan_blocks;
+	uint32_t* sort_keys_alt = nullptr;
+	uint32_t* sort_vals_alt = nullptr;
+	uint32_t* sort_hist = nullptr;
+	void ensure_sort(size_t n, size_t hist_n) {
+		keys_alt.ensure(n);
+		vals_alt.ensure(n);
+		hist.ensure(hist_n);
+		sort_keys_alt = keys_alt.ptr;
+		sort_vals_alt = vals_alt.ptr;
+		sort_hist = hist.ptr;
+	}
+	void release() {
+		keys_alt.release();
+		vals_alt.release();
+		hist.release();
+		scan_blocks.release();
+	}
+};
+
+// One entry of the cell stencil: offsets to add to the home cell.
+struct StencilEntry {
+	int dx, dy, dz, pad;
+};
+
+// sort.cu
+void morton_encode(const float4* pos, uint32_t n, const float* bmin, const float* bmax,
+				   uint32_t* keys, uint32_t* idx, cudaStream_t st);
+void radix_sort_pairs(Scratch& s, uint32_t* keys, uint32_t* vals, uint32_t n, cudaStream_t st);
+void inverse_and_gather(const uint32_t* s2o, uint32_t n, const float4* pos, uint32_t* inv,
+						float4* sorted_pos, cudaStream_t st);
+
+// scan.cu: exclusive prefix sum of n u32 values (in == out allowed). If
+// total is non-null the grand total is stored there (device pointer).
+void exclusive_scan_u32(Scratch& s, const uint32_t* in, uint32_t* out, size_t n, uint32_t* total,
+						cudaStream_t st);
+
+// Exclusion view (src/Interactions/DeviceExclusions.h:22-75), device pointers.
+struct Exclusions {
+	const int* offsets = nullptr;
+	const int* neighbors = nullptr;
+	uint32_t num_particles = 0;
+	const int* rigid_body_id = nullptr;
+};
+
+// pairlist.cu
+struct CellGrid {
+	int m = 0;                 // cells per axis = 2^m
+	int shift = 30;            // 3 * (10 - m)
+	int num_stencil = 0;
+	std::vector<StencilEntry> stencil;
+};
+CellGrid choose_cell_grid(const float* extent, const int* periodic, float rc_list, size_t n);
+void cell_ranges(const uint32_t* keys, uint32_t n, int shift, uint32_t* begin, uint32_t* end,
+				 size_t num_cells, cudaStream_t st);
+void neighbor_count(const float4* sorted_pos, const uint32_t* keys, const uint32_t* s2o,
+					const uint32_t* begin, const uint32_t* end, const StencilEntry* stencil,
+					int num_stencil, int m, int shift, float rc2, uint32_t n, const Box& box,
+					const Exclusions& ex, uint32_t* counts, cudaStream_t st);
+void neighbor_fill(const float4* sorted_pos, const uint32_t* keys, const uint32_t* s2o,
+				   const uint32_t* begin, const uint32_t* end, const StencilEntry* stencil,
+				   int num_stencil, int m, int shift, float rc2, uint32_t n, const Box& box,
+				   const Exclusions& ex, const uint32_t* row_start, uint32_t* nbr,
+				   cudaStream_t st);
+void export_pairs(const uint32_t* row_start, const uint32_t* nbr, const uint32_t* s2o,
+				  uint32_t n, int2* out, cudaStream_t st);
+void max_displacement_sq(const float4* cur, const float4* prev, uint32_t n, const Box& box,
+						 unsigned int* out_bits, cudaStream_t st);
+void pack_sorted_positions(const float4* pos, const int* type_ids, const uint32_t* s2o,
+						   uint32_t n, float4* sorted_pos, cudaStream_t st);
+
+// forces.cu
+struct PairTables {
+	int num_types = 0;
+	int num_tables = 0;
+	uint32_t* term_matrix = nullptr;  // device [T*T]
+	Table* tables = nullptr;          // device [num_tables], pot pointers into values
+	float* values = nullptr;          // device, concatenated
+	uint32_t total_values = 0;
+};
+void pair_forces(const float4* sorted_pos, const uint32_t* row_start, const uint32_t* nbr,
+				 uint32_t n, const PairTables& t, const Box& box, float cutoff_sq, int get_energy,
+				 float4* force_sorted, double* energy_virial, int lanes_per_row,
+				 cudaStream_t st);
+void scatter_add_forces(const float4* force_sorted, const uint32_t* s2o, uint32_t n,
+						float4* force_energy, int get_energy, cudaStream_t st);
+void bond_forces(const int2* bonds, const int* table_idx, uint32_t nb, const float4* pos,
+				 float4* fe, const Table* tables, const Box& box, int get_energy,
+				 double* energy, cudaStream_t st);
+void angle_forces(const int4* angles, const int* table_idx, uint32_t na, const float4* pos,
+				  float4* fe, const Table* tables, const Box& box, int get_energy, double* energy,
+				  cudaStream_t st);
+
+// bd.cu
+struct GridView {
+	const float* data;
+	float origin[3];
+	float basis_inv[9];  // column-major
+	long long dims[3];
+	int boundary_condition;
+};
+struct GridTermDev {
+	int grid_id;
+	float scale;
+	float scale_slope;
+	int boundary_condition;
+};
+struct TypeTable {
+	int num_types = 0;
+	const float* charge = nullptr;          // device [T]
+	const float4* diffusion = nullptr;      // device [T]
+	const int* pmf_offset = nullptr;        // device [T]
+	const int* pmf_count = nullptr;         // device [T]
+	const GridTermDev* terms = nullptr;     // device
+	const int4* force_grid_id = nullptr;    // device [T]
+	const float4* force_grid_scale = nullptr;
+	const GridView* grids = nullptr;        // device
+	int num_grids = 0;
+};
+struct BdParams {
+	float dt;
+	float kT;
+	uint32_t step;
+	uint64_t base_seed;
+	uint32_t base_ctr;
+	float efield[3];
+};
+void bd_integrate(float4* pos, float4* fe, const int* type_ids, const uint32_t* flags, uint32_t n,
+				  const TypeTable& types, const Box& box, const BdParams& p, cudaStream_t st);
+void bd_integrate_sorted(float4* sorted_pos, float4* force_sorted, const uint32_t* s2o,
+						 float4* pos, float4* fe, const int* type_ids, const uint32_t* flags,
+						 uint32_t n, const TypeTable& types, const Box& box, const BdParams& p,
+						 int write_fe, cudaStream_t st);
+void philox_draws(uint64_t seed, uint32_t ctr0, uint32_t ctr1, uint32_t ctr2, uint32_t n,
+				  uint32_t* out4, float* normals4, cudaStream_t st);
+
+}  // namespace mb2

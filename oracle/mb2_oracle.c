@@ -337,8 +337,9 @@ uint64_t or_neighbor_walk(const float* sorted_pos4, const uint32_t* keys, const 
                           const uint32_t* begin, const uint32_t* end, const uint32_t* table,
                           int npc, int shift, float cutoff_sq, size_t n, const or_box* b,
                           const int* excl_offsets, const int* excl_neighbors, size_t excl_n,
-                          const int* rigid_body_id, int* pairs, uint64_t max_pairs) {
-	uint64_t count = 0;
+                          const int* rigid_body_id, int* pairs, uint64_t max_pairs,
+                          uint64_t* checksum) {
+	uint64_t count = 0, sum = 0;
 	for (size_t i = 0; i < n; ++i) {
 		const float* pi = sorted_pos4 + 4 * i;
 		const uint32_t cell = keys[i] >> shift;
@@ -362,11 +363,15 @@ uint64_t or_neighbor_walk(const float* sorted_pos4, const uint32_t* keys, const 
 						pairs[2 * count] = a < bb ? a : bb;
 						pairs[2 * count + 1] = a < bb ? bb : a;
 					}
+					if (checksum)
+						sum += or_pair_hash(a, bb);
 					++count;
 				}
 			}
 		}
 	}
+	if (checksum)
+		*checksum = sum;
 	return count;
 }
 
@@ -388,6 +393,17 @@ uint64_t or_build_pairlist(const float* pos4, size_t n, const or_box* b, float r
                            const int* excl_offsets, const int* excl_neighbors, size_t excl_n,
                            const int* rigid_body_id, int* pairs, uint64_t max_pairs,
                            uint64_t* checksum) {
+	return or_build_pairlist_m(pos4, n, b, rc_list, excl_offsets, excl_neighbors, excl_n,
+	                           rigid_body_id, pairs, max_pairs, checksum, -1);
+}
+
+/* As or_build_pairlist, with the cell level m forced (m_force >= 0) instead of
+ * the reference's choice; the stencil radii follow the reference's rule for
+ * that m (ZOrderPairlist.cpp:48-56). The pair set does not depend on m. */
+uint64_t or_build_pairlist_m(const float* pos4, size_t n, const or_box* b, float rc_list,
+                             const int* excl_offsets, const int* excl_neighbors, size_t excl_n,
+                             const int* rigid_body_id, int* pairs, uint64_t max_pairs,
+                             uint64_t* checksum, int m_force) {
 	if (n == 0) {
 		if (checksum)
 			*checksum = 0;
@@ -411,6 +427,19 @@ uint64_t or_build_pairlist(const float* pos4, size_t n, const or_box* b, float r
 	/* The pair-buffer guard in the grid choice never binds for a grown buffer
 	 * (ZOrderPairlist.h:170-177); pass an effectively unbounded capacity. */
 	or_select_cell_grid(extent, cutoff, n, (size_t)1 << 40, &m, radii, &slots);
+	if (m_force >= 0) {
+		m = m_force;
+		slots = 1;
+		for (int a = 0; a < 3; ++a) {
+			const long long cells = 1LL << m;
+			const double side = (double)extent[a] / (double)cells;
+			radii[a] = (int)ceil((double)cutoff / side);
+			long long span = 2LL * radii[a] + 1LL;
+			if (span > cells)
+				span = cells;
+			slots *= (int)span;
+		}
+	}
 	const size_t num_cells = (size_t)1 << (3 * m);
 	const int shift = 3 * (10 - m);
 	uint32_t* begin = (uint32_t*)calloc(num_cells, 4);
@@ -420,34 +449,8 @@ uint64_t or_build_pairlist(const float* pos4, size_t n, const or_box* b, float r
 	or_cell_neighbors(table, m, radii, slots, box_len);
 	const uint64_t count =
 	    or_neighbor_walk(spos, keys, s2o, begin, end, table, slots, shift, cutoff_sq, n, b,
-	                     excl_offsets, excl_neighbors, excl_n, rigid_body_id, pairs, max_pairs);
-	if (checksum) {
-		/* A second walk without storage accumulates the checksum. */
-		uint64_t sum = 0;
-		for (size_t i = 0; i < n; ++i) {
-			const float* pi = spos + 4 * i;
-			const uint32_t* nbrs = table + (size_t)(keys[i] >> shift) * slots;
-			const int a = (int)s2o[i];
-			for (int k = 0; k < slots; ++k) {
-				const uint32_t nc = nbrs[k];
-				if (nc == 0xFFFFFFFFu)
-					continue;
-				const uint32_t lo = begin[nc] > (uint32_t)i + 1u ? begin[nc] : (uint32_t)i + 1u;
-				for (uint32_t j = lo; j < end[nc]; ++j) {
-					const float* pj = spos + 4 * (size_t)j;
-					const float d[3] = {pj[0] - pi[0], pj[1] - pi[1], pj[2] - pi[2]};
-					float w[3];
-					box_wrap_diff(b, d, w);
-					if (len2(w) <= cutoff_sq) {
-						const int bb = (int)s2o[j];
-						if (!excluded(a, bb, excl_offsets, excl_neighbors, excl_n, rigid_body_id))
-							sum += or_pair_hash(a, bb);
-					}
-				}
-			}
-		}
-		*checksum = sum;
-	}
+	                     excl_offsets, excl_neighbors, excl_n, rigid_body_id, pairs, max_pairs,
+	                     checksum);
 	free(keys);
 	free(s2o);
 	free(spos);

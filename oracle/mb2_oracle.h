@@ -95,11 +95,16 @@ uint64_t or_neighbor_walk(const float* sorted_pos4, const uint32_t* keys, const 
                           const uint32_t* begin, const uint32_t* end, const uint32_t* table,
                           int npc, int shift, float cutoff_sq, size_t n, const or_box* b,
                           const int* excl_offsets, const int* excl_neighbors, size_t excl_n,
-                          const int* rigid_body_id, int* pairs, uint64_t max_pairs);
+                          const int* rigid_body_id, int* pairs, uint64_t max_pairs,
+                          uint64_t* checksum);
 uint64_t or_build_pairlist(const float* pos4, size_t n, const or_box* b, float rc_list,
                            const int* excl_offsets, const int* excl_neighbors, size_t excl_n,
                            const int* rigid_body_id, int* pairs, uint64_t max_pairs,
                            uint64_t* checksum);
+uint64_t or_build_pairlist_m(const float* pos4, size_t n, const or_box* b, float rc_list,
+                             const int* excl_offsets, const int* excl_neighbors, size_t excl_n,
+                             const int* rigid_body_id, int* pairs, uint64_t max_pairs,
+                             uint64_t* checksum, int m_force);
 uint64_t or_pair_hash(int a, int b);
 int or_exclusion_csr(const int* pairs, size_t n_pairs, int* offsets, int* neighbors,
                      size_t* n_excl_particles);

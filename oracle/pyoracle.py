@@ -196,9 +196,11 @@ class Oracle:
         L.or_cell_neighbors.argtypes = [vp, i, vp, i, vp]
         L.or_neighbor_walk.restype = u64
         L.or_neighbor_walk.argtypes = [vp, vp, vp, vp, vp, vp, i, i, f, sz, vp, vp, vp, sz, vp,
-                                       vp, u64]
+                                       vp, u64, vp]
         L.or_build_pairlist.restype = u64
         L.or_build_pairlist.argtypes = [vp, sz, vp, f, vp, vp, sz, vp, vp, u64, vp]
+        L.or_build_pairlist_m.restype = u64
+        L.or_build_pairlist_m.argtypes = [vp, sz, vp, f, vp, vp, sz, vp, vp, u64, vp, i]
         L.or_pair_hash.restype = u64
         L.or_pair_hash.argtypes = [i, i]
         L.or_exclusion_csr.argtypes = [vp, sz, vp, vp, vp]
@@ -285,22 +287,22 @@ class Oracle:
         return t
 
     def build_pairlist(self, pos4, box: Box, rc_list, excl=None, rigid_body_id=None,
-                       want_pairs=True, max_pairs=None):
+                       want_pairs=True, max_pairs=None, m=-1):
         """Pair set within rc_list: returns (pairs int32[P,2] sorted lexicographically
-        or None, count, checksum)."""
+        or None, count, checksum). m >= 0 forces the cell level (speed only)."""
         n = len(pos4)
         off, nb, excl_n = (None, None, 0) if excl is None else excl
         if want_pairs and max_pairs is None:
-            cnt = self.lib.or_build_pairlist(_ptr(pos4), n, C.byref(box), C.c_float(rc_list),
-                                             _ptr(off), _ptr(nb), excl_n, _ptr(rigid_body_id),
-                                             None, 0, None)
+            cnt = self.lib.or_build_pairlist_m(_ptr(pos4), n, C.byref(box), C.c_float(rc_list),
+                                               _ptr(off), _ptr(nb), excl_n, _ptr(rigid_body_id),
+                                               None, 0, None, m)
             max_pairs = int(cnt)
         buf = np.zeros((max_pairs if want_pairs else 0, 2), np.int32)
         cs = C.c_uint64()
-        cnt = self.lib.or_build_pairlist(_ptr(pos4), n, C.byref(box), C.c_float(rc_list),
-                                         _ptr(off), _ptr(nb), excl_n, _ptr(rigid_body_id),
-                                         _ptr(buf) if want_pairs else None,
-                                         max_pairs if want_pairs else 0, C.byref(cs))
+        cnt = self.lib.or_build_pairlist_m(_ptr(pos4), n, C.byref(box), C.c_float(rc_list),
+                                           _ptr(off), _ptr(nb), excl_n, _ptr(rigid_body_id),
+                                           _ptr(buf) if want_pairs else None,
+                                           max_pairs if want_pairs else 0, C.byref(cs), m)
         pairs = None
         if want_pairs:
             pairs = buf[: min(int(cnt), max_pairs)]

@@ -1,0 +1,248 @@
+"""CUDA pair/bond/angle forces, Philox, grid force and BD step against the oracle.
+
+Tolerances (float32 arithmetic):
+* Each pair's float force is rounded exactly as the reference's; per-particle
+  sums differ only by accumulation order, so the error is bounded relative to
+  the sum of |pair force| on that particle: <= 1e-5.
+* Energies: FP64 device reduction vs the FP64 oracle, <= 1e-6 relative.
+* Philox words: bit-exact. BD positions: the Box-Muller transcendentals are
+  CUDA's logf/sinf/cosf vs host libm (a few ulp), so positions agree to
+  1e-5 A absolute per step.
+Mirrors Unit_test/Interactions/NonbondedEnergy.cpp (pair sums vs CPU),
+Unit_test/Compute/BDKernels.cpp (bond chain, Box-Muller moments, free
+diffusion), Unit_test/Interactions/TabulatedBonded.cpp (angles) and
+Unit_test/Interactions/Pmf.cpp (grid forces).
+"""
+import numpy as np
+import pytest
+import torch
+
+import pyoracle
+from conftest import box_of, force_errors, tableset, u32
+from mars_md_b200 import workloads as W
+from mars_md_b200.engine import setup_workload
+
+pytestmark = pytest.mark.gpu
+
+
+def _pair_case(ctx, oracle, w, lanes=0):
+    dev = setup_workload(ctx, w)
+    if lanes:
+        ctx.set_lanes_per_row(lanes)
+    ctx.build_pairlist(dev["pos"], dev["type"], w.list_radius)
+    pairs = ctx.export_pairs().cpu().numpy()
+    ctx.reset_energies()
+    ctx.pair_forces(dev["pos"], dev["type"], dev["fe"], w.cutoff, get_energy=True)
+    e = ctx.energies()
+    fe = dev["fe"].cpu().numpy()
+    tags = oracle.resolve_tags(pairs, w.type_ids, w.term_matrix, w.num_types)
+    rc2 = np.float32(w.cutoff) ** 2
+    f32, f64, fabs = oracle.pair_forces(pairs, w.pos, tags, tableset(w), box_of(w), rc2)
+    e64 = oracle.pair_energy_f64(pairs, w.pos, tags, tableset(w), box_of(w), rc2)
+    return fe, f64, fabs, e, e64
+
+
+@pytest.mark.parametrize("lanes", [0, 4, 8, 16, 32])
+def test_pair_forces_plain_bd(ctx_factory, oracle, lanes):
+    w = W.plain_bd()
+    ctx = ctx_factory(w.n)
+    fe, f64, fabs, e, e64 = _pair_case(ctx, oracle, w, lanes)
+    scaled, plain = force_errors(fe, f64, fabs)
+    assert scaled <= 1e-5, (scaled, plain)
+    # per-particle energy halves sum to the pair energy
+    assert abs(fe[:, 3].astype(np.float64).sum() - f64[:, 3].sum()) <= 1e-5 * abs(f64[:, 3]).sum()
+    assert abs(e[0] - e64) <= 1e-6 * abs(e64)
+    # Newton's third law: total force vanishes
+    assert np.abs(fe[:, :3].astype(np.float64).sum(0)).max() <= 1e-3 * fabs.sum() / len(fabs)
+
+
+def test_pair_forces_large_types(ctx_factory, oracle):
+    # 4 types, 10 tables, Debye-Hueckel + soft core, at 1/64 of the full size
+    w = W.large_plain(n=32768)
+    ctx = ctx_factory(w.n)
+    fe, f64, fabs, e, e64 = _pair_case(ctx, oracle, w)
+    scaled, plain = force_errors(fe, f64, fabs)
+    assert scaled <= 1e-5, (scaled, plain)
+    assert abs(e[0] - e64) <= 1e-6 * abs(e64)
+
+
+def test_pair_forces_match_reference_functor(ctx_factory, oracle, ref):
+    """Against the reference's own host-compiled PairNonbondedComputer."""
+    w = W.plain_bd()
+    ctx = ctx_factory(w.n)
+    fe, f64, fabs, e, e64 = _pair_case(ctx, oracle, w)
+    pairs, _, _ = oracle.build_pairlist(w.pos, box_of(w), w.list_radius)
+    tags = ref.resolve_tags(pairs, w.type_ids, w.term_matrix, w.num_types)
+    fref = ref.pair_forces(pairs, w.pos, w.type_ids, tags, tableset(w), box_of(w),
+                           np.float32(w.cutoff) ** 2)
+    scaled, _ = force_errors(fe, fref.astype(np.float64), fabs)
+    assert scaled <= 2e-5
+
+
+def _bonded_setup(ctx, w):
+    dev = setup_workload(ctx, w)
+    return dev
+
+
+def test_bond_and_angle_forces(ctx_factory, oracle):
+    w = W.polymers(n_chains=4, beads=1024, with_grid=False)
+    ctx = ctx_factory(w.n)
+    dev = _bonded_setup(ctx, w)
+    ctx.reset_energies()
+    ctx.bond_forces(dev["bonds"], dev["bond_idx"], dev["pos"], dev["fe"])
+    fb = dev["fe"].cpu().numpy().copy()
+    dev["fe"].zero_()
+    ctx.angle_forces(dev["angles"], dev["angle_idx"], dev["pos"], dev["fe"])
+    fa = dev["fe"].cpu().numpy()
+    e = ctx.energies()
+    bt = pyoracle.TableSet([(t.values, t.start, t.step_inv) for t in w.bond_tables])
+    at = pyoracle.TableSet([(t.values, t.start, t.step_inv) for t in w.angle_tables], periodic=True)
+    _, b64, babs = oracle.bond_forces(w.bonds, w.bond_table_idx, w.pos, bt, box_of(w))
+    _, a64, aabs = oracle.angle_forces(w.angles, w.angle_table_idx, w.pos, at, box_of(w))
+    sb, _ = force_errors(fb, b64, babs)
+    assert sb <= 1e-5
+    # acosf (CUDA) vs double acos rounded (host): the angle itself differs by an ulp
+    sa, _ = force_errors(fa, a64, aabs)
+    assert sa <= 1e-4, sa
+    assert abs(e[2] - b64[:, 3].sum()) <= 1e-6 * abs(b64[:, 3]).sum()
+    assert abs(e[3] - a64[:, 3].sum()) <= 1e-5 * abs(a64[:, 3]).sum()
+
+
+def test_bond_chain_end_forces(ctx_factory, oracle):
+    """129-bead straight chain at 1.885 A spacing: interior forces cancel, the
+    ends feel -/+ the table force (Unit_test/Compute/BDKernels.cpp:222-305)."""
+    n = 129
+    pos = np.zeros((n, 4), np.float32)
+    pos[:, 2] = 1.885 * np.arange(n, dtype=np.float32)
+    bonds = np.stack([np.arange(n - 1), np.arange(1, n)], axis=1).astype(np.int32)
+    tab = W.harmonic_bond_table(k=19.19, r0=3.8, bins=10001, dx=0.01)
+    ctx = ctx_factory(n)
+    ctx.set_box((0, 0, 0), (500, 500, 500), (1, 1, 1))
+    ctx.set_bonded_tables(0, [(tab.values, tab.start, tab.step_inv)])
+    d = torch.from_numpy(pos).cuda()
+    fe = torch.zeros_like(d)
+    ctx.bond_forces(torch.from_numpy(bonds).cuda(), torch.zeros(n - 1, dtype=torch.int32, device="cuda"),
+                    d, fe)
+    f = fe.cpu().numpy()
+    ts = pyoracle.TableSet([(tab.values, tab.start, tab.step_inv)])
+    fm, _ = oracle.table_lookup(ts, 0, 1.885)
+    assert abs(f[0, 2] + fm) <= 1e-5 * abs(fm)
+    assert abs(f[-1, 2] - fm) <= 1e-5 * abs(fm)
+    assert np.abs(f[1:-1, :3]).max() <= 1e-5 * abs(fm)
+
+
+def test_philox_bit_exact(ctx_factory, oracle):
+    ctx = ctx_factory(1)
+    seed = ctx.bd_seed(20261203, 0, 17)
+    assert seed == oracle.bd_seed(20261203, 0, 17)
+    words, normals = ctx.philox(seed, 0, 0x5324120, 17, 4096)
+    w = u32(words).reshape(-1, 4)
+    for i in (0, 1, 2, 1000, 4095):
+        assert np.array_equal(w[i], oracle.philox(seed, i, 0x5324120, 17))
+    nz = normals.cpu().numpy()[:, :3]
+    # Box-Muller normals: unit variance (BDKernels.cpp:46-91)
+    assert abs(nz.mean()) < 0.05 and abs(nz.var() - 1.0) < 0.05
+
+
+def test_philox_reference_draws(ctx_factory, ref):
+    ctx = ctx_factory(1)
+    words, _ = ctx.philox(123456789012345, 7, 0x5324120, 3, 1)
+    assert np.array_equal(u32(words)[0], ref.philox_int4(123456789012345, 7, 3, 0x5324120, 1)[0])
+
+
+def _bd_compare(ctx, oracle, w, dev, fe_np, step, grids=None):
+    types = pyoracle.TypeSet(w.charge, w.diffusion, w.pmf_terms)
+    gs = pyoracle.GridSet(w.grids) if w.grids else None
+    seed = oracle.bd_seed(w.seed, 0, step)
+    flags = np.zeros(w.n, np.uint32)
+    flags[5] = 4  # rigid-body attached: must not move
+    dflags = torch.from_numpy(flags.view(np.int32)).cuda()
+    dev["fe"].copy_(torch.from_numpy(fe_np))
+    ctx.bd_integrate(dev["pos"], dev["fe"], dev["type"], dflags, w.dt, w.kT, step, seed)
+    p_gpu = dev["pos"].cpu().numpy()
+    f_gpu = dev["fe"].cpu().numpy()
+    p_ref, f_ref, _ = oracle.bd_integrate(w.pos, fe_np, w.type_ids, flags, types, gs, box_of(w),
+                                          w.dt, w.kT, step, seed)
+    return p_gpu, f_gpu, p_ref, f_ref
+
+
+def test_bd_step_plain(ctx_factory, oracle):
+    w = W.plain_bd()
+    ctx = ctx_factory(w.n)
+    dev = setup_workload(ctx, w)
+    rng = np.random.default_rng(3)
+    fe = np.zeros((w.n, 4), np.float32)
+    fe[:, :3] = rng.normal(0, 5, (w.n, 3)).astype(np.float32)
+    p_gpu, f_gpu, p_ref, f_ref = _bd_compare(ctx, oracle, w, dev, fe, step=1)
+    d = np.abs(p_gpu[:, :3] - p_ref[:, :3])
+    d = np.minimum(d, 200.0 - d)  # periodic
+    assert d.max() <= 1e-5
+    assert np.array_equal(p_gpu[5], w.pos[5])
+
+
+def test_bd_step_with_grid(ctx_factory, oracle):
+    w = W.polymers(n_chains=8, beads=1024, with_grid=True)
+    ctx = ctx_factory(w.n)
+    dev = setup_workload(ctx, w)
+    fe = np.zeros((w.n, 4), np.float32)
+    p_gpu, f_gpu, p_ref, f_ref = _bd_compare(ctx, oracle, w, dev, fe, step=3)
+    d = np.abs(p_gpu[:, :3] - p_ref[:, :3])
+    d = np.minimum(d, 600.0 - d)
+    assert d.max() <= 1e-4
+    # grid energy in .w is a pure float function of the position: bit-exact
+    assert np.array_equal(f_gpu[:, 3], f_ref[:, 3])
+    assert (f_ref[:, 3] != 0).sum() > 100
+
+
+def test_free_diffusion_msd(ctx_factory):
+    """Free particles: MSD after k steps = 6 D t within 10 % (BDKernels.cpp:92-220)."""
+    n, steps = 20000, 50
+    w = W.plain_bd(n=n, box=1e5)
+    ctx = ctx_factory(n)
+    dev = setup_workload(ctx, w)
+    start = dev["pos"].clone()
+    for s in range(1, steps + 1):
+        dev["fe"].zero_()
+        ctx.bd_integrate(dev["pos"], dev["fe"], dev["type"], None, w.dt, w.kT, s,
+                         ctx.bd_seed(w.seed, 0, s))
+    d = (dev["pos"] - start)[:, :3].double()
+    d = d - 1e5 * torch.round(d / 1e5)  # minimum image across the periodic box
+    msd = float((d * d).sum(1).mean())
+    expect = 6.0 * W.DIFFUSION * w.dt * steps
+    assert abs(msd - expect) <= 0.1 * expect
+
+
+def test_fused_step_matches_composition(ctx_factory, oracle):
+    """mb2_step over 25 steps (one rebuild at step 21) against the oracle's
+    clear -> pairlist -> pair forces -> BD sequence, positions within 1e-4 A."""
+    from mars_md_b200.engine import step_params
+    w = W.plain_bd(n=2048, box=160.0)
+    ctx = ctx_factory(w.n)
+    dev = setup_workload(ctx, w)
+    prm = step_params(w)
+    box = box_of(w)
+    types = pyoracle.TypeSet(w.charge, w.diffusion)
+    pos = w.pos.copy()
+    rc2 = np.float32(w.cutoff) ** 2
+    pairs = None
+    ts = tableset(w)
+    snap = None
+    skin = w.list_radius - w.cutoff
+    blen = np.array(w.box_size, np.float32)
+    for s in range(1, 26):
+        ctx.step(dev["pos"], dev["fe"], dev["type"], None, s, prm)
+        # Patch.cpp:86-108: scheduled rebuild, skipped while the skin holds
+        rebuild = pairs is None or ((s - 1) % w.rebuild_period == 0 and
+                                    oracle.max_displacement(pos, snap, blen) > skin * 0.5)
+        if rebuild:
+            pairs, _, _ = oracle.build_pairlist(pos, box, w.list_radius)
+            snap = pos.copy()
+        tags = oracle.resolve_tags(pairs, w.type_ids, w.term_matrix, 1)
+        f32, _, _ = oracle.pair_forces(pairs, pos, tags, ts, box, rc2)
+        pos, _, _ = oracle.bd_integrate(pos, f32, w.type_ids, None, types, None, box, w.dt, w.kT,
+                                        s, oracle.bd_seed(w.seed, 0, s))
+    p = dev["pos"].cpu().numpy()
+    d = np.abs(p[:, :3] - pos[:, :3])
+    d = np.minimum(d, 160.0 - d)
+    assert d.max() <= 1e-3, d.max()
+    assert np.sqrt((d ** 2).mean()) <= 1e-5
