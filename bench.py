@@ -1,0 +1,318 @@
+"""Benchmark: Brownian-dynamics particle-steps/s on the 2,097,152-bead workload.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+One step = one full BD step of the hot path (clear forces, pairlist rebuild
+every 20 steps, tabulated pair forces, BD integrate with Philox noise) on the
+`large_plain` workload: 2,097,152 beads of 4 types at 0.002 A^-3 in a periodic
+cube, 10 pair tables of 400 bins, cutoff 30 A, pairlist radius 35 A. Inputs
+are seeded synthetic data (no dataset). The pairlist (~1.5 GB) is far larger
+than L2, so every timed step streams it from HBM (no L2 flush needed).
+
+Multi-GPU: the path does not shard; N GPUs run N independent replicas (one
+process per GPU, weak scaling), and `value` counts all replicas' work over
+the slowest rank's time.
+
+`--impl reference` times the reference's own CPU implementation of the path
+(its functors host-compiled in oracle/_ref) on this host's cores, on a bounded
+sample of the same workload scaled to the full system.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+import numpy as np  # noqa: E402
+
+METRIC = "particle-steps/s"
+WORKLOAD = "large_plain"
+
+
+def _config(w, extra=None):
+    cfg = {"workload": f"{WORKLOAD}: {w.n} beads, 4 types, 10 pair tables x 400 bins, "
+                       f"cutoff {w.cutoff} A, pairlist {w.list_radius} A, rebuild every "
+                       f"{w.rebuild_period} steps, box {w.box_size[0]:.1f} A periodic",
+           "beads": w.n, "rebuild_period": w.rebuild_period,
+           "l2": "inputs larger than L2 (the ~1.5 GB pairlist is streamed every step)",
+           "seed": w.seed}
+    if extra:
+        cfg.update(extra)
+    return cfg
+
+
+def _peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms."""
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index):
+        self.dev = device_index
+        self.proc = None
+        self.path = os.path.join(ROOT, "gpurun_out", f"clocks_{os.getpid()}.csv")
+
+    def start(self):
+        try:
+            os.makedirs(os.path.dirname(self.path), exist_ok=True)
+            self.f = open(self.path, "w")
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.dev}", f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.f,
+                stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.f.close()
+        rows = []
+        with open(self.path) as f:
+            for line in f:
+                parts = [p.strip() for p in line.split(",")]
+                if len(parts) >= 9:
+                    rows.append(parts)
+        if not rows:
+            return None
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        reasons = set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            for k, name in enumerate(names):
+                if r[5 + k].lower() == "active":
+                    reasons.add(name)
+        return {"sm_mhz": float(np.median(sm)) if sm else None,
+                "sm_max_mhz": float(rows[0][2]) if rows[0][2].replace(".", "").isdigit() else None,
+                "reasons": sorted(reasons), "samples": len(rows)}
+
+
+def _dist():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+def _traffic_from_profile():
+    """Per-launch DRAM bytes of the pair-force kernel from the committed ncu summary."""
+    path = os.path.join(ROOT, "profiles", "pair_force_large_plain.json")
+    if not os.path.exists(path):
+        return None
+    try:
+        with open(path) as f:
+            return json.load(f).get("dram_bytes_per_launch")
+    except Exception:
+        return None
+
+
+def run_ours(args):
+    import torch
+    import torch.distributed as dist
+    from mars_md_b200 import _lib, workloads as W
+    from mars_md_b200.engine import Context, setup_workload, step_params
+
+    world, rank, local = _dist()
+    torch.cuda.set_device(local)
+    if world > 1:
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=300))
+    w = W.large_plain(seed=W.DEFAULT_SEED + rank)
+    ctx = Context(w.n, device=local)
+    dev = setup_workload(ctx, w, device=f"cuda:{local}")
+    prm = step_params(w)
+    stream = torch.cuda.current_stream()
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    s = 0
+    for _ in range(args.warmup):
+        s += 1
+        ctx.step(dev["pos"], dev["fe"], dev["type"], None, s, prm)
+    torch.cuda.synchronize()
+    barrier()
+    clocks = ClockSampler(local)
+    clocks.start()
+    L = _lib.load()
+    launches0 = L.mb2_launch_count()
+    start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    start.record(stream)
+    rebuilds = 0
+    for _ in range(args.steps):
+        s += 1
+        if (s - 1) % w.rebuild_period == 0:
+            rebuilds += 1
+        ctx.step(dev["pos"], dev["fe"], dev["type"], None, s, prm)
+    stop.record(stream)
+    torch.cuda.synchronize()
+    launches = int(L.mb2_launch_count() - launches0)
+    barrier()
+    clk = clocks.stop()
+    ms = start.elapsed_time(stop)
+    if world > 1:
+        t = torch.tensor([ms], device=f"cuda:{local}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    value = world * w.n * args.steps / (ms / 1e3)
+
+    # Per-kernel device time over one rebuild period, on the launching stream.
+    ctx.set_profiling(True)
+    for _ in range(w.rebuild_period):
+        s += 1
+        ctx.step(dev["pos"], dev["fe"], dev["type"], None, s, prm)
+    torch.cuda.synchronize()
+    prof = {name: ctx.profile_read(st) for name, st in
+            (("step", _lib.STAGE_STEP), ("pairlist_build", _lib.STAGE_PAIRLIST),
+             ("pair_force_kernel", _lib.STAGE_PAIR_FORCE), ("integrate_kernel", _lib.STAGE_INTEGRATE))}
+    ctx.set_profiling(False)
+    npairs = ctx.num_pairs()
+    p_half = npairs / w.n
+
+    # e2e: the same step through the public C ABI with host buffers: every step
+    # copies positions host->device (pinned) and reads them back.
+    host_pos = torch.from_numpy(w.pos).pin_memory()
+    host_out = torch.empty_like(host_pos).pin_memory()
+    e_steps = args.steps
+    torch.cuda.synchronize()
+    barrier()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(e_steps):
+        s += 1
+        dev["pos"].copy_(host_pos, non_blocking=True)
+        ctx.step(dev["pos"], dev["fe"], dev["type"], None, s, prm)
+        host_out.copy_(dev["pos"], non_blocking=True)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    e_ms = e0.elapsed_time(e1)
+    if world > 1:
+        t = torch.tensor([e_ms], device=f"cuda:{local}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e_ms = float(t.item())
+    e_value = world * w.n * e_steps / (e_ms / 1e3)
+
+    bw, peak_kind = _peaks()
+    pf_ms, pf_n = prof["pair_force_kernel"]
+    pf_avg = pf_ms / max(pf_n, 1)
+    # Algorithmic bytes of one pair-force launch: one u32 index per stored half
+    # pair, plus one float4 position read and one float4 force write per bead.
+    pf_bytes = w.n * (4.0 * p_half + 32.0)
+    achieved = pf_bytes / (pf_avg / 1e3) / 1e9
+    traffic = _traffic_from_profile()
+    b_ps = 32.0 + 4.0 * p_half + (100.0 + 4.0 * p_half) / w.rebuild_period
+    roof_ps = bw * 1e9 / b_ps
+
+    out = {
+        "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded uniform beads, Debye-Hueckel + soft-core tables)",
+        "config": _config(w, {"parallelism": f"replicas x{world}", "pairs": npairs,
+                              "p_half": p_half, "rebuilds_in_timed_region": rebuilds,
+                              "step_roofline_bytes_per_particle_step": b_ps,
+                              "step_roofline_particle_steps_per_s": roof_ps,
+                              "step_roofline_frac": (value / world) / roof_ps,
+                              "kernel_ms": {k: (v[0] / max(v[1], 1)) for k, v in prof.items()},
+                              "hbm_peak": peak_kind}),
+        "roofline": {"bound": "hbm", "kernel": "pair_force", "achieved": achieved, "peak": bw,
+                     "unit": "GB/s", "frac": achieved / bw, "traffic": traffic,
+                     "algorithmic_bytes_per_launch": pf_bytes,
+                     "launch_ms": pf_avg, "peak_source": f"MEASURED_PEAKS.json ({peak_kind})"},
+        "e2e": {"value": e_value, "unit": METRIC, "h2d_bytes_per_step": w.n * 16,
+                "d2h_bytes_per_step": w.n * 16},
+        "gpu_launches": launches,
+        "clocks": clk,
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        out["cpu_baseline"] = cpu_baseline(w)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(out), flush=True)
+
+
+def cpu_baseline(w):
+    """The reference's CPU path on a bounded sample (about 10-30 s of CPU work)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import cpu_step
+    c = cpu_step.SampledStep(w, walk_sample=8192)
+    t_reb = c.rebuild()
+    t_step = c.forces_and_integrate(1)
+    per_step = t_step + t_reb / w.rebuild_period
+    return {"value": w.n / per_step, "unit": METRIC, "cores": c.nthreads, "kind": c.kind,
+            "sample": c.sample_desc + "; threads apply to encode, tag resolve and BD integrate "
+                                      "only (the reference's scatter functors are serial on "
+                                      "the host)",
+            "components_s": dict(c.last)}
+
+
+def run_reference(args):
+    world, rank, local = _dist()
+    if rank != 0:
+        return
+    from mars_md_b200 import workloads as W
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import cpu_step
+    w = W.large_plain()
+    c = cpu_step.SampledStep(w, walk_sample=8192)
+    s = 0
+    for _ in range(args.warmup):
+        s += 1
+        c.step(s)
+    total = 0.0
+    for _ in range(args.steps):
+        s += 1
+        total += c.step(s)
+    value = w.n * args.steps / total
+    print(json.dumps({
+        "impl": "reference", "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * total / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic", "config": _config(w, {"parallelism": "host CPU"}),
+        "cpu_baseline": {"value": value, "unit": METRIC, "cores": c.nthreads, "kind": c.kind,
+                         "sample": c.sample_desc},
+        "e2e": {"value": value, "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=40)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -211,6 +211,22 @@ MB2_API int mb2_step(mb2_context* ctx, float* pos4, float* force_energy4, const 
              const uint32_t* flags, uint32_t n, uint64_t step, const mb2_step_params* params,
              void* stream);
 
+/* --- tracing ---------------------------------------------------------------
+ * Per-stage device timing with CUDA events on the launching stream (replaces
+ * the reference's Profiler event timers, src/Backend/Profiler.h:166-205).
+ * While on, the fused step and the pairlist/pair-force calls record one
+ * event pair per stage; mb2_profile_read synchronises, returns the summed
+ * milliseconds and launch count of a stage, and clears it. */
+#define MB2_STAGE_STEP 0       /* whole mb2_step */
+#define MB2_STAGE_PAIRLIST 1   /* pairlist build: sort + walks */
+#define MB2_STAGE_PAIR_FORCE 2 /* the pair-force kernel alone */
+#define MB2_STAGE_INTEGRATE 3  /* the BD integrate kernel */
+#define MB2_NUM_STAGES 4
+MB2_API int mb2_set_profiling(mb2_context* ctx, int on);
+/* Number of kernels this library has launched in this process (all contexts). */
+MB2_API uint64_t mb2_launch_count(void);
+MB2_API int mb2_profile_read(mb2_context* ctx, int stage, double* total_ms, uint32_t* count);
+
 /* Rows (particles) served by one group of lanes in the pair kernel: 4, 8, 16
  * or 32 lanes per row; 0 = choose from the mean row length. */
 MB2_API int mb2_set_lanes_per_row(mb2_context* ctx, int lanes);

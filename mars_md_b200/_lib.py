@@ -14,6 +14,7 @@ LIB_PATH = os.path.join(HERE, "libmarsb200.so")
 HEADER = os.path.join(os.path.dirname(HERE), "include", "marsb200.h")
 
 MB2_OK, MB2_ERR_ARG, MB2_ERR_CUDA, MB2_ERR_CAPACITY, MB2_ERR_STATE = 0, 1, 2, 3, 4
+STAGE_STEP, STAGE_PAIRLIST, STAGE_PAIR_FORCE, STAGE_INTEGRATE = 0, 1, 2, 3
 
 
 class MB2Error(RuntimeError):
@@ -78,5 +79,9 @@ def load(path: str = LIB_PATH):
     L.mb2_philox.argtypes = [vp, u64, u32, u32, u32, u32, vp, vp, vp]
     L.mb2_step.argtypes = [vp, vp, vp, vp, vp, u32, u64, C.POINTER(StepParams), vp]
     L.mb2_set_lanes_per_row.argtypes = [vp, i]
+    L.mb2_set_profiling.argtypes = [vp, i]
+    L.mb2_profile_read.argtypes = [vp, i, C.POINTER(C.c_double), u32p]
+    L.mb2_launch_count.restype = u64
+    L.mb2_launch_count.argtypes = []
     _lib = L
     return L

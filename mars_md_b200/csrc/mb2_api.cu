@@ -10,6 +10,10 @@
 
 using namespace mb2;
 
+namespace mb2 {
+unsigned long long g_launches = 0;
+}
+
 struct mb2_context {
 	int device = 0;
 	uint32_t max_particles = 0;
@@ -59,9 +63,32 @@ struct mb2_context {
 	DevBuf<int4> fg_id;
 	std::vector<GridView> host_grids;
 	DevBuf<GridView> grids;
+
+	// Optional per-stage CUDA-event timing on the launching stream.
+	bool profiling = false;
+	std::vector<std::pair<cudaEvent_t, cudaEvent_t>> prof[MB2_NUM_STAGES];
 };
 
 namespace {
+
+// Brackets one stage with events when profiling is on.
+struct StageScope {
+	mb2_context* ctx;
+	int stage;
+	cudaStream_t st;
+	cudaEvent_t b = nullptr, e = nullptr;
+	StageScope(mb2_context* c, int s, cudaStream_t stream) : ctx(c), stage(s), st(stream) {
+		if (!ctx->profiling) return;
+		MB2_CUDA(cudaEventCreate(&b));
+		MB2_CUDA(cudaEventCreate(&e));
+		MB2_CUDA(cudaEventRecord(b, st));
+	}
+	~StageScope() {
+		if (!b) return;
+		cudaEventRecord(e, st);
+		ctx->prof[stage].emplace_back(b, e);
+	}
+};
 
 int fail(mb2_context* ctx, int code, const std::string& msg) {
 	if (ctx) ctx->last_error = msg;
@@ -143,8 +170,8 @@ void morton_domain(mb2_context* ctx, const float4* pos, uint32_t n, cudaStream_t
 	if (any_open) {
 		ctx->bbox.ensure(6);
 		int* dev = reinterpret_cast<int*>(ctx->bbox.ptr);
-		bbox_init_kernel<<<1, 32, 0, st>>>(dev);
-		if (n) bbox_kernel<<<(n + 255) / 256, 256, 0, st>>>(pos, n, dev);
+		MB2_LAUNCH bbox_init_kernel<<<1, 32, 0, st>>>(dev);
+		if (n) MB2_LAUNCH bbox_kernel<<<(n + 255) / 256, 256, 0, st>>>(pos, n, dev);
 		int h[6];
 		MB2_CUDA(cudaMemcpyAsync(h, dev, sizeof(h), cudaMemcpyDeviceToHost, st));
 		MB2_CUDA(cudaStreamSynchronize(st));
@@ -191,6 +218,7 @@ void build(mb2_context* ctx, const float4* pos, const int* type_ids, uint32_t n,
 			"mb2_build_pairlist: more particles than the context was created for");
 	require(rc_list > 0.0f && std::isfinite(rc_list), MB2_ERR_ARG,
 			"mb2_build_pairlist: pairlist cutoff must be positive and finite");
+	StageScope scope(ctx, MB2_STAGE_PAIRLIST, st);
 	float bmin[3], bmax[3], extent[3];
 	morton_domain(ctx, pos, n, st, bmin, bmax);
 	for (int a = 0; a < 3; ++a) extent[a] = bmax[a] - bmin[a];
@@ -260,8 +288,12 @@ void pair_forces_impl(mb2_context* ctx, const float4* pos, const int* type_ids, 
 	ctx->force_sorted.ensure(n);
 	MB2_CUDA(cudaMemsetAsync(ctx->force_sorted.ptr, 0, static_cast<size_t>(n) * sizeof(float4), st));
 	const float cutoff_sq = cutoff > 0.0f ? cutoff * cutoff : 0.0f;
-	pair_forces(ctx->sorted_pos.ptr, ctx->row_start.ptr, ctx->nbr.ptr, n, ctx->pt, ctx->box,
-				cutoff_sq, get_energy, ctx->force_sorted.ptr, ctx->energy.ptr, pick_lanes(ctx), st);
+	{
+		StageScope scope(ctx, MB2_STAGE_PAIR_FORCE, st);
+		pair_forces(ctx->sorted_pos.ptr, ctx->row_start.ptr, ctx->nbr.ptr, n, ctx->pt, ctx->box,
+					cutoff_sq, get_energy, ctx->force_sorted.ptr, ctx->energy.ptr, pick_lanes(ctx),
+					st);
+	}
 	scatter_add_forces(ctx->force_sorted.ptr, ctx->s2o.ptr, n, fe, get_energy, st);
 }
 
@@ -665,6 +697,7 @@ int mb2_step(mb2_context* ctx, float* pos4, float* force_energy4, const int* typ
 				"mb2_step: null argument");
 		require(ctx->types_set, MB2_ERR_STATE, "mb2_step: call mb2_set_particle_types");
 		const cudaStream_t st = S(stream);
+		StageScope whole(ctx, MB2_STAGE_STEP, st);
 		float4* pos = reinterpret_cast<float4*>(pos4);
 		float4* fe = reinterpret_cast<float4*>(force_energy4);
 		// DeviceParticle::clear_forces (Patch.cpp:56)
@@ -688,7 +721,33 @@ int mb2_step(mb2_context* ctx, float* pos4, float* force_energy4, const int* typ
 		BdParams p{prm->dt, prm->kT, static_cast<uint32_t>(step),
 				   mb2_bd_seed(prm->seed, prm->patch_id, step), 0u,
 				   {prm->efield[0], prm->efield[1], prm->efield[2]}};
+		StageScope scope(ctx, MB2_STAGE_INTEGRATE, st);
 		bd_integrate(pos, fe, type_ids, flags, n, ctx->types, ctx->box, p, st);
+	});
+}
+
+uint64_t mb2_launch_count(void) { return g_launches; }
+
+int mb2_set_profiling(mb2_context* ctx, int on) {
+	return guarded(ctx, [&] { ctx->profiling = on != 0; });
+}
+
+int mb2_profile_read(mb2_context* ctx, int stage, double* total_ms, uint32_t* count) {
+	return guarded(ctx, [&] {
+		require(stage >= 0 && stage < MB2_NUM_STAGES && total_ms && count, MB2_ERR_ARG,
+				"mb2_profile_read: bad stage or null output");
+		double t = 0.0;
+		for (auto& be : ctx->prof[stage]) {
+			MB2_CUDA(cudaEventSynchronize(be.second));
+			float ms = 0.0f;
+			MB2_CUDA(cudaEventElapsedTime(&ms, be.first, be.second));
+			t += ms;
+			cudaEventDestroy(be.first);
+			cudaEventDestroy(be.second);
+		}
+		*total_ms = t;
+		*count = static_cast<uint32_t>(ctx->prof[stage].size());
+		ctx->prof[stage].clear();
 	});
 }
 

@@ -239,7 +239,7 @@ __global__ void philox_kernel(uint64_t seed, uint32_t ctr0, uint32_t ctr1, uint3
 void bd_integrate(float4* pos, float4* fe, const int* type_ids, const uint32_t* flags, uint32_t n,
 				  const TypeTable& types, const Box& box, const BdParams& p, cudaStream_t st) {
 	if (n == 0) return;
-	bd_kernel<<<(n + 255) / 256, 256, 0, st>>>(pos, fe, type_ids, flags, n, types, box, p);
+	MB2_LAUNCH bd_kernel<<<(n + 255) / 256, 256, 0, st>>>(pos, fe, type_ids, flags, n, types, box, p);
 }
 
 void bd_integrate_sorted(float4* sorted_pos, float4* force_sorted, const uint32_t* s2o,
@@ -247,14 +247,14 @@ void bd_integrate_sorted(float4* sorted_pos, float4* force_sorted, const uint32_
 						 uint32_t n, const TypeTable& types, const Box& box, const BdParams& p,
 						 int write_fe, cudaStream_t st) {
 	if (n == 0) return;
-	bd_sorted_kernel<<<(n + 255) / 256, 256, 0, st>>>(sorted_pos, force_sorted, s2o, pos, fe,
+	MB2_LAUNCH bd_sorted_kernel<<<(n + 255) / 256, 256, 0, st>>>(sorted_pos, force_sorted, s2o, pos, fe,
 													  type_ids, flags, n, types, box, p, write_fe);
 }
 
 void philox_draws(uint64_t seed, uint32_t ctr0, uint32_t ctr1, uint32_t ctr2, uint32_t n,
 				  uint32_t* out4, float* normals4, cudaStream_t st) {
 	if (n == 0) return;
-	philox_kernel<<<(n + 255) / 256, 256, 0, st>>>(seed, ctr0, ctr1, ctr2, n,
+	MB2_LAUNCH philox_kernel<<<(n + 255) / 256, 256, 0, st>>>(seed, ctr0, ctr1, ctr2, n,
 												   reinterpret_cast<uint4*>(out4),
 												   reinterpret_cast<float4*>(normals4));
 }

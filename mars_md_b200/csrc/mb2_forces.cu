@@ -273,7 +273,7 @@ void launch_pair(const float4* sorted_pos, const uint32_t* row_start, const uint
 									  static_cast<int>(smem)));
 	const uint32_t groups = 256 / G;
 	const uint32_t blocks = (n + groups - 1) / groups;
-	kern<<<blocks, 256, smem, st>>>(sorted_pos, row_start, nbr, n, t.term_matrix, t.num_types,
+	MB2_LAUNCH kern<<<blocks, 256, smem, st>>>(sorted_pos, row_start, nbr, n, t.term_matrix, t.num_types,
 									t.tables, t.num_tables, t.values, t.total_values, box,
 									cutoff_sq, get_energy, force_sorted, ev);
 }
@@ -295,7 +295,7 @@ void pair_forces(const float4* sorted_pos, const uint32_t* row_start, const uint
 void scatter_add_forces(const float4* force_sorted, const uint32_t* s2o, uint32_t n,
 						float4* force_energy, int get_energy, cudaStream_t st) {
 	if (n == 0) return;
-	scatter_add_kernel<<<(n + 255) / 256, 256, 0, st>>>(force_sorted, s2o, n, force_energy,
+	MB2_LAUNCH scatter_add_kernel<<<(n + 255) / 256, 256, 0, st>>>(force_sorted, s2o, n, force_energy,
 														get_energy);
 }
 
@@ -303,7 +303,7 @@ void bond_forces(const int2* bonds, const int* table_idx, uint32_t nb, const flo
 				 float4* fe, const Table* tables, const Box& box, int get_energy, double* energy,
 				 cudaStream_t st) {
 	if (nb == 0) return;
-	bond_kernel<<<(nb + 255) / 256, 256, 0, st>>>(bonds, table_idx, nb, pos, fe, tables, box,
+	MB2_LAUNCH bond_kernel<<<(nb + 255) / 256, 256, 0, st>>>(bonds, table_idx, nb, pos, fe, tables, box,
 												  get_energy, energy);
 }
 
@@ -311,7 +311,7 @@ void angle_forces(const int4* angles, const int* table_idx, uint32_t na, const f
 				  float4* fe, const Table* tables, const Box& box, int get_energy, double* energy,
 				  cudaStream_t st) {
 	if (na == 0) return;
-	angle_kernel<<<(na + 255) / 256, 256, 0, st>>>(angles, table_idx, na, pos, fe, tables, box,
+	MB2_LAUNCH angle_kernel<<<(na + 255) / 256, 256, 0, st>>>(angles, table_idx, na, pos, fe, tables, box,
 												   get_energy, energy);
 }
 

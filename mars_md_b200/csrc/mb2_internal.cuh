@@ -11,6 +11,10 @@
 
 namespace mb2 {
 
+// Count of kernels this library has launched (for launch accounting).
+extern unsigned long long g_launches;
+#define MB2_LAUNCH ++::mb2::g_launches,
+
 // Thrown inside the library, turned into a status code at the C boundary.
 struct Error {
 	int code;

@@ -229,7 +229,7 @@ void cell_ranges(const uint32_t* keys, uint32_t n, int shift, uint32_t* begin, u
 	MB2_CUDA(cudaMemsetAsync(begin, 0, num_cells * sizeof(uint32_t), st));
 	MB2_CUDA(cudaMemsetAsync(end, 0, num_cells * sizeof(uint32_t), st));
 	if (n == 0) return;
-	cell_ranges_kernel<<<(n + 255) / 256, 256, 0, st>>>(keys, n, shift, begin, end);
+	MB2_LAUNCH cell_ranges_kernel<<<(n + 255) / 256, 256, 0, st>>>(keys, n, shift, begin, end);
 }
 
 template <bool kFill>
@@ -245,7 +245,7 @@ static void launch_walk(const float4* sorted_pos, const uint32_t* keys, const ui
 	if (smem > 48 * 1024)
 		MB2_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
 									  static_cast<int>(smem)));
-	kern<<<(n + 255) / 256, 256, smem, st>>>(sorted_pos, keys, s2o, begin, end, stencil, ns, m,
+	MB2_LAUNCH kern<<<(n + 255) / 256, 256, smem, st>>>(sorted_pos, keys, s2o, begin, end, stencil, ns, m,
 											 shift, rc2, n, box, ex, counts, row_start, nbr);
 }
 
@@ -269,7 +269,7 @@ void neighbor_fill(const float4* sorted_pos, const uint32_t* keys, const uint32_
 void export_pairs(const uint32_t* row_start, const uint32_t* nbr, const uint32_t* s2o,
 				  uint32_t n, int2* out, cudaStream_t st) {
 	if (n == 0) return;
-	export_kernel<<<(n + 255) / 256, 256, 0, st>>>(row_start, nbr, s2o, n, out);
+	MB2_LAUNCH export_kernel<<<(n + 255) / 256, 256, 0, st>>>(row_start, nbr, s2o, n, out);
 }
 
 void max_displacement_sq(const float4* cur, const float4* prev, uint32_t n, const Box& box,
@@ -279,13 +279,13 @@ void max_displacement_sq(const float4* cur, const float4* prev, uint32_t n, cons
 	const float3 len = make_float3(box.periodic[0] ? box.size[0] : 0.0f,
 								   box.periodic[1] ? box.size[1] : 0.0f,
 								   box.periodic[2] ? box.size[2] : 0.0f);
-	displacement_kernel<<<(n + 255) / 256, 256, 0, st>>>(cur, prev, n, len, out_bits);
+	MB2_LAUNCH displacement_kernel<<<(n + 255) / 256, 256, 0, st>>>(cur, prev, n, len, out_bits);
 }
 
 void pack_sorted_positions(const float4* pos, const int* type_ids, const uint32_t* s2o,
 						   uint32_t n, float4* sorted_pos, cudaStream_t st) {
 	if (n == 0) return;
-	pack_kernel<<<(n + 255) / 256, 256, 0, st>>>(pos, type_ids, s2o, n, sorted_pos);
+	MB2_LAUNCH pack_kernel<<<(n + 255) / 256, 256, 0, st>>>(pos, type_ids, s2o, n, sorted_pos);
 }
 
 }  // namespace mb2

@@ -100,9 +100,9 @@ void exclusive_scan_u32(Scratch& s, const uint32_t* in, uint32_t* out, size_t n,
 	}
 	const size_t blocks = (n + kScanBlock - 1) / kScanBlock;
 	s.scan_blocks.ensure(blocks);
-	scan_reduce_kernel<<<blocks, kScanThreads, 0, st>>>(in, n, s.scan_blocks.ptr);
-	scan_sums_kernel<<<1, kScanThreads, 0, st>>>(s.scan_blocks.ptr, blocks, total);
-	scan_apply_kernel<<<blocks, kScanThreads, 0, st>>>(in, n, s.scan_blocks.ptr, out);
+	MB2_LAUNCH scan_reduce_kernel<<<blocks, kScanThreads, 0, st>>>(in, n, s.scan_blocks.ptr);
+	MB2_LAUNCH scan_sums_kernel<<<1, kScanThreads, 0, st>>>(s.scan_blocks.ptr, blocks, total);
+	MB2_LAUNCH scan_apply_kernel<<<blocks, kScanThreads, 0, st>>>(in, n, s.scan_blocks.ptr, out);
 }
 
 }  // namespace mb2

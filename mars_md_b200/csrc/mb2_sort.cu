@@ -123,9 +123,9 @@ void radix_sort_pairs(Scratch& s, uint32_t* keys, uint32_t* vals, uint32_t n, cu
 	uint32_t *ks = keys, *vs = vals, *kd = s.sort_keys_alt, *vd = s.sort_vals_alt;
 	for (int pass = 0; pass < 4; ++pass) {
 		const int shift = 8 * pass;
-		radix_hist_kernel<<<tiles, kThreads, 0, st>>>(ks, n, shift, tiles, s.sort_hist);
+		MB2_LAUNCH radix_hist_kernel<<<tiles, kThreads, 0, st>>>(ks, n, shift, tiles, s.sort_hist);
 		exclusive_scan_u32(s, s.sort_hist, s.sort_hist, tiles * 256u, nullptr, st);
-		radix_scatter_kernel<<<tiles, kThreads, 0, st>>>(ks, vs, n, shift, tiles, s.sort_hist, kd,
+		MB2_LAUNCH radix_scatter_kernel<<<tiles, kThreads, 0, st>>>(ks, vs, n, shift, tiles, s.sort_hist, kd,
 														 vd);
 		uint32_t* t = ks;
 		ks = kd;
@@ -144,13 +144,13 @@ void morton_encode(const float4* pos, uint32_t n, const float* bmin, const float
 	float3 range = make_float3(fmaxf(bmax[0] - bmin[0], 1e-6f), fmaxf(bmax[1] - bmin[1], 1e-6f),
 							   fmaxf(bmax[2] - bmin[2], 1e-6f));
 	if (n == 0) return;
-	morton_encode_kernel<<<(n + 255) / 256, 256, 0, st>>>(pos, n, lo, range, keys, idx);
+	MB2_LAUNCH morton_encode_kernel<<<(n + 255) / 256, 256, 0, st>>>(pos, n, lo, range, keys, idx);
 }
 
 void inverse_and_gather(const uint32_t* s2o, uint32_t n, const float4* pos, uint32_t* inv,
 						float4* sorted_pos, cudaStream_t st) {
 	if (n == 0) return;
-	inverse_gather_kernel<<<(n + 255) / 256, 256, 0, st>>>(s2o, n, pos, inv, sorted_pos);
+	MB2_LAUNCH inverse_gather_kernel<<<(n + 255) / 256, 256, 0, st>>>(s2o, n, pos, inv, sorted_pos);
 }
 
 }  // namespace mb2

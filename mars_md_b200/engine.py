@@ -138,6 +138,16 @@ class Context:
         self.check(self.lib.mb2_set_grid(self.h, int(grid_id), _p(data), dims, _f3(origin),
                                          colmajor, int(boundary_condition)))
 
+    def set_profiling(self, on: bool):
+        self.check(self.lib.mb2_set_profiling(self.h, int(on)))
+
+    def profile_read(self, stage: int):
+        """(total ms, launches) of one stage since the last read."""
+        ms = C.c_double()
+        cnt = C.c_uint32()
+        self.check(self.lib.mb2_profile_read(self.h, int(stage), C.byref(ms), C.byref(cnt)))
+        return float(ms.value), int(cnt.value)
+
     def set_lanes_per_row(self, lanes: int):
         self.check(self.lib.mb2_set_lanes_per_row(self.h, int(lanes)))
 

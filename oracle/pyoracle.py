@@ -441,6 +441,9 @@ class RefHarness:
         L.ref_neighbor_walk.restype = u32
         L.ref_neighbor_walk.argtypes = [vp, vp, vp, vp, vp, vp, vp, sz, f, sz, i, i, i, vp, vp, vp,
                                         vp, vp, sz, vp]
+        L.ref_neighbor_walk_items.restype = u64
+        L.ref_neighbor_walk_items.argtypes = [vp, vp, vp, vp, vp, vp, f, sz, i, i, vp, vp, vp,
+                                              vp, sz, vp, sz]
         L.ref_resolve_tags.argtypes = [vp, sz, vp, vp, sz, vp, i]
         L.ref_pair_forces.argtypes = [vp, sz, vp, vp, vp, vp, vp, vp, vp, vp, vp, i, vp, vp, vp,
                                       i, f, u32]
@@ -514,10 +517,23 @@ class RefHarness:
                                          _ptr(rigid_body_id))
         return buf[1: cnt + 1], int(cnt)
 
-    def resolve_tags(self, pairs, type_ids, term_matrix, num_types):
+    def neighbor_walk_items(self, sorted_pos, keys, s2o, begin, end, table, cutoff_sq, npc,
+                            shift, box: Box, items, max_pairs=0):
+        """Run the walk for the listed particles only. Returns (pairs or None, count)."""
+        o, s, p = self._box(box)
+        items = np.ascontiguousarray(items, np.uint32)
+        buf = np.zeros((max_pairs + 1, 2), np.int32) if max_pairs else None
+        cnt = int(self.lib.ref_neighbor_walk_items(
+            _ptr(sorted_pos), _ptr(keys), _ptr(s2o), _ptr(begin), _ptr(end), _ptr(table),
+            C.c_float(cutoff_sq), len(keys), npc, shift, _ptr(o), _ptr(s), _ptr(p), _ptr(items),
+            len(items), _ptr(buf), max_pairs))
+        pairs = None if buf is None else np.ascontiguousarray(buf[1: min(cnt, max_pairs) + 1])
+        return pairs, cnt
+
+    def resolve_tags(self, pairs, type_ids, term_matrix, num_types, nthreads=1):
         tags = np.zeros(len(pairs), np.uint32)
         self.lib.ref_resolve_tags(_ptr(pairs), len(pairs), _ptr(type_ids), _ptr(term_matrix),
-                                  num_types, _ptr(tags), 1)
+                                  num_types, _ptr(tags), nthreads)
         return tags
 
     def pair_forces(self, pairs, pos4, type_ids, tags, tables: TableSet, box: Box, cutoff_sq,

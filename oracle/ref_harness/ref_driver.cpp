@@ -173,6 +173,41 @@ uint32_t ref_neighbor_walk(const float* sorted_pos4, const uint32_t* keys, const
 	return count;
 }
 
+// The same functor run only for the listed work items (particle i with one
+// thread per particle), to time a bounded sample of a large walk. Pairs are
+// stored in slots [1, max_pairs] when `pairs` is given (the host ATOMIC_ADD
+// returns the incremented count). Returns the number of pairs emitted.
+uint64_t ref_neighbor_walk_items(const float* sorted_pos4, const uint32_t* keys,
+								 const uint32_t* s2o, const uint32_t* cell_begin,
+								 const uint32_t* cell_end, const uint32_t* table, float cutoff_sq,
+								 size_t n, int npc, int shift, const float* origin,
+								 const float* size, const int* periodic, const uint32_t* items,
+								 size_t n_items, int* pairs, size_t max_pairs) {
+	uint32_t count = 0;
+	int2 sink[2];
+	int2* out = pairs ? reinterpret_cast<int2*>(pairs) : sink;
+	ExclusionView ex;
+	ZOrderCellNeighborKernel k{reinterpret_cast<const Vector3*>(sorted_pos4),
+							   keys,
+							   s2o,
+							   cell_begin,
+							   cell_end,
+							   table,
+							   out,
+							   &count,
+							   cutoff_sq,
+							   n,
+							   pairs ? max_pairs + 1 : 0,
+							   npc,
+							   1,
+							   shift,
+							   make_box(origin, size, periodic),
+							   ex};
+	for (size_t t = 0; t < n_items; ++t)
+		k(items[t]);
+	return count;
+}
+
 // ResolvePairTableKernel (Pairwise.h:104-120).
 void ref_resolve_tags(const int* pairs, size_t n_pairs, const int* type_ids,
 					  const uint32_t* term_matrix, size_t num_types, uint32_t* tags, int nthreads) {
