@@ -139,6 +139,8 @@ def run_ours(args):
     w = W.large_plain(seed=W.DEFAULT_SEED + rank)
     ctx = Context(w.n, device=local)
     dev = setup_workload(ctx, w, device=f"cuda:{local}")
+    if args.lanes:
+        ctx.set_lanes_per_row(args.lanes)
     prm = step_params(w)
     stream = torch.cuda.current_stream()
 
@@ -305,6 +307,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--lanes", type=int, default=0,
+                    help="lanes per pairlist row in the pair kernel (0 = automatic)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

@@ -24,13 +24,14 @@ struct mb2_context {
 	Scratch scratch;
 
 	// Z-order state of the last build
-	DevBuf<uint32_t> keys, s2o, inv, counts, row_start, nbr, cell_begin, cell_end;
+	DevBuf<uint32_t> keys, s2o, inv, row_len, row_off, nbr, cell_begin, cell_end;
 	DevBuf<float4> sorted_pos, ref_pos, force_sorted;
 	DevBuf<StencilEntry> stencil;
 	DevBuf<float> bbox;  // 6 floats, ordered-int min/max
 	DevBuf<unsigned int> disp;
+	DevBuf<unsigned long long> stats;  // build: pairs, longest row
 	DevBuf<double> energy;  // pair E, pair virial, bond E, angle E
-	uint32_t* pinned_u32 = nullptr;
+	uint64_t* pinned = nullptr;
 	CellGrid grid;
 	bool grid_valid = false;
 	float grid_extent[3] = {0, 0, 0};
@@ -39,14 +40,17 @@ struct mb2_context {
 	bool built = false;
 	uint32_t built_n = 0;
 	uint64_t num_pairs = 0;
+	uint32_t cap = 0;        // entries per row of the sliced-ELL list
+	int lanes = 0;           // G: lanes per row in the pair kernel (slice height 32 / G)
+	uint64_t max_row = 0;
 	Exclusions excl;
-	int lanes_per_row = 0;
+	int lanes_request = 0;   // 0 = choose from the mean row length
 
 	// pair tables
 	PairTables pt;
-	DevBuf<uint32_t> term;
-	DevBuf<Table> tables;
-	DevBuf<float> values;
+	DevBuf<PairTableRef> refs;
+	DevBuf<float> bin_force;
+	DevBuf<float2> bin_energy;
 
 	// bonded tables
 	DevBuf<Table> bonded_tables[2];
@@ -243,57 +247,95 @@ void build(mb2_context* ctx, const float4* pos, const int* type_ids, uint32_t n,
 	ctx->cell_end.ensure(num_cells);
 	cell_ranges(ctx->keys.ptr, n, g.shift, ctx->cell_begin.ptr, ctx->cell_end.ptr, num_cells, st);
 
-	ctx->counts.ensure(n);
-	ctx->row_start.ensure(static_cast<size_t>(n) + 1);
-	neighbor_count(ctx->sorted_pos.ptr, ctx->keys.ptr, ctx->s2o.ptr, ctx->cell_begin.ptr,
-				   ctx->cell_end.ptr, ctx->stencil.ptr, g.num_stencil, g.m, g.shift, rc2, n,
-				   ctx->box, ctx->excl, ctx->counts.ptr, st);
-	exclusive_scan_u32(ctx->scratch, ctx->counts.ptr, ctx->row_start.ptr, n,
-					   ctx->row_start.ptr + n, st);
-	MB2_CUDA(cudaMemcpyAsync(ctx->pinned_u32, ctx->row_start.ptr + n, sizeof(uint32_t),
-							 cudaMemcpyDeviceToHost, st));
-	MB2_CUDA(cudaStreamSynchronize(st));
-	const uint32_t total = *ctx->pinned_u32;
-	ctx->nbr.ensure(std::max<size_t>(total, 1));
-	neighbor_fill(ctx->sorted_pos.ptr, ctx->keys.ptr, ctx->s2o.ptr, ctx->cell_begin.ptr,
-				  ctx->cell_end.ptr, ctx->stencil.ptr, g.num_stencil, g.m, g.shift, rc2, n,
-				  ctx->box, ctx->excl, ctx->row_start.ptr, ctx->nbr.ptr, st);
+	WalkGrid wg{};
+	wg.m = g.m;
+	wg.shift = g.shift;
+	wg.emax = 3;
+	for (int a = 0; a < 3; ++a) {
+		wg.radius[a] = g.radius[a];
+		wg.wmin[a] = g.wmin[a];
+		wg.full[a] = ctx->box.periodic[a] && g.m > 0 && (2 * g.radius[a] + 1 >= (1 << g.m));
+		if (g.m == 0) wg.full[a] = ctx->box.periodic[a];
+	}
+	wg.lim = g.lim;
+	wg.rc2 = rc2;
+	fast_test_band(ctx->box, rc_list, &wg.fast_lo, &wg.fast_hi);
+	ctx->row_len.ensure(n);
+	ctx->stats.ensure(2);
+	auto walk = [&](uint32_t cap) {
+		const int hshift = __builtin_ctz(32 / ctx->lanes);
+		build_walk(ctx->sorted_pos.ptr, ctx->keys.ptr, ctx->s2o.ptr, ctx->cell_begin.ptr,
+				   ctx->cell_end.ptr, ctx->stencil.ptr, g.num_stencil, wg, n, ctx->box, ctx->excl,
+				   ctx->nbr.ptr, cap, hshift, ctx->row_len.ptr, ctx->stats.ptr, st);
+		MB2_CUDA(cudaMemcpyAsync(ctx->pinned, ctx->stats.ptr, 2 * sizeof(uint64_t),
+								 cudaMemcpyDeviceToHost, st));
+		MB2_CUDA(cudaStreamSynchronize(st));
+		return std::make_pair(ctx->pinned[0], ctx->pinned[1]);
+	};
+	auto choose_lanes = [&](double mean) {
+		if (ctx->lanes_request) return ctx->lanes_request;
+		if (mean >= 256.0) return 16;
+		if (mean >= 48.0) return 8;
+		return 4;
+	};
+	auto size_list = [&](uint64_t max_row) {
+		const uint32_t G = static_cast<uint32_t>(ctx->lanes);
+		uint64_t cap = max_row + max_row / 4 + G;
+		cap = (cap + G - 1) / G * G;
+		require(cap < 65536u, MB2_ERR_CAPACITY,
+				"mb2_build_pairlist: a particle has more than ~52000 list neighbours");
+		ctx->cap = static_cast<uint32_t>(cap);
+		const size_t slices = (static_cast<size_t>(n) + (32 / G) - 1) / (32 / G);
+		ctx->nbr.ensure(std::max<size_t>(slices * cap * (32 / G), 1));
+	};
+	if (ctx->cap == 0 || ctx->lanes == 0) {
+		// First build: count rows without storing, to size the list.
+		ctx->lanes = 4;
+		const auto counted = walk(0u);
+		ctx->lanes = choose_lanes(n ? static_cast<double>(counted.first) / n : 0.0);
+		size_list(counted.second);
+	}
+	{
+		const size_t h = static_cast<size_t>(32 / ctx->lanes);
+		ctx->nbr.ensure(std::max<size_t>((n + h - 1) / h * ctx->cap * h, 1));
+	}
+	auto stats = walk(ctx->cap);
+	if (stats.second > ctx->cap) {
+		// Longer rows than the list was sized for: grow and walk again.
+		size_list(stats.second);
+		stats = walk(ctx->cap);
+	}
 	// Snapshot for the skin check (ZOrderPairlist.cpp:172-173).
 	ctx->ref_pos.ensure(n);
 	MB2_CUDA(cudaMemcpyAsync(ctx->ref_pos.ptr, pos, static_cast<size_t>(n) * sizeof(float4),
 							 cudaMemcpyDeviceToDevice, st));
-	ctx->num_pairs = total;
+	ctx->num_pairs = stats.first;
+	ctx->max_row = stats.second;
 	ctx->built = true;
 	ctx->built_n = n;
 }
 
-int pick_lanes(const mb2_context* ctx) {
-	if (ctx->lanes_per_row) return ctx->lanes_per_row;
-	const double mean = ctx->built_n ? static_cast<double>(ctx->num_pairs) / ctx->built_n : 0.0;
-	if (mean >= 48.0) return 32;
-	if (mean >= 20.0) return 16;
-	if (mean >= 8.0) return 8;
-	return 4;
-}
-
-void pair_forces_impl(mb2_context* ctx, const float4* pos, const int* type_ids, float4* fe,
-					  uint32_t n, float cutoff, int get_energy, cudaStream_t st) {
+// Pair kernel over the sorted positions into the zeroed sorted accumulator.
+void pair_kernel(mb2_context* ctx, uint32_t n, float cutoff, int get_energy, cudaStream_t st) {
 	require(ctx->built, MB2_ERR_STATE, "mb2_pair_forces: no pairlist; call mb2_build_pairlist");
 	require(n == ctx->built_n, MB2_ERR_ARG,
 			"mb2_pair_forces: particle count differs from the last pairlist build");
 	require(ctx->pt.num_types > 0, MB2_ERR_STATE,
 			"mb2_pair_forces: no pair tables; call mb2_set_pair_tables");
-	if (n == 0) return;
-	pack_sorted_positions(pos, type_ids, ctx->s2o.ptr, n, ctx->sorted_pos.ptr, st);
 	ctx->force_sorted.ensure(n);
 	MB2_CUDA(cudaMemsetAsync(ctx->force_sorted.ptr, 0, static_cast<size_t>(n) * sizeof(float4), st));
 	const float cutoff_sq = cutoff > 0.0f ? cutoff * cutoff : 0.0f;
-	{
-		StageScope scope(ctx, MB2_STAGE_PAIR_FORCE, st);
-		pair_forces(ctx->sorted_pos.ptr, ctx->row_start.ptr, ctx->nbr.ptr, n, ctx->pt, ctx->box,
-					cutoff_sq, get_energy, ctx->force_sorted.ptr, ctx->energy.ptr, pick_lanes(ctx),
-					st);
-	}
+	StageScope scope(ctx, MB2_STAGE_PAIR_FORCE, st);
+	pair_forces(ctx->sorted_pos.ptr, ctx->nbr.ptr, ctx->row_len.ptr, n, ctx->cap, ctx->lanes, ctx->pt,
+				ctx->box, cutoff_sq, get_energy, ctx->force_sorted.ptr, ctx->energy.ptr, st);
+}
+
+void pair_forces_impl(mb2_context* ctx, const float4* pos, const int* type_ids, float4* fe,
+					  uint32_t n, float cutoff, int get_energy, cudaStream_t st) {
+	require(ctx->built, MB2_ERR_STATE, "mb2_pair_forces: no pairlist; call mb2_build_pairlist");
+	if (n == 0) return;
+	pack_sorted_positions(pos, type_ids, ctx->s2o.ptr, n, ctx->sorted_pos.ptr, st);
+	pair_kernel(ctx, n, cutoff, get_energy, st);
 	scatter_add_forces(ctx->force_sorted.ptr, ctx->s2o.ptr, n, fe, get_energy, st);
 }
 
@@ -302,11 +344,11 @@ float max_disp(mb2_context* ctx, const float4* pos, uint32_t n, cudaStream_t st)
 			"mb2_needs_update: no pairlist for this particle count");
 	ctx->disp.ensure(1);
 	max_displacement_sq(pos, ctx->ref_pos.ptr, n, ctx->box, ctx->disp.ptr, st);
-	MB2_CUDA(cudaMemcpyAsync(ctx->pinned_u32, ctx->disp.ptr, sizeof(uint32_t),
+	MB2_CUDA(cudaMemcpyAsync(ctx->pinned, ctx->disp.ptr, sizeof(uint32_t),
 							 cudaMemcpyDeviceToHost, st));
 	MB2_CUDA(cudaStreamSynchronize(st));
 	float d2;
-	std::memcpy(&d2, ctx->pinned_u32, 4);
+	std::memcpy(&d2, ctx->pinned, 4);
 	return sqrtf(d2);
 }
 
@@ -345,7 +387,7 @@ int mb2_create(int device, uint32_t max_particles, mb2_context** out) {
 	ctx->device = device;
 	ctx->max_particles = max_particles;
 	const int rc = guarded(ctx, [&] {
-		MB2_CUDA(cudaMallocHost(&ctx->pinned_u32, 64));
+		MB2_CUDA(cudaMallocHost(&ctx->pinned, 64));
 		ctx->energy.ensure(4);
 		MB2_CUDA(cudaMemset(ctx->energy.ptr, 0, 4 * sizeof(double)));
 	});
@@ -361,31 +403,13 @@ int mb2_destroy(mb2_context* ctx) {
 	if (!ctx) return MB2_ERR_ARG;
 	cudaSetDevice(ctx->device);
 	cudaDeviceSynchronize();
-	for (auto* b : {&ctx->keys, &ctx->s2o, &ctx->inv, &ctx->counts, &ctx->row_start, &ctx->nbr,
-					&ctx->cell_begin, &ctx->cell_end, &ctx->term})
-		b->release();
-	for (auto* b : {&ctx->sorted_pos, &ctx->ref_pos, &ctx->force_sorted, &ctx->diffusion,
-					&ctx->fg_scale})
-		b->release();
-	ctx->stencil.release();
-	ctx->bbox.release();
-	ctx->disp.release();
-	ctx->energy.release();
-	ctx->tables.release();
-	ctx->values.release();
-	for (int k = 0; k < 2; ++k) {
-		ctx->bonded_tables[k].release();
-		ctx->bonded_values[k].release();
-	}
-	ctx->charge.release();
-	ctx->pmf_off.release();
-	ctx->pmf_cnt.release();
-	ctx->terms.release();
-	ctx->fg_id.release();
-	ctx->grids.release();
-	ctx->scratch.release();
-	if (ctx->pinned_u32) cudaFreeHost(ctx->pinned_u32);
-	delete ctx;
+	for (auto& stage : ctx->prof)
+		for (auto& be : stage) {
+			cudaEventDestroy(be.first);
+			cudaEventDestroy(be.second);
+		}
+	if (ctx->pinned) cudaFreeHost(ctx->pinned);
+	delete ctx;  // device buffers free themselves
 	return MB2_OK;
 }
 
@@ -475,8 +499,11 @@ int mb2_export_pairs(mb2_context* ctx, int* pairs2, uint64_t capacity, void* str
 		require(capacity >= ctx->num_pairs, MB2_ERR_CAPACITY,
 				"mb2_export_pairs: output smaller than the pair count");
 		require(ctx->num_pairs == 0 || pairs2, MB2_ERR_ARG, "mb2_export_pairs: null output");
-		export_pairs(ctx->row_start.ptr, ctx->nbr.ptr, ctx->s2o.ptr, ctx->built_n,
-					 reinterpret_cast<int2*>(pairs2), S(stream));
+		const uint32_t n = ctx->built_n;
+		ctx->row_off.ensure(n);
+		exclusive_scan_u32(ctx->scratch, ctx->row_len.ptr, ctx->row_off.ptr, n, nullptr, S(stream));
+		export_pairs(ctx->nbr.ptr, ctx->row_len.ptr, ctx->row_off.ptr, ctx->s2o.ptr, n, ctx->cap,
+					 __builtin_ctz(32 / ctx->lanes), reinterpret_cast<int2*>(pairs2), S(stream));
 	});
 }
 
@@ -501,22 +528,59 @@ int mb2_set_pair_tables(mb2_context* ctx, int num_types, const uint32_t* term_ma
 			require(!(tag & kTermTabulated) || static_cast<int>(tag >> kTableShift) < num_tables,
 					MB2_ERR_ARG, "mb2_set_pair_tables: tag names a missing table");
 		}
-		uint32_t total = 0;
-		upload_tables(ctx->tables, ctx->values, num_tables, values, sizes, starts, step_invs, 0,
-					  &total);
-		const size_t smem = static_cast<size_t>((num_types * num_types + 3) & ~3) * 4 +
-							static_cast<size_t>(num_tables) * 16 + static_cast<size_t>(total) * 4;
+		// Per-bin force and energy, rounded exactly as TabulatedPotential::compute
+		// rounds them (TabulatedPotential.h:41-51): dU = U[k+1] - U[k] and
+		// F = -dU * step_inv in float; the last bin is the home >= size-1 case.
+		std::vector<uint32_t> offset(num_tables);
+		size_t total = 0;
+		for (int k = 0; k < num_tables; ++k) {
+			require(sizes[k] >= 2, MB2_ERR_ARG, "mb2_set_pair_tables: a table needs 2 values");
+			offset[k] = static_cast<uint32_t>(total);
+			total += sizes[k];
+		}
+		std::vector<float> bf(std::max<size_t>(total, 1));
+		std::vector<float2> be(std::max<size_t>(total, 1));
+		for (int k = 0; k < num_tables; ++k) {
+			const float* u = values + offset[k];
+			const uint32_t sz = sizes[k];
+			for (uint32_t b = 0; b + 1 < sz; ++b) {
+				volatile float du = u[b + 1] - u[b];
+				volatile float f = -du * step_invs[k];
+				bf[offset[k] + b] = f;
+				be[offset[k] + b] = make_float2(u[b], du);
+			}
+			bf[offset[k] + sz - 1] = 0.0f;
+			be[offset[k] + sz - 1] = make_float2(u[sz - 1], 0.0f);
+		}
+		const int tt = num_types * num_types;
+		std::vector<PairTableRef> refs(tt);
+		for (int k = 0; k < tt; ++k) {
+			const uint32_t tag = term_matrix[k];
+			if (tag & kTermTabulated) {
+				const int t = static_cast<int>(tag >> kTableShift);
+				refs[k] = PairTableRef{starts[t], step_invs[t], static_cast<int>(sizes[t]) - 1,
+									   static_cast<int>(offset[t])};
+			} else {
+				refs[k] = PairTableRef{0.0f, 0.0f, 0, -1};
+			}
+		}
+		const size_t smem = static_cast<size_t>(tt) * sizeof(PairTableRef) + total * 12 + 8;
 		require(smem <= 200 * 1024, MB2_ERR_CAPACITY,
 				"mb2_set_pair_tables: tables exceed the 200 KB shared-memory budget");
-		ctx->term.ensure(static_cast<size_t>(num_types) * num_types);
-		MB2_CUDA(cudaMemcpy(ctx->term.ptr, term_matrix, sizeof(uint32_t) * num_types * num_types,
+		ctx->refs.ensure(tt);
+		ctx->bin_force.ensure(bf.size());
+		ctx->bin_energy.ensure(be.size());
+		MB2_CUDA(cudaMemcpy(ctx->refs.ptr, refs.data(), tt * sizeof(PairTableRef),
+							cudaMemcpyHostToDevice));
+		MB2_CUDA(cudaMemcpy(ctx->bin_force.ptr, bf.data(), bf.size() * sizeof(float),
+							cudaMemcpyHostToDevice));
+		MB2_CUDA(cudaMemcpy(ctx->bin_energy.ptr, be.data(), be.size() * sizeof(float2),
 							cudaMemcpyHostToDevice));
 		ctx->pt.num_types = num_types;
-		ctx->pt.num_tables = num_tables;
-		ctx->pt.term_matrix = ctx->term.ptr;
-		ctx->pt.tables = ctx->tables.ptr;
-		ctx->pt.values = ctx->values.ptr;
-		ctx->pt.total_values = total;
+		ctx->pt.total_bins = static_cast<uint32_t>(total);
+		ctx->pt.refs = ctx->refs.ptr;
+		ctx->pt.bin_force = ctx->bin_force.ptr;
+		ctx->pt.bin_energy = ctx->bin_energy.ptr;
 	});
 }
 
@@ -700,16 +764,25 @@ int mb2_step(mb2_context* ctx, float* pos4, float* force_energy4, const int* typ
 		StageScope whole(ctx, MB2_STAGE_STEP, st);
 		float4* pos = reinterpret_cast<float4*>(pos4);
 		float4* fe = reinterpret_cast<float4*>(force_energy4);
-		// DeviceParticle::clear_forces (Patch.cpp:56)
-		MB2_CUDA(cudaMemsetAsync(fe, 0, static_cast<size_t>(n) * sizeof(float4), st));
+		// The reference clears ForceEnergy (Patch.cpp:56) and accumulates every
+		// term into it. Here pair forces stay in the Z-ordered accumulator and
+		// the integrate kernel gathers them, adding what the bonded kernels
+		// wrote; ForceEnergy is cleared only when those run.
+		const bool bonded = prm->num_bonds != 0 || prm->num_angles != 0;
+		if (bonded)
+			MB2_CUDA(cudaMemsetAsync(fe, 0, static_cast<size_t>(n) * sizeof(float4), st));
 		// Rebuild schedule and skin check (Patch.cpp:86-108)
 		const bool at_period = prm->rebuild_period == 0 || (step - 1) % prm->rebuild_period == 0;
 		bool rebuild = at_period || !ctx->built || ctx->built_n != n;
 		const float skin = prm->pairlist_cutoff - prm->cutoff;
 		if (rebuild && prm->rebuild_period != 0 && ctx->built && ctx->built_n == n && skin > 0.0f)
 			rebuild = max_disp(ctx, pos, n, st) > skin * 0.5f;
-		if (rebuild) build(ctx, pos, type_ids, n, prm->pairlist_cutoff, st);
-		pair_forces_impl(ctx, pos, type_ids, fe, n, prm->cutoff, prm->get_energy, st);
+		if (rebuild)
+			build(ctx, pos, type_ids, n, prm->pairlist_cutoff, st);  // packs sorted_pos
+		else if (n)
+			pack_sorted_positions(pos, type_ids, ctx->s2o.ptr, n, ctx->sorted_pos.ptr, st);
+		if (n == 0) return;
+		pair_kernel(ctx, n, prm->cutoff, prm->get_energy, st);
 		if (prm->num_bonds)
 			bond_forces(reinterpret_cast<const int2*>(prm->bonds2), prm->bond_table_idx,
 						prm->num_bonds, pos, fe, ctx->bonded_tables[0].ptr, ctx->box,
@@ -722,7 +795,8 @@ int mb2_step(mb2_context* ctx, float* pos4, float* force_energy4, const int* typ
 				   mb2_bd_seed(prm->seed, prm->patch_id, step), 0u,
 				   {prm->efield[0], prm->efield[1], prm->efield[2]}};
 		StageScope scope(ctx, MB2_STAGE_INTEGRATE, st);
-		bd_integrate(pos, fe, type_ids, flags, n, ctx->types, ctx->box, p, st);
+		bd_integrate_gather(pos, fe, ctx->force_sorted.ptr, ctx->inv.ptr, type_ids, flags, n,
+							ctx->types, ctx->box, p, bonded ? 1 : 0, st);
 	});
 }
 
@@ -755,7 +829,13 @@ int mb2_set_lanes_per_row(mb2_context* ctx, int lanes) {
 	return guarded(ctx, [&] {
 		require(lanes == 0 || lanes == 4 || lanes == 8 || lanes == 16 || lanes == 32, MB2_ERR_ARG,
 				"mb2_set_lanes_per_row: 0, 4, 8, 16 or 32");
-		ctx->lanes_per_row = lanes;
+		if (lanes != ctx->lanes_request) {
+			// The list layout depends on the lanes per row: re-size at the next build.
+			ctx->lanes_request = lanes;
+			ctx->cap = 0;
+			ctx->lanes = 0;
+			ctx->built = false;
+		}
 	});
 }
 

@@ -183,44 +183,38 @@ __global__ void __launch_bounds__(256) bd_kernel(float4* __restrict__ pos, float
 	pos[i] = bd_update(p, f.x, f.y, f.z, ty.diffusion[type], xi, box, bp);
 }
 
-// Sorted-order variant used by the fused step: force from the sorted
-// accumulator (zeroed here for the next step) plus the caller's array, noise
-// keyed on the original slot, positions written to both orders.
-__global__ void __launch_bounds__(256) bd_sorted_kernel(
-	float4* __restrict__ sorted_pos, float4* __restrict__ fs, const uint32_t* __restrict__ s2o,
-	float4* __restrict__ pos, float4* __restrict__ fe, const int* __restrict__ type_ids,
+// Fused-step variant: the pair force is gathered from the Z-ordered
+// accumulator through the inverse permutation (random reads, coalesced
+// writes), added to what the bonded kernels left in ForceEnergy when any ran
+// (read_fe), and the result stored to ForceEnergy as the reference leaves it
+// after integrate_motion; then the grid force, noise and update as bd_kernel.
+__global__ void __launch_bounds__(256) bd_gather_kernel(
+	float4* __restrict__ pos, float4* __restrict__ fe, const float4* __restrict__ fs,
+	const uint32_t* __restrict__ inv, const int* __restrict__ type_ids,
 	const uint32_t* __restrict__ flags, uint32_t n, TypeTable ty, Box box, BdParams bp,
-	int write_fe) {
-	const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
-	if (s >= n) return;
-	const uint32_t o = s2o[s];
-	float4 sp = sorted_pos[s];
-	float4 f = fs[s];
-	fs[s] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-	if (fe) {
-		const float4 ext = fe[o];
+	int read_fe) {
+	const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+	if (i >= n) return;
+	float4 f = fs[inv[i]];
+	if (read_fe) {
+		const float4 ext = fe[i];
 		f.x = __fadd_rn(ext.x, f.x);
 		f.y = __fadd_rn(ext.y, f.y);
 		f.z = __fadd_rn(ext.z, f.z);
 		f.w = __fadd_rn(ext.w, f.w);
 	}
-	const int type = type_of(sp);
-	if (!(flags && (flags[o] & kFlagRbAttached))) {
-		const float4 pmf = position_force(ty, type, sp.x, sp.y, sp.z, bp.efield);
-		f.x = __fadd_rn(f.x, pmf.x);
-		f.y = __fadd_rn(f.y, pmf.y);
-		f.z = __fadd_rn(f.z, pmf.z);
-		f.w = __fadd_rn(f.w, pmf.w);
-		const float3 xi = bd_noise(bp.base_seed, bp.base_ctr + o, bp.step);
-		sp = bd_update(sp, f.x, f.y, f.z, ty.diffusion[type], xi, box, bp);
-		sorted_pos[s] = sp;
-		float4 out = pos[o];
-		out.x = sp.x;
-		out.y = sp.y;
-		out.z = sp.z;
-		pos[o] = out;
+	if (flags && (flags[i] & kFlagRbAttached)) {
+		fe[i] = f;
+		return;
 	}
-	if (write_fe && fe) fe[o] = f;
+	const float4 p = pos[i];
+	const int type = type_ids[i];
+	const float4 pmf = position_force(ty, type, p.x, p.y, p.z, bp.efield);
+	const float3 xi = bd_noise(bp.base_seed, bp.base_ctr + i, bp.step);
+	if (pmf.w != 0.0f) f.w = __fadd_rn(f.w, pmf.w);
+	fe[i] = f;
+	pos[i] = bd_update(p, __fadd_rn(f.x, pmf.x), __fadd_rn(f.y, pmf.y), __fadd_rn(f.z, pmf.z),
+					   ty.diffusion[type], xi, box, bp);
 }
 
 __global__ void philox_kernel(uint64_t seed, uint32_t ctr0, uint32_t ctr1, uint32_t ctr2,
@@ -242,13 +236,13 @@ void bd_integrate(float4* pos, float4* fe, const int* type_ids, const uint32_t* 
 	MB2_LAUNCH bd_kernel<<<(n + 255) / 256, 256, 0, st>>>(pos, fe, type_ids, flags, n, types, box, p);
 }
 
-void bd_integrate_sorted(float4* sorted_pos, float4* force_sorted, const uint32_t* s2o,
-						 float4* pos, float4* fe, const int* type_ids, const uint32_t* flags,
-						 uint32_t n, const TypeTable& types, const Box& box, const BdParams& p,
-						 int write_fe, cudaStream_t st) {
+void bd_integrate_gather(float4* pos, float4* fe, const float4* force_sorted, const uint32_t* inv,
+						 const int* type_ids, const uint32_t* flags, uint32_t n,
+						 const TypeTable& types, const Box& box, const BdParams& p, int read_fe,
+						 cudaStream_t st) {
 	if (n == 0) return;
-	MB2_LAUNCH bd_sorted_kernel<<<(n + 255) / 256, 256, 0, st>>>(sorted_pos, force_sorted, s2o, pos, fe,
-													  type_ids, flags, n, types, box, p, write_fe);
+	MB2_LAUNCH bd_gather_kernel<<<(n + 255) / 256, 256, 0, st>>>(pos, fe, force_sorted, inv, type_ids,
+																 flags, n, types, box, p, read_fe);
 }
 
 void philox_draws(uint64_t seed, uint32_t ctr0, uint32_t ctr1, uint32_t ctr2, uint32_t n,

@@ -9,27 +9,27 @@
 // same orientation via bit 31 of the list entry); only the order in which
 // the per-particle sums accumulate differs.
 //
-// Layout: a group of G lanes owns one row (sorted particle i) of the CSR half
-// list. Lanes stride over the row, gather sorted float4 positions (type id in
-// .w), accumulate -f for i in registers and scatter +f to j with one vector
-// `red.global.add.v4.f32` per pair (energy rides in .w). The row's i force is
-// reduced across the group with shuffles and added with one more vector red.
-// Tables and the type-pair tag matrix live in shared memory.
+// Table lookup (TabulatedPotential::compute, TabulatedPotential.h:19-52) is
+// precomputed per bin: bin_force[k] = -(U[k+1] - U[k]) * step_inv rounded as
+// the reference rounds it, and 0 for the last bin (the reference's
+// home >= size-1 branch); bin_energy[k] = (U[k], U[k+1] - U[k]). A lookup is
+// then w = (x - start) * step_inv, home = clamp(floor(w), 0, size-1) and one
+// shared-memory load -- bit-identical to the reference's branches.
 //
-// FP64: the total pair energy and virial are reduced in double on the device
-// (a per-thread double, a block reduction, one double atomic per block).
+// Layout: G lanes own one row (sorted particle i) of the sliced-ELL half list
+// and H = 32 / G rows share a warp, so one warp load of entries k..k+G-1 of
+// H rows is one 128-byte line. Lanes gather sorted float4 positions (type id
+// in .w), accumulate -f for i in registers and scatter +f to j with one
+// vector `red.global.add.v4.f32` (energy rides in .w). The row's i force is
+// reduced across its G lanes with shuffles and added with one more red.
+//
+// FP64: total pair energy and virial are reduced in double on the device
+// (per-thread double, block reduction, one double atomic per block).
 #include "mb2_internal.cuh"
 
 namespace mb2 {
 
 namespace {
-
-struct SmemTable {
-	float start;
-	float step_inv;
-	int size;
-	int offset;
-};
 
 __device__ __forceinline__ void block_add_f64(double a, double b, double* out) {
 	__shared__ double red_a[32], red_b[32];
@@ -60,90 +60,131 @@ __device__ __forceinline__ void block_add_f64(double a, double b, double* out) {
 	}
 }
 
-template <int G>
-__global__ void __launch_bounds__(256) pair_force_kernel(
-	const float4* __restrict__ sorted_pos, const uint32_t* __restrict__ row_start,
-	const uint32_t* __restrict__ nbr, uint32_t n, const uint32_t* __restrict__ term_g, int T,
-	const Table* __restrict__ tables_g, int num_tables, const float* __restrict__ values_g,
-	uint32_t total_values, Box box, float cutoff_sq, int get_energy, float4* force,
-	double* __restrict__ ev) {
-	extern __shared__ uint32_t smem[];
-	uint32_t* term = smem;                                                    // T*T
-	SmemTable* tabs = reinterpret_cast<SmemTable*>(smem + ((T * T + 3) & ~3)); // num_tables
-	float* vals = reinterpret_cast<float*>(tabs + num_tables);               // total_values
-	for (int k = threadIdx.x; k < T * T; k += blockDim.x) term[k] = term_g[k];
-	for (int k = threadIdx.x; k < num_tables; k += blockDim.x) {
-		const Table t = tables_g[k];
-		tabs[k] = SmemTable{t.start, t.step_inv, static_cast<int>(t.size),
-							static_cast<int>(t.pot - values_g)};
-	}
-	for (uint32_t k = threadIdx.x; k < total_values; k += blockDim.x) vals[k] = values_g[k];
-	__syncthreads();
+// Minimum image of one component for an all-periodic box, same rounding as
+// PeriodicBox::wrap_diff_scalar.
+__device__ __forceinline__ float wrap1(float x, float l, float inv, float half) {
+	const float image = floorf(__fmul_rn(x, inv));
+	x = __fsub_rn(x, __fmul_rn(image, l));
+	return x >= half ? __fsub_rn(x, l) : x;
+}
 
-	const int lane = threadIdx.x & (G - 1);
-	const uint32_t groups = blockDim.x / G;
-	const uint32_t i = blockIdx.x * groups + threadIdx.x / G;
-	double e_acc = 0.0, w_acc = 0.0;
-	// Rows past n get an empty range so that every lane reaches the group
-	// reduction below (the shuffles need the whole warp).
+// One pair of the half list, rounded as the reference rounds it. flip
+// (bit 31 of the entry): the reference orients the pair j -> i.
+template <bool kEnergy, bool kAllPeriodic>
+__device__ __forceinline__ void pair_scalar(const float4& pi, const float4& pj, uint32_t j,
+											uint32_t flip,
+											const PairTableRef* trow, const float* bin_f,
+											const float2* bin_e, const Box& box, float cutoff_sq,
+											float4* force, float& fx, float& fy, float& fz,
+											float& fe, double& e_acc, double& w_acc) {
+	// r = wrap_diff(pos[second] - pos[first])
+	// (pi - pj is exactly -(pj - pi) in round-to-nearest, so a sign flip suffices)
+	float dx = __uint_as_float(__float_as_uint(__fsub_rn(pj.x, pi.x)) ^ flip);
+	float dy = __uint_as_float(__float_as_uint(__fsub_rn(pj.y, pi.y)) ^ flip);
+	float dz = __uint_as_float(__float_as_uint(__fsub_rn(pj.z, pi.z)) ^ flip);
+	if (kAllPeriodic) {
+		dx = wrap1(dx, box.size[0], box.inv[0], box.half[0]);
+		dy = wrap1(dy, box.size[1], box.inv[1], box.half[1]);
+		dz = wrap1(dz, box.size[2], box.inv[2], box.half[2]);
+	} else {
+		const float3 r = wrap_diff(box, dx, dy, dz);
+		dx = r.x;
+		dy = r.y;
+		dz = r.z;
+	}
+	const float dist = __fsqrt_rn(len2(dx, dy, dz));
+	if (dist < 1e-6f || (cutoff_sq > 0.0f && __fmul_rn(dist, dist) > cutoff_sq)) return;
+	const PairTableRef t = trow[type_of(pj)];
+	if (t.offset < 0) return;
+	const float w = __fmul_rn(__fsub_rn(dist, t.start), t.step_inv);
+	const float wf = floorf(w);
+	const int home = min(max(static_cast<int>(wf), 0), t.last);
+	const float fm = bin_f[t.offset + home];
+	const float inv = __frcp_rn(dist);
+	// f = unit * F acts on the pair's second particle, -f on its first.
+	const float gx = __fmul_rn(__fmul_rn(inv, dx), fm);
+	const float gy = __fmul_rn(__fmul_rn(inv, dy), fm);
+	const float gz = __fmul_rn(__fmul_rn(inv, dz), fm);
+	float half = 0.0f;
+	if (kEnergy) {
+		const float2 ue = bin_e[t.offset + home];
+		const float e = __fadd_rn(__fmul_rn(ue.y, __fsub_rn(w, wf)), ue.x);
+		half = __fmul_rn(e, 0.5f);
+		e_acc += static_cast<double>(e);
+		w_acc += static_cast<double>(gx) * dx + static_cast<double>(gy) * dy +
+				 static_cast<double>(gz) * dz;
+	}
+	// j is the pair's second particle unless the pair is stored flipped.
+	const float hx = __uint_as_float(__float_as_uint(gx) ^ flip);
+	const float hy = __uint_as_float(__float_as_uint(gy) ^ flip);
+	const float hz = __uint_as_float(__float_as_uint(gz) ^ flip);
+	red_add_v4(&force[j], hx, hy, hz, half);
+	fx -= hx;
+	fy -= hy;
+	fz -= hz;
+	fe += half;
+}
+
+// Shared-memory copy of the per-type-pair table references and per-bin data.
+template <bool kEnergy>
+__device__ __forceinline__ void load_tables(int T, const PairTableRef* __restrict__ refs_g,
+											const float* __restrict__ force_g,
+											const float2* __restrict__ energy_g,
+											uint32_t total_bins, PairTableRef*& refs,
+											float*& bin_f, float2*& bin_e) {
+	extern __shared__ float4 smem4[];
+	refs = reinterpret_cast<PairTableRef*>(smem4);
+	bin_f = reinterpret_cast<float*>(refs + T * T);
+	bin_e = reinterpret_cast<float2*>(bin_f + ((total_bins + 1) & ~1u));
+	for (int k = threadIdx.x; k < T * T; k += blockDim.x) refs[k] = refs_g[k];
+	for (uint32_t k = threadIdx.x; k < total_bins; k += blockDim.x) {
+		bin_f[k] = force_g[k];
+		if (kEnergy) bin_e[k] = energy_g[k];
+	}
+	__syncthreads();
+}
+
+template <int G, bool kEnergy, bool kAllPeriodic>
+__global__ void __launch_bounds__(256) pair_force_kernel(
+	const float4* __restrict__ sorted_pos, const uint32_t* __restrict__ nbr,
+	const uint32_t* __restrict__ row_len, uint32_t n, uint32_t cap, int T,
+	const PairTableRef* __restrict__ refs_g, const float* __restrict__ force_g,
+	const float2* __restrict__ energy_g, uint32_t total_bins, Box box, float cutoff_sq,
+	float4* force, double* __restrict__ ev) {
+	constexpr int H = 32 / G;
+	PairTableRef* refs;
+	float* bin_f;
+	float2* bin_e;
+	load_tables<kEnergy>(T, refs_g, force_g, energy_g, total_bins, refs, bin_f, bin_e);
+
+	const int sub = threadIdx.x & (G - 1);  // lane within the row's group
+	const uint32_t i = blockIdx.x * (blockDim.x / G) + threadIdx.x / G;
 	const bool valid = i < n;
-	const float4 pi = valid ? sorted_pos[i] : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-	const uint32_t* trow = term + (valid ? type_of(pi) : 0) * T;
+	const float4 pi = valid ? sorted_pos[i] : make_float4(0.f, 0.f, 0.f, 0.f);
+	const PairTableRef* trow = refs + (valid ? type_of(pi) : 0) * T;
+	const uint32_t cnt = valid ? row_len[i] : 0u;
+	// Entry k of row i: ((i / H) * cap + k) * H + i % H.
+	const uint32_t* col = nbr + (static_cast<size_t>(i / H) * cap) * H + (i % H);
 	float fx = 0.0f, fy = 0.0f, fz = 0.0f, fe = 0.0f;
-	{
-		const uint32_t beg = valid ? row_start[i] : 0u;
-		const uint32_t end = valid ? row_start[i + 1] : 0u;
-		for (uint32_t p = beg + lane; p < end; p += G) {
-			const uint32_t entry = nbr[p];
-			const uint32_t j = entry & ~kOrientBit;
-			const float4 pj = sorted_pos[j];
-			// Reference orientation: r = wrap_diff(pos[second] - pos[first]).
-			float dx = __fsub_rn(pj.x, pi.x), dy = __fsub_rn(pj.y, pi.y),
-				  dz = __fsub_rn(pj.z, pi.z);
-			const uint32_t flip = entry & kOrientBit;
-			dx = __uint_as_float(__float_as_uint(dx) ^ flip);
-			dy = __uint_as_float(__float_as_uint(dy) ^ flip);
-			dz = __uint_as_float(__float_as_uint(dz) ^ flip);
-			const float3 r = wrap_diff(box, dx, dy, dz);
-			const float dist = __fsqrt_rn(len2(r.x, r.y, r.z));
-			if (dist < 1e-6f) continue;
-			if (cutoff_sq > 0.0f && __fmul_rn(dist, dist) > cutoff_sq) continue;
-			const uint32_t tag = trow[type_of(pj)];
-			if (!(tag & kTermTabulated)) continue;
-			const SmemTable t = tabs[tag >> kTableShift];
-			const float2 fm_e = table_lookup(vals + t.offset, t.size, t.start, t.step_inv, 0, dist);
-			const float inv = __frcp_rn(dist);
-			// f = unit * F (force on the pair's second particle)
-			float gx = __fmul_rn(__fmul_rn(inv, r.x), fm_e.x);
-			float gy = __fmul_rn(__fmul_rn(inv, r.y), fm_e.x);
-			float gz = __fmul_rn(__fmul_rn(inv, r.z), fm_e.x);
-			if (get_energy) {
-				e_acc += static_cast<double>(fm_e.y);
-				w_acc += static_cast<double>(gx) * r.x + static_cast<double>(gy) * r.y +
-						 static_cast<double>(gz) * r.z;
-			}
-			// j is the second particle unless the pair is stored flipped.
-			gx = __uint_as_float(__float_as_uint(gx) ^ flip);
-			gy = __uint_as_float(__float_as_uint(gy) ^ flip);
-			gz = __uint_as_float(__float_as_uint(gz) ^ flip);
-			const float half = get_energy ? __fmul_rn(fm_e.y, 0.5f) : 0.0f;
-			red_add_v4(&force[j], gx, gy, gz, half);
-			fx -= gx;
-			fy -= gy;
-			fz -= gz;
-			fe += half;
+	double e_acc = 0.0, w_acc = 0.0;
+	for (uint32_t t = sub; t < cnt; t += G) {
+		const uint32_t entry = __ldcs(col + static_cast<size_t>(t) * H);
+		const uint32_t j = entry & ~kOrientBit;
+		pair_scalar<kEnergy, kAllPeriodic>(pi, sorted_pos[j], j, entry & kOrientBit, trow, bin_f,
+										   bin_e, box, cutoff_sq, force, fx, fy, fz, fe, e_acc,
+										   w_acc);
+	}
+	if (G > 1) {
+#pragma unroll
+		for (int o = G / 2; o > 0; o >>= 1) {
+			fx += __shfl_xor_sync(0xFFFFFFFFu, fx, o, G);
+			fy += __shfl_xor_sync(0xFFFFFFFFu, fy, o, G);
+			fz += __shfl_xor_sync(0xFFFFFFFFu, fz, o, G);
+			if (kEnergy) fe += __shfl_xor_sync(0xFFFFFFFFu, fe, o, G);
 		}
 	}
-#pragma unroll
-	for (int o = G / 2; o > 0; o >>= 1) {
-		fx += __shfl_xor_sync(0xFFFFFFFFu, fx, o, G);
-		fy += __shfl_xor_sync(0xFFFFFFFFu, fy, o, G);
-		fz += __shfl_xor_sync(0xFFFFFFFFu, fz, o, G);
-		fe += __shfl_xor_sync(0xFFFFFFFFu, fe, o, G);
-	}
-	if (valid && lane == 0 && (fx != 0.0f || fy != 0.0f || fz != 0.0f || fe != 0.0f))
-		red_add_v4(&force[i], fx, fy, fz, fe);
-	if (get_energy) block_add_f64(e_acc, w_acc, ev);
+	if (valid && sub == 0 && cnt != 0u) red_add_v4(&force[i], fx, fy, fz, fe);
+	if (kEnergy) block_add_f64(e_acc, w_acc, ev);
 }
 
 __global__ void __launch_bounds__(256) scatter_add_kernel(const float4* __restrict__ fs,
@@ -176,10 +217,6 @@ __device__ __forceinline__ float calc_distance(const Box& box, const float4& fro
 	return dist;
 }
 
-__device__ __forceinline__ void add_v4(float4* p, float x, float y, float z, float w) {
-	red_add_v4(p, x, y, z, w);
-}
-
 // TabulatedBondComputer::operator() (src/Interactions/Bonded/BondComputer.h:168-191).
 __global__ void __launch_bounds__(256) bond_kernel(const int2* __restrict__ bonds,
 												   const int* __restrict__ table_idx, uint32_t nb,
@@ -199,8 +236,8 @@ __global__ void __launch_bounds__(256) bond_kernel(const int2* __restrict__ bond
 			const float fx = __fmul_rn(u.x, fm_e.x), fy = __fmul_rn(u.y, fm_e.x),
 						fz = __fmul_rn(u.z, fm_e.x);
 			const float half = get_energy ? __fmul_rn(fm_e.y, 0.5f) : 0.0f;
-			add_v4(&fe[b.x], -fx, -fy, -fz, half);
-			add_v4(&fe[b.y], fx, fy, fz, half);
+			red_add_v4(&fe[b.x], -fx, -fy, -fz, half);
+			red_add_v4(&fe[b.y], fx, fy, fz, half);
 			e_acc = get_energy ? static_cast<double>(fm_e.y) : 0.0;
 		}
 	}
@@ -252,67 +289,83 @@ __global__ void __launch_bounds__(256) angle_kernel(const int4* __restrict__ ang
 		const float f3y = __fmul_rn(s3, __fadd_rn(__fmul_rn(bc.y, c_bc), __fmul_rn(ab.y, inv_ab)));
 		const float f3z = __fmul_rn(s3, __fadd_rn(__fmul_rn(bc.z, c_bc), __fmul_rn(ab.z, inv_ab)));
 		const float third = get_energy ? __fmul_rn(fm_e.y, 0.3333333432674408f) : 0.0f;
-		add_v4(&fe[a.x], f1x, f1y, f1z, third);
-		add_v4(&fe[a.y], -__fadd_rn(f1x, f3x), -__fadd_rn(f1y, f3y), -__fadd_rn(f1z, f3z), third);
-		add_v4(&fe[a.z], f3x, f3y, f3z, third);
+		red_add_v4(&fe[a.x], f1x, f1y, f1z, third);
+		red_add_v4(&fe[a.y], -__fadd_rn(f1x, f3x), -__fadd_rn(f1y, f3y), -__fadd_rn(f1z, f3z),
+				   third);
+		red_add_v4(&fe[a.z], f3x, f3y, f3z, third);
 		e_acc = get_energy ? static_cast<double>(fm_e.y) : 0.0;
 	}
 	if (get_energy) block_add_f64(e_acc, 0.0, energy);
 }
 
-template <int G>
-void launch_pair(const float4* sorted_pos, const uint32_t* row_start, const uint32_t* nbr,
-				 uint32_t n, const PairTables& t, const Box& box, float cutoff_sq, int get_energy,
+template <int G, bool kEnergy, bool kAllPeriodic>
+void launch_pair(const float4* sorted_pos, const uint32_t* nbr, const uint32_t* row_len,
+				 uint32_t n, uint32_t cap, const PairTables& t, const Box& box, float cutoff_sq,
 				 float4* force_sorted, double* ev, cudaStream_t st) {
-	const size_t smem = static_cast<size_t>((t.num_types * t.num_types + 3) & ~3) * 4 +
-						static_cast<size_t>(t.num_tables) * sizeof(SmemTable) +
-						static_cast<size_t>(t.total_values) * 4;
-	auto kern = pair_force_kernel<G>;
+	const size_t smem = static_cast<size_t>(t.num_types * t.num_types) * sizeof(PairTableRef) +
+						static_cast<size_t>((t.total_bins + 1) & ~1u) * 4 +
+						(kEnergy ? static_cast<size_t>(t.total_bins) * 8 : 0);
+	const uint32_t rows = 256 / G;
+	const uint32_t blocks = (n + rows - 1) / rows;
+	auto kern = pair_force_kernel<G, kEnergy, kAllPeriodic>;
 	if (smem > 48 * 1024)
 		MB2_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
 									  static_cast<int>(smem)));
-	const uint32_t groups = 256 / G;
-	const uint32_t blocks = (n + groups - 1) / groups;
-	MB2_LAUNCH kern<<<blocks, 256, smem, st>>>(sorted_pos, row_start, nbr, n, t.term_matrix, t.num_types,
-									t.tables, t.num_tables, t.values, t.total_values, box,
-									cutoff_sq, get_energy, force_sorted, ev);
+	MB2_LAUNCH kern<<<blocks, 256, smem, st>>>(sorted_pos, nbr, row_len, n, cap, t.num_types,
+											   t.refs, t.bin_force, t.bin_energy, t.total_bins,
+											   box, cutoff_sq, force_sorted, ev);
+}
+
+template <int G>
+void launch_pair_g(const float4* sorted_pos, const uint32_t* nbr, const uint32_t* row_len,
+				   uint32_t n, uint32_t cap, const PairTables& t, const Box& box, float cutoff_sq,
+				   int get_energy, float4* force_sorted, double* ev, cudaStream_t st) {
+	const bool all_periodic = box.periodic[0] && box.periodic[1] && box.periodic[2];
+	if (get_energy) {
+		if (all_periodic) launch_pair<G, true, true>(sorted_pos, nbr, row_len, n, cap, t, box, cutoff_sq, force_sorted, ev, st);
+		else launch_pair<G, true, false>(sorted_pos, nbr, row_len, n, cap, t, box, cutoff_sq, force_sorted, ev, st);
+	} else {
+		if (all_periodic) launch_pair<G, false, true>(sorted_pos, nbr, row_len, n, cap, t, box, cutoff_sq, force_sorted, ev, st);
+		else launch_pair<G, false, false>(sorted_pos, nbr, row_len, n, cap, t, box, cutoff_sq, force_sorted, ev, st);
+	}
 }
 
 }  // namespace
 
-void pair_forces(const float4* sorted_pos, const uint32_t* row_start, const uint32_t* nbr,
-				 uint32_t n, const PairTables& t, const Box& box, float cutoff_sq, int get_energy,
-				 float4* force_sorted, double* ev, int lanes_per_row, cudaStream_t st) {
+void pair_forces(const float4* sorted_pos, const uint32_t* nbr, const uint32_t* row_len,
+				 uint32_t n, uint32_t cap, int lanes_per_row, const PairTables& t, const Box& box,
+				 float cutoff_sq, int get_energy, float4* force_sorted, double* ev,
+				 cudaStream_t st) {
 	if (n == 0) return;
 	switch (lanes_per_row) {
-	case 4: launch_pair<4>(sorted_pos, row_start, nbr, n, t, box, cutoff_sq, get_energy, force_sorted, ev, st); break;
-	case 8: launch_pair<8>(sorted_pos, row_start, nbr, n, t, box, cutoff_sq, get_energy, force_sorted, ev, st); break;
-	case 16: launch_pair<16>(sorted_pos, row_start, nbr, n, t, box, cutoff_sq, get_energy, force_sorted, ev, st); break;
-	default: launch_pair<32>(sorted_pos, row_start, nbr, n, t, box, cutoff_sq, get_energy, force_sorted, ev, st); break;
+	case 4: launch_pair_g<4>(sorted_pos, nbr, row_len, n, cap, t, box, cutoff_sq, get_energy, force_sorted, ev, st); break;
+	case 8: launch_pair_g<8>(sorted_pos, nbr, row_len, n, cap, t, box, cutoff_sq, get_energy, force_sorted, ev, st); break;
+	case 16: launch_pair_g<16>(sorted_pos, nbr, row_len, n, cap, t, box, cutoff_sq, get_energy, force_sorted, ev, st); break;
+	default: launch_pair_g<32>(sorted_pos, nbr, row_len, n, cap, t, box, cutoff_sq, get_energy, force_sorted, ev, st); break;
 	}
 }
 
 void scatter_add_forces(const float4* force_sorted, const uint32_t* s2o, uint32_t n,
 						float4* force_energy, int get_energy, cudaStream_t st) {
 	if (n == 0) return;
-	MB2_LAUNCH scatter_add_kernel<<<(n + 255) / 256, 256, 0, st>>>(force_sorted, s2o, n, force_energy,
-														get_energy);
+	MB2_LAUNCH scatter_add_kernel<<<(n + 255) / 256, 256, 0, st>>>(force_sorted, s2o, n,
+																   force_energy, get_energy);
 }
 
 void bond_forces(const int2* bonds, const int* table_idx, uint32_t nb, const float4* pos,
 				 float4* fe, const Table* tables, const Box& box, int get_energy, double* energy,
 				 cudaStream_t st) {
 	if (nb == 0) return;
-	MB2_LAUNCH bond_kernel<<<(nb + 255) / 256, 256, 0, st>>>(bonds, table_idx, nb, pos, fe, tables, box,
-												  get_energy, energy);
+	MB2_LAUNCH bond_kernel<<<(nb + 255) / 256, 256, 0, st>>>(bonds, table_idx, nb, pos, fe, tables,
+															 box, get_energy, energy);
 }
 
 void angle_forces(const int4* angles, const int* table_idx, uint32_t na, const float4* pos,
 				  float4* fe, const Table* tables, const Box& box, int get_energy, double* energy,
 				  cudaStream_t st) {
 	if (na == 0) return;
-	MB2_LAUNCH angle_kernel<<<(na + 255) / 256, 256, 0, st>>>(angles, table_idx, na, pos, fe, tables, box,
-												   get_energy, energy);
+	MB2_LAUNCH angle_kernel<<<(na + 255) / 256, 256, 0, st>>>(angles, table_idx, na, pos, fe,
+															  tables, box, get_energy, energy);
 }
 
 }  // namespace mb2

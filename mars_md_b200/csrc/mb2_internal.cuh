@@ -33,6 +33,10 @@ template <typename T>
 struct DevBuf {
 	T* ptr = nullptr;
 	size_t cap = 0;
+	DevBuf() = default;
+	DevBuf(const DevBuf&) = delete;
+	DevBuf& operator=(const DevBuf&) = delete;
+	~DevBuf() { release(); }
 	void ensure(size_t n) {
 		if (n <= cap) return;
 		if (ptr) cudaFree(ptr);
@@ -101,39 +105,59 @@ struct CellGrid {
 	int m = 0;                 // cells per axis = 2^m
 	int shift = 30;            // 3 * (10 - m)
 	int num_stencil = 0;
-	std::vector<StencilEntry> stencil;
+	std::vector<StencilEntry> stencil;  // one cell's pruned stencil
+	int radius[3] = {0, 0, 0};          // stencil half-width in cells per axis
+	float wmin[3] = {0, 0, 0};          // narrowest cell width per axis
+	float lim = 0.0f;                   // pruning bound on the squared cell gap
+};
+// Parameters of the group walk (passed by value to the kernel).
+struct WalkGrid {
+	int m, shift, emax;
+	int full[3];               // periodic axis whose stencil spans every cell
+	int radius[3];
+	float wmin[3];
+	float lim;
+	float rc2;                 // pairlist cutoff squared, as the reference rounds it
+	float fast_lo, fast_hi;    // d^2 band that needs the exact test
 };
 CellGrid choose_cell_grid(const float* extent, const int* periodic, float rc_list, size_t n);
+void fast_test_band(const Box& box, float rc_list, float* fast_lo, float* fast_hi);
 void cell_ranges(const uint32_t* keys, uint32_t n, int shift, uint32_t* begin, uint32_t* end,
 				 size_t num_cells, cudaStream_t st);
-void neighbor_count(const float4* sorted_pos, const uint32_t* keys, const uint32_t* s2o,
-					const uint32_t* begin, const uint32_t* end, const StencilEntry* stencil,
-					int num_stencil, int m, int shift, float rc2, uint32_t n, const Box& box,
-					const Exclusions& ex, uint32_t* counts, cudaStream_t st);
-void neighbor_fill(const float4* sorted_pos, const uint32_t* keys, const uint32_t* s2o,
-				   const uint32_t* begin, const uint32_t* end, const StencilEntry* stencil,
-				   int num_stencil, int m, int shift, float rc2, uint32_t n, const Box& box,
-				   const Exclusions& ex, const uint32_t* row_start, uint32_t* nbr,
-				   cudaStream_t st);
-void export_pairs(const uint32_t* row_start, const uint32_t* nbr, const uint32_t* s2o,
-				  uint32_t n, int2* out, cudaStream_t st);
+// One walk over all groups: rows appended to the sliced-ELL list (entries past
+// `cap` are counted, not stored); stats[0] += pairs, stats[1] = max row length.
+void build_walk(const float4* sorted_pos, const uint32_t* keys, const uint32_t* s2o,
+				const uint32_t* begin, const uint32_t* end, const StencilEntry* stencil,
+				int num_stencil, const WalkGrid& wg, uint32_t n, const Box& box,
+				const Exclusions& ex, uint32_t* nbr, uint32_t cap, int hshift, uint32_t* row_len,
+				unsigned long long* stats, cudaStream_t st);
+void export_pairs(const uint32_t* nbr, const uint32_t* row_len, const uint32_t* row_off,
+				  const uint32_t* s2o, uint32_t n, uint32_t cap, int hshift, int2* out,
+				  cudaStream_t st);
 void max_displacement_sq(const float4* cur, const float4* prev, uint32_t n, const Box& box,
 						 unsigned int* out_bits, cudaStream_t st);
 void pack_sorted_positions(const float4* pos, const int* type_ids, const uint32_t* s2o,
 						   uint32_t n, float4* sorted_pos, cudaStream_t st);
 
 // forces.cu
+// Per type pair: the tabulated table's lookup constants and offset into the
+// per-bin arrays (offset < 0: the pair has no tabulated term).
+struct PairTableRef {
+	float start;
+	float step_inv;
+	int last;    // size - 1
+	int offset;  // into bin_force / bin_energy, or -1
+};
 struct PairTables {
 	int num_types = 0;
-	int num_tables = 0;
-	uint32_t* term_matrix = nullptr;  // device [T*T]
-	Table* tables = nullptr;          // device [num_tables], pot pointers into values
-	float* values = nullptr;          // device, concatenated
-	uint32_t total_values = 0;
+	uint32_t total_bins = 0;
+	const PairTableRef* refs = nullptr;   // device [T*T]
+	const float* bin_force = nullptr;     // device: -(U[k+1]-U[k]) * step_inv, 0 at k = size-1
+	const float2* bin_energy = nullptr;   // device: (U[k], U[k+1]-U[k]), (U[size-1], 0) last
 };
-void pair_forces(const float4* sorted_pos, const uint32_t* row_start, const uint32_t* nbr,
-				 uint32_t n, const PairTables& t, const Box& box, float cutoff_sq, int get_energy,
-				 float4* force_sorted, double* energy_virial, int lanes_per_row,
+void pair_forces(const float4* sorted_pos, const uint32_t* nbr, const uint32_t* row_len,
+				 uint32_t n, uint32_t cap, int lanes_per_row, const PairTables& t, const Box& box,
+				 float cutoff_sq, int get_energy, float4* force_sorted, double* energy_virial,
 				 cudaStream_t st);
 void scatter_add_forces(const float4* force_sorted, const uint32_t* s2o, uint32_t n,
 						float4* force_energy, int get_energy, cudaStream_t st);
@@ -180,10 +204,11 @@ struct BdParams {
 };
 void bd_integrate(float4* pos, float4* fe, const int* type_ids, const uint32_t* flags, uint32_t n,
 				  const TypeTable& types, const Box& box, const BdParams& p, cudaStream_t st);
-void bd_integrate_sorted(float4* sorted_pos, float4* force_sorted, const uint32_t* s2o,
-						 float4* pos, float4* fe, const int* type_ids, const uint32_t* flags,
-						 uint32_t n, const TypeTable& types, const Box& box, const BdParams& p,
-						 int write_fe, cudaStream_t st);
+// The fused step's integrate: force = force_sorted[inv[i]] (+ fe[i] if read_fe).
+void bd_integrate_gather(float4* pos, float4* fe, const float4* force_sorted, const uint32_t* inv,
+						 const int* type_ids, const uint32_t* flags, uint32_t n,
+						 const TypeTable& types, const Box& box, const BdParams& p, int read_fe,
+						 cudaStream_t st);
 void philox_draws(uint64_t seed, uint32_t ctr0, uint32_t ctr1, uint32_t ctr2, uint32_t n,
 				  uint32_t* out4, float* normals4, cudaStream_t st);
 

@@ -6,24 +6,42 @@
 // (src/PatchOperation/PairListKernels/ZOrderPairlist.cpp:208-366).
 //
 // The pair SET is the reference's: for sorted i < sorted j, keep (i, j) when
-// wrap_diff(pos_j - pos_i).length2() <= rc^2 and the pair is not excluded.
-// Only the search structure differs. Cells are the top 3m bits of the 30-bit
-// Morton key, and the stencil is every cell whose box-to-box distance from
-// the home cell can be within rc (a pruned sphere rather than the reference's
-// (2r+1)^3 cube), chosen per run to minimise candidates plus per-cell cost.
+// wrap_diff(pos_j - pos_i).length2() <= rc^2 (float, exactly as the reference
+// rounds it) and the pair is not excluded. Only the search differs.
 //
-// Storage is a CSR half list keyed by sorted i: row_start[i]..row_start[i+1]
-// hold u32 sorted j. Bit 31 of an entry records the reference's pair
-// orientation: set when the original index of j is smaller than that of i,
-// i.e. the reference computes the pair as j -> i. Rows are filled in two
-// walks (count, then exclusive scan, then fill), so the list is exact-size
-// and the fill never overflows.
+// Search. Cells are the top 3m bits of the 30-bit Morton key; a cell's
+// particles are a contiguous run of the sorted array. The stencil is every
+// cell whose box-to-box distance from the home cell can be within rc (a
+// pruned sphere, not the reference's (2r+1)^3 cube), at the cell level chosen
+// per run to minimise candidates plus per-cell cost. One warp owns one
+// group of 32 consecutive sorted particles and walks, in lockstep, the cells
+// within rc of the group's cell bounding box, testing one candidate per
+// step against all of them. The test is a cheap minimum-image distance; only candidates
+// inside a rounding band around rc (sized from the float ulp of the box)
+// take the exact reference computation.
+//
+// Storage. A half list in sliced ELL form: rows of H consecutive particles
+// form a slice; entry k of row i sits at ((i / H) * cap + k) * H + i % H, so
+// that G = 32 / H lanes per row reading k..k+G-1 of H rows touch one 128-byte
+// line. row_len[i] holds the row's length. Bit 31 of an entry records the
+// reference's pair orientation: set when the original index of j is smaller
+// than that of i (the reference computes that pair as j -> i).
 #include "mb2_internal.cuh"
 
 #include <algorithm>
 #include <cmath>
 
 namespace mb2 {
+
+namespace {
+
+double ulp_of(double x) {
+	x = std::fabs(x);
+	if (x < 1e-30) return 1e-45;
+	return std::ldexp(1.0, static_cast<int>(std::floor(std::log2(x))) - 23);
+}
+
+}  // namespace
 
 CellGrid choose_cell_grid(const float* extent, const int* periodic, float rc_list, size_t n) {
 	CellGrid best;
@@ -35,19 +53,23 @@ CellGrid choose_cell_grid(const float* extent, const int* periodic, float rc_lis
 		if (m > 0 && num_cells > 2.0 * static_cast<double>(n)) break;
 		std::vector<int> off[3];
 		std::vector<double> gap[3];
+		int radius[3] = {0, 0, 0};
+		double wmin[3] = {0, 0, 0};
 		for (int a = 0; a < 3; ++a) {
 			if (m == 0) {
 				off[a] = {0};
 				gap[a] = {0.0};
+				wmin[a] = extent[a];
 				continue;
 			}
 			// Real-space cell widths: cell c spans Morton coordinates
 			// [c 2^k, (c+1) 2^k) of the 0..1023 scale over the domain, so it is
 			// extent * 2^k / 1023 wide, except the last, extent * (2^k - 1) / 1023.
 			const int k = 10 - m;
-			const double wmin = static_cast<double>(extent[a]) * (std::ldexp(1.0, k) - 1.0) / 1023.0 *
-								(1.0 - 1e-6);
-			const int r = static_cast<int>(std::floor(rc / wmin)) + 1;
+			wmin[a] = static_cast<double>(extent[a]) * (std::ldexp(1.0, k) - 1.0) / 1023.0 *
+					  (1.0 - 1e-6);
+			const int r = static_cast<int>(std::floor(rc / wmin[a])) + 1;
+			radius[a] = r;
 			if (periodic[a] && 2 * r + 1 >= cells) {
 				for (int d = 0; d < cells; ++d) {
 					off[a].push_back(d);
@@ -56,8 +78,7 @@ CellGrid choose_cell_grid(const float* extent, const int* periodic, float rc_lis
 			} else {
 				for (int d = -r; d <= r; ++d) {
 					off[a].push_back(d);
-					const double g = std::max(0, std::abs(d) - 1) * wmin;
-					gap[a].push_back(g);
+					gap[a].push_back(std::max(0, std::abs(d) - 1) * wmin[a]);
 				}
 			}
 		}
@@ -78,9 +99,29 @@ CellGrid choose_cell_grid(const float* extent, const int* periodic, float rc_lis
 			best.shift = 3 * (10 - m);
 			best.num_stencil = static_cast<int>(st.size());
 			best.stencil = st;
+			for (int a = 0; a < 3; ++a) {
+				best.radius[a] = radius[a];
+				best.wmin[a] = static_cast<float>(wmin[a]);
+			}
+			best.lim = static_cast<float>(lim);
 		}
 	}
 	return best;
+}
+
+void fast_test_band(const Box& box, float rc_list, float* fast_lo, float* fast_hi) {
+	// Each minimum-image component differs from the reference's wrap_diff by at
+	// most a few ulp of the largest coordinate magnitude; bound |d^2 - d_ref^2|.
+	double mag = 0.0;
+	for (int a = 0; a < 3; ++a)
+		mag = std::max({mag, std::fabs(static_cast<double>(box.origin[a])),
+						std::fabs(static_cast<double>(box.origin[a]) + box.size[a]),
+						static_cast<double>(box.size[a])});
+	const double rc = rc_list;
+	const double per_axis = 4.0 * ulp_of(2.0 * mag);
+	const double delta = 2.0 * rc * 3.0 * per_axis * 2.0 + rc * rc * 1e-6;
+	*fast_lo = static_cast<float>(rc * rc - delta);
+	*fast_hi = static_cast<float>(rc * rc + delta);
 }
 
 namespace {
@@ -96,87 +137,237 @@ __global__ void __launch_bounds__(256) cell_ranges_kernel(const uint32_t* __rest
 	if (i + 1 == n || (keys[i + 1] >> shift) != c) end[c] = i + 1;
 }
 
-__device__ __forceinline__ bool is_excluded(const Exclusions& ex, int a, int b, int row_b,
-											int row_e, int body) {
+__device__ __forceinline__ bool is_excluded(const Exclusions& ex, int b, int row_b, int row_e,
+											int body) {
 	if (body >= 0 && ex.rigid_body_id[b] == body) return true;
 	for (int e = row_b; e < row_e; ++e)
 		if (ex.neighbors[e] == b) return true;
 	return false;
 }
 
-template <bool kFill, bool kExcl>
-__global__ void __launch_bounds__(256) walk_kernel(
+// Exact reference test: wrap_diff(pj - pi).length2() <= rc2, same rounding.
+__device__ __forceinline__ bool exact_hit(const Box& box, const float4& pi, const float4& pj,
+										  float rc2) {
+	const float3 d = wrap_diff(box, __fsub_rn(pj.x, pi.x), __fsub_rn(pj.y, pi.y),
+							   __fsub_rn(pj.z, pi.z));
+	return len2(d.x, d.y, d.z) <= rc2;
+}
+
+__device__ __forceinline__ int warp_min(int v) {
+#pragma unroll
+	for (int o = 16; o > 0; o >>= 1) v = min(v, __shfl_xor_sync(0xFFFFFFFFu, v, o));
+	return v;
+}
+__device__ __forceinline__ int warp_max(int v) {
+#pragma unroll
+	for (int o = 16; o > 0; o >>= 1) v = max(v, __shfl_xor_sync(0xFFFFFFFFu, v, o));
+	return v;
+}
+
+// Appends one lane's row of the sliced-ELL list; entries past cap are only
+// counted (the host then grows the list and walks again).
+struct RowWriter {
+	uint32_t* base;  // &nbr[entry 0 of this row]
+	uint32_t len;
+	uint32_t cap;
+	int h;           // slice height: stride between a row's entries
+	__device__ __forceinline__ void append(uint32_t entry) {
+		if (len < cap) base[static_cast<size_t>(len) * h] = entry;
+		++len;
+	}
+};
+
+// One warp owns a group of 32 consecutive sorted particles, lane = particle.
+// The group's cells are Morton-adjacent; the warp walks, in lockstep, every
+// cell within rc of the group's cell bounding box, loading each candidate
+// once for all 32 lanes (a broadcast). Cells before the group's first cell in
+// Morton order hold only earlier particles and are skipped without loading
+// their ranges. A group whose cells straddle a Morton discontinuity (wide
+// bounding box) walks each particle's own pruned stencil instead. Each row
+// keeps candidate order (runs of consecutive sorted j), which keeps the force
+// kernel's gathers local.
+template <bool kExcl>
+__global__ void __launch_bounds__(256) build_walk_kernel(
 	const float4* __restrict__ sorted_pos, const uint32_t* __restrict__ keys,
 	const uint32_t* __restrict__ s2o, const uint32_t* __restrict__ begin,
-	const uint32_t* __restrict__ end, const StencilEntry* __restrict__ stencil_g, int ns, int m,
-	int shift, float rc2, uint32_t n, Box box, Exclusions ex, uint32_t* __restrict__ counts,
-	const uint32_t* __restrict__ row_start, uint32_t* __restrict__ nbr) {
+	const uint32_t* __restrict__ end, const StencilEntry* __restrict__ stencil_g, int ns,
+	WalkGrid wg, uint32_t n, Box box, Exclusions ex, uint32_t* __restrict__ nbr, uint32_t cap,
+	int hshift, uint32_t* __restrict__ row_len, unsigned long long* __restrict__ stats) {
 	extern __shared__ int4 stencil[];
+	__shared__ uint32_t split_tab[256];
+	const int cells = 1 << wg.m;
 	for (int k = threadIdx.x; k < ns; k += blockDim.x) {
 		const StencilEntry e = stencil_g[k];
 		stencil[k] = make_int4(e.dx, e.dy, e.dz, 0);
 	}
+	for (int k = threadIdx.x; k < cells; k += blockDim.x) split_tab[k] = split_by3(k);
 	__syncthreads();
 	const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-	if (i >= n) return;
-	const float4 pi = sorted_pos[i];
-	const uint32_t c = keys[i] >> shift;
-	const int cells = 1 << m;
+	const uint32_t i_first = i & ~31u;
+	if (i_first >= n) return;  // whole warp past the end
+	const bool valid = i < n;
+	const int h = 1 << hshift;
 	const uint32_t mask = static_cast<uint32_t>(cells - 1);
+	const float4 pi = valid ? sorted_pos[i] : make_float4(0.f, 0.f, 0.f, 0.f);
+	const uint32_t c = valid ? keys[i] >> wg.shift : 0u;
 	const int cx = static_cast<int>(compact_by3(c >> 2));
 	const int cy = static_cast<int>(compact_by3(c >> 1));
 	const int cz = static_cast<int>(compact_by3(c));
-	int a = 0, row_b = 0, row_e = 0, body = -1;
-	if (kFill || kExcl) a = static_cast<int>(s2o[i]);
-	if (kExcl) {
-		if (ex.offsets && a >= 0 && static_cast<uint32_t>(a) < ex.num_particles) {
+	const int a = valid ? static_cast<int>(s2o[i]) : 0;
+	int row_b = 0, row_e = 0, body = -1;
+	if (kExcl && valid) {
+		if (ex.offsets && static_cast<uint32_t>(a) < ex.num_particles) {
 			row_b = ex.offsets[a];
 			row_e = ex.offsets[a + 1];
 		}
 		body = ex.rigid_body_id ? ex.rigid_body_id[a] : -1;
 	}
-	uint32_t count = 0;
-	uint32_t out = kFill ? row_start[i] : 0u;
-	for (int k = 0; k < ns; ++k) {
-		const int4 s = stencil[k];
-		int nx = cx + s.x, ny = cy + s.y, nz = cz + s.z;
-		if (box.periodic[0]) nx = static_cast<int>(static_cast<uint32_t>(nx + cells) & mask);
-		else if (nx < 0 || nx >= cells) continue;
-		if (box.periodic[1]) ny = static_cast<int>(static_cast<uint32_t>(ny + cells) & mask);
-		else if (ny < 0 || ny >= cells) continue;
-		if (box.periodic[2]) nz = static_cast<int>(static_cast<uint32_t>(nz + cells) & mask);
-		else if (nz < 0 || nz >= cells) continue;
-		const uint32_t nc = (split_by3(static_cast<uint32_t>(nx)) << 2) |
-							(split_by3(static_cast<uint32_t>(ny)) << 1) |
-							split_by3(static_cast<uint32_t>(nz));
-		const uint32_t b = begin[nc];
-		const uint32_t e = end[nc];
-		for (uint32_t j = b > i + 1u ? b : i + 1u; j < e; ++j) {
-			const float4 pj = sorted_pos[j];
-			const float3 d = wrap_diff(box, __fsub_rn(pj.x, pi.x), __fsub_rn(pj.y, pi.y),
-									   __fsub_rn(pj.z, pi.z));
-			if (len2(d.x, d.y, d.z) <= rc2) {
-				int bj = 0;
-				if (kFill || kExcl) bj = static_cast<int>(s2o[j]);
-				if (kExcl && is_excluded(ex, a, bj, row_b, row_e, body)) continue;
-				if (kFill) nbr[out++] = j | (bj < a ? kOrientBit : 0u);
-				else ++count;
+	RowWriter row{nbr + (static_cast<size_t>(i >> hshift) * cap << hshift) + (i & (h - 1)), 0u,
+				  cap, h};
+	const uint32_t c_first = keys[i_first] >> wg.shift;
+
+	// Cell bounding box of the group (valid lanes only).
+	const int x0 = warp_min(valid ? cx : INT_MAX), x1 = warp_max(valid ? cx : INT_MIN);
+	const int y0 = warp_min(valid ? cy : INT_MAX), y1 = warp_max(valid ? cy : INT_MIN);
+	const int z0 = warp_min(valid ? cz : INT_MAX), z1 = warp_max(valid ? cz : INT_MIN);
+	const bool coherent = (x1 - x0) <= wg.emax && (y1 - y0) <= wg.emax && (z1 - z0) <= wg.emax;
+
+	if (coherent) {
+		const int lo[3] = {x0, y0, z0}, hi[3] = {x1, y1, z1};
+		int from[3], to[3];
+		bool full[3];
+#pragma unroll
+		for (int ax = 0; ax < 3; ++ax) {
+			full[ax] = box.periodic[ax] && (hi[ax] - lo[ax] + 2 * wg.radius[ax] + 1 >= cells);
+			from[ax] = full[ax] ? 0 : lo[ax] - wg.radius[ax];
+			to[ax] = full[ax] ? cells - 1 : hi[ax] + wg.radius[ax];
+		}
+		for (int ux = from[0]; ux <= to[0]; ++ux) {
+			int nx = ux;
+			float shx = 0.0f, gx = 0.0f;
+			if (!full[0]) {
+				const int gc = ux < x0 ? x0 - ux - 1 : (ux > x1 ? ux - x1 - 1 : 0);
+				gx = static_cast<float>(gc) * wg.wmin[0];
+				if (box.periodic[0]) {
+					if (ux < 0) { nx = ux + cells; shx = -box.size[0]; }
+					else if (ux >= cells) { nx = ux - cells; shx = box.size[0]; }
+				} else if (ux < 0 || ux >= cells) {
+					continue;
+				}
+			}
+			const float gx2 = gx * gx;
+			if (gx2 > wg.lim) continue;
+			const uint32_t sx = split_tab[nx] << 2;
+			for (int uy = from[1]; uy <= to[1]; ++uy) {
+				int ny = uy;
+				float shy = 0.0f, gy = 0.0f;
+				if (!full[1]) {
+					const int gc = uy < y0 ? y0 - uy - 1 : (uy > y1 ? uy - y1 - 1 : 0);
+					gy = static_cast<float>(gc) * wg.wmin[1];
+					if (box.periodic[1]) {
+						if (uy < 0) { ny = uy + cells; shy = -box.size[1]; }
+						else if (uy >= cells) { ny = uy - cells; shy = box.size[1]; }
+					} else if (uy < 0 || uy >= cells) {
+						continue;
+					}
+				}
+				const float gxy2 = gx2 + gy * gy;
+				if (gxy2 > wg.lim) continue;
+				const uint32_t sxy = sx | (split_tab[ny] << 1);
+				for (int uz = from[2]; uz <= to[2]; ++uz) {
+					int nz = uz;
+					float shz = 0.0f, gz = 0.0f;
+					if (!full[2]) {
+						const int gc = uz < z0 ? z0 - uz - 1 : (uz > z1 ? uz - z1 - 1 : 0);
+						gz = static_cast<float>(gc) * wg.wmin[2];
+						if (box.periodic[2]) {
+							if (uz < 0) { nz = uz + cells; shz = -box.size[2]; }
+							else if (uz >= cells) { nz = uz - cells; shz = box.size[2]; }
+						} else if (uz < 0 || uz >= cells) {
+							continue;
+						}
+					}
+					if (gxy2 + gz * gz > wg.lim) continue;
+					const uint32_t nc = sxy | split_tab[nz];
+					if (nc < c_first) continue;
+					const uint32_t b = begin[nc], e = end[nc];
+					const uint32_t jlo = b > i_first + 1u ? b : i_first + 1u;
+					if (jlo >= e) continue;
+					// Particle coordinates moved into the candidate cell's image.
+					const float qx = pi.x - shx, qy = pi.y - shy, qz = pi.z - shz;
+					for (uint32_t j = jlo; j < e; ++j) {
+						const float4 pj = sorted_pos[j];
+						if (!valid || j <= i) continue;
+						float dx = pj.x - qx, dy = pj.y - qy, dz = pj.z - qz;
+						if (full[0]) dx -= box.size[0] * rintf(dx * box.inv[0]);
+						if (full[1]) dy -= box.size[1] * rintf(dy * box.inv[1]);
+						if (full[2]) dz -= box.size[2] * rintf(dz * box.inv[2]);
+						const float d2 = dx * dx + dy * dy + dz * dz;
+						bool hit = d2 < wg.fast_lo;
+						if (!hit && d2 <= wg.fast_hi) hit = exact_hit(box, pi, pj, wg.rc2);
+						if (hit) {
+							const int bj = static_cast<int>(s2o[j]);
+							if (kExcl && is_excluded(ex, bj, row_b, row_e, body)) continue;
+							row.append(j | (bj < a ? kOrientBit : 0u));
+						}
+					}
+				}
+			}
+		}
+	} else if (valid) {
+		// Wide group: each lane walks its own pruned cell stencil, exact test.
+		for (int k = 0; k < ns; ++k) {
+			const int4 s = stencil[k];
+			int nx = cx + s.x, ny = cy + s.y, nz = cz + s.z;
+			if (box.periodic[0]) nx = static_cast<int>(static_cast<uint32_t>(nx + cells) & mask);
+			else if (nx < 0 || nx >= cells) continue;
+			if (box.periodic[1]) ny = static_cast<int>(static_cast<uint32_t>(ny + cells) & mask);
+			else if (ny < 0 || ny >= cells) continue;
+			if (box.periodic[2]) nz = static_cast<int>(static_cast<uint32_t>(nz + cells) & mask);
+			else if (nz < 0 || nz >= cells) continue;
+			const uint32_t nc = (split_tab[nx] << 2) | (split_tab[ny] << 1) | split_tab[nz];
+			if (nc < c) continue;  // every particle there precedes i
+			const uint32_t b = begin[nc], e = end[nc];
+			for (uint32_t j = b > i + 1u ? b : i + 1u; j < e; ++j) {
+				const float4 pj = sorted_pos[j];
+				if (exact_hit(box, pi, pj, wg.rc2)) {
+					const int bj = static_cast<int>(s2o[j]);
+					if (kExcl && is_excluded(ex, bj, row_b, row_e, body)) continue;
+					row.append(j | (bj < a ? kOrientBit : 0u));
+				}
 			}
 		}
 	}
-	if (!kFill) counts[i] = count;
+	if (valid) row_len[i] = row.len;
+	// stats[0] = total pairs, stats[1] = longest row
+	unsigned long long tot = valid ? row.len : 0u;
+	int mx = valid ? static_cast<int>(min(row.len, 0x7FFFFFFFu)) : 0;
+#pragma unroll
+	for (int o = 16; o > 0; o >>= 1) {
+		tot += __shfl_xor_sync(0xFFFFFFFFu, tot, o);
+		mx = max(mx, __shfl_xor_sync(0xFFFFFFFFu, mx, o));
+	}
+	if ((threadIdx.x & 31) == 0) {
+		atomicAdd(stats, tot);
+		atomicMax(stats + 1, static_cast<unsigned long long>(mx));
+	}
 }
 
-__global__ void __launch_bounds__(256) export_kernel(const uint32_t* __restrict__ row_start,
-													 const uint32_t* __restrict__ nbr,
+__global__ void __launch_bounds__(256) export_kernel(const uint32_t* __restrict__ nbr,
+													 const uint32_t* __restrict__ row_len,
+													 const uint32_t* __restrict__ row_off,
 													 const uint32_t* __restrict__ s2o, uint32_t n,
+													 uint32_t cap, int hshift,
 													 int2* __restrict__ out) {
 	const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
 	if (i >= n) return;
 	const int a = static_cast<int>(s2o[i]);
-	for (uint32_t p = row_start[i]; p < row_start[i + 1]; ++p) {
-		const int b = static_cast<int>(s2o[nbr[p] & ~kOrientBit]);
-		out[p] = make_int2(a < b ? a : b, a < b ? b : a);
+	const int h = 1 << hshift;
+	const uint32_t* base = nbr + (static_cast<size_t>(i >> hshift) * cap << hshift) + (i & (h - 1));
+	const uint32_t len = row_len[i], off = row_off[i];
+	for (uint32_t k = 0; k < len; ++k) {
+		const int b = static_cast<int>(s2o[base[static_cast<size_t>(k) * h] & ~kOrientBit]);
+		out[off + k] = make_int2(a < b ? a : b, a < b ? b : a);
 	}
 }
 
@@ -232,44 +423,30 @@ void cell_ranges(const uint32_t* keys, uint32_t n, int shift, uint32_t* begin, u
 	MB2_LAUNCH cell_ranges_kernel<<<(n + 255) / 256, 256, 0, st>>>(keys, n, shift, begin, end);
 }
 
-template <bool kFill>
-static void launch_walk(const float4* sorted_pos, const uint32_t* keys, const uint32_t* s2o,
-						const uint32_t* begin, const uint32_t* end, const StencilEntry* stencil,
-						int ns, int m, int shift, float rc2, uint32_t n, const Box& box,
-						const Exclusions& ex, uint32_t* counts, const uint32_t* row_start,
-						uint32_t* nbr, cudaStream_t st) {
+void build_walk(const float4* sorted_pos, const uint32_t* keys, const uint32_t* s2o,
+				const uint32_t* begin, const uint32_t* end, const StencilEntry* stencil,
+				int num_stencil, const WalkGrid& wg, uint32_t n, const Box& box,
+				const Exclusions& ex, uint32_t* nbr, uint32_t cap, int hshift, uint32_t* row_len,
+				unsigned long long* stats, cudaStream_t st) {
+	MB2_CUDA(cudaMemsetAsync(stats, 0, 2 * sizeof(unsigned long long), st));
 	if (n == 0) return;
-	const size_t smem = static_cast<size_t>(ns) * sizeof(int4);
+	const size_t smem = static_cast<size_t>(num_stencil) * sizeof(int4);
 	const bool excl = ex.offsets != nullptr || ex.rigid_body_id != nullptr;
-	auto kern = excl ? walk_kernel<kFill, true> : walk_kernel<kFill, false>;
+	auto kern = excl ? build_walk_kernel<true> : build_walk_kernel<false>;
 	if (smem > 48 * 1024)
 		MB2_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
 									  static_cast<int>(smem)));
-	MB2_LAUNCH kern<<<(n + 255) / 256, 256, smem, st>>>(sorted_pos, keys, s2o, begin, end, stencil, ns, m,
-											 shift, rc2, n, box, ex, counts, row_start, nbr);
+	MB2_LAUNCH kern<<<(n + 255) / 256, 256, smem, st>>>(sorted_pos, keys, s2o, begin, end,
+														 stencil, num_stencil, wg, n, box, ex,
+														 nbr, cap, hshift, row_len, stats);
 }
 
-void neighbor_count(const float4* sorted_pos, const uint32_t* keys, const uint32_t* s2o,
-					const uint32_t* begin, const uint32_t* end, const StencilEntry* stencil,
-					int num_stencil, int m, int shift, float rc2, uint32_t n, const Box& box,
-					const Exclusions& ex, uint32_t* counts, cudaStream_t st) {
-	launch_walk<false>(sorted_pos, keys, s2o, begin, end, stencil, num_stencil, m, shift, rc2, n,
-					   box, ex, counts, nullptr, nullptr, st);
-}
-
-void neighbor_fill(const float4* sorted_pos, const uint32_t* keys, const uint32_t* s2o,
-				   const uint32_t* begin, const uint32_t* end, const StencilEntry* stencil,
-				   int num_stencil, int m, int shift, float rc2, uint32_t n, const Box& box,
-				   const Exclusions& ex, const uint32_t* row_start, uint32_t* nbr,
-				   cudaStream_t st) {
-	launch_walk<true>(sorted_pos, keys, s2o, begin, end, stencil, num_stencil, m, shift, rc2, n,
-					  box, ex, nullptr, row_start, nbr, st);
-}
-
-void export_pairs(const uint32_t* row_start, const uint32_t* nbr, const uint32_t* s2o,
-				  uint32_t n, int2* out, cudaStream_t st) {
+void export_pairs(const uint32_t* nbr, const uint32_t* row_len, const uint32_t* row_off,
+				  const uint32_t* s2o, uint32_t n, uint32_t cap, int hshift, int2* out,
+				  cudaStream_t st) {
 	if (n == 0) return;
-	MB2_LAUNCH export_kernel<<<(n + 255) / 256, 256, 0, st>>>(row_start, nbr, s2o, n, out);
+	MB2_LAUNCH export_kernel<<<(n + 255) / 256, 256, 0, st>>>(nbr, row_len, row_off, s2o, n, cap,
+															  hshift, out);
 }
 
 void max_displacement_sq(const float4* cur, const float4* prev, uint32_t n, const Box& box,
