@@ -77,6 +77,25 @@ MB2_API int mb2_sort_morton(mb2_context* ctx, const float* pos4, uint32_t n, con
 MB2_API int mb2_radix_sort_pairs(mb2_context* ctx, uint32_t* keys, uint32_t* vals, uint32_t n,
                          void* stream);
 
+/* The same stable in-place sort, allocating no device memory: no counterpart
+ * in the reference. mb2_radix_sort_pairs grows context scratch with cudaMalloc
+ * (and frees the old buffer, which synchronises the device) whenever n grows;
+ * callers that cannot allocate — a process whose HBM is already held by another
+ * allocator, or a loop that must never stall on an implicit synchronisation —
+ * use this one. Its scratch is a fixed array in the library's static device
+ * memory (about 8.6 MB per device, present once the module is loaded).
+ *   - n <= MB2_SORT_STATIC_MAX, else MB2_ERR_CAPACITY and nothing is touched.
+ *   - The first call on each device (n = 0 is enough) looks up the array's
+ *     device address with that device current; make it before any stream
+ *     capture.
+ *   - All calls on one device share the array: calls that overlap in time on
+ *     one device race. Order them (one stream, or explicit events).
+ *   - ctx selects the device and receives the error message; the context's
+ *     own buffers are not used. */
+#define MB2_SORT_STATIC_MAX 1048576u
+MB2_API int mb2_radix_sort_pairs_static(mb2_context* ctx, uint32_t* keys, uint32_t* vals,
+                                uint32_t n, void* stream);
+
 /* --- pairlist --------------------------------------------------------------
  * Exclusion CSR (device pointers, borrowed until the next build): replaces
  * Pairlist::set_exclusions with ExclusionView (Pairlist.h:125-127,

@@ -14,6 +14,7 @@ LIB_PATH = os.path.join(HERE, "libmarsb200.so")
 HEADER = os.path.join(os.path.dirname(HERE), "include", "marsb200.h")
 
 MB2_OK, MB2_ERR_ARG, MB2_ERR_CUDA, MB2_ERR_CAPACITY, MB2_ERR_STATE = 0, 1, 2, 3, 4
+MB2_SORT_STATIC_MAX = 1048576  # largest n of mb2_radix_sort_pairs_static
 STAGE_STEP, STAGE_PAIRLIST, STAGE_PAIR_FORCE, STAGE_INTEGRATE = 0, 1, 2, 3
 
 
@@ -59,6 +60,7 @@ def load(path: str = LIB_PATH):
     L.mb2_set_box.argtypes = [vp, fp, fp, ip]
     L.mb2_sort_morton.argtypes = [vp, vp, u32, fp, fp, vp, vp, vp, vp, vp]
     L.mb2_radix_sort_pairs.argtypes = [vp, vp, vp, u32, vp]
+    L.mb2_radix_sort_pairs_static.argtypes = [vp, vp, vp, u32, vp]
     L.mb2_set_exclusions.argtypes = [vp, vp, vp, u32, vp]
     L.mb2_build_pairlist.argtypes = [vp, vp, vp, u32, f, vp, u64p]
     L.mb2_num_pairs.argtypes = [vp, u64p]

@@ -466,6 +466,15 @@ int mb2_radix_sort_pairs(mb2_context* ctx, uint32_t* keys, uint32_t* vals, uint3
 	});
 }
 
+int mb2_radix_sort_pairs_static(mb2_context* ctx, uint32_t* keys, uint32_t* vals, uint32_t n,
+								void* stream) {
+	return guarded(ctx, [&] {
+		require(n == 0 || (keys && vals), MB2_ERR_ARG,
+				"mb2_radix_sort_pairs_static: null argument");
+		radix_sort_pairs_static(keys, vals, n, S(stream));
+	});
+}
+
 int mb2_set_exclusions(mb2_context* ctx, const int* offsets, const int* neighbors,
 					   uint32_t num_particles, const int* rigid_body_id) {
 	return guarded(ctx, [&] {

@@ -86,11 +86,24 @@ void morton_encode(const float4* pos, uint32_t n, const float* bmin, const float
 void radix_sort_pairs(Scratch& s, uint32_t* keys, uint32_t* vals, uint32_t n, cudaStream_t st);
 void inverse_and_gather(const uint32_t* s2o, uint32_t n, const float4* pos, uint32_t* inv,
 						float4* sorted_pos, cudaStream_t st);
+// Elements per radix-sort tile; the digit histogram holds 256 words per tile.
+constexpr uint32_t kSortTile = 2048;
+// Radix sort with caller-supplied scratch: keys_alt and vals_alt of n words,
+// hist of 256 * ceil(n / kSortTile) words, block_sums of
+// scan_blocks_needed(that) words. Nothing there needs to start at zero.
+void radix_sort_pairs_into(uint32_t* keys, uint32_t* vals, uint32_t n, uint32_t* keys_alt,
+						   uint32_t* vals_alt, uint32_t* hist, uint32_t* block_sums,
+						   cudaStream_t st);
+// noalloc.cu: the same sort over the library's static scratch (no allocation).
+void radix_sort_pairs_static(uint32_t* keys, uint32_t* vals, uint32_t n, cudaStream_t st);
 
 // scan.cu: exclusive prefix sum of n u32 values (in == out allowed). If
 // total is non-null the grand total is stored there (device pointer).
 void exclusive_scan_u32(Scratch& s, const uint32_t* in, uint32_t* out, size_t n, uint32_t* total,
 						cudaStream_t st);
+size_t scan_blocks_needed(size_t n);
+void exclusive_scan_u32_into(const uint32_t* in, uint32_t* out, size_t n, uint32_t* block_sums,
+							 cudaStream_t st);
 
 // Exclusion view (src/Interactions/DeviceExclusions.h:22-75), device pointers.
 struct Exclusions {

@@ -105,4 +105,17 @@ void exclusive_scan_u32(Scratch& s, const uint32_t* in, uint32_t* out, size_t n,
 	MB2_LAUNCH scan_apply_kernel<<<blocks, kScanThreads, 0, st>>>(in, n, s.scan_blocks.ptr, out);
 }
 
+// Same scan with the block-sum buffer supplied by the caller: at least
+// scan_blocks_needed(n) words, nothing of it read before it is written.
+size_t scan_blocks_needed(size_t n) { return (n + kScanBlock - 1) / kScanBlock; }
+
+void exclusive_scan_u32_into(const uint32_t* in, uint32_t* out, size_t n, uint32_t* block_sums,
+							 cudaStream_t st) {
+	if (n == 0) return;
+	const size_t blocks = scan_blocks_needed(n);
+	MB2_LAUNCH scan_reduce_kernel<<<blocks, kScanThreads, 0, st>>>(in, n, block_sums);
+	MB2_LAUNCH scan_sums_kernel<<<1, kScanThreads, 0, st>>>(block_sums, blocks, nullptr);
+	MB2_LAUNCH scan_apply_kernel<<<blocks, kScanThreads, 0, st>>>(in, n, block_sums, out);
+}
+
 }  // namespace mb2

@@ -137,6 +137,29 @@ void radix_sort_pairs(Scratch& s, uint32_t* keys, uint32_t* vals, uint32_t n, cu
 	// Four passes: the sorted data is back in the caller's buffers.
 }
 
+static_assert(kTile == kSortTile, "tile size shared with the scratch sizing");
+
+void radix_sort_pairs_into(uint32_t* keys, uint32_t* vals, uint32_t n, uint32_t* keys_alt,
+						   uint32_t* vals_alt, uint32_t* hist, uint32_t* block_sums,
+						   cudaStream_t st) {
+	if (n <= 1) return;
+	const uint32_t tiles = (n + kTile - 1) / kTile;
+	uint32_t *ks = keys, *vs = vals, *kd = keys_alt, *vd = vals_alt;
+	for (int pass = 0; pass < 4; ++pass) {
+		const int shift = 8 * pass;
+		MB2_LAUNCH radix_hist_kernel<<<tiles, kThreads, 0, st>>>(ks, n, shift, tiles, hist);
+		exclusive_scan_u32_into(hist, hist, static_cast<size_t>(tiles) * 256u, block_sums, st);
+		MB2_LAUNCH radix_scatter_kernel<<<tiles, kThreads, 0, st>>>(ks, vs, n, shift, tiles, hist,
+																	kd, vd);
+		uint32_t* t = ks;
+		ks = kd;
+		kd = t;
+		t = vs;
+		vs = vd;
+		vd = t;
+	}
+}
+
 void morton_encode(const float4* pos, uint32_t n, const float* bmin, const float* bmax,
 				   uint32_t* keys, uint32_t* idx, cudaStream_t st) {
 	float3 lo = make_float3(bmin[0], bmin[1], bmin[2]);

@@ -167,6 +167,12 @@ class Context:
         self.check(self.lib.mb2_radix_sort_pairs(self.h, _p(keys), _p(vals), keys.shape[0],
                                                  _stream(stream)))
 
+    def radix_sort_pairs_static(self, keys, vals, stream=None):
+        """Same sort over the library's static scratch: allocates no device memory
+        (n <= MB2_SORT_STATIC_MAX; concurrent calls on one device race)."""
+        self.check(self.lib.mb2_radix_sort_pairs_static(self.h, _p(keys), _p(vals),
+                                                        keys.shape[0], _stream(stream)))
+
     # -- pairlist ----------------------------------------------------------
     def build_pairlist(self, pos, type_ids, pairlist_cutoff, stream=None) -> int:
         npairs = C.c_uint64()
