@@ -107,13 +107,6 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(rows)}
 
 
-def _dist():
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    return world, rank, local
-
-
 def _traffic_from_profile():
     """Per-launch DRAM bytes of the pair-force kernel from the committed ncu summary."""
     path = os.path.join(ROOT, "profiles", "pair_force_large_plain.json")
@@ -131,12 +124,13 @@ def run_ours(args):
     import torch.distributed as dist
     from mars_md_b200 import _lib, workloads as W
     from mars_md_b200.engine import Context, setup_workload, step_params
+    from mars_md_b200.replicas import job_throughput, max_over_ranks, rank_env, replica_seed
 
-    world, rank, local = _dist()
+    world, rank, local = rank_env()
     torch.cuda.set_device(local)
     if world > 1:
         dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=300))
-    w = W.large_plain(seed=W.DEFAULT_SEED + rank)
+    w = W.large_plain(seed=replica_seed(W.DEFAULT_SEED, rank))
     ctx = Context(w.n, device=local)
     dev = setup_workload(ctx, w, device=f"cuda:{local}")
     if args.lanes:
@@ -172,12 +166,8 @@ def run_ours(args):
     launches = int(L.mb2_launch_count() - launches0)
     barrier()
     clk = clocks.stop()
-    ms = start.elapsed_time(stop)
-    if world > 1:
-        t = torch.tensor([ms], device=f"cuda:{local}")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
-    value = world * w.n * args.steps / (ms / 1e3)
+    ms = max_over_ranks(start.elapsed_time(stop), device=f"cuda:{local}")
+    value = job_throughput(w.n, args.steps, ms, world)
 
     # Per-kernel device time over one rebuild period, on the launching stream.
     ctx.set_profiling(True)
@@ -208,12 +198,8 @@ def run_ours(args):
         host_out.copy_(dev["pos"], non_blocking=True)
     e1.record(stream)
     torch.cuda.synchronize()
-    e_ms = e0.elapsed_time(e1)
-    if world > 1:
-        t = torch.tensor([e_ms], device=f"cuda:{local}")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e_ms = float(t.item())
-    e_value = world * w.n * e_steps / (e_ms / 1e3)
+    e_ms = max_over_ranks(e0.elapsed_time(e1), device=f"cuda:{local}")
+    e_value = job_throughput(w.n, e_steps, e_ms, world)
 
     bw, peak_kind = _peaks()
     pf_ms, pf_n = prof["pair_force_kernel"]
@@ -272,7 +258,8 @@ def cpu_baseline(w):
 
 
 def run_reference(args):
-    world, rank, local = _dist()
+    from mars_md_b200.replicas import rank_env
+    world, rank, local = rank_env()
     if rank != 0:
         return
     from mars_md_b200 import workloads as W
