@@ -58,5 +58,30 @@ def build(verbose: bool = False) -> str:
     return LIB
 
 
+HOST_DIR = os.path.join(HERE, "host")
+CPP_TEST_SRC = os.path.join(ROOT, "tests", "cpp", "pairlist_mirror_test.cpp")
+CPP_TEST_BIN = os.path.join(ROOT, "tests", "cpp", "_build", "pairlist_mirror_test")
+
+
+def build_cpp_mirror_test(verbose: bool = False) -> str:
+    """Compile the C++ host-mirror test program (g++ against libmarsb200.so)."""
+    lib = build(verbose)
+    deps = [CPP_TEST_SRC, lib, os.path.join(ROOT, "include", "marsb200.h")] + \
+        glob.glob(os.path.join(HOST_DIR, "*.hpp"))
+    if _stale(CPP_TEST_BIN, deps):
+        os.makedirs(os.path.dirname(CPP_TEST_BIN), exist_ok=True)
+        cuda = os.path.dirname(os.path.dirname(NVCC))
+        cmd = ["g++", "-std=c++17", "-O2", "-ffp-contract=off", "-Wall", "-Wextra",
+               "-I" + os.path.join(ROOT, "include"), "-I" + HOST_DIR,
+               "-I" + os.path.join(cuda, "include"), CPP_TEST_SRC, "-o", CPP_TEST_BIN,
+               "-L" + HERE, "-lmarsb200", "-L" + os.path.join(cuda, "lib64"), "-lcudart",
+               "-Wl,-rpath,$ORIGIN/../../../mars_md_b200",
+               "-Wl,-rpath," + os.path.join(cuda, "lib64")]
+        if verbose:
+            print(" ".join(cmd), flush=True)
+        subprocess.run(cmd, check=True)
+    return CPP_TEST_BIN
+
+
 if __name__ == "__main__":
     print(build(verbose="-v" in sys.argv))

@@ -1,0 +1,272 @@
+// The C++ host mirror (mars_md_b200/host/b200_pairlist.hpp) used the way the
+// reference's own pairlist and patch tests use theirs: a 4x4x4 lattice in an
+// open box (Unit_test/Compute/zorder_pairlist_tests.cpp), the skin check,
+// exclusions and rigid bodies dropped at build time, a periodic random system
+// against an O(N^2) pair set, the error behaviour, and the Patch stages
+// against the fused step. One line per check; exit status 0 only if all pass.
+#include <cmath>
+#include <cstdio>
+#include <random>
+#include <set>
+#include <utility>
+#include <vector>
+
+#include "b200_pairlist.hpp"
+
+using namespace marsb200;
+
+static int failures = 0;
+
+#define EXPECT(cond, name)                                              \
+	do {                                                                \
+		if (cond) {                                                     \
+			std::printf("PASS %s\n", name);                             \
+		} else {                                                        \
+			std::printf("FAIL %s (%s:%d)\n", name, __FILE__, __LINE__); \
+			++failures;                                                 \
+		}                                                               \
+	} while (0)
+
+// Minimum image as the reference's PeriodicBox::wrap_diff_scalar rounds it.
+static float wrap_diff_scalar(float x, float l) {
+	const float image = std::floor(x * (1.0f / l));
+	x = x - image * l;
+	return x >= 0.5f * l ? x - l : x;
+}
+
+static std::set<std::pair<int, int>> host_pairs(const std::vector<Vector3>& p, float l, float rc) {
+	std::set<std::pair<int, int>> out;
+	const float rc2 = rc * rc;
+	for (size_t i = 0; i < p.size(); ++i)
+		for (size_t j = i + 1; j < p.size(); ++j) {
+			const float dx = wrap_diff_scalar(p[j].x - p[i].x, l);
+			const float dy = wrap_diff_scalar(p[j].y - p[i].y, l);
+			const float dz = wrap_diff_scalar(p[j].z - p[i].z, l);
+			const float xx = dx * dx, yy = dy * dy, zz = dz * dz;
+			if ((xx + yy) + zz <= rc2) out.insert({static_cast<int>(i), static_cast<int>(j)});
+		}
+	return out;
+}
+
+static std::set<std::pair<int, int>> device_pairs(const Pairlist& pl) {
+	std::vector<int2> h(pl.get_num_pairs());
+	if (!h.empty()) pl.get_neighbor_pairs().copy_to_host(h.data(), h.size(), true);
+	std::set<std::pair<int, int>> out;
+	for (const int2& q : h) out.insert({q.x, q.y});
+	return out;
+}
+
+static std::vector<Vector3> lattice() {
+	std::vector<Vector3> p;
+	for (int x = 0; x < 4; ++x)
+		for (int y = 0; y < 4; ++y)
+			for (int z = 0; z < 4; ++z) p.emplace_back(1.5f * x, 1.5f * y, 1.5f * z);
+	return p;
+}
+
+static void lattice_tests(const Resource& res) {
+	auto pl = create_pairlist(PairlistBuilderType::B200, res, 64, 64 * 64);
+	EXPECT(pl->get_type() == PairlistBuilderType::B200, "factory returns the B200 strategy");
+	pl->set_periodic_box(PeriodicBox(Vector3(0, 0, 0), Vector3(100, 100, 100), false, false, false));
+	const std::vector<Vector3> h = lattice();
+	DeviceBuffer<Vector3> pos(h.size(), res);
+	pos.copy_from_host(h);
+	pl->build_pairlist(pos, h.size(), 2.0f);
+	EXPECT(pl->get_num_pairs() == 144, "lattice: 144 nearest-neighbour pairs");
+	bool all_bonds = true, ordered = true;
+	for (const auto& q : device_pairs(*pl)) {
+		const float dx = h[q.second].x - h[q.first].x, dy = h[q.second].y - h[q.first].y,
+					dz = h[q.second].z - h[q.first].z;
+		all_bonds &= std::fabs(std::sqrt(dx * dx + dy * dy + dz * dz) - 1.5f) < 1e-5f;
+		ordered &= q.first < q.second;
+	}
+	EXPECT(all_bonds, "lattice: every pair is 1.5 A apart");
+	EXPECT(ordered, "lattice: pairs stored as (min, max) original indices");
+	EXPECT(pl->get_cutoff() == 2.0f, "lattice: cutoff recorded");
+
+	// Skin check against the snapshot taken at the build.
+	EXPECT(!pl->needs_update(pos, pos, h.size(), 1.0f), "needs_update: no motion -> no rebuild");
+	std::vector<Vector3> moved = h;
+	moved[5].x += 0.6f;
+	DeviceBuffer<Vector3> pos2(h.size(), res);
+	pos2.copy_from_host(moved);
+	EXPECT(pl->needs_update(pos2, pos, h.size(), 1.0f), "needs_update: 0.6 A > skin / 2");
+	EXPECT(!pl->needs_update(pos2, pos, h.size(), 2.0f), "needs_update: 0.6 A < skin / 2");
+
+	// Exclusions (0,1) and (0,4) are never emitted.
+	std::vector<int> offsets(65, 0), excl;
+	std::vector<std::vector<int>> rows(64);
+	rows[0] = {1, 4};
+	rows[1] = {0};
+	rows[4] = {0};
+	for (int i = 0; i < 64; ++i) {
+		offsets[i + 1] = offsets[i] + static_cast<int>(rows[i].size());
+		excl.insert(excl.end(), rows[i].begin(), rows[i].end());
+	}
+	DeviceBuffer<int> d_off(offsets.size(), res), d_ex(excl.size(), res);
+	d_off.copy_from_host(offsets);
+	d_ex.copy_from_host(excl);
+	pl->set_exclusions(ExclusionView{d_off.data(), d_ex.data(), 64, nullptr});
+	pl->build_pairlist(pos, h.size(), 2.0f);
+	const auto ex_pairs = device_pairs(*pl);
+	EXPECT(pl->get_num_pairs() == 142 && !ex_pairs.count({0, 1}) && !ex_pairs.count({0, 4}),
+		   "exclusions dropped at build time");
+	// A rigid body: particles 16..19 (a lattice row) never pair with each other.
+	std::vector<int> body(64, -1);
+	for (int i = 16; i < 20; ++i) body[i] = 3;
+	DeviceBuffer<int> d_body(64, res);
+	d_body.copy_from_host(body);
+	pl->set_exclusions(ExclusionView{nullptr, nullptr, 0, d_body.data()});
+	pl->build_pairlist(pos, h.size(), 2.0f);
+	const auto rb = device_pairs(*pl);
+	EXPECT(pl->get_num_pairs() == 141 && !rb.count({16, 17}) && !rb.count({18, 19}),
+		   "same-rigid-body pairs dropped");
+}
+
+static void periodic_random_test(const Resource& res) {
+	const int n = 2000;
+	const float l = 60.0f, rc = 8.0f;
+	std::mt19937 rng(20261203);
+	std::uniform_real_distribution<float> u(0.0f, l);
+	std::vector<Vector3> h(n);
+	for (auto& p : h) p = Vector3(u(rng), u(rng), u(rng));
+	B200Pairlist pl(res, n, static_cast<size_t>(n) * n);
+	pl.set_periodic_box(PeriodicBox(Vector3(0, 0, 0), Vector3(l, l, l)));
+	DeviceBuffer<Vector3> pos(n, res);
+	pos.copy_from_host(h);
+	pl.build_pairlist(pos, n, rc);
+	const auto want = host_pairs(h, l, rc);
+	EXPECT(pl.get_num_pairs() == want.size(), "periodic random: pair count equals O(N^2) count");
+	EXPECT(device_pairs(pl) == want, "periodic random: identical pair set");
+	const auto st = pl.get_statistics();
+	EXPECT(st.num_particles == static_cast<size_t>(n) && st.num_pairs == want.size(),
+		   "statistics reflect the build");
+}
+
+static void error_tests(const Resource& res) {
+	bool threw = false;
+	try {
+		B200Pairlist pl(res, 16, 256);
+		DeviceBuffer<Vector3> pos(16, res);
+		pos.fill_zero();
+		pl.build_pairlist(pos, 16, 2.0f);  // no box set
+	} catch (const Exception& e) {
+		threw = e.type() == ExceptionType::StateError;
+	}
+	EXPECT(threw, "build without a box throws StateError");
+	threw = false;
+	try {
+		create_pairlist(PairlistBuilderType::CellList, res, 16, 256);
+	} catch (const Exception& e) {
+		threw = e.type() == ExceptionType::NotImplementedError;
+	}
+	EXPECT(threw, "unknown strategy throws NotImplementedError");
+	threw = false;
+	try {
+		B200Pairlist pl(res, 16, 256);
+		pl.set_periodic_box(PeriodicBox(Vector3(0, 0, 0), Vector3(10, 10, 10)));
+		DeviceBuffer<Vector3> pos(32, res);
+		pos.fill_zero();
+		pl.build_pairlist(pos, 32, 2.0f);
+	} catch (const Exception& e) {
+		threw = e.type() == ExceptionType::CapacityError;
+	}
+	EXPECT(threw, "more particles than capacity throws CapacityError");
+	threw = false;
+	try {
+		B200Pairlist pl(res, 16, 256);
+		pl.set_periodic_box(PeriodicBox(Vector3(0, 0, 0), Vector3(-1, 10, 10)));
+	} catch (const Exception& e) {
+		threw = e.type() == ExceptionType::ValueError;
+	}
+	EXPECT(threw, "non-positive box edge throws ValueError");
+}
+
+// WCA-like table on 0..19.9 A (sigma 4, eps 0.5, capped at 20).
+static Table wca() {
+	Table t;
+	t.start = 0.0f;
+	t.step_inv = 1.0f / 0.1f;
+	for (int k = 0; k < 200; ++k) {
+		const double r = 0.1 * k, rc = std::pow(2.0, 1.0 / 6.0) * 4.0;
+		double v = 0.0;
+		if (r < rc) {
+			const double s6 = r > 0 ? std::pow(4.0 / r, 6) : 1e30;
+			v = std::min(20.0, 4.0 * 0.5 * (s6 * s6 - s6) + 0.5);
+		}
+		t.values.push_back(static_cast<float>(v));
+	}
+	return t;
+}
+
+static void patch_stage_test(const Resource& res) {
+	const int n = 4096;
+	const float l = 200.0f;
+	std::mt19937 rng(7);
+	std::uniform_real_distribution<float> u(0.0f, l);
+	std::vector<Vector3> h(n);
+	for (auto& p : h) p = Vector3(u(rng), u(rng), u(rng));
+	std::vector<int> types(n, 0);
+	const float kT = 295.0f * 0.001987191f, dt = 1e-4f;
+	auto setup = [&](B200Patch& patch) {
+		patch.set_periodic_box(PeriodicBox(Vector3(0, 0, 0), Vector3(l, l, l)));
+		patch.set_pair_tables(1, {(1u << 5) | (0u << 8)}, {wca()});
+		patch.set_particle_types({0.0f}, {150.0f, 150.0f, 150.0f});
+	};
+	// Staged: clear, nonbonded, integrate -- three Patch calls per step.
+	B200Patch staged(res, n);
+	setup(staged);
+	DeviceBuffer<Vector3> pos_a(n, res), fe_a(n, res);
+	DeviceBuffer<int> d_types(n, res);
+	pos_a.copy_from_host(h);
+	d_types.copy_from_host(types);
+	for (size_t step = 1; step <= 5; ++step) {
+		staged.clear_forces(fe_a);
+		staged.calculate_nonbonded_forces(pos_a, d_types, fe_a, n, 25.0f, 20.0f, step, 20);
+		staged.integrate_motion(pos_a, fe_a, d_types, nullptr, n, dt, kT, step, 99);
+	}
+	// Fused: one mb2_step per step with the same schedule and seed.
+	B200Patch fused(res, n);
+	setup(fused);
+	DeviceBuffer<Vector3> pos_b(n, res), fe_b(n, res);
+	pos_b.copy_from_host(h);
+	mb2_step_params prm{};
+	prm.pairlist_cutoff = 25.0f;
+	prm.cutoff = 20.0f;
+	prm.rebuild_period = 20;
+	prm.dt = dt;
+	prm.kT = kT;
+	prm.seed = 99;
+	for (uint64_t step = 1; step <= 5; ++step)
+		check(mb2_step(fused.handle(), reinterpret_cast<float*>(pos_b.data()),
+					   reinterpret_cast<float*>(fe_b.data()), d_types.data(), nullptr, n, step, &prm,
+					   nullptr),
+			  fused.handle(), "mb2_step");
+	std::vector<Vector3> a, b;
+	pos_a.copy_to_host(a);
+	pos_b.copy_to_host(b);
+	float worst = 0.0f, moved = 0.0f;
+	for (int i = 0; i < n; ++i) {
+		worst = std::max({worst, std::fabs(a[i].x - b[i].x), std::fabs(a[i].y - b[i].y),
+						  std::fabs(a[i].z - b[i].z)});
+		moved = std::max(moved, std::fabs(a[i].x - h[i].x));
+	}
+	EXPECT(worst <= 1e-4f && moved > 0.1f, "Patch stages equal the fused step over 5 steps");
+}
+
+int main() {
+	Resource res;
+	res.device = 0;
+	cuda_check(cudaSetDevice(0), "cudaSetDevice");
+	try {
+		lattice_tests(res);
+		periodic_random_test(res);
+		error_tests(res);
+		patch_stage_test(res);
+	} catch (const std::exception& e) {
+		std::printf("FAIL unexpected exception: %s\n", e.what());
+		++failures;
+	}
+	std::printf(failures ? "FAILED %d\n" : "ALL PASS\n", failures);
+	return failures ? 1 : 0;
+}
