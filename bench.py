@@ -233,6 +233,11 @@ def run_ours(args):
         "gpu_launches": launches,
         "clocks": clk,
     }
+    if world == 1 and not args.no_batched:
+        del dev
+        ctx.close()
+        torch.cuda.empty_cache()
+        out["batched"] = run_batched(local)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         out["cpu_baseline"] = cpu_baseline(w)
     if world > 1:
@@ -240,6 +245,72 @@ def run_ours(args):
         dist.destroy_process_group()
     if rank == 0:
         print(json.dumps(out), flush=True)
+
+
+def run_batched(local, period_steps=20):
+    """512 independent systems (sizes log-uniform in [500, 20000], own periodic boxes at
+    0.002 A^-3, WCA table, cutoff 20 A, list 25 A): one batched run of one rebuild period
+    (autotuned, CUDA-graph step) against the same systems as 512 sequential plain runs."""
+    import torch
+    from mars_md_b200 import _lib, workloads as W
+    from mars_md_b200.engine import Context, setup_batch, setup_workload, step_params
+
+    device = f"cuda:{local}"
+    stream = torch.cuda.current_stream()
+    L = _lib.load()
+    ws = W.batched(seed=W.DEFAULT_SEED)
+    total = sum(w.n for w in ws)
+    prm = step_params(ws[0], seed=W.DEFAULT_SEED)
+    b, dev = setup_batch(ws, device=device)
+    tune = b.autotune(dev["pos"], dev["type"], prm, trial_steps=4)
+    b.run(dev["pos"], dev["fe"], dev["type"], 1, period_steps, prm)  # warm-up period
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    l0 = L.mb2_launch_count()
+    e0.record(stream)
+    b.run(dev["pos"], dev["fe"], dev["type"], period_steps + 1, period_steps, prm)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    batched_launches = int(L.mb2_launch_count() - l0)
+    batched_ms = e0.elapsed_time(e1)
+    npairs = b.num_pairs()
+    b.close()
+    del dev
+    torch.cuda.empty_cache()
+
+    # The same systems as sequential plain runs: one context per system, each run
+    # through its steps before the next system starts.
+    ctxs = []
+    for s, w in enumerate(ws):
+        c = Context(w.n, device=local)
+        d = setup_workload(c, w, device=device)
+        ctxs.append((c, d, step_params(w, seed=W.DEFAULT_SEED + s)))
+    for c, d, p in ctxs:
+        for k in range(1, period_steps + 1):
+            c.step(d["pos"], d["fe"], d["type"], None, k, p)
+    torch.cuda.synchronize()
+    l0 = L.mb2_launch_count()
+    e0.record(stream)
+    for c, d, p in ctxs:
+        for k in range(period_steps + 1, 2 * period_steps + 1):
+            c.step(d["pos"], d["fe"], d["type"], None, k, p)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    seq_launches = int(L.mb2_launch_count() - l0)
+    seq_ms = e0.elapsed_time(e1)
+    for c, _, _ in ctxs:
+        c.close()
+    bv = total * period_steps / (batched_ms / 1e3)
+    sv = total * period_steps / (seq_ms / 1e3)
+    return {"metric": "particle-steps/s, batched vs sequential plain runs", "systems": len(ws),
+            "beads": total, "steps": period_steps, "rebuilds_per_system": 1, "pairs": npairs,
+            "value": bv, "sequential_value": sv, "ratio": bv / sv, "ms": batched_ms,
+            "sequential_ms": seq_ms, "gpu_launches": batched_launches,
+            "sequential_gpu_launches": seq_launches,
+            "tuning": {k: (float(v) if isinstance(v, float) else v) for k, v in tune.items()},
+            "workload": "512 systems, sizes log-uniform in [500, 20000] beads, own periodic "
+                        "boxes at 0.002 A^-3, WCA table, cutoff 20 A, list 25 A, rebuild "
+                        "period 20, seeded synthetic"}
 
 
 def cpu_baseline(w):
@@ -294,6 +365,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-batched", action="store_true",
+                    help="skip the batched-replicas measurement")
     ap.add_argument("--lanes", type=int, default=0,
                     help="lanes per pairlist row in the pair kernel (0 = automatic)")
     args = ap.parse_args()

@@ -250,6 +250,69 @@ MB2_API int mb2_profile_read(mb2_context* ctx, int stage, double* total_ms, uint
  * or 32 lanes per row; 0 = choose from the mean row length. */
 MB2_API int mb2_set_lanes_per_row(mb2_context* ctx, int lanes);
 
+/* --- batched replicas ------------------------------------------------------
+ * Many independent periodic systems of uneven size stepped together, one
+ * launch per stage for all of them. No single counterpart in the reference:
+ * each system is what one reference Patch runs (Patch.cpp:43-352) through
+ * SimManager's step loop (SimManager.cpp:337-504); here all systems share
+ * each launch. Systems are concatenated in the caller's arrays (system s owns
+ * particles [sum(counts[<s]), sum(counts[<=s]))), each in its own periodic box
+ * (origin3/size3 per system, origin NULL = 0; every edge > 2 x list radius).
+ * System s steps exactly as mb2_step would with seed (params->seed + s):
+ * same pair set, same Philox key and counters (index within the system).
+ * Pair tables and particle types are shared by all systems; no grids, no
+ * bonded terms, no exclusions in this mode. At most 2048 systems. */
+typedef struct mb2_batch mb2_batch;
+MB2_API int mb2_batch_create(int device, uint32_t num_systems, const uint32_t* counts,
+                     const float* box_origin3, const float* box_size3, mb2_batch** out);
+MB2_API int mb2_batch_destroy(mb2_batch* b);
+MB2_API const char* mb2_batch_last_error(const mb2_batch* b);
+MB2_API int mb2_batch_set_pair_tables(mb2_batch* b, int num_types, const uint32_t* term_matrix,
+                              int num_tables, const float* values, const uint32_t* sizes,
+                              const float* starts, const float* step_invs);
+MB2_API int mb2_batch_set_particle_types(mb2_batch* b, int num_types, const float* charge,
+                                 const float* diffusion3);
+/* Pairlist of every system within pairlist_cutoff; synchronises once. */
+MB2_API int mb2_batch_build(mb2_batch* b, const float* pos4, const int* type_ids,
+                    float pairlist_cutoff, void* stream, uint64_t* num_pairs);
+MB2_API int mb2_batch_num_pairs(const mb2_batch* b, uint64_t* num_pairs);
+/* All pairs as int2(min, max) of indices into the concatenated arrays. */
+MB2_API int mb2_batch_export_pairs(mb2_batch* b, int* pairs2, uint64_t capacity, void* stream);
+/* One step of every system (the mb2_step sequence, rebuild schedule included:
+ * at scheduled steps the lists are rebuilt when any system moved more than
+ * half the skin). params->num_bonds and num_angles must be 0. */
+MB2_API int mb2_batch_step(mb2_batch* b, float* pos4, float* force_energy4, const int* type_ids,
+                   uint64_t step, const mb2_step_params* params, void* stream);
+/* num_steps steps from first_step: rebuilds run eagerly at scheduled steps;
+ * every step's force-and-integrate body is one replay of a CUDA graph
+ * captured on first use (re-captured when a buffer or parameter changes). */
+MB2_API int mb2_batch_run(mb2_batch* b, float* pos4, float* force_energy4, const int* type_ids,
+                  uint64_t first_step, uint32_t num_steps, const mb2_step_params* params,
+                  void* stream);
+/* Tuning knobs: cell level relative to the cost model's choice (-3..3) and
+ * lanes per pairlist row (0 = automatic, 4, 8, 16, 32). Invalidates the list. */
+MB2_API int mb2_batch_set_tuning(mb2_batch* b, int level_offset, int lanes);
+MB2_API int mb2_batch_tuning(const mb2_batch* b, int* level_offset, int* lanes,
+                     uint32_t* total_cells);
+/* Autotuner: times one pairlist build and `trial_steps` steps for each cell
+ * level offset in {-1, 0, +1} and lanes per row in {4, 8, 16} on a copy of
+ * the positions, keeps the pair minimising build / rebuild_period + step, and
+ * measures, from a fresh list, the largest rebuild cadence (<= the period)
+ * whose maximum displacement stays within half the skin. Positions are not
+ * changed; the next step rebuilds the list with the chosen knobs. */
+typedef struct {
+    int level_offset;                  /* chosen cell level offset */
+    int lanes;                         /* chosen lanes per row */
+    float build_ms;                    /* pairlist build time with the choice */
+    float step_ms;                     /* force-and-integrate time per step */
+    uint32_t safe_rebuild_period;      /* largest cadence keeping the list exact */
+    float max_displacement_at_period;  /* largest displacement after rebuild_period steps (A) */
+    uint32_t total_cells;
+} mb2_batch_tuning_result;
+MB2_API int mb2_batch_autotune(mb2_batch* b, const float* pos4, const int* type_ids,
+                       const mb2_step_params* params, uint32_t trial_steps, void* stream,
+                       mb2_batch_tuning_result* out);
+
 #ifdef __cplusplus
 }
 #endif

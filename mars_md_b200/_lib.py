@@ -33,6 +33,13 @@ class StepParams(C.Structure):
                 ("angle_table_idx", C.c_void_p), ("num_angles", C.c_uint32)]
 
 
+class BatchTuning(C.Structure):
+    """mb2_batch_tuning_result."""
+    _fields_ = [("level_offset", C.c_int), ("lanes", C.c_int), ("build_ms", C.c_float),
+                ("step_ms", C.c_float), ("safe_rebuild_period", C.c_uint32),
+                ("max_displacement_at_period", C.c_float), ("total_cells", C.c_uint32)]
+
+
 _lib = None
 
 
@@ -85,5 +92,20 @@ def load(path: str = LIB_PATH):
     L.mb2_profile_read.argtypes = [vp, i, C.POINTER(C.c_double), u32p]
     L.mb2_launch_count.restype = u64
     L.mb2_launch_count.argtypes = []
+    L.mb2_batch_create.argtypes = [i, u32, u32p, fp, fp, C.POINTER(vp)]
+    L.mb2_batch_destroy.argtypes = [vp]
+    L.mb2_batch_last_error.restype = C.c_char_p
+    L.mb2_batch_last_error.argtypes = [vp]
+    L.mb2_batch_set_pair_tables.argtypes = [vp, i, u32p, i, fp, u32p, fp, fp]
+    L.mb2_batch_set_particle_types.argtypes = [vp, i, fp, fp]
+    L.mb2_batch_build.argtypes = [vp, vp, vp, f, vp, u64p]
+    L.mb2_batch_num_pairs.argtypes = [vp, u64p]
+    L.mb2_batch_export_pairs.argtypes = [vp, vp, u64, vp]
+    L.mb2_batch_step.argtypes = [vp, vp, vp, vp, u64, C.POINTER(StepParams), vp]
+    L.mb2_batch_run.argtypes = [vp, vp, vp, vp, u64, u32, C.POINTER(StepParams), vp]
+    L.mb2_batch_set_tuning.argtypes = [vp, i, i]
+    L.mb2_batch_tuning.argtypes = [vp, ip, ip, u32p]
+    L.mb2_batch_autotune.argtypes = [vp, vp, vp, C.POINTER(StepParams), u32, vp,
+                                     C.POINTER(BatchTuning)]
     _lib = L
     return L

@@ -537,42 +537,12 @@ int mb2_set_pair_tables(mb2_context* ctx, int num_types, const uint32_t* term_ma
 			require(!(tag & kTermTabulated) || static_cast<int>(tag >> kTableShift) < num_tables,
 					MB2_ERR_ARG, "mb2_set_pair_tables: tag names a missing table");
 		}
-		// Per-bin force and energy, rounded exactly as TabulatedPotential::compute
-		// rounds them (TabulatedPotential.h:41-51): dU = U[k+1] - U[k] and
-		// F = -dU * step_inv in float; the last bin is the home >= size-1 case.
-		std::vector<uint32_t> offset(num_tables);
-		size_t total = 0;
-		for (int k = 0; k < num_tables; ++k) {
-			require(sizes[k] >= 2, MB2_ERR_ARG, "mb2_set_pair_tables: a table needs 2 values");
-			offset[k] = static_cast<uint32_t>(total);
-			total += sizes[k];
-		}
-		std::vector<float> bf(std::max<size_t>(total, 1));
-		std::vector<float2> be(std::max<size_t>(total, 1));
-		for (int k = 0; k < num_tables; ++k) {
-			const float* u = values + offset[k];
-			const uint32_t sz = sizes[k];
-			for (uint32_t b = 0; b + 1 < sz; ++b) {
-				volatile float du = u[b + 1] - u[b];
-				volatile float f = -du * step_invs[k];
-				bf[offset[k] + b] = f;
-				be[offset[k] + b] = make_float2(u[b], du);
-			}
-			bf[offset[k] + sz - 1] = 0.0f;
-			be[offset[k] + sz - 1] = make_float2(u[sz - 1], 0.0f);
-		}
+		std::vector<PairTableRef> refs;
+		std::vector<float> bf;
+		std::vector<float2> be;
+		const size_t total = pair_table_arrays(num_types, term_matrix, num_tables, values, sizes,
+											   starts, step_invs, refs, bf, be);
 		const int tt = num_types * num_types;
-		std::vector<PairTableRef> refs(tt);
-		for (int k = 0; k < tt; ++k) {
-			const uint32_t tag = term_matrix[k];
-			if (tag & kTermTabulated) {
-				const int t = static_cast<int>(tag >> kTableShift);
-				refs[k] = PairTableRef{starts[t], step_invs[t], static_cast<int>(sizes[t]) - 1,
-									   static_cast<int>(offset[t])};
-			} else {
-				refs[k] = PairTableRef{0.0f, 0.0f, 0, -1};
-			}
-		}
 		const size_t smem = static_cast<size_t>(tt) * sizeof(PairTableRef) + total * 12 + 8;
 		require(smem <= 200 * 1024, MB2_ERR_CAPACITY,
 				"mb2_set_pair_tables: tables exceed the 200 KB shared-memory budget");

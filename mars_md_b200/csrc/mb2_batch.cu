@@ -1,0 +1,836 @@
+// Batched replicas: many independent periodic systems of uneven size stepped
+// together, one launch per stage for all of them.
+//
+// Layout. Systems are concatenated in the caller's arrays (system s owns
+// particles [offset[s], offset[s+1])). The sort key of a particle is
+// (s << 21) | (21-bit Morton code of its position in its own box), so one
+// radix sort groups the systems and orders each one spatially; cells of
+// system s are the top 3 m_s bits of its 21-bit code, stored after the cells
+// of systems < s. The pairlist is one sliced-ELL half list over all sorted
+// particles (a row's neighbours are always in its own system); a warp whose
+// 32 sorted particles straddle systems walks each system's lanes in turn.
+// Pair forces read each row's box from the system table; the integrator
+// gathers the pair force through the inverse permutation and keys its noise
+// exactly as a plain step of system s with seed (seed + s) would: Philox key
+// mixed from (seed + s, patch_id, step), counter = index within the system.
+//
+// mb2_batch_run captures the non-rebuild step (pack, clear, pair, integrate,
+// step counter) in a CUDA graph and replays it; pairlist rebuilds run eagerly
+// at the rebuild period (the list is re-sized from the walk's counts).
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "marsb200.h"
+#include "mb2_internal.cuh"
+
+using namespace mb2;
+
+namespace {
+
+constexpr int kSysShift = 21;   // key = system << 21 | 21-bit Morton code
+constexpr int kLocalBits = 7;   // Morton bits per axis inside a system
+constexpr uint32_t kLocalMask = (1u << kSysShift) - 1u;
+constexpr int kMaxLevel = kLocalBits;
+
+// Per-system cell grid and walk parameters (device copy per system).
+struct SysGrid {
+	WalkGrid wg;         // wg.shift = 3 * (7 - m)
+	uint32_t cell_base;  // first global cell of the system
+	uint32_t pad[3];
+};
+
+__device__ __forceinline__ uint32_t morton7(float x, float o, float scale) {
+	const float t = __fmul_rn(__fsub_rn(x, o), scale);
+	const int q = static_cast<int>(floorf(t));
+	return static_cast<uint32_t>(min(max(q, 0), (1 << kLocalBits) - 1));
+}
+
+__global__ void __launch_bounds__(256) batch_encode_kernel(const float4* __restrict__ pos,
+														   const uint32_t* __restrict__ sys_of,
+														   const Box* __restrict__ boxes,
+														   uint32_t n, uint32_t* __restrict__ keys,
+														   uint32_t* __restrict__ idx) {
+	const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+	if (i >= n) return;
+	const uint32_t s = sys_of[i];
+	const Box& b = boxes[s];
+	const float4 p = pos[i];
+	const float k = static_cast<float>(1 << kLocalBits);
+	const uint32_t x = morton7(p.x, b.origin[0], __fmul_rn(k, b.inv[0]));
+	const uint32_t y = morton7(p.y, b.origin[1], __fmul_rn(k, b.inv[1]));
+	const uint32_t z = morton7(p.z, b.origin[2], __fmul_rn(k, b.inv[2]));
+	keys[i] = (s << kSysShift) | split_by3(z) | (split_by3(y) << 1) | (split_by3(x) << 2);
+	idx[i] = i;
+}
+
+__global__ void __launch_bounds__(256) batch_cell_ranges_kernel(const uint32_t* __restrict__ keys,
+																uint32_t n,
+																const SysGrid* __restrict__ grids,
+																uint32_t* __restrict__ begin,
+																uint32_t* __restrict__ end) {
+	const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+	if (i >= n) return;
+	auto cell = [&](uint32_t key) {
+		const SysGrid& g = grids[key >> kSysShift];
+		return g.cell_base + ((key & kLocalMask) >> g.wg.shift);
+	};
+	const uint32_t c = cell(keys[i]);
+	if (i == 0 || cell(keys[i - 1]) != c) begin[c] = i;
+	if (i + 1 == n || cell(keys[i + 1]) != c) end[c] = i + 1;
+}
+
+__device__ __forceinline__ int wmin_i(int v) {
+#pragma unroll
+	for (int o = 16; o > 0; o >>= 1) v = min(v, __shfl_xor_sync(0xFFFFFFFFu, v, o));
+	return v;
+}
+__device__ __forceinline__ int wmax_i(int v) {
+#pragma unroll
+	for (int o = 16; o > 0; o >>= 1) v = max(v, __shfl_xor_sync(0xFFFFFFFFu, v, o));
+	return v;
+}
+
+__device__ __forceinline__ bool exact_hit_b(const Box& box, const float4& pi, const float4& pj,
+											float rc2) {
+	const float3 d = wrap_diff(box, __fsub_rn(pj.x, pi.x), __fsub_rn(pj.y, pi.y),
+							   __fsub_rn(pj.z, pi.z));
+	return len2(d.x, d.y, d.z) <= rc2;
+}
+
+// One warp per 32 consecutive sorted particles; the lanes of each system
+// present in the warp walk the cells around their cell box together (the
+// walk over a wide box is a superset of every lane's stencil, so the pair set
+// is exact either way). Rows are appended in candidate order.
+__global__ void __launch_bounds__(256) batch_walk_kernel(
+	const float4* __restrict__ sorted_pos, const uint32_t* __restrict__ keys,
+	const uint32_t* __restrict__ s2o, const uint32_t* __restrict__ begin,
+	const uint32_t* __restrict__ end, const SysGrid* __restrict__ grids,
+	const Box* __restrict__ boxes, uint32_t n, uint32_t* __restrict__ nbr, uint32_t cap,
+	int hshift, uint32_t* __restrict__ row_len, unsigned long long* __restrict__ stats) {
+	__shared__ uint32_t split_tab[1 << kLocalBits];
+	for (int k = threadIdx.x; k < (1 << kLocalBits); k += blockDim.x) split_tab[k] = split_by3(k);
+	__syncthreads();
+	const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+	const int lane = threadIdx.x & 31;
+	if ((i & ~31u) >= n) return;  // whole warp past the end
+	const bool valid = i < n;
+	const int h = 1 << hshift;
+	const float4 pi = valid ? sorted_pos[i] : make_float4(0.f, 0.f, 0.f, 0.f);
+	const uint32_t key = valid ? keys[i] : 0u;
+	const uint32_t sys = key >> kSysShift;
+	const int a = valid ? static_cast<int>(s2o[i]) : 0;
+	uint32_t* base = nbr + (static_cast<size_t>(i >> hshift) * cap << hshift) + (i & (h - 1));
+	uint32_t len = 0;
+	uint32_t remaining = __ballot_sync(0xFFFFFFFFu, valid);
+	while (remaining) {
+		const int leader = __ffs(remaining) - 1;
+		const uint32_t s0 = __shfl_sync(0xFFFFFFFFu, sys, leader);
+		const bool active = valid && sys == s0;
+		remaining &= ~__ballot_sync(0xFFFFFFFFu, active);
+		const SysGrid& g = grids[s0];
+		const WalkGrid& wg = g.wg;
+		const Box& box = boxes[s0];
+		const uint32_t c = (key & kLocalMask) >> wg.shift;
+		const int cx = static_cast<int>(compact_by3(c >> 2));
+		const int cy = static_cast<int>(compact_by3(c >> 1));
+		const int cz = static_cast<int>(compact_by3(c));
+		const int x0 = wmin_i(active ? cx : INT_MAX), x1 = wmax_i(active ? cx : INT_MIN);
+		const int y0 = wmin_i(active ? cy : INT_MAX), y1 = wmax_i(active ? cy : INT_MIN);
+		const int z0 = wmin_i(active ? cz : INT_MAX), z1 = wmax_i(active ? cz : INT_MIN);
+		const uint32_t c_first = __shfl_sync(0xFFFFFFFFu, c, leader);
+		const uint32_t i_first = __shfl_sync(0xFFFFFFFFu, i, leader);
+		const int cells = 1 << wg.m;
+		const int lo[3] = {x0, y0, z0}, hi[3] = {x1, y1, z1};
+		int from[3], to[3];
+		bool full[3];
+#pragma unroll
+		for (int ax = 0; ax < 3; ++ax) {
+			// Every batched box is periodic on every axis.
+			full[ax] = hi[ax] - lo[ax] + 2 * wg.radius[ax] + 1 >= cells;
+			from[ax] = full[ax] ? 0 : lo[ax] - wg.radius[ax];
+			to[ax] = full[ax] ? cells - 1 : hi[ax] + wg.radius[ax];
+		}
+		const uint32_t* cb = begin + g.cell_base;
+		const uint32_t* ce = end + g.cell_base;
+		for (int ux = from[0]; ux <= to[0]; ++ux) {
+			int nx = ux;
+			float shx = 0.0f, gx = 0.0f;
+			if (!full[0]) {
+				const int gc = ux < x0 ? x0 - ux - 1 : (ux > x1 ? ux - x1 - 1 : 0);
+				gx = static_cast<float>(gc) * wg.wmin[0];
+				if (ux < 0) { nx = ux + cells; shx = -box.size[0]; }
+				else if (ux >= cells) { nx = ux - cells; shx = box.size[0]; }
+			}
+			const float gx2 = gx * gx;
+			if (gx2 > wg.lim) continue;
+			for (int uy = from[1]; uy <= to[1]; ++uy) {
+				int ny = uy;
+				float shy = 0.0f, gy = 0.0f;
+				if (!full[1]) {
+					const int gc = uy < y0 ? y0 - uy - 1 : (uy > y1 ? uy - y1 - 1 : 0);
+					gy = static_cast<float>(gc) * wg.wmin[1];
+					if (uy < 0) { ny = uy + cells; shy = -box.size[1]; }
+					else if (uy >= cells) { ny = uy - cells; shy = box.size[1]; }
+				}
+				const float gxy2 = gx2 + gy * gy;
+				if (gxy2 > wg.lim) continue;
+				for (int uz = from[2]; uz <= to[2]; ++uz) {
+					int nz = uz;
+					float shz = 0.0f, gz = 0.0f;
+					if (!full[2]) {
+						const int gc = uz < z0 ? z0 - uz - 1 : (uz > z1 ? uz - z1 - 1 : 0);
+						gz = static_cast<float>(gc) * wg.wmin[2];
+						if (uz < 0) { nz = uz + cells; shz = -box.size[2]; }
+						else if (uz >= cells) { nz = uz - cells; shz = box.size[2]; }
+					}
+					if (gxy2 + gz * gz > wg.lim) continue;
+					const uint32_t nc =
+						(split_tab[nx] << 2) | (split_tab[ny] << 1) | split_tab[nz];
+					if (nc < c_first) continue;
+					const uint32_t b = cb[nc], e = ce[nc];
+					const uint32_t jlo = b > i_first + 1u ? b : i_first + 1u;
+					if (jlo >= e) continue;
+					const float qx = pi.x - shx, qy = pi.y - shy, qz = pi.z - shz;
+					for (uint32_t j = jlo; j < e; ++j) {
+						const float4 pj = sorted_pos[j];
+						if (!active || j <= i) continue;
+						float dx = pj.x - qx, dy = pj.y - qy, dz = pj.z - qz;
+						if (full[0]) dx -= box.size[0] * rintf(dx * box.inv[0]);
+						if (full[1]) dy -= box.size[1] * rintf(dy * box.inv[1]);
+						if (full[2]) dz -= box.size[2] * rintf(dz * box.inv[2]);
+						const float d2 = dx * dx + dy * dy + dz * dz;
+						bool hit = d2 < wg.fast_lo;
+						if (!hit && d2 <= wg.fast_hi) hit = exact_hit_b(box, pi, pj, wg.rc2);
+						if (hit) {
+							const int bj = static_cast<int>(s2o[j]);
+							if (len < cap)
+								base[static_cast<size_t>(len) * h] = j | (bj < a ? kOrientBit : 0u);
+							++len;
+						}
+					}
+				}
+			}
+		}
+	}
+	unsigned long long tot = valid ? len : 0u;
+	int mx = valid ? static_cast<int>(min(len, 0x7FFFFFFFu)) : 0;
+	if (valid) row_len[i] = len;
+#pragma unroll
+	for (int o = 16; o > 0; o >>= 1) {
+		tot += __shfl_xor_sync(0xFFFFFFFFu, tot, o);
+		mx = max(mx, __shfl_xor_sync(0xFFFFFFFFu, mx, o));
+	}
+	if (lane == 0) {
+		atomicAdd(stats, tot);
+		atomicMax(stats + 1, static_cast<unsigned long long>(mx));
+	}
+}
+
+__global__ void __launch_bounds__(256) batch_displacement_kernel(
+	const float4* __restrict__ cur, const float4* __restrict__ prev,
+	const uint32_t* __restrict__ sys_of, const Box* __restrict__ boxes, uint32_t n,
+	unsigned int* __restrict__ out) {
+	const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+	float d2 = 0.0f;
+	if (i < n) {
+		const Box& b = boxes[sys_of[i]];
+		const float4 c = cur[i], p = prev[i];
+		const float3 d = wrap_diff(b, __fsub_rn(c.x, p.x), __fsub_rn(c.y, p.y), __fsub_rn(c.z, p.z));
+		d2 = len2(d.x, d.y, d.z);
+	}
+#pragma unroll
+	for (int o = 16; o > 0; o >>= 1) d2 = fmaxf(d2, __shfl_xor_sync(0xFFFFFFFFu, d2, o));
+	if ((threadIdx.x & 31) == 0) atomicMax(out, __float_as_uint(d2));
+}
+
+}  // namespace
+
+struct mb2_batch {
+	int device = 0;
+	std::string last_error;
+	uint32_t num_systems = 0;
+	uint32_t n = 0;
+	std::vector<uint32_t> offsets;  // host [S + 1]
+	std::vector<Box> boxes_h;
+	DevBuf<uint32_t> offsets_d, sys_of;
+	DevBuf<Box> boxes;
+	Scratch scratch;
+	// sort / list state
+	DevBuf<uint32_t> keys, s2o, inv, row_len, row_off, nbr, cell_begin, cell_end;
+	DevBuf<float4> sorted_pos, ref_pos, force_sorted;
+	DevBuf<SysGrid> grids;
+	std::vector<SysGrid> grids_h;
+	uint32_t total_cells = 0;
+	float grid_rc = -1.0f;
+	int level_offset = 0;
+	DevBuf<unsigned long long> stats, step_d;
+	DevBuf<unsigned int> disp;
+	DevBuf<double> energy;
+	unsigned long long* pinned = nullptr;
+	bool built = false;
+	uint64_t num_pairs = 0;
+	uint32_t cap = 0;
+	int lanes = 0;
+	int lanes_request = 0;
+	// tables and types
+	PairTables pt;
+	DevBuf<PairTableRef> refs;
+	DevBuf<float> bin_force;
+	DevBuf<float2> bin_energy;
+	TypeTable types;
+	bool types_set = false;
+	DevBuf<float> charge;
+	DevBuf<float4> diffusion, fg_scale;
+	DevBuf<int> pmf_off, pmf_cnt;
+	DevBuf<int4> fg_id;
+	// captured step
+	cudaGraphExec_t graph = nullptr;
+	std::vector<uint64_t> graph_key;
+	unsigned long long launches_per_graph = 0;
+
+	~mb2_batch() {
+		if (graph) cudaGraphExecDestroy(graph);
+		if (pinned) cudaFreeHost(pinned);
+	}
+};
+
+namespace {
+
+template <typename F>
+int bguard(mb2_batch* b, F&& f) {
+	if (!b) return MB2_ERR_ARG;
+	try {
+		MB2_CUDA(cudaSetDevice(b->device));
+		f();
+		MB2_CUDA(cudaGetLastError());
+		b->last_error.clear();
+		return MB2_OK;
+	} catch (const Error& e) {
+		b->last_error = e.msg;
+		return e.code;
+	} catch (const std::exception& e) {
+		b->last_error = e.what();
+		return MB2_ERR_CUDA;
+	}
+}
+
+cudaStream_t S(void* s) { return reinterpret_cast<cudaStream_t>(s); }
+
+uint64_t f2u(float f) {
+	uint32_t u;
+	std::memcpy(&u, &f, 4);
+	return u;
+}
+
+// Per-system cell grids for list radius rc: the cost-model level (capped at
+// the 7-bit Morton scale) shifted by the tuner's level offset.
+void choose_grids(mb2_batch* b, float rc) {
+	b->grids_h.resize(b->num_systems);
+	uint32_t base = 0;
+	for (uint32_t s = 0; s < b->num_systems; ++s) {
+		const Box& bx = b->boxes_h[s];
+		const uint32_t ns = b->offsets[s + 1] - b->offsets[s];
+		const CellGrid g0 = choose_cell_grid(bx.size, bx.periodic, rc, ns, 0, kMaxLevel);
+		const int m = std::min(std::max(g0.m + b->level_offset, 0), kMaxLevel);
+		const CellGrid g = (m == g0.m) ? g0 : choose_cell_grid(bx.size, bx.periodic, rc, ns, m, m);
+		SysGrid sg{};
+		WalkGrid& wg = sg.wg;
+		wg.m = g.m;
+		wg.shift = 3 * (kLocalBits - g.m);
+		wg.emax = 3;
+		for (int a = 0; a < 3; ++a) {
+			wg.radius[a] = g.radius[a];
+			wg.wmin[a] = g.wmin[a];
+			wg.full[a] = g.m == 0 || 2 * g.radius[a] + 1 >= (1 << g.m);
+		}
+		wg.lim = g.lim;
+		wg.rc2 = rc * rc;
+		fast_test_band(bx, rc, &wg.fast_lo, &wg.fast_hi);
+		sg.cell_base = base;
+		base += 1u << (3 * g.m);
+		b->grids_h[s] = sg;
+	}
+	b->total_cells = base;
+	b->grids.ensure(b->num_systems);
+	MB2_CUDA(cudaMemcpy(b->grids.ptr, b->grids_h.data(), b->num_systems * sizeof(SysGrid),
+						cudaMemcpyHostToDevice));
+	b->grid_rc = rc;
+}
+
+void batch_build(mb2_batch* b, const float4* pos, const int* type_ids, float rc, cudaStream_t st) {
+	expect_arg(rc > 0.0f && std::isfinite(rc), MB2_ERR_ARG,
+			   "mb2_batch_build: pairlist cutoff must be positive and finite");
+	for (uint32_t s = 0; s < b->num_systems; ++s)
+		for (int a = 0; a < 3; ++a)
+			expect_arg(2.0f * rc < b->boxes_h[s].size[a], MB2_ERR_ARG,
+					   "mb2_batch_build: every box edge must exceed twice the list radius");
+	const uint32_t n = b->n;
+	if (b->grid_rc != rc) choose_grids(b, rc);
+	b->keys.ensure(n);
+	b->s2o.ensure(n);
+	b->inv.ensure(n);
+	b->sorted_pos.ensure(n);
+	if (n)
+		MB2_LAUNCH batch_encode_kernel<<<(n + 255) / 256, 256, 0, st>>>(
+			pos, b->sys_of.ptr, b->boxes.ptr, n, b->keys.ptr, b->s2o.ptr);
+	radix_sort_pairs(b->scratch, b->keys.ptr, b->s2o.ptr, n, st);
+	inverse_and_gather(b->s2o.ptr, n, pos, b->inv.ptr, nullptr, st);
+	pack_sorted_positions(pos, type_ids, b->s2o.ptr, n, b->sorted_pos.ptr, st);
+	b->cell_begin.ensure(b->total_cells);
+	b->cell_end.ensure(b->total_cells);
+	MB2_CUDA(cudaMemsetAsync(b->cell_begin.ptr, 0, b->total_cells * sizeof(uint32_t), st));
+	MB2_CUDA(cudaMemsetAsync(b->cell_end.ptr, 0, b->total_cells * sizeof(uint32_t), st));
+	if (n)
+		MB2_LAUNCH batch_cell_ranges_kernel<<<(n + 255) / 256, 256, 0, st>>>(
+			b->keys.ptr, n, b->grids.ptr, b->cell_begin.ptr, b->cell_end.ptr);
+	b->row_len.ensure(n);
+	b->stats.ensure(2);
+	auto walk = [&](uint32_t cap) {
+		MB2_CUDA(cudaMemsetAsync(b->stats.ptr, 0, 2 * sizeof(unsigned long long), st));
+		if (n) {
+			const int hshift = __builtin_ctz(32 / b->lanes);
+			MB2_LAUNCH batch_walk_kernel<<<(n + 255) / 256, 256, 0, st>>>(
+				b->sorted_pos.ptr, b->keys.ptr, b->s2o.ptr, b->cell_begin.ptr, b->cell_end.ptr,
+				b->grids.ptr, b->boxes.ptr, n, b->nbr.ptr, cap, hshift, b->row_len.ptr,
+				b->stats.ptr);
+		}
+		MB2_CUDA(cudaMemcpyAsync(b->pinned, b->stats.ptr, 2 * sizeof(unsigned long long),
+								 cudaMemcpyDeviceToHost, st));
+		MB2_CUDA(cudaStreamSynchronize(st));
+		return std::make_pair(b->pinned[0], b->pinned[1]);
+	};
+	auto size_list = [&](uint64_t max_row) {
+		const uint32_t G = static_cast<uint32_t>(b->lanes);
+		uint64_t cap = max_row + max_row / 4 + G;
+		cap = (cap + G - 1) / G * G;
+		expect_arg(cap < 65536u, MB2_ERR_CAPACITY,
+				   "mb2_batch_build: a particle has more than ~52000 list neighbours");
+		b->cap = static_cast<uint32_t>(cap);
+	};
+	auto ensure_list = [&]() {
+		const size_t hgt = static_cast<size_t>(32 / b->lanes);
+		b->nbr.ensure(std::max<size_t>((n + hgt - 1) / hgt * b->cap * hgt, 1));
+	};
+	if (b->cap == 0 || b->lanes == 0) {
+		// First build: count rows without storing (cap 0 writes nothing), to size the list.
+		b->lanes = 4;
+		const auto counted = walk(0u);
+		const double mean = n ? static_cast<double>(counted.first) / n : 0.0;
+		b->lanes = b->lanes_request ? b->lanes_request
+									: (mean >= 256.0 ? 16 : (mean >= 48.0 ? 8 : 4));
+		size_list(counted.second);
+	}
+	ensure_list();
+	auto stats = walk(b->cap);
+	if (stats.second > b->cap) {
+		size_list(stats.second);
+		ensure_list();
+		stats = walk(b->cap);
+	}
+	b->ref_pos.ensure(n);
+	if (n)
+		MB2_CUDA(cudaMemcpyAsync(b->ref_pos.ptr, pos, static_cast<size_t>(n) * sizeof(float4),
+								 cudaMemcpyDeviceToDevice, st));
+	b->num_pairs = stats.first;
+	b->built = true;
+}
+
+// Largest displacement (over all systems) since the last build; synchronises.
+float batch_max_disp(mb2_batch* b, const float4* pos, cudaStream_t st) {
+	b->disp.ensure(1);
+	MB2_CUDA(cudaMemsetAsync(b->disp.ptr, 0, sizeof(unsigned int), st));
+	if (b->n)
+		MB2_LAUNCH batch_displacement_kernel<<<(b->n + 255) / 256, 256, 0, st>>>(
+			pos, b->ref_pos.ptr, b->sys_of.ptr, b->boxes.ptr, b->n, b->disp.ptr);
+	MB2_CUDA(cudaMemcpyAsync(b->pinned, b->disp.ptr, sizeof(unsigned int), cudaMemcpyDeviceToHost,
+							 st));
+	MB2_CUDA(cudaStreamSynchronize(st));
+	float d2;
+	std::memcpy(&d2, b->pinned, 4);
+	return std::sqrt(d2);
+}
+
+// The per-step work after any rebuild: pack, clear, pair forces, integrate,
+// advance the device step counter.
+void step_body(mb2_batch* b, float4* pos, float4* fe, const int* type_ids,
+			   const mb2_step_params* prm, cudaStream_t st) {
+	const uint32_t n = b->n;
+	if (n == 0) return;
+	pack_sorted_positions(pos, type_ids, b->s2o.ptr, n, b->sorted_pos.ptr, st);
+	MB2_CUDA(cudaMemsetAsync(b->force_sorted.ptr, 0, static_cast<size_t>(n) * sizeof(float4), st));
+	const float cutoff_sq = prm->cutoff > 0.0f ? prm->cutoff * prm->cutoff : 0.0f;
+	pair_forces_systems(b->sorted_pos.ptr, b->nbr.ptr, b->row_len.ptr, n, b->cap, b->lanes, b->pt,
+						b->boxes.ptr, b->keys.ptr, kSysShift, true, cutoff_sq, 0,
+						b->force_sorted.ptr, b->energy.ptr, st);
+	bd_integrate_systems(pos, fe, b->force_sorted.ptr, b->inv.ptr, type_ids, b->sys_of.ptr,
+						 b->offsets_d.ptr, b->boxes.ptr, n, b->types, prm->dt, prm->kT, prm->seed,
+						 prm->patch_id, b->step_d.ptr, st);
+	step_counter_add(b->step_d.ptr, 1, st);
+}
+
+void check_step_args(mb2_batch* b, const float* pos4, const float* fe4, const int* type_ids,
+					 const mb2_step_params* prm) {
+	expect_arg(prm && (b->n == 0 || (pos4 && fe4 && type_ids)), MB2_ERR_ARG,
+			   "mb2_batch_step: null argument");
+	expect_arg(b->types_set, MB2_ERR_STATE, "mb2_batch_step: call mb2_batch_set_particle_types");
+	expect_arg(b->pt.num_types > 0, MB2_ERR_STATE,
+			   "mb2_batch_step: call mb2_batch_set_pair_tables");
+	expect_arg(prm->num_bonds == 0 && prm->num_angles == 0, MB2_ERR_ARG,
+			   "mb2_batch_step: bonded terms are not supported in batched mode");
+}
+
+// Rebuild decision of the reference (Patch.cpp:86-108), over all systems: at
+// the first step and at each rebuild period, rebuild when any system moved
+// more than half the skin since the last build.
+void maybe_rebuild(mb2_batch* b, const float4* pos, const int* type_ids, uint64_t step,
+				   const mb2_step_params* prm, cudaStream_t st) {
+	const bool at_period = prm->rebuild_period == 0 || (step - 1) % prm->rebuild_period == 0;
+	bool rebuild = at_period || !b->built;
+	const float skin = prm->pairlist_cutoff - prm->cutoff;
+	if (rebuild && b->built && prm->rebuild_period != 0 && skin > 0.0f)
+		rebuild = batch_max_disp(b, pos, st) > skin * 0.5f;
+	if (rebuild) batch_build(b, pos, type_ids, prm->pairlist_cutoff, st);
+	b->force_sorted.ensure(b->n);
+}
+
+void reset_tuning(mb2_batch* b, int level_offset, int lanes) {
+	if (level_offset != b->level_offset) b->grid_rc = -1.0f;
+	b->level_offset = level_offset;
+	b->lanes_request = lanes;
+	b->cap = 0;
+	b->lanes = 0;
+	b->built = false;
+}
+
+}  // namespace
+
+extern "C" {
+
+int mb2_batch_create(int device, uint32_t num_systems, const uint32_t* counts,
+					 const float* box_origin3, const float* box_size3, mb2_batch** out) {
+	if (!out || !counts || !box_size3 || num_systems == 0) return MB2_ERR_ARG;
+	*out = nullptr;
+	if (num_systems > (1u << (32 - kSysShift))) return MB2_ERR_CAPACITY;
+	mb2_batch* b = new mb2_batch();
+	b->device = device;
+	const int rc = bguard(b, [&] {
+		b->num_systems = num_systems;
+		b->offsets.assign(num_systems + 1, 0);
+		uint64_t total = 0;
+		for (uint32_t s = 0; s < num_systems; ++s) {
+			total += counts[s];
+			expect_arg(total < (1ull << 31), MB2_ERR_CAPACITY,
+					   "mb2_batch_create: too many particles");
+			b->offsets[s + 1] = static_cast<uint32_t>(total);
+		}
+		b->n = static_cast<uint32_t>(total);
+		b->boxes_h.resize(num_systems);
+		std::vector<uint32_t> sys_of(b->n);
+		for (uint32_t s = 0; s < num_systems; ++s) {
+			Box& bx = b->boxes_h[s];
+			for (int a = 0; a < 3; ++a) {
+				const float l = box_size3[3 * s + a];
+				expect_arg(l > 0.0f && std::isfinite(l), MB2_ERR_ARG,
+						   "mb2_batch_create: box edges must be positive");
+				bx.origin[a] = box_origin3 ? box_origin3[3 * s + a] : 0.0f;
+				bx.size[a] = l;
+				bx.inv[a] = 1.0f / l;
+				bx.half[a] = 0.5f * l;
+				bx.periodic[a] = 1;
+			}
+			for (uint32_t i = b->offsets[s]; i < b->offsets[s + 1]; ++i) sys_of[i] = s;
+		}
+		b->offsets_d.ensure(num_systems + 1);
+		b->boxes.ensure(num_systems);
+		b->sys_of.ensure(std::max<uint32_t>(b->n, 1));
+		MB2_CUDA(cudaMemcpy(b->offsets_d.ptr, b->offsets.data(), (num_systems + 1) * 4ull,
+							cudaMemcpyHostToDevice));
+		MB2_CUDA(cudaMemcpy(b->boxes.ptr, b->boxes_h.data(), num_systems * sizeof(Box),
+							cudaMemcpyHostToDevice));
+		if (b->n)
+			MB2_CUDA(cudaMemcpy(b->sys_of.ptr, sys_of.data(), b->n * 4ull, cudaMemcpyHostToDevice));
+		MB2_CUDA(cudaMallocHost(&b->pinned, 64));
+		b->step_d.ensure(1);
+		b->energy.ensure(4);
+		MB2_CUDA(cudaMemset(b->energy.ptr, 0, 4 * sizeof(double)));
+	});
+	if (rc != MB2_OK) {
+		delete b;
+		return rc;
+	}
+	*out = b;
+	return MB2_OK;
+}
+
+int mb2_batch_destroy(mb2_batch* b) {
+	if (!b) return MB2_ERR_ARG;
+	cudaSetDevice(b->device);
+	cudaDeviceSynchronize();
+	delete b;
+	return MB2_OK;
+}
+
+const char* mb2_batch_last_error(const mb2_batch* b) {
+	return b ? b->last_error.c_str() : "null batch";
+}
+
+int mb2_batch_set_pair_tables(mb2_batch* b, int num_types, const uint32_t* term_matrix,
+							  int num_tables, const float* values, const uint32_t* sizes,
+							  const float* starts, const float* step_invs) {
+	return bguard(b, [&] {
+		std::vector<PairTableRef> refs;
+		std::vector<float> bf;
+		std::vector<float2> be;
+		const size_t total = pair_table_arrays(num_types, term_matrix, num_tables, values, sizes,
+											   starts, step_invs, refs, bf, be);
+		const int tt = num_types * num_types;
+		expect_arg(tt * sizeof(PairTableRef) + total * 12 + 8 <= 200 * 1024, MB2_ERR_CAPACITY,
+				   "mb2_batch_set_pair_tables: tables exceed the 200 KB shared-memory budget");
+		b->refs.ensure(tt);
+		b->bin_force.ensure(bf.size());
+		b->bin_energy.ensure(be.size());
+		MB2_CUDA(cudaMemcpy(b->refs.ptr, refs.data(), tt * sizeof(PairTableRef),
+							cudaMemcpyHostToDevice));
+		MB2_CUDA(cudaMemcpy(b->bin_force.ptr, bf.data(), bf.size() * 4, cudaMemcpyHostToDevice));
+		MB2_CUDA(cudaMemcpy(b->bin_energy.ptr, be.data(), be.size() * 8, cudaMemcpyHostToDevice));
+		b->pt.num_types = num_types;
+		b->pt.total_bins = static_cast<uint32_t>(total);
+		b->pt.refs = b->refs.ptr;
+		b->pt.bin_force = b->bin_force.ptr;
+		b->pt.bin_energy = b->bin_energy.ptr;
+	});
+}
+
+int mb2_batch_set_particle_types(mb2_batch* b, int num_types, const float* charge,
+								 const float* diffusion3) {
+	return bguard(b, [&] {
+		expect_arg(num_types > 0 && charge && diffusion3, MB2_ERR_ARG,
+				   "mb2_batch_set_particle_types: bad arguments");
+		std::vector<float4> dif(num_types);
+		std::vector<int> zero(num_types, 0);
+		std::vector<int4> fg(num_types, make_int4(-1, -1, -1, -1));
+		std::vector<float4> fs(num_types, make_float4(0.f, 0.f, 0.f, 0.f));
+		for (int t = 0; t < num_types; ++t)
+			dif[t] = make_float4(diffusion3[3 * t], diffusion3[3 * t + 1], diffusion3[3 * t + 2],
+								 0.0f);
+		b->charge.ensure(num_types);
+		b->diffusion.ensure(num_types);
+		b->pmf_off.ensure(num_types);
+		b->pmf_cnt.ensure(num_types);
+		b->fg_id.ensure(num_types);
+		b->fg_scale.ensure(num_types);
+		MB2_CUDA(cudaMemcpy(b->charge.ptr, charge, num_types * 4ull, cudaMemcpyHostToDevice));
+		MB2_CUDA(cudaMemcpy(b->diffusion.ptr, dif.data(), num_types * 16ull, cudaMemcpyHostToDevice));
+		MB2_CUDA(cudaMemcpy(b->pmf_off.ptr, zero.data(), num_types * 4ull, cudaMemcpyHostToDevice));
+		MB2_CUDA(cudaMemcpy(b->pmf_cnt.ptr, zero.data(), num_types * 4ull, cudaMemcpyHostToDevice));
+		MB2_CUDA(cudaMemcpy(b->fg_id.ptr, fg.data(), num_types * 16ull, cudaMemcpyHostToDevice));
+		MB2_CUDA(cudaMemcpy(b->fg_scale.ptr, fs.data(), num_types * 16ull, cudaMemcpyHostToDevice));
+		TypeTable& ty = b->types;
+		ty.num_types = num_types;
+		ty.charge = b->charge.ptr;
+		ty.diffusion = b->diffusion.ptr;
+		ty.pmf_offset = b->pmf_off.ptr;
+		ty.pmf_count = b->pmf_cnt.ptr;
+		ty.terms = nullptr;
+		ty.force_grid_id = b->fg_id.ptr;
+		ty.force_grid_scale = b->fg_scale.ptr;
+		ty.grids = nullptr;
+		ty.num_grids = 0;
+		b->types_set = true;
+	});
+}
+
+int mb2_batch_build(mb2_batch* b, const float* pos4, const int* type_ids, float pairlist_cutoff,
+					void* stream, uint64_t* num_pairs) {
+	return bguard(b, [&] {
+		expect_arg(b->n == 0 || (pos4 && type_ids), MB2_ERR_ARG, "mb2_batch_build: null argument");
+		batch_build(b, reinterpret_cast<const float4*>(pos4), type_ids, pairlist_cutoff,
+					S(stream));
+		if (num_pairs) *num_pairs = b->num_pairs;
+	});
+}
+
+int mb2_batch_num_pairs(const mb2_batch* b, uint64_t* num_pairs) {
+	if (!b || !num_pairs) return MB2_ERR_ARG;
+	*num_pairs = b->built ? b->num_pairs : 0;
+	return MB2_OK;
+}
+
+int mb2_batch_export_pairs(mb2_batch* b, int* pairs2, uint64_t capacity, void* stream) {
+	return bguard(b, [&] {
+		expect_arg(b->built, MB2_ERR_STATE, "mb2_batch_export_pairs: no pairlist");
+		expect_arg(capacity >= b->num_pairs, MB2_ERR_CAPACITY,
+				   "mb2_batch_export_pairs: output smaller than the pair count");
+		expect_arg(b->num_pairs == 0 || pairs2, MB2_ERR_ARG, "mb2_batch_export_pairs: null output");
+		b->row_off.ensure(b->n);
+		exclusive_scan_u32(b->scratch, b->row_len.ptr, b->row_off.ptr, b->n, nullptr, S(stream));
+		export_pairs(b->nbr.ptr, b->row_len.ptr, b->row_off.ptr, b->s2o.ptr, b->n, b->cap,
+					 __builtin_ctz(32 / b->lanes), reinterpret_cast<int2*>(pairs2), S(stream));
+	});
+}
+
+int mb2_batch_step(mb2_batch* b, float* pos4, float* force_energy4, const int* type_ids,
+				   uint64_t step, const mb2_step_params* prm, void* stream) {
+	return bguard(b, [&] {
+		check_step_args(b, pos4, force_energy4, type_ids, prm);
+		const cudaStream_t st = S(stream);
+		float4* pos = reinterpret_cast<float4*>(pos4);
+		maybe_rebuild(b, pos, type_ids, step, prm, st);
+		step_counter_set(b->step_d.ptr, step, st);
+		step_body(b, pos, reinterpret_cast<float4*>(force_energy4), type_ids, prm, st);
+	});
+}
+
+int mb2_batch_run(mb2_batch* b, float* pos4, float* force_energy4, const int* type_ids,
+				  uint64_t first_step, uint32_t num_steps, const mb2_step_params* prm,
+				  void* stream) {
+	return bguard(b, [&] {
+		check_step_args(b, pos4, force_energy4, type_ids, prm);
+		const cudaStream_t st = S(stream);
+		float4* pos = reinterpret_cast<float4*>(pos4);
+		float4* fe = reinterpret_cast<float4*>(force_energy4);
+		for (uint32_t k = 0; k < num_steps; ++k) {
+			const uint64_t step = first_step + k;
+			maybe_rebuild(b, pos, type_ids, step, prm, st);
+			// The graph bakes in every pointer and size of the step body.
+			const std::vector<uint64_t> key = {
+				reinterpret_cast<uint64_t>(pos), reinterpret_cast<uint64_t>(fe),
+				reinterpret_cast<uint64_t>(type_ids), reinterpret_cast<uint64_t>(b->nbr.ptr),
+				reinterpret_cast<uint64_t>(b->force_sorted.ptr), b->cap,
+				static_cast<uint64_t>(b->lanes), b->n, f2u(prm->cutoff), f2u(prm->dt),
+				f2u(prm->kT), prm->seed, prm->patch_id};
+			if (!b->graph || key != b->graph_key) {
+				if (b->graph) {
+					MB2_CUDA(cudaGraphExecDestroy(b->graph));
+					b->graph = nullptr;
+				}
+				cudaStream_t cs;
+				MB2_CUDA(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
+				cudaGraph_t g = nullptr;
+				const unsigned long long l0 = g_launches;
+				MB2_CUDA(cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal));
+				step_body(b, pos, fe, type_ids, prm, cs);
+				const cudaError_t ec = cudaStreamEndCapture(cs, &g);
+				b->launches_per_graph = g_launches - l0;
+				g_launches = l0;  // counted at each replay instead
+				cudaStreamDestroy(cs);
+				MB2_CUDA(ec);
+				const cudaError_t ei = cudaGraphInstantiate(&b->graph, g, 0);
+				cudaGraphDestroy(g);
+				MB2_CUDA(ei);
+				b->graph_key = key;
+			}
+			// Each replay advances the device step counter by one.
+			if (k == 0) step_counter_set(b->step_d.ptr, step, st);
+			MB2_CUDA(cudaGraphLaunch(b->graph, st));
+			g_launches += b->launches_per_graph;
+		}
+	});
+}
+
+int mb2_batch_set_tuning(mb2_batch* b, int level_offset, int lanes) {
+	return bguard(b, [&] {
+		expect_arg(level_offset >= -3 && level_offset <= 3, MB2_ERR_ARG,
+				   "mb2_batch_set_tuning: level offset in [-3, 3]");
+		expect_arg(lanes == 0 || lanes == 4 || lanes == 8 || lanes == 16 || lanes == 32,
+				   MB2_ERR_ARG, "mb2_batch_set_tuning: lanes 0, 4, 8, 16 or 32");
+		reset_tuning(b, level_offset, lanes);
+	});
+}
+
+int mb2_batch_tuning(const mb2_batch* b, int* level_offset, int* lanes, uint32_t* total_cells) {
+	if (!b) return MB2_ERR_ARG;
+	if (level_offset) *level_offset = b->level_offset;
+	if (lanes) *lanes = b->lanes;
+	if (total_cells) *total_cells = b->total_cells;
+	return MB2_OK;
+}
+
+int mb2_batch_autotune(mb2_batch* b, const float* pos4, const int* type_ids,
+					   const mb2_step_params* prm, uint32_t trial_steps, void* stream,
+					   mb2_batch_tuning_result* out) {
+	return bguard(b, [&] {
+		check_step_args(b, pos4, pos4, type_ids, prm);
+		expect_arg(out != nullptr && trial_steps > 0, MB2_ERR_ARG,
+				   "mb2_batch_autotune: bad arguments");
+		const cudaStream_t st = S(stream);
+		const uint32_t n = b->n;
+		DevBuf<float4> tpos, tfe;
+		tpos.ensure(std::max<uint32_t>(n, 1));
+		tfe.ensure(std::max<uint32_t>(n, 1));
+		cudaEvent_t e0, e1, e2;
+		MB2_CUDA(cudaEventCreate(&e0));
+		MB2_CUDA(cudaEventCreate(&e1));
+		MB2_CUDA(cudaEventCreate(&e2));
+		const uint32_t period = prm->rebuild_period ? prm->rebuild_period : 1u;
+		int best_level = 0, best_lanes = 0;
+		float best_cost = -1.0f, best_build = 0.0f, best_step = 0.0f;
+		const int levels[3] = {-1, 0, 1};
+		const int lanes_c[3] = {4, 8, 16};
+		for (int li = 0; li < 3; ++li)
+			for (int gi = 0; gi < 3; ++gi) {
+				reset_tuning(b, levels[li], lanes_c[gi]);
+				MB2_CUDA(cudaMemcpyAsync(tpos.ptr, pos4, static_cast<size_t>(n) * 16,
+										 cudaMemcpyDeviceToDevice, st));
+				batch_build(b, tpos.ptr, type_ids, prm->pairlist_cutoff, st);  // sizes the list
+				MB2_CUDA(cudaEventRecord(e0, st));
+				batch_build(b, tpos.ptr, type_ids, prm->pairlist_cutoff, st);
+				MB2_CUDA(cudaEventRecord(e1, st));
+				b->force_sorted.ensure(n);
+				step_counter_set(b->step_d.ptr, 1, st);
+				for (uint32_t k = 0; k < trial_steps; ++k)
+					step_body(b, tpos.ptr, tfe.ptr, type_ids, prm, st);
+				MB2_CUDA(cudaEventRecord(e2, st));
+				MB2_CUDA(cudaEventSynchronize(e2));
+				float tb = 0.0f, ts = 0.0f;
+				MB2_CUDA(cudaEventElapsedTime(&tb, e0, e1));
+				MB2_CUDA(cudaEventElapsedTime(&ts, e1, e2));
+				ts /= static_cast<float>(trial_steps);
+				const float cost = tb / static_cast<float>(period) + ts;
+				if (best_cost < 0.0f || cost < best_cost) {
+					best_cost = cost;
+					best_level = levels[li];
+					best_lanes = lanes_c[gi];
+					best_build = tb;
+					best_step = ts;
+				}
+			}
+		// Apply the best knobs, then measure how far particles move per step from
+		// a fresh list: the largest cadence whose displacement stays within half
+		// the skin keeps every interacting pair in the list.
+		reset_tuning(b, best_level, best_lanes);
+		MB2_CUDA(cudaMemcpyAsync(tpos.ptr, pos4, static_cast<size_t>(n) * 16,
+								 cudaMemcpyDeviceToDevice, st));
+		batch_build(b, tpos.ptr, type_ids, prm->pairlist_cutoff, st);
+		b->force_sorted.ensure(n);
+		step_counter_set(b->step_d.ptr, 1, st);
+		const float skin = prm->pairlist_cutoff - prm->cutoff;
+		uint32_t cadence = 1;
+		bool exceeded = false;
+		float disp_at_period = 0.0f;
+		for (uint32_t k = 1; k <= period; ++k) {
+			step_body(b, tpos.ptr, tfe.ptr, type_ids, prm, st);
+			const float d = batch_max_disp(b, tpos.ptr, st);
+			exceeded |= d > 0.5f * skin;
+			if (!exceeded) cadence = k;
+			disp_at_period = d;
+		}
+		b->built = false;  // that list was built from the trial positions
+		MB2_CUDA(cudaStreamSynchronize(st));
+		cudaEventDestroy(e0);
+		cudaEventDestroy(e1);
+		cudaEventDestroy(e2);
+		out->level_offset = best_level;
+		out->lanes = best_lanes;
+		out->build_ms = best_build;
+		out->step_ms = best_step;
+		out->safe_rebuild_period = cadence;
+		out->max_displacement_at_period = disp_at_period;
+		out->total_cells = b->total_cells;
+	});
+}
+
+}  // extern "C"

@@ -217,6 +217,43 @@ __global__ void __launch_bounds__(256) bd_gather_kernel(
 					   ty.diffusion[type], xi, box, bp);
 }
 
+__device__ __forceinline__ uint64_t mix_seed(uint64_t seed, uint64_t patch, uint64_t step) {
+	// Patch::integrate_motion seed mixing (Patch.cpp:252-254).
+	return (seed * 0x9E3779B97F4A7C15ULL) ^ (patch << 32) ^ (step * 0xBF58476D1CE4E5B9ULL);
+}
+
+// Batched replicas: particle i of system s = sys_of[i] integrates as a plain
+// step of system s with seed (seed + s) would (counter = index in the
+// system, its own box); the step number comes from device memory so that a
+// captured graph can be replayed step after step.
+__global__ void __launch_bounds__(256) bd_systems_kernel(
+	float4* __restrict__ pos, float4* __restrict__ fe, const float4* __restrict__ fs,
+	const uint32_t* __restrict__ inv, const int* __restrict__ type_ids,
+	const uint32_t* __restrict__ sys_of, const uint32_t* __restrict__ offsets,
+	const Box* __restrict__ boxes, uint32_t n, TypeTable ty, float dt, float kT, uint64_t seed,
+	uint64_t patch_id, const unsigned long long* __restrict__ step_ptr) {
+	const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+	if (i >= n) return;
+	const uint64_t step = *step_ptr;
+	const uint32_t s = sys_of[i];
+	const Box& box = boxes[s];
+	float4 f = fs[inv[i]];
+	const float4 p = pos[i];
+	const int type = type_ids[i];
+	const BdParams bp{dt, kT, static_cast<uint32_t>(step), mix_seed(seed + s, patch_id, step), 0u,
+					  {0.0f, 0.0f, 0.0f}};
+	const float4 pmf = position_force(ty, type, p.x, p.y, p.z, bp.efield);
+	const float3 xi = bd_noise(bp.base_seed, i - offsets[s], bp.step);
+	if (pmf.w != 0.0f) f.w = __fadd_rn(f.w, pmf.w);
+	fe[i] = f;
+	pos[i] = bd_update(p, __fadd_rn(f.x, pmf.x), __fadd_rn(f.y, pmf.y), __fadd_rn(f.z, pmf.z),
+					   ty.diffusion[type], xi, box, bp);
+}
+
+__global__ void step_counter_kernel(unsigned long long* ptr, unsigned long long v, int add) {
+	*ptr = add ? *ptr + v : v;
+}
+
 __global__ void philox_kernel(uint64_t seed, uint32_t ctr0, uint32_t ctr1, uint32_t ctr2,
 							  uint32_t n, uint4* out4, float4* normals4) {
 	const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -243,6 +280,25 @@ void bd_integrate_gather(float4* pos, float4* fe, const float4* force_sorted, co
 	if (n == 0) return;
 	MB2_LAUNCH bd_gather_kernel<<<(n + 255) / 256, 256, 0, st>>>(pos, fe, force_sorted, inv, type_ids,
 																 flags, n, types, box, p, read_fe);
+}
+
+void bd_integrate_systems(float4* pos, float4* fe, const float4* force_sorted,
+						  const uint32_t* inv, const int* type_ids, const uint32_t* sys_of,
+						  const uint32_t* offsets, const Box* boxes, uint32_t n,
+						  const TypeTable& types, float dt, float kT, uint64_t seed,
+						  uint64_t patch_id, const unsigned long long* step_ptr, cudaStream_t st) {
+	if (n == 0) return;
+	MB2_LAUNCH bd_systems_kernel<<<(n + 255) / 256, 256, 0, st>>>(
+		pos, fe, force_sorted, inv, type_ids, sys_of, offsets, boxes, n, types, dt, kT, seed,
+		patch_id, step_ptr);
+}
+
+void step_counter_set(unsigned long long* ptr, uint64_t value, cudaStream_t st) {
+	MB2_LAUNCH step_counter_kernel<<<1, 1, 0, st>>>(ptr, value, 0);
+}
+
+void step_counter_add(unsigned long long* ptr, uint64_t value, cudaStream_t st) {
+	MB2_LAUNCH step_counter_kernel<<<1, 1, 0, st>>>(ptr, value, 1);
 }
 
 void philox_draws(uint64_t seed, uint32_t ctr0, uint32_t ctr1, uint32_t ctr2, uint32_t n,

@@ -25,6 +25,10 @@
 //
 // FP64: total pair energy and virial are reduced in double on the device
 // (per-thread double, block reduction, one double atomic per block).
+#include <algorithm>
+#include <vector>
+
+#include "marsb200.h"
 #include "mb2_internal.cuh"
 
 namespace mb2 {
@@ -144,12 +148,25 @@ __device__ __forceinline__ void load_tables(int T, const PairTableRef* __restric
 	__syncthreads();
 }
 
-template <int G, bool kEnergy, bool kAllPeriodic>
+// Box of a row: one box for the whole list, or the box of the row's system
+// (batched replicas: system id in the top bits of the sorted key).
+struct OneBox {
+	Box b;
+	__device__ __forceinline__ const Box& row(uint32_t) const { return b; }
+};
+struct SystemBoxes {
+	const Box* __restrict__ boxes;
+	const uint32_t* __restrict__ keys;
+	int sys_shift;
+	__device__ __forceinline__ Box row(uint32_t i) const { return boxes[keys[i] >> sys_shift]; }
+};
+
+template <int G, bool kEnergy, bool kAllPeriodic, class BoxSrc>
 __global__ void __launch_bounds__(256) pair_force_kernel(
 	const float4* __restrict__ sorted_pos, const uint32_t* __restrict__ nbr,
 	const uint32_t* __restrict__ row_len, uint32_t n, uint32_t cap, int T,
 	const PairTableRef* __restrict__ refs_g, const float* __restrict__ force_g,
-	const float2* __restrict__ energy_g, uint32_t total_bins, Box box, float cutoff_sq,
+	const float2* __restrict__ energy_g, uint32_t total_bins, BoxSrc boxes, float cutoff_sq,
 	float4* force, double* __restrict__ ev) {
 	constexpr int H = 32 / G;
 	PairTableRef* refs;
@@ -160,6 +177,7 @@ __global__ void __launch_bounds__(256) pair_force_kernel(
 	const int sub = threadIdx.x & (G - 1);  // lane within the row's group
 	const uint32_t i = blockIdx.x * (blockDim.x / G) + threadIdx.x / G;
 	const bool valid = i < n;
+	const Box& box = boxes.row(valid ? i : 0u);
 	const float4 pi = valid ? sorted_pos[i] : make_float4(0.f, 0.f, 0.f, 0.f);
 	const PairTableRef* trow = refs + (valid ? type_of(pi) : 0) * T;
 	const uint32_t cnt = valid ? row_len[i] : 0u;
@@ -298,51 +316,120 @@ __global__ void __launch_bounds__(256) angle_kernel(const int4* __restrict__ ang
 	if (get_energy) block_add_f64(e_acc, 0.0, energy);
 }
 
-template <int G, bool kEnergy, bool kAllPeriodic>
+template <int G, bool kEnergy, bool kAllPeriodic, class BoxSrc>
 void launch_pair(const float4* sorted_pos, const uint32_t* nbr, const uint32_t* row_len,
-				 uint32_t n, uint32_t cap, const PairTables& t, const Box& box, float cutoff_sq,
-				 float4* force_sorted, double* ev, cudaStream_t st) {
+				 uint32_t n, uint32_t cap, const PairTables& t, const BoxSrc& boxes,
+				 float cutoff_sq, float4* force_sorted, double* ev, cudaStream_t st) {
 	const size_t smem = static_cast<size_t>(t.num_types * t.num_types) * sizeof(PairTableRef) +
 						static_cast<size_t>((t.total_bins + 1) & ~1u) * 4 +
 						(kEnergy ? static_cast<size_t>(t.total_bins) * 8 : 0);
 	const uint32_t rows = 256 / G;
 	const uint32_t blocks = (n + rows - 1) / rows;
-	auto kern = pair_force_kernel<G, kEnergy, kAllPeriodic>;
+	auto kern = pair_force_kernel<G, kEnergy, kAllPeriodic, BoxSrc>;
 	if (smem > 48 * 1024)
 		MB2_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
 									  static_cast<int>(smem)));
 	MB2_LAUNCH kern<<<blocks, 256, smem, st>>>(sorted_pos, nbr, row_len, n, cap, t.num_types,
 											   t.refs, t.bin_force, t.bin_energy, t.total_bins,
-											   box, cutoff_sq, force_sorted, ev);
+											   boxes, cutoff_sq, force_sorted, ev);
 }
 
-template <int G>
+template <int G, class BoxSrc>
 void launch_pair_g(const float4* sorted_pos, const uint32_t* nbr, const uint32_t* row_len,
-				   uint32_t n, uint32_t cap, const PairTables& t, const Box& box, float cutoff_sq,
-				   int get_energy, float4* force_sorted, double* ev, cudaStream_t st) {
-	const bool all_periodic = box.periodic[0] && box.periodic[1] && box.periodic[2];
+				   uint32_t n, uint32_t cap, const PairTables& t, const BoxSrc& boxes,
+				   bool all_periodic, float cutoff_sq, int get_energy, float4* force_sorted,
+				   double* ev, cudaStream_t st) {
 	if (get_energy) {
-		if (all_periodic) launch_pair<G, true, true>(sorted_pos, nbr, row_len, n, cap, t, box, cutoff_sq, force_sorted, ev, st);
-		else launch_pair<G, true, false>(sorted_pos, nbr, row_len, n, cap, t, box, cutoff_sq, force_sorted, ev, st);
+		if (all_periodic) launch_pair<G, true, true>(sorted_pos, nbr, row_len, n, cap, t, boxes, cutoff_sq, force_sorted, ev, st);
+		else launch_pair<G, true, false>(sorted_pos, nbr, row_len, n, cap, t, boxes, cutoff_sq, force_sorted, ev, st);
 	} else {
-		if (all_periodic) launch_pair<G, false, true>(sorted_pos, nbr, row_len, n, cap, t, box, cutoff_sq, force_sorted, ev, st);
-		else launch_pair<G, false, false>(sorted_pos, nbr, row_len, n, cap, t, box, cutoff_sq, force_sorted, ev, st);
+		if (all_periodic) launch_pair<G, false, true>(sorted_pos, nbr, row_len, n, cap, t, boxes, cutoff_sq, force_sorted, ev, st);
+		else launch_pair<G, false, false>(sorted_pos, nbr, row_len, n, cap, t, boxes, cutoff_sq, force_sorted, ev, st);
+	}
+}
+
+template <class BoxSrc>
+void launch_pair_lanes(const float4* sorted_pos, const uint32_t* nbr, const uint32_t* row_len,
+					   uint32_t n, uint32_t cap, int lanes_per_row, const PairTables& t,
+					   const BoxSrc& boxes, bool all_periodic, float cutoff_sq, int get_energy,
+					   float4* force_sorted, double* ev, cudaStream_t st) {
+	switch (lanes_per_row) {
+	case 4: launch_pair_g<4>(sorted_pos, nbr, row_len, n, cap, t, boxes, all_periodic, cutoff_sq, get_energy, force_sorted, ev, st); break;
+	case 8: launch_pair_g<8>(sorted_pos, nbr, row_len, n, cap, t, boxes, all_periodic, cutoff_sq, get_energy, force_sorted, ev, st); break;
+	case 16: launch_pair_g<16>(sorted_pos, nbr, row_len, n, cap, t, boxes, all_periodic, cutoff_sq, get_energy, force_sorted, ev, st); break;
+	default: launch_pair_g<32>(sorted_pos, nbr, row_len, n, cap, t, boxes, all_periodic, cutoff_sq, get_energy, force_sorted, ev, st); break;
 	}
 }
 
 }  // namespace
+
+size_t pair_table_arrays(int num_types, const uint32_t* term_matrix, int num_tables,
+						 const float* values, const uint32_t* sizes, const float* starts,
+						 const float* step_invs, std::vector<PairTableRef>& refs,
+						 std::vector<float>& bf, std::vector<float2>& be) {
+	expect_arg(num_types > 0 && num_types <= 64, MB2_ERR_ARG, "pair tables: 1..64 particle types");
+	expect_arg(num_tables >= 0 && term_matrix, MB2_ERR_ARG, "pair tables: bad tables");
+	for (int k = 0; k < num_types * num_types; ++k) {
+		const uint32_t tag = term_matrix[k];
+		expect_arg(!(tag & kTermTabulated) || static_cast<int>(tag >> kTableShift) < num_tables,
+				   MB2_ERR_ARG, "pair tables: a tag names a missing table");
+	}
+	// Per-bin force and energy, rounded exactly as TabulatedPotential::compute
+	// rounds them (TabulatedPotential.h:41-51): dU = U[k+1] - U[k] and
+	// F = -dU * step_inv in float; the last bin is the home >= size-1 case.
+	std::vector<uint32_t> offset(num_tables);
+	size_t total = 0;
+	for (int k = 0; k < num_tables; ++k) {
+		expect_arg(sizes[k] >= 2, MB2_ERR_ARG, "pair tables: a table needs 2 values");
+		offset[k] = static_cast<uint32_t>(total);
+		total += sizes[k];
+	}
+	bf.assign(std::max<size_t>(total, 1), 0.0f);
+	be.assign(std::max<size_t>(total, 1), make_float2(0.0f, 0.0f));
+	for (int k = 0; k < num_tables; ++k) {
+		const float* u = values + offset[k];
+		const uint32_t sz = sizes[k];
+		for (uint32_t b = 0; b + 1 < sz; ++b) {
+			volatile float du = u[b + 1] - u[b];
+			volatile float f = -du * step_invs[k];
+			bf[offset[k] + b] = f;
+			be[offset[k] + b] = make_float2(u[b], du);
+		}
+		bf[offset[k] + sz - 1] = 0.0f;
+		be[offset[k] + sz - 1] = make_float2(u[sz - 1], 0.0f);
+	}
+	const int tt = num_types * num_types;
+	refs.assign(tt, PairTableRef{0.0f, 0.0f, 0, -1});
+	for (int k = 0; k < tt; ++k) {
+		const uint32_t tag = term_matrix[k];
+		if (tag & kTermTabulated) {
+			const int t = static_cast<int>(tag >> kTableShift);
+			refs[k] = PairTableRef{starts[t], step_invs[t], static_cast<int>(sizes[t]) - 1,
+								   static_cast<int>(offset[t])};
+		}
+	}
+	return total;
+}
 
 void pair_forces(const float4* sorted_pos, const uint32_t* nbr, const uint32_t* row_len,
 				 uint32_t n, uint32_t cap, int lanes_per_row, const PairTables& t, const Box& box,
 				 float cutoff_sq, int get_energy, float4* force_sorted, double* ev,
 				 cudaStream_t st) {
 	if (n == 0) return;
-	switch (lanes_per_row) {
-	case 4: launch_pair_g<4>(sorted_pos, nbr, row_len, n, cap, t, box, cutoff_sq, get_energy, force_sorted, ev, st); break;
-	case 8: launch_pair_g<8>(sorted_pos, nbr, row_len, n, cap, t, box, cutoff_sq, get_energy, force_sorted, ev, st); break;
-	case 16: launch_pair_g<16>(sorted_pos, nbr, row_len, n, cap, t, box, cutoff_sq, get_energy, force_sorted, ev, st); break;
-	default: launch_pair_g<32>(sorted_pos, nbr, row_len, n, cap, t, box, cutoff_sq, get_energy, force_sorted, ev, st); break;
-	}
+	const bool all_periodic = box.periodic[0] && box.periodic[1] && box.periodic[2];
+	launch_pair_lanes(sorted_pos, nbr, row_len, n, cap, lanes_per_row, t, OneBox{box},
+					  all_periodic, cutoff_sq, get_energy, force_sorted, ev, st);
+}
+
+void pair_forces_systems(const float4* sorted_pos, const uint32_t* nbr, const uint32_t* row_len,
+						 uint32_t n, uint32_t cap, int lanes_per_row, const PairTables& t,
+						 const Box* boxes, const uint32_t* sorted_keys, int sys_shift,
+						 bool all_periodic, float cutoff_sq, int get_energy, float4* force_sorted,
+						 double* ev, cudaStream_t st) {
+	if (n == 0) return;
+	launch_pair_lanes(sorted_pos, nbr, row_len, n, cap, lanes_per_row, t,
+					  SystemBoxes{boxes, sorted_keys, sys_shift}, all_periodic, cutoff_sq,
+					  get_energy, force_sorted, ev, st);
 }
 
 void scatter_add_forces(const float4* force_sorted, const uint32_t* s2o, uint32_t n,

@@ -28,6 +28,11 @@ struct Error {
 			throw ::mb2::Error{2, std::string(#call) + ": " + cudaGetErrorString(e_)};   \
 	} while (0)
 
+// Throws Error{code, msg} unless cond holds.
+inline void expect_arg(bool cond, int code, const char* msg) {
+	if (!cond) throw Error{code, msg};
+}
+
 // Device buffer that only grows; owned by a context.
 template <typename T>
 struct DevBuf {
@@ -133,7 +138,10 @@ struct WalkGrid {
 	float rc2;                 // pairlist cutoff squared, as the reference rounds it
 	float fast_lo, fast_hi;    // d^2 band that needs the exact test
 };
-CellGrid choose_cell_grid(const float* extent, const int* periodic, float rc_list, size_t n);
+// Cell level m in [m_lo, m_hi] minimising candidates plus per-cell cost; the
+// widths assume the 10-bit Morton scale (conservative for coarser scales).
+CellGrid choose_cell_grid(const float* extent, const int* periodic, float rc_list, size_t n,
+						  int m_lo = 0, int m_hi = 8);
 void fast_test_band(const Box& box, float rc_list, float* fast_lo, float* fast_hi);
 void cell_ranges(const uint32_t* keys, uint32_t n, int shift, uint32_t* begin, uint32_t* end,
 				 size_t num_cells, cudaStream_t st);
@@ -172,6 +180,18 @@ void pair_forces(const float4* sorted_pos, const uint32_t* nbr, const uint32_t* 
 				 uint32_t n, uint32_t cap, int lanes_per_row, const PairTables& t, const Box& box,
 				 float cutoff_sq, int get_energy, float4* force_sorted, double* energy_virial,
 				 cudaStream_t st);
+// Host: per-type-pair lookup constants and per-bin force / (U0, dU) arrays of
+// a set of tabulated pair tables; returns the total number of bins.
+size_t pair_table_arrays(int num_types, const uint32_t* term_matrix, int num_tables,
+						 const float* values, const uint32_t* sizes, const float* starts,
+						 const float* step_invs, std::vector<PairTableRef>& refs,
+						 std::vector<float>& bf, std::vector<float2>& be);
+// Batched replicas: row i's box is boxes[sorted_keys[i] >> sys_shift].
+void pair_forces_systems(const float4* sorted_pos, const uint32_t* nbr, const uint32_t* row_len,
+						 uint32_t n, uint32_t cap, int lanes_per_row, const PairTables& t,
+						 const Box* boxes, const uint32_t* sorted_keys, int sys_shift,
+						 bool all_periodic, float cutoff_sq, int get_energy, float4* force_sorted,
+						 double* ev, cudaStream_t st);
 void scatter_add_forces(const float4* force_sorted, const uint32_t* s2o, uint32_t n,
 						float4* force_energy, int get_energy, cudaStream_t st);
 void bond_forces(const int2* bonds, const int* table_idx, uint32_t nb, const float4* pos,
@@ -222,6 +242,16 @@ void bd_integrate_gather(float4* pos, float4* fe, const float4* force_sorted, co
 						 const int* type_ids, const uint32_t* flags, uint32_t n,
 						 const TypeTable& types, const Box& box, const BdParams& p, int read_fe,
 						 cudaStream_t st);
+// Batched replicas' integrate: per-system box, seed (seed + s) mixed with
+// (patch_id, *step_ptr), Philox counter = index within the system.
+void bd_integrate_systems(float4* pos, float4* fe, const float4* force_sorted,
+						  const uint32_t* inv, const int* type_ids, const uint32_t* sys_of,
+						  const uint32_t* offsets, const Box* boxes, uint32_t n,
+						  const TypeTable& types, float dt, float kT, uint64_t seed,
+						  uint64_t patch_id, const unsigned long long* step_ptr, cudaStream_t st);
+// Device step counter: set to `value`, or add `value` (one-thread launches).
+void step_counter_set(unsigned long long* ptr, uint64_t value, cudaStream_t st);
+void step_counter_add(unsigned long long* ptr, uint64_t value, cudaStream_t st);
 void philox_draws(uint64_t seed, uint32_t ctr0, uint32_t ctr1, uint32_t ctr2, uint32_t n,
 				  uint32_t* out4, float* normals4, cudaStream_t st);
 

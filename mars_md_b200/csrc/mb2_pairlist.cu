@@ -43,14 +43,15 @@ double ulp_of(double x) {
 
 }  // namespace
 
-CellGrid choose_cell_grid(const float* extent, const int* periodic, float rc_list, size_t n) {
+CellGrid choose_cell_grid(const float* extent, const int* periodic, float rc_list, size_t n,
+						  int m_lo, int m_hi) {
 	CellGrid best;
 	double best_cost = -1.0;
 	const double rc = static_cast<double>(rc_list);
-	for (int m = 0; m <= 8; ++m) {
+	for (int m = m_lo; m <= m_hi; ++m) {
 		const int cells = 1 << m;
 		const double num_cells = std::ldexp(1.0, 3 * m);
-		if (m > 0 && num_cells > 2.0 * static_cast<double>(n)) break;
+		if (m > m_lo && num_cells > 2.0 * static_cast<double>(n)) break;
 		std::vector<int> off[3];
 		std::vector<double> gap[3];
 		int radius[3] = {0, 0, 0};

@@ -14,6 +14,10 @@ call surface on the Brownian-dynamics path:
   (src/PatchOperation/Integrator.h:26-54);
 * ``step`` -- one SimManager step for one patch (src/SimManager.cpp:337-504).
 
+``Batch`` wraps one ``mb2_batch``: many independent periodic systems stepped
+together (one launch per stage for all of them, CUDA-graph step replay, an
+autotuner for cell level and lanes per row).
+
 Device arrays are torch CUDA tensors (positions and forces float32 [N, 4]).
 torch is only the allocator and stream provider here; every kernel is the
 library's own.
@@ -289,3 +293,112 @@ def setup_workload(ctx: Context, w, device="cuda:0"):
     dev["grids"] = grids
     ctx.set_particle_types(w.charge, w.diffusion, w.pmf_terms)
     return dev
+
+
+class Batch:
+    """Batched replicas: systems concatenated in one set of arrays; system s
+    steps as a plain context with seed (params.seed + s) would."""
+
+    def __init__(self, counts, box_sizes, box_origins=None, device: int = 0):
+        self.lib = L.load()
+        self.device = device
+        self.counts = np.ascontiguousarray(counts, np.uint32)
+        self.offsets = np.concatenate([[0], np.cumsum(self.counts)]).astype(np.int64)
+        self.n = int(self.offsets[-1])
+        sizes = np.ascontiguousarray(box_sizes, np.float32).reshape(-1, 3)
+        origins = None if box_origins is None else \
+            np.ascontiguousarray(box_origins, np.float32).reshape(-1, 3)
+        fp = C.POINTER(C.c_float)
+        h = C.c_void_p()
+        rc = self.lib.mb2_batch_create(
+            int(device), len(self.counts), self.counts.ctypes.data_as(C.POINTER(C.c_uint32)),
+            None if origins is None else origins.ctypes.data_as(fp), sizes.ctypes.data_as(fp),
+            C.byref(h))
+        if rc != 0:
+            raise L.MB2Error(rc, "mb2_batch_create failed")
+        self.h = h
+
+    def close(self):
+        if getattr(self, "h", None) is not None and self.h.value:
+            self.lib.mb2_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def check(self, rc: int):
+        if rc != 0:
+            raise L.MB2Error(rc, self.lib.mb2_batch_last_error(self.h).decode())
+
+    def set_pair_tables(self, num_types, term_matrix, tables):
+        vals, sizes, starts, sinv = Context._tables(tables)
+        tm = np.ascontiguousarray(term_matrix, np.uint32)
+        fp = C.POINTER(C.c_float)
+        self.check(self.lib.mb2_batch_set_pair_tables(
+            self.h, int(num_types), tm.ctypes.data_as(C.POINTER(C.c_uint32)), len(tables),
+            vals.ctypes.data_as(fp), sizes.ctypes.data_as(C.POINTER(C.c_uint32)),
+            starts.ctypes.data_as(fp), sinv.ctypes.data_as(fp)))
+
+    def set_particle_types(self, charge, diffusion):
+        q = np.ascontiguousarray(charge, np.float32)
+        d = np.ascontiguousarray(diffusion, np.float32).reshape(-1, 3)
+        fp = C.POINTER(C.c_float)
+        self.check(self.lib.mb2_batch_set_particle_types(self.h, len(q), q.ctypes.data_as(fp),
+                                                         d.ctypes.data_as(fp)))
+
+    def build(self, pos, type_ids, pairlist_cutoff, stream=None) -> int:
+        npairs = C.c_uint64()
+        self.check(self.lib.mb2_batch_build(self.h, _p(pos), _p(type_ids), float(pairlist_cutoff),
+                                            _stream(stream), C.byref(npairs)))
+        return int(npairs.value)
+
+    def num_pairs(self) -> int:
+        v = C.c_uint64()
+        self.check(self.lib.mb2_batch_num_pairs(self.h, C.byref(v)))
+        return int(v.value)
+
+    def export_pairs(self, stream=None):
+        n = self.num_pairs()
+        out = torch.empty((max(n, 1), 2), dtype=torch.int32, device=f"cuda:{self.device}")
+        self.check(self.lib.mb2_batch_export_pairs(self.h, _p(out), n, _stream(stream)))
+        return out[:n]
+
+    def step(self, pos, fe, type_ids, step, params: "L.StepParams", stream=None):
+        self.check(self.lib.mb2_batch_step(self.h, _p(pos), _p(fe), _p(type_ids), int(step),
+                                           C.byref(params), _stream(stream)))
+
+    def run(self, pos, fe, type_ids, first_step, num_steps, params: "L.StepParams", stream=None):
+        self.check(self.lib.mb2_batch_run(self.h, _p(pos), _p(fe), _p(type_ids), int(first_step),
+                                          int(num_steps), C.byref(params), _stream(stream)))
+
+    def set_tuning(self, level_offset=0, lanes=0):
+        self.check(self.lib.mb2_batch_set_tuning(self.h, int(level_offset), int(lanes)))
+
+    def tuning(self):
+        lvl, lanes, cells = C.c_int(), C.c_int(), C.c_uint32()
+        self.check(self.lib.mb2_batch_tuning(self.h, C.byref(lvl), C.byref(lanes), C.byref(cells)))
+        return lvl.value, lanes.value, cells.value
+
+    def autotune(self, pos, type_ids, params: "L.StepParams", trial_steps=4, stream=None) -> dict:
+        r = L.BatchTuning()
+        self.check(self.lib.mb2_batch_autotune(self.h, _p(pos), _p(type_ids), C.byref(params),
+                                               int(trial_steps), _stream(stream), C.byref(r)))
+        return {k: getattr(r, k) for k, _ in L.BatchTuning._fields_}
+
+
+def setup_batch(ws, device="cuda:0"):
+    """A Batch over workloads that share tables and types (e.g. workloads.batched());
+    returns (batch, device tensors of the concatenated systems)."""
+    w0 = ws[0]
+    b = Batch([w.n for w in ws], [w.box_size for w in ws], [w.box_origin for w in ws],
+              device=torch.device(device).index or 0)
+    b.set_pair_tables(w0.num_types, w0.term_matrix,
+                      [(t.values, t.start, t.step_inv) for t in w0.pair_tables])
+    b.set_particle_types(w0.charge, w0.diffusion)
+    dev = {"pos": torch.from_numpy(np.concatenate([w.pos for w in ws])).to(device),
+           "type": torch.from_numpy(np.concatenate([w.type_ids for w in ws])).to(device)}
+    dev["fe"] = torch.zeros((b.n, 4), dtype=torch.float32, device=device)
+    return b, dev

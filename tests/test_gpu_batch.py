@@ -1,0 +1,160 @@
+"""Batched replicas (mb2_batch_*) against the oracle and against plain
+per-system steps: the same pair set in every system, the same trajectories
+(system s of a batch steps as a plain context with seed + s), graph replay
+equal to eager steps, and tuning knobs that change speed but not results."""
+import numpy as np
+import pytest
+import torch
+
+from conftest import box_of
+from mars_md_b200 import _lib, workloads as W
+from mars_md_b200.engine import Context, setup_batch, setup_workload, step_params
+
+pytestmark = pytest.mark.gpu
+
+SEED = 4242
+
+
+def _systems(k=10, nmax=3000):
+    return W.batched(seed=SEED, systems=k, nmin=500, nmax=nmax)
+
+
+def _canon(p):
+    p = np.sort(np.asarray(p, np.int64), axis=1)
+    return p[np.lexsort((p[:, 1], p[:, 0]))] if len(p) else p.reshape(0, 2)
+
+
+def _split_pairs(pairs, offsets):
+    sys_a = np.searchsorted(offsets, pairs[:, 0], side="right") - 1
+    sys_b = np.searchsorted(offsets, pairs[:, 1], side="right") - 1
+    assert np.array_equal(sys_a, sys_b), "a pair crosses systems"
+    return [pairs[sys_a == s] - offsets[s] for s in range(len(offsets) - 1)]
+
+
+def _check_pair_sets(oracle, b, ws):
+    per = _split_pairs(b.export_pairs().cpu().numpy().astype(np.int64), b.offsets)
+    for s, w in enumerate(ws):
+        ref, cnt, _ = oracle.build_pairlist(w.pos, box_of(w), w.list_radius)
+        assert len(per[s]) == cnt, f"system {s}"
+        assert np.array_equal(_canon(per[s]), ref.astype(np.int64)), f"system {s}"
+
+
+def test_batch_pair_sets_match_oracle_per_system(oracle):
+    ws = _systems()
+    b, dev = setup_batch(ws)
+    try:
+        n = b.build(dev["pos"], dev["type"], ws[0].list_radius)
+        assert n == b.num_pairs()
+        _check_pair_sets(oracle, b, ws)
+    finally:
+        b.close()
+
+
+@pytest.mark.parametrize("level,lanes", [(1, 16), (-1, 4), (0, 32)])
+def test_batch_tuning_knobs_keep_the_pair_set(oracle, level, lanes):
+    ws = _systems(k=6)
+    b, dev = setup_batch(ws)
+    try:
+        b.set_tuning(level, lanes)
+        b.build(dev["pos"], dev["type"], ws[0].list_radius)
+        assert b.tuning()[1] == lanes
+        _check_pair_sets(oracle, b, ws)
+    finally:
+        b.close()
+
+
+def _plain_trajectories(ws, prm_for, steps):
+    out = []
+    for s, w in enumerate(ws):
+        ctx = Context(w.n)
+        dev = setup_workload(ctx, w)
+        prm = prm_for(w, s)
+        for k in range(1, steps + 1):
+            ctx.step(dev["pos"], dev["fe"], dev["type"], None, k, prm)
+        torch.cuda.synchronize()
+        out.append((dev["pos"].cpu().numpy(), dev["fe"].cpu().numpy()))
+        ctx.close()
+    return out
+
+
+def _periodic_diff(a, b, box_len):
+    d = np.abs(a - b)
+    return np.minimum(d, np.abs(d - box_len))
+
+
+def test_batch_run_equals_plain_steps_per_system():
+    ws = _systems(k=8)
+    steps, period = 7, 3
+
+    def prm_for(w, s):
+        p = step_params(w, seed=SEED + s)
+        p.rebuild_period = period
+        return p
+
+    plain = _plain_trajectories(ws, prm_for, steps)
+    b, dev = setup_batch(ws)
+    try:
+        prm = step_params(ws[0], seed=SEED)
+        prm.rebuild_period = period
+        b.run(dev["pos"], dev["fe"], dev["type"], 1, steps, prm)
+        torch.cuda.synchronize()
+        pos = dev["pos"].cpu().numpy()
+        fe = dev["fe"].cpu().numpy()
+        for s, w in enumerate(ws):
+            lo, hi = b.offsets[s], b.offsets[s + 1]
+            dp = _periodic_diff(pos[lo:hi, :3], plain[s][0][:, :3], w.box_size[0])
+            assert dp.max() < 1e-4, f"system {s}: {dp.max()}"
+            df = np.abs(fe[lo:hi, :3] - plain[s][1][:, :3]).max()
+            scale = np.abs(plain[s][1][:, :3]).max() + 1e-30
+            assert df / scale < 1e-5, f"system {s}: force {df / scale}"
+        start = np.concatenate([w.pos for w in ws])[:, :3]
+        assert np.abs(pos[:, :3] - start).max() > 0.1
+    finally:
+        b.close()
+
+
+def test_batch_graph_replay_equals_eager_steps():
+    ws = _systems(k=5)
+    prm = step_params(ws[0], seed=SEED)
+    prm.rebuild_period = 2
+    b1, d1 = setup_batch(ws)
+    b2, d2 = setup_batch(ws)
+    try:
+        for k in range(1, 6):
+            b1.step(d1["pos"], d1["fe"], d1["type"], k, prm)
+        b2.run(d2["pos"], d2["fe"], d2["type"], 1, 5, prm)
+        torch.cuda.synchronize()
+        box = np.repeat([w.box_size[0] for w in ws], [w.n for w in ws])[:, None]
+        diff = _periodic_diff(d1["pos"].cpu().numpy()[:, :3], d2["pos"].cpu().numpy()[:, :3], box)
+        assert diff.max() < 1e-5
+    finally:
+        b1.close()
+        b2.close()
+
+
+def test_batch_autotune_reports_and_keeps_results(oracle):
+    ws = _systems(k=6)
+    b, dev = setup_batch(ws)
+    try:
+        prm = step_params(ws[0], seed=SEED)
+        before = dev["pos"].clone()
+        r = b.autotune(dev["pos"], dev["type"], prm, trial_steps=2)
+        torch.cuda.synchronize()
+        assert torch.equal(before, dev["pos"])  # tuning runs on a copy
+        assert r["lanes"] in (4, 8, 16) and r["level_offset"] in (-1, 0, 1)
+        assert 1 <= r["safe_rebuild_period"] <= prm.rebuild_period
+        assert r["step_ms"] > 0 and r["build_ms"] > 0
+        b.build(dev["pos"], dev["type"], ws[0].list_radius)
+        _check_pair_sets(oracle, b, ws)
+    finally:
+        b.close()
+
+
+def test_batch_rejects_boxes_smaller_than_twice_the_list_radius():
+    w = W.plain_bd(seed=1, n=600, box=40.0)
+    b, dev = setup_batch([w])
+    try:
+        with pytest.raises(_lib.MB2Error):
+            b.build(dev["pos"], dev["type"], 25.0)
+    finally:
+        b.close()
