@@ -1,0 +1,286 @@
+/*
+ * FP64 CPU reference of the BD window and its adjoint.
+ *
+ * TEST INFRASTRUCTURE ONLY: the checker of the CUDA adjoint
+ * (mars_md_b200/csrc/mb2_adjoint.cu) and of the finite differences. The
+ * reference code base has no adjoint; the forward model restated here in
+ * double is the reference's BD step with tabulated forces:
+ *   - pair force: TabulatedPotential::compute (TabulatedPotential.h:19-52) on
+ *     the minimum-image distance (PeriodicBox.h:134-208), cut off beyond the
+ *     interaction cutoff and below 1e-6 (Pairwise.h:214-304), all non-excluded
+ *     pairs;
+ *   - bond force: TabulatedBondComputer (BondComputer.h:136-192);
+ *   - angle force: TabulatedAngleComputer + AngleGeometry (BondComputer.h:204-269,
+ *     BondGeometry.h:13-45), periodic table;
+ *   - update: x <- wrap(x + (D dt / kT) F + sqrt(2 D dt) xi) (BD.h:80-85).
+ * The adjoint of one step is lambda_k = lambda_{k+1} + J(x_k)^T (c * lambda_{k+1})
+ * with c = D dt / kT. Every force here is minus the gradient of a potential
+ * that is piecewise linear in the distance or angle, so J is symmetric (except
+ * where the angle's sine is floored at 1e-3) and J^T mu is computed as the
+ * directional derivative of the force along mu. Table gradients use
+ * dF/dU[h] = +step_inv, dF/dU[h+1] = -step_inv for the pair's bin h.
+ */
+#include <math.h>
+#include <stdlib.h>
+#include <string.h>
+
+typedef struct {
+	const double* v;
+	int size;
+	double start;
+	double step_inv;
+	int periodic;
+} adj_table;
+
+typedef struct {
+	int n;
+	double L[3];
+	double c[3]; /* D dt / kT per axis */
+	double s[3]; /* sqrt(2 D dt) per axis */
+	adj_table pair;
+	double cutoff;
+	const int* excl_off; /* CSR over particles, or NULL */
+	const int* excl_nb;
+	int excl_n;
+	const int* bonds; /* (i, j) */
+	int nb;
+	adj_table bond;
+	const int* angles; /* (i, j, k, pad) */
+	int na;
+	adj_table angle;
+} adj_sys;
+
+/* Dual number: value and derivative along one direction. */
+typedef struct {
+	double v, d;
+} dual;
+
+static dual dmk(double v, double d) {
+	dual r = {v, d};
+	return r;
+}
+static dual dadd(dual a, dual b) { return dmk(a.v + b.v, a.d + b.d); }
+static dual dsub(dual a, dual b) { return dmk(a.v - b.v, a.d - b.d); }
+static dual dmul(dual a, dual b) { return dmk(a.v * b.v, a.d * b.v + a.v * b.d); }
+static dual ddiv(dual a, dual b) { return dmk(a.v / b.v, (a.d * b.v - a.v * b.d) / (b.v * b.v)); }
+static dual dsqrt(dual a) {
+	const double r = sqrt(a.v);
+	return dmk(r, r > 0.0 ? a.d / (2.0 * r) : 0.0);
+}
+static dual dscale(dual a, double k) { return dmk(a.v * k, a.d * k); }
+
+static double min_image(double x, double l) {
+	const double image = floor(x * (1.0 / l));
+	x -= image * l;
+	return x >= 0.5 * l ? x - l : x;
+}
+
+static int excluded(const adj_sys* s, int a, int b) {
+	if (!s->excl_off || a >= s->excl_n) return 0;
+	for (int e = s->excl_off[a]; e < s->excl_off[a + 1]; ++e)
+		if (s->excl_nb[e] == b) return 1;
+	return 0;
+}
+
+/* Table force F(x) = -dU/dx of the bin's linear interpolant; *bin = home
+ * (or -1 where the force is constant 0: past the end of a non-periodic table). */
+static double table_force(const adj_table* t, double x, int* bin, int* bin1) {
+	const double w = (x - t->start) * t->step_inv;
+	int home = (int)floor(w);
+	if (t->periodic) {
+		home %= t->size;
+		if (home < 0) home += t->size;
+	} else {
+		if (home >= t->size - 1) {
+			*bin = -1;
+			*bin1 = -1;
+			return 0.0;
+		}
+		if (home < 0) home = 0;
+	}
+	const int home1 = t->periodic ? (home + 1) % t->size : home + 1;
+	*bin = home;
+	*bin1 = home1;
+	return -(t->v[home1] - t->v[home]) * t->step_inv;
+}
+
+/* Central-pair term (pair or bond): force on j is F(r) u, on i -F(r) u, with
+ * u = (x_j - x_i) / r. With mu: tangent of the forces along mu (t), and the
+ * table gradient mu . dforce/dU (g). */
+static void radial_term(const adj_sys* s, const adj_table* tab, double cutoff, int i, int j,
+						const double* x, double* f, const double* mu, double* t, double* g) {
+	double r[3];
+	for (int a = 0; a < 3; ++a) r[a] = min_image(x[3 * j + a] - x[3 * i + a], s->L[a]);
+	const double d = sqrt(r[0] * r[0] + r[1] * r[1] + r[2] * r[2]);
+	if (d < 1e-6 || (cutoff > 0.0 && d > cutoff)) return;
+	int h, h1;
+	const double F = table_force(tab, d, &h, &h1);
+	const double u[3] = {r[0] / d, r[1] / d, r[2] / d};
+	if (f)
+		for (int a = 0; a < 3; ++a) {
+			f[3 * j + a] += F * u[a];
+			f[3 * i + a] -= F * u[a];
+		}
+	if (mu) {
+		double dv[3], ud = 0.0;
+		for (int a = 0; a < 3; ++a) {
+			dv[a] = mu[3 * j + a] - mu[3 * i + a];
+			ud += u[a] * dv[a];
+		}
+		for (int a = 0; a < 3; ++a) {
+			const double ta = F / d * (dv[a] - u[a] * ud);
+			t[3 * j + a] += ta;
+			t[3 * i + a] -= ta;
+		}
+		if (g && h >= 0) {
+			g[h] += tab->step_inv * ud;
+			g[h1] -= tab->step_inv * ud;
+		}
+	}
+}
+
+/* Angle term with forward-mode tangents along mu (AngleGeometry formula). */
+static void angle_term(const adj_sys* s, int i, int j, int k, const double* x, double* f,
+					   const double* mu, double* t) {
+	dual ab[3], bc[3], ac[3];
+	for (int a = 0; a < 3; ++a) {
+		const double m_i = mu ? mu[3 * i + a] : 0.0, m_j = mu ? mu[3 * j + a] : 0.0,
+					 m_k = mu ? mu[3 * k + a] : 0.0;
+		ab[a] = dmk(min_image(x[3 * j + a] - x[3 * i + a], s->L[a]), m_j - m_i);
+		bc[a] = dmk(min_image(x[3 * k + a] - x[3 * j + a], s->L[a]), m_k - m_j);
+		ac[a] = dmk(min_image(x[3 * k + a] - x[3 * i + a], s->L[a]), m_k - m_i);
+	}
+	const dual ab2 = dadd(dadd(dmul(ab[0], ab[0]), dmul(ab[1], ab[1])), dmul(ab[2], ab[2]));
+	const dual bc2 = dadd(dadd(dmul(bc[0], bc[0]), dmul(bc[1], bc[1])), dmul(bc[2], bc[2]));
+	const dual ac2 = dadd(dadd(dmul(ac[0], ac[0]), dmul(ac[1], ac[1])), dmul(ac[2], ac[2]));
+	const dual lab = dsqrt(ab2), lbc = dsqrt(bc2);
+	dual cs = ddiv(dscale(dsub(dadd(ab2, bc2), ac2), 0.5), dmul(lab, lbc));
+	if (cs.v < -1.0) cs = dmk(-1.0, 0.0);
+	if (cs.v > 1.0) cs = dmk(1.0, 0.0);
+	const double angle = acos(cs.v);
+	dual sn = dsqrt(dsub(dmk(1.0, 0.0), dmul(cs, cs)));
+	if (sn.v <= 1e-3) sn = dmk(1e-3, 0.0);
+	int h, h1;
+	const double F = table_force(&s->angle, angle, &h, &h1);
+	const dual dudt = ddiv(dmk(-F, 0.0), sn);
+	const dual inv_ab = ddiv(dmk(1.0, 0.0), lab), inv_bc = ddiv(dmk(1.0, 0.0), lbc);
+	const dual s1 = dmul(dudt, inv_ab), c_ab = dmul(cs, inv_ab);
+	const dual s3 = dscale(dmul(dudt, inv_bc), -1.0), c_bc = dmul(cs, inv_bc);
+	for (int a = 0; a < 3; ++a) {
+		const dual f1 = dmul(s1, dadd(dmul(ab[a], c_ab), dmul(bc[a], inv_bc)));
+		const dual f3 = dmul(s3, dadd(dmul(bc[a], c_bc), dmul(ab[a], inv_ab)));
+		if (f) {
+			f[3 * i + a] += f1.v;
+			f[3 * j + a] -= f1.v + f3.v;
+			f[3 * k + a] += f3.v;
+		}
+		if (t) {
+			t[3 * i + a] += f1.d;
+			t[3 * j + a] -= f1.d + f3.d;
+			t[3 * k + a] += f3.d;
+		}
+	}
+}
+
+/* Total force (f) and, when mu is given, its tangent along mu (t) and the
+ * table gradients (gpair, gbond: mu . dforce/dU, accumulated). */
+static void forces(const adj_sys* s, const double* x, double* f, const double* mu, double* t,
+				   double* gpair, double* gbond) {
+	for (int i = 0; i < s->n; ++i)
+		for (int j = i + 1; j < s->n; ++j)
+			if (!excluded(s, i, j)) radial_term(s, &s->pair, s->cutoff, i, j, x, f, mu, t, gpair);
+	for (int b = 0; b < s->nb; ++b)
+		radial_term(s, &s->bond, 0.0, s->bonds[2 * b], s->bonds[2 * b + 1], x, f, mu, t, gbond);
+	for (int a = 0; a < s->na; ++a)
+		angle_term(s, s->angles[4 * a], s->angles[4 * a + 1], s->angles[4 * a + 2], x, f, mu, t);
+}
+
+void adj_forces64(const adj_sys* s, const double* x, double* f) {
+	memset(f, 0, sizeof(double) * 3 * (size_t)s->n);
+	forces(s, x, f, NULL, NULL, NULL, NULL);
+}
+
+/* traj: (steps + 1) * n * 3, traj[0] = x0; noise: steps * n * 3 normals. */
+void adj_forward64(const adj_sys* s, const double* x0, const double* noise, int steps,
+				   double* traj) {
+	const size_t m = 3 * (size_t)s->n;
+	double* f = (double*)malloc(sizeof(double) * m);
+	memcpy(traj, x0, sizeof(double) * m);
+	for (int k = 0; k < steps; ++k) {
+		const double* x = traj + (size_t)k * m;
+		double* y = traj + (size_t)(k + 1) * m;
+		adj_forces64(s, x, f);
+		for (size_t q = 0; q < m; ++q) {
+			const int a = (int)(q % 3);
+			double v = x[q] + s->c[a] * f[q] + s->s[a] * noise[(size_t)k * m + q];
+			v -= s->L[a] * floor(v / s->L[a]);
+			y[q] = v;
+		}
+	}
+	free(f);
+}
+
+/* lam: in lambda_N, out lambda_0; gpair / gbond accumulated. */
+void adj_backward64(const adj_sys* s, const double* traj, int steps, double* lam, double* gpair,
+					double* gbond) {
+	const size_t m = 3 * (size_t)s->n;
+	double* mu = (double*)calloc(m ? m : 1, sizeof(double));
+	double* t = (double*)malloc(sizeof(double) * m);
+	for (int k = steps - 1; k >= 0; --k) {
+		for (size_t q = 0; q < m; ++q) mu[q] = s->c[q % 3] * lam[q];
+		memset(t, 0, sizeof(double) * m);
+		forces(s, traj + (size_t)k * m, NULL, mu, t, gpair, gbond);
+		for (size_t q = 0; q < m; ++q) lam[q] += t[q];
+	}
+	free(mu);
+	free(t);
+}
+
+/* Gaussian-smoothed pair-distance histogram over non-excluded pairs with
+ * r < rmax: hist[b] += exp(-(r - r_b)^2 / (2 sigma^2)) for |r - r_b| <= 5 sigma,
+ * r_b = (b + 1/2) dr. */
+void adj_rdf64(const adj_sys* s, const double* x, int nbins, double dr, double rmax, double sigma,
+			   double* hist) {
+	memset(hist, 0, sizeof(double) * (size_t)nbins);
+	for (int i = 0; i < s->n; ++i)
+		for (int j = i + 1; j < s->n; ++j) {
+			if (excluded(s, i, j)) continue;
+			double r2 = 0.0;
+			for (int a = 0; a < 3; ++a) {
+				const double d = min_image(x[3 * j + a] - x[3 * i + a], s->L[a]);
+				r2 += d * d;
+			}
+			const double r = sqrt(r2);
+			if (!(r < rmax)) continue;
+			for (int b = 0; b < nbins; ++b) {
+				const double z = r - (b + 0.5) * dr;
+				if (fabs(z) <= 5.0 * sigma) hist[b] += exp(-z * z / (2.0 * sigma * sigma));
+			}
+		}
+}
+
+/* grad (n * 3, accumulated) of sum_b dLdh[b] hist[b] with respect to x. */
+void adj_rdf_grad64(const adj_sys* s, const double* x, int nbins, double dr, double rmax,
+					double sigma, const double* dLdh, double* grad) {
+	for (int i = 0; i < s->n; ++i)
+		for (int j = i + 1; j < s->n; ++j) {
+			if (excluded(s, i, j)) continue;
+			double r[3], r2 = 0.0;
+			for (int a = 0; a < 3; ++a) {
+				r[a] = min_image(x[3 * j + a] - x[3 * i + a], s->L[a]);
+				r2 += r[a] * r[a];
+			}
+			const double d = sqrt(r2);
+			if (!(d < rmax) || d < 1e-12) continue;
+			double dLdr = 0.0;
+			for (int b = 0; b < nbins; ++b) {
+				const double z = d - (b + 0.5) * dr;
+				if (fabs(z) <= 5.0 * sigma)
+					dLdr += dLdh[b] * exp(-z * z / (2.0 * sigma * sigma)) * (-z / (sigma * sigma));
+			}
+			for (int a = 0; a < 3; ++a) {
+				grad[3 * j + a] += dLdr * r[a] / d;
+				grad[3 * i + a] -= dLdr * r[a] / d;
+			}
+		}
+}

@@ -619,3 +619,98 @@ class RefHarness:
         out = np.zeros_like(v4)
         self.lib.ref_wrap(_ptr(o), _ptr(s), _ptr(p), _ptr(v4), _ptr(out), len(v4))
         return out
+
+
+# -- FP64 BD window and adjoint (oracle/mb2_adjoint.c) ----------------------------
+
+class AdjTable(C.Structure):
+    _fields_ = [("v", C.c_void_p), ("size", C.c_int), ("start", C.c_double),
+                ("step_inv", C.c_double), ("periodic", C.c_int)]
+
+
+class AdjSys(C.Structure):
+    _fields_ = [("n", C.c_int), ("L", C.c_double * 3), ("c", C.c_double * 3),
+                ("s", C.c_double * 3), ("pair", AdjTable), ("cutoff", C.c_double),
+                ("excl_off", C.c_void_p), ("excl_nb", C.c_void_p), ("excl_n", C.c_int),
+                ("bonds", C.c_void_p), ("nb", C.c_int), ("bond", AdjTable),
+                ("angles", C.c_void_p), ("na", C.c_int), ("angle", AdjTable)]
+
+
+class Adjoint64:
+    """FP64 forward window, RDF loss and adjoint of a BD system with one pair
+    table, one bond table and one (periodic) angle table. Keeps the arrays the
+    C structure points to alive."""
+
+    def __init__(self, oracle: "Oracle", n, box_len, diffusion, dt, kT, pair, cutoff,
+                 bonds=None, bond=None, angles=None, angle=None, exclusions=None):
+        L = self.lib = oracle.lib
+        vp = C.c_void_p
+        L.adj_forces64.argtypes = [vp, vp, vp]
+        L.adj_forward64.argtypes = [vp, vp, vp, C.c_int, vp]
+        L.adj_backward64.argtypes = [vp, vp, C.c_int, vp, vp, vp]
+        L.adj_rdf64.argtypes = [vp, vp, C.c_int, C.c_double, C.c_double, C.c_double, vp]
+        L.adj_rdf_grad64.argtypes = [vp, vp, C.c_int, C.c_double, C.c_double, C.c_double, vp, vp]
+        self.keep = []
+        s = self.sys = AdjSys()
+        s.n = int(n)
+        d = np.asarray(diffusion, np.float64).reshape(3)
+        for a in range(3):
+            s.L[a] = float(box_len[a])
+            s.c[a] = float(d[a] * dt / kT)
+            s.s[a] = float(np.sqrt(2.0 * d[a] * dt))
+        self.pair_values = self._table(s.pair, pair, False)
+        s.cutoff = float(cutoff)
+        if exclusions is not None and len(exclusions):
+            off, nb, npart = oracle.exclusion_csr(exclusions)
+            self.keep += [off, nb]
+            s.excl_off, s.excl_nb, s.excl_n = off.ctypes.data, nb.ctypes.data, int(npart)
+        if bonds is not None and len(bonds):
+            b = np.ascontiguousarray(bonds, np.int32)
+            self.keep.append(b)
+            s.bonds, s.nb = b.ctypes.data, len(b)
+            self.bond_values = self._table(s.bond, bond, False)
+        if angles is not None and len(angles):
+            a4 = np.ascontiguousarray(angles, np.int32)
+            self.keep.append(a4)
+            s.angles, s.na = a4.ctypes.data, len(a4)
+            self._table(s.angle, angle, True)
+
+    def _table(self, dst, spec, periodic):
+        """spec: (values, start, step_inv); returns the float64 values array (mutable)."""
+        v = np.ascontiguousarray(spec[0], np.float64).copy()
+        self.keep.append(v)
+        dst.v, dst.size, dst.start, dst.step_inv, dst.periodic = (
+            v.ctypes.data, len(v), float(spec[1]), float(spec[2]), int(periodic))
+        return v
+
+    def forward(self, x0, noise):
+        """x0 [n, 3] float64, noise [steps, n, 3]; returns trajectory [steps + 1, n, 3]."""
+        steps = len(noise)
+        traj = np.zeros((steps + 1, self.sys.n, 3), np.float64)
+        x0 = np.ascontiguousarray(x0, np.float64)
+        nz = np.ascontiguousarray(noise, np.float64)
+        self.lib.adj_forward64(C.byref(self.sys), x0.ctypes.data, nz.ctypes.data, steps,
+                               traj.ctypes.data)
+        return traj
+
+    def rdf(self, x, nbins, dr, rmax, sigma):
+        h = np.zeros(nbins, np.float64)
+        self.lib.adj_rdf64(C.byref(self.sys), np.ascontiguousarray(x, np.float64).ctypes.data,
+                           nbins, dr, rmax, sigma, h.ctypes.data)
+        return h
+
+    def rdf_grad(self, x, nbins, dr, rmax, sigma, dLdh):
+        g = np.zeros((self.sys.n, 3), np.float64)
+        dl = np.ascontiguousarray(dLdh, np.float64)
+        self.lib.adj_rdf_grad64(C.byref(self.sys), np.ascontiguousarray(x, np.float64).ctypes.data,
+                                nbins, dr, rmax, sigma, dl.ctypes.data, g.ctypes.data)
+        return g
+
+    def backward(self, traj, lamN):
+        """Returns (grad x0 [n, 3], grad pair table, grad bond table)."""
+        lam = np.ascontiguousarray(lamN, np.float64).copy()
+        gp = np.zeros(len(self.pair_values), np.float64)
+        gb = np.zeros(len(getattr(self, "bond_values", [0.0])), np.float64)
+        self.lib.adj_backward64(C.byref(self.sys), np.ascontiguousarray(traj).ctypes.data,
+                                len(traj) - 1, lam.ctypes.data, gp.ctypes.data, gb.ctypes.data)
+        return lam, gp, gb
