@@ -250,6 +250,48 @@ MB2_API int mb2_profile_read(mb2_context* ctx, int stage, double* total_ms, uint
  * or 32 lanes per row; 0 = choose from the mean row length. */
 MB2_API int mb2_set_lanes_per_row(mb2_context* ctx, int lanes);
 
+/* --- adjoint of a BD window ------------------------------------------------
+ * No counterpart in the reference (it computes no gradients). Gradients of a
+ * loss of the final positions of a window of BD steps with fixed Philox noise,
+ * with respect to the pair-table values, the bond-table values and the
+ * initial positions; forward with checkpoints, reverse with recomputation.
+ * Forces are minus gradients of potentials piecewise linear in a distance or
+ * angle (the tabulated lookup), so one reverse step is
+ *   lambda_k = lambda_{k+1} + J(x_k) (c * lambda_{k+1}),  c = D dt / kT,
+ * J the (symmetric) force Jacobian; table gradients accumulate in FP64.
+ * The gradient is that of the piecewise-smooth map: a pair sitting exactly on
+ * a table-bin edge (or the cutoff) contributes its one-sided derivative.
+ *
+ * mb2_window_forward: num_steps steps from first_step (the mb2_step sequence;
+ * the pairlist is rebuilt at every checkpoint), x0 in pos4 -> x_N in pos4.
+ * checkpoint_every must divide params->rebuild_period, and first_step - 1 be
+ * a multiple of checkpoint_every. Particle types without grids; no flags.
+ * params (its bond/angle pointers) and type_ids must stay valid until the
+ * backward call. */
+MB2_API int mb2_window_forward(mb2_context* ctx, float* pos4, float* force_energy4,
+                       const int* type_ids, uint32_t n, uint64_t first_step,
+                       uint32_t num_steps, uint32_t checkpoint_every,
+                       const mb2_step_params* params, void* stream);
+/* Reverse sweep of the last forward window: grad_final4 = dL/dx_N (float4
+ * rows, .w ignored) -> grad_pos0_4 = dL/dx_0; grad_pair_bins (device double,
+ * one per value of the concatenated pair tables) and grad_bond_bins (per
+ * value of the concatenated bond tables; may be NULL without bonds) are
+ * ACCUMULATED. Each segment is recomputed from its checkpoint. */
+MB2_API int mb2_window_backward(mb2_context* ctx, const float* grad_final4, float* grad_pos0_4,
+                        double* grad_pair_bins, double* grad_bond_bins, void* stream);
+/* Gaussian-smoothed pair-distance histogram of non-excluded pairs with
+ * r < r_max: hist[b] (device double [num_bins], overwritten) =
+ * sum exp(-(r - r_b)^2 / (2 sigma^2)) over |r - r_b| <= 5 sigma, r_b = (b + 1/2) dr.
+ * Builds the pairlist at r_max. */
+MB2_API int mb2_rdf_histogram(mb2_context* ctx, const float* pos4, const int* type_ids, uint32_t n,
+                      uint32_t num_bins, float bin_width, float r_max, float sigma,
+                      double* hist, void* stream);
+/* Gradient of sum_b dl_dhist[b] hist[b] with respect to the positions given
+ * to the last mb2_rdf_histogram, ACCUMULATED into grad4 (float4 rows). */
+MB2_API int mb2_rdf_backward(mb2_context* ctx, const float* pos4, uint32_t n, uint32_t num_bins,
+                     float bin_width, float r_max, float sigma, const double* dl_dhist,
+                     float* grad4, void* stream);
+
 /* --- batched replicas ------------------------------------------------------
  * Many independent periodic systems of uneven size stepped together, one
  * launch per stage for all of them. No single counterpart in the reference:

@@ -92,6 +92,10 @@ def load(path: str = LIB_PATH):
     L.mb2_profile_read.argtypes = [vp, i, C.POINTER(C.c_double), u32p]
     L.mb2_launch_count.restype = u64
     L.mb2_launch_count.argtypes = []
+    L.mb2_window_forward.argtypes = [vp, vp, vp, vp, u32, u64, u32, u32, C.POINTER(StepParams), vp]
+    L.mb2_window_backward.argtypes = [vp, vp, vp, vp, vp, vp]
+    L.mb2_rdf_histogram.argtypes = [vp, vp, vp, u32, u32, f, f, f, vp, vp]
+    L.mb2_rdf_backward.argtypes = [vp, vp, u32, u32, f, f, f, vp, vp, vp]
     L.mb2_batch_create.argtypes = [i, u32, u32p, fp, fp, C.POINTER(vp)]
     L.mb2_batch_destroy.argtypes = [vp]
     L.mb2_batch_last_error.restype = C.c_char_p

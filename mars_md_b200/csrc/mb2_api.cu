@@ -68,6 +68,20 @@ struct mb2_context {
 	std::vector<GridView> host_grids;
 	DevBuf<GridView> grids;
 
+	uint32_t bonded_bins[2] = {0, 0};  // values in the bond / angle tables
+
+	// Adjoint window: checkpoints of the forward window and reverse-sweep buffers.
+	struct Window {
+		bool valid = false;
+		uint32_t n = 0, num_steps = 0, every = 0;
+		uint64_t first_step = 0;
+		mb2_step_params prm{};
+		const int* type_ids = nullptr;
+	} win;
+	DevBuf<float4> ckpt, states, wpos, wfe, lam, mu, mu_sorted, tan, tan_sorted;
+	bool rdf_built = false;  // the current list was built by mb2_rdf_histogram
+	uint32_t rdf_n = 0;
+
 	// Optional per-stage CUDA-event timing on the launching stream.
 	bool profiling = false;
 	std::vector<std::pair<cudaEvent_t, cudaEvent_t>> prof[MB2_NUM_STAGES];
@@ -313,6 +327,7 @@ void build(mb2_context* ctx, const float4* pos, const int* type_ids, uint32_t n,
 	ctx->max_row = stats.second;
 	ctx->built = true;
 	ctx->built_n = n;
+	ctx->rdf_built = false;
 }
 
 // Pair kernel over the sorted positions into the zeroed sorted accumulator.
@@ -371,6 +386,33 @@ void upload_tables(DevBuf<Table>& tbuf, DevBuf<float>& vbuf, int num_tables, con
 	tbuf.ensure(std::max(num_tables, 1));
 	MB2_CUDA(cudaMemcpy(tbuf.ptr, host.data(), num_tables * sizeof(Table), cudaMemcpyHostToDevice));
 	if (total_out) *total_out = static_cast<uint32_t>(total);
+}
+
+// One step of the window without the rebuild decision (the segment's list
+// was built at its first step): the mb2_step sequence otherwise.
+void window_step(mb2_context* ctx, float4* pos, float4* fe, const int* type_ids, uint32_t n,
+				 uint64_t step, const mb2_step_params* prm, cudaStream_t st) {
+	const bool bonded = prm->num_bonds != 0 || prm->num_angles != 0;
+	if (bonded) MB2_CUDA(cudaMemsetAsync(fe, 0, static_cast<size_t>(n) * sizeof(float4), st));
+	pack_sorted_positions(pos, type_ids, ctx->s2o.ptr, n, ctx->sorted_pos.ptr, st);
+	pair_kernel(ctx, n, prm->cutoff, 0, st);
+	if (prm->num_bonds)
+		bond_forces(reinterpret_cast<const int2*>(prm->bonds2), prm->bond_table_idx, prm->num_bonds,
+					pos, fe, ctx->bonded_tables[0].ptr, ctx->box, 0, ctx->energy.ptr + 2, st);
+	if (prm->num_angles)
+		angle_forces(reinterpret_cast<const int4*>(prm->angles4), prm->angle_table_idx,
+					 prm->num_angles, pos, fe, ctx->bonded_tables[1].ptr, ctx->box, 0,
+					 ctx->energy.ptr + 3, st);
+	BdParams p{prm->dt, prm->kT, static_cast<uint32_t>(step),
+			   mb2_bd_seed(prm->seed, prm->patch_id, step), 0u,
+			   {prm->efield[0], prm->efield[1], prm->efield[2]}};
+	bd_integrate_gather(pos, fe, ctx->force_sorted.ptr, ctx->inv.ptr, type_ids, nullptr, n,
+						ctx->types, ctx->box, p, bonded ? 1 : 0, st);
+}
+
+void copy4(float4* dst, const float4* src, uint32_t n, cudaStream_t st) {
+	MB2_CUDA(cudaMemcpyAsync(dst, src, static_cast<size_t>(n) * sizeof(float4),
+							 cudaMemcpyDeviceToDevice, st));
 }
 
 }  // namespace
@@ -596,7 +638,7 @@ int mb2_set_bonded_tables(mb2_context* ctx, int kind, int num_tables, const floa
 		require(kind == 0 || kind == 1, MB2_ERR_ARG, "mb2_set_bonded_tables: kind is 0 or 1");
 		require(num_tables > 0, MB2_ERR_ARG, "mb2_set_bonded_tables: no tables");
 		upload_tables(ctx->bonded_tables[kind], ctx->bonded_values[kind], num_tables, values, sizes,
-					  starts, step_invs, kind == 1 ? 1 : 0, nullptr);
+					  starts, step_invs, kind == 1 ? 1 : 0, &ctx->bonded_bins[kind]);
 		ctx->bonded_count[kind] = num_tables;
 	});
 }
@@ -776,6 +818,151 @@ int mb2_step(mb2_context* ctx, float* pos4, float* force_energy4, const int* typ
 		StageScope scope(ctx, MB2_STAGE_INTEGRATE, st);
 		bd_integrate_gather(pos, fe, ctx->force_sorted.ptr, ctx->inv.ptr, type_ids, flags, n,
 							ctx->types, ctx->box, p, bonded ? 1 : 0, st);
+	});
+}
+
+int mb2_window_forward(mb2_context* ctx, float* pos4, float* force_energy4, const int* type_ids,
+					   uint32_t n, uint64_t first_step, uint32_t num_steps,
+					   uint32_t checkpoint_every, const mb2_step_params* prm, void* stream) {
+	return guarded(ctx, [&] {
+		require(prm && n > 0 && pos4 && force_energy4 && type_ids, MB2_ERR_ARG,
+				"mb2_window_forward: null argument");
+		require(ctx->types_set && ctx->types.num_grids == 0, MB2_ERR_STATE,
+				"mb2_window_forward: particle types without grids are required");
+		require(checkpoint_every > 0 && prm->rebuild_period > 0 &&
+					prm->rebuild_period % checkpoint_every == 0 &&
+					(first_step - 1) % checkpoint_every == 0,
+				MB2_ERR_ARG,
+				"mb2_window_forward: checkpoint_every must divide rebuild_period and the "
+				"window must start on a checkpoint (first_step - 1 a multiple of it)");
+		const cudaStream_t st = S(stream);
+		float4* pos = reinterpret_cast<float4*>(pos4);
+		float4* fe = reinterpret_cast<float4*>(force_energy4);
+		const uint32_t segs = (num_steps + checkpoint_every - 1) / checkpoint_every;
+		ctx->ckpt.ensure(static_cast<size_t>(std::max<uint32_t>(segs, 1)) * n);
+		for (uint32_t sgi = 0; sgi < segs; ++sgi) {
+			const uint32_t k0 = sgi * checkpoint_every;
+			const uint32_t k1 = std::min(num_steps, k0 + checkpoint_every);
+			copy4(ctx->ckpt.ptr + static_cast<size_t>(sgi) * n, pos, n, st);
+			build(ctx, pos, type_ids, n, prm->pairlist_cutoff, st);
+			for (uint32_t k = k0; k < k1; ++k)
+				window_step(ctx, pos, fe, type_ids, n, first_step + k, prm, st);
+		}
+		ctx->win.valid = true;
+		ctx->win.n = n;
+		ctx->win.num_steps = num_steps;
+		ctx->win.every = checkpoint_every;
+		ctx->win.first_step = first_step;
+		ctx->win.prm = *prm;
+		ctx->win.type_ids = type_ids;
+	});
+}
+
+int mb2_window_backward(mb2_context* ctx, const float* grad_final4, float* grad_pos0_4,
+						double* grad_pair_bins, double* grad_bond_bins, void* stream) {
+	return guarded(ctx, [&] {
+		require(ctx->win.valid, MB2_ERR_STATE, "mb2_window_backward: no forward window");
+		require(grad_final4 && grad_pos0_4 && grad_pair_bins, MB2_ERR_ARG,
+				"mb2_window_backward: null argument");
+		const auto& w = ctx->win;
+		const mb2_step_params* prm = &w.prm;
+		require(prm->num_bonds == 0 || grad_bond_bins, MB2_ERR_ARG,
+				"mb2_window_backward: bond-table gradient output needed");
+		const cudaStream_t st = S(stream);
+		const uint32_t n = w.n, C = w.every;
+		const uint32_t segs = (w.num_steps + C - 1) / C;
+		ctx->states.ensure(static_cast<size_t>(C) * n);
+		for (auto* b : {&ctx->wpos, &ctx->wfe, &ctx->lam, &ctx->mu, &ctx->mu_sorted, &ctx->tan,
+						&ctx->tan_sorted})
+			b->ensure(n);
+		copy4(ctx->lam.ptr, reinterpret_cast<const float4*>(grad_final4), n, st);
+		AdjointStepArgs a{};
+		a.n = n;
+		a.type_ids = w.type_ids;
+		a.diffusion = ctx->types.diffusion;
+		a.dt_over_kT = prm->dt / prm->kT;
+		a.tables = ctx->pt;
+		a.box = ctx->box;
+		a.cutoff_sq = prm->cutoff > 0.0f ? prm->cutoff * prm->cutoff : 0.0f;
+		a.bonds = reinterpret_cast<const int2*>(prm->bonds2);
+		a.bond_table_idx = prm->bond_table_idx;
+		a.num_bonds = prm->num_bonds;
+		a.bond_tables = ctx->bonded_tables[0].ptr;
+		a.bond_values_base = ctx->bonded_values[0].ptr;
+		a.bond_bins = ctx->bonded_bins[0];
+		a.angles = reinterpret_cast<const int4*>(prm->angles4);
+		a.angle_table_idx = prm->angle_table_idx;
+		a.num_angles = prm->num_angles;
+		a.angle_tables = ctx->bonded_tables[1].ptr;
+		a.lam = ctx->lam.ptr;
+		a.mu = ctx->mu.ptr;
+		a.mu_sorted = ctx->mu_sorted.ptr;
+		a.tan = ctx->tan.ptr;
+		a.tan_sorted = ctx->tan_sorted.ptr;
+		a.grad_pair = grad_pair_bins;
+		a.grad_bond = grad_bond_bins;
+		for (uint32_t sgi = segs; sgi-- > 0;) {
+			const uint32_t k0 = sgi * C;
+			const uint32_t k1 = std::min(w.num_steps, k0 + C);
+			// Recompute the segment from its checkpoint, keeping every state.
+			copy4(ctx->wpos.ptr, ctx->ckpt.ptr + static_cast<size_t>(sgi) * n, n, st);
+			build(ctx, ctx->wpos.ptr, w.type_ids, n, prm->pairlist_cutoff, st);
+			for (uint32_t k = k0; k < k1; ++k) {
+				copy4(ctx->states.ptr + static_cast<size_t>(k - k0) * n, ctx->wpos.ptr, n, st);
+				if (k + 1 < k1)
+					window_step(ctx, ctx->wpos.ptr, ctx->wfe.ptr, w.type_ids, n, w.first_step + k,
+								prm, st);
+			}
+			a.lanes = ctx->lanes;
+			a.cap = ctx->cap;
+			a.inv = ctx->inv.ptr;
+			a.nbr = ctx->nbr.ptr;
+			a.row_len = ctx->row_len.ptr;
+			a.sorted_pos = ctx->sorted_pos.ptr;
+			for (uint32_t k = k1; k-- > k0;) {
+				const float4* xk = ctx->states.ptr + static_cast<size_t>(k - k0) * n;
+				pack_sorted_positions(xk, w.type_ids, ctx->s2o.ptr, n, ctx->sorted_pos.ptr, st);
+				a.pos = xk;
+				adjoint_step(a, st);
+			}
+		}
+		copy4(reinterpret_cast<float4*>(grad_pos0_4), ctx->lam.ptr, n, st);
+		ctx->win.valid = true;
+	});
+}
+
+int mb2_rdf_histogram(mb2_context* ctx, const float* pos4, const int* type_ids, uint32_t n,
+					  uint32_t num_bins, float bin_width, float r_max, float sigma, double* hist,
+					  void* stream) {
+	return guarded(ctx, [&] {
+		require(n > 0 && pos4 && type_ids && hist && num_bins > 0 && num_bins <= 4096 &&
+					bin_width > 0.0f && sigma > 0.0f && r_max > 0.0f,
+				MB2_ERR_ARG, "mb2_rdf_histogram: bad arguments");
+		const cudaStream_t st = S(stream);
+		build(ctx, reinterpret_cast<const float4*>(pos4), type_ids, n, r_max, st);
+		MB2_CUDA(cudaMemsetAsync(hist, 0, num_bins * sizeof(double), st));
+		rdf_pairs(ctx->sorted_pos.ptr, ctx->nbr.ptr, ctx->row_len.ptr, n, ctx->cap, ctx->lanes,
+				  ctx->box, num_bins, bin_width, r_max, sigma, hist, nullptr, nullptr, st);
+		ctx->rdf_built = true;
+		ctx->rdf_n = n;
+	});
+}
+
+int mb2_rdf_backward(mb2_context* ctx, const float* pos4, uint32_t n, uint32_t num_bins,
+					 float bin_width, float r_max, float sigma, const double* dl_dhist,
+					 float* grad4, void* stream) {
+	return guarded(ctx, [&] {
+		require(ctx->rdf_built && ctx->rdf_n == n, MB2_ERR_STATE,
+				"mb2_rdf_backward: call mb2_rdf_histogram on these positions first");
+		require(pos4 && dl_dhist && grad4 && num_bins > 0 && num_bins <= 4096, MB2_ERR_ARG,
+				"mb2_rdf_backward: bad arguments");
+		const cudaStream_t st = S(stream);
+		ctx->tan_sorted.ensure(n);
+		MB2_CUDA(cudaMemsetAsync(ctx->tan_sorted.ptr, 0, static_cast<size_t>(n) * sizeof(float4), st));
+		rdf_pairs(ctx->sorted_pos.ptr, ctx->nbr.ptr, ctx->row_len.ptr, n, ctx->cap, ctx->lanes,
+				  ctx->box, num_bins, bin_width, r_max, sigma, nullptr, dl_dhist,
+				  ctx->tan_sorted.ptr, st);
+		gather_add(reinterpret_cast<float4*>(grad4), ctx->tan_sorted.ptr, ctx->inv.ptr, n, st);
 	});
 }
 

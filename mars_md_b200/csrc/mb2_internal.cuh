@@ -249,6 +249,52 @@ void bd_integrate_systems(float4* pos, float4* fe, const float4* force_sorted,
 						  const uint32_t* offsets, const Box* boxes, uint32_t n,
 						  const TypeTable& types, float dt, float kT, uint64_t seed,
 						  uint64_t patch_id, const unsigned long long* step_ptr, cudaStream_t st);
+// adjoint.cu: one reverse BD step, lambda += J(x_k)^T (c * lambda) (J symmetric:
+// the directional derivative of the force along mu = c * lambda), with table
+// gradients accumulated in FP64. Positions are x_k, in both orders.
+struct AdjointStepArgs {
+	uint32_t n;
+	int lanes;
+	uint32_t cap;
+	const float4* pos;         // x_k, original order
+	const float4* sorted_pos;  // x_k in sorted order (type id in .w)
+	const int* type_ids;
+	const float4* diffusion;   // per type
+	float dt_over_kT;
+	const uint32_t* inv;
+	const uint32_t* nbr;
+	const uint32_t* row_len;
+	PairTables tables;
+	Box box;
+	float cutoff_sq;
+	const int2* bonds;
+	const int* bond_table_idx;
+	uint32_t num_bonds;
+	const Table* bond_tables;
+	const float* bond_values_base;
+	uint32_t bond_bins;
+	const int4* angles;
+	const int* angle_table_idx;
+	uint32_t num_angles;
+	const Table* angle_tables;
+	float4* lam;  // in: lambda_{k+1}; out: lambda_k
+	float4* mu;
+	float4* mu_sorted;
+	float4* tan;
+	float4* tan_sorted;
+	double* grad_pair;  // [total pair bins], accumulated
+	double* grad_bond;  // [total bond bins], accumulated
+};
+void adjoint_step(const AdjointStepArgs& a, cudaStream_t st);
+// Smoothed pair-distance histogram over the list (grad_sorted == nullptr:
+// into hist), or the gradient of sum dldh * hist into grad_sorted.
+void rdf_pairs(const float4* sorted_pos, const uint32_t* nbr, const uint32_t* row_len, uint32_t n,
+			   uint32_t cap, int lanes, const Box& box, uint32_t bins, float dr, float r_max,
+			   float sigma, double* hist, const double* dldh, float4* grad_sorted,
+			   cudaStream_t st);
+// grad[o] += src_sorted[inv[o]].
+void gather_add(float4* grad, const float4* src_sorted, const uint32_t* inv, uint32_t n,
+				cudaStream_t st);
 // Device step counter: set to `value`, or add `value` (one-thread launches).
 void step_counter_set(unsigned long long* ptr, uint64_t value, cudaStream_t st);
 void step_counter_add(unsigned long long* ptr, uint64_t value, cudaStream_t st);
