@@ -233,11 +233,14 @@ def run_ours(args):
         "gpu_launches": launches,
         "clocks": clk,
     }
-    if world == 1 and not args.no_batched:
+    if world == 1 and not (args.no_batched and args.no_adjoint):
         del dev
         ctx.close()
         torch.cuda.empty_cache()
-        out["batched"] = run_batched(local)
+        if not args.no_batched:
+            out["batched"] = run_batched(local)
+        if not args.no_adjoint:
+            out["adjoint"] = run_adjoint(local)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         out["cpu_baseline"] = cpu_baseline(w)
     if world > 1:
@@ -313,6 +316,57 @@ def run_batched(local, period_steps=20):
                         "period 20, seeded synthetic"}
 
 
+def run_adjoint(local, steps=200, every=20):
+    """16 chains x 1,024 beads (bonds, angles, exclusions, WCA table), a 200-step window
+    with fixed Philox noise, checkpoints every 20 steps; loss = squared error of the
+    smoothed pair-distance histogram (100 bins on [0, 25) A) against a target made with
+    the pair table perturbed (sigma 4 -> 4.2 A). Times the forward window and the
+    adjoint (histogram gradient + recompute + reverse sweep) with CUDA events."""
+    import torch
+    from mars_md_b200 import workloads as W
+    from mars_md_b200.adjoint import Window
+
+    device = f"cuda:{local}"
+    stream = torch.cuda.current_stream()
+    w = W.adjoint()
+    rng = np.random.default_rng(W.DEFAULT_SEED)
+    w.pos[:, :3] = np.mod(w.pos[:, :3] + rng.normal(scale=0.02, size=(w.n, 3)),
+                          w.box_size[0]).astype(np.float32)
+    win = Window(w, steps, checkpoint_every=every, device=device)
+    pos0 = win.dev["pos"].clone()
+    pv, bv = win.pair_values().float(), win.bond_values().float()
+    # Target from the perturbed table.
+    win.set_tables(torch.from_numpy(W.wca_table(sigma=4.2).values).to(device), bv)
+    target = win.histogram(win.forward(pos0)) * win.norm
+    win.set_tables(pv, bv)
+    e = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+    for rep in range(2):  # the first repetition warms up
+        e[0].record(stream)
+        xn = win.forward(pos0)
+        e[1].record(stream)
+        hist = win.histogram(xn)
+        dldh = 2.0 * (hist * win.norm - target) * win.norm
+        e[2].record(stream)
+        lam = win.histogram_backward(xn, dldh)
+        g0, gp, gb = win.backward(lam)
+        e[3].record(stream)
+        torch.cuda.synchronize()
+    fwd_ms, bwd_ms = e[0].elapsed_time(e[1]), e[2].elapsed_time(e[3])
+    loss = float(win.loss_of(hist, target).item())
+    win.close()
+    return {"metric": "adjoint step / forward step (device time)", "beads": w.n,
+            "window_steps": steps, "checkpoint_every": every,
+            "forward_ms_per_step": fwd_ms / steps, "adjoint_ms_per_step": bwd_ms / steps,
+            "ratio": bwd_ms / fwd_ms,
+            "forward_particle_steps_per_s": w.n * steps / (fwd_ms / 1e3),
+            "adjoint_particle_steps_per_s": w.n * steps / (bwd_ms / 1e3),
+            "loss": loss, "grad_norms": {"positions": float(g0.norm().item()),
+                                         "pair_table": float(gp.norm().item()),
+                                         "bond_table": float(gb.norm().item())},
+            "workload": "16 chains x 1,024 beads, one type, WCA table, harmonic bonds and "
+                        "angles, 1-2/1-3 exclusions, box 378 A, seeded synthetic"}
+
+
 def cpu_baseline(w):
     """The reference's CPU path on a bounded sample (about 10-30 s of CPU work)."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
@@ -367,6 +421,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-batched", action="store_true",
                     help="skip the batched-replicas measurement")
+    ap.add_argument("--no-adjoint", action="store_true",
+                    help="skip the adjoint-window measurement")
     ap.add_argument("--lanes", type=int, default=0,
                     help="lanes per pairlist row in the pair kernel (0 = automatic)")
     args = ap.parse_args()
