@@ -340,6 +340,9 @@ uint64_t or_neighbor_walk(const float* sorted_pos4, const uint32_t* keys, const 
                           const int* rigid_body_id, int* pairs, uint64_t max_pairs,
                           uint64_t* checksum) {
 	uint64_t count = 0, sum = 0;
+	/* Without a pair buffer only the count and the (order-independent) hash
+	 * sum are wanted, so particles may be walked in parallel. */
+#pragma omp parallel for reduction(+ : count, sum) schedule(dynamic, 4096) if (pairs == NULL)
 	for (size_t i = 0; i < n; ++i) {
 		const float* pi = sorted_pos4 + 4 * i;
 		const uint32_t cell = keys[i] >> shift;
