@@ -40,7 +40,7 @@ def _rank_main(rank, world, port, out):
 
 def test_two_rank_replicas_time_on_the_slowest_rank():
     world = 2
-    mgr = mp.Manager()
+    mgr = mp.get_context("spawn").Manager()
     out = mgr.dict()
     mp.start_processes(_rank_main, args=(world, _free_port(), out), nprocs=world,
                        start_method="spawn", join=True)
