@@ -185,7 +185,21 @@ __global__ void __launch_bounds__(256) pair_force_kernel(
 	const uint32_t* col = nbr + (static_cast<size_t>(i / H) * cap) * H + (i % H);
 	float fx = 0.0f, fy = 0.0f, fz = 0.0f, fe = 0.0f;
 	double e_acc = 0.0, w_acc = 0.0;
-	for (uint32_t t = sub; t < cnt; t += G) {
+	// Two entries per lane per iteration: both neighbour gathers are in flight
+	// before either pair's arithmetic (the kernel is bound by gather latency).
+	uint32_t t = sub;
+	for (; t + G < cnt; t += 2 * G) {
+		const uint32_t e0 = __ldcs(col + static_cast<size_t>(t) * H);
+		const uint32_t e1 = __ldcs(col + static_cast<size_t>(t + G) * H);
+		const uint32_t j0 = e0 & ~kOrientBit, j1 = e1 & ~kOrientBit;
+		const float4 p0 = sorted_pos[j0];
+		const float4 p1 = sorted_pos[j1];
+		pair_scalar<kEnergy, kAllPeriodic>(pi, p0, j0, e0 & kOrientBit, trow, bin_f, bin_e, box,
+										   cutoff_sq, force, fx, fy, fz, fe, e_acc, w_acc);
+		pair_scalar<kEnergy, kAllPeriodic>(pi, p1, j1, e1 & kOrientBit, trow, bin_f, bin_e, box,
+										   cutoff_sq, force, fx, fy, fz, fe, e_acc, w_acc);
+	}
+	if (t < cnt) {
 		const uint32_t entry = __ldcs(col + static_cast<size_t>(t) * H);
 		const uint32_t j = entry & ~kOrientBit;
 		pair_scalar<kEnergy, kAllPeriodic>(pi, sorted_pos[j], j, entry & kOrientBit, trow, bin_f,
