@@ -963,3 +963,67 @@ void or_bd_integrate(float* pos4, float* fe4, const int* type_ids, const uint32_
 				p[a] = or_wrap_scalar(p[a], b->origin[a], b->size[a]);
 	}
 }
+
+/* FORCE_CONVERSION_FACTOR and SQRT_CAL_TO_JOULE (src/Constants.h:30,34). */
+#define OR_FORCE_CONVERSION 4.18679994e4f
+#define OR_SQRT_CAL_TO_JOULE 2.046167337f
+
+static void half_kick(float* m, const float* f, float dt) {
+	const float h = 0.5f * dt;
+	for (int a = 0; a < 3; ++a) m[a] = m[a] + (h * f[a]) * OR_FORCE_CONVERSION;
+}
+
+void or_baoab_integrate(float* pos4, float* mom4, float* fe4, const int* type_ids,
+                        const uint32_t* flags, size_t n, const or_types* types,
+                        const or_grid* grids, const float* mass, const float* damping3,
+                        const or_box* b, float dt, float kT, uint64_t step, uint64_t base_seed,
+                        uint32_t base_ctr, const float* efield, int pending) {
+	if (grids)
+		for (size_t i = 0; i < n; ++i) {
+			float pmf[4];
+			or_position_force(pos4 + 4 * i, type_ids[i], types, grids, efield, pmf);
+			for (int a = 0; a < 4; ++a) fe4[4 * i + a] += pmf[a];
+		}
+	for (size_t i = 0; i < n; ++i) {
+		if (flags && (flags[i] & 4u))
+			continue;
+		float* p = pos4 + 4 * i;
+		float* m = mom4 + 4 * i;
+		const float* f = fe4 + 4 * i;
+		const int type = type_ids[i];
+		const float ms = mass[type];
+		const float* g = damping3 + 3 * type;
+		if (pending) half_kick(m, f, dt);
+		half_kick(m, f, dt); /* B */
+		const float h = 0.5f * dt;
+		/* Vector3 / s multiplies by 1 / s (Vector3.h:194-197). */
+		const float inv_m = 1.0f / ms;
+		for (int a = 0; a < 3; ++a) p[a] = p[a] + ((h * m[a]) * inv_m) * 10000.0f; /* A */
+		uint32_t u[4];
+		or_philox4x32_10(base_seed, base_ctr + (uint32_t)i, 0x1356914u, (uint32_t)step, 0u, u);
+		const float ux = or_u01(u[0]), uy = or_u01(u[1]), uz = or_u01(u[2]), uw = or_u01(u[3]);
+		const float r1 = sqrtf(-2.0f * logf(ux));
+		const float theta1 = 2.0f * 3.1415926535f * uy;
+		const float r2 = sqrtf(-2.0f * logf(uz));
+		const float theta2 = 2.0f * 3.1415926535f * uw;
+		const float xi[3] = {r1 * cosf(theta1), r1 * sinf(theta1), r2 * cosf(theta2)};
+		for (int a = 0; a < 3; ++a) { /* O */
+			const float c = expf(-g[a] * dt);
+			const float ns = sqrtf(kT * ms * (1.0f - c * c)) * OR_SQRT_CAL_TO_JOULE;
+			m[a] = c * m[a] + ns * xi[a];
+		}
+		for (int a = 0; a < 3; ++a) p[a] = p[a] + ((h * m[a]) * inv_m) * 10000.0f; /* A */
+		for (int a = 0; a < 3; ++a)
+			if (b->periodic[a])
+				p[a] = or_wrap_scalar(p[a], b->origin[a], b->size[a]);
+	}
+}
+
+void or_baoab_last_update(float* mom4, const float* fe4, const uint32_t* flags, size_t n,
+                          float dt) {
+	for (size_t i = 0; i < n; ++i) {
+		if (flags && (flags[i] & 4u))
+			continue;
+		half_kick(mom4 + 4 * i, fe4 + 4 * i, dt);
+	}
+}

@@ -136,6 +136,20 @@ void or_philox4x32_10(uint64_t seed, uint32_t ctr0, uint32_t ctr1, uint32_t ctr2
                       uint32_t internal, uint32_t* out4);
 float or_u01(uint32_t x);
 uint64_t or_bd_seed(uint64_t seed, uint64_t patch_id, uint64_t step);
+/* Langevin BAOAB step (Integrator/BAOAB.h:47-128) with the passes that
+ * Patch::integrate_motion runs before it (Patch.cpp:290-335): with grids, the
+ * position-dependent force is accumulated into ForceEnergy for every particle
+ * (ComputePMFKernel, Pmf.h:126-152); with a pending deferred kick, the closing
+ * half-kick (BAOAB_LastUpdate, BAOAB.h:167-186) runs first. mass[T],
+ * damping3[T*3]; grids may be NULL (no PMF pass). */
+void or_baoab_integrate(float* pos4, float* mom4, float* fe4, const int* type_ids,
+                        const uint32_t* flags, size_t n, const or_types* types,
+                        const or_grid* grids, const float* mass, const float* damping3,
+                        const or_box* b, float dt, float kT, uint64_t step, uint64_t base_seed,
+                        uint32_t base_ctr, const float* efield, int pending);
+/* BAOAB_LastUpdate alone (Patch::finish_deferred_kick, Patch.cpp:354-373). */
+void or_baoab_last_update(float* mom4, const float* fe4, const uint32_t* flags, size_t n,
+                          float dt);
 void or_bd_integrate(float* pos4, float* fe4, const int* type_ids, const uint32_t* flags, size_t n,
                      const or_types* types, const or_grid* grids, const or_box* b, float dt,
                      float kT, uint64_t step, uint64_t base_seed, uint32_t base_ctr,

@@ -416,6 +416,27 @@ class Oracle:
         return pos, fe, noise
 
 
+def _oracle_baoab(self, pos4, mom4, fe4, type_ids, flags, types: "TypeSet", grids, mass, damping,
+                  box: Box, dt, kT, step, base_seed, base_ctr=0, efield=(0, 0, 0), pending=0):
+    """Langevin BAOAB step on copies; returns (pos4, mom4, fe4)."""
+    L = self.lib
+    vp = C.c_void_p
+    L.or_baoab_integrate.argtypes = [vp, vp, vp, vp, vp, C.c_size_t, vp, vp, vp, vp, vp, C.c_float,
+                                     C.c_float, C.c_uint64, C.c_uint64, C.c_uint32, vp, C.c_int]
+    pos, mom, fe = (np.array(a, np.float32) for a in (pos4, mom4, fe4))
+    ms = np.ascontiguousarray(mass, np.float32)
+    dmp = np.ascontiguousarray(damping, np.float32).reshape(-1, 3)
+    L.or_baoab_integrate(_ptr(pos), _ptr(mom), _ptr(fe), _ptr(np.ascontiguousarray(type_ids, np.int32)),
+                         _ptr(flags), len(pos), C.byref(types.struct),
+                         grids.ptr() if grids is not None else None, _ptr(ms), _ptr(dmp),
+                         C.byref(box), C.c_float(dt), C.c_float(kT), step, base_seed, base_ctr,
+                         _ptr(np.asarray(efield, np.float32)), int(pending))
+    return pos, mom, fe
+
+
+Oracle.baoab_integrate = _oracle_baoab
+
+
 class RefGrid(C.Structure):
     _fields_ = [("data", C.c_void_p), ("origin", C.c_float * 3), ("basis", C.c_float * 9),
                 ("basis_inv", C.c_float * 9), ("dims", C.c_int64 * 3),
@@ -593,6 +614,36 @@ class RefHarness:
                                   base_seed, base_ctr, _ptr(np.asarray(efield, np.float32)),
                                   nthreads)
         return pos, fe
+
+    def baoab_integrate(self, pos4, mom4, fe4, type_ids, flags, types: TypeSet, grids, mass,
+                        damping, box: Box, dt, kT, step, base_seed, base_ctr=0, efield=(0, 0, 0),
+                        pending=0):
+        vp, f = C.c_void_p, C.c_float
+        self.lib.ref_baoab_integrate.argtypes = [vp, vp, vp, vp, vp, C.c_size_t, C.c_int, vp, vp, vp,
+                                                 vp, vp, vp, C.c_int, vp, vp, vp, C.c_int, vp, vp,
+                                                 vp, f, f, C.c_uint64, C.c_uint64, C.c_uint32, vp,
+                                                 C.c_int]
+        pos, mom, fe = (np.array(a, np.float32) for a in (pos4, mom4, fe4))
+        o, s, p = self._box(box)
+        tid = np.ascontiguousarray(type_ids, np.int32)
+        fl = np.zeros(len(pos), np.uint32) if flags is None else np.ascontiguousarray(flags, np.uint32)
+        ms = np.ascontiguousarray(mass, np.float32)
+        d4 = np.zeros((len(ms), 4), np.float32)
+        d4[:, :3] = np.asarray(damping, np.float32).reshape(-1, 3)
+        rg, ng = None, 0
+        if grids is not None and grids.n:
+            rg = (RefGrid * grids.n)()
+            for k in range(grids.n):
+                C.memmove(C.byref(rg[k]), C.byref(grids.structs[k]), C.sizeof(RefGrid))
+            ng = grids.n
+        self.lib.ref_baoab_integrate(
+            _ptr(pos), _ptr(mom), _ptr(fe), _ptr(tid), _ptr(fl), len(pos), len(types.charge),
+            _ptr(types.charge), _ptr(ms), _ptr(d4), _ptr(types.pmf_offset), _ptr(types.pmf_count),
+            _ptr(types.terms_flat), types.n_terms, _ptr(types.force_grid_id4),
+            _ptr(types.force_grid_scale4), C.cast(rg, C.c_void_p) if rg is not None else None, ng,
+            _ptr(o), _ptr(s), _ptr(p), f(dt), f(kT), step, base_seed, base_ctr,
+            _ptr(np.asarray(efield, np.float32)), int(pending))
+        return pos, mom, fe
 
     def philox_int4(self, seed, ctr, global_seed, ctr1, ndraw=1):
         out = np.zeros((ndraw, 4), np.uint32)

@@ -17,6 +17,7 @@
 
 #include "Interactions/Bonded/BondComputer.h"
 #include "Interactions/Nonbonded/Pairwise.h"
+#include "PatchOperation/Integrator/BAOAB.h"
 #include "PatchOperation/Integrator/BD.h"
 #include "PatchOperation/PairListKernels/ZOrderNeighbor.h"
 #include "PatchOperation/ZOrderKernels/ZOrderKernels.h"
@@ -336,6 +337,70 @@ void ref_bd_integrate(float* pos4, float* fe4, int* type_ids, uint32_t* flags, s
 						 base_ctr, n_grids > 0 ? views.data() : nullptr,
 						 Vector3(efield[0], efield[1], efield[2]), InterpolationOrder::Linear);
 	run_chunked(n, nthreads, [&](size_t i) { k(i); });
+}
+
+// Patch::integrate_motion's Langevin branch (Patch.cpp:290-335): ComputePMFKernel
+// (Pmf.h:126-152) when grids exist, BAOAB_LastUpdate when a kick is pending,
+// then BAOABIntegrate<float> (BAOAB.h:47-128).
+void ref_baoab_integrate(float* pos4, float* mom4, float* fe4, int* type_ids, uint32_t* flags,
+						 size_t n, int num_types, const float* charge, const float* mass,
+						 const float* damping4, const int* pmf_offset, const int* pmf_count,
+						 const float* pmf_terms4, int n_terms, const int* force_grid_id4,
+						 const float* force_grid_scale4, const RefGrid* grids, int n_grids,
+						 const float* origin, const float* size, const int* periodic, float dt,
+						 float kT, uint64_t step, uint64_t base_seed, uint32_t base_ctr,
+						 const float* efield, int pending) {
+	std::vector<GridTerm> terms(n_terms);
+	for (int t = 0; t < n_terms; ++t) {
+		terms[t].grid_id = static_cast<int>(pmf_terms4[4 * t + 0]);
+		terms[t].scale = pmf_terms4[4 * t + 1];
+		terms[t].scale_slope = pmf_terms4[4 * t + 2];
+		terms[t].boundary_condition = static_cast<int>(pmf_terms4[4 * t + 3]);
+	}
+	std::vector<BaseGridView<float>> views(n_grids);
+	for (int g = 0; g < n_grids; ++g) {
+		auto& v = views[g];
+		v.origin = Vector3(grids[g].origin[0], grids[g].origin[1], grids[g].origin[2]);
+		const float* b = grids[g].basis;
+		const float* bi = grids[g].basis_inv;
+		v.basis = Matrix3(Vector3(b[0], b[1], b[2]), Vector3(b[3], b[4], b[5]),
+						  Vector3(b[6], b[7], b[8]));
+		v.basis_inv = Matrix3(Vector3(bi[0], bi[1], bi[2]), Vector3(bi[3], bi[4], bi[5]),
+							  Vector3(bi[6], bi[7], bi[8]));
+		v.dimensions = Vector3_t<idx_t>(grids[g].dims[0], grids[g].dims[1], grids[g].dims[2]);
+		v.grid_id = g;
+		v.boundary_condition = grids[g].boundary_condition;
+		v.data = grids[g].data;
+	}
+	ParticleView pv{};
+	pv.type_id = type_ids;
+	pv.pos = reinterpret_cast<Vector3*>(pos4);
+	pv.mom = reinterpret_cast<Vector3*>(mom4);
+	pv.ForceEnergy = reinterpret_cast<Vector3*>(fe4);
+	pv.flags = flags;
+	ParticleTypeView tv{};
+	tv.charge = charge;
+	tv.mass = mass;
+	tv.trans_damping = reinterpret_cast<const Vector3*>(damping4);
+	tv.pmf_grid_offset = pmf_offset;
+	tv.pmf_grid_count = pmf_count;
+	tv.pmf_grid_terms = terms.data();
+	tv.force_grid_id = reinterpret_cast<const int3*>(force_grid_id4);
+	tv.force_grid_scale = reinterpret_cast<const Vector3*>(force_grid_scale4);
+	const BaseGridView<float>* gv = n_grids > 0 ? views.data() : nullptr;
+	const Vector3 e(efield[0], efield[1], efield[2]);
+	if (gv) {
+		const ComputePMFKernel pmf{e, InterpolationOrder::Linear};
+		for (size_t i = 0; i < n; ++i) pmf(i, pv, tv, gv, static_cast<idx_t>(n));
+	}
+	if (pending) {
+		BAOAB_LastUpdate<float> last(pv, tv, dt, step, kT, n, base_seed, base_ctr, gv, e,
+									 InterpolationOrder::Linear);
+		for (size_t i = 0; i < n; ++i) last(i);
+	}
+	BAOABIntegrate<float> k(pv, tv, make_box(origin, size, periodic), dt, step, kT, n, base_seed,
+							base_ctr, gv, e, InterpolationOrder::Linear);
+	for (size_t i = 0; i < n; ++i) k(i);
 }
 
 // openrand::Philox::draw_int4 (philox.h:60-127), `ndraw` consecutive draws.

@@ -11,7 +11,7 @@ reference checkout.
 
 Run from the repository root, where the reference checkout is available:
 
-    make -C oracle/ref_harness && python tests/golden/make_golden.py
+    make -C oracle/ref_harness && python tests/golden/make_golden.py [case ...]
 
 The fixtures pin the C restatement in ``oracle/`` (tests/test_oracle_golden.py)
 and, through it, the CUDA path.
@@ -253,15 +253,62 @@ def wrap_table(O, R):
                 angle_x=xs_ang, angle_lookup=lookup(ang, xs_ang, True))
 
 
+def baoab(O, R):
+    """One Langevin BAOAB step (BAOABIntegrate, with the PMF pass and the
+    deferred closing half-kick of Patch::integrate_motion) on 3,000 particles of
+    two types with masses and per-axis damping, a 32^3 PMF grid, an electric
+    field and frozen particles; once with and once without a pending kick."""
+    rng = np.random.default_rng(SEED + 4)
+    n, L = 3000, 64.0
+    pos = np.zeros((n, 4), np.float32)
+    pos[:, :3] = rng.uniform(0.0, L, size=(n, 3)).astype(np.float32)
+    mom = np.zeros((n, 4), np.float32)
+    mom[:, :3] = rng.normal(0.0, 5.0, size=(n, 3)).astype(np.float32)
+    fe = np.zeros((n, 4), np.float32)
+    fe[:, :3] = rng.normal(0.0, 2.0, size=(n, 3)).astype(np.float32)
+    types = rng.integers(0, 2, size=n).astype(np.int32)
+    c = np.arange(32, dtype=np.float64)
+    gx, gy, gz = np.meshgrid(c, c, c, indexing="ij")
+    data = (2.0 * np.sin(gx / 5.0) * np.cos(gy / 7.0) + 0.05 * (gz - 16.0) ** 2).astype(np.float32)
+    gs = po.GridSet([dict(data=data, origin=(16.0, 16.0, 16.0), basis=np.eye(3, dtype=np.float32),
+                          boundary_condition=0)])
+    ty = po.TypeSet(np.array([0.5, -1.0], np.float32),
+                    np.array([[150.0, 150.0, 150.0], [80.0, 90.0, 100.0]], np.float32),
+                    [[(0, 1.0, 0.0, -1)], [(0, 1.5, 0.0, -1)]])
+    mass = np.array([12.0, 40.0], np.float32)
+    damping = np.array([[50.0, 50.0, 50.0], [20.0, 30.0, 40.0]], np.float32)
+    flags = np.zeros(n, np.uint32)
+    flags[::97] = FLAG_RB_ATTACHED
+    box = po.Box.make((0.0, 0.0, 0.0), (L, L, L))
+    efield = (0.0, 0.0, 0.1)
+    step = 5
+    seed = O.bd_seed(SEED, 0, step)
+    out = {}
+    for pending in (0, 1):
+        p1, m1, f1 = R.baoab_integrate(pos, mom, fe, types, flags, ty, gs, mass, damping, box,
+                                       W.DT_NS, W.kT(), step, seed, efield=efield, pending=pending)
+        out.update({f"pos_after_{pending}": p1, f"mom_after_{pending}": m1,
+                    f"fe_after_{pending}": f1})
+    return dict(pos=pos, mom=mom, fe=fe, type_ids=types, flags=flags, grid=data,
+                grid_origin=np.float32([16.0, 16.0, 16.0]), charge=ty.charge,
+                diffusion=ty.diffusion4, pmf_scale=np.float32([1.0, 1.5]), mass=mass,
+                damping=damping, efield=np.float32(efield), step=np.int64(step),
+                seed=np.uint64(seed), dt=np.float32(W.DT_NS), kT=np.float32(W.kT()),
+                **_box_arrays(box.origin, box.size, box.periodic), **out)
+
+
 CASES = {"uniform4096": uniform, "lattice_open": lattice, "polymer_excl": polymer,
-         "chain129": chain, "philox": philox, "grid_bd": grid_bd, "wrap_table": wrap_table}
+         "chain129": chain, "philox": philox, "grid_bd": grid_bd, "wrap_table": wrap_table,
+         "baoab": baoab}
 
 
 def main():
     if not po.ref_available():
         sys.exit("reference harness not built: make -C oracle/ref_harness")
     O, R = po.Oracle(), po.RefHarness()
-    for name, fn in CASES.items():
+    names = sys.argv[1:] or list(CASES)
+    for name in names:
+        fn = CASES[name]
         data = fn(O, R)
         path = os.path.join(HERE, f"{name}.npz")
         np.savez_compressed(path, **data)

@@ -130,3 +130,25 @@ def test_noise_keyed_on_absolute_step(oracle):
     assert np.array_equal(_noise(oracle, 64, 7, 6), _noise(oracle, 64, 7, 6))
     assert not np.array_equal(_noise(oracle, 64, 7, 6), _noise(oracle, 64, 7, 7))
     assert oracle.bd_seed(7, 0, 6) != oracle.bd_seed(7, 1, 6)
+
+
+def test_baoab_momentum_reaches_equipartition(oracle):
+    """Free particles under BAOAB: the momentum variance settles at kT m (in the
+    reference's units, times SQRT_CAL_TO_JOULE^2), per axis, for each damping."""
+    n, steps = 4000, 120
+    mass = np.array([12.0], np.float32)
+    damping = np.array([[50.0, 100.0, 200.0]], np.float32)
+    ty = po.TypeSet(np.zeros(1, np.float32), np.full((1, 3), 150.0, np.float32))
+    box = po.Box.make((0, 0, 0), (1e4, 1e4, 1e4))
+    pos = np.zeros((n, 4), np.float32)
+    pos[:, :3] = 5e3
+    mom = np.zeros((n, 4), np.float32)
+    fe = np.zeros((n, 4), np.float32)
+    dt, kT = 1e-3, W.kT()
+    for s in range(1, steps + 1):
+        pos, mom, fe = oracle.baoab_integrate(pos, mom, fe, np.zeros(n, np.int32), None, ty, None,
+                                              mass, damping, box, dt, kT, s,
+                                              oracle.bd_seed(3, 0, s), pending=0)
+    want = kT * 12.0 * 2.046167337 ** 2
+    var = mom[:, :3].astype(np.float64).var(axis=0)
+    assert np.allclose(var, want, rtol=0.08), (var, want)
