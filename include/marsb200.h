@@ -193,6 +193,27 @@ MB2_API int mb2_bd_integrate(mb2_context* ctx, float* pos4, float* force_energy4
                      uint64_t base_seed, uint32_t base_ctr, const float efield[3],
                      void* stream);
 
+/* Langevin (BAOAB) integrator. Per-type mass and translational damping
+ * (ParticleTypeView::mass, trans_damping; src/Objects/DeviceParticle.h:49-64),
+ * host arrays; mb2_set_particle_types must come first (same type count). */
+MB2_API int mb2_set_langevin_types(mb2_context* ctx, int num_types, const float* mass,
+                           const float* damping3);
+/* One Langevin step of Patch::integrate_motion (Patch.cpp:290-335): with
+ * grids, the position-dependent force (and energy) is accumulated into
+ * force_energy for every particle (launch_PMF, Integrator.h:125-143); when
+ * deferred_kick_pending, the closing half-kick of the previous step
+ * (launch_BAOAB_LastUpdate, Integrator.h:98-123); then B-A-O-A and wrap
+ * (launch_BAOAB, Integrator.h:56-86). mom4: caller-owned momenta (float4).
+ * The caller then owes a closing kick (pass pending = 1 next step, or call
+ * mb2_baoab_last_update). Noise: Philox keyed like BAOABIntegrate (stream 0x1356914). */
+MB2_API int mb2_baoab_integrate(mb2_context* ctx, float* pos4, float* mom4, float* force_energy4,
+                        const int* type_ids, const uint32_t* flags, uint32_t n, float dt,
+                        float kT, uint64_t step, uint64_t base_seed, uint32_t base_ctr,
+                        const float efield[3], int deferred_kick_pending, void* stream);
+/* The closing half-kick alone (Patch::finish_deferred_kick, Patch.cpp:354-373). */
+MB2_API int mb2_baoab_last_update(mb2_context* ctx, float* mom4, const float* force_energy4,
+                          const uint32_t* flags, uint32_t n, float dt, void* stream);
+
 /* Patch::integrate_motion seed mixing (src/PatchOperation/Patch.cpp:252-254). */
 MB2_API uint64_t mb2_bd_seed(uint64_t seed, uint64_t patch_id, uint64_t step);
 

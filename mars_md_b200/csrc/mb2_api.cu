@@ -69,6 +69,9 @@ struct mb2_context {
 	DevBuf<GridView> grids;
 
 	uint32_t bonded_bins[2] = {0, 0};  // values in the bond / angle tables
+	DevBuf<float> mass;                // Langevin: per-type mass
+	DevBuf<float4> damping;            // Langevin: per-type damping (x, y, z)
+	int langevin_types = 0;
 
 	// Adjoint window: checkpoints of the forward window and reverse-sweep buffers.
 	struct Window {
@@ -762,6 +765,58 @@ int mb2_bd_integrate(mb2_context* ctx, float* pos4, float* force_energy4, const 
 				   {efield ? efield[0] : 0.f, efield ? efield[1] : 0.f, efield ? efield[2] : 0.f}};
 		bd_integrate(reinterpret_cast<float4*>(pos4), reinterpret_cast<float4*>(force_energy4),
 					 type_ids, flags, n, ctx->types, ctx->box, p, S(stream));
+	});
+}
+
+int mb2_set_langevin_types(mb2_context* ctx, int num_types, const float* mass,
+						   const float* damping3) {
+	return guarded(ctx, [&] {
+		require(num_types > 0 && mass && damping3, MB2_ERR_ARG,
+				"mb2_set_langevin_types: need mass and damping per type");
+		require(ctx->types_set && num_types == ctx->types.num_types, MB2_ERR_STATE,
+				"mb2_set_langevin_types: call mb2_set_particle_types first, same type count");
+		std::vector<float4> d(num_types);
+		for (int t = 0; t < num_types; ++t) {
+			require(mass[t] > 0.0f, MB2_ERR_ARG, "mb2_set_langevin_types: masses must be positive");
+			d[t] = make_float4(damping3[3 * t], damping3[3 * t + 1], damping3[3 * t + 2], 0.0f);
+		}
+		ctx->mass.ensure(num_types);
+		ctx->damping.ensure(num_types);
+		MB2_CUDA(cudaMemcpy(ctx->mass.ptr, mass, num_types * sizeof(float), cudaMemcpyHostToDevice));
+		MB2_CUDA(cudaMemcpy(ctx->damping.ptr, d.data(), num_types * sizeof(float4),
+							cudaMemcpyHostToDevice));
+		ctx->types.mass = ctx->mass.ptr;
+		ctx->types.damping = ctx->damping.ptr;
+		ctx->langevin_types = num_types;
+	});
+}
+
+int mb2_baoab_integrate(mb2_context* ctx, float* pos4, float* mom4, float* force_energy4,
+						const int* type_ids, const uint32_t* flags, uint32_t n, float dt, float kT,
+						uint64_t step, uint64_t base_seed, uint32_t base_ctr, const float efield[3],
+						int deferred_kick_pending, void* stream) {
+	return guarded(ctx, [&] {
+		require(n == 0 || (pos4 && mom4 && force_energy4 && type_ids), MB2_ERR_ARG,
+				"mb2_baoab_integrate: null argument");
+		require(ctx->box_set && ctx->types_set, MB2_ERR_STATE,
+				"mb2_baoab_integrate: call mb2_set_box and mb2_set_particle_types");
+		require(ctx->langevin_types == ctx->types.num_types, MB2_ERR_STATE,
+				"mb2_baoab_integrate: call mb2_set_langevin_types");
+		const float zero[3] = {0.0f, 0.0f, 0.0f};
+		baoab_integrate(reinterpret_cast<float4*>(pos4), reinterpret_cast<float4*>(mom4),
+						reinterpret_cast<float4*>(force_energy4), type_ids, flags, n, ctx->types,
+						ctx->box, dt, kT, static_cast<uint32_t>(step), base_seed, base_ctr,
+						efield ? efield : zero, deferred_kick_pending, S(stream));
+	});
+}
+
+int mb2_baoab_last_update(mb2_context* ctx, float* mom4, const float* force_energy4,
+						  const uint32_t* flags, uint32_t n, float dt, void* stream) {
+	return guarded(ctx, [&] {
+		require(n == 0 || (mom4 && force_energy4), MB2_ERR_ARG,
+				"mb2_baoab_last_update: null argument");
+		baoab_last_update(reinterpret_cast<float4*>(mom4),
+						  reinterpret_cast<const float4*>(force_energy4), flags, n, dt, S(stream));
 	});
 }
 

@@ -133,9 +133,10 @@ __device__ __forceinline__ float4 position_force(const TypeTable& ty, int type, 
 	return f;
 }
 
-// Box-Muller of one Philox draw (BD.h:66-78).
-__device__ __forceinline__ float3 bd_noise(uint64_t seed, uint32_t ctr, uint32_t step) {
-	const uint4 u = philox4x32_10(seed, ctr, kBdStream, step, 0u);
+// Box-Muller of one Philox draw (BD.h:66-78; BAOAB.h:98-110 with its own stream).
+__device__ __forceinline__ float3 bd_noise(uint64_t seed, uint32_t ctr, uint32_t step,
+										   uint32_t stream = kBdStream) {
+	const uint4 u = philox4x32_10(seed, ctr, stream, step, 0u);
 	const float ux = u01(u.x), uy = u01(u.y), uz = u01(u.z), uw = u01(u.w);
 	const float r1 = __fsqrt_rn(__fmul_rn(-2.0f, logf(ux)));
 	const float t1 = __fmul_rn(6.2831854820251465f, uy);  // 2.0f * 3.1415926535f
@@ -217,6 +218,96 @@ __global__ void __launch_bounds__(256) bd_gather_kernel(
 					   ty.diffusion[type], xi, box, bp);
 }
 
+// FORCE_CONVERSION_FACTOR, SQRT_CAL_TO_JOULE (src/Constants.h:30,34) and the
+// BAOAB noise stream (BAOAB.h:30).
+constexpr float kForceConversion = 4.18679994e4f;
+constexpr float kSqrtCalToJoule = 2.046167337f;
+constexpr uint32_t kBaoabStream = 0x1356914u;
+
+// mom += (0.5 dt F) * FORCE_CONVERSION_FACTOR, as Vector3 arithmetic rounds it.
+__device__ __forceinline__ float half_kick(float m, float f, float h) {
+	return __fadd_rn(m, __fmul_rn(__fmul_rn(h, f), kForceConversion));
+}
+
+// Patch::integrate_motion's Langevin branch (Patch.cpp:290-335) for one
+// particle: PMF pass (Pmf.h:126-152), closing kick if pending (BAOAB.h:167-186),
+// then BAOABIntegrate (BAOAB.h:47-128). Vector3 / s is a multiply by 1 / s.
+__global__ void __launch_bounds__(256) baoab_kernel(
+	float4* __restrict__ pos, float4* __restrict__ mom, float4* __restrict__ fe,
+	const int* __restrict__ type_ids, const uint32_t* __restrict__ flags, uint32_t n,
+	TypeTable ty, Box box, float dt, float kT, uint32_t step, uint64_t seed, uint32_t base_ctr,
+	float3 efield, int pending) {
+	const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+	if (i >= n) return;
+	float4 p = pos[i];
+	float4 f = fe[i];
+	const int type = type_ids[i];
+	if (ty.num_grids > 0) {
+		const float e[3] = {efield.x, efield.y, efield.z};
+		const float4 pmf = position_force(ty, type, p.x, p.y, p.z, e);
+		f.x = __fadd_rn(f.x, pmf.x);
+		f.y = __fadd_rn(f.y, pmf.y);
+		f.z = __fadd_rn(f.z, pmf.z);
+		f.w = __fadd_rn(f.w, pmf.w);
+		fe[i] = f;
+	}
+	if (flags && (flags[i] & kFlagRbAttached)) return;
+	float4 m = mom[i];
+	const float h = __fmul_rn(0.5f, dt);
+	if (pending) {
+		m.x = half_kick(m.x, f.x, h);
+		m.y = half_kick(m.y, f.y, h);
+		m.z = half_kick(m.z, f.z, h);
+	}
+	m.x = half_kick(m.x, f.x, h);  // B
+	m.y = half_kick(m.y, f.y, h);
+	m.z = half_kick(m.z, f.z, h);
+	const float ms = ty.mass[type];
+	const float inv_m = __fdiv_rn(1.0f, ms);
+	auto drift = [&](float x, float mv) {
+		return __fadd_rn(x, __fmul_rn(__fmul_rn(__fmul_rn(h, mv), inv_m), 10000.0f));
+	};
+	p.x = drift(p.x, m.x);  // A
+	p.y = drift(p.y, m.y);
+	p.z = drift(p.z, m.z);
+	const float4 g = ty.damping[type];
+	const float3 xi = bd_noise(seed, base_ctr + i, step, kBaoabStream);
+	auto ou = [&](float mv, float gamma, float r) {  // O
+		const float c = expf(__fmul_rn(-gamma, dt));
+		const float ns = __fmul_rn(
+			__fsqrt_rn(__fmul_rn(__fmul_rn(kT, ms), __fsub_rn(1.0f, __fmul_rn(c, c)))),
+			kSqrtCalToJoule);
+		return __fadd_rn(__fmul_rn(c, mv), __fmul_rn(ns, r));
+	};
+	m.x = ou(m.x, g.x, xi.x);
+	m.y = ou(m.y, g.y, xi.y);
+	m.z = ou(m.z, g.z, xi.z);
+	p.x = drift(p.x, m.x);  // A
+	p.y = drift(p.y, m.y);
+	p.z = drift(p.z, m.z);
+	if (box.periodic[0]) p.x = wrap_scalar(p.x, box.origin[0], box.size[0], box.inv[0]);
+	if (box.periodic[1]) p.y = wrap_scalar(p.y, box.origin[1], box.size[1], box.inv[1]);
+	if (box.periodic[2]) p.z = wrap_scalar(p.z, box.origin[2], box.size[2], box.inv[2]);
+	pos[i] = p;
+	mom[i] = m;
+}
+
+__global__ void __launch_bounds__(256) baoab_last_kernel(float4* __restrict__ mom,
+														 const float4* __restrict__ fe,
+														 const uint32_t* __restrict__ flags,
+														 uint32_t n, float dt) {
+	const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+	if (i >= n) return;
+	if (flags && (flags[i] & kFlagRbAttached)) return;
+	const float4 f = fe[i];
+	float4 m = mom[i];
+	const float h = __fmul_rn(0.5f, dt);
+	m.x = half_kick(m.x, f.x, h);
+	m.y = half_kick(m.y, f.y, h);
+	m.z = half_kick(m.z, f.z, h);
+	mom[i] = m;
+}
+
 __device__ __forceinline__ uint64_t mix_seed(uint64_t seed, uint64_t patch, uint64_t step) {
 	// Patch::integrate_motion seed mixing (Patch.cpp:252-254).
 	return (seed * 0x9E3779B97F4A7C15ULL) ^ (patch << 32) ^ (step * 0xBF58476D1CE4E5B9ULL);
@@ -280,6 +371,22 @@ void bd_integrate_gather(float4* pos, float4* fe, const float4* force_sorted, co
 	if (n == 0) return;
 	MB2_LAUNCH bd_gather_kernel<<<(n + 255) / 256, 256, 0, st>>>(pos, fe, force_sorted, inv, type_ids,
 																 flags, n, types, box, p, read_fe);
+}
+
+void baoab_integrate(float4* pos, float4* mom, float4* fe, const int* type_ids,
+					 const uint32_t* flags, uint32_t n, const TypeTable& types, const Box& box,
+					 float dt, float kT, uint32_t step, uint64_t base_seed, uint32_t base_ctr,
+					 const float* efield, int pending, cudaStream_t st) {
+	if (n == 0) return;
+	MB2_LAUNCH baoab_kernel<<<(n + 255) / 256, 256, 0, st>>>(
+		pos, mom, fe, type_ids, flags, n, types, box, dt, kT, step, base_seed, base_ctr,
+		make_float3(efield[0], efield[1], efield[2]), pending);
+}
+
+void baoab_last_update(float4* mom, const float4* fe, const uint32_t* flags, uint32_t n,
+					   float dt, cudaStream_t st) {
+	if (n == 0) return;
+	MB2_LAUNCH baoab_last_kernel<<<(n + 255) / 256, 256, 0, st>>>(mom, fe, flags, n, dt);
 }
 
 void bd_integrate_systems(float4* pos, float4* fe, const float4* force_sorted,

@@ -226,6 +226,8 @@ struct TypeTable {
 	const float4* force_grid_scale = nullptr;
 	const GridView* grids = nullptr;        // device
 	int num_grids = 0;
+	const float* mass = nullptr;            // device [T], Langevin only
+	const float4* damping = nullptr;        // device [T], Langevin only (x, y, z)
 };
 struct BdParams {
 	float dt;
@@ -242,6 +244,16 @@ void bd_integrate_gather(float4* pos, float4* fe, const float4* force_sorted, co
 						 const int* type_ids, const uint32_t* flags, uint32_t n,
 						 const TypeTable& types, const Box& box, const BdParams& p, int read_fe,
 						 cudaStream_t st);
+// Langevin BAOAB (Integrator/BAOAB.h): with grids, ForceEnergy += position
+// force for every particle; `pending` applies the deferred closing half-kick
+// first; then B-A-O-A and wrap. Noise key (seed, base_ctr + i, step, stream 0x1356914).
+void baoab_integrate(float4* pos, float4* mom, float4* fe, const int* type_ids,
+					 const uint32_t* flags, uint32_t n, const TypeTable& types, const Box& box,
+					 float dt, float kT, uint32_t step, uint64_t base_seed, uint32_t base_ctr,
+					 const float* efield, int pending, cudaStream_t st);
+// BAOAB_LastUpdate: mom += 0.5 dt F (closing half-kick) for non-frozen particles.
+void baoab_last_update(float4* mom, const float4* fe, const uint32_t* flags, uint32_t n,
+					   float dt, cudaStream_t st);
 // Batched replicas' integrate: per-system box, seed (seed + s) mixed with
 // (patch_id, *step_ptr), Philox counter = index within the system.
 void bd_integrate_systems(float4* pos, float4* fe, const float4* force_sorted,

@@ -232,6 +232,25 @@ class Context:
                                              int(base_seed), int(base_ctr), _f3(efield),
                                              _stream(stream)))
 
+    def set_langevin_types(self, mass, damping):
+        """Per-type mass and damping (x, y, z) for the BAOAB integrator."""
+        m = np.ascontiguousarray(mass, np.float32)
+        d = np.ascontiguousarray(np.asarray(damping, np.float32).reshape(len(m), 3))
+        fp = C.POINTER(C.c_float)
+        self.check(self.lib.mb2_set_langevin_types(self.h, len(m), m.ctypes.data_as(fp),
+                                                   d.ctypes.data_as(fp)))
+
+    def baoab_integrate(self, pos, mom, fe, type_ids, flags, dt, kT, step, base_seed, base_ctr=0,
+                        efield=(0.0, 0.0, 0.0), pending=False, stream=None):
+        self.check(self.lib.mb2_baoab_integrate(
+            self.h, _p(pos), _p(mom), _p(fe), _p(type_ids), _p(flags), pos.shape[0], float(dt),
+            float(kT), int(step), int(base_seed), int(base_ctr), _f3(efield), int(bool(pending)),
+            _stream(stream)))
+
+    def baoab_last_update(self, mom, fe, flags, dt, stream=None):
+        self.check(self.lib.mb2_baoab_last_update(self.h, _p(mom), _p(fe), _p(flags),
+                                                  mom.shape[0], float(dt), _stream(stream)))
+
     def bd_seed(self, seed, patch_id, step) -> int:
         return int(self.lib.mb2_bd_seed(int(seed), int(patch_id), int(step)))
 

@@ -13,7 +13,8 @@
 //   * B200Patch: the three Patch stages on this path
 //     (src/PatchOperation/Patch.h:222-287, Patch.cpp:43-352) --
 //     calculate_nonbonded_forces (rebuild schedule + skin check + pair
-//     forces), calculate_bonded_forces, integrate_motion (BD).
+//     forces), calculate_bonded_forces, integrate_motion (BD or Langevin
+//     BAOAB with the deferred closing kick) and finish_deferred_kick.
 //
 // Errors are thrown as marsb200::Exception carrying the library's message,
 // as the reference throws MARS::Exception; the C ABI underneath never throws.
@@ -359,6 +360,9 @@ struct Table {
 	float step_inv = 0.0f;
 };
 
+// Integrators of Patch::integrate_motion on this path (Patch.cpp:238-352).
+enum class IntegratorType { BD, Langevin };
+
 // The three Patch stages of the BD path over one context. Set-up mirrors
 // what the reference's Patch reads from its registries (tables, types,
 // exclusions); the stage calls keep Patch's argument meanings.
@@ -464,6 +468,47 @@ class B200Patch {
 			  ctx_->get(), "integrate_motion");
 	}
 
+	// Per-type mass and damping for the Langevin integrator.
+	void set_langevin_types(const std::vector<float>& mass, const std::vector<float>& damping3) {
+		check(mb2_set_langevin_types(ctx_->get(), static_cast<int>(mass.size()), mass.data(),
+									 damping3.data()),
+			  ctx_->get(), "set_langevin_types");
+	}
+
+	// Patch::integrate_motion with either integrator. Langevin keeps the
+	// reference's deferred closing kick: it is paid at the start of the next
+	// Langevin step, or by finish_deferred_kick (Patch.cpp:290-335, 354-373).
+	void integrate_motion(IntegratorType type, DeviceBuffer<Vector3>& pos,
+						  DeviceBuffer<Vector3>& mom, DeviceBuffer<Vector3>& force_energy,
+						  const DeviceBuffer<int>& types, const uint32_t* flags, size_t num_particles,
+						  float dt, float kT, size_t step, uint64_t seed, uint64_t patch_id = 0,
+						  const Vector3& electric_field = Vector3{}) {
+		if (type == IntegratorType::BD) {
+			integrate_motion(pos, force_energy, types, flags, num_particles, dt, kT, step, seed,
+							 patch_id, electric_field);
+			return;
+		}
+		const float e[3] = {electric_field.x, electric_field.y, electric_field.z};
+		check(mb2_baoab_integrate(ctx_->get(), reinterpret_cast<float*>(pos.data()),
+								  reinterpret_cast<float*>(mom.data()),
+								  reinterpret_cast<float*>(force_energy.data()), types.data(), flags,
+								  static_cast<uint32_t>(num_particles), dt, kT, step,
+								  mb2_bd_seed(seed, patch_id, step), 0u, e,
+								  deferred_kick_pending_ ? 1 : 0, ctx_->stream()),
+			  ctx_->get(), "integrate_motion");
+		deferred_kick_pending_ = true;
+	}
+	void finish_deferred_kick(DeviceBuffer<Vector3>& mom, const DeviceBuffer<Vector3>& force_energy,
+							  const uint32_t* flags, size_t num_particles, float dt) {
+		if (!deferred_kick_pending_) return;
+		deferred_kick_pending_ = false;
+		check(mb2_baoab_last_update(ctx_->get(), reinterpret_cast<float*>(mom.data()),
+									reinterpret_cast<const float*>(force_energy.data()), flags,
+									static_cast<uint32_t>(num_particles), dt, ctx_->stream()),
+			  ctx_->get(), "finish_deferred_kick");
+	}
+	bool has_deferred_kick() const { return deferred_kick_pending_; }
+
   private:
 	struct Flat {
 		std::vector<float> values, starts, step_invs;
@@ -481,6 +526,7 @@ class B200Patch {
 	B200Pairlist pairlist_;
 	bool built_ = false;
 	size_t built_n_ = 0;
+	bool deferred_kick_pending_ = false;
 };
 
 }  // namespace marsb200

@@ -254,6 +254,38 @@ static void patch_stage_test(const Resource& res) {
 	EXPECT(worst <= 1e-4f && moved > 0.1f, "Patch stages equal the fused step over 5 steps");
 }
 
+// Langevin through the Patch mirror: the deferred closing kick is owed after a
+// step and paid by finish_deferred_kick (momenta change), not twice.
+static void langevin_stage_test(const Resource& res) {
+	const int n = 1024;
+	B200Patch patch(res, n);
+	patch.set_periodic_box(PeriodicBox(Vector3(0, 0, 0), Vector3(100, 100, 100)));
+	patch.set_particle_types({0.0f}, {150.0f, 150.0f, 150.0f});
+	patch.set_langevin_types({12.0f}, {50.0f, 50.0f, 50.0f});
+	std::vector<Vector3> h(n), f(n, Vector3(1.0f, -2.0f, 0.5f));
+	for (int i = 0; i < n; ++i) h[i] = Vector3(0.09f * i, 50.0f, 50.0f);
+	DeviceBuffer<Vector3> pos(n, res), mom(n, res), fe(n, res);
+	DeviceBuffer<int> types(n, res);
+	pos.copy_from_host(h);
+	mom.fill_zero();
+	fe.copy_from_host(f);
+	types.copy_from_host(std::vector<int>(n, 0));
+	const float kT = 295.0f * 0.001987191f;
+	patch.integrate_motion(IntegratorType::Langevin, pos, mom, fe, types, nullptr, n, 1e-4f, kT, 1, 5);
+	EXPECT(patch.has_deferred_kick(), "Langevin step leaves the closing kick pending");
+	std::vector<Vector3> m1, m2;
+	mom.copy_to_host(m1);
+	patch.finish_deferred_kick(mom, fe, nullptr, n, 1e-4f);
+	mom.copy_to_host(m2);
+	const float kick = 0.5f * 1e-4f * 1.0f * 4.18679994e4f;
+	EXPECT(!patch.has_deferred_kick() && std::fabs((m2[0].x - m1[0].x) - kick) < 1e-3f * kick,
+		   "finish_deferred_kick applies one half-kick");
+	patch.finish_deferred_kick(mom, fe, nullptr, n, 1e-4f);
+	std::vector<Vector3> m3;
+	mom.copy_to_host(m3);
+	EXPECT(m3[0].x == m2[0].x, "no second closing kick");
+}
+
 int main() {
 	Resource res;
 	res.device = 0;
@@ -263,6 +295,7 @@ int main() {
 		periodic_random_test(res);
 		error_tests(res);
 		patch_stage_test(res);
+		langevin_stage_test(res);
 	} catch (const std::exception& e) {
 		std::printf("FAIL unexpected exception: %s\n", e.what());
 		++failures;

@@ -171,3 +171,31 @@ def test_bd_step_with_grid_matches_reference_fixture(ctx_factory):
     frozen = d["flags"] != 0
     assert np.array_equal(got[frozen], d["pos"][frozen])
     assert np.allclose(gfe[:, 3], d["fe_after"][:, 3], rtol=1e-5, atol=1e-5)
+
+
+@pytest.mark.parametrize("pending", [0, 1])
+def test_baoab_step_matches_reference_fixture(ctx_factory, pending):
+    """Langevin BAOAB with the PMF pass and, when pending, the closing kick."""
+    d = _load("baoab")
+    n = len(d["pos"])
+    ctx = ctx_factory(n)
+    _box(ctx, d)
+    grid = _cuda(d["grid"])
+    ctx.set_grid(0, grid, tuple(d["grid_origin"]), np.eye(3, dtype=np.float32), 0)
+    ctx.set_particle_types(d["charge"], d["diffusion"][:, :3],
+                           [[(0, float(s), 0.0, -1)] for s in d["pmf_scale"]])
+    ctx.set_langevin_types(d["mass"], d["damping"])
+    pos, mom, fe = _cuda(d["pos"]), _cuda(d["mom"]), _cuda(d["fe"])
+    ctx.baoab_integrate(pos, mom, fe, _cuda(d["type_ids"]), _cuda(d["flags"].view(np.int32)),
+                        float(d["dt"]), float(d["kT"]), int(d["step"]), int(d["seed"]),
+                        efield=tuple(d["efield"]), pending=pending)
+    got_p, got_m, got_f = pos.cpu().numpy(), mom.cpu().numpy(), fe.cpu().numpy()
+    ref_p, ref_m = d[f"pos_after_{pending}"], d[f"mom_after_{pending}"]
+    dp = np.abs(got_p[:, :3] - ref_p[:, :3])
+    dp = np.minimum(dp, np.abs(dp - d["box_size"][0]))
+    assert dp.max() <= POS_TOL
+    assert np.abs(got_m[:, :3] - ref_m[:, :3]).max() <= 1e-5 * np.abs(ref_m[:, :3]).max()
+    assert np.allclose(got_f, d[f"fe_after_{pending}"], rtol=1e-5, atol=1e-5)
+    frozen = d["flags"] != 0
+    assert np.array_equal(got_p[frozen], d["pos"][frozen])
+    assert np.array_equal(got_m[frozen], d["mom"][frozen])
