@@ -193,6 +193,34 @@ MB2_API int mb2_bd_integrate(mb2_context* ctx, float* pos4, float* force_energy4
                      uint64_t base_seed, uint32_t base_ctr, const float efield[3],
                      void* stream);
 
+/* --- canonical Z-order reorder ---------------------------------------------
+ * Replaces Patch::reorder_particles (src/PatchOperation/Patch.cpp:455-480):
+ * Morton order of the positions over the periodic box (ZOrderSort::sort_particles
+ * with origin .. origin + size as bounds), each per-particle array gathered
+ * into it (DeviceParticle::permute, src/Objects/DeviceParticleManager.h:186-208,
+ * ReorderDataKernel, src/PatchOperation/ZOrderKernels/ZOrderKernels.h:49-63)
+ * and each stored particle index sent through the inverse map
+ * (RemapIndicesKernel, ZOrderKernels.h:87-101). The host rebuilds the
+ * exclusion CSR from remapped pairs as rebuild_exclusions_after_reorder does
+ * (src/Interactions/DeviceBondedInteraction.h:364-430).
+ *   mb2_reorder_begin: compute and keep the permutation of n positions; the
+ *     context's pairlist becomes stale (the next build re-sorts). A box with
+ *     a non-positive size is MB2_ERR_ARG (the reference skips the reorder).
+ *   mb2_reorder_apply: permute one device array of n elements of 4 or 16 bytes
+ *     in place (positions, momenta, orientations, ids, type ids, flags,
+ *     rigid-body ids; force/energy is cleared each step and is not permuted);
+ *     n must equal the last begin's.
+ *   mb2_reorder_remap: indices[i] = inverse[indices[i]] for the `count` device
+ *     ints whose value is in [0, n) (bond / angle / dihedral / restraint
+ *     particle indices); others unchanged.
+ *   mb2_reorder_inverse: copy the old -> new map (device uint32[n]). */
+MB2_API int mb2_reorder_begin(mb2_context* ctx, const float* pos4, uint32_t n, void* stream);
+MB2_API int mb2_reorder_apply(mb2_context* ctx, void* data, uint32_t elem_bytes, uint32_t n,
+                              void* stream);
+MB2_API int mb2_reorder_remap(mb2_context* ctx, int* indices, uint64_t count, void* stream);
+MB2_API int mb2_reorder_inverse(mb2_context* ctx, uint32_t* inverse_out, uint32_t n,
+                                void* stream);
+
 /* Langevin (BAOAB) integrator. Per-type mass and translational damping
  * (ParticleTypeView::mass, trans_damping; src/Objects/DeviceParticle.h:49-64),
  * host arrays; mb2_set_particle_types must come first (same type count). */

@@ -92,6 +92,10 @@ def load(path: str = LIB_PATH):
     L.mb2_profile_read.argtypes = [vp, i, C.POINTER(C.c_double), u32p]
     L.mb2_launch_count.restype = u64
     L.mb2_launch_count.argtypes = []
+    L.mb2_reorder_begin.argtypes = [vp, vp, u32, vp]
+    L.mb2_reorder_apply.argtypes = [vp, vp, u32, u32, vp]
+    L.mb2_reorder_remap.argtypes = [vp, vp, u64, vp]
+    L.mb2_reorder_inverse.argtypes = [vp, vp, u32, vp]
     L.mb2_set_langevin_types.argtypes = [vp, i, fp, fp]
     L.mb2_baoab_integrate.argtypes = [vp, vp, vp, vp, vp, vp, u32, f, f, u64, u64, u32, fp, i, vp]
     L.mb2_baoab_last_update.argtypes = [vp, vp, vp, vp, u32, f, vp]

@@ -69,6 +69,9 @@ struct mb2_context {
 	DevBuf<GridView> grids;
 
 	uint32_t bonded_bins[2] = {0, 0};  // values in the bond / angle tables
+	DevBuf<uint32_t> ro_keys, ro_s2o, ro_inv;  // canonical reorder permutation
+	DevBuf<float4> ro_tmp;
+	uint32_t ro_n = 0;
 	DevBuf<float> mass;                // Langevin: per-type mass
 	DevBuf<float4> damping;            // Langevin: per-type damping (x, y, z)
 	int langevin_types = 0;
@@ -765,6 +768,69 @@ int mb2_bd_integrate(mb2_context* ctx, float* pos4, float* force_energy4, const 
 				   {efield ? efield[0] : 0.f, efield ? efield[1] : 0.f, efield ? efield[2] : 0.f}};
 		bd_integrate(reinterpret_cast<float4*>(pos4), reinterpret_cast<float4*>(force_energy4),
 					 type_ids, flags, n, ctx->types, ctx->box, p, S(stream));
+	});
+}
+
+int mb2_reorder_begin(mb2_context* ctx, const float* pos4, uint32_t n, void* stream) {
+	return guarded(ctx, [&] {
+		require(ctx->box_set, MB2_ERR_STATE, "mb2_reorder_begin: call mb2_set_box first");
+		require(n == 0 || pos4, MB2_ERR_ARG, "mb2_reorder_begin: null positions");
+		require(n <= ctx->max_particles, MB2_ERR_CAPACITY,
+				"mb2_reorder_begin: more particles than the context was created for");
+		float bmin[3], bmax[3];
+		for (int a = 0; a < 3; ++a) {
+			bmin[a] = ctx->box.origin[a];
+			bmax[a] = ctx->box.origin[a] + ctx->box.size[a];
+			require(bmax[a] > bmin[a], MB2_ERR_ARG, "mb2_reorder_begin: degenerate Morton box");
+		}
+		const cudaStream_t st = S(stream);
+		ctx->ro_keys.ensure(n);
+		ctx->ro_s2o.ensure(n);
+		ctx->ro_inv.ensure(n);
+		morton_encode(reinterpret_cast<const float4*>(pos4), n, bmin, bmax, ctx->ro_keys.ptr,
+					  ctx->ro_s2o.ptr, st);
+		radix_sort_pairs(ctx->scratch, ctx->ro_keys.ptr, ctx->ro_s2o.ptr, n, st);
+		inverse_and_gather(ctx->ro_s2o.ptr, n, reinterpret_cast<const float4*>(pos4),
+						   ctx->ro_inv.ptr, nullptr, st);
+		ctx->ro_n = n;
+		ctx->built = false;  // every stored particle index changes: rebuild before use
+		ctx->win.valid = false;
+	});
+}
+
+int mb2_reorder_apply(mb2_context* ctx, void* data, uint32_t elem_bytes, uint32_t n, void* stream) {
+	return guarded(ctx, [&] {
+		require(n == ctx->ro_n, MB2_ERR_STATE,
+				"mb2_reorder_apply: n differs from the last mb2_reorder_begin");
+		require(elem_bytes == 4 || elem_bytes == 16, MB2_ERR_ARG,
+				"mb2_reorder_apply: elements of 4 or 16 bytes");
+		require(n == 0 || data, MB2_ERR_ARG, "mb2_reorder_apply: null data");
+		if (n == 0) return;
+		const cudaStream_t st = S(stream);
+		ctx->ro_tmp.ensure(n);
+		MB2_CUDA(cudaMemcpyAsync(ctx->ro_tmp.ptr, data, static_cast<size_t>(n) * elem_bytes,
+								 cudaMemcpyDeviceToDevice, st));
+		permute_gather(ctx->ro_tmp.ptr, ctx->ro_s2o.ptr, n, static_cast<int>(elem_bytes), data, st);
+	});
+}
+
+int mb2_reorder_remap(mb2_context* ctx, int* indices, uint64_t count, void* stream) {
+	return guarded(ctx, [&] {
+		require(count == 0 || indices, MB2_ERR_ARG, "mb2_reorder_remap: null indices");
+		require(ctx->ro_inv.ptr || ctx->ro_n == 0, MB2_ERR_STATE,
+				"mb2_reorder_remap: call mb2_reorder_begin first");
+		remap_indices(indices, count, ctx->ro_inv.ptr, ctx->ro_n, S(stream));
+	});
+}
+
+int mb2_reorder_inverse(mb2_context* ctx, uint32_t* inverse_out, uint32_t n, void* stream) {
+	return guarded(ctx, [&] {
+		require(n == ctx->ro_n, MB2_ERR_STATE,
+				"mb2_reorder_inverse: n differs from the last mb2_reorder_begin");
+		require(n == 0 || inverse_out, MB2_ERR_ARG, "mb2_reorder_inverse: null output");
+		if (n == 0) return;
+		MB2_CUDA(cudaMemcpyAsync(inverse_out, ctx->ro_inv.ptr, static_cast<size_t>(n) * 4,
+								 cudaMemcpyDeviceToDevice, S(stream)));
 	});
 }
 

@@ -91,6 +91,11 @@ void morton_encode(const float4* pos, uint32_t n, const float* bmin, const float
 void radix_sort_pairs(Scratch& s, uint32_t* keys, uint32_t* vals, uint32_t n, cudaStream_t st);
 void inverse_and_gather(const uint32_t* s2o, uint32_t n, const float4* pos, uint32_t* inv,
 						float4* sorted_pos, cudaStream_t st);
+// out[s] = in[s2o[s]] for elements of 4 or 16 bytes.
+void permute_gather(const void* in, const uint32_t* s2o, uint32_t n, int elem_bytes, void* out,
+					cudaStream_t st);
+// idx[i] = inv[idx[i]] where 0 <= idx[i] < n (others unchanged).
+void remap_indices(int* idx, size_t count, const uint32_t* inv, uint32_t n, cudaStream_t st);
 // Elements per radix-sort tile; the digit histogram holds 256 words per tile.
 constexpr uint32_t kSortTile = 2048;
 // Radix sort with caller-supplied scratch: keys_alt and vals_alt of n words,

@@ -114,6 +114,24 @@ __global__ void __launch_bounds__(256) inverse_gather_kernel(const uint32_t* __r
 	if (sorted_pos) sorted_pos[i] = pos[o];
 }
 
+// out[s] = in[s2o[s]] for 4- or 16-byte elements (DeviceParticle::permute).
+template <typename T>
+__global__ void __launch_bounds__(256) permute_kernel(const T* __restrict__ in,
+													  const uint32_t* __restrict__ s2o, uint32_t n,
+													  T* __restrict__ out) {
+	const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
+	if (s < n) out[s] = in[s2o[s]];
+}
+
+// RemapIndicesKernel (ZOrderKernels.h:87-101): in-range indices go through inv.
+__global__ void __launch_bounds__(256) remap_kernel(int* __restrict__ idx, size_t count,
+													const uint32_t* __restrict__ inv, uint32_t n) {
+	const size_t i = static_cast<size_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+	if (i >= count) return;
+	const int v = idx[i];
+	if (v >= 0 && static_cast<uint32_t>(v) < n) idx[i] = static_cast<int>(inv[v]);
+}
+
 }  // namespace
 
 void radix_sort_pairs(Scratch& s, uint32_t* keys, uint32_t* vals, uint32_t n, cudaStream_t st) {
@@ -174,6 +192,23 @@ void inverse_and_gather(const uint32_t* s2o, uint32_t n, const float4* pos, uint
 						float4* sorted_pos, cudaStream_t st) {
 	if (n == 0) return;
 	MB2_LAUNCH inverse_gather_kernel<<<(n + 255) / 256, 256, 0, st>>>(s2o, n, pos, inv, sorted_pos);
+}
+
+void permute_gather(const void* in, const uint32_t* s2o, uint32_t n, int elem_bytes, void* out,
+					cudaStream_t st) {
+	if (n == 0) return;
+	if (elem_bytes == 16)
+		MB2_LAUNCH permute_kernel<float4><<<(n + 255) / 256, 256, 0, st>>>(
+			static_cast<const float4*>(in), s2o, n, static_cast<float4*>(out));
+	else
+		MB2_LAUNCH permute_kernel<uint32_t><<<(n + 255) / 256, 256, 0, st>>>(
+			static_cast<const uint32_t*>(in), s2o, n, static_cast<uint32_t*>(out));
+}
+
+void remap_indices(int* idx, size_t count, const uint32_t* inv, uint32_t n, cudaStream_t st) {
+	if (count == 0) return;
+	MB2_LAUNCH remap_kernel<<<static_cast<unsigned>((count + 255) / 256), 256, 0, st>>>(idx, count,
+																						inv, n);
 }
 
 }  // namespace mb2

@@ -12,7 +12,9 @@ call surface on the Brownian-dynamics path:
   launch_tabulated_{bonds,angles} (src/Interactions/DeviceBondedInteraction.h:495-549);
 * ``set_particle_types`` / ``set_grid`` / ``bd_integrate`` -- launch_BD
   (src/PatchOperation/Integrator.h:26-54);
-* ``step`` -- one SimManager step for one patch (src/SimManager.cpp:337-504).
+* ``step`` -- one SimManager step for one patch (src/SimManager.cpp:337-504);
+* ``reorder_*`` / ``reorder_particles`` / ``ReorderManager`` -- the canonical
+  Morton reorder of a patch (src/PatchOperation/Patch.cpp:455-480).
 
 ``Batch`` wraps one ``mb2_batch``: many independent periodic systems stepped
 together (one launch per stage for all of them, CUDA-graph step replay, an
@@ -177,6 +179,33 @@ class Context:
         self.check(self.lib.mb2_radix_sort_pairs_static(self.h, _p(keys), _p(vals),
                                                         keys.shape[0], _stream(stream)))
 
+    # -- canonical reorder -------------------------------------------------
+    def reorder_begin(self, pos, stream=None):
+        """Morton permutation of the positions over the periodic box (the
+        pairlist becomes stale)."""
+        self.check(self.lib.mb2_reorder_begin(self.h, _p(pos), pos.shape[0], _stream(stream)))
+        self._reorder_n = pos.shape[0]
+
+    def reorder_apply(self, t, stream=None):
+        """Permute one per-particle tensor in place: [n] of 4-byte or [n, 4] of
+        4-byte elements."""
+        n = t.shape[0]
+        width = t.numel() // max(n, 1) * t.element_size()
+        if width not in (4, 16):
+            raise ValueError("reorder_apply: rows of 4 or 16 bytes")
+        self.check(self.lib.mb2_reorder_apply(self.h, _p(t), width, n, _stream(stream)))
+
+    def reorder_remap(self, indices, stream=None):
+        """indices (int32, any shape) -> inverse[indices] where in [0, n)."""
+        self.check(self.lib.mb2_reorder_remap(self.h, _p(indices), indices.numel(),
+                                              _stream(stream)))
+
+    def reorder_inverse(self, stream=None):
+        n = getattr(self, "_reorder_n", 0)
+        out = torch.empty(max(n, 1), dtype=torch.int32, device=f"cuda:{self.device}")
+        self.check(self.lib.mb2_reorder_inverse(self.h, _p(out), n, _stream(stream)))
+        return out[:n]
+
     # -- pairlist ----------------------------------------------------------
     def build_pairlist(self, pos, type_ids, pairlist_cutoff, stream=None) -> int:
         npairs = C.c_uint64()
@@ -264,6 +293,95 @@ class Context:
     def step(self, pos, fe, type_ids, flags, step, params: "L.StepParams", stream=None):
         self.check(self.lib.mb2_step(self.h, _p(pos), _p(fe), _p(type_ids), _p(flags),
                                      pos.shape[0], int(step), C.byref(params), _stream(stream)))
+
+
+def exclusion_csr(pairs):
+    """Per-particle CSR of excluded pairs, as DeviceBondedInteractions builds it
+    (rebuild_exclusions_after_reorder, src/Interactions/DeviceBondedInteraction.h:385-430):
+    each pair canonicalised to (a < b), pairs sorted, then each particle's
+    neighbours in sorted-pair order. Returns (pairs, offsets, neighbors,
+    num_excl_particles); offsets has num_excl_particles + 1 entries."""
+    e = np.asarray(pairs, np.int64).reshape(-1, 2)
+    if len(e) == 0:
+        return (np.zeros((0, 2), np.int32), np.zeros(1, np.int32), np.zeros(0, np.int32), 0)
+    e = np.sort(e, axis=1)
+    e = e[np.lexsort((e[:, 1], e[:, 0]))]
+    np_ = int(e[:, 1].max()) + 1
+    owner = np.concatenate([e[:, 0], e[:, 1]])
+    other = np.concatenate([e[:, 1], e[:, 0]])
+    edge = np.concatenate([np.arange(len(e)), np.arange(len(e))])
+    order = np.lexsort((edge, owner))
+    offsets = np.zeros(np_ + 1, np.int64)
+    np.add.at(offsets, owner + 1, 1)
+    return (e.astype(np.int32), np.cumsum(offsets).astype(np.int32),
+            other[order].astype(np.int32), np_)
+
+
+def reorder_particles(ctx: Context, box, particles: dict, indices=(), exclusion_pairs=None,
+                      stream=None):
+    """Patch::reorder_particles (src/PatchOperation/Patch.cpp:455-480) for one
+    patch: Morton order over the periodic box of particles["pos"], every tensor
+    in ``particles`` permuted in place (pos, mom, orient, id, type_id, flags,
+    attached_rigid_body_id as DeviceParticle::permute does; force/energy is
+    cleared each step and is left alone), every int32 tensor in ``indices``
+    (bonds, angles, dihedrals, restraint ids) remapped in place, and the
+    exclusion pairs remapped and rebuilt into a CSR on the host, which is
+    handed to the context (the returned dict keeps its device arrays alive).
+
+    box: (origin, size); a degenerate box skips the reorder (returns None), as
+    the reference does. Returns {"inverse", "exclusions"} otherwise."""
+    origin, size = np.asarray(box[0], np.float32), np.asarray(box[1], np.float32)
+    if not np.all(origin + size > origin):
+        return None
+    pos = particles["pos"]
+    ctx.reorder_begin(pos, stream)
+    for t in particles.values():
+        if t is not None:
+            ctx.reorder_apply(t, stream)
+    for t in indices:
+        if t is not None and t.numel():
+            ctx.reorder_remap(t, stream)
+    out = {"inverse": ctx.reorder_inverse(stream), "exclusions": None}
+    if exclusion_pairs is not None and len(exclusion_pairs):
+        inv = out["inverse"].cpu().numpy().astype(np.int64)
+        e, off, nb, npart = exclusion_csr(inv[np.asarray(exclusion_pairs, np.int64)])
+        dev = pos.device
+        off_d, nb_d = torch.from_numpy(off).to(dev), torch.from_numpy(nb).to(dev)
+        rb = particles.get("attached_rigid_body_id")
+        ctx.set_exclusions(off_d, nb_d, npart, rb)
+        out["exclusions"] = (e, off_d, nb_d, npart)
+    return out
+
+
+class ReorderManager:
+    """ParticleReorderManager::maybe_reorder (src/PatchOperation/ReorderManager.cpp:8-25):
+    reorder on steps 1, 1 + period, 1 + 2 period, ... once the bonded topology
+    is on the device. The period defaults to the pairlist rebuild period
+    (src/SimManager.cpp:345-349)."""
+
+    def __init__(self, reorder_period: int, rebuild_period: int = 0):
+        self.period = int(reorder_period) if reorder_period > 0 else int(rebuild_period)
+
+    def should_reorder(self, step: int, bonded_prepared: bool = True) -> bool:
+        if self.period <= 0 or step == 0:
+            return False
+        if (step - 1) % self.period:
+            return False
+        return bool(bonded_prepared)
+
+
+def to_original_order(values, ids):
+    """Rows of a reordered patch back in global-id order, as
+    DeviceParticle::copy_to_host_unpermuted emits them
+    (src/Objects/DeviceParticleManager.h:219-260): out[ids[i]] = values[i]; an id
+    outside [0, n) is an error (dense single-patch ids)."""
+    values, ids = np.asarray(values), np.asarray(ids, np.int64)
+    n = len(ids)
+    if n and (ids.min() < 0 or ids.max() >= n):
+        raise ValueError("to_original_order: global id outside [0, n)")
+    out = np.empty_like(values)
+    out[ids] = values
+    return out
 
 
 def step_params(w, seed=None, patch_id=0, get_energy=False, bonds=None, bond_idx=None,

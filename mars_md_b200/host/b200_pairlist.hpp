@@ -14,7 +14,8 @@
 //     (src/PatchOperation/Patch.h:222-287, Patch.cpp:43-352) --
 //     calculate_nonbonded_forces (rebuild schedule + skin check + pair
 //     forces), calculate_bonded_forces, integrate_motion (BD or Langevin
-//     BAOAB with the deferred closing kick) and finish_deferred_kick.
+//     BAOAB with the deferred closing kick), finish_deferred_kick and
+//     reorder_particles (with ExclusionCSR and ParticleReorderManager).
 //
 // Errors are thrown as marsb200::Exception carrying the library's message,
 // as the reference throws MARS::Exception; the C ABI underneath never throws.
@@ -172,6 +173,108 @@ struct ExclusionView {
 	const int* excluded = nullptr;
 	uint32_t num_particles = 0;
 	const int* rigid_body_id = nullptr;
+};
+
+// Exclusion CSR built on the host from excluded pairs and owned on the device,
+// as DeviceBondedInteractions builds it (rebuild_exclusions_after_reorder,
+// src/Interactions/DeviceBondedInteraction.h:385-430): pairs canonicalised
+// (a < b) and sorted, offsets over 0 .. max index + 1, each particle's
+// neighbours in sorted-pair order.
+class ExclusionCSR {
+  public:
+	void build(std::vector<std::pair<int, int>> pairs, const Resource& r = Resource{}) {
+		res_ = r;
+		for (auto& e : pairs)
+			if (e.first > e.second) std::swap(e.first, e.second);
+		std::sort(pairs.begin(), pairs.end());
+		pairs_ = std::move(pairs);
+		num_ = 0;
+		if (pairs_.empty()) return;
+		int max_idx = 0;
+		for (const auto& e : pairs_) max_idx = std::max(max_idx, e.second);
+		num_ = static_cast<uint32_t>(max_idx) + 1;
+		std::vector<int> off(num_ + 1, 0);
+		for (const auto& e : pairs_) {
+			off[e.first + 1]++;
+			off[e.second + 1]++;
+		}
+		for (uint32_t p = 0; p < num_; ++p) off[p + 1] += off[p];
+		std::vector<int> nb(off[num_]);
+		std::vector<int> cur(off.begin(), off.end() - 1);
+		for (const auto& e : pairs_) {
+			nb[cur[e.first]++] = e.second;
+			nb[cur[e.second]++] = e.first;
+		}
+		offsets_ = DeviceBuffer<int>(off.size(), res_);
+		offsets_.copy_from_host(off);
+		neighbors_ = DeviceBuffer<int>(std::max<size_t>(nb.size(), 1), res_);
+		neighbors_.copy_from_host(nb.data(), nb.size());
+	}
+	// Endpoints through the old -> new map, then the CSR rebuilt.
+	void remap(const std::vector<uint32_t>& inverse) {
+		std::vector<std::pair<int, int>> p = pairs_;
+		for (auto& e : p) {
+			e.first = static_cast<int>(inverse.at(static_cast<size_t>(e.first)));
+			e.second = static_cast<int>(inverse.at(static_cast<size_t>(e.second)));
+		}
+		build(std::move(p), res_);
+	}
+	ExclusionView view(const int* rigid_body_id = nullptr) const {
+		return ExclusionView{num_ ? offsets_.data() : nullptr, num_ ? neighbors_.data() : nullptr,
+							 num_, rigid_body_id};
+	}
+	const std::vector<std::pair<int, int>>& pairs() const { return pairs_; }
+	uint32_t num_particles() const { return num_; }
+
+  private:
+	std::vector<std::pair<int, int>> pairs_;
+	DeviceBuffer<int> offsets_, neighbors_;
+	uint32_t num_ = 0;
+	Resource res_{};
+};
+
+// Per-particle device arrays a reorder permutes: the members DeviceParticle::permute
+// gathers (src/Objects/DeviceParticleManager.h:186-208). Null members are skipped;
+// force/energy is cleared every step and is not permuted.
+struct ParticleArrays {
+	Vector3* pos = nullptr;
+	Vector3* mom = nullptr;
+	Vector3* orient = nullptr;
+	int* id = nullptr;
+	int* type_id = nullptr;
+	uint32_t* flags = nullptr;
+	int* attached_rigid_body_id = nullptr;
+};
+
+// Device particle indices a reorder remaps (DeviceBondedInteractions::
+// remap_particle_indices, src/Interactions/DeviceBondedInteraction.h:364-380).
+struct BondedIndices {
+	int* bonds2 = nullptr;  // int2 per bond
+	size_t num_bonds = 0;
+	int* angles4 = nullptr;  // int4 per angle (fourth word unused)
+	size_t num_angles = 0;
+	int* dihedrals4 = nullptr;  // int4 per dihedral
+	size_t num_dihedrals = 0;
+	int* restraint_ids = nullptr;  // one particle per restraint
+	size_t num_restraints = 0;
+};
+
+// ParticleReorderManager::maybe_reorder (src/PatchOperation/ReorderManager.cpp:8-25):
+// steps 1, 1 + period, ... once the bonded topology is on the device; a
+// period <= 0 falls back to the pairlist rebuild period (SimManager.cpp:345-349).
+class ParticleReorderManager {
+  public:
+	explicit ParticleReorderManager(int reorder_period, size_t rebuild_period = 0)
+		: period_(reorder_period > 0 ? static_cast<size_t>(reorder_period) : rebuild_period) {}
+	bool should_reorder(size_t step, bool bonded_prepared = true) const {
+		if (period_ == 0 || step == 0) return false;
+		if ((step - 1) % period_ != 0) return false;
+		return bonded_prepared;
+	}
+	size_t period() const { return period_; }
+
+  private:
+	size_t period_;
 };
 
 // Pairlist strategies (src/PatchOperation/Pairlist.h:38-43) plus this one.
@@ -508,6 +611,52 @@ class B200Patch {
 			  ctx_->get(), "finish_deferred_kick");
 	}
 	bool has_deferred_kick() const { return deferred_kick_pending_; }
+
+	// Patch::reorder_particles (src/PatchOperation/Patch.cpp:455-480): Morton
+	// order over the periodic box, every particle array gathered, every stored
+	// index remapped, the exclusion CSR rebuilt and handed to the pairlist, and
+	// the next calculate_nonbonded_forces forced to rebuild. A degenerate box
+	// or no particles skips the reorder (returns false), as the reference does.
+	bool reorder_particles(const PeriodicBox& box, const ParticleArrays& p, size_t num_particles,
+						   const BondedIndices& b = BondedIndices{},
+						   ExclusionCSR* exclusions = nullptr) {
+		if (num_particles == 0 || !p.pos) return false;
+		const Vector3& o = box.get_origin();
+		const Vector3& sz = box.get_size();
+		if (!(o.x + sz.x > o.x && o.y + sz.y > o.y && o.z + sz.z > o.z)) return false;
+		mb2_context* c = ctx_->get();
+		void* st = ctx_->stream();
+		const uint32_t n = static_cast<uint32_t>(num_particles);
+		check(mb2_reorder_begin(c, reinterpret_cast<const float*>(p.pos), n, st), c,
+			  "reorder_particles");
+		auto apply = [&](void* a, uint32_t bytes) {
+			if (a) check(mb2_reorder_apply(c, a, bytes, n, st), c, "reorder_particles");
+		};
+		apply(p.pos, 16);
+		apply(p.mom, 16);
+		apply(p.orient, 16);
+		apply(p.id, 4);
+		apply(p.type_id, 4);
+		apply(p.flags, 4);
+		apply(p.attached_rigid_body_id, 4);
+		auto remap = [&](int* a, size_t count) {
+			if (a && count) check(mb2_reorder_remap(c, a, count, st), c, "reorder_particles");
+		};
+		remap(b.bonds2, 2 * b.num_bonds);
+		remap(b.angles4, 4 * b.num_angles);
+		remap(b.dihedrals4, 4 * b.num_dihedrals);
+		remap(b.restraint_ids, b.num_restraints);
+		if (exclusions && !exclusions->pairs().empty()) {
+			DeviceBuffer<uint32_t> inv(num_particles, ctx_->resource());
+			check(mb2_reorder_inverse(c, inv.data(), n, st), c, "reorder_particles");
+			std::vector<uint32_t> h;
+			inv.copy_to_host(h);
+			exclusions->remap(h);
+			pairlist_.set_exclusions(exclusions->view(p.attached_rigid_body_id));
+		}
+		built_ = false;  // force_rebuild_
+		return true;
+	}
 
   private:
 	struct Flat {

@@ -265,6 +265,25 @@ class Oracle:
         return dict(bmin=bmin, bmax=bmax, keys=keys, sorted_to_orig=s2o, inverse=inv,
                     sorted_pos=self.gather4(pos4, s2o))
 
+    def reorder(self, box: Box, pos4):
+        """Patch::reorder_particles (src/PatchOperation/Patch.cpp:455-480): the
+        Morton sort with the periodic box origin .. origin + size as bounds.
+        Returns (sorted_to_orig, inverse)."""
+        o = np.array(list(box.origin), np.float32)
+        hi = (o + np.array(list(box.size), np.float32)).astype(np.float32)
+        keys, idx = self.morton_encode(pos4, o, hi)
+        _, s2o = self.sort_pairs(keys, idx)
+        return s2o, self.inverse(s2o)
+
+    @staticmethod
+    def remap_indices(indices, inv):
+        """RemapIndicesKernel (src/PatchOperation/ZOrderKernels/ZOrderKernels.h:87-101):
+        values in [0, len(inv)) go through inv, others stay."""
+        a = np.array(indices, np.int64)
+        ok = (a >= 0) & (a < len(inv))
+        a[ok] = np.asarray(inv, np.int64)[a[ok]]
+        return a.astype(np.int32)
+
     # -- pairlist ---------------------------------------------------------
     def select_cell_grid(self, extent, cutoff, n, max_pairs):
         m = C.c_int()
@@ -457,6 +476,7 @@ class RefHarness:
         L.ref_sort_pairs.argtypes = [vp, vp, sz]
         L.ref_inverse.argtypes = [vp, vp, sz]
         L.ref_reorder_pos.argtypes = [vp, vp, vp, sz]
+        L.ref_remap_indices.argtypes = [vp, sz, vp, sz]
         L.ref_cell_ranges.argtypes = [vp, sz, i, vp, vp]
         L.ref_cell_neighbors.argtypes = [vp, sz, i, vp, i, vp]
         L.ref_neighbor_walk.restype = u32
@@ -510,6 +530,11 @@ class RefHarness:
     def reorder_pos(self, pos4, s):
         out = np.zeros_like(pos4)
         self.lib.ref_reorder_pos(_ptr(pos4), _ptr(out), _ptr(s), len(s))
+        return out
+
+    def remap_indices(self, indices, inv):
+        out = np.ascontiguousarray(indices, np.int32).copy()
+        self.lib.ref_remap_indices(_ptr(out), out.size, _ptr(np.asarray(inv, np.uint32)), len(inv))
         return out
 
     def cell_ranges(self, keys, shift, num_cells):

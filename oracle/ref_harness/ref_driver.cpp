@@ -120,6 +120,13 @@ void ref_reorder_pos(const float* pos4, float* out4, const uint32_t* sorted, siz
 		k(i);
 }
 
+// RemapIndicesKernel (ZOrderKernels.h:87-101).
+void ref_remap_indices(int* indices, size_t count, const uint32_t* inv, size_t map_size) {
+	RemapIndicesKernel k{indices, inv, count, map_size};
+	for (size_t i = 0; i < count; ++i)
+		k(i);
+}
+
 // BuildCellRangesKernel (ZOrderNeighbor.h:27-43); begin/end must be zeroed.
 void ref_cell_ranges(const uint32_t* keys, size_t n, int shift, uint32_t* begin, uint32_t* end) {
 	BuildCellRangesKernel k{keys, begin, end, n, shift};

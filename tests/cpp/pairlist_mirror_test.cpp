@@ -286,6 +286,86 @@ static void langevin_stage_test(const Resource& res) {
 	EXPECT(m3[0].x == m2[0].x, "no second closing kick");
 }
 
+// Patch::reorder_particles through the mirror: arrays gathered, bonds and the
+// exclusion CSR remapped, and the rebuilt pair set equal to the old one
+// through the new -> old id map.
+static void reorder_stage_test(const Resource& res) {
+	const int n = 2000;
+	const float l = 60.0f, rc = 8.0f;
+	std::mt19937 rng(20261204);
+	std::uniform_real_distribution<float> u(0.0f, l);
+	std::vector<Vector3> h(n);
+	for (auto& p : h) p = Vector3(u(rng), u(rng), u(rng));
+	std::vector<std::pair<int, int>> excl;
+	std::vector<int> bonds;
+	for (int i = 0; i + 1 < n; i += 2) {
+		excl.push_back({i + 1, i});
+		bonds.push_back(i);
+		bonds.push_back(i + 1);
+	}
+	const PeriodicBox box(Vector3(0, 0, 0), Vector3(l, l, l));
+	B200Patch patch(res, n);
+	patch.set_periodic_box(box);
+	ExclusionCSR ex;
+	ex.build(excl, res);
+	patch.set_exclusions(ex.view());
+	DeviceBuffer<Vector3> pos(n, res);
+	DeviceBuffer<int> ids(n, res), bond_dev(bonds.size(), res);
+	pos.copy_from_host(h);
+	std::vector<int> id0(n);
+	for (int i = 0; i < n; ++i) id0[i] = i;
+	ids.copy_from_host(id0);
+	bond_dev.copy_from_host(bonds);
+	patch.pairlist().build_pairlist(pos, n, rc);
+	std::set<std::pair<int, int>> before;
+	for (const auto& q : device_pairs(patch.pairlist()))
+		before.insert({std::min(q.first, q.second), std::max(q.first, q.second)});
+
+	ParticleReorderManager every20(0, 20), every5(5, 20);
+	EXPECT(!every20.should_reorder(0) && every20.should_reorder(1) && !every20.should_reorder(2) &&
+			   every20.should_reorder(21) && every5.should_reorder(6) &&
+			   !every5.should_reorder(6, false),
+		   "reorder cadence: steps 1, 1 + period, ...; period falls back to the rebuild period");
+
+	ParticleArrays arrays;
+	arrays.pos = pos.data();
+	arrays.id = ids.data();
+	BondedIndices bi;
+	bi.bonds2 = bond_dev.data();
+	bi.num_bonds = bonds.size() / 2;
+	EXPECT(patch.reorder_particles(box, arrays, n, bi, &ex), "reorder runs on a valid box");
+	std::vector<Vector3> h1;
+	std::vector<int> id1, b1;
+	pos.copy_to_host(h1);
+	ids.copy_to_host(id1);
+	bond_dev.copy_to_host(b1);
+	std::vector<int> inv(n, -1);
+	bool perm = true, gathered = true;
+	for (int s = 0; s < n; ++s) {
+		const int o = id1[s];
+		if (o < 0 || o >= n || inv[o] != -1) {
+			perm = false;
+			break;
+		}
+		inv[o] = s;
+		gathered = gathered && h1[s].x == h[o].x && h1[s].y == h[o].y && h1[s].z == h[o].z;
+	}
+	EXPECT(perm && gathered, "reorder: ids a permutation, positions gathered by it");
+	bool remapped = perm;
+	for (size_t k = 0; remapped && k < bonds.size(); ++k) remapped = b1[k] == inv[bonds[k]];
+	EXPECT(remapped, "reorder: bond indices through the inverse map");
+	patch.pairlist().build_pairlist(pos, n, rc);
+	std::set<std::pair<int, int>> after;
+	for (const auto& q : device_pairs(patch.pairlist())) {
+		const int a = id1[q.first], b = id1[q.second];
+		after.insert({std::min(a, b), std::max(a, b)});
+	}
+	EXPECT(!before.empty() && after == before,
+		   "reorder: rebuilt pair set (with remapped exclusions) equals the old one");
+	const PeriodicBox flat(Vector3(0, 0, 0), Vector3(l, 0.0f, l));
+	EXPECT(!patch.reorder_particles(flat, arrays, n, bi, &ex), "degenerate box skips the reorder");
+}
+
 int main() {
 	Resource res;
 	res.device = 0;
@@ -296,6 +376,7 @@ int main() {
 		error_tests(res);
 		patch_stage_test(res);
 		langevin_stage_test(res);
+		reorder_stage_test(res);
 	} catch (const std::exception& e) {
 		std::printf("FAIL unexpected exception: %s\n", e.what());
 		++failures;

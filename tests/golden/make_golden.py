@@ -297,9 +297,37 @@ def baoab(O, R):
                 **_box_arrays(box.origin, box.size, box.periodic), **out)
 
 
+def reorder(O, R):
+    """Canonical Morton reorder of a bonded system (8 chains x 64 beads, two
+    types, periodic 120 A box with origin -60 A): the permutation, the
+    permuted positions and the remapped bond / angle indices from the
+    reference's MortonEncodeKernel over the box, stable sort, InverseIndexKernel,
+    ReorderDataKernel and RemapIndicesKernel. The index arrays carry -1 and
+    out-of-range entries, which the remap leaves alone."""
+    rng = np.random.default_rng(SEED + 7)
+    nch, beads, L = 8, 64, 120.0
+    xyz = W._chains(rng, nch, beads, L) - L / 2
+    n = nch * beads
+    pos = np.zeros((n, 4), np.float32)
+    pos[:, :3] = xyz.astype(np.float32)
+    pos[:, 3] = rng.integers(0, 2, n).astype(np.float32)
+    bonds, angles, excl = W._topology(nch, beads)
+    extra = np.array([[-1, 3], [n, 5], [7, n + 100]], np.int32)
+    idx_in = np.concatenate([bonds.reshape(-1), angles.reshape(-1), extra.reshape(-1)])
+    origin, size = np.full(3, -L / 2, np.float32), np.full(3, L, np.float32)
+    bmax = (origin + size).astype(np.float32)
+    keys, idx = R.morton_encode(pos, origin, bmax)
+    keys, s2o = R.sort_pairs(keys, idx)
+    inv = R.inverse(s2o)
+    return dict(pos=pos, **_box_arrays(origin, size, (1, 1, 1)), bonds=bonds, angles=angles,
+                exclusions=excl, indices=idx_in, keys=keys, s2o=s2o, inverse=inv,
+                pos_after=R.reorder_pos(pos, s2o), indices_after=R.remap_indices(idx_in, inv),
+                rc_list=np.float32(25.0))
+
+
 CASES = {"uniform4096": uniform, "lattice_open": lattice, "polymer_excl": polymer,
          "chain129": chain, "philox": philox, "grid_bd": grid_bd, "wrap_table": wrap_table,
-         "baoab": baoab}
+         "baoab": baoab, "reorder": reorder}
 
 
 def main():

@@ -37,6 +37,45 @@ def _canon(pairs):
 
 # --- Z-order sort ----------------------------------------------------------------------
 
+def test_reorder_matches_reference(oracle):
+    """Canonical reorder: permutation over the box bounds, gathered positions
+    and remapped indices (with -1 and out-of-range entries) bit-exact."""
+    d = _load("reorder")
+    s2o, inv = oracle.reorder(_box(d), d["pos"])
+    assert np.array_equal(s2o, d["s2o"])
+    assert np.array_equal(inv, d["inverse"])
+    assert np.array_equal(oracle.gather4(d["pos"], s2o), d["pos_after"])
+    assert np.array_equal(oracle.remap_indices(d["indices"], inv), d["indices_after"])
+
+
+def test_host_exclusion_csr_matches_oracle(oracle):
+    """The host layer's exclusion CSR (engine.exclusion_csr, rebuilt after a
+    reorder) equals the oracle's restatement word for word."""
+    from mars_md_b200.engine import exclusion_csr
+    d = _load("reorder")
+    excl = d["inverse"].astype(np.int64)[d["exclusions"].astype(np.int64)]
+    _, off, nb, npart = exclusion_csr(excl)
+    o_off, o_nb, o_n = oracle.exclusion_csr(excl.astype(np.int32))
+    assert npart == o_n
+    assert np.array_equal(off, o_off[:npart + 1])
+    assert np.array_equal(nb, o_nb[:len(nb)]) and len(nb) == 2 * len(excl)
+    e0, off0, nb0, n0 = exclusion_csr(np.zeros((0, 2), np.int32))
+    assert n0 == 0 and len(nb0) == 0
+
+
+def test_reorder_cadence_and_original_order():
+    from mars_md_b200.engine import ReorderManager, to_original_order
+    m = ReorderManager(0, rebuild_period=20)
+    assert [s for s in range(60) if m.should_reorder(s)] == [1, 21, 41]
+    assert not ReorderManager(5).should_reorder(6, bonded_prepared=False)
+    assert not ReorderManager(0, 0).should_reorder(1)
+    d = _load("reorder")
+    out = to_original_order(d["pos_after"], d["s2o"])
+    assert np.array_equal(out, d["pos"])
+    with pytest.raises(ValueError):
+        to_original_order(d["pos_after"][:2], np.array([0, 5]))
+
+
 @pytest.mark.parametrize("name", ["uniform4096", "lattice_open"])
 def test_morton_sort_matches_reference(oracle, name):
     d = _load(name)
