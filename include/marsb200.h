@@ -135,10 +135,36 @@ MB2_API int mb2_set_pair_tables(mb2_context* ctx, int num_types, const uint32_t*
                         int num_tables, const float* values, const uint32_t* sizes,
                         const float* starts, const float* step_invs);
 
-/* Tabulated pair forces over the last pairlist, ACCUMULATED into
- * force_energy (original order; energy halves into .w when get_energy).
- * Replaces launch_resolve_pair_tables + launch_pairwise_nonbonded
- * (src/Interactions/NonBondedInteraction.h:205-296) with the tabulated term. */
+/* Analytical pair terms: per-type charge, softcore radius and eps
+ * (ParticleTypeView::charge/radius/eps, src/Objects/DeviceParticle.h:49-53)
+ * and the run-wide constants (SolventParams,
+ * src/Interactions/NonBondedInteraction.h:123-129, set on the functors by
+ * launch_pairwise_nonbonded, :289-293; GaussianPotential amp / sigma /
+ * cutoff^2, src/Interactions/Nonbonded/Pairwise.h:50-53, which that launcher
+ * leaves at 1, 1, 0). params NULL = those defaults. Tag bits of the term
+ * matrix (AnalyticalPairTerm, Pairwise.h:19-27): 1 Coulomb, 2 Debye-Hueckel,
+ * 4 Onck, 8 Gaussian, 16 softcore, 32 tabulated; a tag may combine them. A
+ * matrix with analytical bits needs this call before mb2_pair_forces. */
+typedef struct {
+    float debye_length;        /* A */
+    float dielectric;
+    float onck_kappa;          /* 1/A */
+    float onck_sz;
+    float onck_z;              /* A */
+    float gaussian_amp;
+    float gaussian_sigma;      /* A */
+    float gaussian_cutoff_sq;  /* A^2, <= 0: none */
+} mb2_pair_params;
+MB2_API int mb2_set_pair_terms(mb2_context* ctx, int num_types, const float* charge,
+                               const float* radius, const float* eps,
+                               const mb2_pair_params* params);
+
+/* Pair forces over the last pairlist, ACCUMULATED into force_energy
+ * (original order; energy halves into .w when get_energy). Replaces
+ * launch_resolve_pair_tables + launch_pairwise_nonbonded
+ * (src/Interactions/NonBondedInteraction.h:205-296): per pair, the terms of
+ * its type pair's tag summed in PairNonbondedComputer's order (Coulomb,
+ * Debye-Hueckel, Onck, Gaussian, softcore, tabulated; Pairwise.h:214-304). */
 MB2_API int mb2_pair_forces(mb2_context* ctx, const float* pos4, const int* type_ids,
                     float* force_energy4, uint32_t n, float cutoff, int get_energy,
                     void* stream);
@@ -148,12 +174,19 @@ MB2_API int mb2_pair_forces(mb2_context* ctx, const float* pos4, const int* type
  * New on this path: the reference sums per-particle floats on the host
  * (src/SimManager.cpp:1000-1075). */
 MB2_API int mb2_energies(mb2_context* ctx, void* stream, double out[4]);
+/* The same reductions with the remaining terms: out[0..count) of pair
+ * energy, pair virial, bond, angle, dihedral, restraint energy (count <= 6). */
+MB2_API int mb2_energy_terms(mb2_context* ctx, void* stream, double* out, int count);
 MB2_API int mb2_reset_energies(mb2_context* ctx, void* stream);
 
 /* --- bonded forces ---------------------------------------------------------
- * Tables for bonds (kind 0, non-periodic) or angles (kind 1, periodic, radians).
- * Replaces DeviceBondedInteractions::link_tables
- * (src/Interactions/DeviceBondedInteraction.h:205-250). */
+ * Tables for bonds (kind 0, non-periodic), angles (kind 1, periodic, radians)
+ * or dihedrals (kind 2, periodic, radians). Replaces
+ * DeviceBondedInteractions::link_tables
+ * (src/Interactions/DeviceBondedInteraction.h:205-250). In every bonded call a
+ * row whose table_idx is negative is skipped: it stands for a form other than
+ * tabulated, which the reference's tabulated functors skip through forms[]
+ * (Bonded/BondComputer.h:165-166, 233-234, 301-302). */
 MB2_API int mb2_set_bonded_tables(mb2_context* ctx, int kind, int num_tables, const float* values,
                           const uint32_t* sizes, const float* starts, const float* step_invs);
 
@@ -168,6 +201,23 @@ MB2_API int mb2_bond_forces(mb2_context* ctx, const int* bonds2, const int* tabl
  * Bonded/BondComputer.h:204-269). */
 MB2_API int mb2_angle_forces(mb2_context* ctx, const int* angles4, const int* table_idx, uint32_t na,
                      const float* pos4, float* force_energy4, int get_energy, void* stream);
+
+/* Tabulated dihedral forces, accumulated. dihedrals: device int4 [nd].
+ * Replaces launch_tabulated_dihedrals (DeviceBondedInteraction.h:551-578,
+ * TabulatedDihedralComputer, Bonded/BondComputer.h:282-346, with
+ * DihedralGeometry, Bonded/BondGeometry.h:56-87): degenerate quadruples get
+ * no force, magnitudes are clamped to +-1000, energy quarters into .w. */
+MB2_API int mb2_dihedral_forces(mb2_context* ctx, const int* dihedrals4, const int* table_idx,
+                                uint32_t nd, const float* pos4, float* force_energy4,
+                                int get_energy, void* stream);
+
+/* Harmonic position restraints, accumulated: particle_ids device int [nr]
+ * (negative = skipped), anchors4 device float4 [nr], spring_k device float
+ * [nr]. Replaces launch_harmonic_restraints (DeviceBondedInteraction.h:599-620,
+ * HarmonicRestraintComputer, Bonded/BondComputer.h:88-131). */
+MB2_API int mb2_restraint_forces(mb2_context* ctx, const int* particle_ids, const float* anchors4,
+                                 const float* spring_k, uint32_t nr, const float* pos4,
+                                 float* force_energy4, int get_energy, void* stream);
 
 /* --- integrator ------------------------------------------------------------
  * Per-type data for the BD step (ParticleTypeView, src/Objects/DeviceParticle.h:49-64).
@@ -256,7 +306,8 @@ MB2_API int mb2_philox(mb2_context* ctx, uint64_t seed, uint32_t ctr0, uint32_t 
  * execute_integration run it (src/SimManager.cpp:337-504) for one patch:
  * clear forces, rebuild the pairlist when (step - 1) % rebuild_period == 0
  * (unless the skin check says the list is still valid), pair forces, bonded
- * forces (if bonds/angles were given), BD integrate. All device pointers. */
+ * forces (bonds, angles, dihedrals, restraints where given), BD integrate.
+ * All device pointers. */
 typedef struct {
     float pairlist_cutoff;
     float cutoff;
@@ -273,6 +324,13 @@ typedef struct {
     const int* angles4;  /* may be NULL */
     const int* angle_table_idx;
     uint32_t num_angles;
+    const int* dihedrals4;  /* may be NULL */
+    const int* dihedral_table_idx;
+    uint32_t num_dihedrals;
+    const int* restraint_ids;  /* may be NULL */
+    const float* restraint_anchors4;
+    const float* restraint_k;
+    uint32_t num_restraints;
 } mb2_step_params;
 
 MB2_API int mb2_step(mb2_context* ctx, float* pos4, float* force_energy4, const int* type_ids,

@@ -30,7 +30,19 @@ class StepParams(C.Structure):
                 ("seed", C.c_uint64), ("patch_id", C.c_uint64), ("efield", C.c_float * 3),
                 ("get_energy", C.c_int), ("bonds2", C.c_void_p), ("bond_table_idx", C.c_void_p),
                 ("num_bonds", C.c_uint32), ("angles4", C.c_void_p),
-                ("angle_table_idx", C.c_void_p), ("num_angles", C.c_uint32)]
+                ("angle_table_idx", C.c_void_p), ("num_angles", C.c_uint32),
+                ("dihedrals4", C.c_void_p), ("dihedral_table_idx", C.c_void_p),
+                ("num_dihedrals", C.c_uint32), ("restraint_ids", C.c_void_p),
+                ("restraint_anchors4", C.c_void_p), ("restraint_k", C.c_void_p),
+                ("num_restraints", C.c_uint32)]
+
+
+class PairParams(C.Structure):
+    """mb2_pair_params (defaults: the reference's SolventParams and Gaussian)."""
+    _fields_ = [("debye_length", C.c_float), ("dielectric", C.c_float),
+                ("onck_kappa", C.c_float), ("onck_sz", C.c_float), ("onck_z", C.c_float),
+                ("gaussian_amp", C.c_float), ("gaussian_sigma", C.c_float),
+                ("gaussian_cutoff_sq", C.c_float)]
 
 
 class BatchTuning(C.Structure):
@@ -92,6 +104,10 @@ def load(path: str = LIB_PATH):
     L.mb2_profile_read.argtypes = [vp, i, C.POINTER(C.c_double), u32p]
     L.mb2_launch_count.restype = u64
     L.mb2_launch_count.argtypes = []
+    L.mb2_set_pair_terms.argtypes = [vp, i, fp, fp, fp, C.POINTER(PairParams)]
+    L.mb2_dihedral_forces.argtypes = [vp, vp, vp, u32, vp, vp, i, vp]
+    L.mb2_restraint_forces.argtypes = [vp, vp, vp, vp, u32, vp, vp, i, vp]
+    L.mb2_energy_terms.argtypes = [vp, vp, C.POINTER(C.c_double), i]
     L.mb2_reorder_begin.argtypes = [vp, vp, u32, vp]
     L.mb2_reorder_apply.argtypes = [vp, vp, u32, u32, vp]
     L.mb2_reorder_remap.argtypes = [vp, vp, u64, vp]

@@ -14,6 +14,10 @@ namespace mb2 {
 unsigned long long g_launches = 0;
 }
 
+// FP64 reduction slots: pair energy, pair virial, bond, angle, dihedral and
+// restraint energy.
+constexpr int kEnergySlots = 6;
+
 struct mb2_context {
 	int device = 0;
 	uint32_t max_particles = 0;
@@ -52,10 +56,19 @@ struct mb2_context {
 	DevBuf<float> bin_force;
 	DevBuf<float2> bin_energy;
 
-	// bonded tables
-	DevBuf<Table> bonded_tables[2];
-	DevBuf<float> bonded_values[2];
-	int bonded_count[2] = {0, 0};
+	// analytical pair terms: the tag matrix as set, per-type constants, and
+	// the per-type-pair table built from both
+	std::vector<uint32_t> term_matrix_h;
+	bool pair_terms_set = false;
+	std::vector<float> term_charge, term_radius, term_eps;
+	PairSolvent solvent{};
+	float term_dielectric = 80.0f;
+	DevBuf<PairTermRef> term_refs;
+
+	// bonded tables: 0 bonds, 1 angles, 2 dihedrals
+	DevBuf<Table> bonded_tables[3];
+	DevBuf<float> bonded_values[3];
+	int bonded_count[3] = {0, 0, 0};
 
 	// particle types and grids
 	TypeTable types;
@@ -68,7 +81,7 @@ struct mb2_context {
 	std::vector<GridView> host_grids;
 	DevBuf<GridView> grids;
 
-	uint32_t bonded_bins[2] = {0, 0};  // values in the bond / angle tables
+	uint32_t bonded_bins[3] = {0, 0, 0};  // values in the bond / angle / dihedral tables
 	DevBuf<uint32_t> ro_keys, ro_s2o, ro_inv;  // canonical reorder permutation
 	DevBuf<float4> ro_tmp;
 	uint32_t ro_n = 0;
@@ -336,6 +349,12 @@ void build(mb2_context* ctx, const float4* pos, const int* type_ids, uint32_t n,
 	ctx->rdf_built = false;
 }
 
+bool matrix_has_analytical(const mb2_context* ctx) {
+	for (uint32_t tag : ctx->term_matrix_h)
+		if (tag & kTermAnalytical) return true;
+	return false;
+}
+
 // Pair kernel over the sorted positions into the zeroed sorted accumulator.
 void pair_kernel(mb2_context* ctx, uint32_t n, float cutoff, int get_energy, cudaStream_t st) {
 	require(ctx->built, MB2_ERR_STATE, "mb2_pair_forces: no pairlist; call mb2_build_pairlist");
@@ -343,6 +362,8 @@ void pair_kernel(mb2_context* ctx, uint32_t n, float cutoff, int get_energy, cud
 			"mb2_pair_forces: particle count differs from the last pairlist build");
 	require(ctx->pt.num_types > 0, MB2_ERR_STATE,
 			"mb2_pair_forces: no pair tables; call mb2_set_pair_tables");
+	require(ctx->pt.terms || !matrix_has_analytical(ctx), MB2_ERR_STATE,
+			"mb2_pair_forces: the tags carry analytical terms; call mb2_set_pair_terms");
 	ctx->force_sorted.ensure(n);
 	MB2_CUDA(cudaMemsetAsync(ctx->force_sorted.ptr, 0, static_cast<size_t>(n) * sizeof(float4), st));
 	const float cutoff_sq = cutoff > 0.0f ? cutoff * cutoff : 0.0f;
@@ -394,6 +415,70 @@ void upload_tables(DevBuf<Table>& tbuf, DevBuf<float>& vbuf, int num_tables, con
 	if (total_out) *total_out = static_cast<uint32_t>(total);
 }
 
+// Per-type-pair analytical constants from the tag matrix and the per-type
+// data, each rounded as PairNonbondedComputer rounds it per pair
+// (Pairwise.h:248-283, Columb.h:11-97). Leaves pt.terms null when no type
+// pair has an analytical term (the tabulated-only kernel then runs).
+void rebuild_pair_terms(mb2_context* ctx) {
+	ctx->pt.terms = nullptr;
+	if (!ctx->pair_terms_set || !matrix_has_analytical(ctx)) return;
+	const int T = ctx->pt.num_types;
+	require(static_cast<int>(ctx->term_charge.size()) >= T, MB2_ERR_STATE,
+			"mb2_set_pair_terms: fewer types than the pair tables");
+	std::vector<PairTermRef> h(static_cast<size_t>(T) * T);
+	for (int a = 0; a < T; ++a)
+		for (int b = 0; b < T; ++b) {
+			PairTermRef& r = h[static_cast<size_t>(a) * T + b];
+			r.terms = ctx->term_matrix_h[static_cast<size_t>(a) * T + b] & kTermAnalytical;
+			volatile float qq = ctx->term_charge[a] * ctx->term_charge[b];
+			volatile float qc = qq * kCoulomb;
+			volatile float adh = qc / ctx->term_dielectric;
+			volatile float rad = 0.5f * (ctx->term_radius[a] + ctx->term_radius[b]);
+			volatile float rad2 = rad * rad;
+			volatile float rad4 = rad2 * rad2;
+			volatile float rad6 = rad4 * rad2;
+			volatile float ee = ctx->term_eps[a] * ctx->term_eps[b];
+			r.qq = qq;
+			r.a_onck = qc;
+			r.a_dh = adh;
+			r.rad6 = rad6;
+			r.eps = std::sqrt(static_cast<float>(ee));
+			r.pad0 = r.pad1 = 0.0f;
+		}
+	ctx->term_refs.ensure(h.size());
+	MB2_CUDA(cudaMemcpy(ctx->term_refs.ptr, h.data(), h.size() * sizeof(PairTermRef),
+						cudaMemcpyHostToDevice));
+	ctx->pt.terms = ctx->term_refs.ptr;
+	ctx->pt.solvent = ctx->solvent;
+}
+
+// Bonded terms of one step into ForceEnergy (Patch::calculate_bonded_forces,
+// Patch.cpp:180-234): bonds, angles, dihedrals, restraints.
+void bonded_stage(mb2_context* ctx, const float4* pos, float4* fe, const mb2_step_params* prm,
+				  int get_energy, cudaStream_t st) {
+	if (prm->num_bonds)
+		bond_forces(reinterpret_cast<const int2*>(prm->bonds2), prm->bond_table_idx,
+					prm->num_bonds, pos, fe, ctx->bonded_tables[0].ptr, ctx->box, get_energy,
+					ctx->energy.ptr + 2, st);
+	if (prm->num_angles)
+		angle_forces(reinterpret_cast<const int4*>(prm->angles4), prm->angle_table_idx,
+					 prm->num_angles, pos, fe, ctx->bonded_tables[1].ptr, ctx->box, get_energy,
+					 ctx->energy.ptr + 3, st);
+	if (prm->num_dihedrals)
+		dihedral_forces(reinterpret_cast<const int4*>(prm->dihedrals4), prm->dihedral_table_idx,
+						prm->num_dihedrals, pos, fe, ctx->bonded_tables[2].ptr, ctx->box,
+						get_energy, ctx->energy.ptr + 4, st);
+	if (prm->num_restraints)
+		restraint_forces(prm->restraint_ids, reinterpret_cast<const float4*>(prm->restraint_anchors4),
+						 prm->restraint_k, prm->num_restraints, pos, fe, ctx->box, get_energy,
+						 ctx->energy.ptr + 5, st);
+}
+
+bool step_has_bonded(const mb2_step_params* prm) {
+	return prm->num_bonds != 0 || prm->num_angles != 0 || prm->num_dihedrals != 0 ||
+		   prm->num_restraints != 0;
+}
+
 // One step of the window without the rebuild decision (the segment's list
 // was built at its first step): the mb2_step sequence otherwise.
 void window_step(mb2_context* ctx, float4* pos, float4* fe, const int* type_ids, uint32_t n,
@@ -436,8 +521,8 @@ int mb2_create(int device, uint32_t max_particles, mb2_context** out) {
 	ctx->max_particles = max_particles;
 	const int rc = guarded(ctx, [&] {
 		MB2_CUDA(cudaMallocHost(&ctx->pinned, 64));
-		ctx->energy.ensure(4);
-		MB2_CUDA(cudaMemset(ctx->energy.ptr, 0, 4 * sizeof(double)));
+		ctx->energy.ensure(kEnergySlots);
+		MB2_CUDA(cudaMemset(ctx->energy.ptr, 0, kEnergySlots * sizeof(double)));
 	});
 	if (rc != MB2_OK) {
 		delete ctx;
@@ -608,6 +693,38 @@ int mb2_set_pair_tables(mb2_context* ctx, int num_types, const uint32_t* term_ma
 		ctx->pt.refs = ctx->refs.ptr;
 		ctx->pt.bin_force = ctx->bin_force.ptr;
 		ctx->pt.bin_energy = ctx->bin_energy.ptr;
+		ctx->term_matrix_h.assign(term_matrix, term_matrix + tt);
+		rebuild_pair_terms(ctx);
+	});
+}
+
+int mb2_set_pair_terms(mb2_context* ctx, int num_types, const float* charge, const float* radius,
+					   const float* eps, const mb2_pair_params* params) {
+	return guarded(ctx, [&] {
+		require(num_types > 0 && num_types <= 64 && charge && radius && eps, MB2_ERR_ARG,
+				"mb2_set_pair_terms: 1..64 types with charge, radius and eps");
+		mb2_pair_params p{10.0f, 80.0f, 0.1f, 80.0f, 6.86f, 1.0f, 1.0f, 0.0f};
+		if (params) p = *params;
+		require(p.debye_length > 0.0f && p.dielectric != 0.0f && p.onck_z > 0.0f &&
+					p.gaussian_sigma != 0.0f,
+				MB2_ERR_ARG, "mb2_set_pair_terms: bad solvent or Gaussian constants");
+		ctx->term_charge.assign(charge, charge + num_types);
+		ctx->term_radius.assign(radius, radius + num_types);
+		ctx->term_eps.assign(eps, eps + num_types);
+		ctx->term_dielectric = p.dielectric;
+		PairSolvent& sv = ctx->solvent;
+		sv.dh_len = p.debye_length;
+		sv.dh_inv_len = 1.0f / p.debye_length;
+		sv.onck_kappa = p.onck_kappa;
+		sv.onck_sz = p.onck_sz;
+		sv.onck_z = p.onck_z;
+		sv.onck_two_z = 2.0f * p.onck_z;
+		sv.g_amp = p.gaussian_amp;
+		volatile float s2 = p.gaussian_sigma * p.gaussian_sigma;
+		sv.g_inv_s2 = 1.0f / s2;
+		sv.g_cut2 = p.gaussian_cutoff_sq;
+		ctx->pair_terms_set = true;
+		if (ctx->pt.num_types > 0) rebuild_pair_terms(ctx);
 	});
 }
 
@@ -632,19 +749,29 @@ int mb2_energies(mb2_context* ctx, void* stream, double out[4]) {
 	});
 }
 
+int mb2_energy_terms(mb2_context* ctx, void* stream, double* out, int count) {
+	return guarded(ctx, [&] {
+		require(out && count > 0, MB2_ERR_ARG, "mb2_energy_terms: null output");
+		const int c = std::min(count, kEnergySlots);
+		MB2_CUDA(cudaMemcpyAsync(out, ctx->energy.ptr, c * sizeof(double), cudaMemcpyDeviceToHost,
+								 S(stream)));
+		MB2_CUDA(cudaStreamSynchronize(S(stream)));
+	});
+}
+
 int mb2_reset_energies(mb2_context* ctx, void* stream) {
 	return guarded(ctx, [&] {
-		MB2_CUDA(cudaMemsetAsync(ctx->energy.ptr, 0, 4 * sizeof(double), S(stream)));
+		MB2_CUDA(cudaMemsetAsync(ctx->energy.ptr, 0, kEnergySlots * sizeof(double), S(stream)));
 	});
 }
 
 int mb2_set_bonded_tables(mb2_context* ctx, int kind, int num_tables, const float* values,
 						  const uint32_t* sizes, const float* starts, const float* step_invs) {
 	return guarded(ctx, [&] {
-		require(kind == 0 || kind == 1, MB2_ERR_ARG, "mb2_set_bonded_tables: kind is 0 or 1");
+		require(kind >= 0 && kind <= 2, MB2_ERR_ARG, "mb2_set_bonded_tables: kind is 0, 1 or 2");
 		require(num_tables > 0, MB2_ERR_ARG, "mb2_set_bonded_tables: no tables");
 		upload_tables(ctx->bonded_tables[kind], ctx->bonded_values[kind], num_tables, values, sizes,
-					  starts, step_invs, kind == 1 ? 1 : 0, &ctx->bonded_bins[kind]);
+					  starts, step_invs, kind >= 1 ? 1 : 0, &ctx->bonded_bins[kind]);
 		ctx->bonded_count[kind] = num_tables;
 	});
 }
@@ -670,6 +797,36 @@ int mb2_angle_forces(mb2_context* ctx, const int* angles4, const int* table_idx,
 					 reinterpret_cast<const float4*>(pos4), reinterpret_cast<float4*>(force_energy4),
 					 ctx->bonded_tables[1].ptr, ctx->box, get_energy, ctx->energy.ptr + 3,
 					 S(stream));
+	});
+}
+
+int mb2_dihedral_forces(mb2_context* ctx, const int* dihedrals4, const int* table_idx,
+						uint32_t nd, const float* pos4, float* force_energy4, int get_energy,
+						void* stream) {
+	return guarded(ctx, [&] {
+		require(ctx->box_set, MB2_ERR_STATE, "mb2_dihedral_forces: no box");
+		require(nd == 0 || ctx->bonded_count[2] > 0, MB2_ERR_STATE,
+				"mb2_dihedral_forces: no tables");
+		require(nd == 0 || (dihedrals4 && table_idx && pos4 && force_energy4), MB2_ERR_ARG,
+				"mb2_dihedral_forces: null argument");
+		dihedral_forces(reinterpret_cast<const int4*>(dihedrals4), table_idx, nd,
+						reinterpret_cast<const float4*>(pos4),
+						reinterpret_cast<float4*>(force_energy4), ctx->bonded_tables[2].ptr,
+						ctx->box, get_energy, ctx->energy.ptr + 4, S(stream));
+	});
+}
+
+int mb2_restraint_forces(mb2_context* ctx, const int* particle_ids, const float* anchors4,
+						 const float* spring_k, uint32_t nr, const float* pos4,
+						 float* force_energy4, int get_energy, void* stream) {
+	return guarded(ctx, [&] {
+		require(ctx->box_set, MB2_ERR_STATE, "mb2_restraint_forces: no box");
+		require(nr == 0 || (particle_ids && anchors4 && spring_k && pos4 && force_energy4),
+				MB2_ERR_ARG, "mb2_restraint_forces: null argument");
+		restraint_forces(particle_ids, reinterpret_cast<const float4*>(anchors4), spring_k, nr,
+						 reinterpret_cast<const float4*>(pos4),
+						 reinterpret_cast<float4*>(force_energy4), ctx->box, get_energy,
+						 ctx->energy.ptr + 5, S(stream));
 	});
 }
 
@@ -910,7 +1067,9 @@ int mb2_step(mb2_context* ctx, float* pos4, float* force_energy4, const int* typ
 		// term into it. Here pair forces stay in the Z-ordered accumulator and
 		// the integrate kernel gathers them, adding what the bonded kernels
 		// wrote; ForceEnergy is cleared only when those run.
-		const bool bonded = prm->num_bonds != 0 || prm->num_angles != 0;
+		const bool bonded = step_has_bonded(prm);
+		require(prm->num_dihedrals == 0 || ctx->bonded_count[2] > 0, MB2_ERR_STATE,
+				"mb2_step: dihedrals without dihedral tables");
 		if (bonded)
 			MB2_CUDA(cudaMemsetAsync(fe, 0, static_cast<size_t>(n) * sizeof(float4), st));
 		// Rebuild schedule and skin check (Patch.cpp:86-108)
@@ -925,14 +1084,7 @@ int mb2_step(mb2_context* ctx, float* pos4, float* force_energy4, const int* typ
 			pack_sorted_positions(pos, type_ids, ctx->s2o.ptr, n, ctx->sorted_pos.ptr, st);
 		if (n == 0) return;
 		pair_kernel(ctx, n, prm->cutoff, prm->get_energy, st);
-		if (prm->num_bonds)
-			bond_forces(reinterpret_cast<const int2*>(prm->bonds2), prm->bond_table_idx,
-						prm->num_bonds, pos, fe, ctx->bonded_tables[0].ptr, ctx->box,
-						prm->get_energy, ctx->energy.ptr + 2, st);
-		if (prm->num_angles)
-			angle_forces(reinterpret_cast<const int4*>(prm->angles4), prm->angle_table_idx,
-						 prm->num_angles, pos, fe, ctx->bonded_tables[1].ptr, ctx->box,
-						 prm->get_energy, ctx->energy.ptr + 3, st);
+		bonded_stage(ctx, pos, fe, prm, prm->get_energy, st);
 		BdParams p{prm->dt, prm->kT, static_cast<uint32_t>(step),
 				   mb2_bd_seed(prm->seed, prm->patch_id, step), 0u,
 				   {prm->efield[0], prm->efield[1], prm->efield[2]}};
@@ -950,6 +1102,10 @@ int mb2_window_forward(mb2_context* ctx, float* pos4, float* force_energy4, cons
 				"mb2_window_forward: null argument");
 		require(ctx->types_set && ctx->types.num_grids == 0, MB2_ERR_STATE,
 				"mb2_window_forward: particle types without grids are required");
+		require(!matrix_has_analytical(ctx) && prm->num_dihedrals == 0 &&
+					prm->num_restraints == 0,
+				MB2_ERR_STATE,
+				"mb2_window_forward: tabulated pair, bond and angle terms only");
 		require(checkpoint_every > 0 && prm->rebuild_period > 0 &&
 					prm->rebuild_period % checkpoint_every == 0 &&
 					(first_step - 1) % checkpoint_every == 0,

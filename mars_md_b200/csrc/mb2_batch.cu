@@ -478,8 +478,9 @@ void check_step_args(mb2_batch* b, const float* pos4, const float* fe4, const in
 	expect_arg(b->types_set, MB2_ERR_STATE, "mb2_batch_step: call mb2_batch_set_particle_types");
 	expect_arg(b->pt.num_types > 0, MB2_ERR_STATE,
 			   "mb2_batch_step: call mb2_batch_set_pair_tables");
-	expect_arg(prm->num_bonds == 0 && prm->num_angles == 0, MB2_ERR_ARG,
-			   "mb2_batch_step: bonded terms are not supported in batched mode");
+	expect_arg(prm->num_bonds == 0 && prm->num_angles == 0 && prm->num_dihedrals == 0 &&
+				   prm->num_restraints == 0,
+			   MB2_ERR_ARG, "mb2_batch_step: bonded terms are not supported in batched mode");
 }
 
 // Rebuild decision of the reference (Patch.cpp:86-108), over all systems: at
@@ -587,6 +588,9 @@ int mb2_batch_set_pair_tables(mb2_batch* b, int num_types, const uint32_t* term_
 		const size_t total = pair_table_arrays(num_types, term_matrix, num_tables, values, sizes,
 											   starts, step_invs, refs, bf, be);
 		const int tt = num_types * num_types;
+		for (int k = 0; k < tt; ++k)
+			expect_arg(!(term_matrix[k] & kTermAnalytical), MB2_ERR_ARG,
+					   "mb2_batch_set_pair_tables: batched mode takes tabulated pair terms only");
 		expect_arg(tt * sizeof(PairTableRef) + total * 12 + 8 <= 200 * 1024, MB2_ERR_CAPACITY,
 				   "mb2_batch_set_pair_tables: tables exceed the 200 KB shared-memory budget");
 		b->refs.ensure(tt);

@@ -14,7 +14,15 @@
 namespace mb2 {
 
 constexpr uint32_t kInvalidCell = 0xFFFFFFFFu;  // ZOrderNeighbor.h stencil padding
+// AnalyticalPairTerm bits (src/Interactions/Nonbonded/Pairwise.h:19-27).
+constexpr uint32_t kTermCoulomb = 1u << 0;
+constexpr uint32_t kTermDebyeHuckel = 1u << 1;
+constexpr uint32_t kTermOnck = 1u << 2;
+constexpr uint32_t kTermGaussian = 1u << 3;
+constexpr uint32_t kTermSoftcore = 1u << 4;
 constexpr uint32_t kTermTabulated = 1u << 5;    // PAIR_TERM_TABULATED (Pairwise.h:25)
+constexpr uint32_t kTermAnalytical = 0x1Fu;     // every analytical bit
+constexpr float kCoulomb = 332.0636f;           // constants::COULOMB (src/Constants.h:24)
 constexpr uint32_t kTableShift = 8;             // kPairTableShift (Pairwise.h:30)
 constexpr uint32_t kFlagRbAttached = 1u << 2;   // FLAG_RB_ATTACHED (DeviceParticle.h)
 constexpr uint32_t kBdStream = 0x5324120u;      // BDIntegrate::rng_stream (BD.h:25)

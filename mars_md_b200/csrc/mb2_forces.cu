@@ -26,6 +26,7 @@
 // FP64: total pair energy and virial are reduced in double on the device
 // (per-thread double, block reduction, one double atomic per block).
 #include <algorithm>
+#include <type_traits>
 #include <vector>
 
 #include "marsb200.h"
@@ -72,15 +73,115 @@ __device__ __forceinline__ float wrap1(float x, float l, float inv, float half) 
 	return x >= half ? __fsub_rn(x, l) : x;
 }
 
+// math::sinh_minus_x / x_cosh_minus_sinh (src/Types/Math.h:199-216): the
+// reference's series below |x| = 1, the direct difference above.
+__device__ __forceinline__ float sinh_minus_x(float x) {
+	if (x >= 1.0f || x <= -1.0f) return __fsub_rn(sinhf(x), x);
+	constexpr float c0 = static_cast<float>(1.0 / 6), c1 = static_cast<float>(1.0 / 120),
+					c2 = static_cast<float>(1.0 / 5040), c3 = static_cast<float>(1.0 / 362880);
+	const float w = __fmul_rn(x, x);
+	return __fmul_rn(__fmul_rn(x, w),
+					 __fadd_rn(c0, __fmul_rn(w, __fadd_rn(c1, __fmul_rn(w, __fadd_rn(c2, __fmul_rn(w, c3)))))));
+}
+
+__device__ __forceinline__ float x_cosh_minus_sinh(float x) {
+	if (x >= 1.0f || x <= -1.0f) return __fsub_rn(__fmul_rn(x, coshf(x)), sinhf(x));
+	constexpr float c0 = static_cast<float>(1.0 / 3), c1 = static_cast<float>(1.0 / 30),
+					c2 = static_cast<float>(1.0 / 840), c3 = static_cast<float>(1.0 / 45360);
+	const float w = __fmul_rn(x, x);
+	return __fmul_rn(__fmul_rn(x, w),
+					 __fadd_rn(c0, __fmul_rn(w, __fadd_rn(c1, __fmul_rn(w, __fadd_rn(c2, __fmul_rn(w, c3)))))));
+}
+
+// OnckElecPotential::dielectric and dielectric_deriv
+// (src/Interactions/Nonbonded/Columb.h:68-84).
+__device__ __forceinline__ float onck_dielectric(float r, const PairSolvent& s) {
+	const float v = __fdiv_rn(r, s.onck_two_z);
+	if (v < 1e-5f) return __fdiv_rn(__fmul_rn(__fmul_rn(s.onck_sz, v), v), 3.0f);
+	const float sh = sinhf(v);
+	return __fdiv_rn(__fmul_rn(__fmul_rn(s.onck_sz, sinh_minus_x(v)), __fadd_rn(sh, v)),
+					 __fmul_rn(sh, sh));
+}
+
+__device__ __forceinline__ float onck_dielectric_deriv(float r, const PairSolvent& s) {
+	const float v = __fdiv_rn(r, s.onck_two_z);
+	if (v < 1e-5f) return __fdiv_rn(__fmul_rn(s.onck_sz, v), __fmul_rn(3.0f, s.onck_z));
+	const float sh = sinhf(v);
+	return __fdiv_rn(__fmul_rn(__fmul_rn(s.onck_sz, v), x_cosh_minus_sinh(v)),
+					 __fmul_rn(__fmul_rn(__fmul_rn(s.onck_z, sh), sh), sh));
+}
+
+// The analytical terms of PairNonbondedComputer::operator()
+// (src/Interactions/Nonbonded/Pairwise.h:246-283), added in its order into
+// the pair's force magnitude (-dU/dr) and energy: Coulomb (Columb.h:11-20),
+// Debye-Hueckel (Columb.h:29-42), Onck (Columb.h:86-97), Gaussian
+// (Pairwise.h:55-68), softcore (Pairwise.h:82-100; its dU/dr / r becomes
+// -dU/dr by -F r). d = |r|, d2v = r . r of the wrapped vector.
+__device__ __forceinline__ void analytic_terms(uint32_t terms, const PairTermRef& a,
+											   const PairSolvent& s, float d, float d2v,
+											   float& fm, float& en) {
+	if (terms & kTermCoulomb) {
+		const float inv_d2 = __frcp_rn(__fmul_rn(d, d));
+		const float inv_d = __frcp_rn(d);
+		fm = __fadd_rn(fm, __fmul_rn(__fmul_rn(a.qq, inv_d2), kCoulomb));
+		en = __fadd_rn(en, __fmul_rn(__fmul_rn(a.qq, inv_d), kCoulomb));
+	}
+	if (terms & kTermDebyeHuckel) {
+		const float inv_r = __frcp_rn(d);
+		const float screen = expf(__fdiv_rn(-d, s.dh_len));
+		const float e = __fmul_rn(__fmul_rn(a.a_dh, screen), inv_r);
+		fm = __fadd_rn(fm, __fmul_rn(e, __fadd_rn(inv_r, s.dh_inv_len)));
+		en = __fadd_rn(en, e);
+	}
+	if (terms & kTermOnck) {
+		const float r = d < 1e-2f ? 1e-2f : d;
+		const float screen = expf(__fmul_rn(-s.onck_kappa, r));
+		const float eps = onck_dielectric(r, s);
+		const float er = __fmul_rn(eps, r);
+		const float as = __fmul_rn(a.a_onck, screen);
+		const float eps_p = onck_dielectric_deriv(r, s);
+		const float t1 = __fdiv_rn(s.onck_kappa, er);
+		const float t2 = __fdiv_rn(__fadd_rn(__fmul_rn(eps_p, r), eps),
+								   __fmul_rn(__fmul_rn(__fmul_rn(eps, eps), r), r));
+		fm = __fadd_rn(fm, __fmul_rn(as, __fadd_rn(t1, t2)));
+		en = __fadd_rn(en, __fdiv_rn(as, er));
+	}
+	if (terms & kTermGaussian) {
+		const float g2 = __fmul_rn(d, d);
+		if (!(s.g_cut2 > 0.0f && g2 > s.g_cut2)) {
+			const float e = __fmul_rn(s.g_amp, expf(__fmul_rn(-g2, s.g_inv_s2)));
+			fm = __fadd_rn(fm, __fmul_rn(__fmul_rn(__fmul_rn(2.0f, d), e), s.g_inv_s2));
+			en = __fadd_rn(en, e);
+		}
+	}
+	if (terms & kTermSoftcore) {
+		const float d6 = __fmul_rn(__fmul_rn(d2v, d2v), d2v);
+		const float d6_2 = __fmul_rn(d6, d6);
+		const float rad6_2 = __fmul_rn(a.rad6, a.rad6);
+		const float f = __fmul_rn(__fmul_rn(-12.0f, a.eps),
+								  __fsub_rn(__fdiv_rn(rad6_2, __fmul_rn(d6_2, d2v)),
+											__fdiv_rn(a.rad6, __fmul_rn(d6, d2v))));
+		float e = 0.0f;
+		if (d6 < a.rad6)
+			e = __fadd_rn(__fmul_rn(a.eps, __fsub_rn(__fdiv_rn(rad6_2, d6_2),
+													 __fdiv_rn(__fmul_rn(2.0f, a.rad6), d6))),
+						  a.eps);
+		fm = __fadd_rn(fm, __fmul_rn(-f, d));
+		en = __fadd_rn(en, e);
+	}
+}
+
 // One pair of the half list, rounded as the reference rounds it. flip
-// (bit 31 of the entry): the reference orients the pair j -> i.
-template <bool kEnergy, bool kAllPeriodic>
+// (bit 31 of the entry): the reference orients the pair j -> i. With kTerms,
+// the analytical terms of the type pair come first, then the table.
+template <bool kEnergy, bool kAllPeriodic, bool kTerms>
 __device__ __forceinline__ void pair_scalar(const float4& pi, const float4& pj, uint32_t j,
 											uint32_t flip,
 											const PairTableRef* trow, const float* bin_f,
-											const float2* bin_e, const Box& box, float cutoff_sq,
-											float4* force, float& fx, float& fy, float& fz,
-											float& fe, double& e_acc, double& w_acc) {
+											const float2* bin_e, const PairTermRef* arow,
+											const PairSolvent& sv, const Box& box,
+											float cutoff_sq, float4* force, float& fx, float& fy,
+											float& fz, float& fe, double& e_acc, double& w_acc) {
 	// r = wrap_diff(pos[second] - pos[first])
 	// (pi - pj is exactly -(pj - pi) in round-to-nearest, so a sign flip suffices)
 	float dx = __uint_as_float(__float_as_uint(__fsub_rn(pj.x, pi.x)) ^ flip);
@@ -96,14 +197,36 @@ __device__ __forceinline__ void pair_scalar(const float4& pi, const float4& pj, 
 		dy = r.y;
 		dz = r.z;
 	}
-	const float dist = __fsqrt_rn(len2(dx, dy, dz));
+	const float d2v = len2(dx, dy, dz);
+	const float dist = __fsqrt_rn(d2v);
 	if (dist < 1e-6f || (cutoff_sq > 0.0f && __fmul_rn(dist, dist) > cutoff_sq)) return;
 	const PairTableRef t = trow[type_of(pj)];
-	if (t.offset < 0) return;
-	const float w = __fmul_rn(__fsub_rn(dist, t.start), t.step_inv);
-	const float wf = floorf(w);
-	const int home = min(max(static_cast<int>(wf), 0), t.last);
-	const float fm = bin_f[t.offset + home];
+	float fm = 0.0f, e = 0.0f;
+	if (kTerms) {
+		const PairTermRef a = arow[type_of(pj)];
+		if (a.terms == 0u && t.offset < 0) return;
+		analytic_terms(a.terms, a, sv, dist, d2v, fm, e);
+		if (t.offset >= 0) {
+			const float w = __fmul_rn(__fsub_rn(dist, t.start), t.step_inv);
+			const float wf = floorf(w);
+			const int home = min(max(static_cast<int>(wf), 0), t.last);
+			fm = __fadd_rn(fm, bin_f[t.offset + home]);
+			if (kEnergy) {
+				const float2 ue = bin_e[t.offset + home];
+				e = __fadd_rn(e, __fadd_rn(__fmul_rn(ue.y, __fsub_rn(w, wf)), ue.x));
+			}
+		}
+	} else {
+		if (t.offset < 0) return;
+		const float w = __fmul_rn(__fsub_rn(dist, t.start), t.step_inv);
+		const float wf = floorf(w);
+		const int home = min(max(static_cast<int>(wf), 0), t.last);
+		fm = bin_f[t.offset + home];
+		if (kEnergy) {
+			const float2 ue = bin_e[t.offset + home];
+			e = __fadd_rn(__fmul_rn(ue.y, __fsub_rn(w, wf)), ue.x);
+		}
+	}
 	const float inv = __frcp_rn(dist);
 	// f = unit * F acts on the pair's second particle, -f on its first.
 	const float gx = __fmul_rn(__fmul_rn(inv, dx), fm);
@@ -111,8 +234,6 @@ __device__ __forceinline__ void pair_scalar(const float4& pi, const float4& pj, 
 	const float gz = __fmul_rn(__fmul_rn(inv, dz), fm);
 	float half = 0.0f;
 	if (kEnergy) {
-		const float2 ue = bin_e[t.offset + home];
-		const float e = __fadd_rn(__fmul_rn(ue.y, __fsub_rn(w, wf)), ue.x);
 		half = __fmul_rn(e, 0.5f);
 		e_acc += static_cast<double>(e);
 		w_acc += static_cast<double>(gx) * dx + static_cast<double>(gy) * dy +
@@ -161,12 +282,13 @@ struct SystemBoxes {
 	__device__ __forceinline__ Box row(uint32_t i) const { return boxes[keys[i] >> sys_shift]; }
 };
 
-template <int G, bool kEnergy, bool kAllPeriodic, class BoxSrc>
+template <int G, bool kEnergy, bool kAllPeriodic, bool kTerms, class BoxSrc>
 __global__ void __launch_bounds__(256) pair_force_kernel(
 	const float4* __restrict__ sorted_pos, const uint32_t* __restrict__ nbr,
 	const uint32_t* __restrict__ row_len, uint32_t n, uint32_t cap, int T,
 	const PairTableRef* __restrict__ refs_g, const float* __restrict__ force_g,
-	const float2* __restrict__ energy_g, uint32_t total_bins, BoxSrc boxes, float cutoff_sq,
+	const float2* __restrict__ energy_g, uint32_t total_bins,
+	const PairTermRef* __restrict__ terms_g, PairSolvent sv, BoxSrc boxes, float cutoff_sq,
 	float4* force, double* __restrict__ ev) {
 	constexpr int H = 32 / G;
 	PairTableRef* refs;
@@ -180,6 +302,7 @@ __global__ void __launch_bounds__(256) pair_force_kernel(
 	const Box& box = boxes.row(valid ? i : 0u);
 	const float4 pi = valid ? sorted_pos[i] : make_float4(0.f, 0.f, 0.f, 0.f);
 	const PairTableRef* trow = refs + (valid ? type_of(pi) : 0) * T;
+	const PairTermRef* arow = kTerms ? terms_g + (valid ? type_of(pi) : 0) * T : nullptr;
 	const uint32_t cnt = valid ? row_len[i] : 0u;
 	// Entry k of row i: ((i / H) * cap + k) * H + i % H.
 	const uint32_t* col = nbr + (static_cast<size_t>(i / H) * cap) * H + (i % H);
@@ -194,17 +317,19 @@ __global__ void __launch_bounds__(256) pair_force_kernel(
 		const uint32_t j0 = e0 & ~kOrientBit, j1 = e1 & ~kOrientBit;
 		const float4 p0 = sorted_pos[j0];
 		const float4 p1 = sorted_pos[j1];
-		pair_scalar<kEnergy, kAllPeriodic>(pi, p0, j0, e0 & kOrientBit, trow, bin_f, bin_e, box,
-										   cutoff_sq, force, fx, fy, fz, fe, e_acc, w_acc);
-		pair_scalar<kEnergy, kAllPeriodic>(pi, p1, j1, e1 & kOrientBit, trow, bin_f, bin_e, box,
-										   cutoff_sq, force, fx, fy, fz, fe, e_acc, w_acc);
+		pair_scalar<kEnergy, kAllPeriodic, kTerms>(pi, p0, j0, e0 & kOrientBit, trow, bin_f, bin_e,
+												   arow, sv, box, cutoff_sq, force, fx, fy, fz, fe,
+												   e_acc, w_acc);
+		pair_scalar<kEnergy, kAllPeriodic, kTerms>(pi, p1, j1, e1 & kOrientBit, trow, bin_f, bin_e,
+												   arow, sv, box, cutoff_sq, force, fx, fy, fz, fe,
+												   e_acc, w_acc);
 	}
 	if (t < cnt) {
 		const uint32_t entry = __ldcs(col + static_cast<size_t>(t) * H);
 		const uint32_t j = entry & ~kOrientBit;
-		pair_scalar<kEnergy, kAllPeriodic>(pi, sorted_pos[j], j, entry & kOrientBit, trow, bin_f,
-										   bin_e, box, cutoff_sq, force, fx, fy, fz, fe, e_acc,
-										   w_acc);
+		pair_scalar<kEnergy, kAllPeriodic, kTerms>(pi, sorted_pos[j], j, entry & kOrientBit, trow,
+												   bin_f, bin_e, arow, sv, box, cutoff_sq, force,
+												   fx, fy, fz, fe, e_acc, w_acc);
 	}
 	if (G > 1) {
 #pragma unroll
@@ -250,6 +375,8 @@ __device__ __forceinline__ float calc_distance(const Box& box, const float4& fro
 }
 
 // TabulatedBondComputer::operator() (src/Interactions/Bonded/BondComputer.h:168-191).
+// A row with table_idx < 0 has a form other than tabulated and is skipped, as
+// the reference's forms[] check skips it.
 __global__ void __launch_bounds__(256) bond_kernel(const int2* __restrict__ bonds,
 												   const int* __restrict__ table_idx, uint32_t nb,
 												   const float4* __restrict__ pos, float4* fe,
@@ -257,7 +384,7 @@ __global__ void __launch_bounds__(256) bond_kernel(const int2* __restrict__ bond
 												   int get_energy, double* energy) {
 	const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
 	double e_acc = 0.0;
-	if (k < nb) {
+	if (k < nb && table_idx[k] >= 0) {
 		const int2 b = bonds[k];
 		float3 r, u;
 		const float dist = calc_distance(box, pos[b.x], pos[b.y], r, u);
@@ -286,7 +413,7 @@ __global__ void __launch_bounds__(256) angle_kernel(const int4* __restrict__ ang
 													int get_energy, double* energy) {
 	const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
 	double e_acc = 0.0;
-	if (k < na) {
+	if (k < na && table_idx[k] >= 0) {
 		const int4 a = angles[k];
 		const float4 pi = pos[a.x], pj = pos[a.y], pk = pos[a.z];
 		const float3 ab = wrap_diff(box, __fsub_rn(pj.x, pi.x), __fsub_rn(pj.y, pi.y),
@@ -330,7 +457,110 @@ __global__ void __launch_bounds__(256) angle_kernel(const int4* __restrict__ ang
 	if (get_energy) block_add_f64(e_acc, 0.0, energy);
 }
 
-template <int G, bool kEnergy, bool kAllPeriodic, class BoxSrc>
+__device__ __forceinline__ float3 cross3(const float3& a, const float3& b) {
+	return make_float3(__fsub_rn(__fmul_rn(a.y, b.z), __fmul_rn(a.z, b.y)),
+					   __fsub_rn(__fmul_rn(a.z, b.x), __fmul_rn(a.x, b.z)),
+					   __fsub_rn(__fmul_rn(a.x, b.y), __fmul_rn(a.y, b.x)));
+}
+__device__ __forceinline__ float dot3(const float3& a, const float3& b) {
+	return __fadd_rn(__fadd_rn(__fmul_rn(a.x, b.x), __fmul_rn(a.y, b.y)), __fmul_rn(a.z, b.z));
+}
+__device__ __forceinline__ float len2v(const float3& a) { return len2(a.x, a.y, a.z); }
+// Vector3::rLength2 (src/Types/Vector3.h:233-236).
+__device__ __forceinline__ float rlen2(const float3& a) {
+	const float l2 = len2v(a);
+	return l2 != 0.0f ? __frcp_rn(l2) : 0.0f;
+}
+
+// TabulatedDihedralComputer::operator() (src/Interactions/Bonded/BondComputer.h:304-345)
+// with DihedralGeometry::compute (src/Interactions/Bonded/BondGeometry.h:62-86):
+// phi from the two plane normals, periodic table, magnitude 0 when degenerate
+// and clamped to +-1000 (kMaxBondedForce), a quarter of the energy to each of
+// the four particles. Rows with table_idx < 0 are skipped.
+__global__ void __launch_bounds__(256) dihedral_kernel(const int4* __restrict__ dih,
+													   const int* __restrict__ table_idx,
+													   uint32_t nd, const float4* __restrict__ pos,
+													   float4* fe, const Table* __restrict__ tables,
+													   Box box, int get_energy, double* energy) {
+	const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+	double e_acc = 0.0;
+	if (k < nd && table_idx[k] >= 0) {
+		const int4 q = dih[k];
+		const float4 p0 = pos[q.x], p1 = pos[q.y], p2 = pos[q.z], p3 = pos[q.w];
+		const float3 ab = wrap_diff(box, __fsub_rn(p1.x, p0.x), __fsub_rn(p1.y, p0.y),
+									__fsub_rn(p1.z, p0.z));
+		const float3 bc = wrap_diff(box, __fsub_rn(p2.x, p1.x), __fsub_rn(p2.y, p1.y),
+									__fsub_rn(p2.z, p1.z));
+		const float3 cd = wrap_diff(box, __fsub_rn(p3.x, p2.x), __fsub_rn(p3.y, p2.y),
+									__fsub_rn(p3.z, p2.z));
+		const float3 c_abc = cross3(ab, bc), c_bcd = cross3(bc, cd), c_x = cross3(bc, c_abc);
+		const float l_abc = __fsqrt_rn(len2v(c_abc)), l_bcd = __fsqrt_rn(len2v(c_bcd));
+		const float cos_phi = __fdiv_rn(dot3(c_abc, c_bcd), __fmul_rn(l_abc, l_bcd));
+		const float sin_phi =
+			__fdiv_rn(dot3(c_x, c_bcd), __fmul_rn(__fsqrt_rn(len2v(c_x)), l_bcd));
+		const float phi = atan2f(sin_phi, cos_phi);
+		const float lbc = __fsqrt_rn(len2v(bc));
+		const float s1 = __fmul_rn(-lbc, rlen2(c_abc));
+		const float s3 = __fmul_rn(-lbc, rlen2(c_bcd));
+		const float rbc = rlen2(bc);
+		const float g1 = -__fmul_rn(dot3(ab, bc), rbc);
+		const float g3 = __fmul_rn(dot3(bc, cd), rbc);
+		const float3 f1 = make_float3(__fmul_rn(s1, c_abc.x), __fmul_rn(s1, c_abc.y),
+									  __fmul_rn(s1, c_abc.z));
+		const float3 f3 = make_float3(__fmul_rn(s3, c_bcd.x), __fmul_rn(s3, c_bcd.y),
+									  __fmul_rn(s3, c_bcd.z));
+		const float3 f2 = make_float3(__fsub_rn(__fmul_rn(g1, f1.x), __fmul_rn(g3, f3.x)),
+									  __fsub_rn(__fmul_rn(g1, f1.y), __fmul_rn(g3, f3.y)),
+									  __fsub_rn(__fmul_rn(g1, f1.z), __fmul_rn(g3, f3.z)));
+		const bool degenerate =
+			__fmul_rn(__fmul_rn(len2v(ab), len2v(bc)), rlen2(c_abc)) > 100.0f ||
+			__fmul_rn(__fmul_rn(len2v(bc), len2v(cd)), rlen2(c_bcd)) > 100.0f;
+		const Table t = tables[table_idx[k]];
+		const float2 fm_e =
+			table_lookup(t.pot, static_cast<int>(t.size), t.start, t.step_inv, 1, phi);
+		float mag = degenerate ? 0.0f : fm_e.x;
+		mag = mag > 1000.0f ? 1000.0f : (mag < -1000.0f ? -1000.0f : mag);
+		const float3 v1 = make_float3(__fmul_rn(mag, f1.x), __fmul_rn(mag, f1.y), __fmul_rn(mag, f1.z));
+		const float3 v2 = make_float3(__fmul_rn(mag, f2.x), __fmul_rn(mag, f2.y), __fmul_rn(mag, f2.z));
+		const float3 v3 = make_float3(__fmul_rn(mag, f3.x), __fmul_rn(mag, f3.y), __fmul_rn(mag, f3.z));
+		const float quarter = get_energy ? __fmul_rn(fm_e.y, 0.25f) : 0.0f;
+		red_add_v4(&fe[q.x], v1.x, v1.y, v1.z, quarter);
+		red_add_v4(&fe[q.y], __fsub_rn(v2.x, v1.x), __fsub_rn(v2.y, v1.y), __fsub_rn(v2.z, v1.z),
+				   quarter);
+		red_add_v4(&fe[q.z], __fsub_rn(v3.x, v2.x), __fsub_rn(v3.y, v2.y), __fsub_rn(v3.z, v2.z),
+				   quarter);
+		red_add_v4(&fe[q.w], -v3.x, -v3.y, -v3.z, quarter);
+		e_acc = get_energy ? static_cast<double>(fm_e.y) : 0.0;
+	}
+	if (get_energy) block_add_f64(e_acc, 0.0, energy);
+}
+
+// HarmonicRestraintComputer::operator() (src/Interactions/Bonded/BondComputer.h:110-130):
+// r = wrap_diff(pos - anchor), F = unit * (-k |r|), the full energy
+// 0.5 k |r|^2 to the particle; ids < 0 are skipped.
+__global__ void __launch_bounds__(256) restraint_kernel(const int* __restrict__ ids,
+														const float4* __restrict__ anchors,
+														const float* __restrict__ k_spring,
+														uint32_t nr, const float4* __restrict__ pos,
+														float4* fe, Box box, int get_energy,
+														double* energy) {
+	const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+	double e_acc = 0.0;
+	if (k < nr && ids[k] >= 0) {
+		const int id = ids[k];
+		float3 r, u;
+		const float d = calc_distance(box, anchors[k], pos[id], r, u);
+		const float kk = k_spring[k];
+		const float fm = __fmul_rn(-kk, d);
+		const float e = __fmul_rn(__fmul_rn(__fmul_rn(0.5f, kk), d), d);
+		red_add_v4(&fe[id], __fmul_rn(fm, u.x), __fmul_rn(fm, u.y), __fmul_rn(fm, u.z),
+				   get_energy ? e : 0.0f);
+		e_acc = get_energy ? static_cast<double>(e) : 0.0;
+	}
+	if (get_energy) block_add_f64(e_acc, 0.0, energy);
+}
+
+template <int G, bool kEnergy, bool kAllPeriodic, bool kTerms, class BoxSrc>
 void launch_pair(const float4* sorted_pos, const uint32_t* nbr, const uint32_t* row_len,
 				 uint32_t n, uint32_t cap, const PairTables& t, const BoxSrc& boxes,
 				 float cutoff_sq, float4* force_sorted, double* ev, cudaStream_t st) {
@@ -339,13 +569,30 @@ void launch_pair(const float4* sorted_pos, const uint32_t* nbr, const uint32_t* 
 						(kEnergy ? static_cast<size_t>(t.total_bins) * 8 : 0);
 	const uint32_t rows = 256 / G;
 	const uint32_t blocks = (n + rows - 1) / rows;
-	auto kern = pair_force_kernel<G, kEnergy, kAllPeriodic, BoxSrc>;
+	auto kern = pair_force_kernel<G, kEnergy, kAllPeriodic, kTerms, BoxSrc>;
 	if (smem > 48 * 1024)
 		MB2_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
 									  static_cast<int>(smem)));
 	MB2_LAUNCH kern<<<blocks, 256, smem, st>>>(sorted_pos, nbr, row_len, n, cap, t.num_types,
 											   t.refs, t.bin_force, t.bin_energy, t.total_bins,
-											   boxes, cutoff_sq, force_sorted, ev);
+											   t.terms, t.solvent, boxes, cutoff_sq, force_sorted,
+											   ev);
+}
+
+template <int G, bool kEnergy, bool kAllPeriodic, class BoxSrc>
+void launch_pair_t(const float4* sorted_pos, const uint32_t* nbr, const uint32_t* row_len,
+				   uint32_t n, uint32_t cap, const PairTables& t, const BoxSrc& boxes,
+				   float cutoff_sq, float4* force_sorted, double* ev, cudaStream_t st) {
+	// Analytical terms only on the one-box path (batched replicas are tabulated).
+	if constexpr (std::is_same<BoxSrc, OneBox>::value) {
+		if (t.terms) {
+			launch_pair<G, kEnergy, kAllPeriodic, true>(sorted_pos, nbr, row_len, n, cap, t, boxes,
+														cutoff_sq, force_sorted, ev, st);
+			return;
+		}
+	}
+	launch_pair<G, kEnergy, kAllPeriodic, false>(sorted_pos, nbr, row_len, n, cap, t, boxes,
+												 cutoff_sq, force_sorted, ev, st);
 }
 
 template <int G, class BoxSrc>
@@ -354,11 +601,11 @@ void launch_pair_g(const float4* sorted_pos, const uint32_t* nbr, const uint32_t
 				   bool all_periodic, float cutoff_sq, int get_energy, float4* force_sorted,
 				   double* ev, cudaStream_t st) {
 	if (get_energy) {
-		if (all_periodic) launch_pair<G, true, true>(sorted_pos, nbr, row_len, n, cap, t, boxes, cutoff_sq, force_sorted, ev, st);
-		else launch_pair<G, true, false>(sorted_pos, nbr, row_len, n, cap, t, boxes, cutoff_sq, force_sorted, ev, st);
+		if (all_periodic) launch_pair_t<G, true, true>(sorted_pos, nbr, row_len, n, cap, t, boxes, cutoff_sq, force_sorted, ev, st);
+		else launch_pair_t<G, true, false>(sorted_pos, nbr, row_len, n, cap, t, boxes, cutoff_sq, force_sorted, ev, st);
 	} else {
-		if (all_periodic) launch_pair<G, false, true>(sorted_pos, nbr, row_len, n, cap, t, boxes, cutoff_sq, force_sorted, ev, st);
-		else launch_pair<G, false, false>(sorted_pos, nbr, row_len, n, cap, t, boxes, cutoff_sq, force_sorted, ev, st);
+		if (all_periodic) launch_pair_t<G, false, true>(sorted_pos, nbr, row_len, n, cap, t, boxes, cutoff_sq, force_sorted, ev, st);
+		else launch_pair_t<G, false, false>(sorted_pos, nbr, row_len, n, cap, t, boxes, cutoff_sq, force_sorted, ev, st);
 	}
 }
 
@@ -467,6 +714,22 @@ void angle_forces(const int4* angles, const int* table_idx, uint32_t na, const f
 	if (na == 0) return;
 	MB2_LAUNCH angle_kernel<<<(na + 255) / 256, 256, 0, st>>>(angles, table_idx, na, pos, fe,
 															  tables, box, get_energy, energy);
+}
+
+void dihedral_forces(const int4* dihedrals, const int* table_idx, uint32_t nd, const float4* pos,
+					 float4* fe, const Table* tables, const Box& box, int get_energy,
+					 double* energy, cudaStream_t st) {
+	if (nd == 0) return;
+	MB2_LAUNCH dihedral_kernel<<<(nd + 255) / 256, 256, 0, st>>>(dihedrals, table_idx, nd, pos, fe,
+																 tables, box, get_energy, energy);
+}
+
+void restraint_forces(const int* ids, const float4* anchors, const float* k_spring, uint32_t nr,
+					  const float4* pos, float4* fe, const Box& box, int get_energy,
+					  double* energy, cudaStream_t st) {
+	if (nr == 0) return;
+	MB2_LAUNCH restraint_kernel<<<(nr + 255) / 256, 256, 0, st>>>(ids, anchors, k_spring, nr, pos,
+																  fe, box, get_energy, energy);
 }
 
 }  // namespace mb2

@@ -174,12 +174,30 @@ struct PairTableRef {
 	int last;    // size - 1
 	int offset;  // into bin_force / bin_energy, or -1
 };
+// Per type pair: the analytical terms and their per-pair constants, each
+// rounded as PairNonbondedComputer rounds it per pair (Pairwise.h:248-283,
+// Columb.h): qq = qi * qj, a_dh = qq * COULOMB / dielectric, a_onck =
+// qq * COULOMB, rad6 = (0.5 (r_a + r_b))^6, eps = sqrt(eps_a eps_b).
+struct PairTermRef {
+	uint32_t terms;  // analytical bits of the type pair's tag (0: none)
+	float qq, a_dh, a_onck, rad6, eps;
+	float pad0, pad1;
+};
+// Run-wide constants of the analytical terms (SolventParams,
+// NonBondedInteraction.h:123-129; GaussianPotential, Pairwise.h:50-53).
+struct PairSolvent {
+	float dh_len, dh_inv_len;      // Debye length and RN(1 / length)
+	float onck_kappa, onck_sz, onck_z, onck_two_z;
+	float g_amp, g_inv_s2, g_cut2;  // Gaussian: amp, RN(1 / sigma^2), cutoff^2 (<= 0: none)
+};
 struct PairTables {
 	int num_types = 0;
 	uint32_t total_bins = 0;
 	const PairTableRef* refs = nullptr;   // device [T*T]
 	const float* bin_force = nullptr;     // device: -(U[k+1]-U[k]) * step_inv, 0 at k = size-1
 	const float2* bin_energy = nullptr;   // device: (U[k], U[k+1]-U[k]), (U[size-1], 0) last
+	const PairTermRef* terms = nullptr;   // device [T*T], or null: tabulated terms only
+	PairSolvent solvent{};
 };
 void pair_forces(const float4* sorted_pos, const uint32_t* nbr, const uint32_t* row_len,
 				 uint32_t n, uint32_t cap, int lanes_per_row, const PairTables& t, const Box& box,
@@ -205,6 +223,12 @@ void bond_forces(const int2* bonds, const int* table_idx, uint32_t nb, const flo
 void angle_forces(const int4* angles, const int* table_idx, uint32_t na, const float4* pos,
 				  float4* fe, const Table* tables, const Box& box, int get_energy, double* energy,
 				  cudaStream_t st);
+void dihedral_forces(const int4* dihedrals, const int* table_idx, uint32_t nd, const float4* pos,
+					 float4* fe, const Table* tables, const Box& box, int get_energy,
+					 double* energy, cudaStream_t st);
+void restraint_forces(const int* ids, const float4* anchors, const float* k_spring, uint32_t nr,
+					  const float4* pos, float4* fe, const Box& box, int get_energy,
+					  double* energy, cudaStream_t st);
 
 // bd.cu
 struct GridView {

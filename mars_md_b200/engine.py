@@ -8,8 +8,12 @@ call surface on the Brownian-dynamics path:
   virtuals (src/PatchOperation/Pairlist.h:85-172);
 * ``set_pair_tables`` / ``pair_forces`` -- DevicePairNonBondedInteractions and
   launch_pairwise_nonbonded (src/Interactions/NonBondedInteraction.h:205-296);
-* ``set_bonded_tables`` / ``bond_forces`` / ``angle_forces`` --
-  launch_tabulated_{bonds,angles} (src/Interactions/DeviceBondedInteraction.h:495-549);
+* ``set_pair_terms`` -- the analytical pair terms of PairNonbondedComputer
+  (src/Interactions/Nonbonded/Pairwise.h:214-304, Columb.h);
+* ``set_bonded_tables`` / ``bond_forces`` / ``angle_forces`` /
+  ``dihedral_forces`` / ``restraint_forces`` -- launch_tabulated_{bonds,angles,
+  dihedrals} and launch_harmonic_restraints
+  (src/Interactions/DeviceBondedInteraction.h:495-620);
 * ``set_particle_types`` / ``set_grid`` / ``bd_integrate`` -- launch_BD
   (src/PatchOperation/Integrator.h:26-54);
 * ``step`` -- one SimManager step for one patch (src/SimManager.cpp:337-504);
@@ -106,7 +110,21 @@ class Context:
             vals.ctypes.data_as(C.POINTER(C.c_float)), sizes.ctypes.data_as(C.POINTER(C.c_uint32)),
             starts.ctypes.data_as(C.POINTER(C.c_float)), sinv.ctypes.data_as(C.POINTER(C.c_float))))
 
+    def set_pair_terms(self, charge, radius, eps, debye_length=10.0, dielectric=80.0,
+                       onck_kappa=0.1, onck_sz=80.0, onck_z=6.86, gaussian_amp=1.0,
+                       gaussian_sigma=1.0, gaussian_cutoff_sq=0.0):
+        """Analytical pair terms: per-type charge / softcore radius / eps plus
+        the solvent and Gaussian constants (defaults: the reference's)."""
+        T = len(charge)
+        fp = C.POINTER(C.c_float)
+        arrs = [np.ascontiguousarray(a, np.float32) for a in (charge, radius, eps)]
+        prm = L.PairParams(debye_length, dielectric, onck_kappa, onck_sz, onck_z, gaussian_amp,
+                           gaussian_sigma, gaussian_cutoff_sq)
+        self.check(self.lib.mb2_set_pair_terms(self.h, T, *[a.ctypes.data_as(fp) for a in arrs],
+                                               C.byref(prm)))
+
     def set_bonded_tables(self, kind, tables):
+        """kind 0 bonds, 1 angles, 2 dihedrals."""
         vals, sizes, starts, sinv = self._tables(tables)
         self.check(self.lib.mb2_set_bonded_tables(
             self.h, int(kind), len(tables), vals.ctypes.data_as(C.POINTER(C.c_float)),
@@ -244,6 +262,22 @@ class Context:
     def angle_forces(self, angles, table_idx, pos, fe, get_energy=True, stream=None):
         self.check(self.lib.mb2_angle_forces(self.h, _p(angles), _p(table_idx), angles.shape[0],
                                              _p(pos), _p(fe), int(get_energy), _stream(stream)))
+
+    def dihedral_forces(self, dihedrals, table_idx, pos, fe, get_energy=True, stream=None):
+        self.check(self.lib.mb2_dihedral_forces(self.h, _p(dihedrals), _p(table_idx),
+                                                dihedrals.shape[0], _p(pos), _p(fe),
+                                                int(get_energy), _stream(stream)))
+
+    def restraint_forces(self, ids, anchors, spring_k, pos, fe, get_energy=True, stream=None):
+        self.check(self.lib.mb2_restraint_forces(self.h, _p(ids), _p(anchors), _p(spring_k),
+                                                 ids.shape[0], _p(pos), _p(fe), int(get_energy),
+                                                 _stream(stream)))
+
+    def energy_terms(self, stream=None):
+        """[pair, virial, bond, angle, dihedral, restraint] energies (FP64)."""
+        out = (C.c_double * 6)()
+        self.check(self.lib.mb2_energy_terms(self.h, _stream(stream), out, 6))
+        return np.array(list(out))
 
     def energies(self, stream=None):
         out = (C.c_double * 4)()
@@ -385,7 +419,8 @@ def to_original_order(values, ids):
 
 
 def step_params(w, seed=None, patch_id=0, get_energy=False, bonds=None, bond_idx=None,
-                angles=None, angle_idx=None) -> L.StepParams:
+                angles=None, angle_idx=None, dihedrals=None, dihedral_idx=None,
+                restraint_ids=None, restraint_anchors=None, restraint_k=None) -> L.StepParams:
     """StepParams for a workload (see mars_md_b200.workloads)."""
     p = L.StepParams()
     p.pairlist_cutoff = float(w.list_radius)
@@ -400,6 +435,12 @@ def step_params(w, seed=None, patch_id=0, get_energy=False, bonds=None, bond_idx
         p.bonds2, p.bond_table_idx, p.num_bonds = bonds.data_ptr(), bond_idx.data_ptr(), bonds.shape[0]
     if angles is not None:
         p.angles4, p.angle_table_idx, p.num_angles = angles.data_ptr(), angle_idx.data_ptr(), angles.shape[0]
+    if dihedrals is not None:
+        p.dihedrals4, p.dihedral_table_idx = dihedrals.data_ptr(), dihedral_idx.data_ptr()
+        p.num_dihedrals = dihedrals.shape[0]
+    if restraint_ids is not None:
+        p.restraint_ids, p.restraint_anchors4 = restraint_ids.data_ptr(), restraint_anchors.data_ptr()
+        p.restraint_k, p.num_restraints = restraint_k.data_ptr(), restraint_ids.shape[0]
     return p
 
 

@@ -69,9 +69,9 @@ inline void cuda_check(cudaError_t e, const char* what) {
 // 16-byte vector as the reference stores positions and ForceEnergy
 // (src/Types/Vector3.h:41): x, y, z and a fourth word (energy in ForceEnergy).
 struct alignas(16) Vector3 {
-	float x = 0.0f, y = 0.0f, z = 0.0f, w = 0.0f;
+	float x = 0.0f, y = 0.0f, z = 0.0f, t = 0.0f;
 	Vector3() = default;
-	Vector3(float x_, float y_, float z_, float w_ = 0.0f) : x(x_), y(y_), z(z_), w(w_) {}
+	Vector3(float x_, float y_, float z_, float t_ = 0.0f) : x(x_), y(y_), z(z_), t(t_) {}
 };
 static_assert(sizeof(Vector3) == 16, "float4 layout");
 
@@ -490,7 +490,17 @@ class B200Patch {
 								  f.starts.data(), f.step_invs.data()),
 			  ctx_->get(), "set_pair_tables");
 	}
-	// kind 0 = bonds, 1 = angles (angle tables periodic, abscissa in radians).
+	// Analytical pair terms (DevicePairNonBondedInteractions + SolventParams):
+	// per-type charge, softcore radius and eps; params null = the reference's
+	// solvent and Gaussian defaults.
+	void set_pair_terms(const std::vector<float>& charge, const std::vector<float>& radius,
+						const std::vector<float>& eps, const mb2_pair_params* params = nullptr) {
+		check(mb2_set_pair_terms(ctx_->get(), static_cast<int>(charge.size()), charge.data(),
+								 radius.data(), eps.data(), params),
+			  ctx_->get(), "set_pair_terms");
+	}
+	// kind 0 = bonds, 1 = angles, 2 = dihedrals (angle and dihedral tables
+	// periodic, abscissa in radians).
 	void set_bonded_tables(int kind, const std::vector<Table>& tables) {
 		Flat f(tables);
 		check(mb2_set_bonded_tables(ctx_->get(), kind, static_cast<int>(tables.size()),
@@ -553,6 +563,34 @@ class B200Patch {
 								   reinterpret_cast<const float*>(pos.data()),
 								   reinterpret_cast<float*>(force_energy.data()),
 								   compute_energy ? 1 : 0, ctx_->stream()),
+				  ctx_->get(), "calculate_bonded_forces");
+	}
+
+	// The rest of Patch::calculate_bonded_forces (Patch.cpp:208-232): tabulated
+	// dihedrals (int4 per dihedral) and harmonic restraints (particle id,
+	// anchor, spring constant per restraint). A negative table index skips a
+	// row, as a non-tabulated form does in the reference.
+	void calculate_dihedral_and_restraint_forces(const DeviceBuffer<Vector3>& pos,
+												 DeviceBuffer<Vector3>& force_energy,
+												 const int* dihedrals4, const int* dihedral_table_idx,
+												 size_t num_dihedrals, const int* restraint_ids,
+												 const Vector3* restraint_anchors,
+												 const float* restraint_k, size_t num_restraints,
+												 bool compute_energy = false) {
+		if (num_dihedrals)
+			check(mb2_dihedral_forces(ctx_->get(), dihedrals4, dihedral_table_idx,
+									  static_cast<uint32_t>(num_dihedrals),
+									  reinterpret_cast<const float*>(pos.data()),
+									  reinterpret_cast<float*>(force_energy.data()),
+									  compute_energy ? 1 : 0, ctx_->stream()),
+				  ctx_->get(), "calculate_bonded_forces");
+		if (num_restraints)
+			check(mb2_restraint_forces(ctx_->get(), restraint_ids,
+									   reinterpret_cast<const float*>(restraint_anchors),
+									   restraint_k, static_cast<uint32_t>(num_restraints),
+									   reinterpret_cast<const float*>(pos.data()),
+									   reinterpret_cast<float*>(force_energy.data()),
+									   compute_energy ? 1 : 0, ctx_->stream()),
 				  ctx_->get(), "calculate_bonded_forces");
 	}
 

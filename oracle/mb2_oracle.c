@@ -689,11 +689,14 @@ double or_pair_energy_f64(const int* pairs, size_t n_pairs, const float* pos4,
 	return total;
 }
 
-/* TabulatedBondComputer::operator() (src/Interactions/Bonded/BondComputer.h:168-191). */
+/* TabulatedBondComputer::operator() (src/Interactions/Bonded/BondComputer.h:168-191);
+ * rows with table_idx < 0 (a form other than tabulated) are skipped. */
 void or_bond_forces(const int* bonds, const int* table_idx, size_t nb, const float* pos4,
                     const or_table* tables, const or_box* b, int get_energy, float* fe4,
                     double* fe64, double* fabs_sum) {
 	for (size_t k = 0; k < nb; ++k) {
+		if (table_idx[k] < 0)
+			continue;
 		const int i = bonds[2 * k], j = bonds[2 * k + 1];
 		float r[3], u[3];
 		const float d = calc_distance(b, pos4 + 4 * i, pos4 + 4 * j, r, u);
@@ -717,6 +720,8 @@ void or_angle_forces(const int* angles4, const int* table_idx, size_t na, const 
                      const or_table* tables, const or_box* b, int get_energy, float* fe4,
                      double* fe64, double* fabs_sum) {
 	for (size_t k = 0; k < na; ++k) {
+		if (table_idx[k] < 0)
+			continue;
 		const int i = angles4[4 * k], j = angles4[4 * k + 1], l = angles4[4 * k + 2];
 		const float* pi = pos4 + 4 * i;
 		const float* pj = pos4 + 4 * j;
@@ -757,6 +762,245 @@ void or_angle_forces(const int* angles4, const int* table_idx, size_t na, const 
 		accumulate(fe4, fe64, fabs_sum, j, -(f1[0] + f3[0]), -(f1[1] + f3[1]), -(f1[2] + f3[2]),
 		           en, get_energy);
 		accumulate(fe4, fe64, fabs_sum, l, f3[0], f3[1], f3[2], en, get_energy);
+	}
+}
+
+/* --- analytical pair terms ----------------------------------------------- */
+
+#define OR_COULOMB 332.0636f /* constants::COULOMB (src/Constants.h:24) */
+
+/* math::sinh_minus_x / x_cosh_minus_sinh (src/Types/Math.h:199-216): the
+ * series below |x| = 1, the direct difference above. */
+static float sinh_minus_x(float x) {
+	if (x >= 1.0f || x <= -1.0f)
+		return sinhf(x) - x;
+	const float w = x * x;
+	return x * w *
+	       ((float)(1.0 / 6) +
+	        w * ((float)(1.0 / 120) + w * ((float)(1.0 / 5040) + w * (float)(1.0 / 362880))));
+}
+
+static float x_cosh_minus_sinh(float x) {
+	if (x >= 1.0f || x <= -1.0f)
+		return x * coshf(x) - sinhf(x);
+	const float w = x * x;
+	return x * w *
+	       ((float)(1.0 / 3) +
+	        w * ((float)(1.0 / 30) + w * ((float)(1.0 / 840) + w * (float)(1.0 / 45360))));
+}
+
+/* OnckElecPotential::dielectric / dielectric_deriv (Columb.h:68-84). */
+static float onck_dielectric(float r, float sz, float z) {
+	const float v = r / (2.0f * z);
+	if (v < 1e-5f)
+		return sz * v * v / 3.0f;
+	const float s = sinhf(v);
+	return sz * sinh_minus_x(v) * (s + v) / (s * s);
+}
+
+static float onck_dielectric_deriv(float r, float sz, float z) {
+	const float v = r / (2.0f * z);
+	if (v < 1e-5f)
+		return sz * v / (3.0f * z);
+	const float s = sinhf(v);
+	return sz * v * x_cosh_minus_sinh(v) / (z * s * s * s);
+}
+
+/* PairNonbondedComputer::operator() (src/Interactions/Nonbonded/Pairwise.h:214-304)
+ * with every term: Coulomb (ColumbPotential, Columb.h:11-20), Debye-Hueckel
+ * (Columb.h:29-42), Onck (Columb.h:56-97), Gaussian (Pairwise.h:50-69),
+ * softcore (SoftcoreForceKernel::softcoreForce, Pairwise.h:82-100, converted
+ * to -dU/dr by -F * r) and tabulated, summed in that order; F = unit * sum,
+ * -F to the first index, half the energy to each. tags[p] carries the term
+ * bits (bit 0..5) and the table index (>> 8). */
+void or_pair_forces_terms(const int* pairs, size_t n_pairs, const float* pos4,
+                          const int* type_ids, const uint32_t* tags, const or_table* tables,
+                          const or_pair_terms* pt, const or_box* b, float cutoff_sq,
+                          int get_energy, float* fe4, double* fe64, double* fabs_sum) {
+	for (size_t p = 0; p < n_pairs; ++p) {
+		const uint32_t tag = tags[p];
+		const uint32_t terms = tag & pt->enabled_terms;
+		if ((terms & 0xFFu) == 0)
+			continue;
+		const int i = pairs[2 * p], j = pairs[2 * p + 1];
+		float r[3], u[3];
+		const float d = calc_distance(b, pos4 + 4 * i, pos4 + 4 * j, r, u);
+		if (d < 1e-6f)
+			continue;
+		if (cutoff_sq > 0.0f && d * d > cutoff_sq)
+			continue;
+		const int ti = type_ids[i], tj = type_ids[j];
+		float qi = 0.0f, qj = 0.0f;
+		if (terms & 7u) {
+			qi = pt->charge[ti];
+			qj = pt->charge[tj];
+		}
+		float fm = 0.0f, en = 0.0f;
+		if (terms & 1u) { /* Coulomb */
+			const float inv_d2 = 1.0f / (d * d);
+			const float inv_d = 1.0f / d;
+			fm += qi * qj * inv_d2 * OR_COULOMB;
+			en += qi * qj * inv_d * OR_COULOMB;
+		}
+		if (terms & 2u) { /* Debye-Hueckel */
+			const float inv_r = 1.0f / d;
+			const float a = qi * qj * OR_COULOMB / pt->dielectric;
+			const float screen = expf(-d / pt->debye_length);
+			const float e = a * screen * inv_r;
+			fm += e * (inv_r + 1.0f / pt->debye_length);
+			en += e;
+		}
+		if (terms & 4u) { /* Onck */
+			const float rr = d < 1e-2f ? 1e-2f : d;
+			const float a = qi * qj * OR_COULOMB;
+			const float screen = expf(-pt->onck_kappa * rr);
+			const float eps = onck_dielectric(rr, pt->onck_sz, pt->onck_z);
+			const float e = a * screen / (eps * rr);
+			const float eps_p = onck_dielectric_deriv(rr, pt->onck_sz, pt->onck_z);
+			fm += a * screen * (pt->onck_kappa / (eps * rr) + (eps_p * rr + eps) / (eps * eps * rr * rr));
+			en += e;
+		}
+		if (terms & 8u) { /* Gaussian */
+			const float d2 = d * d;
+			if (!(pt->gaussian_cutoff_sq > 0.0f && d2 > pt->gaussian_cutoff_sq)) {
+				const float inv_s2 = 1.0f / (pt->gaussian_sigma * pt->gaussian_sigma);
+				const float e = pt->gaussian_amp * expf(-d2 * inv_s2);
+				fm += 2.0f * d * e * inv_s2;
+				en += e;
+			}
+		}
+		if (terms & 16u) { /* softcore */
+			const float rad = 0.5f * (pt->radius[ti] + pt->radius[tj]);
+			const float rad2 = rad * rad;
+			const float rad6 = rad2 * rad2 * rad2;
+			const float eps = sqrtf(pt->eps[ti] * pt->eps[tj]);
+			const float d2 = len2(r);
+			const float d6 = d2 * d2 * d2;
+			float f, e;
+			if (d6 < rad6) {
+				const float d6_2 = d6 * d6;
+				const float rad6_2 = rad6 * rad6;
+				e = eps * ((rad6_2 / d6_2) - (2.0f * rad6 / d6)) + eps;
+				f = -12.0f * eps * (rad6_2 / (d6_2 * d2) - rad6 / (d6 * d2));
+			} else {
+				f = -12.0f * eps * (rad6 * rad6 / (d6 * d6 * d2) - rad6 / (d6 * d2));
+				e = 0.0f;
+			}
+			fm += -f * d;
+			en += e;
+		}
+		if (terms & 32u) { /* tabulated */
+			float tf, te;
+			or_table_lookup(&tables[tag >> 8], d, &tf, &te);
+			fm += tf;
+			en += te;
+		}
+		const float f[3] = {u[0] * fm, u[1] * fm, u[2] * fm};
+		const float half = en * 0.5f;
+		accumulate(fe4, fe64, fabs_sum, i, -f[0], -f[1], -f[2], half, get_energy);
+		accumulate(fe4, fe64, fabs_sum, j, f[0], f[1], f[2], half, get_energy);
+	}
+}
+
+/* --- dihedrals and restraints --------------------------------------------- */
+
+static void cross3(const float* a, const float* b, float* out) {
+	out[0] = a[1] * b[2] - a[2] * b[1];
+	out[1] = a[2] * b[0] - a[0] * b[2];
+	out[2] = a[0] * b[1] - a[1] * b[0];
+}
+
+static float dot3(const float* a, const float* b) { return a[0] * b[0] + a[1] * b[1] + a[2] * b[2]; }
+
+static float rlen2(const float* a) {
+	const float l2 = len2(a);
+	return l2 != 0.0f ? 1.0f / l2 : 0.0f;
+}
+
+/* TabulatedDihedralComputer::operator() (src/Interactions/Bonded/BondComputer.h:304-345)
+ * with DihedralGeometry::compute (src/Interactions/Bonded/BondGeometry.h:62-86):
+ * phi = atan2(sin, cos) from the two plane normals; periodic table; force
+ * magnitude 0 when degenerate, clamped to +-1000; a quarter of the energy to
+ * each of the four particles. Rows of table_idx < 0 are skipped (a form other
+ * than tabulated). */
+void or_dihedral_forces(const int* dihedrals4, const int* table_idx, size_t nd,
+                        const float* pos4, const or_table* tables, const or_box* b,
+                        int get_energy, float* fe4, double* fe64, double* fabs_sum) {
+	for (size_t k = 0; k < nd; ++k) {
+		if (table_idx[k] < 0)
+			continue;
+		const int* q = dihedrals4 + 4 * k;
+		float ab[3], bc[3], cd[3];
+		const float* p0 = pos4 + 4 * q[0];
+		const float* p1 = pos4 + 4 * q[1];
+		const float* p2 = pos4 + 4 * q[2];
+		const float* p3 = pos4 + 4 * q[3];
+		const float d01[3] = {p1[0] - p0[0], p1[1] - p0[1], p1[2] - p0[2]};
+		const float d12[3] = {p2[0] - p1[0], p2[1] - p1[1], p2[2] - p1[2]};
+		const float d23[3] = {p3[0] - p2[0], p3[1] - p2[1], p3[2] - p2[2]};
+		box_wrap_diff(b, d01, ab);
+		box_wrap_diff(b, d12, bc);
+		box_wrap_diff(b, d23, cd);
+		float c_abc[3], c_bcd[3], c_x[3];
+		cross3(ab, bc, c_abc);
+		cross3(bc, cd, c_bcd);
+		cross3(bc, c_abc, c_x);
+		const float cos_phi = dot3(c_abc, c_bcd) / (sqrtf(len2(c_abc)) * sqrtf(len2(c_bcd)));
+		const float sin_phi = dot3(c_x, c_bcd) / (sqrtf(len2(c_x)) * sqrtf(len2(c_bcd)));
+		const float phi = (float)atan2((double)sin_phi, (double)cos_phi);
+		const float lbc = sqrtf(len2(bc));
+		const float s1 = -lbc * rlen2(c_abc);
+		const float s3 = -lbc * rlen2(c_bcd);
+		float f1[3], f2[3], f3[3];
+		for (int a = 0; a < 3; ++a) {
+			f1[a] = c_abc[a] * s1;
+			f3[a] = c_bcd[a] * s3;
+		}
+		const float g1 = -(dot3(ab, bc) * rlen2(bc));
+		const float g3 = dot3(bc, cd) * rlen2(bc);
+		for (int a = 0; a < 3; ++a)
+			f2[a] = f1[a] * g1 - f3[a] * g3;
+		const int degenerate = (len2(ab) * len2(bc) * rlen2(c_abc) > 100.0f) ||
+		                       (len2(bc) * len2(cd) * rlen2(c_bcd) > 100.0f);
+		float fm, e;
+		or_table_lookup(&tables[table_idx[k]], phi, &fm, &e);
+		float mag = degenerate ? 0.0f : fm;
+		if (mag > 1000.0f)
+			mag = 1000.0f;
+		else if (mag < -1000.0f)
+			mag = -1000.0f;
+		float v1[3], v2[3], v3[3];
+		for (int a = 0; a < 3; ++a) {
+			v1[a] = f1[a] * mag;
+			v2[a] = f2[a] * mag;
+			v3[a] = f3[a] * mag;
+		}
+		const float quarter = e * 0.25f;
+		accumulate(fe4, fe64, fabs_sum, q[0], v1[0], v1[1], v1[2], quarter, get_energy);
+		accumulate(fe4, fe64, fabs_sum, q[1], v2[0] - v1[0], v2[1] - v1[1], v2[2] - v1[2], quarter,
+		           get_energy);
+		accumulate(fe4, fe64, fabs_sum, q[2], v3[0] - v2[0], v3[1] - v2[1], v3[2] - v2[2], quarter,
+		           get_energy);
+		accumulate(fe4, fe64, fabs_sum, q[3], -v3[0], -v3[1], -v3[2], quarter, get_energy);
+	}
+}
+
+/* HarmonicRestraintComputer::operator() (src/Interactions/Bonded/BondComputer.h:110-130):
+ * r = wrap_diff(pos - anchor), F = unit * (-k |r|), full energy 0.5 k |r|^2 to
+ * the particle; ids < 0 are skipped. anchors4: x, y, z, pad per restraint. */
+void or_restraint_forces(const int* ids, const float* anchors4, const float* k_spring, size_t nr,
+                         const float* pos4, const or_box* b, int get_energy, float* fe4,
+                         double* fe64, double* fabs_sum) {
+	for (size_t k = 0; k < nr; ++k) {
+		const int id = ids[k];
+		if (id < 0)
+			continue;
+		float r[3], u[3];
+		const float d = calc_distance(b, anchors4 + 4 * k, pos4 + 4 * id, r, u);
+		const float kk = k_spring[k];
+		const float fm = -kk * (d - 0.0f);
+		const float e = 0.5f * kk * (d - 0.0f) * (d - 0.0f);
+		accumulate(fe4, fe64, fabs_sum, id, fm * u[0], fm * u[1], fm * u[2], e, get_energy);
 	}
 }
 

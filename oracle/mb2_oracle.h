@@ -123,6 +123,27 @@ void or_bond_forces(const int* bonds, const int* table_idx, size_t nb, const flo
 void or_angle_forces(const int* angles4, const int* table_idx, size_t na, const float* pos4,
                      const or_table* tables, const or_box* b, int get_energy, float* fe4,
                      double* fe64, double* fabs_sum);
+/* Analytical pair-term constants: per-type charge, softcore radius and eps,
+ * the solvent constants (SolventParams, src/Interactions/NonBondedInteraction.h:123-129)
+ * and the Gaussian's (GaussianPotential, src/Interactions/Nonbonded/Pairwise.h:50-53). */
+typedef struct {
+	const float* charge;
+	const float* radius;
+	const float* eps;
+	float debye_length, dielectric, onck_kappa, onck_sz, onck_z;
+	float gaussian_amp, gaussian_sigma, gaussian_cutoff_sq;
+	uint32_t enabled_terms;
+} or_pair_terms;
+void or_pair_forces_terms(const int* pairs, size_t n_pairs, const float* pos4,
+                          const int* type_ids, const uint32_t* tags, const or_table* tables,
+                          const or_pair_terms* pt, const or_box* b, float cutoff_sq,
+                          int get_energy, float* fe4, double* fe64, double* fabs_sum);
+void or_dihedral_forces(const int* dihedrals4, const int* table_idx, size_t nd,
+                        const float* pos4, const or_table* tables, const or_box* b,
+                        int get_energy, float* fe4, double* fe64, double* fabs_sum);
+void or_restraint_forces(const int* ids, const float* anchors4, const float* k_spring, size_t nr,
+                         const float* pos4, const or_box* b, int get_energy, float* fe4,
+                         double* fe64, double* fabs_sum);
 double or_pair_energy_f64(const int* pairs, size_t n_pairs, const float* pos4,
                           const uint32_t* tags, const or_table* tables, const or_box* b,
                           float cutoff_sq);

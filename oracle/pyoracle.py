@@ -73,6 +73,35 @@ class Types(C.Structure):
                 ("force_grid_id4", C.c_void_p), ("force_grid_scale4", C.c_void_p)]
 
 
+class PairTerms(C.Structure):
+    _fields_ = [("charge", C.c_void_p), ("radius", C.c_void_p), ("eps", C.c_void_p),
+                ("debye_length", C.c_float), ("dielectric", C.c_float),
+                ("onck_kappa", C.c_float), ("onck_sz", C.c_float), ("onck_z", C.c_float),
+                ("gaussian_amp", C.c_float), ("gaussian_sigma", C.c_float),
+                ("gaussian_cutoff_sq", C.c_float), ("enabled_terms", C.c_uint32)]
+
+
+# Solvent and Gaussian defaults of the reference (SolventParams,
+# NonBondedInteraction.h:123-129; GaussianPotential, Pairwise.h:50-53).
+SOLVENT_DEFAULTS = (10.0, 80.0, 0.1, 80.0, 6.86)
+GAUSSIAN_DEFAULTS = (1.0, 1.0, 0.0)
+
+
+class PairTermSet:
+    """Per-type charge / radius / eps plus solvent and Gaussian constants."""
+
+    def __init__(self, charge, radius, eps, solvent=SOLVENT_DEFAULTS, gaussian=GAUSSIAN_DEFAULTS,
+                 enabled_terms=0xFF):
+        self.charge = np.ascontiguousarray(charge, np.float32)
+        self.radius = np.ascontiguousarray(radius, np.float32)
+        self.eps = np.ascontiguousarray(eps, np.float32)
+        self.solvent = np.asarray(solvent, np.float32)
+        self.gaussian = np.asarray(gaussian, np.float32)
+        self.s = PairTerms(_ptr(self.charge), _ptr(self.radius), _ptr(self.eps),
+                           *[float(x) for x in self.solvent], *[float(x) for x in self.gaussian],
+                           int(enabled_terms))
+
+
 def _ptr(a):
     return a.ctypes.data_as(C.c_void_p) if a is not None else None
 
@@ -211,6 +240,9 @@ class Oracle:
         L.or_pair_forces.argtypes = [vp, sz, vp, vp, vp, vp, f, i, vp, vp, vp]
         L.or_bond_forces.argtypes = [vp, vp, sz, vp, vp, vp, i, vp, vp, vp]
         L.or_angle_forces.argtypes = [vp, vp, sz, vp, vp, vp, i, vp, vp, vp]
+        L.or_pair_forces_terms.argtypes = [vp, sz, vp, vp, vp, vp, vp, vp, f, i, vp, vp, vp]
+        L.or_dihedral_forces.argtypes = [vp, vp, sz, vp, vp, vp, i, vp, vp, vp]
+        L.or_restraint_forces.argtypes = [vp, vp, vp, sz, vp, vp, i, vp, vp, vp]
         L.or_pair_energy_f64.restype = C.c_double
         L.or_pair_energy_f64.argtypes = [vp, sz, vp, vp, vp, vp, f]
         L.or_grid_value.restype = f
@@ -378,6 +410,46 @@ class Oracle:
                                 _ptr(fabs))
         return fe4, fe64, fabs
 
+    def pair_forces_terms(self, pairs, pos4, type_ids, tags, tables: TableSet,
+                          terms: "PairTermSet", box: Box, cutoff_sq, get_energy=True):
+        """Every pair term (analytical and tabulated); returns (fe4, fe64, fabs)."""
+        n = len(pos4)
+        fe4 = np.zeros((n, 4), np.float32)
+        fe64 = np.zeros((n, 4), np.float64)
+        fabs = np.zeros(n, np.float64)
+        self.lib.or_pair_forces_terms(_ptr(np.ascontiguousarray(pairs, np.int32)), len(pairs),
+                                      _ptr(pos4), _ptr(np.ascontiguousarray(type_ids, np.int32)),
+                                      _ptr(np.ascontiguousarray(tags, np.uint32)),
+                                      C.cast(tables.structs, C.c_void_p), C.byref(terms.s),
+                                      C.byref(box), C.c_float(cutoff_sq), int(get_energy),
+                                      _ptr(fe4), _ptr(fe64), _ptr(fabs))
+        return fe4, fe64, fabs
+
+    def dihedral_forces(self, dihedrals4, table_idx, pos4, tables: TableSet, box: Box,
+                        get_energy=True):
+        n = len(pos4)
+        fe4 = np.zeros((n, 4), np.float32)
+        fe64 = np.zeros((n, 4), np.float64)
+        fabs = np.zeros(n, np.float64)
+        self.lib.or_dihedral_forces(_ptr(np.ascontiguousarray(dihedrals4, np.int32)),
+                                    _ptr(np.ascontiguousarray(table_idx, np.int32)),
+                                    len(dihedrals4), _ptr(pos4), C.cast(tables.structs, C.c_void_p),
+                                    C.byref(box), int(get_energy), _ptr(fe4), _ptr(fe64),
+                                    _ptr(fabs))
+        return fe4, fe64, fabs
+
+    def restraint_forces(self, ids, anchors4, k_spring, pos4, box: Box, get_energy=True):
+        n = len(pos4)
+        fe4 = np.zeros((n, 4), np.float32)
+        fe64 = np.zeros((n, 4), np.float64)
+        fabs = np.zeros(n, np.float64)
+        self.lib.or_restraint_forces(_ptr(np.ascontiguousarray(ids, np.int32)),
+                                     _ptr(np.ascontiguousarray(anchors4, np.float32)),
+                                     _ptr(np.ascontiguousarray(k_spring, np.float32)), len(ids),
+                                     _ptr(pos4), C.byref(box), int(get_energy), _ptr(fe4),
+                                     _ptr(fe64), _ptr(fabs))
+        return fe4, fe64, fabs
+
     def pair_energy_f64(self, pairs, pos4, tags, tables: TableSet, box: Box, cutoff_sq):
         return self.lib.or_pair_energy_f64(_ptr(pairs), len(pairs), _ptr(pos4), _ptr(tags),
                                            C.cast(tables.structs, C.c_void_p), C.byref(box),
@@ -477,6 +549,11 @@ class RefHarness:
         L.ref_inverse.argtypes = [vp, vp, sz]
         L.ref_reorder_pos.argtypes = [vp, vp, vp, sz]
         L.ref_remap_indices.argtypes = [vp, sz, vp, sz]
+        L.ref_pair_forces_terms.argtypes = [vp, sz, vp, vp, vp, vp, vp, vp, vp, vp, vp, i, vp, vp,
+                                            vp, i, f, u32, vp, vp, vp, vp, vp]
+        L.ref_dihedral_forces.argtypes = [vp, vp, vp, sz, vp, vp, vp, vp, vp, vp, vp, i, vp, vp,
+                                          vp, i]
+        L.ref_restraint_forces.argtypes = [vp, vp, vp, sz, vp, vp, vp, vp, vp, i]
         L.ref_cell_ranges.argtypes = [vp, sz, i, vp, vp]
         L.ref_cell_neighbors.argtypes = [vp, sz, i, vp, i, vp]
         L.ref_neighbor_walk.restype = u32
@@ -593,10 +670,54 @@ class RefHarness:
                                  C.c_float(cutoff_sq), enabled_terms)
         return fe
 
+    def pair_forces_terms(self, pairs, pos4, type_ids, tags, tables: TableSet,
+                          terms: "PairTermSet", box: Box, cutoff_sq, get_energy=True,
+                          enabled_terms=0xFF):
+        fe = np.zeros((len(pos4), 4), np.float32)
+        o, s, p = self._box(box)
+        tid = np.ascontiguousarray(type_ids, np.int32)
+        self.lib.ref_pair_forces_terms(
+            _ptr(np.ascontiguousarray(pairs, np.int32)), len(pairs), _ptr(pos4), _ptr(tid),
+            _ptr(fe), _ptr(np.ascontiguousarray(tags, np.uint32)), _ptr(tables.values),
+            _ptr(tables.offsets), _ptr(tables.sizes), _ptr(tables.starts),
+            _ptr(tables.step_invs), len(tables), _ptr(o), _ptr(s), _ptr(p), int(get_energy),
+            C.c_float(cutoff_sq), enabled_terms, _ptr(terms.charge), _ptr(terms.radius),
+            _ptr(terms.eps), _ptr(terms.solvent), _ptr(terms.gaussian))
+        return fe
+
+    def dihedral_forces(self, dihedrals4, table_idx, pos4, tables: TableSet, box: Box,
+                        get_energy=True):
+        fe = np.zeros((len(pos4), 4), np.float32)
+        tidx = np.ascontiguousarray(table_idx, np.int32)
+        forms = np.where(tidx >= 0, 1, 2).astype(np.int32)  # Tabulated = 1, Analytical = 2
+        tidx = np.maximum(tidx, 0).astype(np.int32)
+        o, s, p = self._box(box)
+        self.lib.ref_dihedral_forces(_ptr(np.ascontiguousarray(dihedrals4, np.int32)), _ptr(tidx),
+                                     _ptr(forms), len(dihedrals4), _ptr(pos4), _ptr(fe),
+                                     _ptr(tables.values), _ptr(tables.offsets),
+                                     _ptr(tables.sizes), _ptr(tables.starts),
+                                     _ptr(tables.step_invs), len(tables), _ptr(o), _ptr(s),
+                                     _ptr(p), int(get_energy))
+        return fe
+
+    def restraint_forces(self, ids, anchors4, k_spring, pos4, box: Box, get_energy=True):
+        fe = np.zeros((len(pos4), 4), np.float32)
+        o, s, p = self._box(box)
+        self.lib.ref_restraint_forces(_ptr(np.ascontiguousarray(ids, np.int32)),
+                                      _ptr(np.ascontiguousarray(anchors4, np.float32)),
+                                      _ptr(np.ascontiguousarray(k_spring, np.float32)), len(ids),
+                                      _ptr(pos4), _ptr(fe), _ptr(o), _ptr(s), _ptr(p),
+                                      int(get_energy))
+        return fe
+
     def bond_forces(self, bonds, table_idx, pos4, tables: TableSet, box: Box, get_energy=True,
                     fe=None):
         fe = np.zeros((len(pos4), 4), np.float32) if fe is None else fe
-        forms = np.ones(len(bonds), np.int32)  # InteractionForm::Tabulated (SimParam.h:174)
+        # InteractionForm (SimParam.h:174): Tabulated = 1; a negative index
+        # stands for another form, which the tabulated functor skips.
+        table_idx = np.ascontiguousarray(table_idx, np.int32)
+        forms = np.where(table_idx >= 0, 1, 2).astype(np.int32)
+        table_idx = np.maximum(table_idx, 0).astype(np.int32)
         o, s, p = self._box(box)
         self.lib.ref_bond_forces(_ptr(bonds), _ptr(table_idx), _ptr(forms), len(bonds), _ptr(pos4),
                                  _ptr(fe), _ptr(tables.values), _ptr(tables.offsets),
@@ -607,7 +728,9 @@ class RefHarness:
     def angle_forces(self, angles4, table_idx, pos4, tables: TableSet, box: Box, get_energy=True,
                      fe=None):
         fe = np.zeros((len(pos4), 4), np.float32) if fe is None else fe
-        forms = np.ones(len(angles4), np.int32)  # InteractionForm::Tabulated
+        table_idx = np.ascontiguousarray(table_idx, np.int32)
+        forms = np.where(table_idx >= 0, 1, 2).astype(np.int32)
+        table_idx = np.maximum(table_idx, 0).astype(np.int32)
         o, s, p = self._box(box)
         self.lib.ref_angle_forces(_ptr(angles4), _ptr(table_idx), _ptr(forms), len(angles4),
                                   _ptr(pos4), _ptr(fe), _ptr(tables.values), _ptr(tables.offsets),

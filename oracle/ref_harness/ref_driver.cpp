@@ -247,6 +247,77 @@ void ref_pair_forces(const int* pairs, size_t n_pairs, const float* pos4, int* t
 		k(i);
 }
 
+// PairNonbondedComputer (Pairwise.h:214-304) with every analytical term:
+// per-type charge / radius / eps, the solvent constants as
+// launch_pairwise_nonbonded sets them (NonBondedInteraction.h:289-293) and
+// the Gaussian's constants.
+void ref_pair_forces_terms(const int* pairs, size_t n_pairs, const float* pos4, int* type_ids,
+						   float* fe4, const uint32_t* tags, float* table_values,
+						   const uint32_t* table_offsets, const uint32_t* table_sizes,
+						   const float* table_starts, const float* table_step_invs, int n_tables,
+						   const float* origin, const float* size, const int* periodic,
+						   int get_energy, float cutoff_sq, uint32_t enabled_terms,
+						   const float* charge, const float* radius, const float* eps,
+						   const float* solvent5, const float* gaussian3) {
+	std::vector<int> periodic_flags(n_tables, 0);
+	auto tabs = make_tables(table_values, table_offsets, table_sizes, table_starts,
+							table_step_invs, periodic_flags.data(), n_tables);
+	ParticleView pv{};
+	pv.type_id = type_ids;
+	pv.pos = reinterpret_cast<Vector3*>(const_cast<float*>(pos4));
+	pv.ForceEnergy = reinterpret_cast<Vector3*>(fe4);
+	ParticleTypeView tv{};
+	tv.charge = charge;
+	tv.radius = radius;
+	tv.eps = eps;
+	const PeriodicBox box = make_box(origin, size, periodic);
+	PairNonbondedComputer k(reinterpret_cast<const int2*>(pairs), pv, tags, tabs.data(), tv, &box,
+							get_energy != 0, n_pairs, cutoff_sq, enabled_terms);
+	k.debye_huckel.screen_length = solvent5[0];
+	k.debye_huckel.epsilon = solvent5[1];
+	k.onck.kappa = solvent5[2];
+	k.onck.sz = solvent5[3];
+	k.onck.z = solvent5[4];
+	k.gaussian.amp = gaussian3[0];
+	k.gaussian.sigma = gaussian3[1];
+	k.gaussian.cutoff_squared = gaussian3[2];
+	for (size_t i = 0; i < n_pairs; ++i)
+		k(i);
+}
+
+// TabulatedDihedralComputer (BondComputer.h:282-346); dihedral tables wrap
+// (DeviceBondedInteraction.h:250).
+void ref_dihedral_forces(const int* dihedrals4, const int* table_idx, const int* forms, size_t nd,
+						 const float* pos4, float* fe4, float* table_values,
+						 const uint32_t* table_offsets, const uint32_t* table_sizes,
+						 const float* table_starts, const float* table_step_invs, int n_tables,
+						 const float* origin, const float* size, const int* periodic,
+						 int get_energy) {
+	std::vector<int> periodic_flags(n_tables, 1);
+	auto tabs = make_tables(table_values, table_offsets, table_sizes, table_starts,
+							table_step_invs, periodic_flags.data(), n_tables);
+	const PeriodicBox box = make_box(origin, size, periodic);
+	TabulatedDihedralComputer k(reinterpret_cast<const int4*>(dihedrals4),
+								reinterpret_cast<Vector3*>(const_cast<float*>(pos4)),
+								reinterpret_cast<Vector3*>(fe4), tabs.data(), table_idx, forms,
+								&box, get_energy != 0, nd);
+	for (size_t i = 0; i < nd; ++i)
+		k(i);
+}
+
+// HarmonicRestraintComputer (BondComputer.h:88-131); anchors as Vector3 rows.
+void ref_restraint_forces(const int* ids, const float* anchors4, const float* k_spring, size_t nr,
+						  const float* pos4, float* fe4, const float* origin, const float* size,
+						  const int* periodic, int get_energy) {
+	const PeriodicBox box = make_box(origin, size, periodic);
+	HarmonicRestraintComputer k(ids, reinterpret_cast<Vector3*>(const_cast<float*>(pos4)),
+								reinterpret_cast<Vector3*>(fe4),
+								reinterpret_cast<const Vector3*>(anchors4), k_spring, &box,
+								get_energy != 0, nr);
+	for (size_t i = 0; i < nr; ++i)
+		k(i);
+}
+
 // TabulatedBondComputer (BondComputer.h:136-192).
 void ref_bond_forces(const int* bonds, const int* table_idx, const int* forms, size_t nb,
 					 const float* pos4, float* fe4, float* table_values,

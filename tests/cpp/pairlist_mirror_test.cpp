@@ -366,6 +366,43 @@ static void reorder_stage_test(const Resource& res) {
 	EXPECT(!patch.reorder_particles(flat, arrays, n, bi, &ex), "degenerate box skips the reorder");
 }
 
+// Analytical pair terms and restraints through the mirror: a Coulomb pair
+// and a restrained particle, against the closed forms.
+static void analytic_terms_test(const Resource& res) {
+	const int n = 3;
+	B200Patch patch(res, n);
+	patch.set_periodic_box(PeriodicBox(Vector3(0, 0, 0), Vector3(100, 100, 100)));
+	// one type, Coulomb only (tag bit 0), no tables
+	patch.set_pair_tables(1, {1u}, {});
+	patch.set_pair_terms({1.0f}, {2.0f}, {0.5f});
+	std::vector<Vector3> h = {Vector3(10, 10, 10), Vector3(14, 10, 10), Vector3(60, 60, 60)};
+	DeviceBuffer<Vector3> pos(n, res), fe(n, res);
+	DeviceBuffer<int> types(n, res);
+	pos.copy_from_host(h);
+	fe.fill_zero();
+	types.copy_from_host(std::vector<int>(n, 0));
+	patch.calculate_nonbonded_forces(pos, types, fe, n, 12.0f, 10.0f, 1, 20, true);
+	std::vector<Vector3> f;
+	fe.copy_to_host(f);
+	const float want = 332.0636f / 16.0f;  // q q C / r^2 at r = 4
+	EXPECT(std::fabs(f[1].x - want) < 1e-4f * want && std::fabs(f[0].x + want) < 1e-4f * want &&
+			   f[2].x == 0.0f,
+		   "Coulomb pair force q1 q2 C / r^2, opposite on the two particles");
+	EXPECT(std::fabs(f[0].t - 0.5f * 332.0636f / 4.0f) < 1e-3f, "Coulomb energy halves");
+	DeviceBuffer<int> rid(1, res);
+	DeviceBuffer<Vector3> anchor(1, res);
+	DeviceBuffer<float> rk(1, res);
+	rid.copy_from_host(std::vector<int>{2});
+	anchor.copy_from_host(std::vector<Vector3>{Vector3(57, 60, 60)});
+	rk.copy_from_host(std::vector<float>{2.0f});
+	fe.fill_zero();
+	patch.calculate_dihedral_and_restraint_forces(pos, fe, nullptr, nullptr, 0, rid.data(),
+												  anchor.data(), rk.data(), 1, true);
+	fe.copy_to_host(f);
+	EXPECT(std::fabs(f[2].x + 6.0f) < 1e-5f && std::fabs(f[2].t - 9.0f) < 1e-5f,
+		   "restraint: F = -k (x - x0), E = k |x - x0|^2 / 2");
+}
+
 int main() {
 	Resource res;
 	res.device = 0;
@@ -377,6 +414,7 @@ int main() {
 		patch_stage_test(res);
 		langevin_stage_test(res);
 		reorder_stage_test(res);
+		analytic_terms_test(res);
 	} catch (const std::exception& e) {
 		std::printf("FAIL unexpected exception: %s\n", e.what());
 		++failures;

@@ -325,9 +325,112 @@ def reorder(O, R):
                 rc_list=np.float32(25.0))
 
 
+def _dihedral_table(k=2.0, mult=3, delta=0.3, bins=72):
+    """Periodic cosine dihedral table on [-pi, pi): U = k (1 + cos(n phi - delta));
+    step_inv as the bonded tables compute it, float(1 / double(step))."""
+    step = 2.0 * math.pi / bins
+    x = -math.pi + np.arange(bins) * step
+    u = (k * (1.0 + np.cos(mult * x - delta))).astype(np.float32)
+    return u, np.float32(-math.pi), np.float32(1.0 / step)
+
+
+def terms(O, R):
+    """Every remaining term on the path: analytical pair terms (Coulomb,
+    Debye-Hueckel, Onck, Gaussian, softcore, alone and combined with each
+    other and with tables), tabulated dihedrals (periodic tables, degenerate
+    and wrapped quadruples, skipped rows), harmonic restraints (anchors across
+    the boundary, skipped ids) and bonds / angles whose form is not tabulated.
+    14^3 = 2,744 beads, 4 types, jittered lattice in a 60 A periodic box. The
+    pair list (12 A) is the canonical sorted list, rebuilt by the tests."""
+    rng = np.random.default_rng(SEED + 11)
+    m, L = 14, 60.0
+    a = L / m
+    g = np.stack(np.meshgrid(np.arange(m), np.arange(m), np.arange(m), indexing="ij"), -1)
+    g = g.reshape(-1, 3)
+    n = len(g)
+    pos = np.zeros((n, 4), np.float32)
+    pos[:, :3] = ((g + 0.5) * a + rng.uniform(-0.8, 0.8, size=(n, 3)) - L / 2).astype(np.float32)
+    types = rng.integers(0, 4, n).astype(np.int32)
+    charge = np.array([1.0, -1.0, 0.5, -0.25], np.float32)
+    radius = np.array([2.0, 2.5, 3.0, 1.5], np.float32)
+    eps = np.array([0.5, 0.3, 0.2, 0.4], np.float32)
+    solvent = np.array([8.0, 78.5, 0.12, 78.0, 6.0], np.float32)
+    gaussian = np.array([1.0, 1.0, 0.0], np.float32)
+    # term bits: 1 Coulomb, 2 Debye-Hueckel, 4 Onck, 8 Gaussian, 16 softcore, 32 table
+    tag = {(0, 0): 1, (0, 1): 2, (0, 2): 4, (0, 3): 8, (1, 1): 16, (1, 2): 32 | (0 << 8),
+           (1, 3): 2 | 32 | (1 << 8), (2, 2): 1 | 8 | 16, (2, 3): 31 | 32 | (1 << 8), (3, 3): 0}
+    term = np.zeros(16, np.uint32)
+    for (x, y), t in tag.items():
+        term[x * 4 + y] = term[y * 4 + x] = t
+    tab, ts = _tables_arrays([W.wca_table(sigma=3.0), W.dh_softcore_table(1.0, -0.25, rmax=20.0)])
+    box = po.Box.make((-L / 2,) * 3, (L, L, L))
+    rc_list, cutoff = 12.0, 10.0
+    _, pairs, _ = _pair_walk(O, R, pos, box, rc_list)
+    tags = R.resolve_tags(pairs, types, term, 4)
+    pts = po.PairTermSet(charge, radius, eps, solvent, gaussian)
+    cutoff_sq = np.float32(cutoff) ** 2
+    pair_fe = R.pair_forces_terms(pairs, pos, types, tags, ts, pts, box, cutoff_sq)
+    pair_fe_noe = R.pair_forces_terms(pairs, pos, types, tags, ts, pts, box, cutoff_sq,
+                                      get_energy=False)
+
+    def idx(x, y, z):
+        return ((x % m) * m + (y % m)) * m + (z % m)
+    quads = []
+    for x in range(m):
+        for y in range(0, m, 2):
+            for z in range(0, m, 3):
+                quads.append((idx(x, y, z), idx(x + 1, y, z), idx(x + 1, y + 1, z),
+                              idx(x + 1, y + 1, z + 1)))
+    for x in range(0, m, 2):          # nearly collinear rows: the degenerate branch
+        quads.append((idx(x, 0, 0), idx(x + 1, 0, 0), idx(x + 2, 0, 0), idx(x + 3, 0, 0)))
+    dih = np.array(quads, np.int32)
+    d_idx = (np.arange(len(dih)) % 2).astype(np.int32)
+    d_idx[::17] = -1
+    dtabs = [_dihedral_table(), _dihedral_table(k=1.0, mult=1, delta=-1.2, bins=36)]
+    dts = po.TableSet(dtabs, periodic=True)
+    dih_fe = R.dihedral_forces(dih, d_idx, pos, dts, box)
+
+    nr = 400
+    rid = rng.choice(n, nr, replace=False).astype(np.int32)
+    rid[::23] = -1
+    anchors = np.zeros((nr, 4), np.float32)
+    anchors[:, :3] = (pos[np.maximum(rid, 0), :3] + rng.uniform(-3, 3, (nr, 3))).astype(np.float32)
+    anchors[:10, :3] = (anchors[:10, :3] + L * 0.97).astype(np.float32)  # across the boundary
+    rk = rng.uniform(0.5, 5.0, nr).astype(np.float32)
+    rest_fe = R.restraint_forces(rid, anchors, rk, pos, box)
+
+    bonds = np.array([(idx(x, y, z), idx(x, y, z + 1)) for x in range(m) for y in range(m)
+                      for z in range(m - 1)], np.int32)
+    b_idx = np.zeros(len(bonds), np.int32)
+    b_idx[::5] = -1
+    bspec = W.harmonic_bond_table(r0=4.3)
+    bts = po.TableSet([(bspec.values, bspec.start, bspec.step_inv)])
+    bond_fe = R.bond_forces(bonds, b_idx, pos, bts, box)
+    angles = np.array([(idx(x, y, z), idx(x, y, z + 1), idx(x, y + 1, z + 1), 0)
+                       for x in range(m) for y in range(m) for z in range(0, m, 2)], np.int32)
+    a_idx = np.zeros(len(angles), np.int32)
+    a_idx[::7] = -1
+    aspec = W.harmonic_angle_table(k=5.0, theta0_deg=90.0)
+    ats = po.TableSet([(aspec.values, aspec.start, aspec.step_inv)], periodic=True)
+    angle_fe = R.angle_forces(angles, a_idx, pos, ats, box)
+    return dict(pos=pos, type_ids=types, term_matrix=term, **tab, charge=charge, radius=radius,
+                eps=eps, solvent=solvent, gaussian=gaussian,
+                **_box_arrays(box.origin, box.size, box.periodic), rc_list=np.float32(rc_list),
+                cutoff=np.float32(cutoff), num_pairs=np.int64(len(pairs)),
+                checksum=np.uint64(O.pair_hash_sum(pairs)), pair_fe=pair_fe,
+                pair_fe_noe=pair_fe_noe, dihedrals=dih, dihedral_idx=d_idx,
+                dih_values=dts.values, dih_sizes=dts.sizes, dih_starts=dts.starts,
+                dih_step_invs=dts.step_invs, dihedral_fe=dih_fe, restraint_ids=rid,
+                restraint_anchors=anchors, restraint_k=rk, restraint_fe=rest_fe, bonds=bonds,
+                bond_idx=b_idx, bond_values=bts.values, bond_start=np.float32(bts.starts[0]),
+                bond_step_inv=np.float32(bts.step_invs[0]), bond_fe=bond_fe, angles=angles,
+                angle_idx=a_idx, angle_values=ats.values, angle_start=np.float32(ats.starts[0]),
+                angle_step_inv=np.float32(ats.step_invs[0]), angle_fe=angle_fe)
+
+
 CASES = {"uniform4096": uniform, "lattice_open": lattice, "polymer_excl": polymer,
          "chain129": chain, "philox": philox, "grid_bd": grid_bd, "wrap_table": wrap_table,
-         "baoab": baoab, "reorder": reorder}
+         "baoab": baoab, "reorder": reorder, "terms": terms}
 
 
 def main():

@@ -252,3 +252,62 @@ def test_baoab_step_matches_reference(oracle):
         assert np.array_equal(pos, d[f"pos_after_{pending}"])
         assert np.array_equal(mom, d[f"mom_after_{pending}"])
         assert np.array_equal(fe, d[f"fe_after_{pending}"])
+
+
+# --- analytical pair terms, dihedrals, restraints, skipped forms ------------------------
+
+def _terms_setup(oracle):
+    d = _load("terms")
+    box = _box(d)
+    pairs, cnt, _ = oracle.build_pairlist(d["pos"], box, float(d["rc_list"]))
+    pairs = _canon(pairs)
+    tags = oracle.resolve_tags(pairs, d["type_ids"], d["term_matrix"], 4)
+    pts = po.PairTermSet(d["charge"], d["radius"], d["eps"], d["solvent"], d["gaussian"])
+    return d, box, pairs, tags, pts
+
+
+def test_analytical_pair_terms_match_reference_bit_exact(oracle):
+    """Coulomb, Debye-Hueckel, Onck, Gaussian, softcore and tables, alone and
+    summed in one pair, with and without energy."""
+    d, box, pairs, tags, pts = _terms_setup(oracle)
+    assert len(pairs) == int(d["num_pairs"])
+    assert oracle.pair_hash_sum(pairs) == int(d["checksum"])
+    present = {int(t) & 0xFF for t in np.unique(tags)}
+    assert {1, 2, 4, 8, 16, 32, 34, 25, 63} <= present
+    cut2 = np.float32(d["cutoff"]) ** 2
+    fe, _, _ = oracle.pair_forces_terms(pairs, d["pos"], d["type_ids"], tags, _tables(d), pts,
+                                        box, cut2)
+    assert np.array_equal(fe, d["pair_fe"])
+    fe0, _, _ = oracle.pair_forces_terms(pairs, d["pos"], d["type_ids"], tags, _tables(d), pts,
+                                         box, cut2, get_energy=False)
+    assert np.array_equal(fe0, d["pair_fe_noe"])
+
+
+def test_dihedral_and_restraint_forces_match_reference_bit_exact(oracle):
+    d = _load("terms")
+    box = _box(d)
+    vals, sizes = d["dih_values"], d["dih_sizes"]
+    offs = np.concatenate([[0], np.cumsum(sizes)[:-1]]).astype(int)
+    dts = po.TableSet([(vals[o:o + s], float(a), float(b)) for o, s, a, b in
+                       zip(offs, sizes, d["dih_starts"], d["dih_step_invs"])], periodic=True)
+    fd, _, _ = oracle.dihedral_forces(d["dihedrals"], d["dihedral_idx"], d["pos"], dts, box)
+    assert np.array_equal(fd, d["dihedral_fe"])
+    fr, _, _ = oracle.restraint_forces(d["restraint_ids"], d["restraint_anchors"],
+                                       d["restraint_k"], d["pos"], box)
+    assert np.array_equal(fr, d["restraint_fe"])
+    skipped = d["restraint_ids"] < 0
+    assert skipped.any() and (d["dihedral_idx"] < 0).any()
+
+
+def test_bonded_rows_of_other_forms_are_skipped(oracle):
+    """Bond / angle rows whose form is not tabulated (index < 0) add nothing,
+    as TabulatedBondComputer / TabulatedAngleComputer skip them."""
+    d = _load("terms")
+    box = _box(d)
+    bts = po.TableSet([(d["bond_values"], float(d["bond_start"]), float(d["bond_step_inv"]))])
+    fb, _, _ = oracle.bond_forces(d["bonds"], d["bond_idx"], d["pos"], bts, box)
+    assert np.array_equal(fb, d["bond_fe"])
+    ats = po.TableSet([(d["angle_values"], float(d["angle_start"]), float(d["angle_step_inv"]))],
+                      periodic=True)
+    fa, _, _ = oracle.angle_forces(d["angles"], d["angle_idx"], d["pos"], ats, box)
+    assert np.array_equal(fa, d["angle_fe"])
