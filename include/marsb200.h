@@ -43,6 +43,7 @@ extern "C" {
 #define MB2_ERR_CUDA 2     /* CUDA runtime error */
 #define MB2_ERR_CAPACITY 3 /* more particles/pairs than the context allows */
 #define MB2_ERR_STATE 4    /* required set-up missing (box, tables, pairlist) */
+#define MB2_ERR_IO 5       /* file output failed */
 
 typedef struct mb2_context mb2_context;
 
@@ -336,6 +337,54 @@ typedef struct {
 MB2_API int mb2_step(mb2_context* ctx, float* pos4, float* force_energy4, const int* type_ids,
              const uint32_t* flags, uint32_t n, uint64_t step, const mb2_step_params* params,
              void* stream);
+
+/* --- output ------------------------------------------------------------------
+ * The output side of SimManager for one system (src/SimManager.cpp:318-330
+ * initialize_output_writers, :541-575 handle_output): a DCD trajectory
+ * <name>.dcd with DcdWriter's byte layout (src/IO/DcdWriter.h; header on the
+ * first frame with NPRIV = NSAVC = output_period, DELTA = timestep, a CHARMM
+ * unit cell (A, 0, B, 0, 0, C) per frame when any axis is periodic), with
+ * momenta the Langevin momentum DCD <name>.0.momentum.dcd (:833-861);
+ * <name>.energy.dat (write_energy_output, :999-1068); restart files
+ * <name>.restart and <name>.0.momentum.restart, one "type x y z" line per
+ * particle in shortest round-trip decimals (write_restart_files,
+ * :1078-1135). An existing DCD file is renamed to <name>.dcd.BAK.
+ * Rows are written in global-id order: ids (device int[n], may be NULL =
+ * identity) maps each row to its place, as copy_to_host_unpermuted does
+ * after a Morton reorder (src/Objects/DeviceParticleManager.h:219-260).
+ * Frames and restarts are packed on the device and written by a background
+ * thread: a call returns once its copy is queued; at most two are in flight
+ * (a third waits). mb2_output_flush waits for them and reports a failed
+ * write. Device pointers, except mass (host). */
+typedef struct mb2_output mb2_output;
+typedef struct {
+    const char* output_name;
+    uint32_t num_particles;
+    int output_period;   /* DCD NSAVC (values below 1 become 1) */
+    float timestep;      /* DCD DELTA */
+    float box[3];        /* unit cell edges */
+    int periodic[3];
+    int with_momentum;   /* Langevin: momentum DCD and momentum restart */
+    int device;
+} mb2_output_config;
+MB2_API int mb2_output_create(const mb2_output_config* cfg, mb2_output** out);
+/* Waits for queued writes, closes the files. */
+MB2_API int mb2_output_destroy(mb2_output* out);
+MB2_API const char* mb2_output_last_error(const mb2_output* out);
+/* One trajectory frame (and momentum frame). */
+MB2_API int mb2_output_frame(mb2_output* out, const float* pos4, const float* mom4, const int* ids,
+                             uint32_t n, void* stream);
+/* Restart files (positions, type ids; momenta with with_momentum). */
+MB2_API int mb2_output_restart(mb2_output* out, const float* pos4, const float* mom4,
+                               const int* type_ids, const int* ids, uint32_t n, void* stream);
+/* FP64 reductions on the device: potential = sum of force_energy .w (kcal/mol),
+ * kinetic = sum 0.5 |p|^2 / mass[type] / SQRT_CAL_TO_JOULE^2 / kT (kT units;
+ * 0 without momenta); appends both lines to <name>.energy.dat and returns
+ * them in out[0] (kinetic) and out[1] (potential). Synchronises. */
+MB2_API int mb2_output_energy(mb2_output* out, const float* force_energy4, const float* mom4,
+                              const int* type_ids, const float* mass, int num_types, uint32_t n,
+                              float kT, void* stream, double out2[2]);
+MB2_API int mb2_output_flush(mb2_output* out);
 
 /* --- tracing ---------------------------------------------------------------
  * Per-stage device timing with CUDA events on the launching stream (replaces

@@ -37,6 +37,13 @@ class StepParams(C.Structure):
                 ("num_restraints", C.c_uint32)]
 
 
+class OutputConfig(C.Structure):
+    """mb2_output_config."""
+    _fields_ = [("output_name", C.c_char_p), ("num_particles", C.c_uint32),
+                ("output_period", C.c_int), ("timestep", C.c_float), ("box", C.c_float * 3),
+                ("periodic", C.c_int * 3), ("with_momentum", C.c_int), ("device", C.c_int)]
+
+
 class PairParams(C.Structure):
     """mb2_pair_params (defaults: the reference's SolventParams and Gaussian)."""
     _fields_ = [("debye_length", C.c_float), ("dielectric", C.c_float),
@@ -104,6 +111,14 @@ def load(path: str = LIB_PATH):
     L.mb2_profile_read.argtypes = [vp, i, C.POINTER(C.c_double), u32p]
     L.mb2_launch_count.restype = u64
     L.mb2_launch_count.argtypes = []
+    L.mb2_output_create.argtypes = [C.POINTER(OutputConfig), C.POINTER(vp)]
+    L.mb2_output_destroy.argtypes = [vp]
+    L.mb2_output_last_error.restype = C.c_char_p
+    L.mb2_output_last_error.argtypes = [vp]
+    L.mb2_output_frame.argtypes = [vp, vp, vp, vp, u32, vp]
+    L.mb2_output_restart.argtypes = [vp, vp, vp, vp, vp, u32, vp]
+    L.mb2_output_energy.argtypes = [vp, vp, vp, vp, fp, i, u32, f, vp, C.POINTER(C.c_double)]
+    L.mb2_output_flush.argtypes = [vp]
     L.mb2_set_pair_terms.argtypes = [vp, i, fp, fp, fp, C.POINTER(PairParams)]
     L.mb2_dihedral_forces.argtypes = [vp, vp, vp, u32, vp, vp, i, vp]
     L.mb2_restraint_forces.argtypes = [vp, vp, vp, vp, u32, vp, vp, i, vp]

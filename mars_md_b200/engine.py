@@ -18,7 +18,9 @@ call surface on the Brownian-dynamics path:
   (src/PatchOperation/Integrator.h:26-54);
 * ``step`` -- one SimManager step for one patch (src/SimManager.cpp:337-504);
 * ``reorder_*`` / ``reorder_particles`` / ``ReorderManager`` -- the canonical
-  Morton reorder of a patch (src/PatchOperation/Patch.cpp:455-480).
+  Morton reorder of a patch (src/PatchOperation/Patch.cpp:455-480);
+* ``Output`` -- DCD frames, the energy file and restart files
+  (src/SimManager.cpp:541-1135, src/IO/DcdWriter.h).
 
 ``Batch`` wraps one ``mb2_batch``: many independent periodic systems stepped
 together (one launch per stage for all of them, CUDA-graph step replay, an
@@ -402,6 +404,86 @@ class ReorderManager:
         if (step - 1) % self.period:
             return False
         return bool(bonded_prepared)
+
+
+class Output:
+    """SimManager's output side for one system (src/SimManager.cpp:318-330,
+    541-575, 596-633, 833-861, 999-1135) over mb2_output: DCD frames (and the
+    Langevin momentum DCD), the energy file and restart files, rows in
+    global-id order; frames and restarts are written by a background thread.
+
+    ``handle_output(step, ...)`` applies the reference's cadence: a frame when
+    step % output_period == 0, energies (then restart files) when
+    step % energy_output_period == 0."""
+
+    def __init__(self, output_name, num_particles, output_period=1, energy_output_period=0,
+                 timestep=1.0, box=(0.0, 0.0, 0.0), periodic=(1, 1, 1), with_momentum=False,
+                 device=0):
+        self.lib = L.load()
+        cfg = L.OutputConfig()
+        cfg.output_name = str(output_name).encode()
+        cfg.num_particles = int(num_particles)
+        cfg.output_period = int(output_period)
+        cfg.timestep = float(timestep)
+        for a in range(3):
+            cfg.box[a] = float(box[a])
+            cfg.periodic[a] = int(periodic[a])
+        cfg.with_momentum = int(with_momentum)
+        cfg.device = int(device)
+        h = C.c_void_p()
+        rc = self.lib.mb2_output_create(C.byref(cfg), C.byref(h))
+        if rc != 0:
+            raise L.MB2Error(rc, "mb2_output_create failed")
+        self.h = h
+        self.n = int(num_particles)
+        self.output_period = int(output_period)
+        self.energy_output_period = int(energy_output_period)
+        self.with_momentum = bool(with_momentum)
+
+    def check(self, rc):
+        if rc != 0:
+            raise L.MB2Error(rc, self.lib.mb2_output_last_error(self.h).decode())
+
+    def frame(self, pos, mom=None, ids=None, stream=None):
+        self.check(self.lib.mb2_output_frame(self.h, _p(pos), _p(mom), _p(ids), self.n,
+                                             _stream(stream)))
+
+    def restart(self, pos, type_ids, mom=None, ids=None, stream=None):
+        self.check(self.lib.mb2_output_restart(self.h, _p(pos), _p(mom), _p(type_ids), _p(ids),
+                                               self.n, _stream(stream)))
+
+    def energy(self, fe, kT, mom=None, type_ids=None, mass=None, stream=None):
+        """Appends to <name>.energy.dat; returns (kinetic in kT, potential in kcal/mol)."""
+        out = (C.c_double * 2)()
+        m = None if mass is None else np.ascontiguousarray(mass, np.float32)
+        self.check(self.lib.mb2_output_energy(
+            self.h, _p(fe), _p(mom), _p(type_ids),
+            m.ctypes.data_as(C.POINTER(C.c_float)) if m is not None else None,
+            0 if m is None else len(m), self.n, float(kT), _stream(stream), out))
+        return float(out[0]), float(out[1])
+
+    def handle_output(self, step, pos, fe, type_ids, kT, mom=None, mass=None, ids=None,
+                      stream=None):
+        """SimManager::handle_output's schedule for one step."""
+        if self.output_period > 0 and step % self.output_period == 0:
+            self.frame(pos, mom, ids, stream)
+        if self.energy_output_period > 0 and step % self.energy_output_period == 0:
+            self.energy(fe, kT, mom, type_ids, mass, stream)
+            self.restart(pos, type_ids, mom, ids, stream)
+
+    def flush(self):
+        self.check(self.lib.mb2_output_flush(self.h))
+
+    def close(self):
+        if getattr(self, "h", None) is not None and self.h.value:
+            self.lib.mb2_output_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 def to_original_order(values, ids):

@@ -15,7 +15,8 @@
 //     calculate_nonbonded_forces (rebuild schedule + skin check + pair
 //     forces), calculate_bonded_forces, integrate_motion (BD or Langevin
 //     BAOAB with the deferred closing kick), finish_deferred_kick and
-//     reorder_particles (with ExclusionCSR and ParticleReorderManager).
+//     reorder_particles (with ExclusionCSR and ParticleReorderManager);
+//   * SimOutput: SimManager's DCD, energy and restart output.
 //
 // Errors are thrown as marsb200::Exception carrying the library's message,
 // as the reference throws MARS::Exception; the C ABI underneath never throws.
@@ -38,7 +39,14 @@
 
 namespace marsb200 {
 
-enum class ExceptionType { ValueError, CUDAError, CapacityError, StateError, NotImplementedError };
+enum class ExceptionType {
+	ValueError,
+	CUDAError,
+	CapacityError,
+	StateError,
+	NotImplementedError,
+	FileIoError
+};
 
 class Exception : public std::runtime_error {
   public:
@@ -57,6 +65,7 @@ inline void check(int rc, const mb2_context* ctx, const char* what) {
 		case MB2_ERR_CUDA: throw Exception(ExceptionType::CUDAError, msg);
 		case MB2_ERR_CAPACITY: throw Exception(ExceptionType::CapacityError, msg);
 		case MB2_ERR_STATE: throw Exception(ExceptionType::StateError, msg);
+		case MB2_ERR_IO: throw Exception(ExceptionType::FileIoError, msg);
 		default: throw Exception(ExceptionType::ValueError, msg);
 	}
 }
@@ -714,6 +723,97 @@ class B200Patch {
 	bool built_ = false;
 	size_t built_n_ = 0;
 	bool deferred_kick_pending_ = false;
+};
+
+// SimManager's output side for one system (src/SimManager.cpp:318-330,
+// 541-575, 596-633, 833-861, 999-1135) over mb2_output: DCD frames (and the
+// Langevin momentum DCD), <name>.energy.dat, restart files; rows in global-id
+// order through `ids` (may be null). Frames and restarts are written by the
+// library's writer thread; flush() waits for them.
+class SimOutput {
+  public:
+	SimOutput(const std::string& output_name, size_t num_particles, int output_period,
+			  int energy_output_period, float timestep, const PeriodicBox& box,
+			  bool with_momentum = false, const Resource& r = Resource{})
+		: res_(r), n_(num_particles), output_period_(output_period),
+		  energy_output_period_(energy_output_period) {
+		mb2_output_config cfg{};
+		cfg.output_name = output_name.c_str();
+		cfg.num_particles = static_cast<uint32_t>(num_particles);
+		cfg.output_period = output_period;
+		cfg.timestep = timestep;
+		cfg.box[0] = box.get_size().x;
+		cfg.box[1] = box.get_size().y;
+		cfg.box[2] = box.get_size().z;
+		for (int a = 0; a < 3; ++a) cfg.periodic[a] = box.is_periodic(a) ? 1 : 0;
+		cfg.with_momentum = with_momentum ? 1 : 0;
+		cfg.device = r.device;
+		const int rc = mb2_output_create(&cfg, &out_);
+		if (rc != MB2_OK) throw Exception(ExceptionType::ValueError, "SimOutput: mb2_output_create failed");
+	}
+	SimOutput(const SimOutput&) = delete;
+	SimOutput& operator=(const SimOutput&) = delete;
+	~SimOutput() {
+		if (out_) mb2_output_destroy(out_);
+	}
+	void write_dcd_frame(const DeviceBuffer<Vector3>& pos, const DeviceBuffer<Vector3>* mom = nullptr,
+						 const int* ids = nullptr) {
+		ok(mb2_output_frame(out_, reinterpret_cast<const float*>(pos.data()),
+							mom ? reinterpret_cast<const float*>(mom->data()) : nullptr, ids,
+							static_cast<uint32_t>(n_), stream()),
+		   "write_dcd_frame");
+	}
+	void write_restart_files(const DeviceBuffer<Vector3>& pos, const DeviceBuffer<int>& types,
+							 const DeviceBuffer<Vector3>* mom = nullptr, const int* ids = nullptr) {
+		ok(mb2_output_restart(out_, reinterpret_cast<const float*>(pos.data()),
+							  mom ? reinterpret_cast<const float*>(mom->data()) : nullptr,
+							  types.data(), ids, static_cast<uint32_t>(n_), stream()),
+		   "write_restart_files");
+	}
+	// Returns {kinetic (kT), potential (kcal/mol)} and appends them to the file.
+	std::pair<double, double> write_energy_output(const DeviceBuffer<Vector3>& force_energy,
+												  float kT, const DeviceBuffer<Vector3>* mom = nullptr,
+												  const DeviceBuffer<int>* types = nullptr,
+												  const std::vector<float>& mass = {}) {
+		double e[2] = {0.0, 0.0};
+		ok(mb2_output_energy(out_, reinterpret_cast<const float*>(force_energy.data()),
+							 mom ? reinterpret_cast<const float*>(mom->data()) : nullptr,
+							 types ? types->data() : nullptr, mass.empty() ? nullptr : mass.data(),
+							 static_cast<int>(mass.size()), static_cast<uint32_t>(n_), kT, stream(), e),
+		   "write_energy_output");
+		return {e[0], e[1]};
+	}
+	// SimManager::handle_output's schedule: a frame every output_period steps;
+	// energies, then restart files, every energy_output_period steps.
+	void handle_output(size_t step, const DeviceBuffer<Vector3>& pos,
+					   const DeviceBuffer<Vector3>& force_energy, const DeviceBuffer<int>& types,
+					   float kT, const DeviceBuffer<Vector3>* mom = nullptr,
+					   const std::vector<float>& mass = {}, const int* ids = nullptr) {
+		if (output_period_ > 0 && step % static_cast<size_t>(output_period_) == 0)
+			write_dcd_frame(pos, mom, ids);
+		if (energy_output_period_ > 0 && step % static_cast<size_t>(energy_output_period_) == 0) {
+			write_energy_output(force_energy, kT, mom, mom ? &types : nullptr, mass);
+			write_restart_files(pos, types, mom, ids);
+		}
+	}
+	void flush() { ok(mb2_output_flush(out_), "flush"); }
+
+  private:
+	void* stream() const { return reinterpret_cast<void*>(res_.stream); }
+	void ok(int rc, const char* what) {
+		if (rc == MB2_OK) return;
+		const std::string msg = std::string(what) + ": " + mb2_output_last_error(out_);
+		switch (rc) {
+			case MB2_ERR_ARG: throw Exception(ExceptionType::ValueError, msg);
+			case MB2_ERR_IO: throw Exception(ExceptionType::FileIoError, msg);
+			case MB2_ERR_CUDA: throw Exception(ExceptionType::CUDAError, msg);
+			default: throw Exception(ExceptionType::StateError, msg);
+		}
+	}
+	Resource res_;
+	size_t n_;
+	int output_period_, energy_output_period_;
+	mb2_output* out_ = nullptr;
 };
 
 }  // namespace marsb200

@@ -549,6 +549,7 @@ class RefHarness:
         L.ref_inverse.argtypes = [vp, vp, sz]
         L.ref_reorder_pos.argtypes = [vp, vp, vp, sz]
         L.ref_remap_indices.argtypes = [vp, sz, vp, sz]
+        L.ref_dcd_write.argtypes = [C.c_char_p, vp, i, i, i, f, i, vp]
         L.ref_pair_forces_terms.argtypes = [vp, sz, vp, vp, vp, vp, vp, vp, vp, vp, vp, i, vp, vp,
                                             vp, i, f, u32, vp, vp, vp, vp, vp]
         L.ref_dihedral_forces.argtypes = [vp, vp, vp, sz, vp, vp, vp, vp, vp, vp, vp, i, vp, vp,
@@ -608,6 +609,15 @@ class RefHarness:
         out = np.zeros_like(pos4)
         self.lib.ref_reorder_pos(_ptr(pos4), _ptr(out), _ptr(s), len(s))
         return out
+
+    def dcd_write(self, path, frames4, nsavc, delta, with_unitcell, box):
+        """The reference's DcdWriter driven as write_dcd_frame drives it."""
+        fr = np.ascontiguousarray(frames4, np.float32)
+        rc = self.lib.ref_dcd_write(str(path).encode(), _ptr(fr), fr.shape[0], fr.shape[1],
+                                    int(nsavc), C.c_float(delta), int(with_unitcell),
+                                    _ptr(np.asarray(box, np.float32)))
+        if rc != 0:
+            raise RuntimeError("reference DcdWriter failed")
 
     def remap_indices(self, indices, inv):
         out = np.ascontiguousarray(indices, np.int32).copy()

@@ -15,6 +15,7 @@
 // CUDASort.cu:13-98); CUB's LSD radix sort is stable, so std::stable_sort on
 // the key gives the identical permutation.
 
+#include "IO/DcdWriter.h"
 #include "Interactions/Bonded/BondComputer.h"
 #include "Interactions/Nonbonded/Pairwise.h"
 #include "PatchOperation/Integrator/BAOAB.h"
@@ -118,6 +119,33 @@ void ref_reorder_pos(const float* pos4, float* out4, const uint32_t* sorted, siz
 								 reinterpret_cast<Vector3*>(out4), sorted, n};
 	for (size_t i = 0; i < n; ++i)
 		k(i);
+}
+
+// DcdWriter (src/IO/DcdWriter.h) driven as SimManager::write_dcd_frame drives
+// it (SimManager.cpp:596-633): header on the first frame (N, NFILE 1,
+// NPRIV = NSAVC = output period, NSTEP 0, DELTA = timestep, unit cell when any
+// axis is periodic), then one writeStep per frame with the CHARMM unit cell
+// (A, 0, B, 0, 0, C). frames: n_frames x n float4 rows.
+int ref_dcd_write(const char* path, const float* frames4, int n_frames, int n, int nsavc,
+				  float delta, int with_unitcell, const float* box) {
+	try {
+		DcdWriter w(path);
+		for (int f = 0; f < n_frames; ++f) {
+			if (f == 0) w.writeHeader(n, 1, nsavc, nsavc, 0, delta, with_unitcell != 0);
+			std::vector<Vector3> frame(n);
+			for (int i = 0; i < n; ++i) {
+				const float* p = frames4 + (static_cast<size_t>(f) * n + i) * 4;
+				frame[i] = Vector3(p[0], p[1], p[2]);
+			}
+			if (with_unitcell)
+				w.writeStep(frame, std::vector<double>{box[0], 0.0, box[1], 0.0, 0.0, box[2]});
+			else
+				w.writeStep(frame);
+		}
+	} catch (const std::exception&) {
+		return -1;
+	}
+	return 0;
 }
 
 // RemapIndicesKernel (ZOrderKernels.h:87-101).

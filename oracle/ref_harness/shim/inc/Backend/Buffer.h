@@ -24,6 +24,7 @@ class DeviceBuffer {
 	void copy_from_host(const T* src, size_t n, bool = false) { std::memcpy(v_.data(), src, n * sizeof(T)); }
 	void copy_to_host(T* dst, size_t n, bool = false) const { std::memcpy(dst, v_.data(), n * sizeof(T)); }
 	void copy_to_host_sync(T* dst, size_t n) const { copy_to_host(dst, n); }
+	void copy_to_host(std::vector<T>& dst) const { dst = v_; }
 	void fill(const T& v, bool = false) { for (auto& x : v_) x = v; }
   private:
 	std::vector<T> v_;

@@ -6,6 +6,7 @@
 // against the fused step. One line per check; exit status 0 only if all pass.
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <random>
 #include <set>
 #include <utility>
@@ -403,6 +404,38 @@ static void analytic_terms_test(const Resource& res) {
 		   "restraint: F = -k (x - x0), E = k |x - x0|^2 / 2");
 }
 
+// SimOutput through the mirror: a frame and a restart in global-id order.
+static void output_test(const Resource& res) {
+	char dir[] = "/tmp/mb2outXXXXXX";
+	if (!mkdtemp(dir)) {
+		EXPECT(false, "output: temporary directory");
+		return;
+	}
+	const std::string name = std::string(dir) + "/run";
+	const int n = 4;
+	SimOutput out(name, n, 1, 1, 0.5f, PeriodicBox(Vector3(0, 0, 0), Vector3(10, 10, 10)), false,
+				  res);
+	std::vector<Vector3> h = {Vector3(1, 2, 3), Vector3(4, 5, 6), Vector3(7, 8, 9),
+							  Vector3(0.5f, 0.25f, 0.125f)};
+	DeviceBuffer<Vector3> pos(n, res), fe(n, res);
+	DeviceBuffer<int> types(n, res), ids(n, res);
+	pos.copy_from_host(h);
+	fe.copy_from_host(std::vector<Vector3>{Vector3(0, 0, 0, 1.5f), Vector3(0, 0, 0, 2.0f),
+										   Vector3(0, 0, 0, -0.5f), Vector3(0, 0, 0, 0.0f)});
+	types.copy_from_host(std::vector<int>{0, 1, 2, 3});
+	ids.copy_from_host(std::vector<int>{3, 2, 1, 0});  // slot s holds global id 3 - s
+	out.handle_output(1, pos, fe, types, 0.6f, nullptr, {}, ids.data());
+	out.flush();
+	FILE* f = std::fopen((name + ".restart").c_str(), "r");
+	char line[128];
+	std::string first;
+	if (f && std::fgets(line, sizeof(line), f)) first = line;
+	if (f) std::fclose(f);
+	EXPECT(first == "3 0.5 0.25 0.125\n", "restart rows in global-id order, shortest decimals");
+	const auto e = out.write_energy_output(fe, 0.6f);
+	EXPECT(e.second == 3.0 && e.first == 0.0, "energy output: potential sum, no kinetic without momenta");
+}
+
 int main() {
 	Resource res;
 	res.device = 0;
@@ -415,6 +448,7 @@ int main() {
 		langevin_stage_test(res);
 		reorder_stage_test(res);
 		analytic_terms_test(res);
+		output_test(res);
 	} catch (const std::exception& e) {
 		std::printf("FAIL unexpected exception: %s\n", e.what());
 		++failures;

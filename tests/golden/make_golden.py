@@ -428,9 +428,29 @@ def terms(O, R):
                 angle_step_inv=np.float32(ats.step_invs[0]), angle_fe=angle_fe)
 
 
+def dcd(O, R):
+    """DCD files from the reference's own DcdWriter: 3 frames of 100 beads,
+    output period 10, timestep 0.1, with the unit cell of a 60 x 70 x 80 A
+    box; and 2 frames without a unit cell. The two title lines carry the
+    file name and the date, which differ between writers."""
+    import tempfile
+    rng = np.random.default_rng(SEED + 13)
+    frames = np.zeros((3, 100, 4), np.float32)
+    frames[..., :3] = rng.uniform(-30, 30, (3, 100, 3)).astype(np.float32)
+    out = dict(frames=frames, nsavc=np.int32(10), delta=np.float32(0.1),
+               box=np.array([60.0, 70.0, 80.0], np.float32))
+    with tempfile.TemporaryDirectory() as d:
+        for tag, cell, nf in (("cell", 1, 3), ("nocell", 0, 2)):
+            path = os.path.join(d, f"{tag}.dcd")
+            R.dcd_write(path, frames[:nf], 10, 0.1, cell, out["box"])
+            out[f"bytes_{tag}"] = np.frombuffer(open(path, "rb").read(), np.uint8)
+    return out
+
+
 CASES = {"uniform4096": uniform, "lattice_open": lattice, "polymer_excl": polymer,
          "chain129": chain, "philox": philox, "grid_bd": grid_bd, "wrap_table": wrap_table,
-         "baoab": baoab, "reorder": reorder, "terms": terms}
+         "baoab": baoab, "reorder": reorder, "terms": terms,
+         "dcd": dcd}
 
 
 def main():

@@ -311,3 +311,21 @@ def test_bonded_rows_of_other_forms_are_skipped(oracle):
                       periodic=True)
     fa, _, _ = oracle.angle_forces(d["angles"], d["angle_idx"], d["pos"], ats, box)
     assert np.array_equal(fa, d["angle_fe"])
+
+
+# --- output ---------------------------------------------------------------------------
+
+def test_dcd_reader_reads_reference_fixture():
+    """The oracle's DCD reader against the reference DcdWriter's bytes: header
+    counters after three frames, unit cells, frames."""
+    import dcd
+    d = _load("dcd")
+    r = dcd.read_dcd(d["bytes_cell"].tobytes())
+    assert (r["nfile"], r["npriv"], r["nsavc"], r["nstep"]) == (3, 10, 10, 30)
+    assert r["delta"] == np.float32(0.1) and r["unitcell"] == 1 and r["version"] == 24
+    assert r["natoms"] == 100
+    assert r["titles"][0].startswith("REMARKS FILENAME=") and r["titles"][1].startswith("REMARKS DATE: ")
+    assert np.array_equal(r["frames"], d["frames"][..., :3])
+    assert np.array_equal(r["cells"], np.tile([60.0, 0.0, 70.0, 0.0, 0.0, 80.0], (3, 1)))
+    r2 = dcd.read_dcd(d["bytes_nocell"].tobytes())
+    assert (r2["nfile"], r2["nstep"], r2["unitcell"]) == (2, 20, 0) and len(r2["cells"]) == 0
