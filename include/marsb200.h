@@ -406,6 +406,12 @@ MB2_API int mb2_profile_read(mb2_context* ctx, int stage, double* total_ms, uint
  * or 32 lanes per row; 0 = choose from the mean row length. */
 MB2_API int mb2_set_lanes_per_row(mb2_context* ctx, int lanes);
 
+/* Cell level of the pairlist walk relative to the cost model's choice
+ * (-2..2; 0 = the model's), and the level the last build used (-1 before
+ * any). A tuning knob: the pair set does not depend on it. */
+MB2_API int mb2_set_cell_level_offset(mb2_context* ctx, int offset);
+MB2_API int mb2_cell_level(mb2_context* ctx, int* level);
+
 /* --- adjoint of a BD window ------------------------------------------------
  * No counterpart in the reference (it computes no gradients). Gradients of a
  * loss of the final positions of a window of BD steps with fixed Philox noise,

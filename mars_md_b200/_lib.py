@@ -107,6 +107,8 @@ def load(path: str = LIB_PATH):
     L.mb2_philox.argtypes = [vp, u64, u32, u32, u32, u32, vp, vp, vp]
     L.mb2_step.argtypes = [vp, vp, vp, vp, vp, u32, u64, C.POINTER(StepParams), vp]
     L.mb2_set_lanes_per_row.argtypes = [vp, i]
+    L.mb2_set_cell_level_offset.argtypes = [vp, i]
+    L.mb2_cell_level.argtypes = [vp, C.POINTER(C.c_int)]
     L.mb2_set_profiling.argtypes = [vp, i]
     L.mb2_profile_read.argtypes = [vp, i, C.POINTER(C.c_double), u32p]
     L.mb2_launch_count.restype = u64

@@ -49,6 +49,7 @@ struct mb2_context {
 	uint64_t max_row = 0;
 	Exclusions excl;
 	int lanes_request = 0;   // 0 = choose from the mean row length
+	int level_offset = 0;    // cell level relative to the cost model's choice
 
 	// pair tables
 	PairTables pt;
@@ -265,6 +266,10 @@ void build(mb2_context* ctx, const float4* pos, const int* type_ids, uint32_t n,
 	if (!ctx->grid_valid || ctx->grid_rc != rc_list || ctx->grid_n != n ||
 		std::memcmp(ctx->grid_extent, extent, sizeof(extent)) != 0) {
 		ctx->grid = choose_cell_grid(extent, ctx->box.periodic, std::sqrt(rc2), n);
+		if (ctx->level_offset != 0) {
+			const int m = std::min(8, std::max(0, ctx->grid.m + ctx->level_offset));
+			ctx->grid = choose_cell_grid(extent, ctx->box.periodic, std::sqrt(rc2), n, m, m);
+		}
 		ctx->stencil.ensure(ctx->grid.stencil.size());
 		MB2_CUDA(cudaMemcpyAsync(ctx->stencil.ptr, ctx->grid.stencil.data(),
 								 ctx->grid.stencil.size() * sizeof(StencilEntry),
@@ -1265,6 +1270,25 @@ int mb2_profile_read(mb2_context* ctx, int stage, double* total_ms, uint32_t* co
 		*total_ms = t;
 		*count = static_cast<uint32_t>(ctx->prof[stage].size());
 		ctx->prof[stage].clear();
+	});
+}
+
+int mb2_set_cell_level_offset(mb2_context* ctx, int offset) {
+	return guarded(ctx, [&] {
+		require(offset >= -2 && offset <= 2, MB2_ERR_ARG,
+				"mb2_set_cell_level_offset: offset in -2..2");
+		if (offset != ctx->level_offset) {
+			ctx->level_offset = offset;
+			ctx->grid_valid = false;
+			ctx->built = false;
+		}
+	});
+}
+
+int mb2_cell_level(mb2_context* ctx, int* level) {
+	return guarded(ctx, [&] {
+		require(level != nullptr, MB2_ERR_ARG, "mb2_cell_level: null output");
+		*level = ctx->grid_valid ? ctx->grid.m : -1;
 	});
 }
 

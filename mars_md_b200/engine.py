@@ -174,6 +174,14 @@ class Context:
         self.check(self.lib.mb2_profile_read(self.h, int(stage), C.byref(ms), C.byref(cnt)))
         return float(ms.value), int(cnt.value)
 
+    def set_cell_level_offset(self, offset: int):
+        self.check(self.lib.mb2_set_cell_level_offset(self.h, int(offset)))
+
+    def cell_level(self) -> int:
+        v = C.c_int()
+        self.check(self.lib.mb2_cell_level(self.h, C.byref(v)))
+        return int(v.value)
+
     def set_lanes_per_row(self, lanes: int):
         self.check(self.lib.mb2_set_lanes_per_row(self.h, int(lanes)))
 
