@@ -282,8 +282,20 @@ struct SystemBoxes {
 	__device__ __forceinline__ Box row(uint32_t i) const { return boxes[keys[i] >> sys_shift]; }
 };
 
+// Resident 256-thread blocks per SM each pair-kernel variant is compiled for.
+// The force-only tabulated kernel is issue-bound on gather latency: 8 blocks
+// (32 registers, full occupancy) run it 6 % faster than the 40 registers it
+// takes unbounded, in spite of a few bytes of spill; the energy and
+// analytical variants need their registers, and the batched variant (box
+// per row) spills heavily at 32.
+template <bool kEnergy, bool kTerms, bool kOneBox>
+constexpr int pair_min_blocks() {
+	return !kOneBox ? 1 : (kTerms ? 3 : (kEnergy ? 5 : 8));
+}
+
 template <int G, bool kEnergy, bool kAllPeriodic, bool kTerms, class BoxSrc>
-__global__ void __launch_bounds__(256) pair_force_kernel(
+__global__ void __launch_bounds__(
+	256, pair_min_blocks<kEnergy, kTerms, std::is_same<BoxSrc, OneBox>::value>()) pair_force_kernel(
 	const float4* __restrict__ sorted_pos, const uint32_t* __restrict__ nbr,
 	const uint32_t* __restrict__ row_len, uint32_t n, uint32_t cap, int T,
 	const PairTableRef* __restrict__ refs_g, const float* __restrict__ force_g,

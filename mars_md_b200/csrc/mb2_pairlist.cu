@@ -187,8 +187,12 @@ struct RowWriter {
 // bounding box) walks each particle's own pruned stencil instead. Each row
 // keeps candidate order (runs of consecutive sorted j), which keeps the force
 // kernel's gathers local.
+// Six resident blocks per SM (40 registers): the walk is issue-bound with
+// fixed-latency dependency stalls, and the extra warps hide them; on the
+// 2,097,152-bead workload this builds 9 % faster than the 48 registers it
+// takes unbounded (8 blocks at 32 registers spill more and gain less).
 template <bool kExcl>
-__global__ void __launch_bounds__(256) build_walk_kernel(
+__global__ void __launch_bounds__(256, 6) build_walk_kernel(
 	const float4* __restrict__ sorted_pos, const uint32_t* __restrict__ keys,
 	const uint32_t* __restrict__ s2o, const uint32_t* __restrict__ begin,
 	const uint32_t* __restrict__ end, const StencilEntry* __restrict__ stencil_g, int ns,
