@@ -297,6 +297,15 @@ void build(mb2_context* ctx, const float4* pos, const int* type_ids, uint32_t n,
 	}
 	wg.lim = g.lim;
 	wg.rc2 = rc2;
+	for (int a = 0; a < 3; ++a) {
+		// Morton coordinate q = trunc((x - bmin) / range * 1023) on 0..1023, a cell
+		// of level m spanning 2^(10-m) of them; the margin covers the rounding of
+		// that mapping (a few ulp of the coordinates) with room to spare.
+		const double range = std::max(static_cast<double>(bmax[a]) - bmin[a], 1e-6);
+		wg.dom_lo[a] = bmin[a];
+		wg.cell_w[a] = static_cast<float>(std::ldexp(1.0, 10 - g.m) * range / 1023.0);
+		wg.eps[a] = static_cast<float>(1e-5 * (std::fabs(static_cast<double>(bmin[a])) + range) + 1e-6);
+	}
 	fast_test_band(ctx->box, rc_list, &wg.fast_lo, &wg.fast_hi);
 	ctx->row_len.ensure(n);
 	ctx->stats.ensure(2);

@@ -142,6 +142,9 @@ struct WalkGrid {
 	float lim;
 	float rc2;                 // pairlist cutoff squared, as the reference rounds it
 	float fast_lo, fast_hi;    // d^2 band that needs the exact test
+	// Real-space extent of cell c on each axis: [lo + c w - eps, lo + (c+1) w + eps)
+	// (Morton domain origin, cell width, rounding margin of the Morton mapping).
+	float dom_lo[3], cell_w[3], eps[3];
 };
 // Cell level m in [m_lo, m_hi] minimising candidates plus per-cell cost; the
 // widths assume the 10-bit Morton scale (conservative for coarser scales).

@@ -159,6 +159,33 @@ __device__ __forceinline__ int warp_min(int v) {
 	for (int o = 16; o > 0; o >>= 1) v = min(v, __shfl_xor_sync(0xFFFFFFFFu, v, o));
 	return v;
 }
+__device__ __forceinline__ float warp_minf(float v) {
+#pragma unroll
+	for (int o = 16; o > 0; o >>= 1) v = fminf(v, __shfl_xor_sync(0xFFFFFFFFu, v, o));
+	return v;
+}
+__device__ __forceinline__ float warp_maxf(float v) {
+#pragma unroll
+	for (int o = 16; o > 0; o >>= 1) v = fmaxf(v, __shfl_xor_sync(0xFFFFFFFFu, v, o));
+	return v;
+}
+
+// Distance along one axis from the group's coordinate range [glo, ghi] to
+// cell nx (shifted by sh, the periodic image offset): the cell's real extent
+// with the Morton rounding margin; on a periodic axis the edge cells also hold
+// particles that lie outside the box (their Morton coordinate clamps), so
+// they extend outwards without bound.
+__device__ __forceinline__ float cell_gap(const WalkGrid& wg, int ax, int nx, int cells,
+										  bool periodic, float sh, float glo, float ghi) {
+	float lo = wg.dom_lo[ax] + static_cast<float>(nx) * wg.cell_w[ax] + sh - wg.eps[ax];
+	float hi = wg.dom_lo[ax] + static_cast<float>(nx + 1) * wg.cell_w[ax] + sh + wg.eps[ax];
+	if (periodic) {
+		if (nx == 0) lo = -INFINITY;
+		if (nx == cells - 1) hi = INFINITY;
+	}
+	return fmaxf(0.0f, fmaxf(lo - ghi, glo - hi));
+}
+
 __device__ __forceinline__ int warp_max(int v) {
 #pragma unroll
 	for (int o = 16; o > 0; o >>= 1) v = max(v, __shfl_xor_sync(0xFFFFFFFFu, v, o));
@@ -180,19 +207,20 @@ struct RowWriter {
 
 // One warp owns a group of 32 consecutive sorted particles, lane = particle.
 // The group's cells are Morton-adjacent; the warp walks, in lockstep, every
-// cell within rc of the group's cell bounding box, loading each candidate
+// cell whose real extent lies within rc of the group's coordinate range (on
+// the cell index box of the group widened by the stencil radius), loading each candidate
 // once for all 32 lanes (a broadcast). Cells before the group's first cell in
 // Morton order hold only earlier particles and are skipped without loading
 // their ranges. A group whose cells straddle a Morton discontinuity (wide
 // bounding box) walks each particle's own pruned stencil instead. Each row
 // keeps candidate order (runs of consecutive sorted j), which keeps the force
 // kernel's gathers local.
-// Six resident blocks per SM (40 registers): the walk is issue-bound with
-// fixed-latency dependency stalls, and the extra warps hide them; on the
-// 2,097,152-bead workload this builds 9 % faster than the 48 registers it
-// takes unbounded (8 blocks at 32 registers spill more and gain less).
+// Seven resident blocks per SM (32 registers, a little spill): the walk is
+// bound by the latency of its dependent loads (cell ranges, then candidates)
+// and more warps hide it. Measured on the 2,097,152-bead workload: 9.1 ms per
+// build at 7 blocks, 9.4 at 6 (40 registers) and at 5 (48 registers).
 template <bool kExcl>
-__global__ void __launch_bounds__(256, 6) build_walk_kernel(
+__global__ void __launch_bounds__(256, 7) build_walk_kernel(
 	const float4* __restrict__ sorted_pos, const uint32_t* __restrict__ keys,
 	const uint32_t* __restrict__ s2o, const uint32_t* __restrict__ begin,
 	const uint32_t* __restrict__ end, const StencilEntry* __restrict__ stencil_g, int ns,
@@ -236,6 +264,11 @@ __global__ void __launch_bounds__(256, 6) build_walk_kernel(
 	const int y0 = warp_min(valid ? cy : INT_MAX), y1 = warp_max(valid ? cy : INT_MIN);
 	const int z0 = warp_min(valid ? cz : INT_MAX), z1 = warp_max(valid ? cz : INT_MIN);
 	const bool coherent = (x1 - x0) <= wg.emax && (y1 - y0) <= wg.emax && (z1 - z0) <= wg.emax;
+	// The group's coordinate range: cells are pruned by their real distance to
+	// it, which is tighter than the cell-index gap.
+	const float gxlo = warp_minf(valid ? pi.x : INFINITY), gxhi = warp_maxf(valid ? pi.x : -INFINITY);
+	const float gylo = warp_minf(valid ? pi.y : INFINITY), gyhi = warp_maxf(valid ? pi.y : -INFINITY);
+	const float gzlo = warp_minf(valid ? pi.z : INFINITY), gzhi = warp_maxf(valid ? pi.z : -INFINITY);
 
 	if (coherent) {
 		const int lo[3] = {x0, y0, z0}, hi[3] = {x1, y1, z1};
@@ -251,14 +284,13 @@ __global__ void __launch_bounds__(256, 6) build_walk_kernel(
 			int nx = ux;
 			float shx = 0.0f, gx = 0.0f;
 			if (!full[0]) {
-				const int gc = ux < x0 ? x0 - ux - 1 : (ux > x1 ? ux - x1 - 1 : 0);
-				gx = static_cast<float>(gc) * wg.wmin[0];
 				if (box.periodic[0]) {
 					if (ux < 0) { nx = ux + cells; shx = -box.size[0]; }
 					else if (ux >= cells) { nx = ux - cells; shx = box.size[0]; }
 				} else if (ux < 0 || ux >= cells) {
 					continue;
 				}
+				gx = cell_gap(wg, 0, nx, cells, box.periodic[0], shx, gxlo, gxhi);
 			}
 			const float gx2 = gx * gx;
 			if (gx2 > wg.lim) continue;
@@ -267,14 +299,13 @@ __global__ void __launch_bounds__(256, 6) build_walk_kernel(
 				int ny = uy;
 				float shy = 0.0f, gy = 0.0f;
 				if (!full[1]) {
-					const int gc = uy < y0 ? y0 - uy - 1 : (uy > y1 ? uy - y1 - 1 : 0);
-					gy = static_cast<float>(gc) * wg.wmin[1];
 					if (box.periodic[1]) {
 						if (uy < 0) { ny = uy + cells; shy = -box.size[1]; }
 						else if (uy >= cells) { ny = uy - cells; shy = box.size[1]; }
 					} else if (uy < 0 || uy >= cells) {
 						continue;
 					}
+					gy = cell_gap(wg, 1, ny, cells, box.periodic[1], shy, gylo, gyhi);
 				}
 				const float gxy2 = gx2 + gy * gy;
 				if (gxy2 > wg.lim) continue;
@@ -283,14 +314,13 @@ __global__ void __launch_bounds__(256, 6) build_walk_kernel(
 					int nz = uz;
 					float shz = 0.0f, gz = 0.0f;
 					if (!full[2]) {
-						const int gc = uz < z0 ? z0 - uz - 1 : (uz > z1 ? uz - z1 - 1 : 0);
-						gz = static_cast<float>(gc) * wg.wmin[2];
 						if (box.periodic[2]) {
 							if (uz < 0) { nz = uz + cells; shz = -box.size[2]; }
 							else if (uz >= cells) { nz = uz - cells; shz = box.size[2]; }
 						} else if (uz < 0 || uz >= cells) {
 							continue;
 						}
+						gz = cell_gap(wg, 2, nz, cells, box.periodic[2], shz, gzlo, gzhi);
 					}
 					if (gxy2 + gz * gz > wg.lim) continue;
 					const uint32_t nc = sxy | split_tab[nz];
