@@ -186,6 +186,17 @@ __device__ __forceinline__ float cell_gap(const WalkGrid& wg, int ax, int nx, in
 	return fmaxf(0.0f, fmaxf(lo - ghi, glo - hi));
 }
 
+// Cells a warp buffers before walking them (32 tested at a time: at most
+// 31 left over plus 32 new).
+constexpr uint32_t kCellBuf = 64;
+
+// Periodic image offset of a buffered cell on axis ax: code bits 2ax..2ax+1
+// hold 1 (-size) or 2 (+size).
+__device__ __forceinline__ float image_shift(uint32_t code, int ax, const Box& box) {
+	const uint32_t c = (code >> (2 * ax)) & 3u;
+	return c == 1u ? -box.size[ax] : (c == 2u ? box.size[ax] : 0.0f);
+}
+
 __device__ __forceinline__ int warp_max(int v) {
 #pragma unroll
 	for (int o = 16; o > 0; o >>= 1) v = max(v, __shfl_xor_sync(0xFFFFFFFFu, v, o));
@@ -207,9 +218,9 @@ struct RowWriter {
 
 // One warp owns a group of 32 consecutive sorted particles, lane = particle.
 // The group's cells are Morton-adjacent; the warp walks, in lockstep, every
-// cell whose real extent lies within rc of the group's coordinate range (on
-// the cell index box of the group widened by the stencil radius), loading each candidate
-// once for all 32 lanes (a broadcast). Cells before the group's first cell in
+// cell whose real extent lies within rc of the group's coordinate range (found
+// by the lanes in parallel over the group's cell box widened by the stencil
+// radius), loading each candidate once for all 32 lanes (a broadcast). Cells before the group's first cell in
 // Morton order hold only earlier particles and are skipped without loading
 // their ranges. A group whose cells straddle a Morton discontinuity (wide
 // bounding box) walks each particle's own pruned stencil instead. Each row
@@ -217,8 +228,8 @@ struct RowWriter {
 // kernel's gathers local.
 // Seven resident blocks per SM (32 registers, a little spill): the walk is
 // bound by the latency of its dependent loads (cell ranges, then candidates)
-// and more warps hide it. Measured on the 2,097,152-bead workload: 9.1 ms per
-// build at 7 blocks, 9.4 at 6 (40 registers) and at 5 (48 registers).
+// and more warps hide it. Measured on the 2,097,152-bead workload: 7.1 ms per
+// build at 7 blocks, 7.7 at 6 (40 registers), 7.9 at 5 (48 registers).
 template <bool kExcl>
 __global__ void __launch_bounds__(256, 7) build_walk_kernel(
 	const float4* __restrict__ sorted_pos, const uint32_t* __restrict__ keys,
@@ -228,6 +239,7 @@ __global__ void __launch_bounds__(256, 7) build_walk_kernel(
 	int hshift, uint32_t* __restrict__ row_len, unsigned long long* __restrict__ stats) {
 	extern __shared__ int4 stencil[];
 	__shared__ uint32_t split_tab[256];
+	__shared__ uint4 cell_buf[8 * kCellBuf];  // per warp: kept cells (jlo, end, image code)
 	const int cells = 1 << wg.m;
 	for (int k = threadIdx.x; k < ns; k += blockDim.x) {
 		const StencilEntry e = stencil_g[k];
@@ -271,84 +283,100 @@ __global__ void __launch_bounds__(256, 7) build_walk_kernel(
 	const float gzlo = warp_minf(valid ? pi.z : INFINITY), gzhi = warp_maxf(valid ? pi.z : -INFINITY);
 
 	if (coherent) {
+		// Candidate cells: the group's cell box widened by the stencil radius (or
+		// every cell on an axis the stencil spans). The lanes test 32 of them at
+		// a time in parallel, each against the group's coordinate range, and
+		// append the kept ones, in box order, to the warp's buffer; the warp
+		// then walks the buffered cells' candidates together.
 		const int lo[3] = {x0, y0, z0}, hi[3] = {x1, y1, z1};
-		int from[3], to[3];
+		const float glo[3] = {gxlo, gylo, gzlo}, ghi[3] = {gxhi, gyhi, gzhi};
+		int from[3], span[3];
 		bool full[3];
 #pragma unroll
 		for (int ax = 0; ax < 3; ++ax) {
 			full[ax] = box.periodic[ax] && (hi[ax] - lo[ax] + 2 * wg.radius[ax] + 1 >= cells);
 			from[ax] = full[ax] ? 0 : lo[ax] - wg.radius[ax];
-			to[ax] = full[ax] ? cells - 1 : hi[ax] + wg.radius[ax];
+			span[ax] = full[ax] ? cells : hi[ax] - lo[ax] + 2 * wg.radius[ax] + 1;
 		}
-		for (int ux = from[0]; ux <= to[0]; ++ux) {
-			int nx = ux;
-			float shx = 0.0f, gx = 0.0f;
-			if (!full[0]) {
-				if (box.periodic[0]) {
-					if (ux < 0) { nx = ux + cells; shx = -box.size[0]; }
-					else if (ux >= cells) { nx = ux - cells; shx = box.size[0]; }
-				} else if (ux < 0 || ux >= cells) {
-					continue;
+		const uint32_t total = static_cast<uint32_t>(span[0] * span[1] * span[2]);
+		const int lane = static_cast<int>(threadIdx.x & 31u);
+		uint4* buf = cell_buf + (threadIdx.x >> 5) * kCellBuf;
+		uint32_t count = 0;
+		auto walk_buffered = [&](uint32_t m) {
+			for (uint32_t k = 0; k < m; ++k) {
+				const uint4 cb = buf[k];
+				// Particle coordinates moved into the candidate cell's image.
+				const float qx = pi.x - image_shift(cb.z, 0, box);
+				const float qy = pi.y - image_shift(cb.z, 1, box);
+				const float qz = pi.z - image_shift(cb.z, 2, box);
+				for (uint32_t j = cb.x; j < cb.y; ++j) {
+					const float4 pj = sorted_pos[j];
+					if (!valid || j <= i) continue;
+					float dx = pj.x - qx, dy = pj.y - qy, dz = pj.z - qz;
+					if (full[0]) dx -= box.size[0] * rintf(dx * box.inv[0]);
+					if (full[1]) dy -= box.size[1] * rintf(dy * box.inv[1]);
+					if (full[2]) dz -= box.size[2] * rintf(dz * box.inv[2]);
+					const float d2 = dx * dx + dy * dy + dz * dz;
+					bool hit = d2 < wg.fast_lo;
+					if (!hit && d2 <= wg.fast_hi) hit = exact_hit(box, pi, pj, wg.rc2);
+					if (hit) {
+						const int bj = static_cast<int>(s2o[j]);
+						if (kExcl && is_excluded(ex, bj, row_b, row_e, body)) continue;
+						row.append(j | (bj < a ? kOrientBit : 0u));
+					}
 				}
-				gx = cell_gap(wg, 0, nx, cells, box.periodic[0], shx, gxlo, gxhi);
 			}
-			const float gx2 = gx * gx;
-			if (gx2 > wg.lim) continue;
-			const uint32_t sx = split_tab[nx] << 2;
-			for (int uy = from[1]; uy <= to[1]; ++uy) {
-				int ny = uy;
-				float shy = 0.0f, gy = 0.0f;
-				if (!full[1]) {
-					if (box.periodic[1]) {
-						if (uy < 0) { ny = uy + cells; shy = -box.size[1]; }
-						else if (uy >= cells) { ny = uy - cells; shy = box.size[1]; }
-					} else if (uy < 0 || uy >= cells) {
-						continue;
-					}
-					gy = cell_gap(wg, 1, ny, cells, box.periodic[1], shy, gylo, gyhi);
-				}
-				const float gxy2 = gx2 + gy * gy;
-				if (gxy2 > wg.lim) continue;
-				const uint32_t sxy = sx | (split_tab[ny] << 1);
-				for (int uz = from[2]; uz <= to[2]; ++uz) {
-					int nz = uz;
-					float shz = 0.0f, gz = 0.0f;
-					if (!full[2]) {
-						if (box.periodic[2]) {
-							if (uz < 0) { nz = uz + cells; shz = -box.size[2]; }
-							else if (uz >= cells) { nz = uz - cells; shz = box.size[2]; }
-						} else if (uz < 0 || uz >= cells) {
-							continue;
+		};
+		for (uint32_t base = 0; base < total; base += 32u) {
+			const uint32_t idx = base + static_cast<uint32_t>(lane);
+			bool keep = false;
+			uint4 rec = make_uint4(0u, 0u, 0u, 0u);
+			if (idx < total) {
+				const uint32_t iz = idx % static_cast<uint32_t>(span[2]);
+				const uint32_t t = idx / static_cast<uint32_t>(span[2]);
+				const int u[3] = {from[0] + static_cast<int>(t / static_cast<uint32_t>(span[1])),
+								  from[1] + static_cast<int>(t % static_cast<uint32_t>(span[1])),
+								  from[2] + static_cast<int>(iz)};
+				bool in_range = true;
+				float g2 = 0.0f;
+				uint32_t code = 0, nc = 0;
+#pragma unroll
+				for (int ax = 0; ax < 3; ++ax) {
+					int nn = u[ax];
+					float sh = 0.0f;
+					if (!full[ax]) {
+						if (box.periodic[ax]) {
+							if (nn < 0) { nn += cells; sh = -box.size[ax]; code |= 1u << (2 * ax); }
+							else if (nn >= cells) { nn -= cells; sh = box.size[ax]; code |= 2u << (2 * ax); }
+						} else if (nn < 0 || nn >= cells) {
+							in_range = false;
+							nn = 0;
 						}
-						gz = cell_gap(wg, 2, nz, cells, box.periodic[2], shz, gzlo, gzhi);
+						const float g = cell_gap(wg, ax, nn, cells, box.periodic[ax], sh, glo[ax], ghi[ax]);
+						g2 += g * g;
 					}
-					if (gxy2 + gz * gz > wg.lim) continue;
-					const uint32_t nc = sxy | split_tab[nz];
-					if (nc < c_first) continue;
+					nc |= split_tab[nn] << (2 - ax);
+				}
+				if (in_range && g2 <= wg.lim && nc >= c_first) {
 					const uint32_t b = begin[nc], e = end[nc];
 					const uint32_t jlo = b > i_first + 1u ? b : i_first + 1u;
-					if (jlo >= e) continue;
-					// Particle coordinates moved into the candidate cell's image.
-					const float qx = pi.x - shx, qy = pi.y - shy, qz = pi.z - shz;
-					for (uint32_t j = jlo; j < e; ++j) {
-						const float4 pj = sorted_pos[j];
-						if (!valid || j <= i) continue;
-						float dx = pj.x - qx, dy = pj.y - qy, dz = pj.z - qz;
-						if (full[0]) dx -= box.size[0] * rintf(dx * box.inv[0]);
-						if (full[1]) dy -= box.size[1] * rintf(dy * box.inv[1]);
-						if (full[2]) dz -= box.size[2] * rintf(dz * box.inv[2]);
-						const float d2 = dx * dx + dy * dy + dz * dz;
-						bool hit = d2 < wg.fast_lo;
-						if (!hit && d2 <= wg.fast_hi) hit = exact_hit(box, pi, pj, wg.rc2);
-						if (hit) {
-							const int bj = static_cast<int>(s2o[j]);
-							if (kExcl && is_excluded(ex, bj, row_b, row_e, body)) continue;
-							row.append(j | (bj < a ? kOrientBit : 0u));
-						}
+					if (jlo < e) {
+						keep = true;
+						rec = make_uint4(jlo, e, code, 0u);
 					}
 				}
 			}
+			const uint32_t kept = __ballot_sync(0xFFFFFFFFu, keep);
+			if (keep) buf[count + __popc(kept & ((1u << lane) - 1u))] = rec;
+			count += static_cast<uint32_t>(__popc(kept));
+			__syncwarp();
+			if (count >= 32u) {
+				walk_buffered(count);
+				count = 0;
+				__syncwarp();
+			}
 		}
+		walk_buffered(count);
 	} else if (valid) {
 		// Wide group: each lane walks its own pruned cell stencil, exact test.
 		for (int k = 0; k < ns; ++k) {
