@@ -28,7 +28,8 @@ struct mb2_context {
 	Scratch scratch;
 
 	// Z-order state of the last build
-	DevBuf<uint32_t> keys, s2o, inv, row_len, row_off, nbr, cell_begin, cell_end;
+	DevBuf<uint32_t> keys, s2o, inv, row_len, row_off, nbr, cell_begin, cell_end, row_far;
+	float last_cutoff = 0.0f;  // interaction cutoff of the last pair-force call
 	DevBuf<float4> sorted_pos, ref_pos, force_sorted;
 	DevBuf<StencilEntry> stencil;
 	DevBuf<float> bbox;  // 6 floats, ordered-int min/max
@@ -297,6 +298,17 @@ void build(mb2_context* ctx, const float4* pos, const int* type_ids, uint32_t n,
 	}
 	wg.lim = g.lim;
 	wg.rc2 = rc2;
+	// Rows put the pairs that are likely to come within the interaction cutoff
+	// before the next rebuild first (d <= cutoff + 25 % of the skin at build
+	// time) and the rest after them: in a row's tail the whole warp's pairs are
+	// beyond the cutoff for most iterations of the force kernel, which then
+	// skips the force part. The split moves no pair in or out of the list.
+	// Measured on the 2,097,152-bead workload (fused step, rebuild every 20
+	// steps): 1.94 ms without the split; 1.87 ms at 25 % of the skin, 1.89 at
+	// 10 % and at 40 %, 1.92 at 70 %.
+	const float cut = ctx->last_cutoff;
+	const float split = (cut > 0.0f && cut < rc_list) ? cut + 0.25f * (rc_list - cut) : 0.0f;
+	wg.split2 = split > 0.0f ? split * split : INFINITY;
 	for (int a = 0; a < 3; ++a) {
 		// Morton coordinate q = trunc((x - bmin) / range * 1023) on 0..1023, a cell
 		// of level m spanning 2^(10-m) of them; the margin covers the rounding of
@@ -308,12 +320,14 @@ void build(mb2_context* ctx, const float4* pos, const int* type_ids, uint32_t n,
 	}
 	fast_test_band(ctx->box, rc_list, &wg.fast_lo, &wg.fast_hi);
 	ctx->row_len.ensure(n);
+	ctx->row_far.ensure(n);
 	ctx->stats.ensure(2);
 	auto walk = [&](uint32_t cap) {
 		const int hshift = __builtin_ctz(32 / ctx->lanes);
 		build_walk(ctx->sorted_pos.ptr, ctx->keys.ptr, ctx->s2o.ptr, ctx->cell_begin.ptr,
 				   ctx->cell_end.ptr, ctx->stencil.ptr, g.num_stencil, wg, n, ctx->box, ctx->excl,
-				   ctx->nbr.ptr, cap, hshift, ctx->row_len.ptr, ctx->stats.ptr, st);
+				   ctx->nbr.ptr, cap, hshift, ctx->row_len.ptr, ctx->row_far.ptr, ctx->stats.ptr,
+				   st);
 		MB2_CUDA(cudaMemcpyAsync(ctx->pinned, ctx->stats.ptr, 2 * sizeof(uint64_t),
 								 cudaMemcpyDeviceToHost, st));
 		MB2_CUDA(cudaStreamSynchronize(st));
@@ -352,6 +366,9 @@ void build(mb2_context* ctx, const float4* pos, const int* type_ids, uint32_t n,
 		size_list(stats.second);
 		stats = walk(ctx->cap);
 	}
+	if (split > 0.0f)
+		join_far(ctx->nbr.ptr, ctx->row_len.ptr, ctx->row_far.ptr, n, ctx->cap,
+				 __builtin_ctz(32 / ctx->lanes), st);
 	// Snapshot for the skin check (ZOrderPairlist.cpp:172-173).
 	ctx->ref_pos.ensure(n);
 	MB2_CUDA(cudaMemcpyAsync(ctx->ref_pos.ptr, pos, static_cast<size_t>(n) * sizeof(float4),
@@ -380,6 +397,7 @@ void pair_kernel(mb2_context* ctx, uint32_t n, float cutoff, int get_energy, cud
 			"mb2_pair_forces: the tags carry analytical terms; call mb2_set_pair_terms");
 	ctx->force_sorted.ensure(n);
 	MB2_CUDA(cudaMemsetAsync(ctx->force_sorted.ptr, 0, static_cast<size_t>(n) * sizeof(float4), st));
+	ctx->last_cutoff = cutoff;
 	const float cutoff_sq = cutoff > 0.0f ? cutoff * cutoff : 0.0f;
 	StageScope scope(ctx, MB2_STAGE_PAIR_FORCE, st);
 	pair_forces(ctx->sorted_pos.ptr, ctx->nbr.ptr, ctx->row_len.ptr, n, ctx->cap, ctx->lanes, ctx->pt,
@@ -1092,6 +1110,7 @@ int mb2_step(mb2_context* ctx, float* pos4, float* force_energy4, const int* typ
 		const float skin = prm->pairlist_cutoff - prm->cutoff;
 		if (rebuild && prm->rebuild_period != 0 && ctx->built && ctx->built_n == n && skin > 0.0f)
 			rebuild = max_disp(ctx, pos, n, st) > skin * 0.5f;
+		ctx->last_cutoff = prm->cutoff;
 		if (rebuild)
 			build(ctx, pos, type_ids, n, prm->pairlist_cutoff, st);  // packs sorted_pos
 		else if (n)

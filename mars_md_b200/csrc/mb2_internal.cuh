@@ -142,6 +142,7 @@ struct WalkGrid {
 	float lim;
 	float rc2;                 // pairlist cutoff squared, as the reference rounds it
 	float fast_lo, fast_hi;    // d^2 band that needs the exact test
+	float split2;              // entries with d^2 above it go to the row's far segment
 	// Real-space extent of cell c on each axis: [lo + c w - eps, lo + (c+1) w + eps)
 	// (Morton domain origin, cell width, rounding margin of the Morton mapping).
 	float dom_lo[3], cell_w[3], eps[3];
@@ -159,7 +160,10 @@ void build_walk(const float4* sorted_pos, const uint32_t* keys, const uint32_t* 
 				const uint32_t* begin, const uint32_t* end, const StencilEntry* stencil,
 				int num_stencil, const WalkGrid& wg, uint32_t n, const Box& box,
 				const Exclusions& ex, uint32_t* nbr, uint32_t cap, int hshift, uint32_t* row_len,
-				unsigned long long* stats, cudaStream_t st);
+				uint32_t* row_far, unsigned long long* stats, cudaStream_t st);
+// After a storing walk: each row's far entries moved to follow its near ones.
+void join_far(uint32_t* nbr, const uint32_t* row_len, const uint32_t* row_far, uint32_t n,
+			  uint32_t cap, int hshift, cudaStream_t st);
 void export_pairs(const uint32_t* nbr, const uint32_t* row_len, const uint32_t* row_off,
 				  const uint32_t* s2o, uint32_t n, uint32_t cap, int hshift, int2* out,
 				  cudaStream_t st);

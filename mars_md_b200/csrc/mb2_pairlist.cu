@@ -203,17 +203,28 @@ __device__ __forceinline__ int warp_max(int v) {
 	return v;
 }
 
-// Appends one lane's row of the sliced-ELL list; entries past cap are only
-// counted (the host then grows the list and walks again).
+// Appends one lane's row of the sliced-ELL list: near entries from the front,
+// far entries (beyond the split radius) from the back of the row's cap slots;
+// join_far_kernel then moves the far ones to follow the near ones. Entries
+// past cap are only counted (the host then grows the list and walks again).
 struct RowWriter {
 	uint32_t* base;  // &nbr[entry 0 of this row]
-	uint32_t len;
+	uint32_t len;    // near entries
+	uint32_t far;    // far entries
 	uint32_t cap;
 	int h;           // slice height: stride between a row's entries
 	__device__ __forceinline__ void append(uint32_t entry) {
-		if (len < cap) base[static_cast<size_t>(len) * h] = entry;
+		if (len + far < cap) base[static_cast<size_t>(len) * h] = entry;
 		++len;
 	}
+	// Near entry to the front, far entry to the back, without a branch.
+	__device__ __forceinline__ void put(uint32_t entry, bool near) {
+		const uint32_t slot = near ? len : cap - 1u - far;
+		if (len + far < cap) base[static_cast<size_t>(slot) * h] = entry;
+		len += near ? 1u : 0u;
+		far += near ? 0u : 1u;
+	}
+	__device__ __forceinline__ uint32_t total() const { return len + far; }
 };
 
 // One warp owns a group of 32 consecutive sorted particles, lane = particle.
@@ -236,7 +247,8 @@ __global__ void __launch_bounds__(256, 7) build_walk_kernel(
 	const uint32_t* __restrict__ s2o, const uint32_t* __restrict__ begin,
 	const uint32_t* __restrict__ end, const StencilEntry* __restrict__ stencil_g, int ns,
 	WalkGrid wg, uint32_t n, Box box, Exclusions ex, uint32_t* __restrict__ nbr, uint32_t cap,
-	int hshift, uint32_t* __restrict__ row_len, unsigned long long* __restrict__ stats) {
+	int hshift, uint32_t* __restrict__ row_len, uint32_t* __restrict__ row_far,
+	unsigned long long* __restrict__ stats) {
 	extern __shared__ int4 stencil[];
 	__shared__ uint32_t split_tab[256];
 	__shared__ uint4 cell_buf[8 * kCellBuf];  // per warp: kept cells (jlo, end, image code)
@@ -268,7 +280,7 @@ __global__ void __launch_bounds__(256, 7) build_walk_kernel(
 		body = ex.rigid_body_id ? ex.rigid_body_id[a] : -1;
 	}
 	RowWriter row{nbr + (static_cast<size_t>(i >> hshift) * cap << hshift) + (i & (h - 1)), 0u,
-				  cap, h};
+				  0u, cap, h};
 	const uint32_t c_first = keys[i_first] >> wg.shift;
 
 	// Cell bounding box of the group (valid lanes only).
@@ -322,7 +334,7 @@ __global__ void __launch_bounds__(256, 7) build_walk_kernel(
 					if (hit) {
 						const int bj = static_cast<int>(s2o[j]);
 						if (kExcl && is_excluded(ex, bj, row_b, row_e, body)) continue;
-						row.append(j | (bj < a ? kOrientBit : 0u));
+						row.put(j | (bj < a ? kOrientBit : 0u), d2 <= wg.split2);
 					}
 				}
 			}
@@ -401,10 +413,13 @@ __global__ void __launch_bounds__(256, 7) build_walk_kernel(
 			}
 		}
 	}
-	if (valid) row_len[i] = row.len;
+	if (valid) {
+		row_len[i] = row.total();
+		row_far[i] = row.far;
+	}
 	// stats[0] = total pairs, stats[1] = longest row
-	unsigned long long tot = valid ? row.len : 0u;
-	int mx = valid ? static_cast<int>(min(row.len, 0x7FFFFFFFu)) : 0;
+	unsigned long long tot = valid ? row.total() : 0u;
+	int mx = valid ? static_cast<int>(min(row.total(), 0x7FFFFFFFu)) : 0;
 #pragma unroll
 	for (int o = 16; o > 0; o >>= 1) {
 		tot += __shfl_xor_sync(0xFFFFFFFFu, tot, o);
@@ -431,6 +446,40 @@ __global__ void __launch_bounds__(256) export_kernel(const uint32_t* __restrict_
 	for (uint32_t k = 0; k < len; ++k) {
 		const int b = static_cast<int>(s2o[base[static_cast<size_t>(k) * h] & ~kOrientBit]);
 		out[off + k] = make_int2(a < b ? a : b, a < b ? b : a);
+	}
+}
+
+// Moves each row's far entries (stored backwards from the end of its cap
+// slots) to follow its near entries, so that a row is one contiguous run:
+// near entries in candidate order, then the far ones. One warp per slice of
+// H rows: lane l copies entries l / H, l / H + 32 / H, ... of row l % H, so
+// each load and store instruction touches neighbouring words. Destinations
+// precede sources (near + far <= cap) and every batch is loaded before it is
+// stored, so the in-place copy is safe.
+__global__ void __launch_bounds__(256) join_far_kernel(uint32_t* __restrict__ nbr,
+													   const uint32_t* __restrict__ row_len,
+													   const uint32_t* __restrict__ row_far,
+													   uint32_t n, uint32_t cap, int hshift) {
+	const uint32_t slice = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+	const uint32_t lane = threadIdx.x & 31u;
+	const uint32_t h = 1u << hshift;
+	const uint32_t slices = (n + h - 1u) >> hshift;
+	if (slice >= slices) return;  // whole warp
+	const uint32_t r = lane & (h - 1u), kk = lane >> hshift, step = 32u >> hshift;
+	const uint32_t i = (slice << hshift) + r;
+	const uint32_t far = i < n ? row_far[i] : 0u;
+	const uint32_t near = i < n ? row_len[i] - far : 0u;
+	uint32_t most = far;
+#pragma unroll
+	for (int o = 16; o > 0; o >>= 1) most = max(most, __shfl_xor_sync(0xFFFFFFFFu, most, o));
+	uint32_t* base = nbr + static_cast<size_t>(slice) * cap * h + r;
+	for (uint32_t k0 = 0; k0 < most; k0 += step) {
+		const uint32_t k = k0 + kk;
+		uint32_t v = 0u;
+		if (k < far) v = base[static_cast<size_t>(cap - far + k) * h];
+		__syncwarp();
+		if (k < far) base[static_cast<size_t>(near + k) * h] = v;
+		__syncwarp();
 	}
 }
 
@@ -490,7 +539,7 @@ void build_walk(const float4* sorted_pos, const uint32_t* keys, const uint32_t* 
 				const uint32_t* begin, const uint32_t* end, const StencilEntry* stencil,
 				int num_stencil, const WalkGrid& wg, uint32_t n, const Box& box,
 				const Exclusions& ex, uint32_t* nbr, uint32_t cap, int hshift, uint32_t* row_len,
-				unsigned long long* stats, cudaStream_t st) {
+				uint32_t* row_far, unsigned long long* stats, cudaStream_t st) {
 	MB2_CUDA(cudaMemsetAsync(stats, 0, 2 * sizeof(unsigned long long), st));
 	if (n == 0) return;
 	const size_t smem = static_cast<size_t>(num_stencil) * sizeof(int4);
@@ -501,7 +550,15 @@ void build_walk(const float4* sorted_pos, const uint32_t* keys, const uint32_t* 
 									  static_cast<int>(smem)));
 	MB2_LAUNCH kern<<<(n + 255) / 256, 256, smem, st>>>(sorted_pos, keys, s2o, begin, end,
 														 stencil, num_stencil, wg, n, box, ex,
-														 nbr, cap, hshift, row_len, stats);
+														 nbr, cap, hshift, row_len, row_far, stats);
+}
+
+void join_far(uint32_t* nbr, const uint32_t* row_len, const uint32_t* row_far, uint32_t n,
+			  uint32_t cap, int hshift, cudaStream_t st) {
+	if (n == 0) return;
+	const uint32_t slices = (n + (1u << hshift) - 1u) >> hshift;
+	const uint32_t blocks = (slices + 7u) / 8u;  // 8 warps (slices) per block
+	MB2_LAUNCH join_far_kernel<<<blocks, 256, 0, st>>>(nbr, row_len, row_far, n, cap, hshift);
 }
 
 void export_pairs(const uint32_t* nbr, const uint32_t* row_len, const uint32_t* row_off,
