@@ -14,7 +14,7 @@
 // the reference rounds it, and 0 for the last bin (the reference's
 // home >= size-1 branch); bin_energy[k] = (U[k], U[k+1] - U[k]). A lookup is
 // then w = (x - start) * step_inv, home = clamp(floor(w), 0, size-1) and one
-// shared-memory load -- bit-identical to the reference's branches.
+// load (through L1) -- bit-identical to the reference's branches.
 //
 // Layout: G lanes own one row (sorted particle i) of the sliced-ELL half list
 // and H = 32 / G rows share a warp, so one warp load of entries k..k+G-1 of
@@ -250,25 +250,6 @@ __device__ __forceinline__ void pair_scalar(const float4& pi, const float4& pj, 
 	fe += half;
 }
 
-// Shared-memory copy of the per-type-pair table references and per-bin data.
-template <bool kEnergy>
-__device__ __forceinline__ void load_tables(int T, const PairTableRef* __restrict__ refs_g,
-											const float* __restrict__ force_g,
-											const float2* __restrict__ energy_g,
-											uint32_t total_bins, PairTableRef*& refs,
-											float*& bin_f, float2*& bin_e) {
-	extern __shared__ float4 smem4[];
-	refs = reinterpret_cast<PairTableRef*>(smem4);
-	bin_f = reinterpret_cast<float*>(refs + T * T);
-	bin_e = reinterpret_cast<float2*>(bin_f + ((total_bins + 1) & ~1u));
-	for (int k = threadIdx.x; k < T * T; k += blockDim.x) refs[k] = refs_g[k];
-	for (uint32_t k = threadIdx.x; k < total_bins; k += blockDim.x) {
-		bin_f[k] = force_g[k];
-		if (kEnergy) bin_e[k] = energy_g[k];
-	}
-	__syncthreads();
-}
-
 // Box of a row: one box for the whole list, or the box of the row's system
 // (batched replicas: system id in the top bits of the sorted key).
 struct OneBox {
@@ -303,10 +284,31 @@ __global__ void __launch_bounds__(
 	const PairTermRef* __restrict__ terms_g, PairSolvent sv, BoxSrc boxes, float cutoff_sq,
 	float4* force, double* __restrict__ ev) {
 	constexpr int H = 32 / G;
-	PairTableRef* refs;
-	float* bin_f;
-	float2* bin_e;
-	load_tables<kEnergy>(T, refs_g, force_g, energy_g, total_bins, refs, bin_f, bin_e);
+	// The per-type-pair references (T*T, 16 B each) are staged in shared
+	// memory. On the one-box path the per-bin force (and energy) tables are
+	// read through L1 (a few KB, hot in every SM's L1) instead of a copy per
+	// block: that leaves the L1 to the neighbour-position gathers, whose
+	// latency bounds this kernel (1.63 -> 1.51 ms per 2 M-bead launch; asking
+	// the driver for the largest L1 carve-out on top made it slower, 1.80 ms).
+	// The batched path (many small systems, short rows, fewer resident warps)
+	// is faster with the tables in shared memory.
+	constexpr bool kStage = !std::is_same<BoxSrc, OneBox>::value;
+	extern __shared__ float4 smem4[];
+	PairTableRef* refs = reinterpret_cast<PairTableRef*>(smem4);
+	for (int k = threadIdx.x; k < T * T; k += blockDim.x) refs[k] = refs_g[k];
+	const float* __restrict__ bin_f = force_g;
+	const float2* __restrict__ bin_e = energy_g;
+	if (kStage) {
+		float* sf = reinterpret_cast<float*>(refs + T * T);
+		float2* se = reinterpret_cast<float2*>(sf + ((total_bins + 1) & ~1u));
+		for (uint32_t k = threadIdx.x; k < total_bins; k += blockDim.x) {
+			sf[k] = force_g[k];
+			if (kEnergy) se[k] = energy_g[k];
+		}
+		bin_f = sf;
+		bin_e = se;
+	}
+	__syncthreads();
 
 	const int sub = threadIdx.x & (G - 1);  // lane within the row's group
 	const uint32_t i = blockIdx.x * (blockDim.x / G) + threadIdx.x / G;
@@ -576,12 +578,15 @@ template <int G, bool kEnergy, bool kAllPeriodic, bool kTerms, class BoxSrc>
 void launch_pair(const float4* sorted_pos, const uint32_t* nbr, const uint32_t* row_len,
 				 uint32_t n, uint32_t cap, const PairTables& t, const BoxSrc& boxes,
 				 float cutoff_sq, float4* force_sorted, double* ev, cudaStream_t st) {
-	const size_t smem = static_cast<size_t>(t.num_types * t.num_types) * sizeof(PairTableRef) +
-						static_cast<size_t>((t.total_bins + 1) & ~1u) * 4 +
-						(kEnergy ? static_cast<size_t>(t.total_bins) * 8 : 0);
 	const uint32_t rows = 256 / G;
 	const uint32_t blocks = (n + rows - 1) / rows;
 	auto kern = pair_force_kernel<G, kEnergy, kAllPeriodic, kTerms, BoxSrc>;
+	constexpr bool kStage = !std::is_same<BoxSrc, OneBox>::value;
+	const size_t smem =
+		static_cast<size_t>(t.num_types * t.num_types) * sizeof(PairTableRef) +
+		(kStage ? static_cast<size_t>((t.total_bins + 1) & ~1u) * 4 +
+					  (kEnergy ? static_cast<size_t>(t.total_bins) * 8 : 0)
+				: 0);
 	if (smem > 48 * 1024)
 		MB2_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
 									  static_cast<int>(smem)));
