@@ -249,14 +249,9 @@ __global__ void __launch_bounds__(256, 7) build_walk_kernel(
 	WalkGrid wg, uint32_t n, Box box, Exclusions ex, uint32_t* __restrict__ nbr, uint32_t cap,
 	int hshift, uint32_t* __restrict__ row_len, uint32_t* __restrict__ row_far,
 	unsigned long long* __restrict__ stats) {
-	extern __shared__ int4 stencil[];
 	__shared__ uint32_t split_tab[256];
 	__shared__ uint4 cell_buf[8 * kCellBuf];  // per warp: kept cells (jlo, end, image code)
 	const int cells = 1 << wg.m;
-	for (int k = threadIdx.x; k < ns; k += blockDim.x) {
-		const StencilEntry e = stencil_g[k];
-		stencil[k] = make_int4(e.dx, e.dy, e.dz, 0);
-	}
 	for (int k = threadIdx.x; k < cells; k += blockDim.x) split_tab[k] = split_by3(k);
 	__syncthreads();
 	const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -392,7 +387,8 @@ __global__ void __launch_bounds__(256, 7) build_walk_kernel(
 	} else if (valid) {
 		// Wide group: each lane walks its own pruned cell stencil, exact test.
 		for (int k = 0; k < ns; ++k) {
-			const int4 s = stencil[k];
+			const StencilEntry se = stencil_g[k];
+			const int4 s = make_int4(se.dx, se.dy, se.dz, 0);
 			int nx = cx + s.x, ny = cy + s.y, nz = cz + s.z;
 			if (box.periodic[0]) nx = static_cast<int>(static_cast<uint32_t>(nx + cells) & mask);
 			else if (nx < 0 || nx >= cells) continue;
@@ -542,13 +538,11 @@ void build_walk(const float4* sorted_pos, const uint32_t* keys, const uint32_t* 
 				uint32_t* row_far, unsigned long long* stats, cudaStream_t st) {
 	MB2_CUDA(cudaMemsetAsync(stats, 0, 2 * sizeof(unsigned long long), st));
 	if (n == 0) return;
-	const size_t smem = static_cast<size_t>(num_stencil) * sizeof(int4);
 	const bool excl = ex.offsets != nullptr || ex.rigid_body_id != nullptr;
 	auto kern = excl ? build_walk_kernel<true> : build_walk_kernel<false>;
-	if (smem > 48 * 1024)
-		MB2_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
-									  static_cast<int>(smem)));
-	MB2_LAUNCH kern<<<(n + 255) / 256, 256, smem, st>>>(sorted_pos, keys, s2o, begin, end,
+	// The stencil (used by the few groups that walk per particle) is read
+	// through L1, leaving shared memory to the cell buffers.
+	MB2_LAUNCH kern<<<(n + 255) / 256, 256, 0, st>>>(sorted_pos, keys, s2o, begin, end,
 														 stencil, num_stencil, wg, n, box, ex,
 														 nbr, cap, hshift, row_len, row_far, stats);
 }
