@@ -307,7 +307,10 @@ MB2_API int mb2_philox(mb2_context* ctx, uint64_t seed, uint32_t ctr0, uint32_t 
  * execute_integration run it (src/SimManager.cpp:337-504) for one patch:
  * clear forces, rebuild the pairlist when (step - 1) % rebuild_period == 0
  * (unless the skin check says the list is still valid), pair forces, bonded
- * forces (bonds, angles, dihedrals, restraints where given), BD integrate.
+ * forces (bonds, angles, dihedrals, restraints where given), then the BD
+ * update or, with integrator = 1, the Langevin branch of
+ * Patch::integrate_motion (PMF pass, the deferred closing kick when pending,
+ * B-A-O-A; the caller then owes the closing kick, as with mb2_baoab_integrate).
  * All device pointers. */
 typedef struct {
     float pairlist_cutoff;
@@ -332,6 +335,9 @@ typedef struct {
     const float* restraint_anchors4;
     const float* restraint_k;
     uint32_t num_restraints;
+    int integrator;             /* 0 Brownian (BD), 1 Langevin (BAOAB; needs mb2_set_langevin_types) */
+    float* mom4;                /* Langevin: momenta (float4 [n]), updated in place */
+    int deferred_kick_pending;  /* Langevin: the previous step's closing kick is owed */
 } mb2_step_params;
 
 MB2_API int mb2_step(mb2_context* ctx, float* pos4, float* force_energy4, const int* type_ids,

@@ -34,7 +34,8 @@ class StepParams(C.Structure):
                 ("dihedrals4", C.c_void_p), ("dihedral_table_idx", C.c_void_p),
                 ("num_dihedrals", C.c_uint32), ("restraint_ids", C.c_void_p),
                 ("restraint_anchors4", C.c_void_p), ("restraint_k", C.c_void_p),
-                ("num_restraints", C.c_uint32)]
+                ("num_restraints", C.c_uint32), ("integrator", C.c_int), ("mom4", C.c_void_p),
+                ("deferred_kick_pending", C.c_int)]
 
 
 class OutputConfig(C.Structure):

@@ -1102,6 +1102,10 @@ int mb2_step(mb2_context* ctx, float* pos4, float* force_energy4, const int* typ
 		const bool bonded = step_has_bonded(prm);
 		require(prm->num_dihedrals == 0 || ctx->bonded_count[2] > 0, MB2_ERR_STATE,
 				"mb2_step: dihedrals without dihedral tables");
+		require(prm->integrator == 0 || prm->integrator == 1, MB2_ERR_ARG,
+				"mb2_step: integrator is 0 (BD) or 1 (Langevin)");
+		require(prm->integrator == 0 || (prm->mom4 && ctx->langevin_types > 0), MB2_ERR_STATE,
+				"mb2_step: Langevin needs momenta and mb2_set_langevin_types");
 		if (bonded)
 			MB2_CUDA(cudaMemsetAsync(fe, 0, static_cast<size_t>(n) * sizeof(float4), st));
 		// Rebuild schedule and skin check (Patch.cpp:86-108)
@@ -1118,10 +1122,20 @@ int mb2_step(mb2_context* ctx, float* pos4, float* force_energy4, const int* typ
 		if (n == 0) return;
 		pair_kernel(ctx, n, prm->cutoff, prm->get_energy, st);
 		bonded_stage(ctx, pos, fe, prm, prm->get_energy, st);
+		StageScope scope(ctx, MB2_STAGE_INTEGRATE, st);
+		if (prm->integrator == 1) {
+			// Patch::integrate_motion, Langevin branch (Patch.cpp:290-335).
+			baoab_integrate_gather(pos, reinterpret_cast<float4*>(prm->mom4), fe,
+								   ctx->force_sorted.ptr, ctx->inv.ptr, bonded ? 1 : 0, type_ids,
+								   flags, n, ctx->types, ctx->box, prm->dt, prm->kT,
+								   static_cast<uint32_t>(step),
+								   mb2_bd_seed(prm->seed, prm->patch_id, step), 0u, prm->efield,
+								   prm->deferred_kick_pending ? 1 : 0, st);
+			return;
+		}
 		BdParams p{prm->dt, prm->kT, static_cast<uint32_t>(step),
 				   mb2_bd_seed(prm->seed, prm->patch_id, step), 0u,
 				   {prm->efield[0], prm->efield[1], prm->efield[2]}};
-		StageScope scope(ctx, MB2_STAGE_INTEGRATE, st);
 		bd_integrate_gather(pos, fe, ctx->force_sorted.ptr, ctx->inv.ptr, type_ids, flags, n,
 							ctx->types, ctx->box, p, bonded ? 1 : 0, st);
 	});
@@ -1136,9 +1150,9 @@ int mb2_window_forward(mb2_context* ctx, float* pos4, float* force_energy4, cons
 		require(ctx->types_set && ctx->types.num_grids == 0, MB2_ERR_STATE,
 				"mb2_window_forward: particle types without grids are required");
 		require(!matrix_has_analytical(ctx) && prm->num_dihedrals == 0 &&
-					prm->num_restraints == 0,
+					prm->num_restraints == 0 && prm->integrator == 0,
 				MB2_ERR_STATE,
-				"mb2_window_forward: tabulated pair, bond and angle terms only");
+				"mb2_window_forward: BD with tabulated pair, bond and angle terms only");
 		require(checkpoint_every > 0 && prm->rebuild_period > 0 &&
 					prm->rebuild_period % checkpoint_every == 0 &&
 					(first_step - 1) % checkpoint_every == 0,

@@ -479,8 +479,8 @@ void check_step_args(mb2_batch* b, const float* pos4, const float* fe4, const in
 	expect_arg(b->pt.num_types > 0, MB2_ERR_STATE,
 			   "mb2_batch_step: call mb2_batch_set_pair_tables");
 	expect_arg(prm->num_bonds == 0 && prm->num_angles == 0 && prm->num_dihedrals == 0 &&
-				   prm->num_restraints == 0,
-			   MB2_ERR_ARG, "mb2_batch_step: bonded terms are not supported in batched mode");
+				   prm->num_restraints == 0 && prm->integrator == 0,
+			   MB2_ERR_ARG, "mb2_batch_step: BD without bonded terms in batched mode");
 }
 
 // Rebuild decision of the reference (Patch.cpp:86-108), over all systems: at

@@ -232,15 +232,33 @@ __device__ __forceinline__ float half_kick(float m, float f, float h) {
 // Patch::integrate_motion's Langevin branch (Patch.cpp:290-335) for one
 // particle: PMF pass (Pmf.h:126-152), closing kick if pending (BAOAB.h:167-186),
 // then BAOABIntegrate (BAOAB.h:47-128). Vector3 / s is a multiply by 1 / s.
+// kGather (the fused step): the pair force comes from the Z-ordered
+// accumulator through the inverse permutation, plus what the bonded kernels
+// left in ForceEnergy when any ran (read_fe), and ForceEnergy receives the
+// sum as the reference leaves it.
+template <bool kGather>
 __global__ void __launch_bounds__(256) baoab_kernel(
 	float4* __restrict__ pos, float4* __restrict__ mom, float4* __restrict__ fe,
+	const float4* __restrict__ fs, const uint32_t* __restrict__ inv, int read_fe,
 	const int* __restrict__ type_ids, const uint32_t* __restrict__ flags, uint32_t n,
 	TypeTable ty, Box box, float dt, float kT, uint32_t step, uint64_t seed, uint32_t base_ctr,
 	float3 efield, int pending) {
 	const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
 	if (i >= n) return;
 	float4 p = pos[i];
-	float4 f = fe[i];
+	float4 f;
+	if (kGather) {
+		f = fs[inv[i]];
+		if (read_fe) {
+			const float4 ext = fe[i];
+			f.x = __fadd_rn(ext.x, f.x);
+			f.y = __fadd_rn(ext.y, f.y);
+			f.z = __fadd_rn(ext.z, f.z);
+			f.w = __fadd_rn(ext.w, f.w);
+		}
+	} else {
+		f = fe[i];
+	}
 	const int type = type_ids[i];
 	if (ty.num_grids > 0) {
 		const float e[3] = {efield.x, efield.y, efield.z};
@@ -249,8 +267,9 @@ __global__ void __launch_bounds__(256) baoab_kernel(
 		f.y = __fadd_rn(f.y, pmf.y);
 		f.z = __fadd_rn(f.z, pmf.z);
 		f.w = __fadd_rn(f.w, pmf.w);
-		fe[i] = f;
+		if (!kGather) fe[i] = f;
 	}
+	if (kGather) fe[i] = f;
 	if (flags && (flags[i] & kFlagRbAttached)) return;
 	float4 m = mom[i];
 	const float h = __fmul_rn(0.5f, dt);
@@ -378,9 +397,20 @@ void baoab_integrate(float4* pos, float4* mom, float4* fe, const int* type_ids,
 					 float dt, float kT, uint32_t step, uint64_t base_seed, uint32_t base_ctr,
 					 const float* efield, int pending, cudaStream_t st) {
 	if (n == 0) return;
-	MB2_LAUNCH baoab_kernel<<<(n + 255) / 256, 256, 0, st>>>(
-		pos, mom, fe, type_ids, flags, n, types, box, dt, kT, step, base_seed, base_ctr,
-		make_float3(efield[0], efield[1], efield[2]), pending);
+	MB2_LAUNCH baoab_kernel<false><<<(n + 255) / 256, 256, 0, st>>>(
+		pos, mom, fe, nullptr, nullptr, 0, type_ids, flags, n, types, box, dt, kT, step, base_seed,
+		base_ctr, make_float3(efield[0], efield[1], efield[2]), pending);
+}
+
+void baoab_integrate_gather(float4* pos, float4* mom, float4* fe, const float4* force_sorted,
+							const uint32_t* inv, int read_fe, const int* type_ids,
+							const uint32_t* flags, uint32_t n, const TypeTable& types,
+							const Box& box, float dt, float kT, uint32_t step, uint64_t base_seed,
+							uint32_t base_ctr, const float* efield, int pending, cudaStream_t st) {
+	if (n == 0) return;
+	MB2_LAUNCH baoab_kernel<true><<<(n + 255) / 256, 256, 0, st>>>(
+		pos, mom, fe, force_sorted, inv, read_fe, type_ids, flags, n, types, box, dt, kT, step,
+		base_seed, base_ctr, make_float3(efield[0], efield[1], efield[2]), pending);
 }
 
 void baoab_last_update(float4* mom, const float4* fe, const uint32_t* flags, uint32_t n,

@@ -287,6 +287,13 @@ void baoab_integrate(float4* pos, float4* mom, float4* fe, const int* type_ids,
 					 const uint32_t* flags, uint32_t n, const TypeTable& types, const Box& box,
 					 float dt, float kT, uint32_t step, uint64_t base_seed, uint32_t base_ctr,
 					 const float* efield, int pending, cudaStream_t st);
+// Fused-step variant: pair force gathered from the Z-ordered accumulator
+// (plus ForceEnergy when read_fe), ForceEnergy left as the reference leaves it.
+void baoab_integrate_gather(float4* pos, float4* mom, float4* fe, const float4* force_sorted,
+							const uint32_t* inv, int read_fe, const int* type_ids,
+							const uint32_t* flags, uint32_t n, const TypeTable& types,
+							const Box& box, float dt, float kT, uint32_t step, uint64_t base_seed,
+							uint32_t base_ctr, const float* efield, int pending, cudaStream_t st);
 // BAOAB_LastUpdate: mom += 0.5 dt F (closing half-kick) for non-frozen particles.
 void baoab_last_update(float4* mom, const float4* fe, const uint32_t* flags, uint32_t n,
 					   float dt, cudaStream_t st);

@@ -14,6 +14,7 @@ import pyoracle as po
 from conftest import GOLDEN
 from mars_md_b200 import _lib as L
 from mars_md_b200 import engine as E
+from mars_md_b200 import workloads as W
 
 pytestmark = pytest.mark.gpu
 
@@ -201,3 +202,48 @@ def test_fused_step_with_every_term_equals_separate_calls(ctx_factory):
     rc = a.lib.mb2_window_forward(a.h, E._p(pos_a), E._p(fe_a), E._p(dev["type_ids"]), n, 21, 20,
                                   20, po.C.byref(p), None)
     assert rc != 0 and b"tabulated" in a.lib.mb2_last_error(a.h)
+
+
+def test_fused_langevin_step_equals_separate_calls(ctx_factory):
+    """mb2_step with integrator = 1 (pair and bonded forces gathered into the
+    BAOAB kernel, grid PMF, deferred closing kick) moves particles and momenta
+    as mb2_pair_forces + bonded calls + mb2_baoab_integrate do."""
+    w = W.polymers(n_chains=8, beads=256, with_grid=True)
+    n = w.n
+    mass = np.array([120.0, 80.0], np.float32)[:w.num_types]
+    damping = np.full((w.num_types, 3), 40.0, np.float32)
+    rng = np.random.default_rng(4)
+    mom0 = np.zeros((n, 4), np.float32)
+    mom0[:, :3] = rng.normal(0, 20, (n, 3)).astype(np.float32)
+
+    def make():
+        ctx = ctx_factory(n)
+        dev = E.setup_workload(ctx, w)
+        ctx.set_langevin_types(mass, damping)
+        return ctx, dev
+
+    a, da = make()
+    mom_a = torch.from_numpy(mom0.copy()).cuda()
+    p = E.step_params(w, bonds=da["bonds"], bond_idx=da["bond_idx"], angles=da["angles"],
+                      angle_idx=da["angle_idx"])
+    p.integrator, p.mom4 = 1, mom_a.data_ptr()
+    b, db = make()
+    mom_b = torch.from_numpy(mom0.copy()).cuda()
+    for s in (1, 2):
+        p.deferred_kick_pending = int(s > 1)
+        a.step(da["pos"], da["fe"], da["type"], None, s, p)
+        db["fe"].zero_()
+        b.build_pairlist(db["pos"], db["type"], w.list_radius)
+        b.pair_forces(db["pos"], db["type"], db["fe"], w.cutoff, get_energy=False)
+        b.bond_forces(db["bonds"], db["bond_idx"], db["pos"], db["fe"], get_energy=False)
+        b.angle_forces(db["angles"], db["angle_idx"], db["pos"], db["fe"], get_energy=False)
+        b.baoab_integrate(db["pos"], mom_b, db["fe"], db["type"], None, w.dt, w.kT, s,
+                          b.bd_seed(w.seed, 0, s), pending=s > 1)
+    torch.cuda.synchronize()
+    L = float(w.box_size[0])
+    dp = np.abs(da["pos"].cpu().numpy()[:, :3] - db["pos"].cpu().numpy()[:, :3])
+    dp = np.minimum(dp, L - dp)
+    assert dp.max() <= 1e-4
+    ma, mb = mom_a.cpu().numpy()[:, :3], mom_b.cpu().numpy()[:, :3]
+    assert np.abs(ma - mb).max() <= 1e-4 * np.abs(mb).max()
+    assert np.abs(ma - mom0[:, :3]).max() > 1.0  # the momenta did move
