@@ -22,6 +22,7 @@ from __future__ import annotations
 import argparse
 import json
 import os
+import tempfile
 import subprocess
 import sys
 import time
@@ -65,7 +66,7 @@ class ClockSampler:
     def __init__(self, device_index):
         self.dev = device_index
         self.proc = None
-        self.path = os.path.join(ROOT, "gpurun_out", f"clocks_{os.getpid()}.csv")
+        self.path = os.path.join(tempfile.gettempdir(), f"mb2_clocks_{os.getpid()}.csv")
 
     def start(self):
         try:
