@@ -250,7 +250,8 @@ __global__ void __launch_bounds__(256, 7) build_walk_kernel(
 	int hshift, uint32_t* __restrict__ row_len, uint32_t* __restrict__ row_far,
 	unsigned long long* __restrict__ stats) {
 	__shared__ uint32_t split_tab[256];
-	__shared__ uint4 cell_buf[8 * kCellBuf];  // per warp: kept cells (jlo, end, image code)
+	__shared__ uint4 cell_buf[8 * kCellBuf];  // per warp: kept cells (jlo, end, image code, offset)
+	__shared__ float4 cand_buf[8 * 32];       // per warp: candidates that pass the group test
 	const int cells = 1 << wg.m;
 	for (int k = threadIdx.x; k < cells; k += blockDim.x) split_tab[k] = split_by3(k);
 	__syncthreads();
@@ -309,29 +310,74 @@ __global__ void __launch_bounds__(256, 7) build_walk_kernel(
 		const int lane = static_cast<int>(threadIdx.x & 31u);
 		uint4* buf = cell_buf + (threadIdx.x >> 5) * kCellBuf;
 		uint32_t count = 0;
+		float4* cbuf = cand_buf + (threadIdx.x >> 5) * 32;
+		const uint32_t lt_mask = (1u << lane) - 1u;
+		// A candidate whose distance from the group's coordinate range (less
+		// the Morton rounding margin) is above the fast test's upper bound gives
+		// every lane d^2 > fast_hi below, so no lane keeps it; such candidates
+		// are dropped 32 at a time before the lanes test the rest one by one.
+		const float gate = wg.fast_hi;
 		auto walk_buffered = [&](uint32_t m) {
-			for (uint32_t k = 0; k < m; ++k) {
-				const uint4 cb = buf[k];
-				// Particle coordinates moved into the candidate cell's image.
-				const float qx = pi.x - image_shift(cb.z, 0, box);
-				const float qy = pi.y - image_shift(cb.z, 1, box);
-				const float qz = pi.z - image_shift(cb.z, 2, box);
-				for (uint32_t j = cb.x; j < cb.y; ++j) {
+			// Offsets of the buffered cells' candidate ranges in one stream.
+			const uint32_t l0 = static_cast<uint32_t>(lane) < m ? buf[lane].y - buf[lane].x : 0u;
+			const uint32_t l1 = static_cast<uint32_t>(lane) + 32u < m ? buf[lane + 32].y - buf[lane + 32].x : 0u;
+			uint32_t s0 = l0, s1 = l1;
+#pragma unroll
+			for (int o = 1; o < 32; o <<= 1) {
+				const uint32_t a0 = __shfl_up_sync(0xFFFFFFFFu, s0, o);
+				const uint32_t a1 = __shfl_up_sync(0xFFFFFFFFu, s1, o);
+				if (lane >= o) {
+					s0 += a0;
+					s1 += a1;
+				}
+			}
+			const uint32_t tot0 = __shfl_sync(0xFFFFFFFFu, s0, 31);
+			const uint32_t stream = tot0 + __shfl_sync(0xFFFFFFFFu, s1, 31);
+			if (static_cast<uint32_t>(lane) < m) buf[lane].w = s0 - l0;
+			if (static_cast<uint32_t>(lane) + 32u < m) buf[lane + 32].w = tot0 + s1 - l1;
+			__syncwarp();
+			uint32_t kc = 0;  // this lane's cell in the stream (advances monotonically)
+			for (uint32_t t0 = 0; t0 < stream; t0 += 32u) {
+				const uint32_t t = t0 + static_cast<uint32_t>(lane);
+				bool pass = false;
+				float4 cand = make_float4(0.f, 0.f, 0.f, 0.f);
+				if (t < stream) {
+					while (kc + 1u < m && buf[kc + 1u].w <= t) ++kc;
+					const uint4 cb = buf[kc];
+					const uint32_t j = cb.x + (t - cb.w);
 					const float4 pj = sorted_pos[j];
+					// The candidate moved into the group's image.
+					const float sx = pj.x + image_shift(cb.z, 0, box);
+					const float sy = pj.y + image_shift(cb.z, 1, box);
+					const float sz = pj.z + image_shift(cb.z, 2, box);
+					const float gx = full[0] ? 0.0f : fmaxf(0.0f, fmaxf(gxlo - sx, sx - gxhi) - wg.eps[0]);
+					const float gy = full[1] ? 0.0f : fmaxf(0.0f, fmaxf(gylo - sy, sy - gyhi) - wg.eps[1]);
+					const float gz = full[2] ? 0.0f : fmaxf(0.0f, fmaxf(gzlo - sz, sz - gzhi) - wg.eps[2]);
+					pass = gx * gx + gy * gy + gz * gz <= gate;
+					cand = make_float4(sx, sy, sz, __uint_as_float(j));
+				}
+				const uint32_t pm = __ballot_sync(0xFFFFFFFFu, pass);
+				if (pass) cbuf[__popc(pm & lt_mask)] = cand;
+				__syncwarp();
+				const int np = __popc(pm);
+				for (int q = 0; q < np; ++q) {
+					const float4 c4 = cbuf[q];
+					const uint32_t j = __float_as_uint(c4.w);
 					if (!valid || j <= i) continue;
-					float dx = pj.x - qx, dy = pj.y - qy, dz = pj.z - qz;
+					float dx = c4.x - pi.x, dy = c4.y - pi.y, dz = c4.z - pi.z;
 					if (full[0]) dx -= box.size[0] * rintf(dx * box.inv[0]);
 					if (full[1]) dy -= box.size[1] * rintf(dy * box.inv[1]);
 					if (full[2]) dz -= box.size[2] * rintf(dz * box.inv[2]);
 					const float d2 = dx * dx + dy * dy + dz * dz;
 					bool hit = d2 < wg.fast_lo;
-					if (!hit && d2 <= wg.fast_hi) hit = exact_hit(box, pi, pj, wg.rc2);
+					if (!hit && d2 <= wg.fast_hi) hit = exact_hit(box, pi, sorted_pos[j], wg.rc2);
 					if (hit) {
 						const int bj = static_cast<int>(s2o[j]);
 						if (kExcl && is_excluded(ex, bj, row_b, row_e, body)) continue;
 						row.put(j | (bj < a ? kOrientBit : 0u), d2 <= wg.split2);
 					}
 				}
+				__syncwarp();
 			}
 		};
 		for (uint32_t base = 0; base < total; base += 32u) {
