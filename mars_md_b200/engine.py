@@ -20,7 +20,9 @@ call surface on the Brownian-dynamics path:
 * ``reorder_*`` / ``reorder_particles`` / ``ReorderManager`` -- the canonical
   Morton reorder of a patch (src/PatchOperation/Patch.cpp:455-480);
 * ``Output`` -- DCD frames, the energy file and restart files
-  (src/SimManager.cpp:541-1135, src/IO/DcdWriter.h).
+  (src/SimManager.cpp:541-1135, src/IO/DcdWriter.h);
+* ``HostStepper`` -- steps fed from and read back to pinned host memory, the
+  copies of neighbouring steps overlapping the device work.
 
 ``Batch`` wraps one ``mb2_batch``: many independent periodic systems stepped
 together (one launch per stage for all of them, CUDA-graph step replay, an
@@ -492,6 +494,110 @@ class Output:
             self.close()
         except Exception:
             pass
+
+
+class HostStepper:
+    """Steps whose positions live in pinned host memory.
+
+    Two patterns, both through ``Context.step`` on the compute stream with
+    the copies on two copy streams of their own:
+
+    * ``advance(host_pos, step)``: a trajectory owned by the host. The step
+      uploads ``host_pos``, runs, and reads the integrated positions back
+      into ``host_pos``, which the next ``advance`` uploads. The copies are
+      split into chunks: chunk c of the next upload waits only for chunk c of
+      the last read-back, so the two directions overlap each other.
+    * ``submit(host_in, host_out, step)``: independent inputs. Two device
+      position buffers alternate, so the upload of one submission and the
+      read-back of another overlap the steps on the device.
+
+    A stepper serves one of the two patterns. Both return the CUDA event that
+    marks the host buffer as written: read it (or change ``host_in``) only
+    after ``event.synchronize()``. ``finish()``
+    joins the copy streams into the compute stream, so that work queued there
+    afterwards (an event, a synchronize) follows every copy."""
+
+    def __init__(self, ctx: Context, type_ids, params: "L.StepParams", flags=None, n=None,
+                 chunks: int = 8):
+        self.ctx = ctx
+        self.type_ids = type_ids
+        self.flags = flags
+        self.params = params
+        self.n = int(type_ids.shape[0] if n is None else n)
+        dev = type_ids.device
+        self.pos = [torch.empty((self.n, 4), dtype=torch.float32, device=dev) for _ in range(2)]
+        self.fe = torch.zeros((self.n, 4), dtype=torch.float32, device=dev)
+        self.compute = torch.cuda.current_stream(dev)
+        self.up = torch.cuda.Stream(dev)
+        self.down = torch.cuda.Stream(dev)
+        self._uploaded = [torch.cuda.Event() for _ in range(2)]
+        self._stepped = [torch.cuda.Event() for _ in range(2)]
+        self._read = [torch.cuda.Event() for _ in range(2)]
+        self._used = [False, False]
+        self.k = 0
+        step = -(-self.n // max(int(chunks), 1))
+        self._chunks = [(a, min(a + step, self.n)) for a in range(0, self.n, step)] or [(0, 0)]
+        self._chunk_read = [torch.cuda.Event() for _ in self._chunks]
+        self._traj_used = False
+        self._mode = None
+
+    def _use(self, mode):
+        assert self._mode in (None, mode), "a HostStepper serves either advance() or submit()"
+        self._mode = mode
+
+    def _check(self, *bufs):
+        for b in bufs:
+            assert b.is_pinned(), "host buffers must be pinned"
+            assert tuple(b.shape) == (self.n, 4) and b.dtype == torch.float32
+
+    def advance(self, host_pos, step: int):
+        self._use("advance")
+        self._check(host_pos)
+        buf = self.pos[0]
+        with torch.cuda.stream(self.up):
+            for (a, b), ev in zip(self._chunks, self._chunk_read):
+                if self._traj_used:
+                    self.up.wait_event(ev)  # this chunk's last read-back
+                buf[a:b].copy_(host_pos[a:b], non_blocking=True)
+            self._uploaded[0].record(self.up)
+        self.compute.wait_event(self._uploaded[0])
+        self.ctx.step(buf, self.fe, self.type_ids, self.flags, step, self.params,
+                      stream=self.compute)
+        self._stepped[0].record(self.compute)
+        self.down.wait_event(self._stepped[0])
+        with torch.cuda.stream(self.down):
+            for (a, b), ev in zip(self._chunks, self._chunk_read):
+                host_pos[a:b].copy_(buf[a:b], non_blocking=True)
+                ev.record(self.down)
+        self._traj_used = True
+        return self._chunk_read[-1]
+
+    def submit(self, host_in, host_out, step: int):
+        self._use("submit")
+        self._check(host_in, host_out)
+        b = self.k & 1
+        self.k += 1
+        buf = self.pos[b]
+        if self._used[b]:
+            self.up.wait_event(self._read[b])  # the previous read-back of this buffer
+        with torch.cuda.stream(self.up):
+            buf.copy_(host_in, non_blocking=True)
+            self._uploaded[b].record(self.up)
+        self.compute.wait_event(self._uploaded[b])
+        self.ctx.step(buf, self.fe, self.type_ids, self.flags, step, self.params,
+                      stream=self.compute)
+        self._stepped[b].record(self.compute)
+        self.down.wait_event(self._stepped[b])
+        with torch.cuda.stream(self.down):
+            host_out.copy_(buf, non_blocking=True)
+            self._read[b].record(self.down)
+        self._used[b] = True
+        return self._read[b]
+
+    def finish(self):
+        """Make the compute stream wait for every copy submitted so far."""
+        self.compute.wait_stream(self.up)
+        self.compute.wait_stream(self.down)
 
 
 def to_original_order(values, ids):
