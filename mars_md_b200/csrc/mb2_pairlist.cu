@@ -241,7 +241,9 @@ struct RowWriter {
 // bound by the latency of its dependent loads (cell ranges, then candidates)
 // and more warps hide it. Measured on the 2,097,152-bead workload: 7.1 ms per
 // build at 7 blocks, 7.7 at 6 (40 registers), 7.9 at 5 (48 registers).
-template <bool kExcl>
+// kFull: some periodic axis is spanned whole by the group's candidate cells
+// (small boxes); without it the candidate test needs no minimum-image wrap.
+template <bool kExcl, bool kFull>
 __global__ void __launch_bounds__(256, 7) build_walk_kernel(
 	const float4* __restrict__ sorted_pos, const uint32_t* __restrict__ keys,
 	const uint32_t* __restrict__ s2o, const uint32_t* __restrict__ begin,
@@ -302,7 +304,7 @@ __global__ void __launch_bounds__(256, 7) build_walk_kernel(
 		bool full[3];
 #pragma unroll
 		for (int ax = 0; ax < 3; ++ax) {
-			full[ax] = box.periodic[ax] && (hi[ax] - lo[ax] + 2 * wg.radius[ax] + 1 >= cells);
+			full[ax] = kFull && box.periodic[ax] && (hi[ax] - lo[ax] + 2 * wg.radius[ax] + 1 >= cells);
 			from[ax] = full[ax] ? 0 : lo[ax] - wg.radius[ax];
 			span[ax] = full[ax] ? cells : hi[ax] - lo[ax] + 2 * wg.radius[ax] + 1;
 		}
@@ -363,14 +365,20 @@ __global__ void __launch_bounds__(256, 7) build_walk_kernel(
 				for (int q = 0; q < np; ++q) {
 					const float4 c4 = cbuf[q];
 					const uint32_t j = __float_as_uint(c4.w);
-					if (!valid || j <= i) continue;
 					float dx = c4.x - pi.x, dy = c4.y - pi.y, dz = c4.z - pi.z;
-					if (full[0]) dx -= box.size[0] * rintf(dx * box.inv[0]);
-					if (full[1]) dy -= box.size[1] * rintf(dy * box.inv[1]);
-					if (full[2]) dz -= box.size[2] * rintf(dz * box.inv[2]);
+					if (kFull) {
+						if (full[0]) dx -= box.size[0] * rintf(dx * box.inv[0]);
+						if (full[1]) dy -= box.size[1] * rintf(dy * box.inv[1]);
+						if (full[2]) dz -= box.size[2] * rintf(dz * box.inv[2]);
+					}
 					const float d2 = dx * dx + dy * dy + dz * dz;
-					bool hit = d2 < wg.fast_lo;
-					if (!hit && d2 <= wg.fast_hi) hit = exact_hit(box, pi, sorted_pos[j], wg.rc2);
+					bool hit = valid && j > i && d2 < wg.fast_lo;
+					// The exact test for the few lanes within rounding of the radius,
+					// behind a warp vote so that the other candidates skip it.
+					const bool band = valid && j > i && !hit && d2 <= wg.fast_hi;
+					if (__any_sync(0xFFFFFFFFu, band)) {
+						if (band) hit = exact_hit(box, pi, sorted_pos[j], wg.rc2);
+					}
 					if (hit) {
 						const int bj = static_cast<int>(s2o[j]);
 						if (kExcl && is_excluded(ex, bj, row_b, row_e, body)) continue;
@@ -585,7 +593,14 @@ void build_walk(const float4* sorted_pos, const uint32_t* keys, const uint32_t* 
 	MB2_CUDA(cudaMemsetAsync(stats, 0, 2 * sizeof(unsigned long long), st));
 	if (n == 0) return;
 	const bool excl = ex.offsets != nullptr || ex.rigid_body_id != nullptr;
-	auto kern = excl ? build_walk_kernel<true> : build_walk_kernel<false>;
+	// The kernel variant with the minimum-image wrap is needed when a coherent
+	// group's candidate cells can span a whole periodic axis: a cell spread of
+	// up to emax plus the stencil's 2 * radius + 1 reaching the cell count.
+	bool full = false;
+	for (int a = 0; a < 3; ++a)
+		full = full || (box.periodic[a] && wg.emax + 2 * wg.radius[a] + 1 >= (1 << wg.m));
+	auto kern = excl ? (full ? build_walk_kernel<true, true> : build_walk_kernel<true, false>)
+					 : (full ? build_walk_kernel<false, true> : build_walk_kernel<false, false>);
 	// The stencil (used by the few groups that walk per particle) is read
 	// through L1, leaving shared memory to the cell buffers.
 	MB2_LAUNCH kern<<<(n + 255) / 256, 256, 0, st>>>(sorted_pos, keys, s2o, begin, end,
