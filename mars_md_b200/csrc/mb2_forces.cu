@@ -171,33 +171,53 @@ __device__ __forceinline__ void analytic_terms(uint32_t terms, const PairTermRef
 	}
 }
 
+// Flips the sign bits of both halves when flip is the sign bit.
+__device__ __forceinline__ float2 xor_sign2(float2 v, uint32_t flip) {
+	return make_float2(__uint_as_float(__float_as_uint(v.x) ^ flip),
+					   __uint_as_float(__float_as_uint(v.y) ^ flip));
+}
+
 // One pair of the half list, rounded as the reference rounds it. flip
 // (bit 31 of the entry): the reference orients the pair j -> i. With kTerms,
 // the analytical terms of the type pair come first, then the table.
+//
+// The x and y components go through sm_100's packed FP32 instructions
+// (__fadd2_rn / __fmul2_rn: two IEEE round-to-nearest operations each, so
+// every value is the scalar one bit for bit), z stays scalar. npi = (-pi.x,
+// -pi.y); a - b is computed as a + (-b) and b * l as -(b * (-l)), both exact
+// rewrites. The i-force is accumulated negated (nxy, nz): -(a - h) = (-a) + h
+// in round-to-nearest, so the caller's negation at the end gives the same sum.
 template <bool kEnergy, bool kAllPeriodic, bool kTerms>
-__device__ __forceinline__ void pair_scalar(const float4& pi, const float4& pj, uint32_t j,
-											uint32_t flip,
+__device__ __forceinline__ void pair_scalar(const float4& pi, float2 npi, const float4& pj,
+											uint32_t j, uint32_t flip,
 											const PairTableRef* trow, const float* bin_f,
 											const float2* bin_e, const PairTermRef* arow,
 											const PairSolvent& sv, const Box& box,
-											float cutoff_sq, float4* force, float& fx, float& fy,
-											float& fz, float& fe, double& e_acc, double& w_acc) {
+											float cutoff_sq, float4* force, float2& nxy, float& nz,
+											float& fe, double& e_acc, double& w_acc) {
 	// r = wrap_diff(pos[second] - pos[first])
 	// (pi - pj is exactly -(pj - pi) in round-to-nearest, so a sign flip suffices)
-	float dx = __uint_as_float(__float_as_uint(__fsub_rn(pj.x, pi.x)) ^ flip);
-	float dy = __uint_as_float(__float_as_uint(__fsub_rn(pj.y, pi.y)) ^ flip);
+	float2 dxy = xor_sign2(__fadd2_rn(make_float2(pj.x, pj.y), npi), flip);
 	float dz = __uint_as_float(__float_as_uint(__fsub_rn(pj.z, pi.z)) ^ flip);
 	if (kAllPeriodic) {
-		dx = wrap1(dx, box.size[0], box.inv[0], box.half[0]);
-		dy = wrap1(dy, box.size[1], box.inv[1], box.half[1]);
+		// wrap1 on x and y: image = floor(d / l); d -= image * l; d >= l/2 -> d - l.
+		const float2 negl = make_float2(-box.size[0], -box.size[1]);
+		float2 img = __fmul2_rn(dxy, make_float2(box.inv[0], box.inv[1]));
+		img.x = floorf(img.x);
+		img.y = floorf(img.y);
+		dxy = __fadd2_rn(dxy, __fmul2_rn(img, negl));
+		const float2 up = __fadd2_rn(dxy, negl);
+		dxy.x = dxy.x >= box.half[0] ? up.x : dxy.x;
+		dxy.y = dxy.y >= box.half[1] ? up.y : dxy.y;
 		dz = wrap1(dz, box.size[2], box.inv[2], box.half[2]);
 	} else {
-		const float3 r = wrap_diff(box, dx, dy, dz);
-		dx = r.x;
-		dy = r.y;
+		const float3 r = wrap_diff(box, dxy.x, dxy.y, dz);
+		dxy = make_float2(r.x, r.y);
 		dz = r.z;
 	}
-	const float d2v = len2(dx, dy, dz);
+	const float dx = dxy.x, dy = dxy.y;
+	const float2 sq = __fmul2_rn(dxy, dxy);
+	const float d2v = __fadd_rn(__fadd_rn(sq.x, sq.y), __fmul_rn(dz, dz));
 	const float dist = __fsqrt_rn(d2v);
 	if (dist < 1e-6f || (cutoff_sq > 0.0f && __fmul_rn(dist, dist) > cutoff_sq)) return;
 	const PairTableRef t = trow[type_of(pj)];
@@ -229,8 +249,8 @@ __device__ __forceinline__ void pair_scalar(const float4& pi, const float4& pj, 
 	}
 	const float inv = __frcp_rn(dist);
 	// f = unit * F acts on the pair's second particle, -f on its first.
-	const float gx = __fmul_rn(__fmul_rn(inv, dx), fm);
-	const float gy = __fmul_rn(__fmul_rn(inv, dy), fm);
+	const float2 gxy = __fmul2_rn(__fmul2_rn(make_float2(inv, inv), dxy), make_float2(fm, fm));
+	const float gx = gxy.x, gy = gxy.y;
 	const float gz = __fmul_rn(__fmul_rn(inv, dz), fm);
 	float half = 0.0f;
 	if (kEnergy) {
@@ -240,13 +260,11 @@ __device__ __forceinline__ void pair_scalar(const float4& pi, const float4& pj, 
 				 static_cast<double>(gz) * dz;
 	}
 	// j is the pair's second particle unless the pair is stored flipped.
-	const float hx = __uint_as_float(__float_as_uint(gx) ^ flip);
-	const float hy = __uint_as_float(__float_as_uint(gy) ^ flip);
+	const float2 hxy = xor_sign2(gxy, flip);
 	const float hz = __uint_as_float(__float_as_uint(gz) ^ flip);
-	red_add_v4(&force[j], hx, hy, hz, half);
-	fx -= hx;
-	fy -= hy;
-	fz -= hz;
+	red_add_v4(&force[j], hxy.x, hxy.y, hz, half);
+	nxy = __fadd2_rn(nxy, hxy);
+	nz = __fadd_rn(nz, hz);
 	fe += half;
 }
 
@@ -320,7 +338,9 @@ __global__ void __launch_bounds__(
 	const uint32_t cnt = valid ? row_len[i] : 0u;
 	// Entry k of row i: ((i / H) * cap + k) * H + i % H.
 	const uint32_t* col = nbr + (static_cast<size_t>(i / H) * cap) * H + (i % H);
-	float fx = 0.0f, fy = 0.0f, fz = 0.0f, fe = 0.0f;
+	const float2 npi = make_float2(-pi.x, -pi.y);
+	float2 nxy = make_float2(0.0f, 0.0f);  // minus the i-force, x and y
+	float nz = 0.0f, fe = 0.0f;
 	double e_acc = 0.0, w_acc = 0.0;
 	// Two entries per lane per iteration: both neighbour gathers are in flight
 	// before either pair's arithmetic (the kernel is bound by gather latency).
@@ -331,20 +351,22 @@ __global__ void __launch_bounds__(
 		const uint32_t j0 = e0 & ~kOrientBit, j1 = e1 & ~kOrientBit;
 		const float4 p0 = sorted_pos[j0];
 		const float4 p1 = sorted_pos[j1];
-		pair_scalar<kEnergy, kAllPeriodic, kTerms>(pi, p0, j0, e0 & kOrientBit, trow, bin_f, bin_e,
-												   arow, sv, box, cutoff_sq, force, fx, fy, fz, fe,
-												   e_acc, w_acc);
-		pair_scalar<kEnergy, kAllPeriodic, kTerms>(pi, p1, j1, e1 & kOrientBit, trow, bin_f, bin_e,
-												   arow, sv, box, cutoff_sq, force, fx, fy, fz, fe,
-												   e_acc, w_acc);
+		pair_scalar<kEnergy, kAllPeriodic, kTerms>(pi, npi, p0, j0, e0 & kOrientBit, trow, bin_f,
+												   bin_e, arow, sv, box, cutoff_sq, force, nxy, nz,
+												   fe, e_acc, w_acc);
+		pair_scalar<kEnergy, kAllPeriodic, kTerms>(pi, npi, p1, j1, e1 & kOrientBit, trow, bin_f,
+												   bin_e, arow, sv, box, cutoff_sq, force, nxy, nz,
+												   fe, e_acc, w_acc);
 	}
 	if (t < cnt) {
 		const uint32_t entry = __ldcs(col + static_cast<size_t>(t) * H);
 		const uint32_t j = entry & ~kOrientBit;
-		pair_scalar<kEnergy, kAllPeriodic, kTerms>(pi, sorted_pos[j], j, entry & kOrientBit, trow,
-												   bin_f, bin_e, arow, sv, box, cutoff_sq, force,
-												   fx, fy, fz, fe, e_acc, w_acc);
+		pair_scalar<kEnergy, kAllPeriodic, kTerms>(pi, npi, sorted_pos[j], j, entry & kOrientBit,
+												   trow, bin_f, bin_e, arow, sv, box, cutoff_sq,
+												   force, nxy, nz, fe, e_acc, w_acc);
 	}
+	// The lanes' sums of minus the i-force, then negated (exact).
+	float fx = nxy.x, fy = nxy.y, fz = nz;
 	if (G > 1) {
 #pragma unroll
 		for (int o = G / 2; o > 0; o >>= 1) {
@@ -354,7 +376,7 @@ __global__ void __launch_bounds__(
 			if (kEnergy) fe += __shfl_xor_sync(0xFFFFFFFFu, fe, o, G);
 		}
 	}
-	if (valid && sub == 0 && cnt != 0u) red_add_v4(&force[i], fx, fy, fz, fe);
+	if (valid && sub == 0 && cnt != 0u) red_add_v4(&force[i], -fx, -fy, -fz, fe);
 	if (kEnergy) block_add_f64(e_acc, w_acc, ev);
 }
 
