@@ -58,28 +58,100 @@ def _peaks():
 
 
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons sampled every 200 ms."""
+    """SM clocks and clock-event (throttle) reasons sampled during the timed
+    region: NVML read every 5 ms from a thread (the timed region is tens of
+    milliseconds), else nvidia-smi every 50 ms. Read-only; nothing is set."""
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    NAMES = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
 
     def __init__(self, device_index):
         self.dev = device_index
+        self.samples = []      # (time, sm MHz, set of reason names)
+        self.max_mhz = None
+        self.window = None
+        self._stop = None
         self.proc = None
         self.path = os.path.join(tempfile.gettempdir(), f"mb2_clocks_{os.getpid()}.csv")
 
+    def _nvml_handle(self, nv):
+        try:
+            import torch
+            p = torch.cuda.get_device_properties(self.dev)
+            bus = f"{p.pci_domain_id:08x}:{p.pci_bus_id:02x}:{p.pci_device_id:02x}.0"
+            return nv.nvmlDeviceGetHandleByPciBusId(bus)
+        except Exception:
+            return nv.nvmlDeviceGetHandleByIndex(self.dev)
+
     def start(self):
         try:
-            os.makedirs(os.path.dirname(self.path), exist_ok=True)
+            import threading
+            import pynvml as nv
+            nv.nvmlInit()
+            h = self._nvml_handle(nv)
+            self.max_mhz = float(nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM))
+            bits = (nv.nvmlClocksEventReasonHwSlowdown, nv.nvmlClocksEventReasonHwThermalSlowdown,
+                    nv.nvmlClocksEventReasonSwThermalSlowdown, nv.nvmlClocksEventReasonSwPowerCap)
+            self._stop = threading.Event()
+
+            def poll():
+                while not self._stop.is_set():
+                    try:
+                        sm = float(nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM))
+                        r = nv.nvmlDeviceGetCurrentClocksEventReasons(h)
+                        self.samples.append((time.perf_counter(), sm,
+                                             {n for n, b in zip(self.NAMES, bits) if r & b}))
+                    except Exception:
+                        pass
+                    self._stop.wait(0.005)
+
+            self.thread = threading.Thread(target=poll, daemon=True)
+            self.thread.start()
+            return
+        except Exception:
+            self._stop = None
+        try:
             self.f = open(self.path, "w")
             self.proc = subprocess.Popen(
                 ["nvidia-smi", f"--id={self.dev}", f"--query-gpu={self.FIELDS}",
-                 "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.f,
+                 "--format=csv,noheader,nounits", "-lms", "50"], stdout=self.f,
                 stderr=subprocess.DEVNULL)
+            time.sleep(1.0)  # first sample before the timed region
         except Exception:
             self.proc = None
 
+    def begin(self):
+        self.window = [time.perf_counter(), None]
+        self._lines0 = self._count_lines()
+
+    def end(self):
+        if self.window is not None:
+            self.window[1] = time.perf_counter()
+
+    def _count_lines(self):
+        if self.proc is None:
+            return 0
+        try:
+            self.f.flush()
+            with open(self.path) as f:
+                return sum(1 for _ in f)
+        except Exception:
+            return 0
+
     def stop(self):
+        if self._stop is not None:
+            self._stop.set()
+            self.thread.join(timeout=2)
+            t0, t1 = self.window if self.window else (0.0, float("inf"))
+            inside = [x for x in self.samples if t0 <= x[0] <= (t1 or float("inf"))]
+            if not inside:  # nearest sample after the region began
+                inside = [x for x in self.samples if x[0] >= t0][:1]
+            if not inside:
+                return None
+            return {"sm_mhz": float(np.median([x[1] for x in inside])), "sm_max_mhz": self.max_mhz,
+                    "reasons": sorted(set().union(*[x[2] for x in inside])),
+                    "samples": len(inside), "source": "nvml, 5 ms"}
         if self.proc is None:
             return None
         self.proc.terminate()
@@ -94,18 +166,18 @@ class ClockSampler:
                 parts = [p.strip() for p in line.split(",")]
                 if len(parts) >= 9:
                     rows.append(parts)
+        rows = rows[getattr(self, "_lines0", 0):] or rows[-1:]
         if not rows:
             return None
         sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
         reasons = set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
         for r in rows:
-            for k, name in enumerate(names):
+            for k, name in enumerate(self.NAMES):
                 if r[5 + k].lower() == "active":
                     reasons.add(name)
         return {"sm_mhz": float(np.median(sm)) if sm else None,
                 "sm_max_mhz": float(rows[0][2]) if rows[0][2].replace(".", "").isdigit() else None,
-                "reasons": sorted(reasons), "samples": len(rows)}
+                "reasons": sorted(reasons), "samples": len(rows), "source": "nvidia-smi, 50 ms"}
 
 
 def _traffic_from_profile():
@@ -155,6 +227,7 @@ def run_ours(args):
     launches0 = L.mb2_launch_count()
     start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     torch.cuda.synchronize()
+    clocks.begin()
     start.record(stream)
     rebuilds = 0
     for _ in range(args.steps):
@@ -164,6 +237,7 @@ def run_ours(args):
         ctx.step(dev["pos"], dev["fe"], dev["type"], None, s, prm)
     stop.record(stream)
     torch.cuda.synchronize()
+    clocks.end()
     launches = int(L.mb2_launch_count() - launches0)
     barrier()
     clk = clocks.stop()
