@@ -55,6 +55,7 @@ struct mb2_context {
 	// pair tables
 	PairTables pt;
 	DevBuf<PairTableRef> refs;
+	DevBuf<int> table_offsets;  // per type pair: offset of its table's bins, -1 none
 	DevBuf<float> bin_force;
 	DevBuf<float2> bin_energy;
 
@@ -720,9 +721,33 @@ int mb2_set_pair_tables(mb2_context* ctx, int num_types, const uint32_t* term_ma
 							cudaMemcpyHostToDevice));
 		MB2_CUDA(cudaMemcpy(ctx->bin_energy.ptr, be.data(), be.size() * sizeof(float2),
 							cudaMemcpyHostToDevice));
+		// Tables of one start, bin width and length for every type pair that
+		// has one (compared bit for bit): the kernel reads 4-byte offsets.
+		std::vector<int> offs(tt, -1);
+		bool uniform = false, any = false;
+		PairTableRef u{0.0f, 0.0f, 0, -1};
+		for (int k = 0; k < tt; ++k) {
+			offs[k] = refs[k].offset;
+			if (refs[k].offset < 0) continue;
+			if (!any) {
+				u = refs[k];
+				any = uniform = true;
+			} else if (std::memcmp(&u.start, &refs[k].start, sizeof(float)) != 0 ||
+					   std::memcmp(&u.step_inv, &refs[k].step_inv, sizeof(float)) != 0 ||
+					   u.last != refs[k].last) {
+				uniform = false;
+			}
+		}
+		u.offset = -1;
+		ctx->table_offsets.ensure(tt);
+		MB2_CUDA(cudaMemcpy(ctx->table_offsets.ptr, offs.data(), tt * sizeof(int),
+							cudaMemcpyHostToDevice));
 		ctx->pt.num_types = num_types;
 		ctx->pt.total_bins = static_cast<uint32_t>(total);
 		ctx->pt.refs = ctx->refs.ptr;
+		ctx->pt.offsets = ctx->table_offsets.ptr;
+		ctx->pt.uniform = uniform;
+		ctx->pt.uniform_ref = u;
 		ctx->pt.bin_force = ctx->bin_force.ptr;
 		ctx->pt.bin_energy = ctx->bin_energy.ptr;
 		ctx->term_matrix_h.assign(term_matrix, term_matrix + tt);

@@ -171,6 +171,25 @@ __device__ __forceinline__ void analytic_terms(uint32_t terms, const PairTermRef
 	}
 }
 
+// The table references of one row's type: the full 16-byte reference per j
+// type, or (kUniform) the shared start / step_inv / last with a 4-byte offset
+// per j type, one broadcast shared-memory word for the warp instead of a
+// 128-bit load.
+template <bool kUniform>
+struct TableRow {
+	const PairTableRef* row;
+	const int* off;
+	PairTableRef u;
+	__device__ __forceinline__ PairTableRef operator()(int tj) const {
+		if (kUniform) {
+			PairTableRef t = u;
+			t.offset = off[tj];
+			return t;
+		}
+		return row[tj];
+	}
+};
+
 // Flips the sign bits of both halves when flip is the sign bit.
 __device__ __forceinline__ float2 xor_sign2(float2 v, uint32_t flip) {
 	return make_float2(__uint_as_float(__float_as_uint(v.x) ^ flip),
@@ -187,10 +206,10 @@ __device__ __forceinline__ float2 xor_sign2(float2 v, uint32_t flip) {
 // -pi.y); a - b is computed as a + (-b) and b * l as -(b * (-l)), both exact
 // rewrites. The i-force is accumulated negated (nxy, nz): -(a - h) = (-a) + h
 // in round-to-nearest, so the caller's negation at the end gives the same sum.
-template <bool kEnergy, bool kAllPeriodic, bool kTerms>
+template <bool kEnergy, bool kAllPeriodic, bool kTerms, class TRow>
 __device__ __forceinline__ void pair_scalar(const float4& pi, float2 npi, const float4& pj,
 											uint32_t j, uint32_t flip,
-											const PairTableRef* trow, const float* bin_f,
+											const TRow& trow, const float* bin_f,
 											const float2* bin_e, const PairTermRef* arow,
 											const PairSolvent& sv, const Box& box,
 											float cutoff_sq, float4* force, float2& nxy, float& nz,
@@ -220,7 +239,7 @@ __device__ __forceinline__ void pair_scalar(const float4& pi, float2 npi, const 
 	const float d2v = __fadd_rn(__fadd_rn(sq.x, sq.y), __fmul_rn(dz, dz));
 	const float dist = __fsqrt_rn(d2v);
 	if (dist < 1e-6f || (cutoff_sq > 0.0f && __fmul_rn(dist, dist) > cutoff_sq)) return;
-	const PairTableRef t = trow[type_of(pj)];
+	const PairTableRef t = trow(type_of(pj));
 	float fm = 0.0f, e = 0.0f;
 	if (kTerms) {
 		const PairTermRef a = arow[type_of(pj)];
@@ -292,12 +311,13 @@ constexpr int pair_min_blocks() {
 	return !kOneBox ? 1 : (kTerms ? 3 : (kEnergy ? 5 : 8));
 }
 
-template <int G, bool kEnergy, bool kAllPeriodic, bool kTerms, class BoxSrc>
+template <int G, bool kEnergy, bool kAllPeriodic, bool kTerms, bool kUniform, class BoxSrc>
 __global__ void __launch_bounds__(
 	256, pair_min_blocks<kEnergy, kTerms, std::is_same<BoxSrc, OneBox>::value>()) pair_force_kernel(
 	const float4* __restrict__ sorted_pos, const uint32_t* __restrict__ nbr,
 	const uint32_t* __restrict__ row_len, uint32_t n, uint32_t cap, int T,
-	const PairTableRef* __restrict__ refs_g, const float* __restrict__ force_g,
+	const PairTableRef* __restrict__ refs_g, const int* __restrict__ offs_g, PairTableRef uref,
+	const float* __restrict__ force_g,
 	const float2* __restrict__ energy_g, uint32_t total_bins,
 	const PairTermRef* __restrict__ terms_g, PairSolvent sv, BoxSrc boxes, float cutoff_sq,
 	float4* force, double* __restrict__ ev) {
@@ -313,7 +333,11 @@ __global__ void __launch_bounds__(
 	constexpr bool kStage = !std::is_same<BoxSrc, OneBox>::value;
 	extern __shared__ float4 smem4[];
 	PairTableRef* refs = reinterpret_cast<PairTableRef*>(smem4);
-	for (int k = threadIdx.x; k < T * T; k += blockDim.x) refs[k] = refs_g[k];
+	int* soff = reinterpret_cast<int*>(smem4);
+	for (int k = threadIdx.x; k < T * T; k += blockDim.x) {
+		if (kUniform) soff[k] = offs_g[k];
+		else refs[k] = refs_g[k];
+	}
 	const float* __restrict__ bin_f = force_g;
 	const float2* __restrict__ bin_e = energy_g;
 	if (kStage) {
@@ -333,7 +357,10 @@ __global__ void __launch_bounds__(
 	const bool valid = i < n;
 	const Box& box = boxes.row(valid ? i : 0u);
 	const float4 pi = valid ? sorted_pos[i] : make_float4(0.f, 0.f, 0.f, 0.f);
-	const PairTableRef* trow = refs + (valid ? type_of(pi) : 0) * T;
+	TableRow<kUniform> trow;
+	trow.row = refs + (valid ? type_of(pi) : 0) * T;
+	trow.off = soff + (valid ? type_of(pi) : 0) * T;
+	trow.u = uref;
 	const PairTermRef* arow = kTerms ? terms_g + (valid ? type_of(pi) : 0) * T : nullptr;
 	const uint32_t cnt = valid ? row_len[i] : 0u;
 	// Entry k of row i: ((i / H) * cap + k) * H + i % H.
@@ -596,13 +623,13 @@ __global__ void __launch_bounds__(256) restraint_kernel(const int* __restrict__ 
 	if (get_energy) block_add_f64(e_acc, 0.0, energy);
 }
 
-template <int G, bool kEnergy, bool kAllPeriodic, bool kTerms, class BoxSrc>
+template <int G, bool kEnergy, bool kAllPeriodic, bool kTerms, class BoxSrc, bool kUniform = false>
 void launch_pair(const float4* sorted_pos, const uint32_t* nbr, const uint32_t* row_len,
 				 uint32_t n, uint32_t cap, const PairTables& t, const BoxSrc& boxes,
 				 float cutoff_sq, float4* force_sorted, double* ev, cudaStream_t st) {
 	const uint32_t rows = 256 / G;
 	const uint32_t blocks = (n + rows - 1) / rows;
-	auto kern = pair_force_kernel<G, kEnergy, kAllPeriodic, kTerms, BoxSrc>;
+	auto kern = pair_force_kernel<G, kEnergy, kAllPeriodic, kTerms, kUniform, BoxSrc>;
 	constexpr bool kStage = !std::is_same<BoxSrc, OneBox>::value;
 	const size_t smem =
 		static_cast<size_t>(t.num_types * t.num_types) * sizeof(PairTableRef) +
@@ -613,7 +640,8 @@ void launch_pair(const float4* sorted_pos, const uint32_t* nbr, const uint32_t* 
 		MB2_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
 									  static_cast<int>(smem)));
 	MB2_LAUNCH kern<<<blocks, 256, smem, st>>>(sorted_pos, nbr, row_len, n, cap, t.num_types,
-											   t.refs, t.bin_force, t.bin_energy, t.total_bins,
+											   t.refs, t.offsets, t.uniform_ref, t.bin_force,
+											   t.bin_energy, t.total_bins,
 											   t.terms, t.solvent, boxes, cutoff_sq, force_sorted,
 											   ev);
 }
@@ -627,6 +655,11 @@ void launch_pair_t(const float4* sorted_pos, const uint32_t* nbr, const uint32_t
 		if (t.terms) {
 			launch_pair<G, kEnergy, kAllPeriodic, true>(sorted_pos, nbr, row_len, n, cap, t, boxes,
 														cutoff_sq, force_sorted, ev, st);
+			return;
+		}
+		if (t.uniform && t.offsets) {
+			launch_pair<G, kEnergy, kAllPeriodic, false, BoxSrc, true>(
+				sorted_pos, nbr, row_len, n, cap, t, boxes, cutoff_sq, force_sorted, ev, st);
 			return;
 		}
 	}

@@ -205,6 +205,12 @@ struct PairTables {
 	const float2* bin_energy = nullptr;   // device: (U[k], U[k+1]-U[k]), (U[size-1], 0) last
 	const PairTermRef* terms = nullptr;   // device [T*T], or null: tabulated terms only
 	PairSolvent solvent{};
+	// Every type pair with a table uses tables of one start, bin width and
+	// length (uniform.start / step_inv / last): the kernel then reads only
+	// each type pair's offset (device [T*T], -1: no table).
+	const int* offsets = nullptr;
+	bool uniform = false;
+	PairTableRef uniform_ref{0.0f, 0.0f, 0, -1};
 };
 void pair_forces(const float4* sorted_pos, const uint32_t* nbr, const uint32_t* row_len,
 				 uint32_t n, uint32_t cap, int lanes_per_row, const PairTables& t, const Box& box,

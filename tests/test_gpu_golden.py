@@ -115,6 +115,39 @@ def test_pair_forces_match_reference_fixture(ctx_factory, oracle):
     assert np.allclose(got[:, 3], d["pair_fe"][:, 3], rtol=1e-5, atol=1e-6)
 
 
+def test_pair_forces_nonuniform_tables_match_oracle(ctx_factory, oracle):
+    """The fixture's positions and tags with tables of different lengths,
+    starts and bin widths (the kernel's general table path; uniform tables
+    take a path that reads only each type pair's offset) against the FP64
+    restatement, forces and energies."""
+    d = _load("uniform4096")
+    n = len(d["pos"])
+    base = _tables(d)
+    tabs = []
+    for k, (vals, start, sinv) in enumerate(base):
+        m = len(vals) - 23 * k                  # 400, 377, ... bins
+        step = (1.0 / sinv) * (1.0 + 0.05 * k)  # wider bins for later tables
+        r = start + 0.25 * k + step * np.arange(m)
+        tabs.append((np.interp(r, start + np.arange(len(vals)) / sinv, vals).astype(np.float32),
+                     float(np.float32(start + 0.25 * k)), float(np.float32(1.0 / step))))
+    ctx = ctx_factory(n)
+    _box(ctx, d)
+    ctx.set_pair_tables(4, d["term_matrix"], tabs)
+    pos, types = _cuda(d["pos"]), _cuda(d["type_ids"])
+    ctx.build_pairlist(pos, types, float(d["rc_list"]))
+    fe = torch.zeros((n, 4), dtype=torch.float32, device="cuda")
+    ctx.pair_forces(pos, types, fe, float(d["cutoff"]), get_energy=True)
+    got = fe.cpu().numpy()
+    box = po.Box.make(d["box_origin"], d["box_size"], d["box_periodic"])
+    pairs, _, _ = oracle.build_pairlist(d["pos"], box, float(d["rc_list"]))
+    tags = oracle.resolve_tags(pairs, d["type_ids"], d["term_matrix"], 4)
+    _, f64, fabs = oracle.pair_forces(pairs, d["pos"], tags, po.TableSet(tabs), box,
+                                      np.float32(d["cutoff"]) ** 2)
+    assert np.abs(f64[:, :3]).max() > 0.0
+    assert _force_err(got, f64, fabs) <= FORCE_TOL
+    assert np.allclose(got[:, 3], f64[:, 3], rtol=1e-5, atol=1e-6)
+
+
 def test_bonded_forces_match_reference_fixture(ctx_factory):
     d = _load("polymer_excl")
     n = len(d["pos"])
