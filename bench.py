@@ -331,6 +331,8 @@ def run_ours(args):
             out["batched"] = run_batched(local)
         if not args.no_adjoint:
             out["adjoint"] = run_adjoint(local)
+        if not args.no_batched:
+            out["small_plain"] = run_small(local)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         out["cpu_baseline"] = cpu_baseline(w)
     if world > 1:
@@ -338,6 +340,40 @@ def run_ours(args):
         dist.destroy_process_group()
     if rank == 0:
         print(json.dumps(out), flush=True)
+
+
+def run_small(local, steps=400):
+    """The 4,096-bead plain workload (one type, 200 A periodic box, WCA table,
+    20 / 25 A radii, rebuild checks every 20 steps): device time per step with
+    one mb2_step call per step and with mb2_run (steps between rebuild checks
+    replayed from a CUDA graph)."""
+    import torch
+    from mars_md_b200 import workloads as W
+    from mars_md_b200.engine import Context, setup_workload, step_params
+    w = W.plain_bd()
+    res = {"metric": "particle-steps/s, small plain system: step calls vs graph-replayed run",
+           "beads": w.n, "steps": steps}
+    for mode in ("step", "run"):
+        ctx = Context(w.n, device=local)
+        dev = setup_workload(ctx, w, device=f"cuda:{local}")
+        prm = step_params(w)
+        ctx.run(dev["pos"], dev["fe"], dev["type"], None, 1, 40, prm)  # warm-up and capture
+        torch.cuda.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        if mode == "step":
+            for s in range(41, 41 + steps):
+                ctx.step(dev["pos"], dev["fe"], dev["type"], None, s, prm)
+        else:
+            ctx.run(dev["pos"], dev["fe"], dev["type"], None, 41, steps, prm)
+        b.record()
+        torch.cuda.synchronize()
+        ms = a.elapsed_time(b)
+        res[f"us_per_step_{mode}"] = 1e3 * ms / steps
+        res[f"value_{mode}"] = w.n * steps / (ms / 1e3)
+        ctx.close()
+    res["ratio"] = res["value_run"] / res["value_step"]
+    return res
 
 
 def run_batched(local, period_steps=20):

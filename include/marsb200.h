@@ -344,6 +344,18 @@ MB2_API int mb2_step(mb2_context* ctx, float* pos4, float* force_energy4, const 
              const uint32_t* flags, uint32_t n, uint64_t step, const mb2_step_params* params,
              void* stream);
 
+/* Steps first_step .. first_step + num_steps - 1, with the results of one
+ * mb2_step call per step (the loop of SimManager::run over one patch,
+ * src/SimManager.cpp:337-504). The BD steps that are not rebuild checks
+ * replay one CUDA graph of the step body, the step number read from a device
+ * counter, so that small systems are not bound by launch overhead; the graph
+ * is captured on first use and again whenever a pointer, size or parameter it
+ * bakes in changes. Rebuild checks, Langevin steps and steps while per-stage
+ * profiling is on run as mb2_step. */
+MB2_API int mb2_run(mb2_context* ctx, float* pos4, float* force_energy4, const int* type_ids,
+            const uint32_t* flags, uint32_t n, uint64_t first_step, uint32_t num_steps,
+            const mb2_step_params* params, void* stream);
+
 /* --- output ------------------------------------------------------------------
  * The output side of SimManager for one system (src/SimManager.cpp:318-330
  * initialize_output_writers, :541-575 handle_output): a DCD trajectory

@@ -107,6 +107,7 @@ def load(path: str = LIB_PATH):
     L.mb2_bd_seed.argtypes = [u64, u64, u64]
     L.mb2_philox.argtypes = [vp, u64, u32, u32, u32, u32, vp, vp, vp]
     L.mb2_step.argtypes = [vp, vp, vp, vp, vp, u32, u64, C.POINTER(StepParams), vp]
+    L.mb2_run.argtypes = [vp, vp, vp, vp, vp, u32, u64, u32, C.POINTER(StepParams), vp]
     L.mb2_set_lanes_per_row.argtypes = [vp, i]
     L.mb2_set_cell_level_offset.argtypes = [vp, i]
     L.mb2_cell_level.argtypes = [vp, C.POINTER(C.c_int)]

@@ -106,6 +106,12 @@ struct mb2_context {
 
 	// Optional per-stage CUDA-event timing on the launching stream.
 	bool profiling = false;
+	// mb2_run: the replayed graph of one step body between rebuild checks, the
+	// values it bakes in, its kernel launches and the device step counter.
+	cudaGraphExec_t run_graph = nullptr;
+	std::vector<uint64_t> run_key;
+	unsigned long long run_launches = 0;
+	DevBuf<unsigned long long> step_d;
 	std::vector<std::pair<cudaEvent_t, cudaEvent_t>> prof[MB2_NUM_STAGES];
 };
 
@@ -152,6 +158,9 @@ int guarded(mb2_context* ctx, F&& f) {
 }
 
 void require(bool cond, int code, const char* msg) {
+	if (!cond) throw Error{code, msg};
+}
+void require(bool cond, int code, const std::string& msg) {
 	if (!cond) throw Error{code, msg};
 }
 
@@ -575,6 +584,7 @@ int mb2_destroy(mb2_context* ctx) {
 			cudaEventDestroy(be.second);
 		}
 	if (ctx->pinned) cudaFreeHost(ctx->pinned);
+	if (ctx->run_graph) cudaGraphExecDestroy(ctx->run_graph);
 	delete ctx;  // device buffers free themselves
 	return MB2_OK;
 }
@@ -1109,60 +1119,199 @@ int mb2_philox(mb2_context* ctx, uint64_t seed, uint32_t ctr0, uint32_t ctr1, ui
 	return guarded(ctx, [&] { philox_draws(seed, ctr0, ctr1, ctr2, n, out4, normals4, S(stream)); });
 }
 
+}  // extern "C"
+
+namespace {
+
+void check_step(mb2_context* ctx, float* pos4, float* force_energy4, const int* type_ids,
+				uint32_t n, const mb2_step_params* prm, const char* what) {
+	require(prm && (n == 0 || (pos4 && force_energy4 && type_ids)), MB2_ERR_ARG,
+			std::string(what) + ": null argument");
+	require(ctx->types_set, MB2_ERR_STATE, std::string(what) + ": call mb2_set_particle_types");
+	require(prm->num_dihedrals == 0 || ctx->bonded_count[2] > 0, MB2_ERR_STATE,
+			std::string(what) + ": dihedrals without dihedral tables");
+	require(prm->integrator == 0 || prm->integrator == 1, MB2_ERR_ARG,
+			std::string(what) + ": integrator is 0 (BD) or 1 (Langevin)");
+	require(prm->integrator == 0 || (prm->mom4 && ctx->langevin_types > 0), MB2_ERR_STATE,
+			std::string(what) + ": Langevin needs momenta and mb2_set_langevin_types");
+}
+
+// One whole step (the body of mb2_step).
+void step_once(mb2_context* ctx, float4* pos, float4* fe, const int* type_ids,
+			   const uint32_t* flags, uint32_t n, uint64_t step, const mb2_step_params* prm,
+			   cudaStream_t st) {
+	StageScope whole(ctx, MB2_STAGE_STEP, st);
+	// The reference clears ForceEnergy (Patch.cpp:56) and accumulates every
+	// term into it. Here pair forces stay in the Z-ordered accumulator and
+	// the integrate kernel gathers them, adding what the bonded kernels
+	// wrote; ForceEnergy is cleared only when those run.
+	const bool bonded = step_has_bonded(prm);
+	if (bonded) MB2_CUDA(cudaMemsetAsync(fe, 0, static_cast<size_t>(n) * sizeof(float4), st));
+	// Rebuild schedule and skin check (Patch.cpp:86-108)
+	const bool at_period = prm->rebuild_period == 0 || (step - 1) % prm->rebuild_period == 0;
+	bool rebuild = at_period || !ctx->built || ctx->built_n != n;
+	const float skin = prm->pairlist_cutoff - prm->cutoff;
+	if (rebuild && prm->rebuild_period != 0 && ctx->built && ctx->built_n == n && skin > 0.0f)
+		rebuild = max_disp(ctx, pos, n, st) > skin * 0.5f;
+	ctx->last_cutoff = prm->cutoff;
+	if (rebuild)
+		build(ctx, pos, type_ids, n, prm->pairlist_cutoff, st);  // packs sorted_pos
+	else if (n)
+		pack_sorted_positions(pos, type_ids, ctx->s2o.ptr, n, ctx->sorted_pos.ptr, st);
+	if (n == 0) return;
+	pair_kernel(ctx, n, prm->cutoff, prm->get_energy, st);
+	bonded_stage(ctx, pos, fe, prm, prm->get_energy, st);
+	StageScope scope(ctx, MB2_STAGE_INTEGRATE, st);
+	if (prm->integrator == 1) {
+		// Patch::integrate_motion, Langevin branch (Patch.cpp:290-335).
+		baoab_integrate_gather(pos, reinterpret_cast<float4*>(prm->mom4), fe,
+							   ctx->force_sorted.ptr, ctx->inv.ptr, bonded ? 1 : 0, type_ids, flags,
+							   n, ctx->types, ctx->box, prm->dt, prm->kT,
+							   static_cast<uint32_t>(step),
+							   mb2_bd_seed(prm->seed, prm->patch_id, step), 0u, prm->efield,
+							   prm->deferred_kick_pending ? 1 : 0, st);
+		return;
+	}
+	BdParams p{prm->dt, prm->kT, static_cast<uint32_t>(step),
+			   mb2_bd_seed(prm->seed, prm->patch_id, step), 0u,
+			   {prm->efield[0], prm->efield[1], prm->efield[2]}};
+	bd_integrate_gather(pos, fe, ctx->force_sorted.ptr, ctx->inv.ptr, type_ids, flags, n,
+						ctx->types, ctx->box, p, bonded ? 1 : 0, st);
+}
+
+// A BD step that is not a rebuild check, with the step number taken from
+// ctx->step_d and advanced by one at the end: the body mb2_run captures.
+void step_body_replayable(mb2_context* ctx, float4* pos, float4* fe, const int* type_ids,
+						  const uint32_t* flags, uint32_t n, const mb2_step_params* prm,
+						  cudaStream_t st) {
+	const bool bonded = step_has_bonded(prm);
+	if (bonded) MB2_CUDA(cudaMemsetAsync(fe, 0, static_cast<size_t>(n) * sizeof(float4), st));
+	pack_sorted_positions(pos, type_ids, ctx->s2o.ptr, n, ctx->sorted_pos.ptr, st);
+	pair_kernel(ctx, n, prm->cutoff, prm->get_energy, st);
+	bonded_stage(ctx, pos, fe, prm, prm->get_energy, st);
+	BdParams p{prm->dt, prm->kT, 0u, 0u, 0u, {prm->efield[0], prm->efield[1], prm->efield[2]}};
+	bd_integrate_gather(pos, fe, ctx->force_sorted.ptr, ctx->inv.ptr, type_ids, flags, n,
+						ctx->types, ctx->box, p, bonded ? 1 : 0, st, ctx->step_d.ptr, prm->seed,
+						prm->patch_id);
+	step_counter_add(ctx->step_d.ptr, 1, st);
+}
+
+uint64_t fbits(float f) {
+	uint32_t u;
+	std::memcpy(&u, &f, 4);
+	return u;
+}
+
+template <class T>
+void push_words(std::vector<uint64_t>& k, const T& v) {
+	static_assert(sizeof(T) % 4 == 0, "word-sized fields only");
+	uint32_t w[sizeof(T) / 4];
+	std::memcpy(w, &v, sizeof(T));
+	for (uint32_t x : w) k.push_back(x);
+}
+
+// Every value the captured step body bakes into its launches.
+std::vector<uint64_t> run_graph_key(const mb2_context* ctx, const float4* pos, const float4* fe,
+									const int* type_ids, const uint32_t* flags, uint32_t n,
+									const mb2_step_params* prm) {
+	auto P = [](const void* p) { return static_cast<uint64_t>(reinterpret_cast<uintptr_t>(p)); };
+	std::vector<uint64_t> k = {
+		P(pos), P(fe), P(type_ids), P(flags), n, fbits(prm->cutoff), fbits(prm->dt),
+		fbits(prm->kT), prm->seed, prm->patch_id, fbits(prm->efield[0]), fbits(prm->efield[1]),
+		fbits(prm->efield[2]), static_cast<uint64_t>(prm->get_energy), P(prm->bonds2),
+		P(prm->bond_table_idx), prm->num_bonds, P(prm->angles4), P(prm->angle_table_idx),
+		prm->num_angles, P(prm->dihedrals4), P(prm->dihedral_table_idx), prm->num_dihedrals,
+		P(prm->restraint_ids), P(prm->restraint_anchors4), P(prm->restraint_k),
+		prm->num_restraints, P(ctx->nbr.ptr), P(ctx->row_len.ptr), ctx->cap,
+		static_cast<uint64_t>(ctx->lanes), P(ctx->sorted_pos.ptr), P(ctx->s2o.ptr),
+		P(ctx->inv.ptr), P(ctx->force_sorted.ptr), P(ctx->energy.ptr), P(ctx->step_d.ptr),
+		P(ctx->bonded_tables[0].ptr), P(ctx->bonded_tables[1].ptr), P(ctx->bonded_tables[2].ptr),
+		static_cast<uint64_t>(ctx->pt.num_types), ctx->pt.total_bins, P(ctx->pt.refs),
+		P(ctx->pt.offsets), static_cast<uint64_t>(ctx->pt.uniform), fbits(ctx->pt.uniform_ref.start),
+		fbits(ctx->pt.uniform_ref.step_inv), static_cast<uint64_t>(ctx->pt.uniform_ref.last),
+		P(ctx->pt.bin_force), P(ctx->pt.bin_energy), P(ctx->pt.terms),
+		static_cast<uint64_t>(ctx->types.num_types), P(ctx->types.charge), P(ctx->types.diffusion),
+		P(ctx->types.pmf_offset), P(ctx->types.pmf_count), P(ctx->types.terms),
+		P(ctx->types.force_grid_id), P(ctx->types.force_grid_scale), P(ctx->types.grids),
+		static_cast<uint64_t>(ctx->types.num_grids)};
+	push_words(k, ctx->pt.solvent);
+	push_words(k, ctx->box);
+	return k;
+}
+
+}  // namespace
+
+extern "C" {
+
 int mb2_step(mb2_context* ctx, float* pos4, float* force_energy4, const int* type_ids,
 			 const uint32_t* flags, uint32_t n, uint64_t step, const mb2_step_params* prm,
 			 void* stream) {
 	return guarded(ctx, [&] {
-		require(prm && (n == 0 || (pos4 && force_energy4 && type_ids)), MB2_ERR_ARG,
-				"mb2_step: null argument");
-		require(ctx->types_set, MB2_ERR_STATE, "mb2_step: call mb2_set_particle_types");
+		check_step(ctx, pos4, force_energy4, type_ids, n, prm, "mb2_step");
+		step_once(ctx, reinterpret_cast<float4*>(pos4), reinterpret_cast<float4*>(force_energy4),
+				  type_ids, flags, n, step, prm, S(stream));
+	});
+}
+
+int mb2_run(mb2_context* ctx, float* pos4, float* force_energy4, const int* type_ids,
+			const uint32_t* flags, uint32_t n, uint64_t first_step, uint32_t num_steps,
+			const mb2_step_params* prm, void* stream) {
+	return guarded(ctx, [&] {
+		check_step(ctx, pos4, force_energy4, type_ids, n, prm, "mb2_run");
 		const cudaStream_t st = S(stream);
-		StageScope whole(ctx, MB2_STAGE_STEP, st);
 		float4* pos = reinterpret_cast<float4*>(pos4);
 		float4* fe = reinterpret_cast<float4*>(force_energy4);
-		// The reference clears ForceEnergy (Patch.cpp:56) and accumulates every
-		// term into it. Here pair forces stay in the Z-ordered accumulator and
-		// the integrate kernel gathers them, adding what the bonded kernels
-		// wrote; ForceEnergy is cleared only when those run.
-		const bool bonded = step_has_bonded(prm);
-		require(prm->num_dihedrals == 0 || ctx->bonded_count[2] > 0, MB2_ERR_STATE,
-				"mb2_step: dihedrals without dihedral tables");
-		require(prm->integrator == 0 || prm->integrator == 1, MB2_ERR_ARG,
-				"mb2_step: integrator is 0 (BD) or 1 (Langevin)");
-		require(prm->integrator == 0 || (prm->mom4 && ctx->langevin_types > 0), MB2_ERR_STATE,
-				"mb2_step: Langevin needs momenta and mb2_set_langevin_types");
-		if (bonded)
-			MB2_CUDA(cudaMemsetAsync(fe, 0, static_cast<size_t>(n) * sizeof(float4), st));
-		// Rebuild schedule and skin check (Patch.cpp:86-108)
-		const bool at_period = prm->rebuild_period == 0 || (step - 1) % prm->rebuild_period == 0;
-		bool rebuild = at_period || !ctx->built || ctx->built_n != n;
-		const float skin = prm->pairlist_cutoff - prm->cutoff;
-		if (rebuild && prm->rebuild_period != 0 && ctx->built && ctx->built_n == n && skin > 0.0f)
-			rebuild = max_disp(ctx, pos, n, st) > skin * 0.5f;
-		ctx->last_cutoff = prm->cutoff;
-		if (rebuild)
-			build(ctx, pos, type_ids, n, prm->pairlist_cutoff, st);  // packs sorted_pos
-		else if (n)
-			pack_sorted_positions(pos, type_ids, ctx->s2o.ptr, n, ctx->sorted_pos.ptr, st);
-		if (n == 0) return;
-		pair_kernel(ctx, n, prm->cutoff, prm->get_energy, st);
-		bonded_stage(ctx, pos, fe, prm, prm->get_energy, st);
-		StageScope scope(ctx, MB2_STAGE_INTEGRATE, st);
-		if (prm->integrator == 1) {
-			// Patch::integrate_motion, Langevin branch (Patch.cpp:290-335).
-			baoab_integrate_gather(pos, reinterpret_cast<float4*>(prm->mom4), fe,
-								   ctx->force_sorted.ptr, ctx->inv.ptr, bonded ? 1 : 0, type_ids,
-								   flags, n, ctx->types, ctx->box, prm->dt, prm->kT,
-								   static_cast<uint32_t>(step),
-								   mb2_bd_seed(prm->seed, prm->patch_id, step), 0u, prm->efield,
-								   prm->deferred_kick_pending ? 1 : 0, st);
-			return;
+		// Graph replay serves BD steps that are not rebuild checks; the rest (and
+		// every step while per-stage profiling is on) run as mb2_step does.
+		const bool replayable = prm->integrator == 0 && prm->rebuild_period != 0 && n > 0;
+		ctx->step_d.ensure(1);
+		bool counter_set = false;
+		for (uint32_t k = 0; k < num_steps; ++k) {
+			const uint64_t step = first_step + k;
+			const bool check = (step - 1) % (prm->rebuild_period ? prm->rebuild_period : 1) == 0;
+			if (!replayable || check || ctx->profiling || !ctx->built || ctx->built_n != n) {
+				step_once(ctx, pos, fe, type_ids, flags, n, step, prm, st);
+				counter_set = false;
+				continue;
+			}
+			ctx->force_sorted.ensure(n);  // no allocation inside the capture
+			const std::vector<uint64_t> key = run_graph_key(ctx, pos, fe, type_ids, flags, n, prm);
+			if (!ctx->run_graph || key != ctx->run_key) {
+				if (ctx->run_graph) {
+					MB2_CUDA(cudaGraphExecDestroy(ctx->run_graph));
+					ctx->run_graph = nullptr;
+				}
+				cudaStream_t cs;
+				MB2_CUDA(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
+				cudaGraph_t g = nullptr;
+				const unsigned long long l0 = g_launches;
+				MB2_CUDA(cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal));
+				try {
+					step_body_replayable(ctx, pos, fe, type_ids, flags, n, prm, cs);
+				} catch (...) {
+					cudaStreamEndCapture(cs, &g);
+					if (g) cudaGraphDestroy(g);
+					cudaStreamDestroy(cs);
+					g_launches = l0;
+					throw;
+				}
+				const cudaError_t ec = cudaStreamEndCapture(cs, &g);
+				ctx->run_launches = g_launches - l0;
+				g_launches = l0;  // counted at each replay instead
+				cudaStreamDestroy(cs);
+				MB2_CUDA(ec);
+				const cudaError_t ei = cudaGraphInstantiate(&ctx->run_graph, g, 0);
+				cudaGraphDestroy(g);
+				MB2_CUDA(ei);
+				ctx->run_key = key;
+			}
+			if (!counter_set) {
+				step_counter_set(ctx->step_d.ptr, step, st);
+				counter_set = true;
+			}
+			MB2_CUDA(cudaGraphLaunch(ctx->run_graph, st));
+			g_launches += ctx->run_launches;
 		}
-		BdParams p{prm->dt, prm->kT, static_cast<uint32_t>(step),
-				   mb2_bd_seed(prm->seed, prm->patch_id, step), 0u,
-				   {prm->efield[0], prm->efield[1], prm->efield[2]}};
-		bd_integrate_gather(pos, fe, ctx->force_sorted.ptr, ctx->inv.ptr, type_ids, flags, n,
-							ctx->types, ctx->box, p, bonded ? 1 : 0, st);
 	});
 }
 

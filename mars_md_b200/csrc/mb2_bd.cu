@@ -184,18 +184,32 @@ __global__ void __launch_bounds__(256) bd_kernel(float4* __restrict__ pos, float
 	pos[i] = bd_update(p, f.x, f.y, f.z, ty.diffusion[type], xi, box, bp);
 }
 
+__device__ __forceinline__ uint64_t mix_seed(uint64_t seed, uint64_t patch, uint64_t step) {
+	// Patch::integrate_motion seed mixing (Patch.cpp:252-254).
+	return (seed * 0x9E3779B97F4A7C15ULL) ^ (patch << 32) ^ (step * 0xBF58476D1CE4E5B9ULL);
+}
+
 // Fused-step variant: the pair force is gathered from the Z-ordered
 // accumulator through the inverse permutation (random reads, coalesced
 // writes), added to what the bonded kernels left in ForceEnergy when any ran
 // (read_fe), and the result stored to ForceEnergy as the reference leaves it
 // after integrate_motion; then the grid force, noise and update as bd_kernel.
+// step_ptr (graph replay): the step number comes from device memory and the
+// Philox key is mixed here from (seed, patch_id, step), as the host does for
+// bp.base_seed otherwise.
 __global__ void __launch_bounds__(256) bd_gather_kernel(
 	float4* __restrict__ pos, float4* __restrict__ fe, const float4* __restrict__ fs,
 	const uint32_t* __restrict__ inv, const int* __restrict__ type_ids,
 	const uint32_t* __restrict__ flags, uint32_t n, TypeTable ty, Box box, BdParams bp,
-	int read_fe) {
+	int read_fe, const unsigned long long* __restrict__ step_ptr, uint64_t seed,
+	uint64_t patch_id) {
 	const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
 	if (i >= n) return;
+	if (step_ptr) {
+		const uint64_t step = *step_ptr;
+		bp.step = static_cast<uint32_t>(step);
+		bp.base_seed = mix_seed(seed, patch_id, step);
+	}
 	float4 f = fs[inv[i]];
 	if (read_fe) {
 		const float4 ext = fe[i];
@@ -327,11 +341,6 @@ __global__ void __launch_bounds__(256) baoab_last_kernel(float4* __restrict__ mo
 	mom[i] = m;
 }
 
-__device__ __forceinline__ uint64_t mix_seed(uint64_t seed, uint64_t patch, uint64_t step) {
-	// Patch::integrate_motion seed mixing (Patch.cpp:252-254).
-	return (seed * 0x9E3779B97F4A7C15ULL) ^ (patch << 32) ^ (step * 0xBF58476D1CE4E5B9ULL);
-}
-
 // Batched replicas: particle i of system s = sys_of[i] integrates as a plain
 // step of system s with seed (seed + s) would (counter = index in the
 // system, its own box); the step number comes from device memory so that a
@@ -386,10 +395,12 @@ void bd_integrate(float4* pos, float4* fe, const int* type_ids, const uint32_t* 
 void bd_integrate_gather(float4* pos, float4* fe, const float4* force_sorted, const uint32_t* inv,
 						 const int* type_ids, const uint32_t* flags, uint32_t n,
 						 const TypeTable& types, const Box& box, const BdParams& p, int read_fe,
-						 cudaStream_t st) {
+						 cudaStream_t st, const unsigned long long* step_ptr, uint64_t seed,
+						 uint64_t patch_id) {
 	if (n == 0) return;
 	MB2_LAUNCH bd_gather_kernel<<<(n + 255) / 256, 256, 0, st>>>(pos, fe, force_sorted, inv, type_ids,
-																 flags, n, types, box, p, read_fe);
+																 flags, n, types, box, p, read_fe,
+																 step_ptr, seed, patch_id);
 }
 
 void baoab_integrate(float4* pos, float4* mom, float4* fe, const int* type_ids,

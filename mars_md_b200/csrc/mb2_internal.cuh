@@ -282,10 +282,14 @@ struct BdParams {
 void bd_integrate(float4* pos, float4* fe, const int* type_ids, const uint32_t* flags, uint32_t n,
 				  const TypeTable& types, const Box& box, const BdParams& p, cudaStream_t st);
 // The fused step's integrate: force = force_sorted[inv[i]] (+ fe[i] if read_fe).
+// step_ptr non-null: the step number is read from device memory at run time
+// (a replayed graph) and the Philox key mixed on the device from seed and
+// patch_id; p.step and p.base_seed are then unused.
 void bd_integrate_gather(float4* pos, float4* fe, const float4* force_sorted, const uint32_t* inv,
 						 const int* type_ids, const uint32_t* flags, uint32_t n,
 						 const TypeTable& types, const Box& box, const BdParams& p, int read_fe,
-						 cudaStream_t st);
+						 cudaStream_t st, const unsigned long long* step_ptr = nullptr,
+						 uint64_t seed = 0, uint64_t patch_id = 0);
 // Langevin BAOAB (Integrator/BAOAB.h): with grids, ForceEnergy += position
 // force for every particle; `pending` applies the deferred closing half-kick
 // first; then B-A-O-A and wrap. Noise key (seed, base_ctr + i, step, stream 0x1356914).

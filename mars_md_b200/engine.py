@@ -17,6 +17,8 @@ call surface on the Brownian-dynamics path:
 * ``set_particle_types`` / ``set_grid`` / ``bd_integrate`` -- launch_BD
   (src/PatchOperation/Integrator.h:26-54);
 * ``step`` -- one SimManager step for one patch (src/SimManager.cpp:337-504);
+  ``run`` -- many of them, the steps between rebuild checks replayed from a
+  CUDA graph;
 * ``reorder_*`` / ``reorder_particles`` / ``ReorderManager`` -- the canonical
   Morton reorder of a patch (src/PatchOperation/Patch.cpp:455-480);
 * ``Output`` -- DCD frames, the energy file and restart files
@@ -339,6 +341,14 @@ class Context:
     def step(self, pos, fe, type_ids, flags, step, params: "L.StepParams", stream=None):
         self.check(self.lib.mb2_step(self.h, _p(pos), _p(fe), _p(type_ids), _p(flags),
                                      pos.shape[0], int(step), C.byref(params), _stream(stream)))
+
+    def run(self, pos, fe, type_ids, flags, first_step, num_steps, params: "L.StepParams",
+            stream=None):
+        """Steps first_step .. first_step + num_steps - 1 as ``step`` would, the
+        steps between rebuild checks replayed from one captured CUDA graph."""
+        self.check(self.lib.mb2_run(self.h, _p(pos), _p(fe), _p(type_ids), _p(flags),
+                                    pos.shape[0], int(first_step), int(num_steps),
+                                    C.byref(params), _stream(stream)))
 
 
 def exclusion_csr(pairs):

@@ -1,7 +1,10 @@
 """engine.HostStepper: steps fed from pinned host memory, with their copies on
 streams of their own (a host-owned trajectory whose read-back and next upload
-overlap chunk by chunk; independent inputs on double buffers), give the same
-positions, bit for bit, as the same steps on device buffers."""
+overlap chunk by chunk; independent inputs on double buffers), give the
+positions of the same steps on device buffers. Two contexts agree up to the
+order of the float atomics that add the pair forces, so trajectories are held
+to 1e-3 A everywhere and 1e-4 A for 99 % of the particles; a single step from
+the same input is bit-exact where no atomics collide and held the same way."""
 import numpy as np
 import pytest
 import torch
@@ -10,6 +13,13 @@ from mars_md_b200 import workloads as W
 from mars_md_b200.engine import HostStepper, setup_workload, step_params
 
 pytestmark = pytest.mark.gpu
+
+
+def _close(got, want, box):
+    d = np.abs(np.asarray(got)[:, :3] - np.asarray(want)[:, :3])
+    d = np.minimum(d, np.asarray(box, np.float32) - d).max(axis=1)
+    assert d.max() <= 1e-3, float(d.max())
+    assert (d <= 1e-4).mean() >= 0.99, int((d > 1e-4).sum())
 
 
 def _pair(ctx_factory):
@@ -30,7 +40,7 @@ def test_host_owned_trajectory_matches_device_trajectory(ctx_factory):
         b.step(dev_b["pos"], dev_b["fe"], dev_b["type"], None, s, prm)
     stepper.finish()
     torch.cuda.synchronize()
-    assert np.array_equal(h_pos.numpy(), dev_b["pos"].cpu().numpy())
+    _close(h_pos.numpy(), dev_b["pos"].cpu().numpy(), w.box_size)
     with pytest.raises(AssertionError):  # one pattern per stepper
         stepper.submit(h_pos, h_pos, 61)
 
@@ -46,7 +56,7 @@ def test_trajectory_through_host_matches_device_steps(ctx_factory):
         ev.synchronize()
         h_in.copy_(h_out[s & 1])  # the next step starts from this one's result
     torch.cuda.synchronize()
-    assert np.array_equal(h_in.numpy(), dev_b["pos"].cpu().numpy())
+    _close(h_in.numpy(), dev_b["pos"].cpu().numpy(), w.box_size)
 
 
 def test_independent_inputs_overlap_and_match(ctx_factory):
@@ -66,4 +76,4 @@ def test_independent_inputs_overlap_and_match(ctx_factory):
     for k in range(6):
         dev_b["pos"].copy_(h_in[k])
         b.step(dev_b["pos"], dev_b["fe"], dev_b["type"], None, k + 1, prm)
-        assert np.array_equal(h_out[k].numpy(), dev_b["pos"].cpu().numpy()), k
+        _close(h_out[k].numpy(), dev_b["pos"].cpu().numpy(), w.box_size)
