@@ -253,6 +253,32 @@ static void patch_stage_test(const Resource& res) {
 		moved = std::max(moved, std::fabs(a[i].x - h[i].x));
 	}
 	EXPECT(worst <= 1e-4f && moved > 0.1f, "Patch stages equal the fused step over 5 steps");
+
+	// Many steps in one call (graph-replayed between rebuild checks) against
+	// one mb2_step per step, across two rebuild checks.
+	B200Patch looped(res, n), ran(res, n);
+	setup(looped);
+	setup(ran);
+	DeviceBuffer<Vector3> pos_c(n, res), fe_c(n, res), pos_d(n, res), fe_d(n, res);
+	pos_c.copy_from_host(h);
+	pos_d.copy_from_host(h);
+	for (uint64_t step = 1; step <= 30; ++step)
+		check(mb2_step(looped.handle(), reinterpret_cast<float*>(pos_c.data()),
+					   reinterpret_cast<float*>(fe_c.data()), d_types.data(), nullptr, n, step, &prm,
+					   nullptr),
+			  looped.handle(), "mb2_step");
+	check(mb2_run(ran.handle(), reinterpret_cast<float*>(pos_d.data()),
+				  reinterpret_cast<float*>(fe_d.data()), d_types.data(), nullptr, n, 1, 30, &prm,
+				  nullptr),
+		  ran.handle(), "mb2_run");
+	std::vector<Vector3> c, d;
+	pos_c.copy_to_host(c);
+	pos_d.copy_to_host(d);
+	float worst_run = 0.0f;
+	for (int i = 0; i < n; ++i)
+		worst_run = std::max({worst_run, std::fabs(c[i].x - d[i].x), std::fabs(c[i].y - d[i].y),
+							  std::fabs(c[i].z - d[i].z)});
+	EXPECT(worst_run <= 1e-3f, "mb2_run equals one mb2_step per step over 30 steps");
 }
 
 // Langevin through the Patch mirror: the deferred closing kick is owed after a
