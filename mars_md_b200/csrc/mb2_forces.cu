@@ -212,7 +212,7 @@ __device__ __forceinline__ void pair_scalar(const float4& pi, float2 npi, const 
 											const TRow& trow, const float* bin_f,
 											const float2* bin_e, const PairTermRef* arow,
 											const PairSolvent& sv, const Box& box,
-											float cutoff_sq, float4* force, float2& nxy, float& nz,
+											float cutoff_sq, float skip2, float4* force, float2& nxy, float& nz,
 											float& fe, double& e_acc, double& w_acc) {
 	// r = wrap_diff(pos[second] - pos[first])
 	// (pi - pj is exactly -(pj - pi) in round-to-nearest, so a sign flip suffices)
@@ -237,6 +237,10 @@ __device__ __forceinline__ void pair_scalar(const float4& pi, float2 npi, const 
 	const float dx = dxy.x, dy = dxy.y;
 	const float2 sq = __fmul2_rn(dxy, dxy);
 	const float d2v = __fadd_rn(__fadd_rn(sq.x, sq.y), __fmul_rn(dz, dz));
+	// d2v above skip2 = cutoff_sq (1 + 2^-20) or more makes RN(RN(sqrt)^2)
+	// exceed cutoff_sq, so the pair fails the reference's test below: such
+	// lanes, and whole warps in the rows' far ends, leave before the root.
+	if (d2v > skip2) return;
 	const float dist = __fsqrt_rn(d2v);
 	if (dist < 1e-6f || (cutoff_sq > 0.0f && __fmul_rn(dist, dist) > cutoff_sq)) return;
 	const PairTableRef t = trow(type_of(pj));
@@ -365,6 +369,7 @@ __global__ void __launch_bounds__(
 	const uint32_t cnt = valid ? row_len[i] : 0u;
 	// Entry k of row i: ((i / H) * cap + k) * H + i % H.
 	const uint32_t* col = nbr + (static_cast<size_t>(i / H) * cap) * H + (i % H);
+	const float skip2 = cutoff_sq > 0.0f ? cutoff_sq * 1.000001f : INFINITY;
 	const float2 npi = make_float2(-pi.x, -pi.y);
 	float2 nxy = make_float2(0.0f, 0.0f);  // minus the i-force, x and y
 	float nz = 0.0f, fe = 0.0f;
@@ -379,10 +384,10 @@ __global__ void __launch_bounds__(
 		const float4 p0 = sorted_pos[j0];
 		const float4 p1 = sorted_pos[j1];
 		pair_scalar<kEnergy, kAllPeriodic, kTerms>(pi, npi, p0, j0, e0 & kOrientBit, trow, bin_f,
-												   bin_e, arow, sv, box, cutoff_sq, force, nxy, nz,
+												   bin_e, arow, sv, box, cutoff_sq, skip2, force, nxy, nz,
 												   fe, e_acc, w_acc);
 		pair_scalar<kEnergy, kAllPeriodic, kTerms>(pi, npi, p1, j1, e1 & kOrientBit, trow, bin_f,
-												   bin_e, arow, sv, box, cutoff_sq, force, nxy, nz,
+												   bin_e, arow, sv, box, cutoff_sq, skip2, force, nxy, nz,
 												   fe, e_acc, w_acc);
 	}
 	if (t < cnt) {
@@ -390,7 +395,7 @@ __global__ void __launch_bounds__(
 		const uint32_t j = entry & ~kOrientBit;
 		pair_scalar<kEnergy, kAllPeriodic, kTerms>(pi, npi, sorted_pos[j], j, entry & kOrientBit,
 												   trow, bin_f, bin_e, arow, sv, box, cutoff_sq,
-												   force, nxy, nz, fe, e_acc, w_acc);
+												   skip2, force, nxy, nz, fe, e_acc, w_acc);
 	}
 	// The lanes' sums of minus the i-force, then negated (exact).
 	float fx = nxy.x, fy = nxy.y, fz = nz;
