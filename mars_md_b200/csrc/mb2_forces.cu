@@ -305,11 +305,11 @@ struct SystemBoxes {
 };
 
 // Resident 256-thread blocks per SM each pair-kernel variant is compiled for.
-// The force-only tabulated kernel is issue-bound on gather latency: 8 blocks
-// (32 registers, full occupancy) run it 6 % faster than the 40 registers it
-// takes unbounded, in spite of a few bytes of spill; the energy and
-// analytical variants need their registers, and the batched variant (box
-// per row) spills heavily at 32.
+// The force-only tabulated kernel is bound by issue and gather latency: 8
+// blocks (32 registers, full occupancy) ran it 6 % faster than the 40
+// registers it takes unbounded, in spite of a few bytes of spill (none in the
+// uniform-table variant); the energy and analytical variants need their
+// registers, and the batched variant (box per row) spills heavily at 32.
 template <bool kEnergy, bool kTerms, bool kOneBox>
 constexpr int pair_min_blocks() {
 	return !kOneBox ? 1 : (kTerms ? 3 : (kEnergy ? 5 : 8));

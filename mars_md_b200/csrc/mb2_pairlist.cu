@@ -238,9 +238,11 @@ struct RowWriter {
 // keeps candidate order (runs of consecutive sorted j), which keeps the force
 // kernel's gathers local.
 // Seven resident blocks per SM (32 registers, a little spill): the walk is
-// bound by the latency of its dependent loads (cell ranges, then candidates)
-// and more warps hide it. Measured on the 2,097,152-bead workload: 7.1 ms per
-// build at 7 blocks, 7.7 at 6 (40 registers), 7.9 at 5 (48 registers).
+// bound by instruction issue and the latency of its dependent loads (cell
+// ranges, then candidates), and more warps hide the latency. Measured on the
+// 2,097,152-bead workload when the budget was set: 7.1 ms per build at 7
+// blocks, 7.7 at 6 (40 registers), 7.9 at 5 (48 registers); with the group
+// test and the voted exact test, 6.0 ms at 7 blocks and 6.05 at 6.
 // kFull: some periodic axis is spanned whole by the group's candidate cells
 // (small boxes); without it the candidate test needs no minimum-image wrap.
 template <bool kExcl, bool kFull>
