@@ -190,6 +190,10 @@ __device__ __forceinline__ float cell_gap(const WalkGrid& wg, int ax, int nx, in
 // 31 left over plus 32 new).
 constexpr uint32_t kCellBuf = 64;
 
+// Up to this many particles the pairlist is walked one warp per particle
+// (build_rows_kernel) instead of one warp per 32 (build_walk_kernel).
+constexpr uint32_t kRowWalkMaxN = 16384;
+
 // Periodic image offset of a buffered cell on axis ax: code bits 2ax..2ax+1
 // hold 1 (-size) or 2 (+size).
 __device__ __forceinline__ float image_shift(uint32_t code, int ax, const Box& box) {
@@ -501,6 +505,110 @@ __global__ void __launch_bounds__(256) export_kernel(const uint32_t* __restrict_
 	}
 }
 
+// Small systems: one warp per particle row. The lanes take the row's pruned
+// stencil cells 32 at a time (cells whose Morton code precedes the particle's
+// hold only earlier particles and are skipped), then walk their cells'
+// candidates in lockstep rounds, each lane its own cell, with the reference's
+// exact test; a round's hits are appended with two ballots (near entries from
+// the front of the row, far ones from the back, as the group walk does). The
+// group walk runs one warp per 32 particles and leaves most of the GPU idle
+// below a few tens of thousands of particles; here every particle has a warp.
+// Rows hold the same pairs in another order.
+template <bool kExcl>
+__global__ void __launch_bounds__(256) build_rows_kernel(
+	const float4* __restrict__ sorted_pos, const uint32_t* __restrict__ keys,
+	const uint32_t* __restrict__ s2o, const uint32_t* __restrict__ begin,
+	const uint32_t* __restrict__ end, const StencilEntry* __restrict__ stencil_g, int ns,
+	WalkGrid wg, uint32_t n, Box box, Exclusions ex, uint32_t* __restrict__ nbr, uint32_t cap,
+	int hshift, uint32_t* __restrict__ row_len, uint32_t* __restrict__ row_far,
+	unsigned long long* __restrict__ stats) {
+	const uint32_t i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+	if (i >= n) return;  // whole warp
+	const uint32_t lane = threadIdx.x & 31u;
+	const uint32_t lt = (1u << lane) - 1u;
+	const int cells = 1 << wg.m;
+	const uint32_t mask = static_cast<uint32_t>(cells - 1);
+	const float4 pi = sorted_pos[i];
+	const uint32_t c = keys[i] >> wg.shift;
+	const int cx = static_cast<int>(compact_by3(c >> 2));
+	const int cy = static_cast<int>(compact_by3(c >> 1));
+	const int cz = static_cast<int>(compact_by3(c));
+	const int a = static_cast<int>(s2o[i]);
+	int row_b = 0, row_e = 0, body = -1;
+	if (kExcl) {
+		if (ex.offsets && static_cast<uint32_t>(a) < ex.num_particles) {
+			row_b = ex.offsets[a];
+			row_e = ex.offsets[a + 1];
+		}
+		body = ex.rigid_body_id ? ex.rigid_body_id[a] : -1;
+	}
+	const uint32_t h = 1u << hshift;
+	uint32_t* base = nbr + (static_cast<size_t>(i >> hshift) * cap << hshift) + (i & (h - 1u));
+	uint32_t len = 0, far = 0;
+	for (int k0 = 0; k0 < ns; k0 += 32) {
+		uint32_t jb = 0, je = 0;
+		const int k = k0 + static_cast<int>(lane);
+		if (k < ns) {
+			const StencilEntry se = stencil_g[k];
+			int nx = cx + se.dx, ny = cy + se.dy, nz = cz + se.dz;
+			bool in = true;
+			if (box.periodic[0]) nx = static_cast<int>(static_cast<uint32_t>(nx + cells) & mask);
+			else in = in && nx >= 0 && nx < cells;
+			if (box.periodic[1]) ny = static_cast<int>(static_cast<uint32_t>(ny + cells) & mask);
+			else in = in && ny >= 0 && ny < cells;
+			if (box.periodic[2]) nz = static_cast<int>(static_cast<uint32_t>(nz + cells) & mask);
+			else in = in && nz >= 0 && nz < cells;
+			if (in) {
+				const uint32_t nc = (split_by3(static_cast<uint32_t>(nx)) << 2) |
+									(split_by3(static_cast<uint32_t>(ny)) << 1) |
+									split_by3(static_cast<uint32_t>(nz));
+				if (nc >= c) {  // earlier cells hold only earlier particles
+					const uint32_t b = begin[nc];
+					jb = b > i + 1u ? b : i + 1u;
+					je = end[nc];
+				}
+			}
+		}
+		while (__any_sync(0xFFFFFFFFu, jb < je)) {
+			bool hit = false, near = false;
+			uint32_t entry = 0;
+			if (jb < je) {
+				const uint32_t j = jb++;
+				const float4 pj = sorted_pos[j];
+				const float3 d = wrap_diff(box, __fsub_rn(pj.x, pi.x), __fsub_rn(pj.y, pi.y),
+										   __fsub_rn(pj.z, pi.z));
+				const float d2 = len2(d.x, d.y, d.z);
+				if (d2 <= wg.rc2) {
+					const int bj = static_cast<int>(s2o[j]);
+					if (!(kExcl && is_excluded(ex, bj, row_b, row_e, body))) {
+						hit = true;
+						near = d2 <= wg.split2;
+						entry = j | (bj < a ? kOrientBit : 0u);
+					}
+				}
+			}
+			const uint32_t nm = __ballot_sync(0xFFFFFFFFu, hit && near);
+			const uint32_t fm = __ballot_sync(0xFFFFFFFFu, hit && !near);
+			if (hit) {
+				// Position among all of the row's entries (for the capacity check)
+				// and the slot: near entries from the front, far from the back.
+				const uint32_t p = len + far + static_cast<uint32_t>(__popc((nm | fm) & lt));
+				const uint32_t slot = near ? len + static_cast<uint32_t>(__popc(nm & lt))
+										   : cap - 1u - (far + static_cast<uint32_t>(__popc(fm & lt)));
+				if (p < cap) base[static_cast<size_t>(slot) * h] = entry;
+			}
+			len += static_cast<uint32_t>(__popc(nm));
+			far += static_cast<uint32_t>(__popc(fm));
+		}
+	}
+	if (lane == 0) {
+		row_len[i] = len + far;
+		row_far[i] = far;
+		atomicAdd(stats, static_cast<unsigned long long>(len + far));
+		atomicMax(stats + 1, static_cast<unsigned long long>(len + far));
+	}
+}
+
 // Moves each row's far entries (stored backwards from the end of its cap
 // slots) to follow its near entries, so that a row is one contiguous run:
 // near entries in candidate order, then the far ones. One warp per slice of
@@ -601,6 +709,14 @@ void build_walk(const float4* sorted_pos, const uint32_t* keys, const uint32_t* 
 	bool full = false;
 	for (int a = 0; a < 3; ++a)
 		full = full || (box.periodic[a] && wg.emax + 2 * wg.radius[a] + 1 >= (1 << wg.m));
+	if (n <= kRowWalkMaxN) {
+		// One warp per particle (8 particles per 256-thread block).
+		auto rows = excl ? build_rows_kernel<true> : build_rows_kernel<false>;
+		MB2_LAUNCH rows<<<(n + 7) / 8, 256, 0, st>>>(sorted_pos, keys, s2o, begin, end, stencil,
+													 num_stencil, wg, n, box, ex, nbr, cap,
+													 hshift, row_len, row_far, stats);
+		return;
+	}
 	auto kern = excl ? (full ? build_walk_kernel<true, true> : build_walk_kernel<true, false>)
 					 : (full ? build_walk_kernel<false, true> : build_walk_kernel<false, false>);
 	// The stencil (used by the few groups that walk per particle) is read
