@@ -572,11 +572,34 @@ __global__ void __launch_bounds__(256) build_rows_kernel(
 				}
 			}
 		}
-		while (__any_sync(0xFFFFFFFFu, jb < je)) {
+		// The batch's candidate ranges laid end to end (a scan of their
+		// lengths); each round the lanes take the next 32 candidates, lane l
+		// finding the cell that holds candidate t0 + l by a binary search over
+		// the lanes' running totals.
+		// An empty cell (begin = end = 0) or one ending at i has jb >= je.
+		const uint32_t cnt = je > jb ? je - jb : 0u;
+		uint32_t incl = cnt;
+#pragma unroll
+		for (int o = 1; o < 32; o <<= 1) {
+			const uint32_t v = __shfl_up_sync(0xFFFFFFFFu, incl, o);
+			if (static_cast<int>(lane) >= o) incl += v;
+		}
+		const uint32_t total = __shfl_sync(0xFFFFFFFFu, incl, 31);
+		const uint32_t excl = incl - cnt;
+		for (uint32_t t0 = 0; t0 < total; t0 += 32u) {
+			const uint32_t t = t0 + lane;
+			int owner = 0;  // first lane whose running total exceeds t
+#pragma unroll
+			for (int step = 16; step > 0; step >>= 1) {
+				const uint32_t v = __shfl_sync(0xFFFFFFFFu, incl, owner + step - 1);
+				if (v <= t) owner += step;
+			}
+			const uint32_t ob = __shfl_sync(0xFFFFFFFFu, jb, owner & 31);
+			const uint32_t oe = __shfl_sync(0xFFFFFFFFu, excl, owner & 31);
 			bool hit = false, near = false;
 			uint32_t entry = 0;
-			if (jb < je) {
-				const uint32_t j = jb++;
+			if (t < total) {
+				const uint32_t j = ob + (t - oe);
 				const float4 pj = sorted_pos[j];
 				const float3 d = wrap_diff(box, __fsub_rn(pj.x, pi.x), __fsub_rn(pj.y, pi.y),
 										   __fsub_rn(pj.z, pi.z));
