@@ -192,10 +192,11 @@ constexpr uint32_t kCellBuf = 64;
 
 // Up to this many particles the pairlist is walked one warp per particle
 // (build_rows_kernel) instead of one warp per 32 (build_walk_kernel).
-// Measured per build, group walk against row walk: 65,536-bead polymers 0.81
-// vs 0.74 ms; uniform beads at 0.002 A^-3, 32,768: 1.04 vs 0.44 ms; 131,072:
-// 1.05 vs 1.03 ms; 524,288: 1.75 vs 3.70 ms.
-constexpr uint32_t kRowWalkMaxN = 65536;
+// Measured per build, group walk against row walk: 65,536-bead polymers 0.75
+// vs 0.30 ms; uniform beads at 0.002 A^-3, 32,768: 0.43 vs 0.34 ms (the group
+// walk's best at that size); 131,072: 1.06 vs 0.75 ms; 262,144: 1.36 vs
+// 1.48 ms; 524,288: 1.74 vs 2.30 ms; 2,097,152: 5.45 vs 10.6 ms.
+constexpr uint32_t kRowWalkMaxN = 131072;
 
 // Periodic image offset of a buffered cell on axis ax: code bits 2ax..2ax+1
 // hold 1 (-size) or 2 (+size).
