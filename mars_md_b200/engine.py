@@ -517,15 +517,18 @@ class HostStepper:
       into ``host_pos``, which the next ``advance`` uploads. The copies are
       split into chunks: chunk c of the next upload waits only for chunk c of
       the last read-back, so the two directions overlap each other.
-    * ``submit(host_in, host_out, step)``: independent inputs. Two device
-      position buffers alternate, so the upload of one submission and the
-      read-back of another overlap the steps on the device.
+    * ``submit(host_in, host_out, step)``: inputs that do not depend on the
+      previous result. Two device position buffers alternate, so the upload
+      of one submission and the read-back of another overlap the steps on
+      the device. The submissions step one context, whose pairlist follows
+      the rebuild schedule and skin check of ``Context.step``: the inputs
+      must be nearby states of one system, as successive frames are.
 
     A stepper serves one of the two patterns. Both return the CUDA event that
     marks the host buffer as written: read it (or change ``host_in``) only
-    after ``event.synchronize()``. ``finish()``
-    joins the copy streams into the compute stream, so that work queued there
-    afterwards (an event, a synchronize) follows every copy."""
+    after ``event.synchronize()``. ``finish()`` joins the copy streams into
+    the compute stream, so that work queued there afterwards (an event, a
+    synchronize) follows every copy."""
 
     def __init__(self, ctx: Context, type_ids, params: "L.StepParams", flags=None, n=None,
                  chunks: int = 8):
@@ -552,13 +555,16 @@ class HostStepper:
         self._mode = None
 
     def _use(self, mode):
-        assert self._mode in (None, mode), "a HostStepper serves either advance() or submit()"
+        if self._mode not in (None, mode):
+            raise RuntimeError("a HostStepper serves either advance() or submit(), not both")
         self._mode = mode
 
     def _check(self, *bufs):
         for b in bufs:
-            assert b.is_pinned(), "host buffers must be pinned"
-            assert tuple(b.shape) == (self.n, 4) and b.dtype == torch.float32
+            if not b.is_pinned():
+                raise ValueError("host buffers must be pinned")
+            if tuple(b.shape) != (self.n, 4) or b.dtype != torch.float32:
+                raise ValueError(f"host buffers must be float32 [{self.n}, 4]")
 
     def advance(self, host_pos, step: int):
         self._use("advance")

@@ -41,8 +41,10 @@ def test_host_owned_trajectory_matches_device_trajectory(ctx_factory):
     stepper.finish()
     torch.cuda.synchronize()
     _close(h_pos.numpy(), dev_b["pos"].cpu().numpy(), w.box_size)
-    with pytest.raises(AssertionError):  # one pattern per stepper
+    with pytest.raises(RuntimeError):  # one pattern per stepper
         stepper.submit(h_pos, h_pos, 61)
+    with pytest.raises(ValueError):  # pageable host memory
+        stepper.advance(torch.from_numpy(w.pos.copy()), 61)
 
 
 def test_trajectory_through_host_matches_device_steps(ctx_factory):
