@@ -13,6 +13,13 @@ Multi-GPU: the path does not shard; N GPUs run N independent replicas (one
 process per GPU, weak scaling), and `value` counts all replicas' work over
 the slowest rank's time.
 
+`e2e` is the same trajectory with the positions owned by the host
+(engine.HostStepper.advance: pinned upload, fused step, read-back every
+step). At N=1 the line also carries `batched` (512 independent systems in one
+batch against the same systems run one after another), `adjoint` (adjoint
+window step against the forward step) and `small_plain` (a 4,096-bead system
+through one mb2_step call per step and through mb2_run).
+
 `--impl reference` times the reference's own CPU implementation of the path
 (its functors host-compiled in oracle/_ref) on this host's cores, on a bounded
 sample of the same workload scaled to the full system.
