@@ -84,11 +84,15 @@ MB2_API int mb2_radix_sort_pairs(mb2_context* ctx, uint32_t* keys, uint32_t* val
  * callers that cannot allocate — a process whose HBM is already held by another
  * allocator, or a loop that must never stall on an implicit synchronisation —
  * use this one. Its scratch is a fixed array in the library's static device
- * memory (about 8.6 MB per device, present once the module is loaded).
+ * memory (about 8.6 MB per device, held until the process exits).
  *   - n <= MB2_SORT_STATIC_MAX, else MB2_ERR_CAPACITY and nothing is touched.
- *   - The first call on each device (n = 0 is enough) looks up the array's
- *     device address with that device current; make it before any stream
- *     capture.
+ *   - Each call looks up the array's device address with the context's device
+ *     current. Under CUDA's lazy module loading (the CUDA 12 default) the first
+ *     call on a device may load the module and so reserve the 8.6 MB then: make
+ *     one call with n = 0 at start-up, before another allocator takes the
+ *     device's free memory and before any stream capture. After
+ *     cudaDeviceReset, make that n = 0 call again (the module reloads, possibly
+ *     at another address, which the next lookup finds).
  *   - All calls on one device share the array: calls that overlap in time on
  *     one device race. Order them (one stream, or explicit events).
  *   - ctx selects the device and receives the error message; the context's
@@ -107,9 +111,19 @@ MB2_API int mb2_set_exclusions(mb2_context* ctx, const int* offsets, const int* 
 
 /* Build the half pairlist within `pairlist_cutoff`. Replaces
  * ZOrderPairlist::build_pairlist (PairListKernels/ZOrderPairlist.cpp:102-178).
- * Synchronises `stream` once (to size the list); returns the pair count. */
+ * Synchronises `stream` once (to size the list); returns the pair count.
+ * `interaction_cutoff` is the force cutoff the list will serve. When it lies
+ * in (0, pairlist_cutoff), each row stores the pairs within
+ * interaction_cutoff + 25 % of the skin first and the rest after them, so
+ * the pair kernel skips whole warps in the rows' tails; otherwise (0, or not
+ * below pairlist_cutoff) rows keep the walk's candidate order. The pair set
+ * is the same either way; only the order in which per-particle force sums
+ * accumulate differs. The result depends on the arguments alone, not on
+ * earlier calls; mb2_step and mb2_run pass their params' cutoff. NaN is
+ * rejected with MB2_ERR_ARG. */
 MB2_API int mb2_build_pairlist(mb2_context* ctx, const float* pos4, const int* type_ids, uint32_t n,
-                       float pairlist_cutoff, void* stream, uint64_t* num_pairs);
+                       float pairlist_cutoff, float interaction_cutoff, void* stream,
+                       uint64_t* num_pairs);
 
 /* Pair count of the last build (Pairlist::get_num_pairs, Pairlist.h:139-141). */
 MB2_API int mb2_num_pairs(const mb2_context* ctx, uint64_t* num_pairs);

@@ -89,7 +89,7 @@ def load(path: str = LIB_PATH):
     L.mb2_radix_sort_pairs.argtypes = [vp, vp, vp, u32, vp]
     L.mb2_radix_sort_pairs_static.argtypes = [vp, vp, vp, u32, vp]
     L.mb2_set_exclusions.argtypes = [vp, vp, vp, u32, vp]
-    L.mb2_build_pairlist.argtypes = [vp, vp, vp, u32, f, vp, u64p]
+    L.mb2_build_pairlist.argtypes = [vp, vp, vp, u32, f, f, vp, u64p]
     L.mb2_num_pairs.argtypes = [vp, u64p]
     L.mb2_export_pairs.argtypes = [vp, vp, u64, vp]
     L.mb2_needs_update.argtypes = [vp, vp, u32, f, vp, fp, ip]

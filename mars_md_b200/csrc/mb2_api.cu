@@ -29,7 +29,6 @@ struct mb2_context {
 
 	// Z-order state of the last build
 	DevBuf<uint32_t> keys, s2o, inv, row_len, row_off, nbr, cell_begin, cell_end, row_far;
-	float last_cutoff = 0.0f;  // interaction cutoff of the last pair-force call
 	DevBuf<float4> sorted_pos, ref_pos, force_sorted;
 	DevBuf<StencilEntry> stencil;
 	DevBuf<float> bbox;  // 6 floats, ordered-int min/max
@@ -260,8 +259,11 @@ void sort_particles(mb2_context* ctx, const float4* pos, const int* type_ids, ui
 	pack_sorted_positions(pos, type_ids, ctx->s2o.ptr, n, ctx->sorted_pos.ptr, st);
 }
 
+// cutoff: the interaction cutoff the list will serve. When it lies in
+// (0, rc_list), rows are split near / far (below); otherwise rows keep the
+// walk's candidate order.
 void build(mb2_context* ctx, const float4* pos, const int* type_ids, uint32_t n, float rc_list,
-		   cudaStream_t st) {
+		   float cutoff, cudaStream_t st) {
 	require(ctx->box_set, MB2_ERR_STATE, "mb2_build_pairlist: call mb2_set_box first");
 	require(n <= ctx->max_particles, MB2_ERR_CAPACITY,
 			"mb2_build_pairlist: more particles than the context was created for");
@@ -316,8 +318,8 @@ void build(mb2_context* ctx, const float4* pos, const int* type_ids, uint32_t n,
 	// Measured on the 2,097,152-bead workload (fused step, rebuild every 20
 	// steps): 1.94 ms without the split; 1.87 ms at 25 % of the skin, 1.89 at
 	// 10 % and at 40 %, 1.92 at 70 %.
-	const float cut = ctx->last_cutoff;
-	const float split = (cut > 0.0f && cut < rc_list) ? cut + 0.25f * (rc_list - cut) : 0.0f;
+	const float split =
+		(cutoff > 0.0f && cutoff < rc_list) ? cutoff + 0.25f * (rc_list - cutoff) : 0.0f;
 	wg.split2 = split > 0.0f ? split * split : INFINITY;
 	for (int a = 0; a < 3; ++a) {
 		// Morton coordinate q = trunc((x - bmin) / range * 1023) on 0..1023, a cell
@@ -407,7 +409,6 @@ void pair_kernel(mb2_context* ctx, uint32_t n, float cutoff, int get_energy, cud
 			"mb2_pair_forces: the tags carry analytical terms; call mb2_set_pair_terms");
 	ctx->force_sorted.ensure(n);
 	MB2_CUDA(cudaMemsetAsync(ctx->force_sorted.ptr, 0, static_cast<size_t>(n) * sizeof(float4), st));
-	ctx->last_cutoff = cutoff;
 	const float cutoff_sq = cutoff > 0.0f ? cutoff * cutoff : 0.0f;
 	StageScope scope(ctx, MB2_STAGE_PAIR_FORCE, st);
 	pair_forces(ctx->sorted_pos.ptr, ctx->nbr.ptr, ctx->row_len.ptr, n, ctx->cap, ctx->lanes, ctx->pt,
@@ -664,10 +665,14 @@ int mb2_set_exclusions(mb2_context* ctx, const int* offsets, const int* neighbor
 }
 
 int mb2_build_pairlist(mb2_context* ctx, const float* pos4, const int* type_ids, uint32_t n,
-					   float pairlist_cutoff, void* stream, uint64_t* num_pairs) {
+					   float pairlist_cutoff, float interaction_cutoff, void* stream,
+					   uint64_t* num_pairs) {
 	return guarded(ctx, [&] {
 		require(n == 0 || pos4, MB2_ERR_ARG, "mb2_build_pairlist: null positions");
-		build(ctx, reinterpret_cast<const float4*>(pos4), type_ids, n, pairlist_cutoff, S(stream));
+		require(!std::isnan(interaction_cutoff), MB2_ERR_ARG,
+				"mb2_build_pairlist: interaction cutoff is NaN");
+		build(ctx, reinterpret_cast<const float4*>(pos4), type_ids, n, pairlist_cutoff,
+			  interaction_cutoff, S(stream));
 		if (num_pairs) *num_pairs = ctx->num_pairs;
 	});
 }
@@ -1153,9 +1158,8 @@ void step_once(mb2_context* ctx, float4* pos, float4* fe, const int* type_ids,
 	const float skin = prm->pairlist_cutoff - prm->cutoff;
 	if (rebuild && prm->rebuild_period != 0 && ctx->built && ctx->built_n == n && skin > 0.0f)
 		rebuild = max_disp(ctx, pos, n, st) > skin * 0.5f;
-	ctx->last_cutoff = prm->cutoff;
 	if (rebuild)
-		build(ctx, pos, type_ids, n, prm->pairlist_cutoff, st);  // packs sorted_pos
+		build(ctx, pos, type_ids, n, prm->pairlist_cutoff, prm->cutoff, st);  // packs sorted_pos
 	else if (n)
 		pack_sorted_positions(pos, type_ids, ctx->s2o.ptr, n, ctx->sorted_pos.ptr, st);
 	if (n == 0) return;
@@ -1342,7 +1346,7 @@ int mb2_window_forward(mb2_context* ctx, float* pos4, float* force_energy4, cons
 			const uint32_t k0 = sgi * checkpoint_every;
 			const uint32_t k1 = std::min(num_steps, k0 + checkpoint_every);
 			copy4(ctx->ckpt.ptr + static_cast<size_t>(sgi) * n, pos, n, st);
-			build(ctx, pos, type_ids, n, prm->pairlist_cutoff, st);
+			build(ctx, pos, type_ids, n, prm->pairlist_cutoff, prm->cutoff, st);
 			for (uint32_t k = k0; k < k1; ++k)
 				window_step(ctx, pos, fe, type_ids, n, first_step + k, prm, st);
 		}
@@ -1404,7 +1408,7 @@ int mb2_window_backward(mb2_context* ctx, const float* grad_final4, float* grad_
 			const uint32_t k1 = std::min(w.num_steps, k0 + C);
 			// Recompute the segment from its checkpoint, keeping every state.
 			copy4(ctx->wpos.ptr, ctx->ckpt.ptr + static_cast<size_t>(sgi) * n, n, st);
-			build(ctx, ctx->wpos.ptr, w.type_ids, n, prm->pairlist_cutoff, st);
+			build(ctx, ctx->wpos.ptr, w.type_ids, n, prm->pairlist_cutoff, prm->cutoff, st);
 			for (uint32_t k = k0; k < k1; ++k) {
 				copy4(ctx->states.ptr + static_cast<size_t>(k - k0) * n, ctx->wpos.ptr, n, st);
 				if (k + 1 < k1)
@@ -1437,7 +1441,7 @@ int mb2_rdf_histogram(mb2_context* ctx, const float* pos4, const int* type_ids, 
 					bin_width > 0.0f && sigma > 0.0f && r_max > 0.0f,
 				MB2_ERR_ARG, "mb2_rdf_histogram: bad arguments");
 		const cudaStream_t st = S(stream);
-		build(ctx, reinterpret_cast<const float4*>(pos4), type_ids, n, r_max, st);
+		build(ctx, reinterpret_cast<const float4*>(pos4), type_ids, n, r_max, 0.0f, st);
 		MB2_CUDA(cudaMemsetAsync(hist, 0, num_bins * sizeof(double), st));
 		rdf_pairs(ctx->sorted_pos.ptr, ctx->nbr.ptr, ctx->row_len.ptr, n, ctx->cap, ctx->lanes,
 				  ctx->box, num_bins, bin_width, r_max, sigma, hist, nullptr, nullptr, st);

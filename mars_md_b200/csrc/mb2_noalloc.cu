@@ -11,15 +11,21 @@
 // array instead and so allocates nothing, at any n up to MB2_SORT_STATIC_MAX.
 //
 // Rules that follow from the shared array:
-//  * Set-up: the first call on each device looks up the array's device
-//    address (cudaGetSymbolAddress, with that device current) and caches it.
-//    Make that first call (n = 0 is enough) before any stream capture.
+//  * Set-up: every call looks up the array's device address on the current
+//    device (cudaGetSymbolAddress, a host-side lookup once the module is
+//    loaded). With CUDA's lazy module loading the first lookup on a device
+//    can itself load this module, which reserves the array's ~8.6 MB of
+//    device memory then; so make one call (n = 0 is enough) at start-up,
+//    before another allocator takes the device's free memory and before any
+//    stream capture. After cudaDeviceReset the module is loaded anew, at a
+//    possibly different address, by the next call's lookup (nothing stale is
+//    kept); repeat the n = 0 call then.
 //  * Every call on one device uses the same array, so calls that overlap in
 //    time on one device (different streams, or host threads without ordering)
 //    race and corrupt each other's results. Order them, e.g. one stream.
 //  * Nothing in the array has to start at zero: each word a call reads was
 //    written earlier in the same call.
-#include <mutex>
+#include <string>
 
 #include "marsb200.h"
 #include "mb2_internal.cuh"
@@ -43,26 +49,16 @@ constexpr size_t kWords = kSumsOff + round_up(kBlockSumWords);
 // keys_alt | vals_alt | digit histogram | scan block sums (~8.6 MB).
 static __device__ __align__(256) uint32_t g_sort_scratch[kWords];
 
-constexpr int kMaxDevices = 64;
-std::mutex g_setup_mutex;
-uint32_t* g_scratch[kMaxDevices] = {};
-
-// Device address of the array on the current device, looked up once.
+// Device address of the array on the current device. In host code the
+// array's name is only a host-side stand-in, never a device address, so the
+// address is looked up (not cached: a cudaDeviceReset may move it).
 uint32_t* scratch_on_current_device() {
-	int dev = 0;
-	MB2_CUDA(cudaGetDevice(&dev));
-	if (dev < 0 || dev >= kMaxDevices)
-		throw Error{MB2_ERR_ARG, "mb2_radix_sort_pairs_static: device ordinal out of range"};
-	std::lock_guard<std::mutex> lock(g_setup_mutex);
-	if (g_scratch[dev] == nullptr) {
-		void* p = nullptr;
-		const cudaError_t e = cudaGetSymbolAddress(&p, g_sort_scratch);
-		if (e != cudaSuccess || p == nullptr)
-			throw Error{MB2_ERR_CUDA, std::string("mb2_radix_sort_pairs_static: cudaGetSymbolAddress: ") +
-										  cudaGetErrorString(e)};
-		g_scratch[dev] = static_cast<uint32_t*>(p);
-	}
-	return g_scratch[dev];
+	void* p = nullptr;
+	const cudaError_t e = cudaGetSymbolAddress(&p, g_sort_scratch);
+	if (e != cudaSuccess || p == nullptr)
+		throw Error{MB2_ERR_CUDA, std::string("mb2_radix_sort_pairs_static: cudaGetSymbolAddress: ") +
+									  cudaGetErrorString(e)};
+	return static_cast<uint32_t*>(p);
 }
 
 }  // namespace

@@ -511,13 +511,16 @@ __global__ void __launch_bounds__(256) export_kernel(const uint32_t* __restrict_
 
 // Small systems: one warp per particle row. The lanes take the row's pruned
 // stencil cells 32 at a time (cells whose Morton code precedes the particle's
-// hold only earlier particles and are skipped), then walk their cells'
-// candidates in lockstep rounds, each lane its own cell, with the reference's
-// exact test; a round's hits are appended with two ballots (near entries from
+// hold only earlier particles and are skipped). The kept cells' candidate
+// ranges are laid end to end by a warp scan of their lengths, and every round
+// tests 32 consecutive candidates of that stream, one per lane, with the
+// reference's exact test: each lane finds the cell its candidate falls in by a
+// binary search over the running totals, held one per lane and read with warp
+// shuffles. A round's hits are appended with two ballots (near entries from
 // the front of the row, far ones from the back, as the group walk does). The
 // group walk runs one warp per 32 particles and leaves most of the GPU idle
-// below a few tens of thousands of particles; here every particle has a warp.
-// Rows hold the same pairs in another order.
+// below some 10^5 particles; here every particle has a warp. Rows hold the
+// same pairs in another order.
 template <bool kExcl>
 __global__ void __launch_bounds__(256) build_rows_kernel(
 	const float4* __restrict__ sorted_pos, const uint32_t* __restrict__ keys,

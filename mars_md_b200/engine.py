@@ -239,11 +239,15 @@ class Context:
         return out[:n]
 
     # -- pairlist ----------------------------------------------------------
-    def build_pairlist(self, pos, type_ids, pairlist_cutoff, stream=None) -> int:
+    def build_pairlist(self, pos, type_ids, pairlist_cutoff, interaction_cutoff=0.0,
+                       stream=None) -> int:
+        """Half pairlist within pairlist_cutoff. With an interaction_cutoff in
+        (0, pairlist_cutoff) rows hold the pairs likely to interact first
+        (same pair set, another summation order); 0 keeps candidate order."""
         npairs = C.c_uint64()
         self.check(self.lib.mb2_build_pairlist(self.h, _p(pos), _p(type_ids), pos.shape[0],
-                                               float(pairlist_cutoff), _stream(stream),
-                                               C.byref(npairs)))
+                                               float(pairlist_cutoff), float(interaction_cutoff),
+                                               _stream(stream), C.byref(npairs)))
         return int(npairs.value)
 
     def num_pairs(self) -> int:

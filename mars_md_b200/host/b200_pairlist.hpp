@@ -385,18 +385,22 @@ class B200Pairlist : public Pairlist {
 
 	void build_pairlist(const DeviceBuffer<Vector3>& positions, size_t num_particles,
 						float cutoff) override {
-		build_with_types(positions.data(), nullptr, num_particles, cutoff);
+		build_with_types(positions.data(), nullptr, num_particles, cutoff, interaction_cutoff_);
 	}
+	// The force cutoff this list serves (0, the default: none given). Builds
+	// through build_pairlist then store the pairs likely to interact first in
+	// each row (same pair set; see mb2_build_pairlist).
+	void set_interaction_cutoff(float cutoff) { interaction_cutoff_ = cutoff; }
 	// Build with type ids (the pair-force stage reads them beside the positions).
 	void build_with_types(const Vector3* positions, const int* type_ids, size_t num_particles,
-						  float cutoff) {
+						  float cutoff, float interaction_cutoff) {
 		if (num_particles > max_particles_)
 			throw Exception(ExceptionType::CapacityError,
 							"build_pairlist: more particles than the pairlist was created for");
 		uint64_t pairs = 0;
 		check(mb2_build_pairlist(ctx_->get(), reinterpret_cast<const float*>(positions), type_ids,
-								 static_cast<uint32_t>(num_particles), cutoff, ctx_->stream(),
-								 &pairs),
+								 static_cast<uint32_t>(num_particles), cutoff, interaction_cutoff,
+								 ctx_->stream(), &pairs),
 			  ctx_->get(), "build_pairlist");
 		if (pairs > max_pairs_ceiling_)
 			throw Exception(ExceptionType::CapacityError,
@@ -449,6 +453,7 @@ class B200Pairlist : public Pairlist {
 	mutable DeviceBuffer<int2> pairs_;
 	mutable bool exported_ = false;
 	mutable float last_max_displacement_ = 0.0f;
+	float interaction_cutoff_ = 0.0f;
 };
 
 // Factory (src/PatchOperation/Pairlist.cpp:7-31) with the B200 strategy
@@ -542,7 +547,8 @@ class B200Patch {
 		if (rebuild && !first && rebuild_period != 0 && skin > 0.0f && interaction_cutoff > 0.0f)
 			rebuild = pairlist_.needs_update(pos, pos, num_particles, skin);
 		if (rebuild) {
-			pairlist_.build_with_types(pos.data(), types.data(), num_particles, pairlist_cutoff);
+			pairlist_.build_with_types(pos.data(), types.data(), num_particles, pairlist_cutoff,
+									   interaction_cutoff);
 			built_ = true;
 			built_n_ = num_particles;
 		}

@@ -5,8 +5,8 @@
 Builds the large_plain workload at N beads (same density and tables as the
 2,097,152-bead benchmark; default 1,048,576 so the pairlist still exceeds L2),
 runs one pairlist build, two pair-force launches (with --split-rows one more
-build, whose rows put near pairs first, and two more launches) and S fused
-steps, then exits.
+build, whose rows put near pairs first as the fused step's builds do, and two
+more launches) and S fused steps, then exits.
 Few launches precede the kernels of interest, as ncu captures need.
 """
 import argparse
@@ -23,7 +23,7 @@ def main(argv=None):
     ap.add_argument("n", nargs="?", type=int, default=1_048_576)
     ap.add_argument("--steps", type=int, default=0)
     ap.add_argument("--split-rows", action="store_true",
-                    help="rebuild once more after a pair-force call (near/far rows)")
+                    help="rebuild once more with near/far rows at the interaction cutoff")
     a = ap.parse_args(argv)
     w = W.large_plain(n=a.n)
     ctx = Context(w.n)
@@ -33,9 +33,9 @@ def main(argv=None):
         dev["fe"].zero_()
         ctx.pair_forces(dev["pos"], dev["type"], dev["fe"], w.cutoff, get_energy=False)
     if a.split_rows:
-        # A build after a pair-force call splits rows at the interaction cutoff
-        # (near pairs first), as the fused step's builds do; two more launches.
-        ctx.build_pairlist(dev["pos"], dev["type"], w.list_radius)
+        # Rows split at the interaction cutoff (near pairs first), as the fused
+        # step's builds are; two more launches.
+        ctx.build_pairlist(dev["pos"], dev["type"], w.list_radius, w.cutoff)
         for _ in range(2):
             dev["fe"].zero_()
             ctx.pair_forces(dev["pos"], dev["type"], dev["fe"], w.cutoff, get_energy=False)

@@ -11,7 +11,7 @@ reference checkout.
 
 Run from the repository root, where the reference checkout is available:
 
-    make -C oracle/ref_harness && python tests/golden/make_golden.py [case ...]
+    make -C oracle/ref_harness REF=<reference checkout> && python tests/golden/make_golden.py [case ...]
 
 The fixtures pin the C restatement in ``oracle/`` (tests/test_oracle_golden.py)
 and, through it, the CUDA path.
@@ -455,7 +455,7 @@ CASES = {"uniform4096": uniform, "lattice_open": lattice, "polymer_excl": polyme
 
 def main():
     if not po.ref_available():
-        sys.exit("reference harness not built: make -C oracle/ref_harness")
+        sys.exit("reference harness not built: make -C oracle/ref_harness REF=<reference checkout>")
     O, R = po.Oracle(), po.RefHarness()
     names = sys.argv[1:] or list(CASES)
     for name in names:

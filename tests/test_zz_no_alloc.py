@@ -1,10 +1,11 @@
 """mb2_radix_sort_pairs_static: the sort that allocates no device memory.
 
 It must give exactly the result of the context sort (mb2_radix_sort_pairs) on
-the same keys, on consecutive calls that share its static scratch, without
-changing the device's free memory, and refuse sizes above its maximum before
-touching anything. Called through the C ABI. This file is collected last so
-that it also runs after every other GPU test in the same process.
+the same keys, and of a stable host sort (numpy argsort, kind "stable"), on
+consecutive calls that share its static scratch, without changing the
+device's free memory, and refuse sizes above its maximum before touching
+anything. Called through the C ABI. This file is collected last so that it
+also runs after every other GPU test in the same process.
 """
 import ctypes as C
 
@@ -39,6 +40,9 @@ def test_static_sort_matches_context_sort_on_consecutive_calls(ctx_factory):
     assert lib.mb2_radix_sort_pairs_static(ctx.h, None, None, 0, sp) == _lib.MB2_OK
     for n, seed in [(300_001, 11), (_lib.MB2_SORT_STATIC_MAX, 12), (2049, 13)]:
         keys, vals = _random_pairs(n, seed)
+        k_host = keys.cpu().numpy().view(np.uint32)
+        v_host = vals.cpu().numpy()
+        order = np.argsort(k_host, kind="stable")
         k_ctx, v_ctx = keys.clone(), vals.clone()
         ctx.radix_sort_pairs(k_ctx, v_ctx, stream=stream)
         k_st, v_st = keys.clone(), vals.clone()
@@ -52,8 +56,9 @@ def test_static_sort_matches_context_sort_on_consecutive_calls(ctx_factory):
         # Integer sort: the results must be identical, payload order included.
         assert torch.equal(k_st, k_ctx)
         assert torch.equal(v_st, v_ctx)
-        k = k_st.cpu().numpy().view(np.uint32).astype(np.int64)
-        assert np.all(np.diff(k) >= 0)
+        # Independent of either GPU sort: a stable sort of the same pairs on the host.
+        assert np.array_equal(k_st.cpu().numpy().view(np.uint32), k_host[order])
+        assert np.array_equal(v_st.cpu().numpy(), v_host[order])
 
 
 def test_static_sort_rejects_sizes_above_maximum(ctx_factory):
