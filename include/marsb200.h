@@ -466,6 +466,13 @@ MB2_API int mb2_window_forward(mb2_context* ctx, float* pos4, float* force_energ
                        const int* type_ids, uint32_t n, uint64_t first_step,
                        uint32_t num_steps, uint32_t checkpoint_every,
                        const mb2_step_params* params, void* stream);
+/* The positions the last forward window stored at its checkpoints (x_0,
+ * x_C, x_2C, ...; ceil(num_steps / C) blocks of n float4 rows, in order), for
+ * inspecting or restarting a window; the reverse sweep recomputes each
+ * segment from these. capacity_rows counts float4 rows. No counterpart in the
+ * reference (it has no adjoint). */
+MB2_API int mb2_window_checkpoints(mb2_context* ctx, float* out4, uint64_t capacity_rows,
+                           void* stream);
 /* Reverse sweep of the last forward window: grad_final4 = dL/dx_N (float4
  * rows, .w ignored) -> grad_pos0_4 = dL/dx_0; grad_pair_bins (device double,
  * one per value of the concatenated pair tables) and grad_bond_bins (per

@@ -102,6 +102,15 @@ class Window:
             self.every, C.byref(self.prm), _stream(stream)))
         return pos
 
+    def checkpoints(self, stream=None) -> torch.Tensor:
+        """Positions stored at the last forward window's checkpoints
+        (ceil(steps / checkpoint_every) x n x 4, x_0 first)."""
+        segs = (self.steps + self.every - 1) // self.every
+        out = torch.empty((segs, self.w.n, 4), dtype=torch.float32, device=self.device)
+        self.ctx.check(self.ctx.lib.mb2_window_checkpoints(
+            self.ctx.h, _p(out), segs * self.w.n, _stream(stream)))
+        return out
+
     def histogram(self, pos: torch.Tensor, stream=None) -> torch.Tensor:
         h = torch.zeros(self.rdf.bins, dtype=torch.float64, device=self.device)
         r = self.rdf

@@ -1360,6 +1360,18 @@ int mb2_window_forward(mb2_context* ctx, float* pos4, float* force_energy4, cons
 	});
 }
 
+int mb2_window_checkpoints(mb2_context* ctx, float* out4, uint64_t capacity_rows, void* stream) {
+	return guarded(ctx, [&] {
+		require(ctx->win.valid, MB2_ERR_STATE, "mb2_window_checkpoints: no forward window");
+		const uint32_t segs = (ctx->win.num_steps + ctx->win.every - 1) / ctx->win.every;
+		const uint64_t rows = static_cast<uint64_t>(segs) * ctx->win.n;
+		require(capacity_rows >= rows && out4, MB2_ERR_CAPACITY,
+				"mb2_window_checkpoints: output smaller than checkpoints x particles");
+		MB2_CUDA(cudaMemcpyAsync(out4, ctx->ckpt.ptr, rows * sizeof(float4),
+								 cudaMemcpyDeviceToDevice, S(stream)));
+	});
+}
+
 int mb2_window_backward(mb2_context* ctx, const float* grad_final4, float* grad_pos0_4,
 						double* grad_pair_bins, double* grad_bond_bins, void* stream) {
 	return guarded(ctx, [&] {

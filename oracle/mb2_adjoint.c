@@ -21,6 +21,9 @@
  * dF/dU[h] = +step_inv, dF/dU[h+1] = -step_inv for the pair's bin h.
  */
 #include <math.h>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
 #include <stdlib.h>
 #include <string.h>
 
@@ -182,13 +185,143 @@ static void angle_term(const adj_sys* s, int i, int j, int k, const double* x, d
 	}
 }
 
+/* Candidate pairs (i < j, not excluded) whose minimum-image distance may be
+ * within rmax: a periodic cell list with cells at least rmax wide when every
+ * axis holds three or more of them, else all pairs. Each caller applies its
+ * own exact distance test, so the candidate set only has to contain every pair
+ * within rmax. Threads take contiguous ranges of i and their lists are joined
+ * in thread order, so the order is fixed for a given thread count. Returns the
+ * count; *out (i, j) is malloc'd, the caller frees. */
+static size_t near_pairs(const adj_sys* s, const double* x, double rmax, int** out) {
+	const int n = s->n;
+	int nc[3];
+	int cells_ok = 1;
+	for (int a = 0; a < 3; ++a) {
+		nc[a] = (int)floor(s->L[a] / rmax);
+		if (nc[a] < 3) cells_ok = 0;
+	}
+	if (!cells_ok) nc[0] = nc[1] = nc[2] = 1;
+	const size_t ncell = (size_t)nc[0] * nc[1] * nc[2];
+	int* cell_of = (int*)malloc(sizeof(int) * (size_t)(n ? n : 1));
+	int* start = (int*)calloc(ncell + 1, sizeof(int));
+	int* members = (int*)malloc(sizeof(int) * (size_t)(n ? n : 1));
+	for (int i = 0; i < n; ++i) {
+		int c[3];
+		for (int a = 0; a < 3; ++a) {
+			double u = x[3 * i + a] / s->L[a];
+			u -= floor(u);
+			c[a] = (int)(u * nc[a]);
+			if (c[a] >= nc[a]) c[a] = nc[a] - 1;
+			if (c[a] < 0) c[a] = 0;
+		}
+		cell_of[i] = (c[0] * nc[1] + c[1]) * nc[2] + c[2];
+		++start[cell_of[i] + 1];
+	}
+	for (size_t c = 0; c < ncell; ++c) start[c + 1] += start[c];
+	int* fill = (int*)malloc(sizeof(int) * ncell);
+	for (size_t c = 0; c < ncell; ++c) fill[c] = start[c];
+	for (int i = 0; i < n; ++i) members[fill[cell_of[i]]++] = i;
+	free(fill);
+	int nthreads = 1;
+#ifdef _OPENMP
+	nthreads = omp_get_max_threads();
+#endif
+	int** tp = (int**)calloc((size_t)nthreads, sizeof(int*));
+	size_t* tc = (size_t*)calloc((size_t)nthreads, sizeof(size_t));
+#pragma omp parallel num_threads(nthreads)
+	{
+		int tid = 0;
+#ifdef _OPENMP
+		tid = omp_get_thread_num();
+#endif
+		size_t cap = 1024, cnt = 0;
+		int* p = (int*)malloc(sizeof(int) * 2 * cap);
+#pragma omp for schedule(static)
+		for (int i = 0; i < n; ++i) {
+			const int ci = cell_of[i];
+			const int cx = ci / (nc[1] * nc[2]), cy = (ci / nc[2]) % nc[1], cz = ci % nc[2];
+			const int span = cells_ok ? 1 : 0;
+			for (int dx = -span; dx <= span; ++dx)
+				for (int dy = -span; dy <= span; ++dy)
+					for (int dz = -span; dz <= span; ++dz) {
+						const int ox = (cx + dx + nc[0]) % nc[0], oy = (cy + dy + nc[1]) % nc[1],
+								  oz = (cz + dz + nc[2]) % nc[2];
+						const int c = (ox * nc[1] + oy) * nc[2] + oz;
+						for (int q = start[c]; q < start[c + 1]; ++q) {
+							const int j = members[q];
+							if (j <= i || excluded(s, i, j)) continue;
+							if (cnt == cap) {
+								cap *= 2;
+								p = (int*)realloc(p, sizeof(int) * 2 * cap);
+							}
+							p[2 * cnt] = i;
+							p[2 * cnt + 1] = j;
+							++cnt;
+						}
+					}
+		}
+		tp[tid] = p;
+		tc[tid] = cnt;
+	}
+	size_t total = 0;
+	for (int t = 0; t < nthreads; ++t) total += tc[t];
+	int* all = (int*)malloc(sizeof(int) * 2 * (total ? total : 1));
+	size_t at = 0;
+	for (int t = 0; t < nthreads; ++t) {
+		if (tc[t]) memcpy(all + 2 * at, tp[t], sizeof(int) * 2 * tc[t]);
+		at += tc[t];
+		free(tp[t]);
+	}
+	free(tp);
+	free(tc);
+	free(cell_of);
+	free(start);
+	free(members);
+	*out = all;
+	return total;
+}
+
+/* Adds thread-private accumulators into the shared ones in thread order. */
+static void add_into(double* dst, const double* src, size_t len) {
+	if (!dst) return;
+	for (size_t q = 0; q < len; ++q) dst[q] += src[q];
+}
+
 /* Total force (f) and, when mu is given, its tangent along mu (t) and the
  * table gradients (gpair, gbond: mu . dforce/dU, accumulated). */
 static void forces(const adj_sys* s, const double* x, double* f, const double* mu, double* t,
 				   double* gpair, double* gbond) {
-	for (int i = 0; i < s->n; ++i)
-		for (int j = i + 1; j < s->n; ++j)
-			if (!excluded(s, i, j)) radial_term(s, &s->pair, s->cutoff, i, j, x, f, mu, t, gpair);
+	int* pr = NULL;
+	const size_t np = near_pairs(s, x, s->cutoff, &pr);
+	const size_t m = 3 * (size_t)s->n, gs = (size_t)s->pair.size;
+	int nthreads = 1;
+#ifdef _OPENMP
+	nthreads = omp_get_max_threads();
+#endif
+	double** acc = (double**)calloc((size_t)nthreads, sizeof(double*));
+#pragma omp parallel num_threads(nthreads)
+	{
+		int tid = 0;
+#ifdef _OPENMP
+		tid = omp_get_thread_num();
+#endif
+		double* buf = (double*)calloc(2 * m + gs + 1, sizeof(double));
+		double* fl = f ? buf : NULL;
+		double* tl = t ? buf + m : NULL;
+		double* gl = gpair ? buf + 2 * m : NULL;
+#pragma omp for schedule(static)
+		for (size_t q = 0; q < np; ++q)
+			radial_term(s, &s->pair, s->cutoff, pr[2 * q], pr[2 * q + 1], x, fl, mu, tl, gl);
+		acc[tid] = buf;
+	}
+	for (int th = 0; th < nthreads; ++th) {
+		add_into(f, acc[th], m);
+		add_into(t, acc[th] + m, m);
+		add_into(gpair, acc[th] + 2 * m, gs);
+		free(acc[th]);
+	}
+	free(acc);
+	free(pr);
 	for (int b = 0; b < s->nb; ++b)
 		radial_term(s, &s->bond, 0.0, s->bonds[2 * b], s->bonds[2 * b + 1], x, f, mu, t, gbond);
 	for (int a = 0; a < s->na; ++a)
@@ -242,9 +375,11 @@ void adj_backward64(const adj_sys* s, const double* traj, int steps, double* lam
 void adj_rdf64(const adj_sys* s, const double* x, int nbins, double dr, double rmax, double sigma,
 			   double* hist) {
 	memset(hist, 0, sizeof(double) * (size_t)nbins);
-	for (int i = 0; i < s->n; ++i)
-		for (int j = i + 1; j < s->n; ++j) {
-			if (excluded(s, i, j)) continue;
+	int* pr = NULL;
+	const size_t np = near_pairs(s, x, rmax, &pr);
+	for (size_t q = 0; q < np; ++q) {
+		const int i = pr[2 * q], j = pr[2 * q + 1];
+		{
 			double r2 = 0.0;
 			for (int a = 0; a < 3; ++a) {
 				const double d = min_image(x[3 * j + a] - x[3 * i + a], s->L[a]);
@@ -257,14 +392,18 @@ void adj_rdf64(const adj_sys* s, const double* x, int nbins, double dr, double r
 				if (fabs(z) <= 5.0 * sigma) hist[b] += exp(-z * z / (2.0 * sigma * sigma));
 			}
 		}
+	}
+	free(pr);
 }
 
 /* grad (n * 3, accumulated) of sum_b dLdh[b] hist[b] with respect to x. */
 void adj_rdf_grad64(const adj_sys* s, const double* x, int nbins, double dr, double rmax,
 					double sigma, const double* dLdh, double* grad) {
-	for (int i = 0; i < s->n; ++i)
-		for (int j = i + 1; j < s->n; ++j) {
-			if (excluded(s, i, j)) continue;
+	int* pr = NULL;
+	const size_t np = near_pairs(s, x, rmax, &pr);
+	for (size_t q = 0; q < np; ++q) {
+		const int i = pr[2 * q], j = pr[2 * q + 1];
+		{
 			double r[3], r2 = 0.0;
 			for (int a = 0; a < 3; ++a) {
 				r[a] = min_image(x[3 * j + a] - x[3 * i + a], s->L[a]);
@@ -283,4 +422,6 @@ void adj_rdf_grad64(const adj_sys* s, const double* x, int nbins, double dr, dou
 				grad[3 * i + a] -= dLdr * r[a] / d;
 			}
 		}
+	}
+	free(pr);
 }

@@ -116,3 +116,102 @@ def test_window_forward_keeps_x0_and_matches_plain_steps():
         ctx.close()
     finally:
         win.close()
+
+
+C5_STEPS, C5_EVERY = 200, 20
+
+
+def _c5_workload():
+    w = W.adjoint()
+    rng = np.random.default_rng(W.DEFAULT_SEED)
+    # Off the bond table's bin edges: seeded chains have bonds exactly 5.0 A long.
+    w.pos[:, :3] = np.mod(w.pos[:, :3] + rng.normal(scale=0.02, size=(w.n, 3)),
+                          w.box_size[0]).astype(np.float32)
+    return w
+
+
+def _c5_device(w, steps, rdf):
+    """Device gradients of the window loss against a target made with the pair
+    table perturbed (sigma 4 -> 4.2 A), the device's noise and checkpoints."""
+    win = Window(w, steps, checkpoint_every=C5_EVERY, rdf=rdf)
+    try:
+        pos0 = win.dev["pos"].clone()
+        pv0, bv0 = win.pair_values().float(), win.bond_values().float()
+        win.set_tables(torch.from_numpy(W.wca_table(sigma=4.2).values).cuda(), bv0)
+        target = win.histogram(win.forward(pos0)) * win.norm
+        pv = pv0.clone().requires_grad_(True)
+        bv = bv0.clone().requires_grad_(True)
+        p0 = pos0.clone().requires_grad_(True)
+        loss = BDWindowLoss.apply(pv, bv, p0, win, target)
+        gp, gb, g0 = torch.autograd.grad(loss, [pv, bv, p0])
+        ckpt = win.checkpoints()[:, :, :3].double().cpu().numpy()
+        torch.cuda.synchronize()
+        noise = _noise(win, steps)
+        return dict(loss=loss.item(), gp=gp.double().cpu().numpy(), gb=gb.double().cpu().numpy(),
+                    g0=g0[:, :3].double().cpu().numpy(), ckpt=ckpt, noise=noise,
+                    target=target.cpu().numpy())
+    finally:
+        win.close()
+
+
+def _fp64_grads(A, tr, rdf, w, tgt):
+    norm = rdf.norm(w.n, float(np.prod(w.box_size)))
+    h = A.rdf(tr[-1], rdf.bins, rdf.bin_width, rdf.r_max, rdf.sigma)
+    dldh = 2.0 * (h * norm - tgt) * norm
+    lam = A.rdf_grad(tr[-1], rdf.bins, rdf.bin_width, rdf.r_max, rdf.sigma, dldh)
+    c0, cp, cb = A.backward(tr, lam)
+    return float(np.sum((h * norm - tgt) ** 2)), cp, cb, c0
+
+
+@pytest.mark.slow
+def test_window_gradients_c5_match_fp64_adjoint(oracle):
+    """The benchmark's adjoint workload (16 chains x 1,024 beads, box 378 A,
+    bonds, angles, 1-2/1-3 exclusions, WCA table), checkpoints every 20 steps,
+    the device's Philox noise. Gradients with respect to the 200 pair-table
+    entries, the 200 bond-table entries and the 16,384 x 3 initial positions,
+    each within 1e-4 of its largest FP64 component:
+
+    * the full 200-step window against the FP64 adjoint along the device's own
+      checkpoints (each 20-step segment recomputed in FP64 from the device's
+      checkpoint, as the device's reverse sweep recomputes it in FP32);
+    * a 20-step window (one segment) against the FP64 adjoint of the FP64
+      forward from the same x_0.
+
+    The tangent dynamics of this model grow by about 10^4 over 200 steps (the
+    forces are piecewise constant in distance, so no radial stiffness damps a
+    perturbation), so an FP32 and an FP64 forward from the same x_0 drift apart
+    over the full window; that comparison is printed, not asserted."""
+    w = _c5_workload()
+    rdf = RdfSpec()
+    A = _cpu_case(oracle, w)
+
+    d = _c5_device(w, C5_STEPS, rdf)
+    # FP64 recompute of each segment from the device's checkpoint.
+    segs = []
+    for s in range(len(d["ckpt"])):
+        seg = A.forward(d["ckpt"][s], d["noise"][s * C5_EVERY:(s + 1) * C5_EVERY])
+        segs.append(seg if s == len(d["ckpt"]) - 1 else seg[:-1])
+    tr = np.concatenate(segs)
+    assert len(tr) == C5_STEPS + 1
+    loss64, cp, cb, c0 = _fp64_grads(A, tr, rdf, w, d["target"])
+    errs = (_rel(d["gp"], cp), _rel(d["gb"], cb), _rel(d["g0"], c0))
+    print(f"C5 200 steps vs FP64 along the device checkpoints: loss {d['loss']:.6e} / "
+          f"{loss64:.6e}; pair table {errs[0]:.2e}, bond table {errs[1]:.2e}, positions "
+          f"{errs[2]:.2e}")
+    own = _fp64_grads(A, A.forward(w.pos[:, :3].astype(np.float64), d["noise"]), rdf, w,
+                      d["target"])
+    print(f"C5 200 steps vs FP64 on its own trajectory (not asserted): loss {own[0]:.6e}; "
+          f"pair table {_rel(d['gp'], own[1]):.2e}, bond table {_rel(d['gb'], own[2]):.2e}, "
+          f"positions {_rel(d['g0'], own[3]):.2e}")
+    assert abs(d["loss"] - loss64) <= 1e-4 * abs(loss64)
+    assert max(errs) <= 1e-4, errs
+
+    d20 = _c5_device(w, C5_EVERY, rdf)
+    loss20, cp, cb, c0 = _fp64_grads(A, A.forward(w.pos[:, :3].astype(np.float64), d20["noise"]),
+                                     rdf, w, d20["target"])
+    errs20 = (_rel(d20["gp"], cp), _rel(d20["gb"], cb), _rel(d20["g0"], c0))
+    print(f"C5 system, 20 steps vs FP64 forward and adjoint: loss {d20['loss']:.6e} / "
+          f"{loss20:.6e}; pair table {errs20[0]:.2e}, bond table {errs20[1]:.2e}, positions "
+          f"{errs20[2]:.2e}")
+    assert abs(d20["loss"] - loss20) <= 1e-4 * abs(loss20)
+    assert max(errs20) <= 1e-4, errs20

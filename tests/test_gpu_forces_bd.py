@@ -1,9 +1,16 @@
 """CUDA pair/bond/angle forces, Philox, grid force and BD step against the oracle.
 
 Tolerances (float32 arithmetic):
-* Each pair's float force is rounded exactly as the reference's; per-particle
-  sums differ only by accumulation order, so the error is bounded relative to
-  the sum of |pair force| on that particle: <= 1e-5.
+* Per-particle forces: |F_gpu - F_64| / max(|F_64|, 1e-3 F_rms) <= 1e-5, with
+  F_64 the FP64 oracle's sum and F_rms the RMS force over all particles. Each
+  pair's float force is rounded exactly as the reference's, so the gap is the
+  float summation order alone. The error relative to the sum of |pair force|
+  on the particle is held to 1e-5 as well.
+* Angles: the tabulated force is constant within a table bin, and the device
+  acosf and the host's acos may differ by an ulp or two, so an angle within
+  rounding of a bin edge can take the neighbouring bin's force on one side.
+  The particles of such angles are counted and reported; every other particle
+  is held to the bar above.
 * Energies: FP64 device reduction vs the FP64 oracle, <= 1e-6 relative.
 * Philox words: bit-exact. BD positions: the Box-Muller transcendentals are
   CUDA's logf/sinf/cosf vs host libm (a few ulp), so positions agree to
@@ -25,11 +32,11 @@ from mars_md_b200.engine import setup_workload
 pytestmark = pytest.mark.gpu
 
 
-def _pair_case(ctx, oracle, w, lanes=0):
+def _pair_case(ctx, oracle, w, lanes=0, split=False):
     dev = setup_workload(ctx, w)
     if lanes:
         ctx.set_lanes_per_row(lanes)
-    ctx.build_pairlist(dev["pos"], dev["type"], w.list_radius)
+    ctx.build_pairlist(dev["pos"], dev["type"], w.list_radius, w.cutoff if split else 0.0)
     pairs = ctx.export_pairs().cpu().numpy()
     ctx.reset_energies()
     ctx.pair_forces(dev["pos"], dev["type"], dev["fe"], w.cutoff, get_energy=True)
@@ -42,12 +49,15 @@ def _pair_case(ctx, oracle, w, lanes=0):
     return fe, f64, fabs, e, e64
 
 
-@pytest.mark.parametrize("lanes", [0, 4, 8, 16, 32])
-def test_pair_forces_plain_bd(ctx_factory, oracle, lanes):
+@pytest.mark.parametrize("lanes,split", [(0, False), (0, True), (4, False), (8, True),
+                                         (16, False), (32, True)])
+def test_pair_forces_plain_bd(ctx_factory, oracle, lanes, split):
     w = W.plain_bd()
     ctx = ctx_factory(w.n)
-    fe, f64, fabs, e, e64 = _pair_case(ctx, oracle, w, lanes)
+    fe, f64, fabs, e, e64 = _pair_case(ctx, oracle, w, lanes, split)
     scaled, plain = force_errors(fe, f64, fabs)
+    print(f"plain_bd lanes={lanes} split={split}: worst {plain:.3e} (scaled {scaled:.3e})")
+    assert plain <= 1e-5, (plain, scaled)
     assert scaled <= 1e-5, (scaled, plain)
     # per-particle energy halves sum to the pair energy
     assert abs(fe[:, 3].astype(np.float64).sum() - f64[:, 3].sum()) <= 1e-5 * abs(f64[:, 3]).sum()
@@ -56,14 +66,49 @@ def test_pair_forces_plain_bd(ctx_factory, oracle, lanes):
     assert np.abs(fe[:, :3].astype(np.float64).sum(0)).max() <= 1e-3 * fabs.sum() / len(fabs)
 
 
-def test_pair_forces_large_types(ctx_factory, oracle):
+@pytest.mark.parametrize("split", [False, True])
+def test_pair_forces_large_types(ctx_factory, oracle, split):
     # 4 types, 10 tables, Debye-Hueckel + soft core, at 1/64 of the full size
     w = W.large_plain(n=32768)
     ctx = ctx_factory(w.n)
-    fe, f64, fabs, e, e64 = _pair_case(ctx, oracle, w)
+    fe, f64, fabs, e, e64 = _pair_case(ctx, oracle, w, split=split)
     scaled, plain = force_errors(fe, f64, fabs)
+    print(f"large_plain 32768 split={split}: worst {plain:.3e} (scaled {scaled:.3e})")
+    assert plain <= 1e-5, (plain, scaled)
     assert scaled <= 1e-5, (scaled, plain)
     assert abs(e[0] - e64) <= 1e-6 * abs(e64)
+
+
+@pytest.mark.slow
+def test_pair_forces_large_plain_full_size_sample(ctx_factory, oracle):
+    """All 2,097,152 forces of the benchmark workload from the GPU (rows split
+    at the cutoff, as the fused step builds them); 65,536 strided particles
+    checked against FP64 sums the oracle forms from the exported pairs that
+    touch them (the pair set itself is checked at this size elsewhere)."""
+    w = W.large_plain()
+    ctx = ctx_factory(w.n)
+    dev = setup_workload(ctx, w)
+    ctx.build_pairlist(dev["pos"], dev["type"], w.list_radius, w.cutoff)
+    dev["fe"].zero_()
+    ctx.pair_forces(dev["pos"], dev["type"], dev["fe"], w.cutoff, get_energy=False)
+    fe = dev["fe"].cpu().numpy()
+    sample = np.arange(0, w.n, 32)
+    mask = torch.zeros(w.n, dtype=torch.bool, device="cuda")
+    mask[torch.from_numpy(sample).cuda()] = True
+    pairs = ctx.export_pairs()
+    keep = mask[pairs[:, 0].long()] | mask[pairs[:, 1].long()]
+    sub = pairs[keep].cpu().numpy()
+    del pairs, keep
+    torch.cuda.empty_cache()
+    tags = oracle.resolve_tags(sub, w.type_ids, w.term_matrix, w.num_types)
+    _, f64, fabs = oracle.pair_forces(sub, w.pos, tags, tableset(w), box_of(w),
+                                      np.float32(w.cutoff) ** 2)
+    # F_rms over the sample stands in for the RMS over all particles.
+    scaled, plain = force_errors(fe[sample], f64[sample], fabs[sample])
+    print(f"large_plain full size, {len(sample)} particles, {len(sub)} pairs: worst {plain:.3e} "
+          f"(scaled {scaled:.3e})")
+    assert plain <= 1e-5, (plain, scaled)
+    assert scaled <= 1e-5, (scaled, plain)
 
 
 def test_pair_forces_match_reference_functor(ctx_factory, oracle, ref):
@@ -99,13 +144,42 @@ def test_bond_and_angle_forces(ctx_factory, oracle):
     at = pyoracle.TableSet([(t.values, t.start, t.step_inv) for t in w.angle_tables], periodic=True)
     _, b64, babs = oracle.bond_forces(w.bonds, w.bond_table_idx, w.pos, bt, box_of(w))
     _, a64, aabs = oracle.angle_forces(w.angles, w.angle_table_idx, w.pos, at, box_of(w))
-    sb, _ = force_errors(fb, b64, babs)
-    assert sb <= 1e-5
-    # acosf (CUDA) vs double acos rounded (host): the angle itself differs by an ulp
-    sa, _ = force_errors(fa, a64, aabs)
-    assert sa <= 1e-4, sa
+    sb, pb = force_errors(fb, b64, babs)
+    print(f"bonds: worst {pb:.3e} (scaled {sb:.3e})")
+    assert pb <= 1e-5 and sb <= 1e-5, (pb, sb)
+    # Angles within rounding of a table-bin edge may take the neighbouring
+    # bin's force (device acosf vs host acos): their particles are reported.
+    edge = _angles_near_bin_edge(w, tol=2e-5)
+    touched = np.zeros(w.n, bool)
+    touched[w.angles[edge, :3].ravel()] = True
+    ok = ~touched
+    sa, pa = force_errors(fa[ok], a64[ok], aabs[ok])
+    print(f"angles: {int(edge.sum())} of {len(w.angles)} within 2e-5 rad of a bin edge "
+          f"({int(touched.sum())} particles set aside); others worst {pa:.3e} (scaled {sa:.3e})")
+    assert edge.sum() <= max(3, len(w.angles) // 500)
+    assert pa <= 1e-5 and sa <= 1e-5, (pa, sa)
     assert abs(e[2] - b64[:, 3].sum()) <= 1e-6 * abs(b64[:, 3]).sum()
     assert abs(e[3] - a64[:, 3].sum()) <= 1e-5 * abs(a64[:, 3]).sum()
+
+
+def _angles_near_bin_edge(w, tol):
+    """Angles whose FP64 angle lies within tol radians of an edge of their
+    (periodic, degree-abscissa) table's bins."""
+    p = w.pos[:, :3].astype(np.float64)
+    L = np.array(w.box_size, np.float64)
+    a = w.angles[:, :3]
+
+    def wrap(d):
+        return d - L * np.floor(d / L + 0.5)
+    ab = np.linalg.norm(wrap(p[a[:, 1]] - p[a[:, 0]]), axis=1)
+    bc = np.linalg.norm(wrap(p[a[:, 2]] - p[a[:, 1]]), axis=1)
+    ac = np.linalg.norm(wrap(p[a[:, 2]] - p[a[:, 0]]), axis=1)
+    cos = np.clip((ab ** 2 + bc ** 2 - ac ** 2) / (2 * ab * bc), -1.0, 1.0)
+    th = np.arccos(cos)
+    t = w.angle_tables[0]
+    step = 1.0 / float(t.step_inv)
+    u = (th - float(t.start)) / step
+    return np.abs(u - np.round(u)) * step < tol
 
 
 def test_bond_chain_end_forces(ctx_factory, oracle):

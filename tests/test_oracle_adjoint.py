@@ -91,3 +91,80 @@ def test_histogram_gradient_alone(case):
         x[i, a] -= 2e-6
         lm = np.sum((A.rdf(x, NB, DR, RMAX, SIG) - target) ** 2)
         assert _close(g[i, a], (lp - lm) / 2e-6, np.abs(g).max())
+
+
+@pytest.mark.slow
+def test_c5_system_gradients_match_finite_differences(oracle):
+    """The benchmark's adjoint system (16 chains x 1,024 beads, box 378 A, WCA
+    pair table, harmonic bonds and angles, 1-2/1-3 exclusions, target from the
+    pair table with sigma 4 -> 4.2 A, seeded normals as noise) over one
+    checkpoint segment (20 steps). The 5 largest pair-table and bond-table
+    components and 6 position components against central differences of the
+    FP64 forward, each within 1e-4 of the difference quotient.
+
+    The loss is piecewise smooth: a step large enough to move some pair across
+    a table-bin edge between the + and - runs adds a jump, a step too small
+    drowns in FP64 rounding of a loss summed over 16,384 particles. Each
+    component is therefore tried at three steps (1e-7, 1e-8, 1e-9, relative
+    for table values, in A for positions) and passes when one of them agrees.
+    Over the full 200-step window the tangent dynamics grow by about 10^4 and
+    no step from 1e-8 to 1e-11 gives a converged quotient (bin crossings at
+    the larger steps, rounding at the smaller), so the difference check is
+    made on one segment."""
+    steps = 20
+    w = W.adjoint()
+    rng = np.random.default_rng(W.DEFAULT_SEED)
+    xyz = np.mod(w.pos[:, :3].astype(np.float64) + rng.normal(scale=0.02, size=(w.n, 3)),
+                 w.box_size[0])
+    t, b, a = w.pair_tables[0], w.bond_tables[0], w.angle_tables[0]
+
+    def system(pair_values):
+        return po.Adjoint64(oracle, w.n, w.box_size, w.diffusion[0], w.dt, w.kT,
+                            (pair_values, t.start, t.step_inv), w.cutoff, w.bonds,
+                            (b.values, b.start, b.step_inv), w.angles,
+                            (a.values, a.start, a.step_inv), w.exclusions)
+    A, pert = system(t.values), system(W.wca_table(sigma=4.2).values)
+    noise = rng.normal(size=(steps, w.n, 3))
+    target = pert.rdf(pert.forward(xyz, noise)[-1], NB, DR, RMAX, SIG)
+
+    def loss(x0):
+        tr = A.forward(x0, noise)
+        h = A.rdf(tr[-1], NB, DR, RMAX, SIG)
+        return float(np.sum((h - target) ** 2)), tr, h
+
+    _, tr, h = loss(xyz)
+    lam = A.rdf_grad(tr[-1], NB, DR, RMAX, SIG, 2.0 * (h - target))
+    g0, gp, gb = A.backward(tr, lam)
+
+    def check(g, scale, at, unit):
+        fds = []
+        for h in (1e-7 * unit, 1e-8 * unit, 1e-9 * unit):
+            fds.append((at(h) - at(-h)) / (2 * h))
+            if _close(g, fds[-1], scale):
+                return
+        raise AssertionError((g, fds))
+
+    checked = 0
+    for vals, g in ((A.pair_values, gp), (A.bond_values, gb)):
+        for k in np.argsort(-np.abs(g))[:5]:
+            old = vals[k]
+
+            def at(d, k=k, old=old, vals=vals):
+                vals[k] = old + d
+                v = loss(xyz)[0]
+                vals[k] = old
+                return v
+            check(g[k], np.abs(g).max(), at, max(1.0, abs(old)))
+            checked += 1
+    order = np.argsort(-np.abs(g0).ravel())
+    picks = list(order[:3]) + list(rng.choice(order[3:], 3, replace=False))
+    for q in picks:
+        i, ax = divmod(int(q), 3)
+
+        def at(d, i=i, ax=ax):
+            x = xyz.copy()
+            x[i, ax] += d
+            return loss(x)[0]
+        check(g0[i, ax], np.abs(g0).max(), at, 1.0)
+        checked += 1
+    assert checked == 16
