@@ -105,24 +105,32 @@ __global__ void __launch_bounds__(256) adj_pair_kernel(
 		const uint32_t* col = nbr + (static_cast<size_t>(i / H) * cap) * H + (i % H);
 		float tx = 0.0f, ty = 0.0f, tz = 0.0f;
 		for (uint32_t t = sub; t < cnt; t += G) {
-			const uint32_t j = __ldg(col + static_cast<size_t>(t) * H) & ~kOrientBit;
+			const uint32_t e = __ldg(col + static_cast<size_t>(t) * H);
+			const uint32_t j = e & ~kOrientBit;
 			const float4 pj = sorted_pos[j];
-			float3 r = f3sub(pj, pi);
+			// Distance, cutoff test and table bin exactly as the forward pair
+			// kernel decides them (the pair oriented as the reference orients
+			// it, reference rounding), so the derivative is that of the map
+			// the forward computed.
+			const bool flip = (e & kOrientBit) != 0u;
+			float3 r = flip ? make_float3(__fsub_rn(pi.x, pj.x), __fsub_rn(pi.y, pj.y),
+										  __fsub_rn(pi.z, pj.z))
+							: make_float3(__fsub_rn(pj.x, pi.x), __fsub_rn(pj.y, pi.y),
+										  __fsub_rn(pj.z, pi.z));
 			r = wrap_diff(box, r.x, r.y, r.z);
-			const float r2 = r.x * r.x + r.y * r.y + r.z * r.z;
-			const float d = sqrtf(r2);
-			if (d < 1e-6f || (cutoff_sq > 0.0f && r2 > cutoff_sq)) continue;
+			const float d = __fsqrt_rn(len2(r.x, r.y, r.z));
+			if (d < 1e-6f || (cutoff_sq > 0.0f && __fmul_rn(d, d) > cutoff_sq)) continue;
 			const PairTableRef tr = trow[type_of(pj)];
 			if (tr.offset < 0) continue;
-			const float w = (d - tr.start) * tr.step_inv;
+			const float w = __fmul_rn(__fsub_rn(d, tr.start), tr.step_inv);
 			const int home = min(max(static_cast<int>(floorf(w)), 0), tr.last);
 			const float F = bin_f[tr.offset + home];
 			const float4 mj = mu_sorted[j];
-			const float inv = 1.0f / d;
+			const float inv = flip ? -1.0f / d : 1.0f / d;  // u points from i to j
 			const float ux = r.x * inv, uy = r.y * inv, uz = r.z * inv;
 			const float dvx = mj.x - mi.x, dvy = mj.y - mi.y, dvz = mj.z - mi.z;
 			const float ud = ux * dvx + uy * dvy + uz * dvz;
-			const float k = F * inv;
+			const float k = F / d;
 			const float gx = k * (dvx - ux * ud), gy = k * (dvy - uy * ud), gz = k * (dvz - uz * ud);
 			red_add_v4(&tan_sorted[j], gx, gy, gz, 0.0f);
 			tx -= gx;
@@ -156,13 +164,15 @@ __global__ void __launch_bounds__(256) adj_bond_kernel(
 	__syncthreads();
 	for (uint32_t b = blockIdx.x * blockDim.x + threadIdx.x; b < nb; b += gridDim.x * blockDim.x) {
 		const int2 e = bonds[b];
-		float3 r = f3sub(pos[e.y], pos[e.x]);
-		r = wrap_diff(box, r.x, r.y, r.z);
-		const float d = sqrtf(r.x * r.x + r.y * r.y + r.z * r.z);
+		// Distance and bin as the forward bond kernel decides them.
+		const float4 pa = pos[e.x], pb = pos[e.y];
+		float3 r = wrap_diff(box, __fsub_rn(pb.x, pa.x), __fsub_rn(pb.y, pa.y),
+							 __fsub_rn(pb.z, pa.z));
+		const float d = __fsqrt_rn(len2(r.x, r.y, r.z));
 		if (d < 1e-6f) continue;
 		const Table t = tables[table_idx[b]];
 		const int size = static_cast<int>(t.size);
-		int home = static_cast<int>(floorf((d - t.start) * t.step_inv));
+		int home = static_cast<int>(floorf(__fmul_rn(__fsub_rn(d, t.start), t.step_inv)));
 		if (home >= size - 1) continue;  // constant zero force: no derivative
 		if (home < 0) home = 0;
 		const float F = -(t.pot[home + 1] - t.pot[home]) * t.step_inv;
@@ -205,13 +215,25 @@ __global__ void __launch_bounds__(256) adj_angle_kernel(
 	const Dual ac2 = ac[0] * ac[0] + ac[1] * ac[1] + ac[2] * ac[2];
 	const Dual lab = dsqrt(ab2), lbc = dsqrt(bc2);
 	Dual cs = ((ab2 + bc2 - ac2) * dm(0.5f, 0.0f)) / (lab * lbc);
-	if (cs.v < -1.0f) cs = dm(-1.0f, 0.0f);
-	if (cs.v > 1.0f) cs = dm(1.0f, 0.0f);
+	// The angle, its table bin and the clamps as the forward angle kernel
+	// decides them (reference rounding); the duals carry the derivatives.
+	const float eab2 = len2(rab.x, rab.y, rab.z), ebc2 = len2(rbc.x, rbc.y, rbc.z),
+				eac2 = len2(rac.x, rac.y, rac.z);
+	float ecs = __fdiv_rn(__fmul_rn(__fsub_rn(__fadd_rn(eab2, ebc2), eac2), 0.5f),
+						  __fmul_rn(__fsqrt_rn(eab2), __fsqrt_rn(ebc2)));
+	if (ecs < -1.0f) {
+		ecs = -1.0f;
+		cs = dm(-1.0f, 0.0f);
+	}
+	if (ecs > 1.0f) {
+		ecs = 1.0f;
+		cs = dm(1.0f, 0.0f);
+	}
 	Dual sn = dsqrt(dm(1.0f, 0.0f) - cs * cs);
-	if (sn.v <= 1e-3f) sn = dm(1e-3f, 0.0f);
+	if (__fsqrt_rn(__fsub_rn(1.0f, __fmul_rn(ecs, ecs))) <= 1e-3f) sn = dm(1e-3f, 0.0f);
 	const Table t = tables[table_idx[q]];
 	const float F = table_lookup(t.pot, static_cast<int>(t.size), t.start, t.step_inv, 1,
-								 acosf(cs.v)).x;
+								 acosf(ecs)).x;
 	const Dual dudt = dm(-F, 0.0f) / sn;
 	const Dual inv_ab = dm(1.0f, 0.0f) / lab, inv_bc = dm(1.0f, 0.0f) / lbc;
 	const Dual s1 = dudt * inv_ab, c_ab = cs * inv_ab;

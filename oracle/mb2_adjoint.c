@@ -51,6 +51,13 @@ typedef struct {
 	const int* angles; /* (i, j, k, pad) */
 	int na;
 	adj_table angle;
+	/* 0: table bins, cutoffs and angle clamps decided in double. 1: decided
+	 * with the reference's float arithmetic on the float-rounded coordinates
+	 * (PeriodicBox::wrap_diff, Vector3::length2, sqrtf, TabulatedPotential's
+	 * w = (x - start) * step_inv, AngleGeometry's cosine and acosf), as the
+	 * float forward decides them; everything else stays double. With float
+	 * states this gives the derivative of the map a float forward computes. */
+	int float_bins;
 } adj_sys;
 
 /* Dual number: value and derivative along one direction. */
@@ -85,11 +92,36 @@ static int excluded(const adj_sys* s, int a, int b) {
 	return 0;
 }
 
+/* PeriodicBox::wrap_diff_scalar in float (PeriodicBox.h:453-461). */
+static float wrapf(float x, float l) {
+	const float inv = 1.0f / l;
+	const float image = floorf(x * inv);
+	x = x - image * l;
+	return x >= 0.5f * l ? x - l : x;
+}
+
+/* Minimum-image vector x_j - x_i and its length in the reference's float
+ * arithmetic. */
+static float float_dist(const adj_sys* s, const double* x, int i, int j, float r[3]) {
+	for (int a = 0; a < 3; ++a) r[a] = wrapf((float)x[3 * j + a] - (float)x[3 * i + a], (float)s->L[a]);
+	return sqrtf(r[0] * r[0] + r[1] * r[1] + r[2] * r[2]);
+}
+
+/* The table bin h of abscissa x (w = (x - start) * step_inv, floor) in float
+ * or double arithmetic. */
+static int table_home(const adj_table* t, double x, int in_float) {
+	if (in_float) {
+		const float w = ((float)x - (float)t->start) * (float)t->step_inv;
+		return (int)floorf(w);
+	}
+	return (int)floor((x - t->start) * t->step_inv);
+}
+
 /* Table force F(x) = -dU/dx of the bin's linear interpolant; *bin = home
- * (or -1 where the force is constant 0: past the end of a non-periodic table). */
-static double table_force(const adj_table* t, double x, int* bin, int* bin1) {
-	const double w = (x - t->start) * t->step_inv;
-	int home = (int)floor(w);
+ * (or -1 where the force is constant 0: past the end of a non-periodic table).
+ * in_float: the bin is decided in float arithmetic. */
+static double table_force_at(const adj_table* t, double x, int in_float, int* bin, int* bin1) {
+	int home = table_home(t, x, in_float);
 	if (t->periodic) {
 		home %= t->size;
 		if (home < 0) home += t->size;
@@ -107,6 +139,10 @@ static double table_force(const adj_table* t, double x, int* bin, int* bin1) {
 	return -(t->v[home1] - t->v[home]) * t->step_inv;
 }
 
+static double table_force(const adj_table* t, double x, int* bin, int* bin1) {
+	return table_force_at(t, x, 0, bin, bin1);
+}
+
 /* Central-pair term (pair or bond): force on j is F(r) u, on i -F(r) u, with
  * u = (x_j - x_i) / r. With mu: tangent of the forces along mu (t), and the
  * table gradient mu . dforce/dU (g). */
@@ -115,9 +151,21 @@ static void radial_term(const adj_sys* s, const adj_table* tab, double cutoff, i
 	double r[3];
 	for (int a = 0; a < 3; ++a) r[a] = min_image(x[3 * j + a] - x[3 * i + a], s->L[a]);
 	const double d = sqrt(r[0] * r[0] + r[1] * r[1] + r[2] * r[2]);
-	if (d < 1e-6 || (cutoff > 0.0 && d > cutoff)) return;
 	int h, h1;
-	const double F = table_force(tab, d, &h, &h1);
+	double F;
+	if (s->float_bins) {
+		/* The forward's float decisions: the pair's (i < j) float distance, the
+		 * cutoff test dist * dist > rc * rc and the bin (Pairwise.h:214-304,
+		 * BondComputer.h:168-191). */
+		float rf[3];
+		const float df = float_dist(s, x, i, j, rf);
+		const float cf = (float)cutoff;
+		if (df < 1e-6f || (cutoff > 0.0 && df * df > cf * cf)) return;
+		F = table_force_at(tab, (double)df, 1, &h, &h1);
+	} else {
+		if (d < 1e-6 || (cutoff > 0.0 && d > cutoff)) return;
+		F = table_force(tab, d, &h, &h1);
+	}
 	const double u[3] = {r[0] / d, r[1] / d, r[2] / d};
 	if (f)
 		for (int a = 0; a < 3; ++a) {
@@ -158,13 +206,38 @@ static void angle_term(const adj_sys* s, int i, int j, int k, const double* x, d
 	const dual ac2 = dadd(dadd(dmul(ac[0], ac[0]), dmul(ac[1], ac[1])), dmul(ac[2], ac[2]));
 	const dual lab = dsqrt(ab2), lbc = dsqrt(bc2);
 	dual cs = ddiv(dscale(dsub(dadd(ab2, bc2), ac2), 0.5), dmul(lab, lbc));
-	if (cs.v < -1.0) cs = dmk(-1.0, 0.0);
-	if (cs.v > 1.0) cs = dmk(1.0, 0.0);
-	const double angle = acos(cs.v);
-	dual sn = dsqrt(dsub(dmk(1.0, 0.0), dmul(cs, cs)));
-	if (sn.v <= 1e-3) sn = dmk(1e-3, 0.0);
 	int h, h1;
-	const double F = table_force(&s->angle, angle, &h, &h1);
+	double F;
+	dual sn;
+	if (s->float_bins) {
+		/* AngleGeometry (BondGeometry.h:19-44) in float: cosine by the law of
+		 * cosines, clamps, acosf, the sine floor, the periodic table bin. */
+		float rab[3], rbc[3], rac[3];
+		const float lab_f = float_dist(s, x, i, j, rab), lbc_f = float_dist(s, x, j, k, rbc);
+		float_dist(s, x, i, k, rac);
+		const float ab2f = rab[0] * rab[0] + rab[1] * rab[1] + rab[2] * rab[2];
+		const float bc2f = rbc[0] * rbc[0] + rbc[1] * rbc[1] + rbc[2] * rbc[2];
+		const float ac2f = rac[0] * rac[0] + rac[1] * rac[1] + rac[2] * rac[2];
+		float csf = (ab2f + bc2f - ac2f) * 0.5f / (lab_f * lbc_f);
+		if (csf < -1.0f) {
+			csf = -1.0f;
+			cs = dmk(-1.0, 0.0);
+		}
+		if (csf > 1.0f) {
+			csf = 1.0f;
+			cs = dmk(1.0, 0.0);
+		}
+		sn = dsqrt(dsub(dmk(1.0, 0.0), dmul(cs, cs)));
+		if (sqrtf(1.0f - csf * csf) <= 1e-3f) sn = dmk(1e-3, 0.0);
+		F = table_force_at(&s->angle, (double)acosf(csf), 1, &h, &h1);
+	} else {
+		if (cs.v < -1.0) cs = dmk(-1.0, 0.0);
+		if (cs.v > 1.0) cs = dmk(1.0, 0.0);
+		const double angle = acos(cs.v);
+		sn = dsqrt(dsub(dmk(1.0, 0.0), dmul(cs, cs)));
+		if (sn.v <= 1e-3) sn = dmk(1e-3, 0.0);
+		F = table_force(&s->angle, angle, &h, &h1);
+	}
 	const dual dudt = ddiv(dmk(-F, 0.0), sn);
 	const dual inv_ab = ddiv(dmk(1.0, 0.0), lab), inv_bc = ddiv(dmk(1.0, 0.0), lbc);
 	const dual s1 = dmul(dudt, inv_ab), c_ab = dmul(cs, inv_ab);

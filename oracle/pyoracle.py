@@ -842,7 +842,8 @@ class AdjSys(C.Structure):
                 ("s", C.c_double * 3), ("pair", AdjTable), ("cutoff", C.c_double),
                 ("excl_off", C.c_void_p), ("excl_nb", C.c_void_p), ("excl_n", C.c_int),
                 ("bonds", C.c_void_p), ("nb", C.c_int), ("bond", AdjTable),
-                ("angles", C.c_void_p), ("na", C.c_int), ("angle", AdjTable)]
+                ("angles", C.c_void_p), ("na", C.c_int), ("angle", AdjTable),
+                ("float_bins", C.c_int)]
 
 
 class Adjoint64:
@@ -851,7 +852,12 @@ class Adjoint64:
     C structure points to alive."""
 
     def __init__(self, oracle: "Oracle", n, box_len, diffusion, dt, kT, pair, cutoff,
-                 bonds=None, bond=None, angles=None, angle=None, exclusions=None):
+                 bonds=None, bond=None, angles=None, angle=None, exclusions=None,
+                 float_bins=False):
+        """The box edges are taken as float32 values, as the library holds
+        them. float_bins: decide table bins, cutoffs and angle clamps with the
+        reference's float arithmetic (the derivative of a float forward along
+        float states); otherwise in double."""
         L = self.lib = oracle.lib
         vp = C.c_void_p
         L.adj_forces64.argtypes = [vp, vp, vp]
@@ -863,8 +869,9 @@ class Adjoint64:
         s = self.sys = AdjSys()
         s.n = int(n)
         d = np.asarray(diffusion, np.float64).reshape(3)
+        s.float_bins = int(bool(float_bins))
         for a in range(3):
-            s.L[a] = float(box_len[a])
+            s.L[a] = float(np.float32(box_len[a]))
             s.c[a] = float(d[a] * dt / kT)
             s.s[a] = float(np.sqrt(2.0 * d[a] * dt))
         self.pair_values = self._table(s.pair, pair, False)

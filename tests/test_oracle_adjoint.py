@@ -168,3 +168,28 @@ def test_c5_system_gradients_match_finite_differences(oracle):
         check(g0[i, ax], np.abs(g0).max(), at, 1.0)
         checked += 1
     assert checked == 16
+
+
+def test_float_bin_decisions_match_double_off_edges(oracle):
+    """With float states away from table-bin edges, deciding bins in the
+    reference's float arithmetic gives the double adjoint's gradients."""
+    rng = np.random.default_rng(3)
+    nch, beads, L = 4, 32, 52.0
+    xyz = np.mod(W._chains(rng, nch, beads, L) + rng.normal(scale=0.02, size=(nch * beads, 3)),
+                 L).astype(np.float32).astype(np.float64)
+    bonds, angles, excl = W._topology(nch, beads)
+    wca, bt = W.wca_table(), W.harmonic_bond_table()
+    at = W.harmonic_angle_table(theta0_deg=150.0)
+    grads = []
+    for fb in (False, True):
+        A = po.Adjoint64(oracle, len(xyz), (L, L, L), (150.0, 150.0, 150.0), W.DT_NS, W.kT(),
+                         (wca.values, wca.start, wca.step_inv), 20.0, bonds,
+                         (bt.values, bt.start, bt.step_inv), angles,
+                         (at.values, at.start, at.step_inv), excl, float_bins=fb)
+        noise = rng.normal(size=(3, len(xyz), 3)) if not grads else grads[0][3]
+        tr = A.forward(xyz, noise)
+        h = A.rdf(tr[-1], NB, DR, RMAX, SIG)
+        g0, gp, gb = A.backward(tr, A.rdf_grad(tr[-1], NB, DR, RMAX, SIG, 2.0 * h))
+        grads.append((g0, gp, gb, noise))
+    for a, b in zip(grads[0][:3], grads[1][:3]):
+        assert np.abs(a - b).max() <= 1e-6 * np.abs(a).max()
