@@ -83,5 +83,48 @@ def build_cpp_mirror_test(verbose: bool = False) -> str:
     return CPP_TEST_BIN
 
 
+REF_ADAPTER_SRC = os.path.join(ROOT, "tests", "cpp", "ref_adapter", "ref_adapter_test.cpp")
+REF_ADAPTER_BIN = os.path.join(ROOT, "tests", "cpp", "_build", "ref_adapter_test")
+
+
+def reference_checkout():
+    """The reference source tree: the MARS_MD_REFERENCE environment variable,
+    else a directory named "reference" beside this repository; None if absent."""
+    path = os.environ.get("MARS_MD_REFERENCE") or os.path.join(os.path.dirname(ROOT), "reference")
+    return path if os.path.isdir(os.path.join(path, "src", "PatchOperation")) else None
+
+
+def build_ref_adapter_test(reference=None, verbose: bool = False):
+    """Compile the test program of the adapter that derives from the
+    reference's own MARS::Pairlist (host/b200_ref_adapter.hpp) against the
+    reference's headers, with tests/cpp/ref_adapter/inc standing in for the
+    reference's Backend layer (CUDA device memory) and the oracle harness's fmt
+    stand-in. Returns the binary, or None when no reference checkout is here
+    and no binary was built earlier."""
+    reference = reference or reference_checkout()
+    if reference is None:
+        return REF_ADAPTER_BIN if os.path.exists(REF_ADAPTER_BIN) else None
+    lib = build(verbose)
+    shim = os.path.join(ROOT, "tests", "cpp", "ref_adapter", "inc")
+    deps = [REF_ADAPTER_SRC, lib, os.path.join(ROOT, "include", "marsb200.h"),
+            os.path.join(HOST_DIR, "b200_ref_adapter.hpp")] + \
+        glob.glob(os.path.join(shim, "Backend", "*.h"))
+    if _stale(REF_ADAPTER_BIN, deps):
+        os.makedirs(os.path.dirname(REF_ADAPTER_BIN), exist_ok=True)
+        cuda = os.path.dirname(os.path.dirname(NVCC))
+        cmd = ["g++", "-std=c++20", "-O2", "-ffp-contract=off", "-Wall",
+               "-I" + shim, "-I" + os.path.join(ROOT, "oracle", "ref_harness", "shim", "inc"),
+               "-I" + os.path.join(reference, "src"), "-I" + os.path.join(ROOT, "include"),
+               "-I" + HOST_DIR, "-I" + os.path.join(cuda, "include"), REF_ADAPTER_SRC,
+               "-o", REF_ADAPTER_BIN, "-L" + HERE, "-lmarsb200",
+               "-L" + os.path.join(cuda, "lib64"), "-lcudart",
+               "-Wl,-rpath,$ORIGIN/../../../mars_md_b200",
+               "-Wl,-rpath," + os.path.join(cuda, "lib64")]
+        if verbose:
+            print(" ".join(cmd), flush=True)
+        subprocess.run(cmd, check=True)
+    return REF_ADAPTER_BIN
+
+
 if __name__ == "__main__":
     print(build(verbose="-v" in sys.argv))
