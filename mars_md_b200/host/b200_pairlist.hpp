@@ -27,9 +27,12 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cmath>
 #include <cstddef>
 #include <cstdint>
+#include <fstream>
 #include <memory>
+#include <sstream>
 #include <stdexcept>
 #include <string>
 #include <utility>
@@ -475,6 +478,99 @@ struct Table {
 	std::vector<float> values;
 	float start = 0.0f;
 	float step_inv = 0.0f;
+};
+
+// Kinds of tabulated potential (src/Objects/Tables.h:21).
+enum class TabulatedType { NonBondedPair, Bond, Angle, Dihedral, Default };
+
+// A table read from the reference's "x y" text files, restating
+// Table::read_file, check_same_step_size and convert_angular_abscissa_to_radians
+// (src/Objects/Tables.h:27-120): lines whose first character is '#' are
+// comments; a line that does not start with two numbers is skipped with a
+// warning; numbers are read into float by stream extraction; step = X[1] - X[0]
+// and start = X[0] in float, uniform unless some |X[i] - X[i-1]| - step exceeds
+// 1e-4 (a warning only, as in the reference); angle and dihedral abscissae are
+// degrees, multiplied by float(pi / 180) after the check. The reference's
+// warnings are kept in `warnings` instead of being logged.
+struct TableFile {
+	std::string name;
+	TabulatedType type;
+	float step_size = 0.0f;
+	float start = 0.0f;
+	std::vector<float> X, Y;
+	std::vector<std::string> warnings;
+
+	explicit TableFile(TabulatedType t) : type(t) {
+		if (t == TabulatedType::Dihedral) start = static_cast<float>(-3.14159265358979323846);
+	}
+
+	bool check_same_step_size() {
+		if (X.size() < 2) {
+			warnings.push_back("Table " + name + ": Not enough values to check step size");
+			return false;
+		}
+		step_size = X[1] - X[0];
+		start = X[0];
+		for (size_t i = 2; i < X.size(); ++i) {
+			const float d = std::fabs(X[i] - X[i - 1]) - step_size;
+			if (d > 1e-4) {
+				warnings.push_back("Table " + name + ": Step size is not the same for all values at index " +
+								   std::to_string(i));
+				return false;
+			}
+		}
+		return true;
+	}
+
+	void read_file(const std::string& file_name, const std::string& name_ = "") {
+		if (name_.empty()) {
+			const size_t slash = file_name.find_last_of('/');
+			std::string stem = slash == std::string::npos ? file_name : file_name.substr(slash + 1);
+			const size_t dot = stem.find_last_of('.');
+			name = dot == std::string::npos || dot == 0 ? stem : stem.substr(0, dot);
+		} else {
+			name = name_;
+		}
+		std::ifstream in(file_name);
+		if (!in) throw Exception(ExceptionType::FileIoError, "Table::read_file: cannot open " + file_name);
+		std::string line;
+		size_t number = 0;
+		while (std::getline(in, line)) {
+			++number;
+			if (!line.empty() && line[0] == '#') continue;
+			std::istringstream iss(line);
+			float x = 0.0f, y = 0.0f;
+			if (iss >> x >> y) {
+				X.push_back(x);
+				Y.push_back(y);
+			} else {
+				warnings.push_back("Tables: Failed to parse line " + std::to_string(number) + ": " + line);
+			}
+		}
+		check_same_step_size();
+		convert_angular_abscissa_to_radians();
+	}
+
+	void convert_angular_abscissa_to_radians() {
+		if (type != TabulatedType::Angle && type != TabulatedType::Dihedral) return;
+		constexpr float deg_to_rad = static_cast<float>(3.14159265358979323846 / 180.0);
+		for (float& x : X) x *= deg_to_rad;
+		start *= deg_to_rad;
+		step_size *= deg_to_rad;
+	}
+
+	// The table as set_pair_tables / set_bonded_tables take it: the non-bonded
+	// step inverse is 1.0f / step (DevicePairNonBondedInteraction.h:183), the
+	// bonded one float(1.0 / double(step)) (DeviceBondedInteraction.h:213-214).
+	Table to_table() const {
+		Table t;
+		t.values = Y;
+		t.start = start;
+		t.step_inv = type == TabulatedType::NonBondedPair
+						 ? 1.0f / step_size
+						 : static_cast<float>(1.0 / static_cast<double>(step_size));
+		return t;
+	}
 };
 
 // Integrators of Patch::integrate_motion on this path (Patch.cpp:238-352).

@@ -564,6 +564,7 @@ class RefHarness:
         L.ref_neighbor_walk_items.argtypes = [vp, vp, vp, vp, vp, vp, f, sz, i, i, vp, vp, vp,
                                               vp, sz, vp, sz]
         L.ref_resolve_tags.argtypes = [vp, sz, vp, vp, sz, vp, i]
+        L.ref_read_table.argtypes = [C.c_char_p, i, vp, vp, sz, vp, vp, vp, vp]
         L.ref_pair_forces.argtypes = [vp, sz, vp, vp, vp, vp, vp, vp, vp, vp, vp, i, vp, vp, vp,
                                       i, f, u32]
         L.ref_bond_forces.argtypes = [vp, vp, vp, sz, vp, vp, vp, vp, vp, vp, vp, i, vp, vp, vp, i]
@@ -662,6 +663,20 @@ class RefHarness:
             len(items), _ptr(buf), max_pairs))
         pairs = None if buf is None else np.ascontiguousarray(buf[1: min(cnt, max_pairs) + 1])
         return pairs, cnt
+
+    def read_table(self, path, kind):
+        """Table::read_file of one text table; kind 0 pair, 1 bond, 2 angle,
+        3 dihedral. Returns (X, Y, start, step, uniform) as float32."""
+        cap = 1 << 20
+        x = np.zeros(cap, np.float32)
+        y = np.zeros(cap, np.float32)
+        n = C.c_size_t()
+        start, step, uniform = C.c_float(), C.c_float(), C.c_int()
+        rc = self.lib.ref_read_table(str(path).encode(), int(kind), _ptr(x), _ptr(y), cap,
+                                     C.byref(n), C.byref(start), C.byref(step), C.byref(uniform))
+        assert rc == 0 and n.value <= cap
+        return (x[:n.value].copy(), y[:n.value].copy(), np.float32(start.value),
+                np.float32(step.value), bool(uniform.value))
 
     def resolve_tags(self, pairs, type_ids, term_matrix, num_types, nthreads=1):
         tags = np.zeros(len(pairs), np.uint32)

@@ -16,6 +16,7 @@
 // the key gives the identical permutation.
 
 #include "IO/DcdWriter.h"
+#include "Objects/Tables.h"
 #include "Interactions/Bonded/BondComputer.h"
 #include "Interactions/Nonbonded/Pairwise.h"
 #include "PatchOperation/Integrator/BAOAB.h"
@@ -586,6 +587,30 @@ void ref_table_lookup(float x, float* values, uint32_t size, float start, float 
 	const ScalarForceEnergy fe = TabulatedPotential::compute(x, &t);
 	out2[0] = fe.force_magnitude;
 	out2[1] = fe.energy;
+}
+
+// Table::read_file (src/Objects/Tables.h:61-102) of one "x y" text file, with
+// the type's abscissa conversion. kind: 0 non-bonded pair, 1 bond, 2 angle,
+// 3 dihedral. Writes up to cap rows of X and Y, the row count, start, step and
+// whether check_same_step_size accepts the (unconverted) abscissa.
+int ref_read_table(const char* path, int kind, float* x_out, float* y_out, size_t cap,
+				   size_t* count, float* start, float* step, int* uniform) {
+	static const TabulatedType kinds[4] = {TabulatedType::NonBondedPair, TabulatedType::Bond,
+										   TabulatedType::Angle, TabulatedType::Dihedral};
+	if (kind < 0 || kind > 3) return -1;
+	Table t(kinds[kind]);
+	t.read_file(path);
+	*count = t.X.size();
+	for (size_t i = 0; i < t.X.size() && i < cap; ++i) {
+		x_out[i] = t.X[i];
+		y_out[i] = t.Y[i];
+	}
+	*start = t.start;
+	*step = t.step_size;
+	Table raw(TabulatedType::Bond);  // same file, no conversion: the step check alone
+	raw.read_file(path);
+	*uniform = raw.check_same_step_size() ? 1 : 0;
+	return 0;
 }
 
 } // extern "C"
