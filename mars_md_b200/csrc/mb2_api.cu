@@ -226,6 +226,9 @@ void morton_domain(mb2_context* ctx, const float4* pos, uint32_t n, cudaStream_t
 		for (int a = 0; a < 3; ++a) {
 			lo[a] = n ? o2f(h[a]) : std::numeric_limits<float>::max();
 			hi[a] = n ? o2f(h[3 + a]) : std::numeric_limits<float>::lowest();
+			// A NaN or infinite coordinate on an open axis has no Morton domain.
+			require(b.periodic[a] || (std::isfinite(lo[a]) && std::isfinite(hi[a])), MB2_ERR_ARG,
+					"mb2_build_pairlist: a particle has a non-finite coordinate on an open axis");
 		}
 	}
 	for (int a = 0; a < 3; ++a) {
@@ -248,7 +251,8 @@ void morton_domain(mb2_context* ctx, const float4* pos, uint32_t n, cudaStream_t
 }
 
 void sort_particles(mb2_context* ctx, const float4* pos, const int* type_ids, uint32_t n,
-					const float* bmin, const float* bmax, cudaStream_t st) {
+					const float* bmin, const float* bmax, cudaStream_t st,
+					unsigned long long* nonfinite = nullptr) {
 	ctx->keys.ensure(n);
 	ctx->s2o.ensure(n);
 	ctx->inv.ensure(n);
@@ -256,7 +260,7 @@ void sort_particles(mb2_context* ctx, const float4* pos, const int* type_ids, ui
 	morton_encode(pos, n, bmin, bmax, ctx->keys.ptr, ctx->s2o.ptr, st);
 	radix_sort_pairs(ctx->scratch, ctx->keys.ptr, ctx->s2o.ptr, n, st);
 	inverse_and_gather(ctx->s2o.ptr, n, pos, ctx->inv.ptr, nullptr, st);
-	pack_sorted_positions(pos, type_ids, ctx->s2o.ptr, n, ctx->sorted_pos.ptr, st);
+	pack_sorted_positions(pos, type_ids, ctx->s2o.ptr, n, ctx->sorted_pos.ptr, st, nonfinite);
 }
 
 // cutoff: the interaction cutoff the list will serve. When it lies in
@@ -270,10 +274,17 @@ void build(mb2_context* ctx, const float4* pos, const int* type_ids, uint32_t n,
 	require(rc_list > 0.0f && std::isfinite(rc_list), MB2_ERR_ARG,
 			"mb2_build_pairlist: pairlist cutoff must be positive and finite");
 	StageScope scope(ctx, MB2_STAGE_PAIRLIST, st);
+	// A failed build leaves no list behind.
+	ctx->built = false;
 	float bmin[3], bmax[3], extent[3];
 	morton_domain(ctx, pos, n, st, bmin, bmax);
 	for (int a = 0; a < 3; ++a) extent[a] = bmax[a] - bmin[a];
-	sort_particles(ctx, pos, type_ids, n, bmin, bmax, st);
+	// stats: [0] pairs, [1] longest row (both set by each walk), [2] particles
+	// with a non-finite coordinate (counted while packing, read with the
+	// walk's statistics, so no extra synchronisation).
+	ctx->stats.ensure(3);
+	MB2_CUDA(cudaMemsetAsync(ctx->stats.ptr + 2, 0, sizeof(unsigned long long), st));
+	sort_particles(ctx, pos, type_ids, n, bmin, bmax, st, ctx->stats.ptr + 2);
 
 	const float rc2 = rc_list * rc_list;
 	if (!ctx->grid_valid || ctx->grid_rc != rc_list || ctx->grid_n != n ||
@@ -333,16 +344,21 @@ void build(mb2_context* ctx, const float4* pos, const int* type_ids, uint32_t n,
 	fast_test_band(ctx->box, rc_list, &wg.fast_lo, &wg.fast_hi);
 	ctx->row_len.ensure(n);
 	ctx->row_far.ensure(n);
-	ctx->stats.ensure(2);
 	auto walk = [&](uint32_t cap) {
 		const int hshift = __builtin_ctz(32 / ctx->lanes);
 		build_walk(ctx->sorted_pos.ptr, ctx->keys.ptr, ctx->s2o.ptr, ctx->cell_begin.ptr,
 				   ctx->cell_end.ptr, ctx->stencil.ptr, g.num_stencil, wg, n, ctx->box, ctx->excl,
 				   ctx->nbr.ptr, cap, hshift, ctx->row_len.ptr, ctx->row_far.ptr, ctx->stats.ptr,
 				   st);
-		MB2_CUDA(cudaMemcpyAsync(ctx->pinned, ctx->stats.ptr, 2 * sizeof(uint64_t),
+		MB2_CUDA(cudaMemcpyAsync(ctx->pinned, ctx->stats.ptr, 3 * sizeof(uint64_t),
 								 cudaMemcpyDeviceToHost, st));
 		MB2_CUDA(cudaStreamSynchronize(st));
+		// The walk runs on such particles without harm (cell indices come from
+		// the clamped Morton keys, and a NaN fails every distance test), but
+		// the list is not the reference's meaning of one: refuse it.
+		require(ctx->pinned[2] == 0, MB2_ERR_ARG,
+				"mb2_build_pairlist: " + std::to_string(ctx->pinned[2]) +
+					" particle(s) with a NaN or infinite coordinate");
 		return std::make_pair(ctx->pinned[0], ctx->pinned[1]);
 	};
 	auto choose_lanes = [&](double mean) {
@@ -443,6 +459,8 @@ void upload_tables(DevBuf<Table>& tbuf, DevBuf<float>& vbuf, int num_tables, con
 	size_t total = 0;
 	for (int k = 0; k < num_tables; ++k) {
 		require(sizes[k] >= 2, MB2_ERR_ARG, "table needs at least 2 values");
+		require(std::isfinite(starts[k]) && std::isfinite(step_invs[k]) && step_invs[k] != 0.0f,
+				MB2_ERR_ARG, "table start and step inverse must be finite, step inverse nonzero");
 		total += sizes[k];
 	}
 	vbuf.ensure(total);

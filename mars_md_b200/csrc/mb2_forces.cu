@@ -26,6 +26,7 @@
 // FP64: total pair energy and virial are reduced in double on the device
 // (per-thread double, block reduction, one double atomic per block).
 #include <algorithm>
+#include <cmath>
 #include <type_traits>
 #include <vector>
 
@@ -719,6 +720,10 @@ size_t pair_table_arrays(int num_types, const uint32_t* term_matrix, int num_tab
 	size_t total = 0;
 	for (int k = 0; k < num_tables; ++k) {
 		expect_arg(sizes[k] >= 2, MB2_ERR_ARG, "pair tables: a table needs 2 values");
+		// A step of 0 (fewer than two distinct abscissae) gives an infinite
+		// inverse: refused, as is a NaN or infinite start.
+		expect_arg(std::isfinite(starts[k]) && std::isfinite(step_invs[k]) && step_invs[k] != 0.0f,
+				   MB2_ERR_ARG, "pair tables: start and step inverse must be finite, step inverse nonzero");
 		offset[k] = static_cast<uint32_t>(total);
 		total += sizes[k];
 	}

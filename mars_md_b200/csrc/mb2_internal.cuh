@@ -169,8 +169,11 @@ void export_pairs(const uint32_t* nbr, const uint32_t* row_len, const uint32_t* 
 				  cudaStream_t st);
 void max_displacement_sq(const float4* cur, const float4* prev, uint32_t n, const Box& box,
 						 unsigned int* out_bits, cudaStream_t st);
+// nonfinite (optional): incremented once per particle with a NaN or infinite
+// coordinate.
 void pack_sorted_positions(const float4* pos, const int* type_ids, const uint32_t* s2o,
-						   uint32_t n, float4* sorted_pos, cudaStream_t st);
+						   uint32_t n, float4* sorted_pos, cudaStream_t st,
+						   unsigned long long* nonfinite = nullptr);
 
 // forces.cu
 // Per type pair: the tabulated table's lookup constants and offset into the

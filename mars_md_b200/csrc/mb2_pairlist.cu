@@ -706,11 +706,13 @@ __global__ void __launch_bounds__(256) displacement_kernel(const float4* __restr
 __global__ void __launch_bounds__(256) pack_kernel(const float4* __restrict__ pos,
 												   const int* __restrict__ type_ids,
 												   const uint32_t* __restrict__ s2o, uint32_t n,
-												   float4* __restrict__ sorted_pos) {
+												   float4* __restrict__ sorted_pos,
+												   unsigned long long* nonfinite) {
 	const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
 	if (s >= n) return;
 	const uint32_t o = s2o[s];
 	float4 p = pos[o];
+	if (nonfinite && !(isfinite(p.x) && isfinite(p.y) && isfinite(p.z))) atomicAdd(nonfinite, 1ull);
 	p.w = __int_as_float(type_ids ? type_ids[o] : 0);
 	sorted_pos[s] = p;
 }
@@ -783,9 +785,11 @@ void max_displacement_sq(const float4* cur, const float4* prev, uint32_t n, cons
 }
 
 void pack_sorted_positions(const float4* pos, const int* type_ids, const uint32_t* s2o,
-						   uint32_t n, float4* sorted_pos, cudaStream_t st) {
+						   uint32_t n, float4* sorted_pos, cudaStream_t st,
+						   unsigned long long* nonfinite) {
 	if (n == 0) return;
-	MB2_LAUNCH pack_kernel<<<(n + 255) / 256, 256, 0, st>>>(pos, type_ids, s2o, n, sorted_pos);
+	MB2_LAUNCH pack_kernel<<<(n + 255) / 256, 256, 0, st>>>(pos, type_ids, s2o, n, sorted_pos,
+															 nonfinite);
 }
 
 }  // namespace mb2
