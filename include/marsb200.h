@@ -537,18 +537,32 @@ MB2_API int mb2_batch_run(mb2_batch* b, float* pos4, float* force_energy4, const
 MB2_API int mb2_batch_set_tuning(mb2_batch* b, int level_offset, int lanes);
 MB2_API int mb2_batch_tuning(const mb2_batch* b, int* level_offset, int* lanes,
                      uint32_t* total_cells);
+/* Rebuild cadence: with period > 0, mb2_batch_step and mb2_batch_run rebuild
+ * at every period-th step (skipped while no particle moved more than half the
+ * skin, the rule of Patch.cpp:86-108) instead of at params->rebuild_period;
+ * 0 (the default) uses the params'. mb2_batch_autotune sets it to its choice.
+ * mb2_batch_rebuild_schedule reports the cadence in force and the number of
+ * list builds so far. */
+MB2_API int mb2_batch_set_rebuild_period(mb2_batch* b, uint32_t period);
+MB2_API int mb2_batch_rebuild_schedule(const mb2_batch* b, uint32_t* period, uint64_t* rebuilds);
 /* Autotuner: times one pairlist build and `trial_steps` steps for each cell
  * level offset in {-1, 0, +1} and lanes per row in {4, 8, 16} on a copy of
- * the positions, keeps the pair minimising build / rebuild_period + step, and
- * measures, from a fresh list, the largest rebuild cadence (<= the period)
- * whose maximum displacement stays within half the skin. Positions are not
- * changed; the next step rebuilds the list with the chosen knobs. */
+ * the positions, and keeps the pair minimising build / rebuild_period + step.
+ * Then the rebuild cadence, on the copy: after an equilibration segment of
+ * one params->rebuild_period (so the overlaps of a fresh start have relaxed),
+ * two intervals of one period, each from a fresh list, record the largest
+ * displacement after every step; the cadence is the largest k <= the period
+ * whose displacement stayed within half the skin in both (at least 1). The
+ * chosen knobs and cadence are put in force (mb2_batch_set_tuning,
+ * mb2_batch_set_rebuild_period) and reported; max_displacement_at_period is
+ * the displacement after a whole period from a fresh list. Positions are not
+ * changed; the next step rebuilds the list. */
 typedef struct {
     int level_offset;                  /* chosen cell level offset */
     int lanes;                         /* chosen lanes per row */
     float build_ms;                    /* pairlist build time with the choice */
     float step_ms;                     /* force-and-integrate time per step */
-    uint32_t safe_rebuild_period;      /* largest cadence keeping the list exact */
+    uint32_t safe_rebuild_period;      /* chosen cadence, put in force */
     float max_displacement_at_period;  /* largest displacement after rebuild_period steps (A) */
     uint32_t total_cells;
 } mb2_batch_tuning_result;

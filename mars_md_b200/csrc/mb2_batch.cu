@@ -266,6 +266,10 @@ struct mb2_batch {
 	uint32_t total_cells = 0;
 	float grid_rc = -1.0f;
 	int level_offset = 0;
+	// Rebuild cadence in force (0: the params' rebuild_period), set by
+	// mb2_batch_set_rebuild_period or chosen by mb2_batch_autotune.
+	uint32_t rebuild_period = 0;
+	unsigned long long rebuilds = 0;  // list builds since creation
 	DevBuf<unsigned long long> stats, step_d;
 	DevBuf<unsigned int> disp;
 	DevBuf<double> energy;
@@ -486,14 +490,21 @@ void check_step_args(mb2_batch* b, const float* pos4, const float* fe4, const in
 // Rebuild decision of the reference (Patch.cpp:86-108), over all systems: at
 // the first step and at each rebuild period, rebuild when any system moved
 // more than half the skin since the last build.
+// The rebuild schedule of Patch.cpp:86-108 (a rebuild at every period step,
+// skipped while no particle moved more than half the skin) at the cadence in
+// force: the batch's own (the autotuner's choice) when set, else the params'.
 void maybe_rebuild(mb2_batch* b, const float4* pos, const int* type_ids, uint64_t step,
 				   const mb2_step_params* prm, cudaStream_t st) {
-	const bool at_period = prm->rebuild_period == 0 || (step - 1) % prm->rebuild_period == 0;
+	const uint32_t period = b->rebuild_period ? b->rebuild_period : prm->rebuild_period;
+	const bool at_period = period == 0 || (step - 1) % period == 0;
 	bool rebuild = at_period || !b->built;
 	const float skin = prm->pairlist_cutoff - prm->cutoff;
-	if (rebuild && b->built && prm->rebuild_period != 0 && skin > 0.0f)
+	if (rebuild && b->built && period != 0 && skin > 0.0f)
 		rebuild = batch_max_disp(b, pos, st) > skin * 0.5f;
-	if (rebuild) batch_build(b, pos, type_ids, prm->pairlist_cutoff, st);
+	if (rebuild) {
+		batch_build(b, pos, type_ids, prm->pairlist_cutoff, st);
+		++b->rebuilds;
+	}
 	b->force_sorted.ensure(b->n);
 }
 
@@ -735,6 +746,17 @@ int mb2_batch_run(mb2_batch* b, float* pos4, float* force_energy4, const int* ty
 	});
 }
 
+int mb2_batch_set_rebuild_period(mb2_batch* b, uint32_t period) {
+	return bguard(b, [&] { b->rebuild_period = period; });
+}
+
+int mb2_batch_rebuild_schedule(const mb2_batch* b, uint32_t* period, uint64_t* rebuilds) {
+	if (!b) return MB2_ERR_ARG;
+	if (period) *period = b->rebuild_period;
+	if (rebuilds) *rebuilds = b->rebuilds;
+	return MB2_OK;
+}
+
 int mb2_batch_set_tuning(mb2_batch* b, int level_offset, int lanes) {
 	return bguard(b, [&] {
 		expect_arg(level_offset >= -3 && level_offset <= 3, MB2_ERR_ARG,
@@ -802,26 +824,38 @@ int mb2_batch_autotune(mb2_batch* b, const float* pos4, const int* type_ids,
 					best_step = ts;
 				}
 			}
-		// Apply the best knobs, then measure how far particles move per step from
-		// a fresh list: the largest cadence whose displacement stays within half
-		// the skin keeps every interacting pair in the list.
+		// Apply the best knobs. Then the cadence: on the copy, an equilibration
+		// segment of one period (rebuilt at its start), so that the overlaps of
+		// a fresh start have relaxed; then two intervals of one period, each
+		// from a fresh list, recording the largest displacement after every
+		// step. The cadence is the largest k <= period whose displacement stayed
+		// within half the skin in both: rebuilt every k steps, the list keeps
+		// every pair that comes within the cutoff.
 		reset_tuning(b, best_level, best_lanes);
 		MB2_CUDA(cudaMemcpyAsync(tpos.ptr, pos4, static_cast<size_t>(n) * 16,
 								 cudaMemcpyDeviceToDevice, st));
-		batch_build(b, tpos.ptr, type_ids, prm->pairlist_cutoff, st);
 		b->force_sorted.ensure(n);
 		step_counter_set(b->step_d.ptr, 1, st);
+		batch_build(b, tpos.ptr, type_ids, prm->pairlist_cutoff, st);
+		for (uint32_t k = 0; k < period; ++k) step_body(b, tpos.ptr, tfe.ptr, type_ids, prm, st);
 		const float skin = prm->pairlist_cutoff - prm->cutoff;
-		uint32_t cadence = 1;
-		bool exceeded = false;
+		uint32_t cadence = period;
 		float disp_at_period = 0.0f;
-		for (uint32_t k = 1; k <= period; ++k) {
-			step_body(b, tpos.ptr, tfe.ptr, type_ids, prm, st);
-			const float d = batch_max_disp(b, tpos.ptr, st);
-			exceeded |= d > 0.5f * skin;
-			if (!exceeded) cadence = k;
-			disp_at_period = d;
+		for (int rep = 0; rep < 2; ++rep) {
+			batch_build(b, tpos.ptr, type_ids, prm->pairlist_cutoff, st);
+			bool exceeded = false;
+			for (uint32_t k = 1; k <= period; ++k) {
+				step_body(b, tpos.ptr, tfe.ptr, type_ids, prm, st);
+				const float d = batch_max_disp(b, tpos.ptr, st);
+				if (d > 0.5f * skin && !exceeded) {
+					exceeded = true;
+					cadence = std::min(cadence, std::max<uint32_t>(k - 1, 1u));
+				}
+				if (k == period) disp_at_period = std::max(disp_at_period, d);
+			}
 		}
+		if (skin <= 0.0f) cadence = 1;
+		b->rebuild_period = cadence;  // in force from the next step
 		b->built = false;  // that list was built from the trial positions
 		MB2_CUDA(cudaStreamSynchronize(st));
 		cudaEventDestroy(e0);

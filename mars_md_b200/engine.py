@@ -777,10 +777,22 @@ class Batch:
         return lvl.value, lanes.value, cells.value
 
     def autotune(self, pos, type_ids, params: "L.StepParams", trial_steps=4, stream=None) -> dict:
+        """Cell level, lanes per row and rebuild cadence chosen on a copy of the
+        positions and put in force (see mb2_batch_autotune)."""
         r = L.BatchTuning()
         self.check(self.lib.mb2_batch_autotune(self.h, _p(pos), _p(type_ids), C.byref(params),
                                                int(trial_steps), _stream(stream), C.byref(r)))
         return {k: getattr(r, k) for k, _ in L.BatchTuning._fields_}
+
+    def set_rebuild_period(self, period: int):
+        """Rebuild cadence for step/run (0: the params' rebuild_period)."""
+        self.check(self.lib.mb2_batch_set_rebuild_period(self.h, int(period)))
+
+    def rebuild_schedule(self):
+        """(cadence in force, 0 = the params'; list builds so far)."""
+        p, r = C.c_uint32(), C.c_uint64()
+        self.check(self.lib.mb2_batch_rebuild_schedule(self.h, C.byref(p), C.byref(r)))
+        return int(p.value), int(r.value)
 
 
 def setup_batch(ws, device="cuda:0"):

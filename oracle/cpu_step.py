@@ -16,15 +16,18 @@ integrate.
 
 Threads: race-free functors (encode, tag resolve, BD integrate) are chunked
 over `nthreads` host threads, following the reference's launch_cpu_kernel
-(src/Backend/Kernels.h:204-238); the scatter functors (neighbour emit, pair
-forces) and the sort run on one thread, because the reference's host atomics
-are plain `+=`.
+(src/Backend/Kernels.h:204-238). The scatter functors (neighbour emit, pair
+forces) cannot share outputs between threads, because the reference's host
+atomics are plain `+=`: with the reference's functors each thread runs them
+over its own range into its own outputs, joined in order (the harness's
+``_mt`` calls); the port runs them on one thread. The sort runs on one thread.
 
 ``SampledStep`` bounds the work on a large system: the whole sort and the
 whole BD integrate run on all N particles, while the neighbour walk runs for
 a strided sample of particles and the pair forces for the pairs that sample
 emits. Their times are scaled by N / sample and P / sample, and the rebuild
-is amortised over `rebuild_period` steps.
+is amortised over `rebuild_period` steps. With ``walk_sample=None`` every
+particle is walked and every pair computed: nothing is scaled.
 """
 from __future__ import annotations
 
@@ -50,7 +53,7 @@ class SampledStep:
         self.types = po.TypeSet(w.charge, w.diffusion, w.pmf_terms)
         self.pos = w.pos.copy()
         self.flags = np.zeros(w.n, np.uint32)
-        self.walk_sample = min(walk_sample, w.n)
+        self.walk_sample = w.n if walk_sample is None else min(walk_sample, w.n)
         self.pairs = None
         self.total_pairs_est = 0.0
         self.last = {}
@@ -93,8 +96,16 @@ class SampledStep:
         t0 = time.perf_counter()
         rc2 = np.float32(w.list_radius) ** 2
         if R is not None:
-            pairs, cnt = R.neighbor_walk_items(spos, keys, s2o, begin, end, table, rc2, slots,
-                                               shift, self.box, items, max_pairs=self.walk_sample * 600)
+            # Room for 1.5x the half pairs a uniform density would give each item.
+            vol = float(np.prod(bmax - bmin))
+            per_item = w.n / max(vol, 1e-30) * (4.0 / 3.0) * np.pi * w.list_radius ** 3 / 2.0
+            max_pairs = int(self.walk_sample * (1.5 * per_item + 8)) + 4096
+            pairs, cnt = R.neighbor_walk_items_mt(spos, keys, s2o, begin, end, table, rc2, slots,
+                                                  shift, self.box, items, max_pairs, self.nthreads)
+            if pairs is None:
+                pairs, cnt = R.neighbor_walk_items_mt(spos, keys, s2o, begin, end, table, rc2,
+                                                      slots, shift, self.box, items, cnt,
+                                                      self.nthreads)
         else:
             # the port walks the same items through the full-list restatement
             pairs, cnt, _ = O.build_pairlist(self.pos, self.box, w.list_radius)
@@ -123,8 +134,8 @@ class SampledStep:
         seed = self.O.bd_seed(w.seed, 0, s)
         t0 = time.perf_counter()
         if self.R is not None:
-            fe = self.R.pair_forces(self.pairs, self.pos, w.type_ids, self.tags, self.tables,
-                                    self.box, rc2, get_energy=False)
+            fe = self.R.pair_forces_mt(self.pairs, self.pos, w.type_ids, self.tags, self.tables,
+                                       self.box, rc2, self.nthreads, get_energy=False)
         else:
             fe, _, _ = self.O.pair_forces(self.pairs, self.pos, self.tags, self.tables, self.box,
                                           rc2, get_energy=False)

@@ -565,6 +565,11 @@ class RefHarness:
                                               vp, sz, vp, sz]
         L.ref_resolve_tags.argtypes = [vp, sz, vp, vp, sz, vp, i]
         L.ref_read_table.argtypes = [C.c_char_p, i, vp, vp, sz, vp, vp, vp, vp]
+        L.ref_neighbor_walk_items_mt.restype = u64
+        L.ref_neighbor_walk_items_mt.argtypes = [vp, vp, vp, vp, vp, vp, f, sz, i, i, vp, vp, vp,
+                                                 vp, sz, vp, sz, i]
+        L.ref_pair_forces_mt.argtypes = [vp, sz, sz, vp, vp, vp, vp, vp, vp, vp, vp, vp, i, vp, vp,
+                                         vp, i, f, u32, i]
         L.ref_pair_forces.argtypes = [vp, sz, vp, vp, vp, vp, vp, vp, vp, vp, vp, i, vp, vp, vp,
                                       i, f, u32]
         L.ref_bond_forces.argtypes = [vp, vp, vp, sz, vp, vp, vp, vp, vp, vp, vp, i, vp, vp, vp, i]
@@ -664,6 +669,19 @@ class RefHarness:
         pairs = None if buf is None else np.ascontiguousarray(buf[1: min(cnt, max_pairs) + 1])
         return pairs, cnt
 
+    def neighbor_walk_items_mt(self, sorted_pos, keys, s2o, begin, end, table, cutoff_sq, npc,
+                               shift, box: Box, items, max_pairs, nthreads):
+        """neighbor_walk_items on host threads (per-thread outputs joined in
+        order). Returns (pairs or None when they exceed max_pairs, count)."""
+        o, s, p = self._box(box)
+        items = np.ascontiguousarray(items, np.uint32)
+        buf = np.zeros((max_pairs + 1, 2), np.int32)
+        cnt = int(self.lib.ref_neighbor_walk_items_mt(
+            _ptr(sorted_pos), _ptr(keys), _ptr(s2o), _ptr(begin), _ptr(end), _ptr(table),
+            C.c_float(cutoff_sq), len(keys), npc, shift, _ptr(o), _ptr(s), _ptr(p), _ptr(items),
+            len(items), _ptr(buf), max_pairs, int(nthreads)))
+        return (np.ascontiguousarray(buf[1:cnt + 1]) if cnt <= max_pairs else None), cnt
+
     def read_table(self, path, kind):
         """Table::read_file of one text table; kind 0 pair, 1 bond, 2 angle,
         3 dihedral. Returns (X, Y, start, step, uniform) as float32."""
@@ -693,6 +711,19 @@ class RefHarness:
                                  _ptr(tables.sizes), _ptr(tables.starts), _ptr(tables.step_invs),
                                  len(tables), _ptr(o), _ptr(s), _ptr(p), int(get_energy),
                                  C.c_float(cutoff_sq), enabled_terms)
+        return fe
+
+    def pair_forces_mt(self, pairs, pos4, type_ids, tags, tables: TableSet, box: Box, cutoff_sq,
+                       nthreads, get_energy=True, enabled_terms=0xFF):
+        """pair_forces on host threads (per-thread ForceEnergy arrays added in order)."""
+        fe = np.zeros((len(pos4), 4), np.float32)
+        o, s, p = self._box(box)
+        self.lib.ref_pair_forces_mt(_ptr(pairs), len(pairs), len(pos4), _ptr(pos4), _ptr(type_ids),
+                                    _ptr(fe), _ptr(tags), _ptr(tables.values),
+                                    _ptr(tables.offsets), _ptr(tables.sizes),
+                                    _ptr(tables.starts), _ptr(tables.step_invs), len(tables),
+                                    _ptr(o), _ptr(s), _ptr(p), int(get_energy),
+                                    C.c_float(cutoff_sq), enabled_terms, int(nthreads))
         return fe
 
     def pair_forces_terms(self, pairs, pos4, type_ids, tags, tables: TableSet,

@@ -26,6 +26,7 @@
 
 #include <algorithm>
 #include <cstdint>
+#include <cstring>
 #include <numeric>
 #include <thread>
 #include <vector>
@@ -245,6 +246,75 @@ uint64_t ref_neighbor_walk_items(const float* sorted_pos4, const uint32_t* keys,
 	return count;
 }
 
+// The same walk on `nthreads` host threads. The reference's host atomics are
+// plain `+=`, so its functor is not run on shared outputs from several
+// threads: each thread walks a contiguous range of the items into its own
+// counter and buffer (the functor unchanged), and the buffers are joined in
+// thread order, so the emitted order is the serial walk's. A buffer that turns
+// out too small is regrown and its range walked again. Writes slots
+// [1, count] of `pairs` (slot 0 unused, as the serial emit does) when the
+// total fits in max_pairs.
+uint64_t ref_neighbor_walk_items_mt(const float* sorted_pos4, const uint32_t* keys,
+									const uint32_t* s2o, const uint32_t* cell_begin,
+									const uint32_t* cell_end, const uint32_t* table,
+									float cutoff_sq, size_t n, int npc, int shift,
+									const float* origin, const float* size, const int* periodic,
+									const uint32_t* items, size_t n_items, int* pairs,
+									size_t max_pairs, int nthreads) {
+	if (nthreads < 1) nthreads = 1;
+	const PeriodicBox box = make_box(origin, size, periodic);
+	const size_t chunk = (n_items + nthreads - 1) / nthreads;
+	std::vector<std::vector<int2>> bufs(nthreads);
+	std::vector<uint64_t> counts(nthreads, 0);
+	auto walk = [&](int t) {
+		const size_t lo = std::min(n_items, t * chunk), hi = std::min(n_items, lo + chunk);
+		size_t cap = (max_pairs + 1) / std::max<size_t>(n_items, 1) * (hi - lo) + (hi - lo) / 4 + 1024;
+		for (;;) {
+			bufs[t].assign(cap + 1, int2{});
+			uint32_t count = 0;
+			ExclusionView ex;
+			ZOrderCellNeighborKernel k{reinterpret_cast<const Vector3*>(sorted_pos4),
+									   keys,
+									   s2o,
+									   cell_begin,
+									   cell_end,
+									   table,
+									   bufs[t].data(),
+									   &count,
+									   cutoff_sq,
+									   n,
+									   cap + 1,
+									   npc,
+									   1,
+									   shift,
+									   box,
+									   ex};
+			for (size_t i = lo; i < hi; ++i)
+				k(items[i]);
+			counts[t] = count;
+			if (count <= cap) return;
+			cap = static_cast<size_t>(count) + count / 8 + 1024;
+		}
+	};
+	std::vector<std::thread> pool;
+	for (int t = 1; t < nthreads; ++t)
+		pool.emplace_back(walk, t);
+	walk(0);
+	for (auto& th : pool)
+		th.join();
+	uint64_t total = 0;
+	for (int t = 0; t < nthreads; ++t)
+		total += counts[t];
+	if (pairs && total <= max_pairs) {
+		int2* out = reinterpret_cast<int2*>(pairs) + 1;
+		for (int t = 0; t < nthreads; ++t) {
+			std::memcpy(out, bufs[t].data() + 1, counts[t] * sizeof(int2));
+			out += counts[t];
+		}
+	}
+	return total;
+}
+
 // ResolvePairTableKernel (Pairwise.h:104-120).
 void ref_resolve_tags(const int* pairs, size_t n_pairs, const int* type_ids,
 					  const uint32_t* term_matrix, size_t num_types, uint32_t* tags, int nthreads) {
@@ -274,6 +344,50 @@ void ref_pair_forces(const int* pairs, size_t n_pairs, const float* pos4, int* t
 							get_energy != 0, n_pairs, cutoff_sq, enabled_terms);
 	for (size_t i = 0; i < n_pairs; ++i)
 		k(i);
+}
+
+// The same pair forces on `nthreads` host threads: each thread runs the
+// functor (unchanged) over a contiguous range of the pairs into its own
+// ForceEnergy array, and the arrays are added into fe4 in thread order.
+void ref_pair_forces_mt(const int* pairs, size_t n_pairs, size_t n_particles, const float* pos4,
+						int* type_ids, float* fe4, const uint32_t* tags, float* table_values,
+						const uint32_t* table_offsets, const uint32_t* table_sizes,
+						const float* table_starts, const float* table_step_invs, int n_tables,
+						const float* origin, const float* size, const int* periodic,
+						int get_energy, float cutoff_sq, uint32_t enabled_terms, int nthreads) {
+	if (nthreads < 1) nthreads = 1;
+	std::vector<int> periodic_flags(n_tables, 0);
+	auto tabs = make_tables(table_values, table_offsets, table_sizes, table_starts,
+							table_step_invs, periodic_flags.data(), n_tables);
+	const PeriodicBox box = make_box(origin, size, periodic);
+	const size_t chunk = (n_pairs + nthreads - 1) / nthreads;
+	std::vector<std::vector<Vector3>> part(nthreads);
+	auto run = [&](int t) {
+		const size_t lo = std::min(n_pairs, t * chunk), hi = std::min(n_pairs, lo + chunk);
+		part[t].assign(n_particles, Vector3());
+		ParticleView pv{};
+		pv.type_id = type_ids;
+		pv.pos = reinterpret_cast<Vector3*>(const_cast<float*>(pos4));
+		pv.ForceEnergy = part[t].data();
+		ParticleTypeView tv{};
+		PairNonbondedComputer k(reinterpret_cast<const int2*>(pairs), pv, tags, tabs.data(), tv,
+								&box, get_energy != 0, n_pairs, cutoff_sq, enabled_terms);
+		for (size_t i = lo; i < hi; ++i)
+			k(i);
+	};
+	std::vector<std::thread> pool;
+	for (int t = 1; t < nthreads; ++t)
+		pool.emplace_back(run, t);
+	run(0);
+	for (auto& th : pool)
+		th.join();
+	for (int t = 0; t < nthreads; ++t)
+		for (size_t i = 0; i < n_particles; ++i) {
+			fe4[4 * i + 0] += part[t][i].x;
+			fe4[4 * i + 1] += part[t][i].y;
+			fe4[4 * i + 2] += part[t][i].z;
+			fe4[4 * i + 3] += part[t][i].t;
+		}
 }
 
 // PairNonbondedComputer (Pairwise.h:214-304) with every analytical term:

@@ -150,6 +150,41 @@ def test_batch_autotune_reports_and_keeps_results(oracle):
         b.close()
 
 
+def test_batch_autotuned_cadence_in_force_and_list_stays_exact(oracle):
+    """The tuner's cadence is the one the run uses (its rebuilds follow it),
+    and a list built past the transient still holds every pair within the
+    interaction cutoff after that many steps (checked per system against the
+    oracle's pair set at the cutoff on the current positions)."""
+    ws = _systems(k=6)
+    b, dev = setup_batch(ws)
+    try:
+        prm = step_params(ws[0], seed=SEED)
+        r = b.autotune(dev["pos"], dev["type"], prm, trial_steps=2)
+        c = r["safe_rebuild_period"]
+        assert b.rebuild_schedule()[0] == c
+        # Past the transient of the fresh start: the first step builds, then one
+        # scheduled check every c steps (a rebuild unless the skin still holds).
+        steps = 2 * prm.rebuild_period
+        b.run(dev["pos"], dev["fe"], dev["type"], 1, steps, prm)
+        torch.cuda.synchronize()
+        _, rebuilds = b.rebuild_schedule()
+        assert 1 <= rebuilds <= (steps - 1) // c + 1
+        # A fresh list, then c steps.
+        b.build(dev["pos"], dev["type"], ws[0].list_radius)
+        b.run(dev["pos"], dev["fe"], dev["type"], steps + 1, c, prm)
+        torch.cuda.synchronize()
+        listed = _split_pairs(b.export_pairs().cpu().numpy().astype(np.int64), b.offsets)
+        pos = dev["pos"].cpu().numpy()
+        for s, w in enumerate(ws):
+            p = pos[b.offsets[s]:b.offsets[s + 1]]
+            near, _, _ = oracle.build_pairlist(p, box_of(w), w.cutoff)
+            have = {tuple(x) for x in _canon(listed[s]).tolist()}
+            missing = [tuple(x) for x in near.tolist() if tuple(x) not in have]
+            assert not missing, f"system {s}: {len(missing)} pairs within the cutoff not listed"
+    finally:
+        b.close()
+
+
 def test_batch_rejects_boxes_smaller_than_twice_the_list_radius():
     w = W.plain_bd(seed=1, n=600, box=40.0)
     b, dev = setup_batch([w])
