@@ -191,12 +191,6 @@ struct TableRow {
 	}
 };
 
-// Flips the sign bits of both halves when flip is the sign bit.
-__device__ __forceinline__ float2 xor_sign2(float2 v, uint32_t flip) {
-	return make_float2(__uint_as_float(__float_as_uint(v.x) ^ flip),
-					   __uint_as_float(__float_as_uint(v.y) ^ flip));
-}
-
 // One pair of the half list, rounded as the reference rounds it. flip
 // (bit 31 of the entry): the reference orients the pair j -> i. With kTerms,
 // the analytical terms of the type pair come first, then the table.
@@ -216,9 +210,11 @@ __device__ __forceinline__ void pair_scalar(const float4& pi, float2 npi, const 
 											float cutoff_sq, float skip2, float4* force, float2& nxy, float& nz,
 											float& fe, double& e_acc, double& w_acc) {
 	// r = wrap_diff(pos[second] - pos[first])
-	// (pi - pj is exactly -(pj - pi) in round-to-nearest, so a sign flip suffices)
-	float2 dxy = xor_sign2(__fadd2_rn(make_float2(pj.x, pj.y), npi), flip);
-	float dz = __uint_as_float(__float_as_uint(__fsub_rn(pj.z, pi.z)) ^ flip);
+	// (pi - pj is exactly -(pj - pi) in round-to-nearest, so a sign flip
+	// suffices; a multiply by -1 is that flip, on the FMA pipe)
+	const float sgn = __uint_as_float(flip | 0x3F800000u);  // +1, or -1 when flipped
+	float2 dxy = __fmul2_rn(__fadd2_rn(make_float2(pj.x, pj.y), npi), make_float2(sgn, sgn));
+	float dz = __fmul_rn(__fsub_rn(pj.z, pi.z), sgn);
 	if (kAllPeriodic) {
 		// wrap1 on x and y: image = floor(d / l); d -= image * l; d >= l/2 -> d - l.
 		const float2 negl = make_float2(-box.size[0], -box.size[1]);
@@ -263,12 +259,12 @@ __device__ __forceinline__ void pair_scalar(const float4& pi, float2 npi, const 
 	} else {
 		if (t.offset < 0) return;
 		const float w = __fmul_rn(__fsub_rn(dist, t.start), t.step_inv);
-		const float wf = floorf(w);
-		const int home = min(max(static_cast<int>(wf), 0), t.last);
+		// floor to int in one conversion (equal to int(floorf(w)) for every w)
+		const int home = min(max(__float2int_rd(w), 0), t.last);
 		fm = bin_f[t.offset + home];
 		if (kEnergy) {
 			const float2 ue = bin_e[t.offset + home];
-			e = __fadd_rn(__fmul_rn(ue.y, __fsub_rn(w, wf)), ue.x);
+			e = __fadd_rn(__fmul_rn(ue.y, __fsub_rn(w, floorf(w))), ue.x);
 		}
 	}
 	const float inv = __frcp_rn(dist);
@@ -284,8 +280,8 @@ __device__ __forceinline__ void pair_scalar(const float4& pi, float2 npi, const 
 				 static_cast<double>(gz) * dz;
 	}
 	// j is the pair's second particle unless the pair is stored flipped.
-	const float2 hxy = xor_sign2(gxy, flip);
-	const float hz = __uint_as_float(__float_as_uint(gz) ^ flip);
+	const float2 hxy = __fmul2_rn(gxy, make_float2(sgn, sgn));
+	const float hz = __fmul_rn(gz, sgn);
 	red_add_v4(&force[j], hxy.x, hxy.y, hz, half);
 	nxy = __fadd2_rn(nxy, hxy);
 	nz = __fadd_rn(nz, hz);
