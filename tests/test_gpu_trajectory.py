@@ -59,3 +59,86 @@ def test_thousand_step_trajectory_matches_oracle(ctx_factory, oracle):
                 assert (d <= TOL).mean() >= 0.99, (s, int((d > TOL).sum()))
                 assert d.max() <= 0.5, (s, float(d.max()))  # diverged paths stay bounded
     assert worst_strict <= TOL, worst_strict
+
+
+def _f32_bins(pos_a, pos_b, pairs, L, start, step_inv):
+    """Table bins of each pair's distance, computed as the reference does in
+    float (wrap_diff with floor(x * (1/L)), left-to-right length2, sqrt,
+    w = (d - start) * step_inv), for two position sets."""
+    f = np.float32
+    out = []
+    inv = f(1.0) / f(L)
+    for pos in (pos_a, pos_b):
+        i, j = pairs[:, 0], pairs[:, 1]
+        x = (pos[j, :3] - pos[i, :3]).astype(np.float32)
+        img = np.floor(x * inv).astype(np.float32)
+        x = (x - img * f(L)).astype(np.float32)
+        x = np.where(x >= f(0.5) * f(L), (x - f(L)).astype(np.float32), x)
+        d2 = ((x[:, 0] * x[:, 0] + x[:, 1] * x[:, 1]) + x[:, 2] * x[:, 2]).astype(np.float32)
+        d = np.sqrt(d2).astype(np.float32)
+        w = ((d - f(start)) * f(step_inv)).astype(np.float32)
+        out.append((np.floor(w).astype(np.int64), d))
+    return out
+
+
+def test_trajectory_divergences_are_table_bin_flips(ctx_factory, oracle):
+    """Every particle whose device path leaves the oracle's by more than 1e-4 A
+    does so because, at this or an earlier step, it or a particle it
+    interacts with was in a pair that took different table bins on the two
+    sides while both ends still agreed to 1e-4 A (its distance within rounding
+    of a bin edge), or because a partner had already diverged. Every step's
+    pairs within the cutoff are checked for such flips; each is reported with
+    its step, pair, the two bins and the distance gap."""
+    w = W.plain_bd()
+    ctx = ctx_factory(w.n)
+    dev = setup_workload(ctx, w)
+    prm = step_params(w)
+    box = pyoracle.Box.make(w.box_origin, w.box_size, w.periodic)
+    types = pyoracle.TypeSet(w.charge, w.diffusion)
+    ts = pyoracle.TableSet([(t.values, t.start, t.step_inv) for t in w.pair_tables])
+    t0 = w.pair_tables[0]
+    pos = w.pos.copy()
+    rc2 = np.float32(w.cutoff) ** 2
+    skin = w.list_radius - w.cutoff
+    blen = np.array(w.box_size, np.float32)
+    L = float(w.box_size[0])
+    pairs = snap = None
+    diverged = np.zeros(w.n, bool)
+    touched = np.zeros(w.n, bool)
+    flips, unexplained = [], []
+    prev_gpu, prev_ref = w.pos.copy(), w.pos.copy()
+    for s in range(1, 1001):
+        ctx.step(dev["pos"], dev["fe"], dev["type"], None, s, prm)
+        if pairs is None or ((s - 1) % w.rebuild_period == 0 and
+                             oracle.max_displacement(pos, snap, blen) > skin * 0.5):
+            pairs, _, _ = oracle.build_pairlist(pos, box, w.list_radius)
+            snap = pos.copy()
+        tags = oracle.resolve_tags(pairs, w.type_ids, w.term_matrix, 1)
+        f32, _, _ = oracle.pair_forces(pairs, pos, tags, ts, box, rc2)
+        pos, _, _ = oracle.bd_integrate(pos, f32, w.type_ids, None, types, None, box, w.dt,
+                                        w.kT, s, oracle.bd_seed(w.seed, 0, s))
+        # Bins of this step's pairs from the positions the step started from.
+        (bg, dg), (br, dr) = _f32_bins(prev_gpu, prev_ref, pairs, L, t0.start, t0.step_inv)
+        near = (dg * dg <= rc2) | (dr * dr <= rc2)
+        fresh = ~diverged[pairs[:, 0]] & ~diverged[pairs[:, 1]]
+        flip = near & fresh & (bg != br)
+        for (a, b), x, y, u, v in zip(pairs[flip], bg[flip], br[flip], dg[flip], dr[flip]):
+            flips.append((s, int(a), int(b), int(x), int(y), float(abs(float(u) - float(v)))))
+        touched[pairs[flip].ravel()] = True
+        gpu = dev["pos"].cpu().numpy()
+        d = np.abs(gpu[:, :3] - pos[:, :3])
+        d = np.minimum(d, L - d).max(axis=1)
+        new = np.flatnonzero((d > TOL) & ~diverged)
+        for p in new:
+            mine = ((pairs[:, 0] == p) | (pairs[:, 1] == p)) & near
+            partners = np.where(pairs[mine, 0] == p, pairs[mine, 1], pairs[mine, 0])
+            if not (touched[p] or touched[partners].any() or diverged[partners].any()):
+                unexplained.append((s, int(p), float(d[p])))
+        diverged[new] = True
+        prev_gpu, prev_ref = gpu, pos.copy()
+    gaps = np.array([f[5] for f in flips]) if flips else np.zeros(0)
+    print(f"{int(diverged.sum())} of {w.n} particles past {TOL} A by step 1000; "
+          f"{len(flips)} table-bin flips between agreeing particles, distance gap median "
+          f"{np.median(gaps) if len(gaps) else 0:.2e} A, max {gaps.max() if len(gaps) else 0:.2e} A; "
+          f"first (step, i, j, bin device, bin oracle, gap A): {flips[:4]}")
+    assert not unexplained, unexplained[:10]
