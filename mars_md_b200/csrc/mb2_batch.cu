@@ -487,12 +487,10 @@ void check_step_args(mb2_batch* b, const float* pos4, const float* fe4, const in
 			   MB2_ERR_ARG, "mb2_batch_step: BD without bonded terms in batched mode");
 }
 
-// Rebuild decision of the reference (Patch.cpp:86-108), over all systems: at
-// the first step and at each rebuild period, rebuild when any system moved
-// more than half the skin since the last build.
-// The rebuild schedule of Patch.cpp:86-108 (a rebuild at every period step,
-// skipped while no particle moved more than half the skin) at the cadence in
-// force: the batch's own (the autotuner's choice) when set, else the params'.
+// The rebuild schedule of Patch.cpp:86-108 over all systems (a rebuild at the
+// first step and at every period step, skipped while no particle of any
+// system moved more than half the skin) at the cadence in force: the batch's
+// own (the autotuner's choice) when set, else the params'.
 void maybe_rebuild(mb2_batch* b, const float4* pos, const int* type_ids, uint64_t step,
 				   const mb2_step_params* prm, cudaStream_t st) {
 	const uint32_t period = b->rebuild_period ? b->rebuild_period : prm->rebuild_period;
