@@ -647,8 +647,9 @@ def cpu_baseline_adjoint(local, steps=200, every=20):
     """The adjoint workload on the host: the FP64 restatement of the window and
     its adjoint (oracle/mb2_adjoint.c, threaded pair loops) timed over the
     200-step window, particle-steps/s of the reverse sweep. Beside it, as the
-    checker: the device's gradients of a window with a checkpoint at every step
-    against the FP64 adjoint along the device's own states (max-normalised
+    checker: the device's gradients of the benchmark's window (checkpoints
+    every 20 steps) against the FP64 adjoint along the states the device's
+    reverse sweep differentiated (recorded as it recomputed them; max-normalised
     relative errors)."""
     import torch
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
@@ -660,7 +661,9 @@ def cpu_baseline_adjoint(local, steps=200, every=20):
     rng = np.random.default_rng(W.DEFAULT_SEED)
     w.pos[:, :3] = np.mod(w.pos[:, :3] + rng.normal(scale=0.02, size=(w.n, 3)),
                           w.box_size[0]).astype(np.float32)
-    win = Window(w, steps, checkpoint_every=1, device=device)
+    win = Window(w, steps, checkpoint_every=every, device=device)
+    recorded = torch.empty((steps, w.n, 4), dtype=torch.float32, device=device)
+    win.record_states(recorded)
     pos0 = win.dev["pos"].clone()
     pv, bv = win.pair_values().float(), win.bond_values().float()
     win.set_tables(torch.from_numpy(W.wca_table(sigma=4.2).values).to(device), bv)
@@ -670,7 +673,7 @@ def cpu_baseline_adjoint(local, steps=200, every=20):
     hist = win.histogram(xn)
     dldh = 2.0 * (hist * win.norm - target) * win.norm
     g0, gp, gb = win.backward(win.histogram_backward(xn, dldh))
-    states = np.concatenate([win.checkpoints()[:, :, :3].double().cpu().numpy(),
+    states = np.concatenate([recorded[:, :, :3].double().cpu().numpy(),
                              xn[None, :, :3].double().cpu().numpy()])
     noise = []
     for k in range(1, steps + 1):
@@ -689,7 +692,8 @@ def cpu_baseline_adjoint(local, steps=200, every=20):
                             (t.values, t.start, t.step_inv), w.cutoff, w.bonds,
                             (bt.values, bt.start, bt.step_inv), w.angles,
                             (at.values, at.start, at.step_inv), w.exclusions,
-                            float_bins=float_bins)
+                            float_bins=float_bins, list_every=every if float_bins else 0,
+                            list_radius=w.list_radius)
 
     def grads(A, tr):
         h = A.rdf(tr[-1], r.bins, r.bin_width, r.r_max, r.sigma)
@@ -716,9 +720,10 @@ def cpu_baseline_adjoint(local, steps=200, every=20):
                 "pair_table": rel(gp.double().cpu().numpy(), cp),
                 "bond_table": rel(gb.double().cpu().numpy(), cb),
                 "positions": rel(g0[:, :3].double().cpu().numpy(), c0),
-                "how": "device window with a checkpoint at every step against the FP64 "
-                       "adjoint along the device's states (table bins as the float forward "
-                       "decided them), max-normalised"}}
+                "how": f"device window with checkpoints every {every} steps against the "
+                       "FP64 adjoint along the states its reverse sweep differentiated "
+                       "(table bins as the float forward decided them, pairs from a list "
+                       "built at each checkpoint), max-normalised"}}
 
 
 def cpu_baseline(w):

@@ -473,6 +473,13 @@ MB2_API int mb2_window_forward(mb2_context* ctx, float* pos4, float* force_energ
  * reference (it has no adjoint). */
 MB2_API int mb2_window_checkpoints(mb2_context* ctx, float* out4, uint64_t capacity_rows,
                            void* stream);
+/* Record the states each following mb2_window_backward differentiates: x_0 ..
+ * x_{N-1} of the window (N = num_steps), n float4 rows each in step order,
+ * written into out4 (device, at least N x n rows, checked at the backward
+ * call) as the reverse sweep recomputes each segment from its checkpoint.
+ * NULL stops recording. For checking a reverse sweep against another adjoint
+ * along the very states it used. No counterpart in the reference. */
+MB2_API int mb2_window_record_states(mb2_context* ctx, float* out4, uint64_t capacity_rows);
 /* Reverse sweep of the last forward window: grad_final4 = dL/dx_N (float4
  * rows, .w ignored) -> grad_pos0_4 = dL/dx_0; grad_pair_bins (device double,
  * one per value of the concatenated pair tables) and grad_bond_bins (per

@@ -137,6 +137,7 @@ def load(path: str = LIB_PATH):
     L.mb2_window_forward.argtypes = [vp, vp, vp, vp, u32, u64, u32, u32, C.POINTER(StepParams), vp]
     L.mb2_window_backward.argtypes = [vp, vp, vp, vp, vp, vp]
     L.mb2_window_checkpoints.argtypes = [vp, vp, u64, vp]
+    L.mb2_window_record_states.argtypes = [vp, vp, u64]
     L.mb2_rdf_histogram.argtypes = [vp, vp, vp, u32, u32, f, f, f, vp, vp]
     L.mb2_rdf_backward.argtypes = [vp, vp, u32, u32, f, f, f, vp, vp, vp]
     L.mb2_batch_create.argtypes = [i, u32, u32p, fp, fp, C.POINTER(vp)]

@@ -111,6 +111,19 @@ class Window:
             self.ctx.h, _p(out), segs * self.w.n, _stream(stream)))
         return out
 
+    def record_states(self, out: torch.Tensor | None):
+        """Have each following backward write the states it differentiates
+        (x_0 .. x_{steps-1}) into `out` (float32 [steps, n, 4] on the device),
+        or stop with None."""
+        if out is None:
+            self.ctx.check(self.ctx.lib.mb2_window_record_states(self.ctx.h, None, 0))
+            return
+        if out.dtype != torch.float32 or tuple(out.shape) != (self.steps, self.w.n, 4):
+            raise ValueError(f"record_states: float32 [{self.steps}, {self.w.n}, 4] expected")
+        self._recorded = out
+        self.ctx.check(self.ctx.lib.mb2_window_record_states(self.ctx.h, _p(out),
+                                                             self.steps * self.w.n))
+
     def histogram(self, pos: torch.Tensor, stream=None) -> torch.Tensor:
         h = torch.zeros(self.rdf.bins, dtype=torch.float64, device=self.device)
         r = self.rdf

@@ -10,7 +10,8 @@
 //     u = (x_j - x_i) / r and F constant within a table bin:
 //     t = F / r (dv - u (u . dv)), dv = mu_j - mu_i, added to j, subtracted from i;
 //   * angle term: forward-mode (dual number) derivative of the reference's
-//     AngleGeometry force formula (exact except where the sine is floored).
+//     AngleGeometry force formula (exact except where the sine is floored),
+//     its sine taken from the cross product rather than sqrt(1 - cos^2).
 // Table gradients: dF/dU[h] = +step_inv, dF/dU[h+1] = -step_inv for the bin h
 // a pair falls in, so dL/dU[h] += step_inv (u . dv) and dL/dU[h+1] -= it;
 // accumulated in FP64 per block in shared memory, then one atomic per bin.
@@ -229,7 +230,14 @@ __global__ void __launch_bounds__(256) adj_angle_kernel(
 		ecs = 1.0f;
 		cs = dm(1.0f, 0.0f);
 	}
-	Dual sn = dsqrt(dm(1.0f, 0.0f) - cs * cs);
+	// sin(theta) = |ab x bc| / (|ab| |bc|), the same function as the forward's
+	// sqrt(1 - cos^2) but without its float cancellation: near 180 degrees
+	// (the harmonic angle tables' minimum) 1 - cos^2 carries a relative error
+	// of about eps / sin^2, the cross product about eps / sin, and dU/dtheta =
+	// -F / sin amplifies it into the tangent.
+	const Dual cx = ab[1] * bc[2] - ab[2] * bc[1], cy = ab[2] * bc[0] - ab[0] * bc[2],
+			   cz = ab[0] * bc[1] - ab[1] * bc[0];
+	Dual sn = dsqrt(cx * cx + cy * cy + cz * cz) / (lab * lbc);
 	if (__fsqrt_rn(__fsub_rn(1.0f, __fmul_rn(ecs, ecs))) <= 1e-3f) sn = dm(1e-3f, 0.0f);
 	const Table t = tables[table_idx[q]];
 	const float F = table_lookup(t.pot, static_cast<int>(t.size), t.start, t.step_inv, 1,

@@ -100,6 +100,8 @@ struct mb2_context {
 		const int* type_ids = nullptr;
 	} win;
 	DevBuf<float4> ckpt, states, wpos, wfe, lam, mu, mu_sorted, tan, tan_sorted;
+	float4* record_states = nullptr;  // caller's buffer for the states a reverse sweep differentiates
+	uint64_t record_cap = 0;          // its capacity in float4 rows
 	bool rdf_built = false;  // the current list was built by mb2_rdf_histogram
 	uint32_t rdf_n = 0;
 
@@ -1378,6 +1380,13 @@ int mb2_window_forward(mb2_context* ctx, float* pos4, float* force_energy4, cons
 	});
 }
 
+int mb2_window_record_states(mb2_context* ctx, float* out4, uint64_t capacity_rows) {
+	return guarded(ctx, [&] {
+		ctx->record_states = reinterpret_cast<float4*>(out4);
+		ctx->record_cap = out4 ? capacity_rows : 0;
+	});
+}
+
 int mb2_window_checkpoints(mb2_context* ctx, float* out4, uint64_t capacity_rows, void* stream) {
 	return guarded(ctx, [&] {
 		require(ctx->win.valid, MB2_ERR_STATE, "mb2_window_checkpoints: no forward window");
@@ -1403,6 +1412,10 @@ int mb2_window_backward(mb2_context* ctx, const float* grad_final4, float* grad_
 		const cudaStream_t st = S(stream);
 		const uint32_t n = w.n, C = w.every;
 		const uint32_t segs = (w.num_steps + C - 1) / C;
+		require(!ctx->record_states ||
+					ctx->record_cap >= static_cast<uint64_t>(w.num_steps) * n,
+				MB2_ERR_CAPACITY,
+				"mb2_window_backward: the recorded-states buffer holds fewer than steps x n rows");
 		ctx->states.ensure(static_cast<size_t>(C) * n);
 		for (auto* b : {&ctx->wpos, &ctx->wfe, &ctx->lam, &ctx->mu, &ctx->mu_sorted, &ctx->tan,
 						&ctx->tan_sorted})
@@ -1445,6 +1458,11 @@ int mb2_window_backward(mb2_context* ctx, const float* grad_final4, float* grad_
 					window_step(ctx, ctx->wpos.ptr, ctx->wfe.ptr, w.type_ids, n, w.first_step + k,
 								prm, st);
 			}
+			if (ctx->record_states)
+				MB2_CUDA(cudaMemcpyAsync(ctx->record_states + static_cast<size_t>(k0) * n,
+										 ctx->states.ptr,
+										 static_cast<size_t>(k1 - k0) * n * sizeof(float4),
+										 cudaMemcpyDeviceToDevice, st));
 			a.lanes = ctx->lanes;
 			a.cap = ctx->cap;
 			a.inv = ctx->inv.ptr;

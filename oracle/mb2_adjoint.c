@@ -58,6 +58,12 @@ typedef struct {
 	 * float forward decides them; everything else stays double. With float
 	 * states this gives the derivative of the map a float forward computes. */
 	int float_bins;
+	/* 0: every step's pairs are all pairs within the cutoff. k > 0: as the
+	 * window's pairlist, the candidate pairs of step j are those within
+	 * list_radius at step k * floor(j / k), the segment's start (the list the
+	 * device builds at each checkpoint), tested against the cutoff at step j. */
+	int list_every;
+	double list_radius;
 } adj_sys;
 
 /* Dual number: value and derivative along one direction. */
@@ -362,10 +368,73 @@ static void add_into(double* dst, const double* src, size_t len) {
 
 /* Total force (f) and, when mu is given, its tangent along mu (t) and the
  * table gradients (gpair, gbond: mu . dforce/dU, accumulated). */
+/* Pairs within list_radius of each other at x (the float test of the
+ * device's list build when float_bins, else double): a segment's pairlist. */
+static size_t list_pairs(const adj_sys* s, const double* x, int** out) {
+	int* cand = NULL;
+	const size_t nc = near_pairs(s, x, s->list_radius, &cand);
+	size_t k = 0;
+	const float rl = (float)s->list_radius;
+	for (size_t q = 0; q < nc; ++q) {
+		const int i = cand[2 * q], j = cand[2 * q + 1];
+		int keep;
+		if (s->float_bins) {
+			float r[3];
+			for (int a = 0; a < 3; ++a)
+				r[a] = wrapf((float)x[3 * j + a] - (float)x[3 * i + a], (float)s->L[a]);
+			keep = r[0] * r[0] + r[1] * r[1] + r[2] * r[2] <= rl * rl;
+		} else {
+			double d2 = 0.0;
+			for (int a = 0; a < 3; ++a) {
+				const double d = min_image(x[3 * j + a] - x[3 * i + a], s->L[a]);
+				d2 += d * d;
+			}
+			keep = d2 <= s->list_radius * s->list_radius;
+		}
+		if (keep) {
+			cand[2 * k] = i;
+			cand[2 * k + 1] = j;
+			++k;
+		}
+	}
+	*out = cand;
+	return k;
+}
+
+/* The candidate pairs of step k of a trajectory under s->list_every, kept in
+ * *cache (built for segment *cache_k0). */
+static const int* step_pairs(const adj_sys* s, const double* traj, int k, int* cache_k0,
+							 int** cache, size_t* np) {
+	const size_t m = 3 * (size_t)s->n;
+	const int k0 = (k / s->list_every) * s->list_every;
+	if (*cache == NULL || *cache_k0 != k0) {
+		free(*cache);
+		*np = list_pairs(s, traj + (size_t)k0 * m, cache);
+		*cache_k0 = k0;
+	}
+	return *cache;
+}
+
+static void forces_on(const adj_sys* s, const double* x, double* f, const double* mu, double* t,
+					  double* gpair, double* gbond, const int* list, size_t nlist);
+
 static void forces(const adj_sys* s, const double* x, double* f, const double* mu, double* t,
 				   double* gpair, double* gbond) {
+	forces_on(s, x, f, mu, t, gpair, gbond, NULL, 0);
+}
+
+/* forces() over the candidate pairs `list` (all pairs within the cutoff when
+ * NULL); each candidate is tested against the cutoff at x. */
+static void forces_on(const adj_sys* s, const double* x, double* f, const double* mu, double* t,
+					  double* gpair, double* gbond, const int* list, size_t nlist) {
 	int* pr = NULL;
-	const size_t np = near_pairs(s, x, s->cutoff, &pr);
+	size_t np;
+	if (list) {
+		np = nlist;
+	} else {
+		np = near_pairs(s, x, s->cutoff, &pr);
+		list = pr;
+	}
 	const size_t m = 3 * (size_t)s->n, gs = (size_t)s->pair.size;
 	int nthreads = 1;
 #ifdef _OPENMP
@@ -384,7 +453,7 @@ static void forces(const adj_sys* s, const double* x, double* f, const double* m
 		double* gl = gpair ? buf + 2 * m : NULL;
 #pragma omp for schedule(static)
 		for (size_t q = 0; q < np; ++q)
-			radial_term(s, &s->pair, s->cutoff, pr[2 * q], pr[2 * q + 1], x, fl, mu, tl, gl);
+			radial_term(s, &s->pair, s->cutoff, list[2 * q], list[2 * q + 1], x, fl, mu, tl, gl);
 		acc[tid] = buf;
 	}
 	for (int th = 0; th < nthreads; ++th) {
@@ -411,11 +480,20 @@ void adj_forward64(const adj_sys* s, const double* x0, const double* noise, int 
 				   double* traj) {
 	const size_t m = 3 * (size_t)s->n;
 	double* f = (double*)malloc(sizeof(double) * m);
+	int* cache = NULL;
+	int cache_k0 = -1;
+	size_t np = 0;
 	memcpy(traj, x0, sizeof(double) * m);
 	for (int k = 0; k < steps; ++k) {
 		const double* x = traj + (size_t)k * m;
 		double* y = traj + (size_t)(k + 1) * m;
-		adj_forces64(s, x, f);
+		memset(f, 0, sizeof(double) * m);
+		if (s->list_every > 0) {
+			const int* list = step_pairs(s, traj, k, &cache_k0, &cache, &np);
+			forces_on(s, x, f, NULL, NULL, NULL, NULL, list, np);
+		} else {
+			forces(s, x, f, NULL, NULL, NULL, NULL);
+		}
 		for (size_t q = 0; q < m; ++q) {
 			const int a = (int)(q % 3);
 			double v = x[q] + s->c[a] * f[q] + s->s[a] * noise[(size_t)k * m + q];
@@ -423,6 +501,7 @@ void adj_forward64(const adj_sys* s, const double* x0, const double* noise, int 
 			y[q] = v;
 		}
 	}
+	free(cache);
 	free(f);
 }
 
@@ -432,12 +511,21 @@ void adj_backward64(const adj_sys* s, const double* traj, int steps, double* lam
 	const size_t m = 3 * (size_t)s->n;
 	double* mu = (double*)calloc(m ? m : 1, sizeof(double));
 	double* t = (double*)malloc(sizeof(double) * m);
+	int* cache = NULL;
+	int cache_k0 = -1;
+	size_t np = 0;
 	for (int k = steps - 1; k >= 0; --k) {
 		for (size_t q = 0; q < m; ++q) mu[q] = s->c[q % 3] * lam[q];
 		memset(t, 0, sizeof(double) * m);
-		forces(s, traj + (size_t)k * m, NULL, mu, t, gpair, gbond);
+		if (s->list_every > 0) {
+			const int* list = step_pairs(s, traj, k, &cache_k0, &cache, &np);
+			forces_on(s, traj + (size_t)k * m, NULL, mu, t, gpair, gbond, list, np);
+		} else {
+			forces(s, traj + (size_t)k * m, NULL, mu, t, gpair, gbond);
+		}
 		for (size_t q = 0; q < m; ++q) lam[q] += t[q];
 	}
+	free(cache);
 	free(mu);
 	free(t);
 }

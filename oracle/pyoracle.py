@@ -889,7 +889,7 @@ class AdjSys(C.Structure):
                 ("excl_off", C.c_void_p), ("excl_nb", C.c_void_p), ("excl_n", C.c_int),
                 ("bonds", C.c_void_p), ("nb", C.c_int), ("bond", AdjTable),
                 ("angles", C.c_void_p), ("na", C.c_int), ("angle", AdjTable),
-                ("float_bins", C.c_int)]
+                ("float_bins", C.c_int), ("list_every", C.c_int), ("list_radius", C.c_double)]
 
 
 class Adjoint64:
@@ -899,7 +899,7 @@ class Adjoint64:
 
     def __init__(self, oracle: "Oracle", n, box_len, diffusion, dt, kT, pair, cutoff,
                  bonds=None, bond=None, angles=None, angle=None, exclusions=None,
-                 float_bins=False):
+                 float_bins=False, list_every=0, list_radius=0.0):
         """The box edges are taken as float32 values, as the library holds
         them. float_bins: decide table bins, cutoffs and angle clamps with the
         reference's float arithmetic (the derivative of a float forward along
@@ -916,6 +916,10 @@ class Adjoint64:
         s.n = int(n)
         d = np.asarray(diffusion, np.float64).reshape(3)
         s.float_bins = int(bool(float_bins))
+        # list_every > 0: pairs as the window's pairlist (built every list_every
+        # steps within list_radius) instead of all pairs within the cutoff.
+        s.list_every = int(list_every)
+        s.list_radius = float(list_radius)
         for a in range(3):
             s.L[a] = float(np.float32(box_len[a]))
             s.c[a] = float(d[a] * dt / kT)

@@ -193,3 +193,31 @@ def test_float_bin_decisions_match_double_off_edges(oracle):
         grads.append((g0, gp, gb, noise))
     for a, b in zip(grads[0][:3], grads[1][:3]):
         assert np.abs(a - b).max() <= 1e-6 * np.abs(a).max()
+
+
+def test_pairlist_segments_match_fresh_pairs_when_rebuilt_every_step(oracle):
+    """list_every = 1 (a list within the list radius built at every step) gives
+    the all-pairs-within-the-cutoff forward and adjoint; with longer segments
+    on a short window the pairs within the cutoff stay in the list too."""
+    rng = np.random.default_rng(5)
+    w = W.adjoint(seed=7, n_chains=4, beads=256)
+    x0 = np.mod(w.pos[:, :3].astype(np.float64) + rng.normal(scale=0.02, size=(w.n, 3)),
+                w.box_size[0])
+    t, b, a = w.pair_tables[0], w.bond_tables[0], w.angle_tables[0]
+
+    def system(every):
+        return po.Adjoint64(oracle, w.n, w.box_size, w.diffusion[0], w.dt, w.kT,
+                            (t.values, t.start, t.step_inv), w.cutoff, w.bonds,
+                            (b.values, b.start, b.step_inv), w.angles,
+                            (a.values, a.start, a.step_inv), w.exclusions, list_every=every,
+                            list_radius=w.list_radius)
+    noise = rng.normal(size=(10, w.n, 3))
+    lam = rng.normal(size=(w.n, 3))
+    ref_tr = system(0).forward(x0, noise)
+    ref_g = system(0).backward(ref_tr, lam)
+    for every in (1, 5):
+        A = system(every)
+        tr = A.forward(x0, noise)
+        assert np.abs(tr - ref_tr).max() < 1e-10
+        for g, h in zip(A.backward(ref_tr, lam), ref_g):
+            assert np.abs(g - h).max() <= 1e-12 * np.abs(h).max()
