@@ -184,6 +184,18 @@ MB2_API int mb2_pair_forces(mb2_context* ctx, const float* pos4, const int* type
                     float* force_energy4, uint32_t n, float cutoff, int get_energy,
                     void* stream);
 
+/* The pair kernels' form of the reference's pair test
+ * (PairNonbondedComputer, Pairwise.h:214-304: a pair is skipped when
+ * dist = sqrt(d2) < 1e-6 or dist * dist > cutoff * cutoff, in float): the
+ * test is d2 < *d2_lo or d2 > *d2_hi exactly, both bounds found by bisection
+ * over the floats (cutoff <= 0: no upper bound, *d2_hi = +inf). Host only. */
+MB2_API int mb2_pair_distance_window(float cutoff, float* d2_lo, float* d2_hi);
+/* Exhaustive device check of the pair kernels' correctly rounded square root
+ * (one Newton-Raphson step on the hardware estimate) against the CUDA
+ * intrinsic __fsqrt_rn on every float in [2^-60, FLT_MAX]: the mismatch count
+ * (0 when the kernels' root is the IEEE one). Synchronises. */
+MB2_API int mb2_selftest_sqrt(mb2_context* ctx, uint64_t* mismatches);
+
 /* FP64 reductions of the last force calls made with get_energy: pair energy,
  * pair virial (sum of r . f), bond energy, angle energy. Synchronises.
  * New on this path: the reference sums per-particle floats on the host

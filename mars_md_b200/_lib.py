@@ -138,6 +138,8 @@ def load(path: str = LIB_PATH):
     L.mb2_window_backward.argtypes = [vp, vp, vp, vp, vp, vp]
     L.mb2_window_checkpoints.argtypes = [vp, vp, u64, vp]
     L.mb2_window_record_states.argtypes = [vp, vp, u64]
+    L.mb2_pair_distance_window.argtypes = [f, fp, fp]
+    L.mb2_selftest_sqrt.argtypes = [vp, u64p]
     L.mb2_rdf_histogram.argtypes = [vp, vp, vp, u32, u32, f, f, f, vp, vp]
     L.mb2_rdf_backward.argtypes = [vp, vp, u32, u32, f, f, f, vp, vp, vp]
     L.mb2_batch_create.argtypes = [i, u32, u32p, fp, fp, C.POINTER(vp)]

@@ -820,6 +820,27 @@ int mb2_set_pair_terms(mb2_context* ctx, int num_types, const float* charge, con
 	});
 }
 
+int mb2_pair_distance_window(float cutoff, float* d2_lo, float* d2_hi) {
+	if (!d2_lo || !d2_hi) return MB2_ERR_ARG;
+	const DistWindow w = dist_window(cutoff > 0.0f ? cutoff * cutoff : 0.0f);
+	*d2_lo = w.lo;
+	*d2_hi = w.hi;
+	return MB2_OK;
+}
+
+int mb2_selftest_sqrt(mb2_context* ctx, uint64_t* mismatches) {
+	return guarded(ctx, [&] {
+		require(mismatches, MB2_ERR_ARG, "mb2_selftest_sqrt: null output");
+		DevBuf<unsigned long long> bad;
+		bad.ensure(1);
+		MB2_CUDA(cudaMemset(bad.ptr, 0, sizeof(unsigned long long)));
+		selftest_sqrt(bad.ptr, nullptr);
+		unsigned long long h = 0;
+		MB2_CUDA(cudaMemcpy(&h, bad.ptr, sizeof(h), cudaMemcpyDeviceToHost));
+		*mismatches = h;
+	});
+}
+
 int mb2_pair_forces(mb2_context* ctx, const float* pos4, const int* type_ids,
 					float* force_energy4, uint32_t n, float cutoff, int get_energy,
 					void* stream) {

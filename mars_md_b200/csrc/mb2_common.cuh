@@ -59,6 +59,31 @@ __device__ __forceinline__ float3 wrap_diff(const Box& b, float dx, float dy, fl
 	return make_float3(dx, dy, dz);
 }
 
+// Correctly rounded square root by Markstein's method (P. W. Markstein,
+// "Computation of elementary functions on the IBM RISC System/6000
+// processor", IBM J. Res. Develop. 34(1), 1990): the hardware estimate y of
+// 1/sqrt(a) (PTX rsqrt.approx), g = a y, and one Newton-Raphson correction
+// g + (a - g g) y / 2 whose residual a fused multiply-add computes exactly.
+// Equal to __fsqrt_rn on [2^-60, FLT_MAX], every float checked on the device
+// by mb2_selftest_sqrt; the pair kernel takes it only on squared distances
+// inside its window (from about 1e-12 up).
+__device__ __forceinline__ float sqrt_rn_nr(float a) {
+	float y;
+	asm("rsqrt.approx.f32 %0, %1;" : "=f"(y) : "f"(a));
+	const float g = __fmul_rn(a, y);
+	const float h = __fmul_rn(0.5f, y);
+	return __fmaf_rn(__fmaf_rn(-g, g, a), h, g);
+}
+
+// The reference's pair test as a window on the squared distance d2: it skips
+// a pair when dist = RN(sqrt(d2)) < 1e-6 or RN(dist * dist) > cutoff_sq
+// (cutoff_sq > 0). Both sides are monotone in d2, so the test is d2 < lo or
+// d2 > hi exactly, with lo and hi found on the host (dist_window).
+struct DistWindow {
+	float lo, hi;
+};
+DistWindow dist_window(float cutoff_sq);
+
 // Vector3_t::length2: x*x + y*y + z*z, left to right, no contraction.
 __device__ __forceinline__ float len2(float x, float y, float z) {
 	return __fadd_rn(__fadd_rn(__fmul_rn(x, x), __fmul_rn(y, y)), __fmul_rn(z, z));

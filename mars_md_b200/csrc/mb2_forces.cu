@@ -27,6 +27,7 @@
 // (per-thread double, block reduction, one double atomic per block).
 #include <algorithm>
 #include <cmath>
+#include <cstring>
 #include <type_traits>
 #include <vector>
 
@@ -207,7 +208,7 @@ __device__ __forceinline__ void pair_scalar(const float4& pi, float2 npi, const 
 											const TRow& trow, const float* bin_f,
 											const float2* bin_e, const PairTermRef* arow,
 											const PairSolvent& sv, const Box& box,
-											float cutoff_sq, float skip2, float4* force, float2& nxy, float& nz,
+											const DistWindow& win, float4* force, float2& nxy, float& nz,
 											float& fe, double& e_acc, double& w_acc) {
 	// r = wrap_diff(pos[second] - pos[first])
 	// (pi - pj is exactly -(pj - pi) in round-to-nearest, so a sign flip
@@ -234,12 +235,12 @@ __device__ __forceinline__ void pair_scalar(const float4& pi, float2 npi, const 
 	const float dx = dxy.x, dy = dxy.y;
 	const float2 sq = __fmul2_rn(dxy, dxy);
 	const float d2v = __fadd_rn(__fadd_rn(sq.x, sq.y), __fmul_rn(dz, dz));
-	// d2v above skip2 = cutoff_sq (1 + 2^-20) or more makes RN(RN(sqrt)^2)
-	// exceed cutoff_sq, so the pair fails the reference's test below: such
-	// lanes, and whole warps in the rows' far ends, leave before the root.
-	if (d2v > skip2) return;
-	const float dist = __fsqrt_rn(d2v);
-	if (dist < 1e-6f || (cutoff_sq > 0.0f && __fmul_rn(dist, dist) > cutoff_sq)) return;
+	// The reference's test (dist < 1e-6 or RN(dist^2) > cutoff_sq skips the
+	// pair) taken exactly on d2v, before the root: lanes beyond the cutoff,
+	// and whole warps in the rows' far ends, leave here. Inside the window the
+	// root below is the correctly rounded one.
+	if (d2v > win.hi || d2v < win.lo) return;
+	const float dist = sqrt_rn_nr(d2v);
 	const PairTableRef t = trow(type_of(pj));
 	float fm = 0.0f, e = 0.0f;
 	if (kTerms) {
@@ -320,7 +321,7 @@ __global__ void __launch_bounds__(
 	const PairTableRef* __restrict__ refs_g, const int* __restrict__ offs_g, PairTableRef uref,
 	const float* __restrict__ force_g,
 	const float2* __restrict__ energy_g, uint32_t total_bins,
-	const PairTermRef* __restrict__ terms_g, PairSolvent sv, BoxSrc boxes, float cutoff_sq,
+	const PairTermRef* __restrict__ terms_g, PairSolvent sv, BoxSrc boxes, DistWindow win,
 	float4* force, double* __restrict__ ev) {
 	constexpr int H = 32 / G;
 	// The per-type-pair references (T*T, 16 B each) are staged in shared
@@ -366,7 +367,6 @@ __global__ void __launch_bounds__(
 	const uint32_t cnt = valid ? row_len[i] : 0u;
 	// Entry k of row i: ((i / H) * cap + k) * H + i % H.
 	const uint32_t* col = nbr + (static_cast<size_t>(i / H) * cap) * H + (i % H);
-	const float skip2 = cutoff_sq > 0.0f ? cutoff_sq * 1.000001f : INFINITY;
 	const float2 npi = make_float2(-pi.x, -pi.y);
 	float2 nxy = make_float2(0.0f, 0.0f);  // minus the i-force, x and y
 	float nz = 0.0f, fe = 0.0f;
@@ -381,18 +381,18 @@ __global__ void __launch_bounds__(
 		const float4 p0 = sorted_pos[j0];
 		const float4 p1 = sorted_pos[j1];
 		pair_scalar<kEnergy, kAllPeriodic, kTerms>(pi, npi, p0, j0, e0 & kOrientBit, trow, bin_f,
-												   bin_e, arow, sv, box, cutoff_sq, skip2, force, nxy, nz,
+												   bin_e, arow, sv, box, win, force, nxy, nz,
 												   fe, e_acc, w_acc);
 		pair_scalar<kEnergy, kAllPeriodic, kTerms>(pi, npi, p1, j1, e1 & kOrientBit, trow, bin_f,
-												   bin_e, arow, sv, box, cutoff_sq, skip2, force, nxy, nz,
+												   bin_e, arow, sv, box, win, force, nxy, nz,
 												   fe, e_acc, w_acc);
 	}
 	if (t < cnt) {
 		const uint32_t entry = __ldcs(col + static_cast<size_t>(t) * H);
 		const uint32_t j = entry & ~kOrientBit;
 		pair_scalar<kEnergy, kAllPeriodic, kTerms>(pi, npi, sorted_pos[j], j, entry & kOrientBit,
-												   trow, bin_f, bin_e, arow, sv, box, cutoff_sq,
-												   skip2, force, nxy, nz, fe, e_acc, w_acc);
+												   trow, bin_f, bin_e, arow, sv, box, win, force,
+												   nxy, nz, fe, e_acc, w_acc);
 	}
 	// The lanes' sums of minus the i-force, then negated (exact).
 	float fx = nxy.x, fy = nxy.y, fz = nz;
@@ -644,8 +644,8 @@ void launch_pair(const float4* sorted_pos, const uint32_t* nbr, const uint32_t* 
 	MB2_LAUNCH kern<<<blocks, 256, smem, st>>>(sorted_pos, nbr, row_len, n, cap, t.num_types,
 											   t.refs, t.offsets, t.uniform_ref, t.bin_force,
 											   t.bin_energy, t.total_bins,
-											   t.terms, t.solvent, boxes, cutoff_sq, force_sorted,
-											   ev);
+											   t.terms, t.solvent, boxes, dist_window(cutoff_sq),
+											   force_sorted, ev);
 }
 
 template <int G, bool kEnergy, bool kAllPeriodic, class BoxSrc>
@@ -697,6 +697,55 @@ void launch_pair_lanes(const float4* sorted_pos, const uint32_t* nbr, const uint
 }
 
 }  // namespace
+
+namespace {
+
+// RN(sqrt(x)) and RN(s * s) in float on the host: the double root rounded to
+// float is the correctly rounded float root (53 >= 2 * 24 + 2 bits), and the
+// product of two floats is exact in double.
+float host_sqrt_rn(float x) { return static_cast<float>(std::sqrt(static_cast<double>(x))); }
+float host_sq_rn(float s) { return static_cast<float>(static_cast<double>(s) * s); }
+
+// Smallest non-negative float bit pattern in [lo, hi] for which pred holds
+// (pred monotone false -> true over the ordered patterns), or hi + 1.
+template <class P>
+uint32_t first_true(uint32_t lo, uint32_t hi, P pred) {
+	uint64_t a = lo, b = static_cast<uint64_t>(hi) + 1;
+	while (a < b) {
+		const uint64_t m = (a + b) / 2;
+		float x;
+		const uint32_t bits = static_cast<uint32_t>(m);
+		std::memcpy(&x, &bits, 4);
+		if (pred(x)) b = m;
+		else a = m + 1;
+	}
+	return static_cast<uint32_t>(a);
+}
+
+float from_bits(uint32_t b) {
+	float x;
+	std::memcpy(&x, &b, 4);
+	return x;
+}
+
+}  // namespace
+
+DistWindow dist_window(float cutoff_sq) {
+	constexpr uint32_t kMaxFinite = 0x7F7FFFFFu;
+	DistWindow w;
+	// lo: the least d2 whose root is not below 1e-6.
+	w.lo = from_bits(first_true(0u, kMaxFinite, [](float x) { return host_sqrt_rn(x) >= 1e-6f; }));
+	// hi: the largest d2 with RN(RN(sqrt(d2))^2) <= cutoff_sq.
+	if (!(cutoff_sq > 0.0f)) {
+		w.hi = INFINITY;
+	} else {
+		const uint32_t first_out = first_true(0u, kMaxFinite, [cutoff_sq](float x) {
+			return host_sq_rn(host_sqrt_rn(x)) > cutoff_sq;
+		});
+		w.hi = first_out > kMaxFinite ? INFINITY : from_bits(first_out - 1u);
+	}
+	return w;
+}
 
 size_t pair_table_arrays(int num_types, const uint32_t* term_matrix, int num_tables,
 						 const float* values, const uint32_t* sizes, const float* starts,
@@ -769,6 +818,36 @@ void pair_forces_systems(const float4* sorted_pos, const uint32_t* nbr, const ui
 	launch_pair_lanes(sorted_pos, nbr, row_len, n, cap, lanes_per_row, t,
 					  SystemBoxes{boxes, sorted_keys, sys_shift}, all_periodic, cutoff_sq,
 					  get_energy, force_sorted, ev, st);
+}
+
+namespace {
+
+// Every float with bit pattern in [lo, hi]: sqrt_rn_nr against __fsqrt_rn,
+// mismatches counted.
+__global__ void __launch_bounds__(256) sqrt_check_kernel(uint32_t lo, uint32_t hi,
+														unsigned long long* bad) {
+	const uint64_t count = static_cast<uint64_t>(hi) - lo + 1;
+	unsigned long long mine = 0;
+	for (uint64_t k = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; k < count;
+		 k += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
+		const float a = __uint_as_float(lo + static_cast<uint32_t>(k));
+		mine += __float_as_uint(__fsqrt_rn(a)) != __float_as_uint(sqrt_rn_nr(a));
+	}
+	if (mine) atomicAdd(bad, mine);
+}
+
+}  // namespace
+
+void selftest_sqrt(unsigned long long* bad, cudaStream_t st) {
+	int sms = 148;
+	int dev = 0;
+	MB2_CUDA(cudaGetDevice(&dev));
+	MB2_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+	const float lo = 0x1p-60f, hi = 3.40282347e38f;
+	uint32_t b[2];
+	std::memcpy(&b[0], &lo, 4);
+	std::memcpy(&b[1], &hi, 4);
+	MB2_LAUNCH sqrt_check_kernel<<<sms * 8, 256, 0, st>>>(b[0], b[1], bad);
 }
 
 void scatter_add_forces(const float4* force_sorted, const uint32_t* s2o, uint32_t n,

@@ -233,6 +233,9 @@ void pair_forces_systems(const float4* sorted_pos, const uint32_t* nbr, const ui
 						 double* ev, cudaStream_t st);
 void scatter_add_forces(const float4* force_sorted, const uint32_t* s2o, uint32_t n,
 						float4* force_energy, int get_energy, cudaStream_t st);
+// Exhaustive device check of sqrt_rn_nr against __fsqrt_rn on [2^-60,
+// FLT_MAX]: adds the mismatch count into *bad.
+void selftest_sqrt(unsigned long long* bad, cudaStream_t st);
 void bond_forces(const int2* bonds, const int* table_idx, uint32_t nb, const float4* pos,
 				 float4* fe, const Table* tables, const Box& box, int get_energy,
 				 double* energy, cudaStream_t st);

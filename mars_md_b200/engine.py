@@ -332,6 +332,13 @@ class Context:
         self.check(self.lib.mb2_baoab_last_update(self.h, _p(mom), _p(fe), _p(flags),
                                                   mom.shape[0], float(dt), _stream(stream)))
 
+    def selftest_sqrt(self) -> int:
+        """Mismatches of the pair kernels' square root against __fsqrt_rn over
+        every float in [2^-60, FLT_MAX] (0 expected)."""
+        a = C.c_uint64(0)
+        self.check(self.lib.mb2_selftest_sqrt(self.h, C.byref(a)))
+        return a.value
+
     def bd_seed(self, seed, patch_id, step) -> int:
         return int(self.lib.mb2_bd_seed(int(seed), int(patch_id), int(step)))
 
