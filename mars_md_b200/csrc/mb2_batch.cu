@@ -37,9 +37,11 @@ constexpr int kMaxLevel = kLocalBits;
 
 // Per-system cell grid and walk parameters (device copy per system).
 struct SysGrid {
-	WalkGrid wg;         // wg.shift = 3 * (7 - m)
-	uint32_t cell_base;  // first global cell of the system
-	uint32_t pad[3];
+	WalkGrid wg;           // wg.shift = 3 * (7 - m)
+	uint32_t cell_base;    // first global cell of the system
+	uint32_t stencil_off;  // the system's pruned cell stencil in the batch's array
+	uint32_t stencil_n;
+	uint32_t pad;
 };
 
 __device__ __forceinline__ uint32_t morton7(float x, float o, float scale) {
@@ -82,150 +84,113 @@ __global__ void __launch_bounds__(256) batch_cell_ranges_kernel(const uint32_t* 
 	if (i + 1 == n || cell(keys[i + 1]) != c) end[c] = i + 1;
 }
 
-__device__ __forceinline__ int wmin_i(int v) {
-#pragma unroll
-	for (int o = 16; o > 0; o >>= 1) v = min(v, __shfl_xor_sync(0xFFFFFFFFu, v, o));
-	return v;
-}
-__device__ __forceinline__ int wmax_i(int v) {
-#pragma unroll
-	for (int o = 16; o > 0; o >>= 1) v = max(v, __shfl_xor_sync(0xFFFFFFFFu, v, o));
-	return v;
-}
-
-__device__ __forceinline__ bool exact_hit_b(const Box& box, const float4& pi, const float4& pj,
-											float rc2) {
-	const float3 d = wrap_diff(box, __fsub_rn(pj.x, pi.x), __fsub_rn(pj.y, pi.y),
-							   __fsub_rn(pj.z, pi.z));
-	return len2(d.x, d.y, d.z) <= rc2;
-}
-
-// One warp per 32 consecutive sorted particles; the lanes of each system
-// present in the warp walk the cells around their cell box together (the
-// walk over a wide box is a superset of every lane's stencil, so the pair set
-// is exact either way). Rows are appended in candidate order.
-__global__ void __launch_bounds__(256) batch_walk_kernel(
+// One warp per particle row, the plain path's row walk (build_rows_kernel)
+// with the row's own system: its cell grid, its box (periodic on every axis)
+// and its pruned stencil. The lanes take the stencil's cells 32 at a time
+// (cells whose Morton code precedes the particle's hold only earlier
+// particles of the system and are skipped), lay their candidate ranges end to
+// end by a warp scan, and test 32 consecutive candidates a round with the
+// reference's exact test, each lane finding its candidate's cell by a binary
+// search over the running totals held one per lane. Hits are appended in
+// candidate order. Six resident blocks per SM (40 registers): 1 % faster per
+// build than 48 registers at five, and than 32 at eight.
+__global__ void __launch_bounds__(256, 6) batch_rows_kernel(
 	const float4* __restrict__ sorted_pos, const uint32_t* __restrict__ keys,
 	const uint32_t* __restrict__ s2o, const uint32_t* __restrict__ begin,
 	const uint32_t* __restrict__ end, const SysGrid* __restrict__ grids,
-	const Box* __restrict__ boxes, uint32_t n, uint32_t* __restrict__ nbr, uint32_t cap,
-	int hshift, uint32_t* __restrict__ row_len, unsigned long long* __restrict__ stats) {
-	__shared__ uint32_t split_tab[1 << kLocalBits];
-	for (int k = threadIdx.x; k < (1 << kLocalBits); k += blockDim.x) split_tab[k] = split_by3(k);
-	__syncthreads();
-	const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-	const int lane = threadIdx.x & 31;
-	if ((i & ~31u) >= n) return;  // whole warp past the end
-	const bool valid = i < n;
-	const int h = 1 << hshift;
-	const float4 pi = valid ? sorted_pos[i] : make_float4(0.f, 0.f, 0.f, 0.f);
-	const uint32_t key = valid ? keys[i] : 0u;
+	const Box* __restrict__ boxes, const uint4* __restrict__ stencil, uint32_t n,
+	uint32_t* __restrict__ nbr, uint32_t cap, int hshift, uint32_t* __restrict__ row_len,
+	unsigned long long* __restrict__ stats) {
+	const uint32_t i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+	if (i >= n) return;  // whole warp
+	const uint32_t lane = threadIdx.x & 31u;
+	const uint32_t lt = (1u << lane) - 1u;
+	const uint32_t key = keys[i];
 	const uint32_t sys = key >> kSysShift;
-	const int a = valid ? static_cast<int>(s2o[i]) : 0;
-	uint32_t* base = nbr + (static_cast<size_t>(i >> hshift) * cap << hshift) + (i & (h - 1));
+	const SysGrid* g = grids + sys;
+	const int m = g->wg.m;
+	const uint32_t c = (key & kLocalMask) >> g->wg.shift;
+	const float rc2 = g->wg.rc2;
+	const uint32_t cell_base = g->cell_base;
+	const uint4* st = stencil + g->stencil_off;
+	const int ns = static_cast<int>(g->stencil_n);
+	const Box* bx = boxes + sys;
+	const float lx = bx->size[0], ly = bx->size[1], lz = bx->size[2];
+	const float ix = bx->inv[0], iy = bx->inv[1], iz = bx->inv[2];
+	const float hx = bx->half[0], hy = bx->half[1], hz = bx->half[2];
+	// Interleaved (Morton) cell codes: x bits at 3k + 2, y at 3k + 1, z at 3k.
+	// A neighbour's code is the home code plus the stencil offset on each axis
+	// in interleaved form, carried through the other axes' bits (set to one)
+	// and masked, which wraps every axis modulo 2^m.
+	const uint32_t lvl = (1u << (3 * m)) - 1u;
+	const uint32_t mx = 0x24924924u & lvl, my = 0x12492492u & lvl, mz = 0x09249249u & lvl;
+	const uint32_t cxo = c | ~mx, cyo = c | ~my, czo = c | ~mz;
+	const float4 pi = sorted_pos[i];
+	const int a = static_cast<int>(s2o[i]);
+	const uint32_t h = 1u << hshift;
+	uint32_t* base = nbr + (static_cast<size_t>(i >> hshift) * cap << hshift) + (i & (h - 1u));
 	uint32_t len = 0;
-	uint32_t remaining = __ballot_sync(0xFFFFFFFFu, valid);
-	while (remaining) {
-		const int leader = __ffs(remaining) - 1;
-		const uint32_t s0 = __shfl_sync(0xFFFFFFFFu, sys, leader);
-		const bool active = valid && sys == s0;
-		remaining &= ~__ballot_sync(0xFFFFFFFFu, active);
-		const SysGrid& g = grids[s0];
-		const WalkGrid& wg = g.wg;
-		const Box& box = boxes[s0];
-		const uint32_t c = (key & kLocalMask) >> wg.shift;
-		const int cx = static_cast<int>(compact_by3(c >> 2));
-		const int cy = static_cast<int>(compact_by3(c >> 1));
-		const int cz = static_cast<int>(compact_by3(c));
-		const int x0 = wmin_i(active ? cx : INT_MAX), x1 = wmax_i(active ? cx : INT_MIN);
-		const int y0 = wmin_i(active ? cy : INT_MAX), y1 = wmax_i(active ? cy : INT_MIN);
-		const int z0 = wmin_i(active ? cz : INT_MAX), z1 = wmax_i(active ? cz : INT_MIN);
-		const uint32_t c_first = __shfl_sync(0xFFFFFFFFu, c, leader);
-		const uint32_t i_first = __shfl_sync(0xFFFFFFFFu, i, leader);
-		const int cells = 1 << wg.m;
-		const int lo[3] = {x0, y0, z0}, hi[3] = {x1, y1, z1};
-		int from[3], to[3];
-		bool full[3];
-#pragma unroll
-		for (int ax = 0; ax < 3; ++ax) {
-			// Every batched box is periodic on every axis.
-			full[ax] = hi[ax] - lo[ax] + 2 * wg.radius[ax] + 1 >= cells;
-			from[ax] = full[ax] ? 0 : lo[ax] - wg.radius[ax];
-			to[ax] = full[ax] ? cells - 1 : hi[ax] + wg.radius[ax];
-		}
-		const uint32_t* cb = begin + g.cell_base;
-		const uint32_t* ce = end + g.cell_base;
-		for (int ux = from[0]; ux <= to[0]; ++ux) {
-			int nx = ux;
-			float shx = 0.0f, gx = 0.0f;
-			if (!full[0]) {
-				const int gc = ux < x0 ? x0 - ux - 1 : (ux > x1 ? ux - x1 - 1 : 0);
-				gx = static_cast<float>(gc) * wg.wmin[0];
-				if (ux < 0) { nx = ux + cells; shx = -box.size[0]; }
-				else if (ux >= cells) { nx = ux - cells; shx = box.size[0]; }
-			}
-			const float gx2 = gx * gx;
-			if (gx2 > wg.lim) continue;
-			for (int uy = from[1]; uy <= to[1]; ++uy) {
-				int ny = uy;
-				float shy = 0.0f, gy = 0.0f;
-				if (!full[1]) {
-					const int gc = uy < y0 ? y0 - uy - 1 : (uy > y1 ? uy - y1 - 1 : 0);
-					gy = static_cast<float>(gc) * wg.wmin[1];
-					if (uy < 0) { ny = uy + cells; shy = -box.size[1]; }
-					else if (uy >= cells) { ny = uy - cells; shy = box.size[1]; }
-				}
-				const float gxy2 = gx2 + gy * gy;
-				if (gxy2 > wg.lim) continue;
-				for (int uz = from[2]; uz <= to[2]; ++uz) {
-					int nz = uz;
-					float shz = 0.0f, gz = 0.0f;
-					if (!full[2]) {
-						const int gc = uz < z0 ? z0 - uz - 1 : (uz > z1 ? uz - z1 - 1 : 0);
-						gz = static_cast<float>(gc) * wg.wmin[2];
-						if (uz < 0) { nz = uz + cells; shz = -box.size[2]; }
-						else if (uz >= cells) { nz = uz - cells; shz = box.size[2]; }
-					}
-					if (gxy2 + gz * gz > wg.lim) continue;
-					const uint32_t nc =
-						(split_tab[nx] << 2) | (split_tab[ny] << 1) | split_tab[nz];
-					if (nc < c_first) continue;
-					const uint32_t b = cb[nc], e = ce[nc];
-					const uint32_t jlo = b > i_first + 1u ? b : i_first + 1u;
-					if (jlo >= e) continue;
-					const float qx = pi.x - shx, qy = pi.y - shy, qz = pi.z - shz;
-					for (uint32_t j = jlo; j < e; ++j) {
-						const float4 pj = sorted_pos[j];
-						if (!active || j <= i) continue;
-						float dx = pj.x - qx, dy = pj.y - qy, dz = pj.z - qz;
-						if (full[0]) dx -= box.size[0] * rintf(dx * box.inv[0]);
-						if (full[1]) dy -= box.size[1] * rintf(dy * box.inv[1]);
-						if (full[2]) dz -= box.size[2] * rintf(dz * box.inv[2]);
-						const float d2 = dx * dx + dy * dy + dz * dz;
-						bool hit = d2 < wg.fast_lo;
-						if (!hit && d2 <= wg.fast_hi) hit = exact_hit_b(box, pi, pj, wg.rc2);
-						if (hit) {
-							const int bj = static_cast<int>(s2o[j]);
-							if (len < cap)
-								base[static_cast<size_t>(len) * h] = j | (bj < a ? kOrientBit : 0u);
-							++len;
-						}
-					}
-				}
+	for (int k0 = 0; k0 < ns; k0 += 32) {
+		uint32_t jb = 0, je = 0;
+		const int k = k0 + static_cast<int>(lane);
+		if (k < ns) {
+			const uint4 se = st[k];  // interleaved offsets, modulo 2^m per axis
+			const uint32_t nc = ((cxo + se.x) & mx) | ((cyo + se.y) & my) | ((czo + se.z) & mz);
+			if (nc >= c) {
+				const uint32_t b = begin[cell_base + nc];
+				jb = b > i + 1u ? b : i + 1u;
+				je = end[cell_base + nc];
 			}
 		}
-	}
-	unsigned long long tot = valid ? len : 0u;
-	int mx = valid ? static_cast<int>(min(len, 0x7FFFFFFFu)) : 0;
-	if (valid) row_len[i] = len;
+		// The chunk's candidate ranges laid end to end (a scan of their
+		// lengths); each round the lanes take the next 32 candidates, lane l
+		// finding the cell that holds candidate t0 + l by a binary search over
+		// the lanes' running totals. An empty cell (begin = end = 0) or one
+		// ending at i has jb >= je.
+		const uint32_t cnt = je > jb ? je - jb : 0u;
+		uint32_t incl = cnt;
 #pragma unroll
-	for (int o = 16; o > 0; o >>= 1) {
-		tot += __shfl_xor_sync(0xFFFFFFFFu, tot, o);
-		mx = max(mx, __shfl_xor_sync(0xFFFFFFFFu, mx, o));
+		for (int o = 1; o < 32; o <<= 1) {
+			const uint32_t v = __shfl_up_sync(0xFFFFFFFFu, incl, o);
+			if (static_cast<int>(lane) >= o) incl += v;
+		}
+		const uint32_t total = __shfl_sync(0xFFFFFFFFu, incl, 31);
+		const uint32_t excl = incl - cnt;
+		for (uint32_t t0 = 0; t0 < total; t0 += 32u) {
+			const uint32_t t = t0 + lane;
+			int owner = 0;  // first lane whose running total exceeds t
+#pragma unroll
+			for (int step = 16; step > 0; step >>= 1) {
+				const uint32_t v = __shfl_sync(0xFFFFFFFFu, incl, owner + step - 1);
+				if (v <= t) owner += step;
+			}
+			const uint32_t ob = __shfl_sync(0xFFFFFFFFu, jb, owner & 31);
+			const uint32_t oe = __shfl_sync(0xFFFFFFFFu, excl, owner & 31);
+			bool hit = false;
+			uint32_t entry = 0;
+			if (t < total) {
+				const uint32_t j = ob + (t - oe);
+				const float4 pj = sorted_pos[j];
+				const float dx = wrap_diff_scalar(__fsub_rn(pj.x, pi.x), lx, ix, hx);
+				const float dy = wrap_diff_scalar(__fsub_rn(pj.y, pi.y), ly, iy, hy);
+				const float dz = wrap_diff_scalar(__fsub_rn(pj.z, pi.z), lz, iz, hz);
+				if (len2(dx, dy, dz) <= rc2) {
+					hit = true;
+					entry = j | (static_cast<int>(s2o[j]) < a ? kOrientBit : 0u);
+				}
+			}
+			const uint32_t hm = __ballot_sync(0xFFFFFFFFu, hit);
+			if (hit) {
+				const uint32_t p = len + static_cast<uint32_t>(__popc(hm & lt));
+				if (p < cap) base[static_cast<size_t>(p) * h] = entry;
+			}
+			len += static_cast<uint32_t>(__popc(hm));
+		}
 	}
 	if (lane == 0) {
-		atomicAdd(stats, tot);
-		atomicMax(stats + 1, static_cast<unsigned long long>(mx));
+		row_len[i] = len;
+		atomicAdd(stats, static_cast<unsigned long long>(len));
+		atomicMax(stats + 1, static_cast<unsigned long long>(len));
 	}
 }
 
@@ -263,6 +228,7 @@ struct mb2_batch {
 	DevBuf<float4> sorted_pos, ref_pos, force_sorted;
 	DevBuf<SysGrid> grids;
 	std::vector<SysGrid> grids_h;
+	DevBuf<uint4> stencil;  // every system's pruned cell stencil (interleaved offsets), concatenated
 	uint32_t total_cells = 0;
 	float grid_rc = -1.0f;
 	int level_offset = 0;
@@ -333,6 +299,7 @@ uint64_t f2u(float f) {
 // the 7-bit Morton scale) shifted by the tuner's level offset.
 void choose_grids(mb2_batch* b, float rc) {
 	b->grids_h.resize(b->num_systems);
+	std::vector<uint4> stencil;
 	uint32_t base = 0;
 	for (uint32_t s = 0; s < b->num_systems; ++s) {
 		const Box& bx = b->boxes_h[s];
@@ -353,10 +320,24 @@ void choose_grids(mb2_batch* b, float rc) {
 		wg.lim = g.lim;
 		wg.rc2 = rc * rc;
 		fast_test_band(bx, rc, &wg.fast_lo, &wg.fast_hi);
+		wg.split2 = INFINITY;
 		sg.cell_base = base;
+		sg.stencil_off = static_cast<uint32_t>(stencil.size());
+		sg.stencil_n = static_cast<uint32_t>(g.stencil.size());
+		// Offsets modulo 2^m per axis (every batched box is periodic), interleaved
+		// into Morton bit positions.
+		const int cells = 1 << g.m;
+		for (const StencilEntry& e : g.stencil) {
+			auto d = [cells](int v) { return split_by3(static_cast<uint32_t>((v % cells + cells) % cells)); };
+			stencil.push_back(make_uint4(d(e.dx) << 2, d(e.dy) << 1, d(e.dz), 0u));
+		}
 		base += 1u << (3 * g.m);
 		b->grids_h[s] = sg;
 	}
+	b->stencil.ensure(std::max<size_t>(stencil.size(), 1));
+	if (!stencil.empty())
+		MB2_CUDA(cudaMemcpy(b->stencil.ptr, stencil.data(), stencil.size() * sizeof(uint4),
+							cudaMemcpyHostToDevice));
 	b->total_cells = base;
 	b->grids.ensure(b->num_systems);
 	MB2_CUDA(cudaMemcpy(b->grids.ptr, b->grids_h.data(), b->num_systems * sizeof(SysGrid),
@@ -396,10 +377,10 @@ void batch_build(mb2_batch* b, const float4* pos, const int* type_ids, float rc,
 		MB2_CUDA(cudaMemsetAsync(b->stats.ptr, 0, 2 * sizeof(unsigned long long), st));
 		if (n) {
 			const int hshift = __builtin_ctz(32 / b->lanes);
-			MB2_LAUNCH batch_walk_kernel<<<(n + 255) / 256, 256, 0, st>>>(
+			MB2_LAUNCH batch_rows_kernel<<<(n + 7) / 8, 256, 0, st>>>(
 				b->sorted_pos.ptr, b->keys.ptr, b->s2o.ptr, b->cell_begin.ptr, b->cell_end.ptr,
-				b->grids.ptr, b->boxes.ptr, n, b->nbr.ptr, cap, hshift, b->row_len.ptr,
-				b->stats.ptr);
+				b->grids.ptr, b->boxes.ptr, b->stencil.ptr, n, b->nbr.ptr, cap, hshift,
+				b->row_len.ptr, b->stats.ptr);
 		}
 		MB2_CUDA(cudaMemcpyAsync(b->pinned, b->stats.ptr, 2 * sizeof(unsigned long long),
 								 cudaMemcpyDeviceToHost, st));

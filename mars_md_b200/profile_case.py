@@ -13,6 +13,10 @@ polymers: the 65,536-bead polymer workload with bonds, angles, 1-2/1-3
 exclusions and the 256^3 grid potential; S fused steps (the integrate kernel
 samples the grid for every bead each step).
 
+batched: the 512 batched systems (500 to 20,000 beads each, 2,742,131 in
+all) at the default tuning with a rebuild at every step (the cadence the
+autotuner picks for them); S batched steps.
+
 Few launches precede the kernels of interest, as ncu captures need.
 """
 import argparse
@@ -30,10 +34,13 @@ def main(argv=None):
     ap.add_argument("--steps", type=int, default=0)
     ap.add_argument("--split-rows", action="store_true",
                     help="rebuild once more with near/far rows at the interaction cutoff")
-    ap.add_argument("--workload", choices=("large_plain", "polymers"), default="large_plain")
+    ap.add_argument("--workload", choices=("large_plain", "polymers", "batched"),
+                    default="large_plain")
     a = ap.parse_args(argv)
     if a.workload == "polymers":
         return polymers(a.steps)
+    if a.workload == "batched":
+        return batched(a.steps)
     w = W.large_plain(n=a.n)
     ctx = Context(w.n)
     dev = setup_workload(ctx, w)
@@ -70,6 +77,18 @@ def polymers(steps):
     torch.cuda.synchronize()
     print("ok", w.n, ctx.num_pairs())
     ctx.close()
+
+
+def batched(steps):
+    from .engine import setup_batch
+    ws = W.batched(seed=W.DEFAULT_SEED)
+    prm = step_params(ws[0], seed=W.DEFAULT_SEED)
+    b, dev = setup_batch(ws)
+    b.set_rebuild_period(1)
+    b.run(dev["pos"], dev["fe"], dev["type"], 1, steps, prm)
+    torch.cuda.synchronize()
+    print("ok", sum(w.n for w in ws), b.num_pairs())
+    b.close()
 
 
 if __name__ == "__main__":
