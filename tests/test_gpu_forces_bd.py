@@ -66,6 +66,28 @@ def test_pair_forces_plain_bd(ctx_factory, oracle, lanes, split):
     assert np.abs(fe[:, :3].astype(np.float64).sum(0)).max() <= 1e-3 * fabs.sum() / len(fabs)
 
 
+def test_pair_forces_without_cutoff(ctx_factory, oracle):
+    """cutoff 0: the reference evaluates every listed pair (its test then has
+    no upper bound), here the window's upper bound is +inf; pairs between
+    the 20 A table end and the 25 A list radius take the last bin."""
+    w = W.plain_bd()
+    ctx = ctx_factory(w.n)
+    dev = setup_workload(ctx, w)
+    ctx.build_pairlist(dev["pos"], dev["type"], w.list_radius)
+    pairs = ctx.export_pairs().cpu().numpy()
+    ctx.reset_energies()
+    ctx.pair_forces(dev["pos"], dev["type"], dev["fe"], 0.0, get_energy=True)
+    e = ctx.energies()
+    fe = dev["fe"].cpu().numpy()
+    tags = oracle.resolve_tags(pairs, w.type_ids, w.term_matrix, w.num_types)
+    f32, f64, fabs = oracle.pair_forces(pairs, w.pos, tags, tableset(w), box_of(w),
+                                        np.float32(0.0))
+    e64 = oracle.pair_energy_f64(pairs, w.pos, tags, tableset(w), box_of(w), np.float32(0.0))
+    scaled, plain = force_errors(fe, f64, fabs)
+    assert plain <= 1e-5, (plain, scaled)
+    assert abs(e[0] - e64) <= 1e-6 * abs(e64)
+
+
 @pytest.mark.parametrize("split", [False, True])
 def test_pair_forces_large_types(ctx_factory, oracle, split):
     # 4 types, 10 tables, Debye-Hueckel + soft core, at 1/64 of the full size
