@@ -758,22 +758,9 @@ int mb2_set_pair_tables(mb2_context* ctx, int num_types, const uint32_t* term_ma
 							cudaMemcpyHostToDevice));
 		// Tables of one start, bin width and length for every type pair that
 		// has one (compared bit for bit): the kernel reads 4-byte offsets.
-		std::vector<int> offs(tt, -1);
-		bool uniform = false, any = false;
-		PairTableRef u{0.0f, 0.0f, 0, -1};
-		for (int k = 0; k < tt; ++k) {
-			offs[k] = refs[k].offset;
-			if (refs[k].offset < 0) continue;
-			if (!any) {
-				u = refs[k];
-				any = uniform = true;
-			} else if (std::memcmp(&u.start, &refs[k].start, sizeof(float)) != 0 ||
-					   std::memcmp(&u.step_inv, &refs[k].step_inv, sizeof(float)) != 0 ||
-					   u.last != refs[k].last) {
-				uniform = false;
-			}
-		}
-		u.offset = -1;
+		std::vector<int> offs;
+		PairTableRef u;
+		const bool uniform = uniform_tables(refs, offs, u);
 		ctx->table_offsets.ensure(tt);
 		MB2_CUDA(cudaMemcpy(ctx->table_offsets.ptr, offs.data(), tt * sizeof(int),
 							cudaMemcpyHostToDevice));

@@ -248,6 +248,7 @@ struct mb2_batch {
 	// tables and types
 	PairTables pt;
 	DevBuf<PairTableRef> refs;
+	DevBuf<int> table_offsets;
 	DevBuf<float> bin_force;
 	DevBuf<float2> bin_energy;
 	TypeTable types;
@@ -590,9 +591,18 @@ int mb2_batch_set_pair_tables(mb2_batch* b, int num_types, const uint32_t* term_
 							cudaMemcpyHostToDevice));
 		MB2_CUDA(cudaMemcpy(b->bin_force.ptr, bf.data(), bf.size() * 4, cudaMemcpyHostToDevice));
 		MB2_CUDA(cudaMemcpy(b->bin_energy.ptr, be.data(), be.size() * 8, cudaMemcpyHostToDevice));
+		std::vector<int> offs;
+		PairTableRef u;
+		const bool uniform = uniform_tables(refs, offs, u);
+		b->table_offsets.ensure(tt);
+		MB2_CUDA(cudaMemcpy(b->table_offsets.ptr, offs.data(), tt * sizeof(int),
+							cudaMemcpyHostToDevice));
 		b->pt.num_types = num_types;
 		b->pt.total_bins = static_cast<uint32_t>(total);
 		b->pt.refs = b->refs.ptr;
+		b->pt.offsets = b->table_offsets.ptr;
+		b->pt.uniform = uniform;
+		b->pt.uniform_ref = u;
 		b->pt.bin_force = b->bin_force.ptr;
 		b->pt.bin_energy = b->bin_energy.ptr;
 	});
@@ -695,7 +705,17 @@ int mb2_batch_run(mb2_batch* b, float* pos4, float* force_energy4, const int* ty
 				reinterpret_cast<uint64_t>(type_ids), reinterpret_cast<uint64_t>(b->nbr.ptr),
 				reinterpret_cast<uint64_t>(b->force_sorted.ptr), b->cap,
 				static_cast<uint64_t>(b->lanes), b->n, f2u(prm->cutoff), f2u(prm->dt),
-				f2u(prm->kT), prm->seed, prm->patch_id};
+				f2u(prm->kT), prm->seed, prm->patch_id,
+				// tables and types (pointers, sizes, the uniform-table constants)
+				reinterpret_cast<uint64_t>(b->pt.refs), reinterpret_cast<uint64_t>(b->pt.offsets),
+				reinterpret_cast<uint64_t>(b->pt.bin_force),
+				reinterpret_cast<uint64_t>(b->pt.bin_energy), b->pt.total_bins,
+				static_cast<uint64_t>(b->pt.num_types), static_cast<uint64_t>(b->pt.uniform),
+				f2u(b->pt.uniform_ref.start), f2u(b->pt.uniform_ref.step_inv),
+				static_cast<uint64_t>(b->pt.uniform_ref.last),
+				reinterpret_cast<uint64_t>(b->types.charge),
+				reinterpret_cast<uint64_t>(b->types.diffusion),
+				static_cast<uint64_t>(b->types.num_types)};
 			if (!b->graph || key != b->graph_key) {
 				if (b->graph) {
 					MB2_CUDA(cudaGraphExecDestroy(b->graph));

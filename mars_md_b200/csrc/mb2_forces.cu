@@ -307,10 +307,12 @@ struct SystemBoxes {
 // blocks (32 registers, full occupancy) ran it 6 % faster than the 40
 // registers it takes unbounded, in spite of a few bytes of spill (none in the
 // uniform-table variant); the energy and analytical variants need their
-// registers, and the batched variant (box per row) spills heavily at 32.
+// registers. The batched variant (box per row) runs best at 6 blocks (40
+// registers, a few bytes of spill): 1.06 -> 1.02 ms per batched step against
+// 48 registers, and 1.08 at 8 blocks, where it spills 60 bytes.
 template <bool kEnergy, bool kTerms, bool kOneBox>
 constexpr int pair_min_blocks() {
-	return !kOneBox ? 1 : (kTerms ? 3 : (kEnergy ? 5 : 8));
+	return !kOneBox ? 6 : (kTerms ? 3 : (kEnergy ? 5 : 8));
 }
 
 template <int G, bool kEnergy, bool kAllPeriodic, bool kTerms, bool kUniform, class BoxSrc>
@@ -659,11 +661,11 @@ void launch_pair_t(const float4* sorted_pos, const uint32_t* nbr, const uint32_t
 														cutoff_sq, force_sorted, ev, st);
 			return;
 		}
-		if (t.uniform && t.offsets) {
-			launch_pair<G, kEnergy, kAllPeriodic, false, BoxSrc, true>(
-				sorted_pos, nbr, row_len, n, cap, t, boxes, cutoff_sq, force_sorted, ev, st);
-			return;
-		}
+	}
+	if (t.uniform && t.offsets) {
+		launch_pair<G, kEnergy, kAllPeriodic, false, BoxSrc, true>(
+			sorted_pos, nbr, row_len, n, cap, t, boxes, cutoff_sq, force_sorted, ev, st);
+		return;
 	}
 	launch_pair<G, kEnergy, kAllPeriodic, false>(sorted_pos, nbr, row_len, n, cap, t, boxes,
 												 cutoff_sq, force_sorted, ev, st);
@@ -797,6 +799,27 @@ size_t pair_table_arrays(int num_types, const uint32_t* term_matrix, int num_tab
 		}
 	}
 	return total;
+}
+
+bool uniform_tables(const std::vector<PairTableRef>& refs, std::vector<int>& offsets,
+					PairTableRef& u) {
+	bool uniform = false, any = false;
+	u = PairTableRef{0.0f, 0.0f, 0, -1};
+	offsets.assign(refs.size(), -1);
+	for (size_t k = 0; k < refs.size(); ++k) {
+		offsets[k] = refs[k].offset;
+		if (refs[k].offset < 0) continue;
+		if (!any) {
+			u = refs[k];
+			any = uniform = true;
+		} else if (std::memcmp(&u.start, &refs[k].start, sizeof(float)) != 0 ||
+				   std::memcmp(&u.step_inv, &refs[k].step_inv, sizeof(float)) != 0 ||
+				   u.last != refs[k].last) {
+			uniform = false;
+		}
+	}
+	u.offset = -1;
+	return uniform;
 }
 
 void pair_forces(const float4* sorted_pos, const uint32_t* nbr, const uint32_t* row_len,

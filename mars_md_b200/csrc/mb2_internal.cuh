@@ -225,6 +225,11 @@ size_t pair_table_arrays(int num_types, const uint32_t* term_matrix, int num_tab
 						 const float* values, const uint32_t* sizes, const float* starts,
 						 const float* step_invs, std::vector<PairTableRef>& refs,
 						 std::vector<float>& bf, std::vector<float2>& be);
+// Host: per-type-pair table offsets (-1: no table) and whether every type
+// pair with a table uses one start, step inverse and length (compared bit for
+// bit), which *u then holds (offset -1).
+bool uniform_tables(const std::vector<PairTableRef>& refs, std::vector<int>& offsets,
+					PairTableRef& u);
 // Batched replicas: row i's box is boxes[sorted_keys[i] >> sys_shift].
 void pair_forces_systems(const float4* sorted_pos, const uint32_t* nbr, const uint32_t* row_len,
 						 uint32_t n, uint32_t cap, int lanes_per_row, const PairTables& t,
