@@ -319,6 +319,19 @@ def run_ours(args):
     traffic = _traffic_from_profile()
     b_ps = 32.0 + 4.0 * p_half + (100.0 + 4.0 * p_half) / w.rebuild_period
     roof_ps = bw * 1e9 / b_ps
+    # HBM GB/s per kernel from algorithmic bytes over the CUDA-event time: the
+    # pair-force launch (above); the integrate (position read and write, the
+    # pair force gathered through the inverse map with its index, type id,
+    # ForceEnergy write: 72 B per bead); the rebuild (sort, cell ranges and
+    # list writes: 100 B per bead plus 4 B per stored half pair).
+    per_kernel_bytes = {"pair_force_kernel": pf_bytes, "integrate_kernel": w.n * 72.0,
+                        "pairlist_build": w.n * (100.0 + 4.0 * p_half)}
+    kernel_gbs = {}
+    for k, nbytes in per_kernel_bytes.items():
+        t_ms, cnt = prof[k]
+        if cnt:
+            gbs = nbytes / (t_ms / cnt / 1e3) / 1e9
+            kernel_gbs[k] = {"gbs": gbs, "frac": gbs / bw, "bytes_per_launch": nbytes}
 
     out = {
         "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps,
@@ -331,6 +344,7 @@ def run_ours(args):
                               "step_roofline_particle_steps_per_s": roof_ps,
                               "step_roofline_frac": (value / world) / roof_ps,
                               "kernel_ms": {k: (v[0] / max(v[1], 1)) for k, v in prof.items()},
+                              "kernel_gbs": kernel_gbs,
                               "hbm_peak": peak_kind}),
         "roofline": {"bound": "hbm", "kernel": "pair_force", "achieved": achieved, "peak": bw,
                      "unit": "GB/s", "frac": achieved / bw, "traffic": traffic,

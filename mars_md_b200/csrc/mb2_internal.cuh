@@ -80,7 +80,8 @@ struct Scratch {
 	}
 };
 
-// One entry of the cell stencil: offsets to add to the home cell.
+// One entry of the cell stencil: offsets to add to the home cell; pad holds
+// the same offsets modulo 2^m interleaved into Morton bit positions.
 struct StencilEntry {
 	int dx, dy, dz, pad;
 };

@@ -90,7 +90,18 @@ CellGrid choose_cell_grid(const float* extent, const int* periodic, float rc_lis
 				for (size_t z = 0; z < off[2].size(); ++z) {
 					const double g2 =
 						gap[0][x] * gap[0][x] + gap[1][y] * gap[1][y] + gap[2][z] * gap[2][z];
-					if (g2 <= lim) st.push_back(StencilEntry{off[0][x], off[1][y], off[2][z], 0});
+					if (g2 <= lim) {
+						// pad: the offsets modulo 2^m interleaved into Morton bit
+						// positions (x at 3k + 2, y at 3k + 1, z at 3k).
+						const auto wrap = [cells](int v) {
+							return static_cast<uint32_t>(((v % cells) + cells) % cells);
+						};
+						const uint32_t d = (split_by3(wrap(off[0][x])) << 2) |
+										   (split_by3(wrap(off[1][y])) << 1) |
+										   split_by3(wrap(off[2][z]));
+						st.push_back(StencilEntry{off[0][x], off[1][y], off[2][z],
+												  static_cast<int>(d)});
+					}
 				}
 		const double per_cell = static_cast<double>(n) / num_cells;
 		const double cost = static_cast<double>(st.size()) * (per_cell + 2.0);
@@ -534,12 +545,18 @@ __global__ void __launch_bounds__(256) build_rows_kernel(
 	const uint32_t lane = threadIdx.x & 31u;
 	const uint32_t lt = (1u << lane) - 1u;
 	const int cells = 1 << wg.m;
-	const uint32_t mask = static_cast<uint32_t>(cells - 1);
 	const float4 pi = sorted_pos[i];
 	const uint32_t c = keys[i] >> wg.shift;
 	const int cx = static_cast<int>(compact_by3(c >> 2));
 	const int cy = static_cast<int>(compact_by3(c >> 1));
 	const int cz = static_cast<int>(compact_by3(c));
+	// A neighbour's cell code is the home code plus the stencil entry's
+	// interleaved offset on each axis, carried through the other axes' bits
+	// (set to one) and masked: modulo 2^m per axis, so open axes also check
+	// the plain coordinate range.
+	const uint32_t lvl = (1u << (3 * wg.m)) - 1u;
+	const uint32_t mx = 0x24924924u & lvl, my = 0x12492492u & lvl, mz = 0x09249249u & lvl;
+	const uint32_t cxo = c | ~mx, cyo = c | ~my, czo = c | ~mz;
 	const int a = static_cast<int>(s2o[i]);
 	int row_b = 0, row_e = 0, body = -1;
 	if (kExcl) {
@@ -557,18 +574,14 @@ __global__ void __launch_bounds__(256) build_rows_kernel(
 		const int k = k0 + static_cast<int>(lane);
 		if (k < ns) {
 			const StencilEntry se = stencil_g[k];
-			int nx = cx + se.dx, ny = cy + se.dy, nz = cz + se.dz;
 			bool in = true;
-			if (box.periodic[0]) nx = static_cast<int>(static_cast<uint32_t>(nx + cells) & mask);
-			else in = in && nx >= 0 && nx < cells;
-			if (box.periodic[1]) ny = static_cast<int>(static_cast<uint32_t>(ny + cells) & mask);
-			else in = in && ny >= 0 && ny < cells;
-			if (box.periodic[2]) nz = static_cast<int>(static_cast<uint32_t>(nz + cells) & mask);
-			else in = in && nz >= 0 && nz < cells;
+			if (!box.periodic[0]) in = in && static_cast<unsigned>(cx + se.dx) < static_cast<unsigned>(cells);
+			if (!box.periodic[1]) in = in && static_cast<unsigned>(cy + se.dy) < static_cast<unsigned>(cells);
+			if (!box.periodic[2]) in = in && static_cast<unsigned>(cz + se.dz) < static_cast<unsigned>(cells);
 			if (in) {
-				const uint32_t nc = (split_by3(static_cast<uint32_t>(nx)) << 2) |
-									(split_by3(static_cast<uint32_t>(ny)) << 1) |
-									split_by3(static_cast<uint32_t>(nz));
+				const uint32_t d = static_cast<uint32_t>(se.pad);
+				const uint32_t nc = ((cxo + (d & mx)) & mx) | ((cyo + (d & my)) & my) |
+									((czo + (d & mz)) & mz);
 				if (nc >= c) {  // earlier cells hold only earlier particles
 					const uint32_t b = begin[nc];
 					jb = b > i + 1u ? b : i + 1u;
