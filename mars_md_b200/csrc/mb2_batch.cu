@@ -7,8 +7,8 @@
 // radix sort groups the systems and orders each one spatially; cells of
 // system s are the top 3 m_s bits of its 21-bit code, stored after the cells
 // of systems < s. The pairlist is one sliced-ELL half list over all sorted
-// particles (a row's neighbours are always in its own system); a warp whose
-// 32 sorted particles straddle systems walks each system's lanes in turn.
+// particles (a row's neighbours are always in its own system), walked one
+// warp per row over the row's own system grid, box and stencil.
 // Pair forces read each row's box from the system table; the integrator
 // gathers the pair force through the inverse permutation and keys its noise
 // exactly as a plain step of system s with seed (seed + s) would: Philox key
