@@ -25,6 +25,7 @@
 
 #include "marsb200.h"
 #include "mb2_internal.cuh"
+#include "mb2_walk.cuh"
 
 using namespace mb2;
 
@@ -94,16 +95,12 @@ __global__ void __launch_bounds__(256) batch_cell_ranges_kernel(const uint32_t* 
 // search over the running totals held one per lane. Hits are appended in
 // candidate order. Six resident blocks per SM (40 registers): 1 % faster per
 // build than 48 registers at five, and than 32 at eight.
-__global__ void __launch_bounds__(256, 6) batch_rows_kernel(
-	const float4* __restrict__ sorted_pos, const uint32_t* __restrict__ keys,
-	const uint32_t* __restrict__ s2o, const uint32_t* __restrict__ begin,
-	const uint32_t* __restrict__ end, const SysGrid* __restrict__ grids,
-	const Box* __restrict__ boxes, const uint4* __restrict__ stencil, uint32_t n,
-	uint32_t* __restrict__ nbr, uint32_t cap, int hshift, uint32_t* __restrict__ row_len,
-	unsigned long long* __restrict__ stats) {
-	const uint32_t i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-	if (i >= n) return;  // whole warp
-	const uint32_t lane = threadIdx.x & 31u;
+__device__ __forceinline__ uint32_t batch_row(
+	uint32_t i, uint32_t lane, const float4* __restrict__ sorted_pos,
+	const uint32_t* __restrict__ keys, const uint32_t* __restrict__ s2o,
+	const uint32_t* __restrict__ begin, const uint32_t* __restrict__ end,
+	const SysGrid* __restrict__ grids, const Box* __restrict__ boxes,
+	const uint4* __restrict__ stencil, uint32_t* __restrict__ nbr, uint32_t cap, int hshift) {
 	const uint32_t lt = (1u << lane) - 1u;
 	const uint32_t key = keys[i];
 	const uint32_t sys = key >> kSysShift;
@@ -187,10 +184,86 @@ __global__ void __launch_bounds__(256, 6) batch_rows_kernel(
 			len += static_cast<uint32_t>(__popc(hm));
 		}
 	}
+	return len;
+}
+
+// One warp per group of 32 consecutive sorted particles: a group whose
+// particles all belong to one system and sit in cells within emax of each
+// other walks as the plain group walk does (walk_coherent_group, over the
+// system's grid and box: candidate cells pruned by their real distance from
+// the group's coordinate range, candidates dropped 32 at a time by the group
+// test, each survivor loaded once for all 32 lanes and decided by the cheap
+// test, the exact test behind a warp vote). Any other group (at a system's
+// start or end, or across a Morton discontinuity) walks its rows one at a
+// time with the row walk. Same pair set; rows in candidate order.
+__global__ void __launch_bounds__(256, 7) batch_group_kernel(
+	const float4* __restrict__ sorted_pos, const uint32_t* __restrict__ keys,
+	const uint32_t* __restrict__ s2o, const uint32_t* __restrict__ begin,
+	const uint32_t* __restrict__ end, const SysGrid* __restrict__ grids,
+	const Box* __restrict__ boxes, const uint4* __restrict__ stencil, uint32_t n,
+	uint32_t* __restrict__ nbr, uint32_t cap, int hshift, uint32_t* __restrict__ row_len,
+	unsigned long long* __restrict__ stats) {
+	__shared__ uint32_t split_tab[1 << kLocalBits];
+	__shared__ uint4 cell_buf[8 * kCellBuf];  // per warp: kept cells (jlo, end, image code, offset)
+	__shared__ float4 cand_buf[8 * 32];       // per warp: candidates that pass the group test
+	for (int k = threadIdx.x; k < (1 << kLocalBits); k += blockDim.x) split_tab[k] = split_by3(k);
+	__syncthreads();
+	const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+	const uint32_t i_first = i & ~31u;
+	if (i_first >= n) return;  // whole warp past the end
+	const uint32_t lane = threadIdx.x & 31u;
+	const bool valid = i < n;
+	const uint32_t key = valid ? keys[i] : 0u;
+	const uint32_t sys = key >> kSysShift;
+	const uint32_t sys0 = __shfl_sync(0xFFFFFFFFu, sys, 0);
+	const bool one_system = __all_sync(0xFFFFFFFFu, !valid || sys == sys0);
+	const SysGrid* g = grids + sys0;
+	const WalkGrid& wg = g->wg;
+	const uint32_t c = (key & kLocalMask) >> wg.shift;
+	const int cx = static_cast<int>(compact_by3(c >> 2));
+	const int cy = static_cast<int>(compact_by3(c >> 1));
+	const int cz = static_cast<int>(compact_by3(c));
+	const int x0 = warp_min(valid ? cx : INT_MAX), x1 = warp_max(valid ? cx : INT_MIN);
+	const int y0 = warp_min(valid ? cy : INT_MAX), y1 = warp_max(valid ? cy : INT_MIN);
+	const int z0 = warp_min(valid ? cz : INT_MAX), z1 = warp_max(valid ? cz : INT_MIN);
+	const bool coherent = one_system && (x1 - x0) <= wg.emax && (y1 - y0) <= wg.emax &&
+						  (z1 - z0) <= wg.emax;
+	uint32_t len = 0;
+	if (coherent) {
+		const float4 pi = valid ? sorted_pos[i] : make_float4(0.f, 0.f, 0.f, 0.f);
+		const int a = valid ? static_cast<int>(s2o[i]) : 0;
+		const float gxlo = warp_minf(valid ? pi.x : INFINITY), gxhi = warp_maxf(valid ? pi.x : -INFINITY);
+		const float gylo = warp_minf(valid ? pi.y : INFINITY), gyhi = warp_maxf(valid ? pi.y : -INFINITY);
+		const float gzlo = warp_minf(valid ? pi.z : INFINITY), gzhi = warp_maxf(valid ? pi.z : -INFINITY);
+		const int h = 1 << hshift;
+		RowWriter row{nbr + (static_cast<size_t>(i >> hshift) * cap << hshift) + (i & (h - 1)), 0u,
+					  0u, cap, h};
+		const uint32_t c_first = __shfl_sync(0xFFFFFFFFu, c, 0);
+		walk_coherent_group<false, true>(sorted_pos, s2o, begin + g->cell_base, end + g->cell_base,
+										 split_tab, cell_buf,
+										 cand_buf, wg, boxes[sys0], Exclusions{}, i, i_first,
+										 valid, pi, a, 0, 0, -1, c_first, x0, x1, y0, y1, z0, z1,
+										 gxlo, gxhi, gylo, gyhi, gzlo, gzhi, row);
+		len = row.total();
+	} else {
+		const uint32_t last = min(i_first + 32u, n);
+		for (uint32_t r = i_first; r < last; ++r) {
+			const uint32_t l = batch_row(r, lane, sorted_pos, keys, s2o, begin, end, grids, boxes,
+										 stencil, nbr, cap, hshift);
+			if (r == i) len = l;
+		}
+	}
+	if (valid) row_len[i] = len;
+	unsigned long long tot = valid ? len : 0u;
+	int mx = valid ? static_cast<int>(min(len, 0x7FFFFFFFu)) : 0;
+#pragma unroll
+	for (int o = 16; o > 0; o >>= 1) {
+		tot += __shfl_xor_sync(0xFFFFFFFFu, tot, o);
+		mx = max(mx, __shfl_xor_sync(0xFFFFFFFFu, mx, o));
+	}
 	if (lane == 0) {
-		row_len[i] = len;
-		atomicAdd(stats, static_cast<unsigned long long>(len));
-		atomicMax(stats + 1, static_cast<unsigned long long>(len));
+		atomicAdd(stats, tot);
+		atomicMax(stats + 1, static_cast<unsigned long long>(mx));
 	}
 }
 
@@ -312,7 +385,10 @@ void choose_grids(mb2_batch* b, float rc) {
 		WalkGrid& wg = sg.wg;
 		wg.m = g.m;
 		wg.shift = 3 * (kLocalBits - g.m);
-		wg.emax = 3;
+		// Groups whose cells spread up to 5 apart walk together (coherent);
+		// the rest walk row by row: 5.27 ms per build against 5.33 at 3 and
+		// 5.75 at 7 (wider candidate boxes).
+		wg.emax = 5;
 		for (int a = 0; a < 3; ++a) {
 			wg.radius[a] = g.radius[a];
 			wg.wmin[a] = g.wmin[a];
@@ -322,6 +398,15 @@ void choose_grids(mb2_batch* b, float rc) {
 		wg.rc2 = rc * rc;
 		fast_test_band(bx, rc, &wg.fast_lo, &wg.fast_hi);
 		wg.split2 = INFINITY;
+		// Cell c of level m spans Morton coordinates [c, c + 1) * 2^(7 - m) of
+		// the 7-bit scale over the box, L / 2^m wide; the margin covers the
+		// rounding of that mapping, as on the plain path.
+		for (int a = 0; a < 3; ++a) {
+			wg.dom_lo[a] = bx.origin[a];
+			wg.cell_w[a] = static_cast<float>(static_cast<double>(bx.size[a]) / (1 << g.m));
+			wg.eps[a] = static_cast<float>(
+				1e-5 * (std::fabs(static_cast<double>(bx.origin[a])) + bx.size[a]) + 1e-6);
+		}
 		sg.cell_base = base;
 		sg.stencil_off = static_cast<uint32_t>(stencil.size());
 		sg.stencil_n = static_cast<uint32_t>(g.stencil.size());
@@ -378,7 +463,7 @@ void batch_build(mb2_batch* b, const float4* pos, const int* type_ids, float rc,
 		MB2_CUDA(cudaMemsetAsync(b->stats.ptr, 0, 2 * sizeof(unsigned long long), st));
 		if (n) {
 			const int hshift = __builtin_ctz(32 / b->lanes);
-			MB2_LAUNCH batch_rows_kernel<<<(n + 7) / 8, 256, 0, st>>>(
+			MB2_LAUNCH batch_group_kernel<<<(n + 255) / 256, 256, 0, st>>>(
 				b->sorted_pos.ptr, b->keys.ptr, b->s2o.ptr, b->cell_begin.ptr, b->cell_end.ptr,
 				b->grids.ptr, b->boxes.ptr, b->stencil.ptr, n, b->nbr.ptr, cap, hshift,
 				b->row_len.ptr, b->stats.ptr);
