@@ -556,14 +556,19 @@ MB2_API int mb2_batch_run(mb2_batch* b, float* pos4, float* force_energy4, const
 MB2_API int mb2_batch_set_tuning(mb2_batch* b, int level_offset, int lanes);
 MB2_API int mb2_batch_tuning(const mb2_batch* b, int* level_offset, int* lanes,
                      uint32_t* total_cells);
-/* Rebuild cadence: with period > 0, mb2_batch_step and mb2_batch_run rebuild
- * at every period-th step (skipped while no particle moved more than half the
- * skin, the rule of Patch.cpp:86-108) instead of at params->rebuild_period;
- * 0 (the default) uses the params'. mb2_batch_autotune sets it to its choice.
- * mb2_batch_rebuild_schedule reports the cadence in force and the number of
- * list builds so far. */
+/* Rebuild cadence: with period > 0, mb2_batch_step and mb2_batch_run check
+ * every system at every period-th step instead of at params->rebuild_period
+ * (0, the default, uses the params'), and rebuild the lists of the systems
+ * one of whose particles moved more than half the skin since that system's
+ * own last build, the rule of Patch.cpp:86-108 applied to each system as to a
+ * patch; the others keep their lists. mb2_batch_autotune sets the cadence to
+ * its choice. mb2_batch_rebuild_schedule reports the cadence in force and the
+ * number of list builds so far (steps that rebuilt any system);
+ * mb2_batch_system_rebuilds the number of system lists rebuilt, summed over
+ * those builds. */
 MB2_API int mb2_batch_set_rebuild_period(mb2_batch* b, uint32_t period);
 MB2_API int mb2_batch_rebuild_schedule(const mb2_batch* b, uint32_t* period, uint64_t* rebuilds);
+MB2_API int mb2_batch_system_rebuilds(const mb2_batch* b, uint64_t* count);
 /* Autotuner: times one pairlist build and `trial_steps` steps for each cell
  * level offset in {-1, 0, +1} and lanes per row in {4, 8, 16} on a copy of
  * the positions, and keeps the pair minimising build / rebuild_period + step.

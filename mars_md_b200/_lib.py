@@ -156,6 +156,7 @@ def load(path: str = LIB_PATH):
     L.mb2_batch_set_tuning.argtypes = [vp, i, i]
     L.mb2_batch_set_rebuild_period.argtypes = [vp, u32]
     L.mb2_batch_rebuild_schedule.argtypes = [vp, C.POINTER(C.c_uint32), C.POINTER(C.c_uint64)]
+    L.mb2_batch_system_rebuilds.argtypes = [vp, C.POINTER(C.c_uint64)]
     L.mb2_batch_tuning.argtypes = [vp, ip, ip, u32p]
     L.mb2_batch_autotune.argtypes = [vp, vp, vp, C.POINTER(StepParams), u32, vp,
                                      C.POINTER(BatchTuning)]

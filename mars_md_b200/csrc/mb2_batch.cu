@@ -51,14 +51,24 @@ __device__ __forceinline__ uint32_t morton7(float x, float o, float scale) {
 	return static_cast<uint32_t>(min(max(q, 0), (1 << kLocalBits) - 1));
 }
 
-__global__ void __launch_bounds__(256) batch_encode_kernel(const float4* __restrict__ pos,
-														   const uint32_t* __restrict__ sys_of,
-														   const Box* __restrict__ boxes,
-														   uint32_t n, uint32_t* __restrict__ keys,
-														   uint32_t* __restrict__ idx) {
+// Sort keys in original order. A system being rebuilt (flags null: every
+// system) gets the Morton keys of its current positions; any other keeps the
+// keys of its last build (old_sorted_keys through the last inverse
+// permutation), so that the stable sort puts its particles back in the same
+// sorted slots and its rows of the list stay valid.
+__global__ void __launch_bounds__(256) batch_encode_kernel(
+	const float4* __restrict__ pos, const uint32_t* __restrict__ sys_of,
+	const Box* __restrict__ boxes, uint32_t n, const uint32_t* __restrict__ flags,
+	const uint32_t* __restrict__ old_sorted_keys, const uint32_t* __restrict__ old_inv,
+	uint32_t* __restrict__ keys, uint32_t* __restrict__ idx) {
 	const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
 	if (i >= n) return;
 	const uint32_t s = sys_of[i];
+	idx[i] = i;
+	if (flags && !flags[s]) {
+		keys[i] = old_sorted_keys[old_inv[i]];
+		return;
+	}
 	const Box& b = boxes[s];
 	const float4 p = pos[i];
 	const float k = static_cast<float>(1 << kLocalBits);
@@ -66,7 +76,37 @@ __global__ void __launch_bounds__(256) batch_encode_kernel(const float4* __restr
 	const uint32_t y = morton7(p.y, b.origin[1], __fmul_rn(k, b.inv[1]));
 	const uint32_t z = morton7(p.z, b.origin[2], __fmul_rn(k, b.inv[2]));
 	keys[i] = (s << kSysShift) | split_by3(z) | (split_by3(y) << 1) | (split_by3(x) << 2);
-	idx[i] = i;
+}
+
+// Row statistics of the whole list: stats[0] += entries, stats[1] = the
+// longest row.
+__global__ void __launch_bounds__(256) batch_row_stats_kernel(const uint32_t* __restrict__ row_len,
+															  uint32_t n,
+															  unsigned long long* __restrict__ stats) {
+	const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+	unsigned long long tot = i < n ? row_len[i] : 0u;
+	unsigned long long mx = tot;
+#pragma unroll
+	for (int o = 16; o > 0; o >>= 1) {
+		tot += __shfl_xor_sync(0xFFFFFFFFu, tot, o);
+		mx = max(mx, __shfl_xor_sync(0xFFFFFFFFu, mx, o));
+	}
+	if ((threadIdx.x & 31) == 0 && tot) {
+		atomicAdd(stats, tot);
+		atomicMax(stats + 1, mx);
+	}
+}
+
+// The list-build snapshot of the rebuilt systems' positions (flags null:
+// every system), from which their displacements are measured.
+__global__ void __launch_bounds__(256) batch_snapshot_kernel(const float4* __restrict__ pos,
+															 const uint32_t* __restrict__ sys_of,
+															 const uint32_t* __restrict__ flags,
+															 uint32_t n, float4* __restrict__ ref) {
+	const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+	if (i >= n) return;
+	if (flags && !flags[sys_of[i]]) return;
+	ref[i] = pos[i];
 }
 
 __global__ void __launch_bounds__(256) batch_cell_ranges_kernel(const uint32_t* __restrict__ keys,
@@ -200,9 +240,9 @@ __global__ void __launch_bounds__(256, 7) batch_group_kernel(
 	const float4* __restrict__ sorted_pos, const uint32_t* __restrict__ keys,
 	const uint32_t* __restrict__ s2o, const uint32_t* __restrict__ begin,
 	const uint32_t* __restrict__ end, const SysGrid* __restrict__ grids,
-	const Box* __restrict__ boxes, const uint4* __restrict__ stencil, uint32_t n,
-	uint32_t* __restrict__ nbr, uint32_t cap, int hshift, uint32_t* __restrict__ row_len,
-	unsigned long long* __restrict__ stats) {
+	const Box* __restrict__ boxes, const uint4* __restrict__ stencil,
+	const uint32_t* __restrict__ flags, uint32_t n, uint32_t* __restrict__ nbr, uint32_t cap,
+	int hshift, uint32_t* __restrict__ row_len) {
 	__shared__ uint32_t split_tab[1 << kLocalBits];
 	__shared__ uint4 cell_buf[8 * kCellBuf];  // per warp: kept cells (jlo, end, image code, offset)
 	__shared__ float4 cand_buf[8 * 32];       // per warp: candidates that pass the group test
@@ -217,6 +257,10 @@ __global__ void __launch_bounds__(256, 7) batch_group_kernel(
 	const uint32_t sys = key >> kSysShift;
 	const uint32_t sys0 = __shfl_sync(0xFFFFFFFFu, sys, 0);
 	const bool one_system = __all_sync(0xFFFFFFFFu, !valid || sys == sys0);
+	// Only the rows of systems being rebuilt (flags null: all) are walked;
+	// the others keep their rows.
+	const bool walked = valid && (!flags || flags[sys]);
+	if (!__any_sync(0xFFFFFFFFu, walked)) return;
 	const SysGrid* g = grids + sys0;
 	const WalkGrid& wg = g->wg;
 	const uint32_t c = (key & kLocalMask) >> wg.shift;
@@ -246,42 +290,45 @@ __global__ void __launch_bounds__(256, 7) batch_group_kernel(
 										 gxlo, gxhi, gylo, gyhi, gzlo, gzhi, row);
 		len = row.total();
 	} else {
-		const uint32_t last = min(i_first + 32u, n);
-		for (uint32_t r = i_first; r < last; ++r) {
-			const uint32_t l = batch_row(r, lane, sorted_pos, keys, s2o, begin, end, grids, boxes,
-										 stencil, nbr, cap, hshift);
-			if (r == i) len = l;
+		uint32_t todo = __ballot_sync(0xFFFFFFFFu, walked);
+		while (todo) {
+			const int l = __ffs(todo) - 1;
+			todo &= todo - 1u;
+			const uint32_t len_l = batch_row(i_first + static_cast<uint32_t>(l), lane, sorted_pos,
+											 keys, s2o, begin, end, grids, boxes, stencil, nbr,
+											 cap, hshift);
+			if (static_cast<int>(lane) == l) len = len_l;
 		}
 	}
-	if (valid) row_len[i] = len;
-	unsigned long long tot = valid ? len : 0u;
-	int mx = valid ? static_cast<int>(min(len, 0x7FFFFFFFu)) : 0;
-#pragma unroll
-	for (int o = 16; o > 0; o >>= 1) {
-		tot += __shfl_xor_sync(0xFFFFFFFFu, tot, o);
-		mx = max(mx, __shfl_xor_sync(0xFFFFFFFFu, mx, o));
-	}
-	if (lane == 0) {
-		atomicAdd(stats, tot);
-		atomicMax(stats + 1, static_cast<unsigned long long>(mx));
-	}
+	if (walked) row_len[i] = len;
 }
 
+// Largest squared displacement of each system's particles since their
+// list-build snapshot, into out[system] (float bits; non-negative floats
+// order like their bit patterns).
 __global__ void __launch_bounds__(256) batch_displacement_kernel(
 	const float4* __restrict__ cur, const float4* __restrict__ prev,
 	const uint32_t* __restrict__ sys_of, const Box* __restrict__ boxes, uint32_t n,
 	unsigned int* __restrict__ out) {
 	const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+	const uint32_t i_first = i & ~31u;
+	if (i_first >= n) return;  // whole warp past the end
 	float d2 = 0.0f;
+	const uint32_t s = sys_of[i < n ? i : i_first];
 	if (i < n) {
-		const Box& b = boxes[sys_of[i]];
+		const Box& b = boxes[s];
 		const float4 c = cur[i], p = prev[i];
 		const float3 d = wrap_diff(b, __fsub_rn(c.x, p.x), __fsub_rn(c.y, p.y), __fsub_rn(c.z, p.z));
 		d2 = len2(d.x, d.y, d.z);
 	}
+	const uint32_t s0 = __shfl_sync(0xFFFFFFFFu, s, 0);
+	if (__all_sync(0xFFFFFFFFu, s == s0)) {
 #pragma unroll
-	for (int o = 16; o > 0; o >>= 1) d2 = fmaxf(d2, __shfl_xor_sync(0xFFFFFFFFu, d2, o));
-	if ((threadIdx.x & 31) == 0) atomicMax(out, __float_as_uint(d2));
+		for (int o = 16; o > 0; o >>= 1) d2 = fmaxf(d2, __shfl_xor_sync(0xFFFFFFFFu, d2, o));
+		if ((threadIdx.x & 31) == 0) atomicMax(&out[s0], __float_as_uint(d2));
+	} else if (i < n) {
+		atomicMax(&out[s], __float_as_uint(d2));
+	}
 }
 
 }  // namespace
@@ -298,6 +345,7 @@ struct mb2_batch {
 	Scratch scratch;
 	// sort / list state
 	DevBuf<uint32_t> keys, s2o, inv, row_len, row_off, nbr, cell_begin, cell_end;
+	DevBuf<uint32_t> keys_in, sys_flags;  // original-order sort keys; systems to rebuild
 	DevBuf<float4> sorted_pos, ref_pos, force_sorted;
 	DevBuf<SysGrid> grids;
 	std::vector<SysGrid> grids_h;
@@ -308,11 +356,13 @@ struct mb2_batch {
 	// Rebuild cadence in force (0: the params' rebuild_period), set by
 	// mb2_batch_set_rebuild_period or chosen by mb2_batch_autotune.
 	uint32_t rebuild_period = 0;
-	unsigned long long rebuilds = 0;  // list builds since creation
+	unsigned long long rebuilds = 0;         // list builds since creation (steps with any)
+	unsigned long long system_rebuilds = 0;  // systems rebuilt, summed over those builds
 	DevBuf<unsigned long long> stats, step_d;
 	DevBuf<unsigned int> disp;
 	DevBuf<double> energy;
 	unsigned long long* pinned = nullptr;
+	unsigned int* pinned_sys = nullptr;  // per system: displacement readback, then rebuild flags
 	bool built = false;
 	uint64_t num_pairs = 0;
 	uint32_t cap = 0;
@@ -338,6 +388,7 @@ struct mb2_batch {
 	~mb2_batch() {
 		if (graph) cudaGraphExecDestroy(graph);
 		if (pinned) cudaFreeHost(pinned);
+		if (pinned_sys) cudaFreeHost(pinned_sys);
 	}
 };
 
@@ -431,7 +482,14 @@ void choose_grids(mb2_batch* b, float rc) {
 	b->grid_rc = rc;
 }
 
-void batch_build(mb2_batch* b, const float4* pos, const int* type_ids, float rc, cudaStream_t st) {
+// The list build. flags_h (pinned, one word per system; null: every system)
+// names the systems to rebuild: the others keep their sort keys, sorted slots,
+// rows and displacement snapshot from their own last build, as each system's
+// list would if it ran alone (a patch of the reference rebuilds on its own
+// skin check). A change of grid, or a row longer than the list's row
+// capacity, rebuilds every system.
+void batch_build(mb2_batch* b, const float4* pos, const int* type_ids, float rc, cudaStream_t st,
+				 const unsigned int* flags_h = nullptr) {
 	expect_arg(rc > 0.0f && std::isfinite(rc), MB2_ERR_ARG,
 			   "mb2_batch_build: pairlist cutoff must be positive and finite");
 	for (uint32_t s = 0; s < b->num_systems; ++s)
@@ -439,14 +497,34 @@ void batch_build(mb2_batch* b, const float4* pos, const int* type_ids, float rc,
 			expect_arg(2.0f * rc < b->boxes_h[s].size[a], MB2_ERR_ARG,
 					   "mb2_batch_build: every box edge must exceed twice the list radius");
 	const uint32_t n = b->n;
-	if (b->grid_rc != rc) choose_grids(b, rc);
+	if (b->grid_rc != rc) {
+		choose_grids(b, rc);
+		flags_h = nullptr;
+	}
+	if (!(b->built && b->cap && b->lanes)) flags_h = nullptr;
+	const uint32_t* dflags = nullptr;
+	uint64_t rebuilt = b->num_systems;
+	if (flags_h) {
+		rebuilt = 0;
+		for (uint32_t s = 0; s < b->num_systems; ++s) rebuilt += flags_h[s] ? 1u : 0u;
+		b->sys_flags.ensure(b->num_systems);
+		MB2_CUDA(cudaMemcpyAsync(b->sys_flags.ptr, flags_h, b->num_systems * sizeof(unsigned int),
+								 cudaMemcpyHostToDevice, st));
+		dflags = b->sys_flags.ptr;
+	}
 	b->keys.ensure(n);
+	b->keys_in.ensure(n);
 	b->s2o.ensure(n);
 	b->inv.ensure(n);
 	b->sorted_pos.ensure(n);
 	if (n)
 		MB2_LAUNCH batch_encode_kernel<<<(n + 255) / 256, 256, 0, st>>>(
-			pos, b->sys_of.ptr, b->boxes.ptr, n, b->keys.ptr, b->s2o.ptr);
+			pos, b->sys_of.ptr, b->boxes.ptr, n, dflags, b->keys.ptr, b->inv.ptr, b->keys_in.ptr,
+			b->s2o.ptr);
+	// (copied, not swapped: the captured step reads the sorted keys at a fixed address)
+	if (n)
+		MB2_CUDA(cudaMemcpyAsync(b->keys.ptr, b->keys_in.ptr, static_cast<size_t>(n) * sizeof(uint32_t),
+								 cudaMemcpyDeviceToDevice, st));
 	radix_sort_pairs(b->scratch, b->keys.ptr, b->s2o.ptr, n, st);
 	inverse_and_gather(b->s2o.ptr, n, pos, b->inv.ptr, nullptr, st);
 	pack_sorted_positions(pos, type_ids, b->s2o.ptr, n, b->sorted_pos.ptr, st);
@@ -459,14 +537,16 @@ void batch_build(mb2_batch* b, const float4* pos, const int* type_ids, float rc,
 			b->keys.ptr, n, b->grids.ptr, b->cell_begin.ptr, b->cell_end.ptr);
 	b->row_len.ensure(n);
 	b->stats.ensure(2);
-	auto walk = [&](uint32_t cap) {
+	auto walk = [&](uint32_t cap, const uint32_t* fl) {
 		MB2_CUDA(cudaMemsetAsync(b->stats.ptr, 0, 2 * sizeof(unsigned long long), st));
 		if (n) {
 			const int hshift = __builtin_ctz(32 / b->lanes);
 			MB2_LAUNCH batch_group_kernel<<<(n + 255) / 256, 256, 0, st>>>(
 				b->sorted_pos.ptr, b->keys.ptr, b->s2o.ptr, b->cell_begin.ptr, b->cell_end.ptr,
-				b->grids.ptr, b->boxes.ptr, b->stencil.ptr, n, b->nbr.ptr, cap, hshift,
-				b->row_len.ptr, b->stats.ptr);
+				b->grids.ptr, b->boxes.ptr, b->stencil.ptr, fl, n, b->nbr.ptr, cap, hshift,
+				b->row_len.ptr);
+			MB2_LAUNCH batch_row_stats_kernel<<<(n + 255) / 256, 256, 0, st>>>(b->row_len.ptr, n,
+																			   b->stats.ptr);
 		}
 		MB2_CUDA(cudaMemcpyAsync(b->pinned, b->stats.ptr, 2 * sizeof(unsigned long long),
 								 cudaMemcpyDeviceToHost, st));
@@ -488,40 +568,58 @@ void batch_build(mb2_batch* b, const float4* pos, const int* type_ids, float rc,
 	if (b->cap == 0 || b->lanes == 0) {
 		// First build: count rows without storing (cap 0 writes nothing), to size the list.
 		b->lanes = 4;
-		const auto counted = walk(0u);
+		const auto counted = walk(0u, nullptr);
 		const double mean = n ? static_cast<double>(counted.first) / n : 0.0;
 		b->lanes = b->lanes_request ? b->lanes_request
 									: (mean >= 256.0 ? 16 : (mean >= 48.0 ? 8 : 4));
 		size_list(counted.second);
 	}
 	ensure_list();
-	auto stats = walk(b->cap);
+	auto stats = walk(b->cap, dflags);
 	if (stats.second > b->cap) {
+		// A longer row than the capacity: a new row stride, so every system's
+		// rows are walked again.
 		size_list(stats.second);
 		ensure_list();
-		stats = walk(b->cap);
+		if (dflags) {
+			batch_build(b, pos, type_ids, rc, st, nullptr);
+			return;
+		}
+		stats = walk(b->cap, nullptr);
 	}
 	b->ref_pos.ensure(n);
 	if (n)
-		MB2_CUDA(cudaMemcpyAsync(b->ref_pos.ptr, pos, static_cast<size_t>(n) * sizeof(float4),
-								 cudaMemcpyDeviceToDevice, st));
+		MB2_LAUNCH batch_snapshot_kernel<<<(n + 255) / 256, 256, 0, st>>>(pos, b->sys_of.ptr, dflags,
+																		  n, b->ref_pos.ptr);
 	b->num_pairs = stats.first;
 	b->built = true;
+	b->system_rebuilds += rebuilt;
+}
+
+// Each system's largest displacement since its own last build, squared, into
+// b->pinned_sys (float bits); synchronises. Returns the largest displacement.
+float batch_sys_disp(mb2_batch* b, const float4* pos, cudaStream_t st) {
+	const uint32_t S = b->num_systems;
+	b->disp.ensure(S);
+	MB2_CUDA(cudaMemsetAsync(b->disp.ptr, 0, S * sizeof(unsigned int), st));
+	if (b->n)
+		MB2_LAUNCH batch_displacement_kernel<<<(b->n + 255) / 256, 256, 0, st>>>(
+			pos, b->ref_pos.ptr, b->sys_of.ptr, b->boxes.ptr, b->n, b->disp.ptr);
+	MB2_CUDA(cudaMemcpyAsync(b->pinned_sys, b->disp.ptr, S * sizeof(unsigned int),
+							 cudaMemcpyDeviceToHost, st));
+	MB2_CUDA(cudaStreamSynchronize(st));
+	float worst = 0.0f;
+	for (uint32_t s = 0; s < S; ++s) {
+		float d2;
+		std::memcpy(&d2, &b->pinned_sys[s], 4);
+		worst = std::max(worst, d2);
+	}
+	return std::sqrt(worst);
 }
 
 // Largest displacement (over all systems) since the last build; synchronises.
 float batch_max_disp(mb2_batch* b, const float4* pos, cudaStream_t st) {
-	b->disp.ensure(1);
-	MB2_CUDA(cudaMemsetAsync(b->disp.ptr, 0, sizeof(unsigned int), st));
-	if (b->n)
-		MB2_LAUNCH batch_displacement_kernel<<<(b->n + 255) / 256, 256, 0, st>>>(
-			pos, b->ref_pos.ptr, b->sys_of.ptr, b->boxes.ptr, b->n, b->disp.ptr);
-	MB2_CUDA(cudaMemcpyAsync(b->pinned, b->disp.ptr, sizeof(unsigned int), cudaMemcpyDeviceToHost,
-							 st));
-	MB2_CUDA(cudaStreamSynchronize(st));
-	float d2;
-	std::memcpy(&d2, b->pinned, 4);
-	return std::sqrt(d2);
+	return batch_sys_disp(b, pos, st);
 }
 
 // The per-step work after any rebuild: pack, clear, pair forces, integrate,
@@ -554,21 +652,35 @@ void check_step_args(mb2_batch* b, const float* pos4, const float* fe4, const in
 			   MB2_ERR_ARG, "mb2_batch_step: BD without bonded terms in batched mode");
 }
 
-// The rebuild schedule of Patch.cpp:86-108 over all systems (a rebuild at the
-// first step and at every period step, skipped while no particle of any
-// system moved more than half the skin) at the cadence in force: the batch's
-// own (the autotuner's choice) when set, else the params'.
+// The rebuild schedule of Patch.cpp:86-108 for each system, as each would
+// run alone: a rebuild at the first step and at every period step, skipped
+// for a system none of whose particles moved more than half the skin since
+// its own last build. The period is the cadence in force: the batch's own
+// (the autotuner's choice) when set, else the params'. The systems due are
+// rebuilt together in one build.
 void maybe_rebuild(mb2_batch* b, const float4* pos, const int* type_ids, uint64_t step,
 				   const mb2_step_params* prm, cudaStream_t st) {
 	const uint32_t period = b->rebuild_period ? b->rebuild_period : prm->rebuild_period;
 	const bool at_period = period == 0 || (step - 1) % period == 0;
-	bool rebuild = at_period || !b->built;
 	const float skin = prm->pairlist_cutoff - prm->cutoff;
-	if (rebuild && b->built && period != 0 && skin > 0.0f)
-		rebuild = batch_max_disp(b, pos, st) > skin * 0.5f;
-	if (rebuild) {
+	if (!b->built || (at_period && (period == 0 || skin <= 0.0f))) {
 		batch_build(b, pos, type_ids, prm->pairlist_cutoff, st);
 		++b->rebuilds;
+	} else if (at_period) {
+		batch_sys_disp(b, pos, st);
+		uint32_t due = 0;
+		for (uint32_t s = 0; s < b->num_systems; ++s) {
+			float d2;
+			std::memcpy(&d2, &b->pinned_sys[s], 4);
+			const bool r = std::sqrt(d2) > skin * 0.5f;
+			b->pinned_sys[s] = r ? 1u : 0u;
+			due += r ? 1u : 0u;
+		}
+		if (due) {
+			batch_build(b, pos, type_ids, prm->pairlist_cutoff, st,
+						due == b->num_systems ? nullptr : b->pinned_sys);
+			++b->rebuilds;
+		}
 	}
 	b->force_sorted.ensure(b->n);
 }
@@ -630,6 +742,7 @@ int mb2_batch_create(int device, uint32_t num_systems, const uint32_t* counts,
 		if (b->n)
 			MB2_CUDA(cudaMemcpy(b->sys_of.ptr, sys_of.data(), b->n * 4ull, cudaMemcpyHostToDevice));
 		MB2_CUDA(cudaMallocHost(&b->pinned, 64));
+		MB2_CUDA(cudaMallocHost(&b->pinned_sys, num_systems * sizeof(unsigned int)));
 		b->step_d.ensure(1);
 		b->energy.ensure(4);
 		MB2_CUDA(cudaMemset(b->energy.ptr, 0, 4 * sizeof(double)));
@@ -832,6 +945,12 @@ int mb2_batch_run(mb2_batch* b, float* pos4, float* force_energy4, const int* ty
 
 int mb2_batch_set_rebuild_period(mb2_batch* b, uint32_t period) {
 	return bguard(b, [&] { b->rebuild_period = period; });
+}
+
+int mb2_batch_system_rebuilds(const mb2_batch* b, uint64_t* count) {
+	if (!b || !count) return MB2_ERR_ARG;
+	*count = b->system_rebuilds;
+	return MB2_OK;
 }
 
 int mb2_batch_rebuild_schedule(const mb2_batch* b, uint32_t* period, uint64_t* rebuilds) {

@@ -801,6 +801,13 @@ class Batch:
         self.check(self.lib.mb2_batch_rebuild_schedule(self.h, C.byref(p), C.byref(r)))
         return int(p.value), int(r.value)
 
+    def system_rebuilds(self) -> int:
+        """System lists rebuilt so far, summed over the list builds (each
+        build rebuilds only the systems whose own skin check failed)."""
+        c = C.c_uint64()
+        self.check(self.lib.mb2_batch_system_rebuilds(self.h, C.byref(c)))
+        return int(c.value)
+
 
 def setup_batch(ws, device="cuda:0"):
     """A Batch over workloads that share tables and types (e.g. workloads.batched());

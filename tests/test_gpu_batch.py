@@ -185,6 +185,49 @@ def test_batch_autotuned_cadence_in_force_and_list_stays_exact(oracle):
         b.close()
 
 
+def test_batch_rebuilds_only_the_systems_whose_skin_failed(oracle):
+    """Each system is checked as a patch of its own: from a list built on the
+    current positions, every other particle of system 0 is moved 3 A (beyond
+    half the 5 A skin) and of system 1 by 0.8 A; the next step's check
+    rebuilds system 0 alone. System
+    0's rows then hold the pair set of the positions it was rebuilt from;
+    system 1 keeps the set of the earlier build, which its current positions
+    no longer give."""
+    ws = _systems(k=4)
+    b, dev = setup_batch(ws)
+    try:
+        prm = step_params(ws[0], seed=SEED)
+        prm.rebuild_period = 1
+        b.step(dev["pos"], dev["fe"], dev["type"], 1, prm)
+        b.build(dev["pos"], dev["type"], ws[0].list_radius)
+        torch.cuda.synchronize()
+        built_at = dev["pos"].cpu().numpy().copy()
+        builds, systems = b.rebuild_schedule()[1], b.system_rebuilds()
+        pos = dev["pos"]
+        for s, shift in ((0, 3.0), (1, 0.8)):  # every other particle, so pairs change
+            lo, hi = b.offsets[s], b.offsets[s + 1]
+            L = float(ws[s].box_size[0])
+            pos[lo:hi:2, 0] = torch.remainder(pos[lo:hi:2, 0] + shift, L)
+        at_rebuild = pos.cpu().numpy().copy()
+        b.step(dev["pos"], dev["fe"], dev["type"], 2, prm)
+        torch.cuda.synchronize()
+        assert b.rebuild_schedule()[1] == builds + 1
+        assert b.system_rebuilds() == systems + 1
+        per = _split_pairs(b.export_pairs().cpu().numpy().astype(np.int64), b.offsets)
+        for s, w in enumerate(ws):
+            src = at_rebuild if s == 0 else built_at
+            ref, _, _ = oracle.build_pairlist(src[b.offsets[s]:b.offsets[s + 1]], box_of(w),
+                                              w.list_radius)
+            assert np.array_equal(_canon(per[s]), ref.astype(np.int64)), f"system {s}"
+        p1 = at_rebuild[b.offsets[1]:b.offsets[2]]
+        now1, _, _ = oracle.build_pairlist(p1, box_of(ws[1]), ws[1].list_radius)
+        ref1, _, _ = oracle.build_pairlist(built_at[b.offsets[1]:b.offsets[2]], box_of(ws[1]),
+                                           ws[1].list_radius)
+        assert not np.array_equal(now1, ref1)  # the kept list is the earlier one
+    finally:
+        b.close()
+
+
 def test_batch_rejects_boxes_smaller_than_twice_the_list_radius():
     w = W.plain_bd(seed=1, n=600, box=40.0)
     b, dev = setup_batch([w])
