@@ -79,21 +79,38 @@ __global__ void __launch_bounds__(256) batch_encode_kernel(
 }
 
 // Row statistics of the whole list: stats[0] += entries, stats[1] = the
-// longest row.
+// longest row. A grid-stride loop reduced per block, one pair of atomics per
+// block (per-warp atomics on the two words serialised to ~0.1 ms).
 __global__ void __launch_bounds__(256) batch_row_stats_kernel(const uint32_t* __restrict__ row_len,
 															  uint32_t n,
 															  unsigned long long* __restrict__ stats) {
-	const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-	unsigned long long tot = i < n ? row_len[i] : 0u;
-	unsigned long long mx = tot;
+	__shared__ unsigned long long part[2][8];
+	unsigned long long tot = 0, mx = 0;
+	for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+		const unsigned long long v = row_len[i];
+		tot += v;
+		mx = max(mx, v);
+	}
 #pragma unroll
 	for (int o = 16; o > 0; o >>= 1) {
 		tot += __shfl_xor_sync(0xFFFFFFFFu, tot, o);
 		mx = max(mx, __shfl_xor_sync(0xFFFFFFFFu, mx, o));
 	}
-	if ((threadIdx.x & 31) == 0 && tot) {
-		atomicAdd(stats, tot);
-		atomicMax(stats + 1, mx);
+	const int w = threadIdx.x >> 5;
+	if ((threadIdx.x & 31) == 0) {
+		part[0][w] = tot;
+		part[1][w] = mx;
+	}
+	__syncthreads();
+	if (threadIdx.x == 0) {
+		for (int k = 1; k < static_cast<int>(blockDim.x >> 5); ++k) {
+			tot += part[0][k];
+			mx = max(mx, part[1][k]);
+		}
+		if (tot) {
+			atomicAdd(stats, tot);
+			atomicMax(stats + 1, mx);
+		}
 	}
 }
 
@@ -312,22 +329,47 @@ __global__ void __launch_bounds__(256) batch_displacement_kernel(
 	unsigned int* __restrict__ out) {
 	const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
 	const uint32_t i_first = i & ~31u;
-	if (i_first >= n) return;  // whole warp past the end
 	float d2 = 0.0f;
-	const uint32_t s = sys_of[i < n ? i : i_first];
+	const uint32_t s = i_first < n ? sys_of[i < n ? i : i_first] : 0u;
 	if (i < n) {
 		const Box& b = boxes[s];
 		const float4 c = cur[i], p = prev[i];
 		const float3 d = wrap_diff(b, __fsub_rn(c.x, p.x), __fsub_rn(c.y, p.y), __fsub_rn(c.z, p.z));
 		d2 = len2(d.x, d.y, d.z);
 	}
+	// A warp of one system reduces first; the block's warps then merge runs
+	// of one system, so that a system takes about one atomic per block.
+	__shared__ uint32_t wsys[8];
+	__shared__ float wmax[8];
 	const uint32_t s0 = __shfl_sync(0xFFFFFFFFu, s, 0);
+	const int w = threadIdx.x >> 5;
 	if (__all_sync(0xFFFFFFFFu, s == s0)) {
 #pragma unroll
 		for (int o = 16; o > 0; o >>= 1) d2 = fmaxf(d2, __shfl_xor_sync(0xFFFFFFFFu, d2, o));
-		if ((threadIdx.x & 31) == 0) atomicMax(&out[s0], __float_as_uint(d2));
-	} else if (i < n) {
-		atomicMax(&out[s], __float_as_uint(d2));
+		if ((threadIdx.x & 31) == 0) {
+			wsys[w] = s0;
+			wmax[w] = d2;
+		}
+	} else {
+		if (i < n) atomicMax(&out[s], __float_as_uint(d2));
+		if ((threadIdx.x & 31) == 0) wsys[w] = 0xFFFFFFFFu;  // already applied
+	}
+	__syncthreads();
+	if (threadIdx.x == 0) {
+		const int warps = static_cast<int>(blockDim.x >> 5);
+		uint32_t run = 0xFFFFFFFFu;  // system of the current run of warps
+		float m = 0.0f;
+		for (int k = 0; k < warps; ++k) {
+			// Warps past the end of the particles hold nothing.
+			if (blockIdx.x * blockDim.x + static_cast<uint32_t>(k) * 32u >= n) break;
+			if (wsys[k] != run) {
+				if (run != 0xFFFFFFFFu) atomicMax(&out[run], __float_as_uint(m));
+				run = wsys[k];
+				m = 0.0f;
+			}
+			if (run != 0xFFFFFFFFu) m = fmaxf(m, wmax[k]);
+		}
+		if (run != 0xFFFFFFFFu) atomicMax(&out[run], __float_as_uint(m));
 	}
 }
 
@@ -545,8 +587,8 @@ void batch_build(mb2_batch* b, const float4* pos, const int* type_ids, float rc,
 				b->sorted_pos.ptr, b->keys.ptr, b->s2o.ptr, b->cell_begin.ptr, b->cell_end.ptr,
 				b->grids.ptr, b->boxes.ptr, b->stencil.ptr, fl, n, b->nbr.ptr, cap, hshift,
 				b->row_len.ptr);
-			MB2_LAUNCH batch_row_stats_kernel<<<(n + 255) / 256, 256, 0, st>>>(b->row_len.ptr, n,
-																			   b->stats.ptr);
+			MB2_LAUNCH batch_row_stats_kernel<<<std::min<uint32_t>((n + 255) / 256, 1184), 256, 0,
+												 st>>>(b->row_len.ptr, n, b->stats.ptr);
 		}
 		MB2_CUDA(cudaMemcpyAsync(b->pinned, b->stats.ptr, 2 * sizeof(unsigned long long),
 								 cudaMemcpyDeviceToHost, st));
