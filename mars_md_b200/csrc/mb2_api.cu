@@ -519,14 +519,12 @@ void rebuild_pair_terms(mb2_context* ctx) {
 // Patch.cpp:180-234): bonds, angles, dihedrals, restraints.
 void bonded_stage(mb2_context* ctx, const float4* pos, float4* fe, const mb2_step_params* prm,
 				  int get_energy, cudaStream_t st) {
-	if (prm->num_bonds)
-		bond_forces(reinterpret_cast<const int2*>(prm->bonds2), prm->bond_table_idx,
-					prm->num_bonds, pos, fe, ctx->bonded_tables[0].ptr, ctx->box, get_energy,
-					ctx->energy.ptr + 2, st);
-	if (prm->num_angles)
-		angle_forces(reinterpret_cast<const int4*>(prm->angles4), prm->angle_table_idx,
-					 prm->num_angles, pos, fe, ctx->bonded_tables[1].ptr, ctx->box, get_energy,
-					 ctx->energy.ptr + 3, st);
+	if (prm->num_bonds || prm->num_angles)
+		bond_angle_forces(reinterpret_cast<const int2*>(prm->bonds2), prm->bond_table_idx,
+						  prm->num_bonds, ctx->bonded_tables[0].ptr,
+						  reinterpret_cast<const int4*>(prm->angles4), prm->angle_table_idx,
+						  prm->num_angles, ctx->bonded_tables[1].ptr, pos, fe, ctx->box, get_energy,
+						  ctx->energy.ptr + 2, ctx->energy.ptr + 3, st);
 	if (prm->num_dihedrals)
 		dihedral_forces(reinterpret_cast<const int4*>(prm->dihedrals4), prm->dihedral_table_idx,
 						prm->num_dihedrals, pos, fe, ctx->bonded_tables[2].ptr, ctx->box,
@@ -550,13 +548,12 @@ void window_step(mb2_context* ctx, float4* pos, float4* fe, const int* type_ids,
 	if (bonded) MB2_CUDA(cudaMemsetAsync(fe, 0, static_cast<size_t>(n) * sizeof(float4), st));
 	pack_sorted_positions(pos, type_ids, ctx->s2o.ptr, n, ctx->sorted_pos.ptr, st);
 	pair_kernel(ctx, n, prm->cutoff, 0, st);
-	if (prm->num_bonds)
-		bond_forces(reinterpret_cast<const int2*>(prm->bonds2), prm->bond_table_idx, prm->num_bonds,
-					pos, fe, ctx->bonded_tables[0].ptr, ctx->box, 0, ctx->energy.ptr + 2, st);
-	if (prm->num_angles)
-		angle_forces(reinterpret_cast<const int4*>(prm->angles4), prm->angle_table_idx,
-					 prm->num_angles, pos, fe, ctx->bonded_tables[1].ptr, ctx->box, 0,
-					 ctx->energy.ptr + 3, st);
+	if (bonded)
+		bond_angle_forces(reinterpret_cast<const int2*>(prm->bonds2), prm->bond_table_idx,
+						  prm->num_bonds, ctx->bonded_tables[0].ptr,
+						  reinterpret_cast<const int4*>(prm->angles4), prm->angle_table_idx,
+						  prm->num_angles, ctx->bonded_tables[1].ptr, pos, fe, ctx->box, 0,
+						  ctx->energy.ptr + 2, ctx->energy.ptr + 3, st);
 	BdParams p{prm->dt, prm->kT, static_cast<uint32_t>(step),
 			   mb2_bd_seed(prm->seed, prm->patch_id, step), 0u,
 			   {prm->efield[0], prm->efield[1], prm->efield[2]}};

@@ -444,12 +444,11 @@ __device__ __forceinline__ float calc_distance(const Box& box, const float4& fro
 // TabulatedBondComputer::operator() (src/Interactions/Bonded/BondComputer.h:168-191).
 // A row with table_idx < 0 has a form other than tabulated and is skipped, as
 // the reference's forms[] check skips it.
-__global__ void __launch_bounds__(256) bond_kernel(const int2* __restrict__ bonds,
-												   const int* __restrict__ table_idx, uint32_t nb,
-												   const float4* __restrict__ pos, float4* fe,
-												   const Table* __restrict__ tables, Box box,
-												   int get_energy, double* energy) {
-	const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+__device__ __forceinline__ double bond_term(uint32_t k, const int2* __restrict__ bonds,
+											const int* __restrict__ table_idx, uint32_t nb,
+											const float4* __restrict__ pos, float4* fe,
+											const Table* __restrict__ tables, const Box& box,
+											int get_energy) {
 	double e_acc = 0.0;
 	if (k < nb && table_idx[k] >= 0) {
 		const int2 b = bonds[k];
@@ -467,18 +466,27 @@ __global__ void __launch_bounds__(256) bond_kernel(const int2* __restrict__ bond
 			e_acc = get_energy ? static_cast<double>(fm_e.y) : 0.0;
 		}
 	}
+	return e_acc;
+}
+
+__global__ void __launch_bounds__(256) bond_kernel(const int2* __restrict__ bonds,
+												   const int* __restrict__ table_idx, uint32_t nb,
+												   const float4* __restrict__ pos, float4* fe,
+												   const Table* __restrict__ tables, Box box,
+												   int get_energy, double* energy) {
+	const double e_acc = bond_term(blockIdx.x * blockDim.x + threadIdx.x, bonds, table_idx, nb,
+								   pos, fe, tables, box, get_energy);
 	if (get_energy) block_add_f64(e_acc, 0.0, energy);
 }
 
 // TabulatedAngleComputer::operator() (BondComputer.h:236-268) with
 // AngleGeometry::compute (src/Interactions/Bonded/BondGeometry.h:19-44).
 // Angle tables wrap (src/Interactions/DeviceBondedInteraction.h:234).
-__global__ void __launch_bounds__(256) angle_kernel(const int4* __restrict__ angles,
-													const int* __restrict__ table_idx, uint32_t na,
-													const float4* __restrict__ pos, float4* fe,
-													const Table* __restrict__ tables, Box box,
-													int get_energy, double* energy) {
-	const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+__device__ __forceinline__ double angle_term(uint32_t k, const int4* __restrict__ angles,
+											 const int* __restrict__ table_idx, uint32_t na,
+											 const float4* __restrict__ pos, float4* fe,
+											 const Table* __restrict__ tables, const Box& box,
+											 int get_energy) {
 	double e_acc = 0.0;
 	if (k < na && table_idx[k] >= 0) {
 		const int4 a = angles[k];
@@ -521,7 +529,38 @@ __global__ void __launch_bounds__(256) angle_kernel(const int4* __restrict__ ang
 		red_add_v4(&fe[a.z], f3x, f3y, f3z, third);
 		e_acc = get_energy ? static_cast<double>(fm_e.y) : 0.0;
 	}
+	return e_acc;
+}
+
+__global__ void __launch_bounds__(256) angle_kernel(const int4* __restrict__ angles,
+													const int* __restrict__ table_idx, uint32_t na,
+													const float4* __restrict__ pos, float4* fe,
+													const Table* __restrict__ tables, Box box,
+													int get_energy, double* energy) {
+	const double e_acc = angle_term(blockIdx.x * blockDim.x + threadIdx.x, angles, table_idx, na,
+									pos, fe, tables, box, get_energy);
 	if (get_energy) block_add_f64(e_acc, 0.0, energy);
+}
+
+// Bonds and angles in one launch: the first ceil(nb / 256) blocks take the
+// bonds, the rest the angles (one launch fewer per step; the two kernels'
+// arithmetic unchanged).
+__global__ void __launch_bounds__(256) bond_angle_kernel(
+	const int2* __restrict__ bonds, const int* __restrict__ bond_idx, uint32_t nb,
+	const Table* __restrict__ bond_tables, const int4* __restrict__ angles,
+	const int* __restrict__ angle_idx, uint32_t na, const Table* __restrict__ angle_tables,
+	const float4* __restrict__ pos, float4* fe, Box box, int get_energy, double* bond_energy,
+	double* angle_energy) {
+	const uint32_t bond_blocks = (nb + blockDim.x - 1) / blockDim.x;
+	if (blockIdx.x < bond_blocks) {
+		const double e = bond_term(blockIdx.x * blockDim.x + threadIdx.x, bonds, bond_idx, nb, pos,
+								   fe, bond_tables, box, get_energy);
+		if (get_energy) block_add_f64(e, 0.0, bond_energy);
+	} else {
+		const double e = angle_term((blockIdx.x - bond_blocks) * blockDim.x + threadIdx.x, angles,
+									angle_idx, na, pos, fe, angle_tables, box, get_energy);
+		if (get_energy) block_add_f64(e, 0.0, angle_energy);
+	}
 }
 
 __device__ __forceinline__ float3 cross3(const float3& a, const float3& b) {
@@ -894,6 +933,17 @@ void angle_forces(const int4* angles, const int* table_idx, uint32_t na, const f
 	if (na == 0) return;
 	MB2_LAUNCH angle_kernel<<<(na + 255) / 256, 256, 0, st>>>(angles, table_idx, na, pos, fe,
 															  tables, box, get_energy, energy);
+}
+
+void bond_angle_forces(const int2* bonds, const int* bond_idx, uint32_t nb, const Table* bond_tables,
+					   const int4* angles, const int* angle_idx, uint32_t na,
+					   const Table* angle_tables, const float4* pos, float4* fe, const Box& box,
+					   int get_energy, double* bond_energy, double* angle_energy, cudaStream_t st) {
+	const uint32_t blocks = (nb + 255) / 256 + (na + 255) / 256;
+	if (blocks == 0) return;
+	MB2_LAUNCH bond_angle_kernel<<<blocks, 256, 0, st>>>(bonds, bond_idx, nb, bond_tables, angles,
+														 angle_idx, na, angle_tables, pos, fe, box,
+														 get_energy, bond_energy, angle_energy);
 }
 
 void dihedral_forces(const int4* dihedrals, const int* table_idx, uint32_t nd, const float4* pos,

@@ -245,6 +245,11 @@ void selftest_sqrt(unsigned long long* bad, cudaStream_t st);
 void bond_forces(const int2* bonds, const int* table_idx, uint32_t nb, const float4* pos,
 				 float4* fe, const Table* tables, const Box& box, int get_energy,
 				 double* energy, cudaStream_t st);
+// Bonds and angles in one launch (either count may be 0).
+void bond_angle_forces(const int2* bonds, const int* bond_idx, uint32_t nb, const Table* bond_tables,
+					   const int4* angles, const int* angle_idx, uint32_t na,
+					   const Table* angle_tables, const float4* pos, float4* fe, const Box& box,
+					   int get_energy, double* bond_energy, double* angle_energy, cudaStream_t st);
 void angle_forces(const int4* angles, const int* table_idx, uint32_t na, const float4* pos,
 				  float4* fe, const Table* tables, const Box& box, int get_energy, double* energy,
 				  cudaStream_t st);
