@@ -51,31 +51,57 @@ __device__ __forceinline__ uint32_t morton7(float x, float o, float scale) {
 	return static_cast<uint32_t>(min(max(q, 0), (1 << kLocalBits) - 1));
 }
 
-// Sort keys in original order. A system being rebuilt (flags null: every
-// system) gets the Morton keys of its current positions; any other keeps the
-// keys of its last build (old_sorted_keys through the last inverse
-// permutation), so that the stable sort puts its particles back in the same
-// sorted slots and its rows of the list stay valid.
-__global__ void __launch_bounds__(256) batch_encode_kernel(
-	const float4* __restrict__ pos, const uint32_t* __restrict__ sys_of,
-	const Box* __restrict__ boxes, uint32_t n, const uint32_t* __restrict__ flags,
-	const uint32_t* __restrict__ old_sorted_keys, const uint32_t* __restrict__ old_inv,
-	uint32_t* __restrict__ keys, uint32_t* __restrict__ idx) {
-	const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-	if (i >= n) return;
-	const uint32_t s = sys_of[i];
-	idx[i] = i;
-	if (flags && !flags[s]) {
-		keys[i] = old_sorted_keys[old_inv[i]];
-		return;
-	}
-	const Box& b = boxes[s];
-	const float4 p = pos[i];
+// Morton key of one particle in its own system's box.
+__device__ __forceinline__ uint32_t batch_key(const float4& p, const Box& b, uint32_t s) {
 	const float k = static_cast<float>(1 << kLocalBits);
 	const uint32_t x = morton7(p.x, b.origin[0], __fmul_rn(k, b.inv[0]));
 	const uint32_t y = morton7(p.y, b.origin[1], __fmul_rn(k, b.inv[1]));
 	const uint32_t z = morton7(p.z, b.origin[2], __fmul_rn(k, b.inv[2]));
-	keys[i] = (s << kSysShift) | split_by3(z) | (split_by3(y) << 1) | (split_by3(x) << 2);
+	return (s << kSysShift) | split_by3(z) | (split_by3(y) << 1) | (split_by3(x) << 2);
+}
+
+__global__ void __launch_bounds__(256) batch_encode_kernel(const float4* __restrict__ pos,
+														   const uint32_t* __restrict__ sys_of,
+														   const Box* __restrict__ boxes,
+														   uint32_t n, uint32_t* __restrict__ keys,
+														   uint32_t* __restrict__ idx) {
+	const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+	if (i >= n) return;
+	const uint32_t s = sys_of[i];
+	keys[i] = batch_key(pos[i], boxes[s], s);
+	idx[i] = i;
+}
+
+// A rebuild of some systems: their particles' keys, packed system after
+// system (cstart[s]: the number of rebuilt particles before system s; the
+// systems' particles are contiguous in the caller's order too).
+__global__ void __launch_bounds__(256) batch_compact_kernel(
+	const float4* __restrict__ pos, const uint32_t* __restrict__ sys_of,
+	const Box* __restrict__ boxes, const uint32_t* __restrict__ offsets,
+	const uint32_t* __restrict__ flags, const uint32_t* __restrict__ cstart, uint32_t n,
+	uint32_t* __restrict__ ckeys, uint32_t* __restrict__ cidx) {
+	const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+	if (i >= n) return;
+	const uint32_t s = sys_of[i];
+	if (!flags[s]) return;
+	const uint32_t c = cstart[s] + (i - offsets[s]);
+	ckeys[c] = batch_key(pos[i], boxes[s], s);
+	cidx[c] = i;
+}
+
+// The rebuilt systems' sorted keys into their systems' fixed ranges of the
+// sorted arrays (system s owns sorted slots [offsets[s], offsets[s + 1])).
+__global__ void __launch_bounds__(256) batch_scatter_sorted_kernel(
+	const uint32_t* __restrict__ ckeys, const uint32_t* __restrict__ cidx, uint32_t m,
+	const uint32_t* __restrict__ offsets, const uint32_t* __restrict__ cstart,
+	uint32_t* __restrict__ keys, uint32_t* __restrict__ s2o) {
+	const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+	if (k >= m) return;
+	const uint32_t key = ckeys[k];
+	const uint32_t s = key >> kSysShift;
+	const uint32_t g = offsets[s] + (k - cstart[s]);
+	keys[g] = key;
+	s2o[g] = cidx[k];
 }
 
 // Row statistics of the whole list: stats[0] += entries, stats[1] = the
@@ -387,7 +413,7 @@ struct mb2_batch {
 	Scratch scratch;
 	// sort / list state
 	DevBuf<uint32_t> keys, s2o, inv, row_len, row_off, nbr, cell_begin, cell_end;
-	DevBuf<uint32_t> keys_in, sys_flags;  // original-order sort keys; systems to rebuild
+	DevBuf<uint32_t> ckeys, cidx, sys_flags, cstart;  // a partial rebuild's keys, flags, starts
 	DevBuf<float4> sorted_pos, ref_pos, force_sorted;
 	DevBuf<SysGrid> grids;
 	std::vector<SysGrid> grids_h;
@@ -405,6 +431,7 @@ struct mb2_batch {
 	DevBuf<double> energy;
 	unsigned long long* pinned = nullptr;
 	unsigned int* pinned_sys = nullptr;  // per system: displacement readback, then rebuild flags
+	unsigned int* pinned_cstart = nullptr;  // per system: rebuilt particles before it
 	bool built = false;
 	uint64_t num_pairs = 0;
 	uint32_t cap = 0;
@@ -431,6 +458,7 @@ struct mb2_batch {
 		if (graph) cudaGraphExecDestroy(graph);
 		if (pinned) cudaFreeHost(pinned);
 		if (pinned_sys) cudaFreeHost(pinned_sys);
+		if (pinned_cstart) cudaFreeHost(pinned_cstart);
 	}
 };
 
@@ -546,28 +574,46 @@ void batch_build(mb2_batch* b, const float4* pos, const int* type_ids, float rc,
 	if (!(b->built && b->cap && b->lanes)) flags_h = nullptr;
 	const uint32_t* dflags = nullptr;
 	uint64_t rebuilt = b->num_systems;
-	if (flags_h) {
-		rebuilt = 0;
-		for (uint32_t s = 0; s < b->num_systems; ++s) rebuilt += flags_h[s] ? 1u : 0u;
-		b->sys_flags.ensure(b->num_systems);
-		MB2_CUDA(cudaMemcpyAsync(b->sys_flags.ptr, flags_h, b->num_systems * sizeof(unsigned int),
-								 cudaMemcpyHostToDevice, st));
-		dflags = b->sys_flags.ptr;
-	}
 	b->keys.ensure(n);
-	b->keys_in.ensure(n);
 	b->s2o.ensure(n);
 	b->inv.ensure(n);
 	b->sorted_pos.ensure(n);
-	if (n)
-		MB2_LAUNCH batch_encode_kernel<<<(n + 255) / 256, 256, 0, st>>>(
-			pos, b->sys_of.ptr, b->boxes.ptr, n, dflags, b->keys.ptr, b->inv.ptr, b->keys_in.ptr,
-			b->s2o.ptr);
-	// (copied, not swapped: the captured step reads the sorted keys at a fixed address)
-	if (n)
-		MB2_CUDA(cudaMemcpyAsync(b->keys.ptr, b->keys_in.ptr, static_cast<size_t>(n) * sizeof(uint32_t),
-								 cudaMemcpyDeviceToDevice, st));
-	radix_sort_pairs(b->scratch, b->keys.ptr, b->s2o.ptr, n, st);
+	if (flags_h) {
+		// Only the rebuilt systems' particles are sorted: the others keep their
+		// sorted slots (keys and order of their own last build).
+		const uint32_t S = b->num_systems;
+		uint32_t m = 0;
+		rebuilt = 0;
+		for (uint32_t s = 0; s < S; ++s) {
+			b->pinned_cstart[s] = m;
+			if (flags_h[s]) {
+				m += b->offsets[s + 1] - b->offsets[s];
+				++rebuilt;
+			}
+		}
+		b->sys_flags.ensure(S);
+		b->cstart.ensure(S);
+		MB2_CUDA(cudaMemcpyAsync(b->sys_flags.ptr, flags_h, S * sizeof(unsigned int),
+								 cudaMemcpyHostToDevice, st));
+		MB2_CUDA(cudaMemcpyAsync(b->cstart.ptr, b->pinned_cstart, S * sizeof(unsigned int),
+								 cudaMemcpyHostToDevice, st));
+		dflags = b->sys_flags.ptr;
+		b->ckeys.ensure(std::max<uint32_t>(m, 1));
+		b->cidx.ensure(std::max<uint32_t>(m, 1));
+		MB2_LAUNCH batch_compact_kernel<<<(n + 255) / 256, 256, 0, st>>>(
+			pos, b->sys_of.ptr, b->boxes.ptr, b->offsets_d.ptr, dflags, b->cstart.ptr, n,
+			b->ckeys.ptr, b->cidx.ptr);
+		if (m) radix_sort_pairs(b->scratch, b->ckeys.ptr, b->cidx.ptr, m, st);
+		if (m)
+			MB2_LAUNCH batch_scatter_sorted_kernel<<<(m + 255) / 256, 256, 0, st>>>(
+				b->ckeys.ptr, b->cidx.ptr, m, b->offsets_d.ptr, b->cstart.ptr, b->keys.ptr,
+				b->s2o.ptr);
+	} else {
+		if (n)
+			MB2_LAUNCH batch_encode_kernel<<<(n + 255) / 256, 256, 0, st>>>(
+				pos, b->sys_of.ptr, b->boxes.ptr, n, b->keys.ptr, b->s2o.ptr);
+		radix_sort_pairs(b->scratch, b->keys.ptr, b->s2o.ptr, n, st);
+	}
 	inverse_and_gather(b->s2o.ptr, n, pos, b->inv.ptr, nullptr, st);
 	pack_sorted_positions(pos, type_ids, b->s2o.ptr, n, b->sorted_pos.ptr, st);
 	b->cell_begin.ensure(b->total_cells);
@@ -785,6 +831,7 @@ int mb2_batch_create(int device, uint32_t num_systems, const uint32_t* counts,
 			MB2_CUDA(cudaMemcpy(b->sys_of.ptr, sys_of.data(), b->n * 4ull, cudaMemcpyHostToDevice));
 		MB2_CUDA(cudaMallocHost(&b->pinned, 64));
 		MB2_CUDA(cudaMallocHost(&b->pinned_sys, num_systems * sizeof(unsigned int)));
+		MB2_CUDA(cudaMallocHost(&b->pinned_cstart, num_systems * sizeof(unsigned int)));
 		b->step_d.ensure(1);
 		b->energy.ensure(4);
 		MB2_CUDA(cudaMemset(b->energy.ptr, 0, 4 * sizeof(double)));
