@@ -7,6 +7,8 @@
 
 namespace mb2 {
 
+// ExclusionView::row_contains / same_body (src/Interactions/DeviceExclusions.h:22-75):
+// b is excluded from the row [row_b, row_e) of the CSR or shares its rigid body.
 __device__ __forceinline__ bool is_excluded(const Exclusions& ex, int b, int row_b, int row_e,
 											int body) {
 	if (body >= 0 && ex.rigid_body_id[b] == body) return true;
