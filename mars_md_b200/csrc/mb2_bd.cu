@@ -32,13 +32,35 @@ __device__ __forceinline__ bool map_index(int& j, long long n, int bc) {
 	return false;
 }
 
-__device__ __forceinline__ float fetch(const GridView& g, int jx, int jy, int jz, int bc) {
-	if (!map_index(jx, g.dims[0], bc) || !map_index(jy, g.dims[1], bc) ||
-		!map_index(jz, g.dims[2], bc))
-		return 0.0f;
-	const size_t idx = static_cast<size_t>(jz) + static_cast<size_t>(jy) * g.dims[2] +
-					   static_cast<size_t>(jx) * g.dims[1] * g.dims[2];
-	return __ldg(g.data + idx);
+// fetch_grid_value (BaseGridDevice.h:479-500) for the 2 x 2 x 2 taps of a
+// trilinear sample at (i0, j0, k0): each axis' two indices are mapped once,
+// and all eight loads are issued before any is used (a tap outside a
+// Dirichlet grid reads element 0 and is replaced by 0), so the taps' memory
+// latencies overlap instead of following one another.
+__device__ __forceinline__ void fetch8(const GridView& g, int i0, int j0, int k0, int bc,
+									   float v[8]) {
+	int ix[2] = {i0, i0 + 1}, iy[2] = {j0, j0 + 1}, iz[2] = {k0, k0 + 1};
+	bool ox[2], oy[2], oz[2];
+#pragma unroll
+	for (int t = 0; t < 2; ++t) {
+		ox[t] = map_index(ix[t], g.dims[0], bc);
+		oy[t] = map_index(iy[t], g.dims[1], bc);
+		oz[t] = map_index(iz[t], g.dims[2], bc);
+	}
+	const size_t ny = static_cast<size_t>(g.dims[1]), nz = static_cast<size_t>(g.dims[2]);
+	bool ok[8];
+#pragma unroll
+	for (int t = 0; t < 8; ++t) {
+		const int a = t >> 2, b = (t >> 1) & 1, c = t & 1;  // tap (x, y, z) = (a, b, c)
+		ok[t] = ox[a] && oy[b] && oz[c];
+		const size_t idx = ok[t] ? static_cast<size_t>(iz[c]) + static_cast<size_t>(iy[b]) * nz +
+									   static_cast<size_t>(ix[a]) * ny * nz
+								 : 0;
+		v[t] = __ldg(g.data + idx);
+	}
+#pragma unroll
+	for (int t = 0; t < 8; ++t)
+		if (!ok[t]) v[t] = 0.0f;
 }
 
 // Trilinear value and analytic gradient (interpolate_grid_point and
@@ -59,11 +81,10 @@ __device__ __forceinline__ void grid_sample(const GridView& g, float px, float p
 	const float fx = __fsub_rn(gp[0], static_cast<float>(i0));
 	const float fy = __fsub_rn(gp[1], static_cast<float>(j0));
 	const float fz = __fsub_rn(gp[2], static_cast<float>(k0));
-	const float v000 = fetch(g, i0, j0, k0, bc), v001 = fetch(g, i0, j0, k0 + 1, bc);
-	const float v010 = fetch(g, i0, j0 + 1, k0, bc), v011 = fetch(g, i0, j0 + 1, k0 + 1, bc);
-	const float v100 = fetch(g, i0 + 1, j0, k0, bc), v101 = fetch(g, i0 + 1, j0, k0 + 1, bc);
-	const float v110 = fetch(g, i0 + 1, j0 + 1, k0, bc),
-				v111 = fetch(g, i0 + 1, j0 + 1, k0 + 1, bc);
+	float v[8];
+	fetch8(g, i0, j0, k0, bc, v);
+	const float v000 = v[0], v001 = v[1], v010 = v[2], v011 = v[3];
+	const float v100 = v[4], v101 = v[5], v110 = v[6], v111 = v[7];
 	const float ox = __fsub_rn(1.0f, fx), oy = __fsub_rn(1.0f, fy), oz = __fsub_rn(1.0f, fz);
 	auto lerp = [](float a, float wa, float b, float wb) {
 		return __fadd_rn(__fmul_rn(a, wa), __fmul_rn(b, wb));
