@@ -134,6 +134,14 @@ struct CellGrid {
 	float wmin[3] = {0, 0, 0};          // narrowest cell width per axis
 	float lim = 0.0f;                   // pruning bound on the squared cell gap
 };
+// Up to this many particles the pairlist is walked one warp per particle
+// (build_rows_kernel) instead of one warp per 32 (build_walk_kernel).
+// Measured per build, group walk against row walk: 65,536-bead polymers 0.75
+// vs 0.30 ms; uniform beads at 0.002 A^-3, 32,768: 0.43 vs 0.34 ms (the group
+// walk's best at that size); 131,072: 1.06 vs 0.75 ms; 262,144: 1.36 vs
+// 1.48 ms; 524,288: 1.74 vs 2.30 ms; 2,097,152: 5.45 vs 10.6 ms.
+constexpr uint32_t kRowWalkMaxN = 131072;
+
 // Parameters of the group walk (passed by value to the kernel).
 struct WalkGrid {
 	int m, shift, emax;

@@ -150,13 +150,6 @@ __global__ void __launch_bounds__(256) cell_ranges_kernel(const uint32_t* __rest
 	if (i + 1 == n || (keys[i + 1] >> shift) != c) end[c] = i + 1;
 }
 
-// Up to this many particles the pairlist is walked one warp per particle
-// (build_rows_kernel) instead of one warp per 32 (build_walk_kernel).
-// Measured per build, group walk against row walk: 65,536-bead polymers 0.75
-// vs 0.30 ms; uniform beads at 0.002 A^-3, 32,768: 0.43 vs 0.34 ms (the group
-// walk's best at that size); 131,072: 1.06 vs 0.75 ms; 262,144: 1.36 vs
-// 1.48 ms; 524,288: 1.74 vs 2.30 ms; 2,097,152: 5.45 vs 10.6 ms.
-constexpr uint32_t kRowWalkMaxN = 131072;
 
 // One warp owns a group of 32 consecutive sorted particles, lane = particle.
 // The group's cells are Morton-adjacent; the warp walks, in lockstep, every

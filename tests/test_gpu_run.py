@@ -6,10 +6,13 @@ a new capture, and the Langevin branch (which runs step by step).
 
 Two contexts stepping the same system agree to the last bits only up to the
 order of the float atomics that add the pair forces (a few ulps of
-ForceEnergy on some particles from the first step), so the trajectories are
-held as the trajectory test holds them: every particle within 1e-3 A and
-99 % within 1e-4 A. A wrong step number in the replayed graph (another Philox
-stream) would move every particle by the noise, about 0.2 A a step."""
+ForceEnergy on some particles from the first step). Where that puts a pair
+on the other side of a table-bin edge, the particle's path jumps by D dt / kT
+times the bins' force difference (of order 1e-2 A) and follows its own
+course from there. So the trajectories are held as the trajectory test holds
+them: 99 % of the particles within 1e-4 A and every particle within 0.05 A
+(a few such jumps). A wrong step number in the replayed graph (another
+Philox stream) would move every particle by the noise, about 0.2 A a step."""
 import numpy as np
 import pytest
 import torch
@@ -46,7 +49,7 @@ def _same(a, b, box=None):
     if box is not None:
         d = np.minimum(d, np.asarray(box, np.float32) - d)
     d = d.max(axis=1)
-    assert d.max() <= 1e-3, float(d.max())
+    assert d.max() <= 0.05, float(d.max())
     assert (d <= 1e-4).mean() >= 0.99, int((d > 1e-4).sum())
     fa, fb = a["fe"].cpu().numpy()[:, :3], b["fe"].cpu().numpy()[:, :3]
     scale = np.abs(fb).max()
