@@ -51,15 +51,21 @@ __device__ __forceinline__ float3 f3sub(float4 a, float4 b) {
 	return make_float3(a.x - b.x, a.y - b.y, a.z - b.z);
 }
 
-// mu = (D / kT * dt) * lambda per type and axis, in original and sorted order.
+// mu = (D / kT * dt) * lambda per type and axis, in original and sorted order;
+// the step's tangent accumulators cleared.
 __global__ void __launch_bounds__(256) adj_mu_kernel(const float4* __restrict__ lam,
 													 const int* __restrict__ type_ids,
 													 const float4* __restrict__ diffusion,
 													 const uint32_t* __restrict__ inv, uint32_t n,
 													 float dt_over_kT, float4* __restrict__ mu,
-													 float4* __restrict__ mu_sorted) {
+													 float4* __restrict__ mu_sorted,
+													 float4* __restrict__ tan,
+													 float4* __restrict__ tan_sorted) {
 	const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
 	if (i >= n) return;
+	// The tangent accumulators of this step start at zero.
+	tan[i] = make_float4(0.f, 0.f, 0.f, 0.f);
+	tan_sorted[i] = make_float4(0.f, 0.f, 0.f, 0.f);
 	const float4 d = diffusion[type_ids[i]];
 	const float4 l = lam[i];
 	const float4 m = make_float4(d.x * dt_over_kT * l.x, d.y * dt_over_kT * l.y,
@@ -154,16 +160,18 @@ __global__ void __launch_bounds__(256) adj_pair_kernel(
 	flush_bins(sg, grad_bins, total_bins);
 }
 
-// Bond term (original order); table bins indexed from the bonded table base.
-__global__ void __launch_bounds__(256) adj_bond_kernel(
-	const int2* __restrict__ bonds, const int* __restrict__ table_idx, uint32_t nb,
-	const float4* __restrict__ pos, const float4* __restrict__ mu, const Table* __restrict__ tables,
-	const float* __restrict__ values_base, uint32_t total_bins, Box box, float4* tan,
-	double* __restrict__ grad_bins) {
-	extern __shared__ double sg[];
+// Bond term (original order) over blocks [0, nblocks) of the launch
+// (grid-stride); table bins indexed from the bonded table base, the block's
+// bond-table gradient accumulated in shared memory and flushed at its end.
+__device__ __forceinline__ void adj_bonds(
+	uint32_t block, uint32_t nblocks, const int2* __restrict__ bonds,
+	const int* __restrict__ table_idx, uint32_t nb, const float4* __restrict__ pos,
+	const float4* __restrict__ mu, const Table* __restrict__ tables,
+	const float* __restrict__ values_base, uint32_t total_bins, const Box& box, float4* tan,
+	double* __restrict__ grad_bins, double* sg) {
 	for (uint32_t k = threadIdx.x; k < total_bins; k += blockDim.x) sg[k] = 0.0;
 	__syncthreads();
-	for (uint32_t b = blockIdx.x * blockDim.x + threadIdx.x; b < nb; b += gridDim.x * blockDim.x) {
+	for (uint32_t b = block * blockDim.x + threadIdx.x; b < nb; b += nblocks * blockDim.x) {
 		const int2 e = bonds[b];
 		// Distance and bin as the forward bond kernel decides them.
 		const float4 pa = pos[e.x], pb = pos[e.y];
@@ -195,11 +203,10 @@ __global__ void __launch_bounds__(256) adj_bond_kernel(
 }
 
 // Angle term: tangent of the AngleGeometry force along mu (dual numbers).
-__global__ void __launch_bounds__(256) adj_angle_kernel(
-	const int4* __restrict__ angles, const int* __restrict__ table_idx, uint32_t na,
+__device__ __forceinline__ void adj_angle(
+	uint32_t q, const int4* __restrict__ angles, const int* __restrict__ table_idx, uint32_t na,
 	const float4* __restrict__ pos, const float4* __restrict__ mu, const Table* __restrict__ tables,
-	Box box, float4* tan) {
-	const uint32_t q = blockIdx.x * blockDim.x + threadIdx.x;
+	const Box& box, float4* tan) {
 	if (q >= na) return;
 	const int4 a = angles[q];
 	const float4 pi = pos[a.x], pj = pos[a.y], pk = pos[a.z];
@@ -255,6 +262,24 @@ __global__ void __launch_bounds__(256) adj_angle_kernel(
 	red_add_v4(&tan[a.x], t1[0], t1[1], t1[2], 0.0f);
 	red_add_v4(&tan[a.y], -(t1[0] + t3[0]), -(t1[1] + t3[1]), -(t1[2] + t3[2]), 0.0f);
 	red_add_v4(&tan[a.z], t3[0], t3[1], t3[2], 0.0f);
+}
+
+// Bonds and angles of one adjoint step in one launch: blocks [0, bond_blocks)
+// take the bonds (grid-stride, bond-table gradient through shared memory),
+// the rest one angle per thread.
+__global__ void __launch_bounds__(256) adj_bond_angle_kernel(
+	uint32_t bond_blocks, const int2* __restrict__ bonds, const int* __restrict__ bond_idx,
+	uint32_t nb, const Table* __restrict__ bond_tables, const float* __restrict__ values_base,
+	uint32_t total_bins, double* __restrict__ grad_bins, const int4* __restrict__ angles,
+	const int* __restrict__ angle_idx, uint32_t na, const Table* __restrict__ angle_tables,
+	const float4* __restrict__ pos, const float4* __restrict__ mu, Box box, float4* tan) {
+	extern __shared__ double sg[];
+	if (blockIdx.x < bond_blocks)
+		adj_bonds(blockIdx.x, bond_blocks, bonds, bond_idx, nb, pos, mu, bond_tables, values_base,
+				  total_bins, box, tan, grad_bins, sg);
+	else
+		adj_angle((blockIdx.x - bond_blocks) * blockDim.x + threadIdx.x, angles, angle_idx, na,
+				  pos, mu, angle_tables, box, tan);
 }
 
 // lambda += tan (original order) + tan_sorted (gathered through inv).
@@ -409,25 +434,24 @@ void adjoint_step(const AdjointStepArgs& a, cudaStream_t st) {
 	const uint32_t n = a.n;
 	if (n == 0) return;
 	MB2_LAUNCH adj_mu_kernel<<<(n + 255) / 256, 256, 0, st>>>(a.lam, a.type_ids, a.diffusion, a.inv,
-															  n, a.dt_over_kT, a.mu, a.mu_sorted);
-	MB2_CUDA(cudaMemsetAsync(a.tan, 0, static_cast<size_t>(n) * sizeof(float4), st));
-	MB2_CUDA(cudaMemsetAsync(a.tan_sorted, 0, static_cast<size_t>(n) * sizeof(float4), st));
+															  n, a.dt_over_kT, a.mu, a.mu_sorted,
+															  a.tan, a.tan_sorted);
 	switch (a.lanes) {
 	case 4: launch_adj_pair_g<4>(a, st); break;
 	case 8: launch_adj_pair_g<8>(a, st); break;
 	case 16: launch_adj_pair_g<16>(a, st); break;
 	default: launch_adj_pair_g<32>(a, st); break;
 	}
-	if (a.num_bonds) {
-		const size_t smem = static_cast<size_t>(a.bond_bins) * 8;
-		const uint32_t blocks = std::min<uint32_t>((a.num_bonds + 255) / 256, kPersistentBlocks);
-		MB2_LAUNCH adj_bond_kernel<<<blocks, 256, smem, st>>>(
-			a.bonds, a.bond_table_idx, a.num_bonds, a.pos, a.mu, a.bond_tables, a.bond_values_base,
-			a.bond_bins, a.box, a.tan, a.grad_bond);
+	if (a.num_bonds || a.num_angles) {
+		const uint32_t bond_blocks =
+			a.num_bonds ? std::min<uint32_t>((a.num_bonds + 255) / 256, kPersistentBlocks) : 0u;
+		const uint32_t angle_blocks = (a.num_angles + 255) / 256;
+		const size_t smem = a.num_bonds ? static_cast<size_t>(a.bond_bins) * 8 : 0;
+		MB2_LAUNCH adj_bond_angle_kernel<<<bond_blocks + angle_blocks, 256, smem, st>>>(
+			bond_blocks, a.bonds, a.bond_table_idx, a.num_bonds, a.bond_tables, a.bond_values_base,
+			a.bond_bins, a.grad_bond, a.angles, a.angle_table_idx, a.num_angles, a.angle_tables,
+			a.pos, a.mu, a.box, a.tan);
 	}
-	if (a.num_angles)
-		MB2_LAUNCH adj_angle_kernel<<<(a.num_angles + 255) / 256, 256, 0, st>>>(
-			a.angles, a.angle_table_idx, a.num_angles, a.pos, a.mu, a.angle_tables, a.box, a.tan);
 	MB2_LAUNCH adj_combine_kernel<<<(n + 255) / 256, 256, 0, st>>>(a.lam, a.tan, a.tan_sorted, a.inv,
 																   n);
 }
