@@ -51,6 +51,15 @@ __device__ __forceinline__ float3 f3sub(float4 a, float4 b) {
 	return make_float3(a.x - b.x, a.y - b.y, a.z - b.z);
 }
 
+// Tangent accumulators hold 4 doubles per particle (x, y, z, unused): the
+// per-particle sums of many float terms that largely cancel are kept in FP64,
+// so a step adds no more rounding than its float terms carry.
+__device__ __forceinline__ void add_d3(double* t, double x, double y, double z) {
+	atomicAdd(t, x);
+	atomicAdd(t + 1, y);
+	atomicAdd(t + 2, z);
+}
+
 // mu = (D / kT * dt) * lambda per type and axis, in original and sorted order;
 // the step's tangent accumulators cleared.
 __global__ void __launch_bounds__(256) adj_mu_kernel(const float4* __restrict__ lam,
@@ -59,13 +68,13 @@ __global__ void __launch_bounds__(256) adj_mu_kernel(const float4* __restrict__ 
 													 const uint32_t* __restrict__ inv, uint32_t n,
 													 float dt_over_kT, float4* __restrict__ mu,
 													 float4* __restrict__ mu_sorted,
-													 float4* __restrict__ tan,
-													 float4* __restrict__ tan_sorted) {
+													 double4* __restrict__ tan,
+													 double4* __restrict__ tan_sorted) {
 	const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
 	if (i >= n) return;
 	// The tangent accumulators of this step start at zero.
-	tan[i] = make_float4(0.f, 0.f, 0.f, 0.f);
-	tan_sorted[i] = make_float4(0.f, 0.f, 0.f, 0.f);
+	tan[i] = make_double4(0.0, 0.0, 0.0, 0.0);
+	tan_sorted[i] = make_double4(0.0, 0.0, 0.0, 0.0);
 	const float4 d = diffusion[type_ids[i]];
 	const float4 l = lam[i];
 	const float4 m = make_float4(d.x * dt_over_kT * l.x, d.y * dt_over_kT * l.y,
@@ -89,7 +98,7 @@ __global__ void __launch_bounds__(256) adj_pair_kernel(
 	const uint32_t* __restrict__ nbr, const uint32_t* __restrict__ row_len, uint32_t n,
 	uint32_t cap, int T, const PairTableRef* __restrict__ refs_g,
 	const float* __restrict__ force_g, uint32_t total_bins, Box box, float cutoff_sq,
-	float4* tan_sorted, double* __restrict__ grad_bins) {
+	double* tan_sorted, double* __restrict__ grad_bins) {
 	constexpr int H = 32 / G;
 	extern __shared__ double sg[];
 	PairTableRef* refs = reinterpret_cast<PairTableRef*>(sg + total_bins);
@@ -110,7 +119,7 @@ __global__ void __launch_bounds__(256) adj_pair_kernel(
 		const PairTableRef* trow = refs + (valid ? type_of(pi) : 0) * T;
 		const uint32_t cnt = valid ? row_len[i] : 0u;
 		const uint32_t* col = nbr + (static_cast<size_t>(i / H) * cap) * H + (i % H);
-		float tx = 0.0f, ty = 0.0f, tz = 0.0f;
+		double tx = 0.0, ty = 0.0, tz = 0.0;
 		for (uint32_t t = sub; t < cnt; t += G) {
 			const uint32_t e = __ldg(col + static_cast<size_t>(t) * H);
 			const uint32_t j = e & ~kOrientBit;
@@ -139,7 +148,7 @@ __global__ void __launch_bounds__(256) adj_pair_kernel(
 			const float ud = ux * dvx + uy * dvy + uz * dvz;
 			const float k = F / d;
 			const float gx = k * (dvx - ux * ud), gy = k * (dvy - uy * ud), gz = k * (dvz - uz * ud);
-			red_add_v4(&tan_sorted[j], gx, gy, gz, 0.0f);
+			add_d3(tan_sorted + 4 * static_cast<size_t>(j), gx, gy, gz);
 			tx -= gx;
 			ty -= gy;
 			tz -= gz;
@@ -155,7 +164,7 @@ __global__ void __launch_bounds__(256) adj_pair_kernel(
 			ty += __shfl_xor_sync(0xFFFFFFFFu, ty, o, G);
 			tz += __shfl_xor_sync(0xFFFFFFFFu, tz, o, G);
 		}
-		if (valid && sub == 0 && cnt != 0u) red_add_v4(&tan_sorted[i], tx, ty, tz, 0.0f);
+		if (valid && sub == 0 && cnt != 0u) add_d3(tan_sorted + 4 * static_cast<size_t>(i), tx, ty, tz);
 	}
 	flush_bins(sg, grad_bins, total_bins);
 }
@@ -167,7 +176,7 @@ __device__ __forceinline__ void adj_bonds(
 	uint32_t block, uint32_t nblocks, const int2* __restrict__ bonds,
 	const int* __restrict__ table_idx, uint32_t nb, const float4* __restrict__ pos,
 	const float4* __restrict__ mu, const Table* __restrict__ tables,
-	const float* __restrict__ values_base, uint32_t total_bins, const Box& box, float4* tan,
+	const float* __restrict__ values_base, uint32_t total_bins, const Box& box, double* tan,
 	double* __restrict__ grad_bins, double* sg) {
 	for (uint32_t k = threadIdx.x; k < total_bins; k += blockDim.x) sg[k] = 0.0;
 	__syncthreads();
@@ -192,8 +201,8 @@ __device__ __forceinline__ void adj_bonds(
 		const float ud = ux * dvx + uy * dvy + uz * dvz;
 		const float k = F * inv;
 		const float gx = k * (dvx - ux * ud), gy = k * (dvy - uy * ud), gz = k * (dvz - uz * ud);
-		red_add_v4(&tan[e.y], gx, gy, gz, 0.0f);
-		red_add_v4(&tan[e.x], -gx, -gy, -gz, 0.0f);
+		add_d3(tan + 4 * static_cast<size_t>(e.y), gx, gy, gz);
+		add_d3(tan + 4 * static_cast<size_t>(e.x), -gx, -gy, -gz);
 		const uint32_t base = static_cast<uint32_t>(t.pot - values_base) + home;
 		const double gb = static_cast<double>(t.step_inv) * ud;
 		atomicAdd(&sg[base], gb);
@@ -206,7 +215,7 @@ __device__ __forceinline__ void adj_bonds(
 __device__ __forceinline__ void adj_angle(
 	uint32_t q, const int4* __restrict__ angles, const int* __restrict__ table_idx, uint32_t na,
 	const float4* __restrict__ pos, const float4* __restrict__ mu, const Table* __restrict__ tables,
-	const Box& box, float4* tan) {
+	const Box& box, double* tan) {
 	if (q >= na) return;
 	const int4 a = angles[q];
 	const float4 pi = pos[a.x], pj = pos[a.y], pk = pos[a.z];
@@ -259,9 +268,10 @@ __device__ __forceinline__ void adj_angle(
 		t1[c] = (s1 * (ab[c] * c_ab + bc[c] * inv_bc)).d;
 		t3[c] = (s3 * (bc[c] * c_bc + ab[c] * inv_ab)).d;
 	}
-	red_add_v4(&tan[a.x], t1[0], t1[1], t1[2], 0.0f);
-	red_add_v4(&tan[a.y], -(t1[0] + t3[0]), -(t1[1] + t3[1]), -(t1[2] + t3[2]), 0.0f);
-	red_add_v4(&tan[a.z], t3[0], t3[1], t3[2], 0.0f);
+	add_d3(tan + 4 * static_cast<size_t>(a.x), t1[0], t1[1], t1[2]);
+	add_d3(tan + 4 * static_cast<size_t>(a.y), -(t1[0] + t3[0]), -(t1[1] + t3[1]),
+		   -(t1[2] + t3[2]));
+	add_d3(tan + 4 * static_cast<size_t>(a.z), t3[0], t3[1], t3[2]);
 }
 
 // Bonds and angles of one adjoint step in one launch: blocks [0, bond_blocks)
@@ -272,7 +282,7 @@ __global__ void __launch_bounds__(256) adj_bond_angle_kernel(
 	uint32_t nb, const Table* __restrict__ bond_tables, const float* __restrict__ values_base,
 	uint32_t total_bins, double* __restrict__ grad_bins, const int4* __restrict__ angles,
 	const int* __restrict__ angle_idx, uint32_t na, const Table* __restrict__ angle_tables,
-	const float4* __restrict__ pos, const float4* __restrict__ mu, Box box, float4* tan) {
+	const float4* __restrict__ pos, const float4* __restrict__ mu, Box box, double* tan) {
 	extern __shared__ double sg[];
 	if (blockIdx.x < bond_blocks)
 		adj_bonds(blockIdx.x, bond_blocks, bonds, bond_idx, nb, pos, mu, bond_tables, values_base,
@@ -284,17 +294,17 @@ __global__ void __launch_bounds__(256) adj_bond_angle_kernel(
 
 // lambda += tan (original order) + tan_sorted (gathered through inv).
 __global__ void __launch_bounds__(256) adj_combine_kernel(float4* __restrict__ lam,
-														  const float4* __restrict__ tan,
-														  const float4* __restrict__ tan_sorted,
+														  const double4* __restrict__ tan,
+														  const double4* __restrict__ tan_sorted,
 														  const uint32_t* __restrict__ inv,
 														  uint32_t n) {
 	const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
 	if (i >= n) return;
-	const float4 a = tan[i], b = tan_sorted[inv[i]];
+	const double4 a = tan[i], b = tan_sorted[inv[i]];
 	float4 l = lam[i];
-	l.x += a.x + b.x;
-	l.y += a.y + b.y;
-	l.z += a.z + b.z;
+	l.x = static_cast<float>(static_cast<double>(l.x) + (a.x + b.x));
+	l.y = static_cast<float>(static_cast<double>(l.y) + (a.y + b.y));
+	l.z = static_cast<float>(static_cast<double>(l.z) + (a.z + b.z));
 	lam[i] = l;
 }
 
@@ -405,7 +415,8 @@ void launch_adj_pair(const AdjointStepArgs& a, cudaStream_t st) {
 									  static_cast<int>(smem)));
 	MB2_LAUNCH kern<<<grid_for_rows(a.n, G), 256, smem, st>>>(
 		a.sorted_pos, a.mu_sorted, a.nbr, a.row_len, a.n, a.cap, a.tables.num_types,
-		a.tables.refs, a.tables.bin_force, a.tables.total_bins, a.box, a.cutoff_sq, a.tan_sorted,
+		a.tables.refs, a.tables.bin_force, a.tables.total_bins, a.box, a.cutoff_sq,
+		reinterpret_cast<double*>(a.tan_sorted),
 		a.grad_pair);
 }
 
@@ -450,7 +461,7 @@ void adjoint_step(const AdjointStepArgs& a, cudaStream_t st) {
 		MB2_LAUNCH adj_bond_angle_kernel<<<bond_blocks + angle_blocks, 256, smem, st>>>(
 			bond_blocks, a.bonds, a.bond_table_idx, a.num_bonds, a.bond_tables, a.bond_values_base,
 			a.bond_bins, a.grad_bond, a.angles, a.angle_table_idx, a.num_angles, a.angle_tables,
-			a.pos, a.mu, a.box, a.tan);
+			a.pos, a.mu, a.box, reinterpret_cast<double*>(a.tan));
 	}
 	MB2_LAUNCH adj_combine_kernel<<<(n + 255) / 256, 256, 0, st>>>(a.lam, a.tan, a.tan_sorted, a.inv,
 																   n);

@@ -100,6 +100,7 @@ struct mb2_context {
 		const int* type_ids = nullptr;
 	} win;
 	DevBuf<float4> ckpt, states, wpos, wfe, lam, mu, mu_sorted, tan, tan_sorted;
+	DevBuf<double4> adj_tan, adj_tan_sorted;  // FP64 tangent accumulators of the reverse sweep
 	float4* record_states = nullptr;  // caller's buffer for the states a reverse sweep differentiates
 	uint64_t record_cap = 0;          // its capacity in float4 rows
 	bool rdf_built = false;  // the current list was built by mb2_rdf_histogram
@@ -424,7 +425,15 @@ bool matrix_has_analytical(const mb2_context* ctx) {
 }
 
 // Pair kernel over the sorted positions into the zeroed sorted accumulator.
-void pair_kernel(mb2_context* ctx, uint32_t n, float cutoff, int get_energy, cudaStream_t st) {
+// The Z-ordered pair-force accumulator, sized for n (for a pack that clears it).
+float4* sorted_forces(mb2_context* ctx, uint32_t n) {
+	ctx->force_sorted.ensure(n);
+	return ctx->force_sorted.ptr;
+}
+
+// cleared: the accumulator was zeroed by this step's pack.
+void pair_kernel(mb2_context* ctx, uint32_t n, float cutoff, int get_energy, cudaStream_t st,
+				 bool cleared = false) {
 	require(ctx->built, MB2_ERR_STATE, "mb2_pair_forces: no pairlist; call mb2_build_pairlist");
 	require(n == ctx->built_n, MB2_ERR_ARG,
 			"mb2_pair_forces: particle count differs from the last pairlist build");
@@ -433,7 +442,9 @@ void pair_kernel(mb2_context* ctx, uint32_t n, float cutoff, int get_energy, cud
 	require(ctx->pt.terms || !matrix_has_analytical(ctx), MB2_ERR_STATE,
 			"mb2_pair_forces: the tags carry analytical terms; call mb2_set_pair_terms");
 	ctx->force_sorted.ensure(n);
-	MB2_CUDA(cudaMemsetAsync(ctx->force_sorted.ptr, 0, static_cast<size_t>(n) * sizeof(float4), st));
+	if (!cleared)
+		MB2_CUDA(cudaMemsetAsync(ctx->force_sorted.ptr, 0, static_cast<size_t>(n) * sizeof(float4),
+								 st));
 	const float cutoff_sq = cutoff > 0.0f ? cutoff * cutoff : 0.0f;
 	StageScope scope(ctx, MB2_STAGE_PAIR_FORCE, st);
 	pair_forces(ctx->sorted_pos.ptr, ctx->nbr.ptr, ctx->row_len.ptr, n, ctx->cap, ctx->lanes, ctx->pt,
@@ -444,8 +455,9 @@ void pair_forces_impl(mb2_context* ctx, const float4* pos, const int* type_ids, 
 					  uint32_t n, float cutoff, int get_energy, cudaStream_t st) {
 	require(ctx->built, MB2_ERR_STATE, "mb2_pair_forces: no pairlist; call mb2_build_pairlist");
 	if (n == 0) return;
-	pack_sorted_positions(pos, type_ids, ctx->s2o.ptr, n, ctx->sorted_pos.ptr, st);
-	pair_kernel(ctx, n, cutoff, get_energy, st);
+	pack_sorted_positions(pos, type_ids, ctx->s2o.ptr, n, ctx->sorted_pos.ptr, st, nullptr,
+						  sorted_forces(ctx, n));
+	pair_kernel(ctx, n, cutoff, get_energy, st, true);
 	scatter_add_forces(ctx->force_sorted.ptr, ctx->s2o.ptr, n, fe, get_energy, st);
 }
 
@@ -552,9 +564,9 @@ bool step_has_bonded(const mb2_step_params* prm) {
 void window_step(mb2_context* ctx, float4* pos, float4* fe, const int* type_ids, uint32_t n,
 				 uint64_t step, const mb2_step_params* prm, cudaStream_t st) {
 	const bool bonded = prm->num_bonds != 0 || prm->num_angles != 0;
-	if (bonded) MB2_CUDA(cudaMemsetAsync(fe, 0, static_cast<size_t>(n) * sizeof(float4), st));
-	pack_sorted_positions(pos, type_ids, ctx->s2o.ptr, n, ctx->sorted_pos.ptr, st);
-	pair_kernel(ctx, n, prm->cutoff, 0, st);
+	pack_sorted_positions(pos, type_ids, ctx->s2o.ptr, n, ctx->sorted_pos.ptr, st, nullptr,
+						  sorted_forces(ctx, n), bonded ? fe : nullptr);
+	pair_kernel(ctx, n, prm->cutoff, 0, st, true);
 	if (bonded)
 		bond_angle_forces(reinterpret_cast<const int2*>(prm->bonds2), prm->bond_table_idx,
 						  prm->num_bonds, ctx->bonded_tables[0].ptr,
@@ -1183,19 +1195,23 @@ void step_once(mb2_context* ctx, float4* pos, float4* fe, const int* type_ids,
 	// the integrate kernel gathers them, adding what the bonded kernels
 	// wrote; ForceEnergy is cleared only when those run.
 	const bool bonded = step_has_bonded(prm);
-	if (bonded) MB2_CUDA(cudaMemsetAsync(fe, 0, static_cast<size_t>(n) * sizeof(float4), st));
 	// Rebuild schedule and skin check (Patch.cpp:86-108)
 	const bool at_period = prm->rebuild_period == 0 || (step - 1) % prm->rebuild_period == 0;
 	bool rebuild = at_period || !ctx->built || ctx->built_n != n;
 	const float skin = prm->pairlist_cutoff - prm->cutoff;
 	if (rebuild && prm->rebuild_period != 0 && ctx->built && ctx->built_n == n && skin > 0.0f)
 		rebuild = max_disp(ctx, pos, n, st) > skin * 0.5f;
-	if (rebuild)
+	if (rebuild) {
+		if (bonded) MB2_CUDA(cudaMemsetAsync(fe, 0, static_cast<size_t>(n) * sizeof(float4), st));
 		build(ctx, pos, type_ids, n, prm->pairlist_cutoff, prm->cutoff, st);  // packs sorted_pos
-	else if (n)
-		pack_sorted_positions(pos, type_ids, ctx->s2o.ptr, n, ctx->sorted_pos.ptr, st);
+	} else if (n) {
+		// The pack also clears the pair-force accumulator and, when bonded
+		// terms run, ForceEnergy.
+		pack_sorted_positions(pos, type_ids, ctx->s2o.ptr, n, ctx->sorted_pos.ptr, st, nullptr,
+							  sorted_forces(ctx, n), bonded ? fe : nullptr);
+	}
 	if (n == 0) return;
-	pair_kernel(ctx, n, prm->cutoff, prm->get_energy, st);
+	pair_kernel(ctx, n, prm->cutoff, prm->get_energy, st, !rebuild);
 	bonded_stage(ctx, pos, fe, prm, prm->get_energy, st);
 	StageScope scope(ctx, MB2_STAGE_INTEGRATE, st);
 	if (prm->integrator == 1) {
@@ -1221,9 +1237,9 @@ void step_body_replayable(mb2_context* ctx, float4* pos, float4* fe, const int* 
 						  const uint32_t* flags, uint32_t n, const mb2_step_params* prm,
 						  cudaStream_t st) {
 	const bool bonded = step_has_bonded(prm);
-	if (bonded) MB2_CUDA(cudaMemsetAsync(fe, 0, static_cast<size_t>(n) * sizeof(float4), st));
-	pack_sorted_positions(pos, type_ids, ctx->s2o.ptr, n, ctx->sorted_pos.ptr, st);
-	pair_kernel(ctx, n, prm->cutoff, prm->get_energy, st);
+	pack_sorted_positions(pos, type_ids, ctx->s2o.ptr, n, ctx->sorted_pos.ptr, st, nullptr,
+						  sorted_forces(ctx, n), bonded ? fe : nullptr);
+	pair_kernel(ctx, n, prm->cutoff, prm->get_energy, st, true);
 	bonded_stage(ctx, pos, fe, prm, prm->get_energy, st);
 	BdParams p{prm->dt, prm->kT, 0u, 0u, 0u, {prm->efield[0], prm->efield[1], prm->efield[2]}};
 	bd_integrate_gather(pos, fe, ctx->force_sorted.ptr, ctx->inv.ptr, type_ids, flags, n,
@@ -1429,9 +1445,10 @@ int mb2_window_backward(mb2_context* ctx, const float* grad_final4, float* grad_
 				MB2_ERR_CAPACITY,
 				"mb2_window_backward: the recorded-states buffer holds fewer than steps x n rows");
 		ctx->states.ensure(static_cast<size_t>(C) * n);
-		for (auto* b : {&ctx->wpos, &ctx->wfe, &ctx->lam, &ctx->mu, &ctx->mu_sorted, &ctx->tan,
-						&ctx->tan_sorted})
+		for (auto* b : {&ctx->wpos, &ctx->wfe, &ctx->lam, &ctx->mu, &ctx->mu_sorted})
 			b->ensure(n);
+		ctx->adj_tan.ensure(n);
+		ctx->adj_tan_sorted.ensure(n);
 		copy4(ctx->lam.ptr, reinterpret_cast<const float4*>(grad_final4), n, st);
 		AdjointStepArgs a{};
 		a.n = n;
@@ -1454,8 +1471,8 @@ int mb2_window_backward(mb2_context* ctx, const float* grad_final4, float* grad_
 		a.lam = ctx->lam.ptr;
 		a.mu = ctx->mu.ptr;
 		a.mu_sorted = ctx->mu_sorted.ptr;
-		a.tan = ctx->tan.ptr;
-		a.tan_sorted = ctx->tan_sorted.ptr;
+		a.tan = ctx->adj_tan.ptr;
+		a.tan_sorted = ctx->adj_tan_sorted.ptr;
 		a.grad_pair = grad_pair_bins;
 		a.grad_bond = grad_bond_bins;
 		for (uint32_t sgi = segs; sgi-- > 0;) {

@@ -180,9 +180,11 @@ void max_displacement_sq(const float4* cur, const float4* prev, uint32_t n, cons
 						 unsigned int* out_bits, cudaStream_t st);
 // nonfinite (optional): incremented once per particle with a NaN or infinite
 // coordinate.
+// clear_a / clear_b (may be null): float4[n] arrays zeroed by the same launch.
 void pack_sorted_positions(const float4* pos, const int* type_ids, const uint32_t* s2o,
 						   uint32_t n, float4* sorted_pos, cudaStream_t st,
-						   unsigned long long* nonfinite = nullptr);
+						   unsigned long long* nonfinite = nullptr, float4* clear_a = nullptr,
+						   float4* clear_b = nullptr);
 
 // forces.cu
 // Per type pair: the tabulated table's lookup constants and offset into the
@@ -370,8 +372,8 @@ struct AdjointStepArgs {
 	float4* lam;  // in: lambda_{k+1}; out: lambda_k
 	float4* mu;
 	float4* mu_sorted;
-	float4* tan;
-	float4* tan_sorted;
+	double4* tan;         // FP64 tangent accumulators, original order (x, y, z, unused)
+	double4* tan_sorted;  // and sorted order
 	double* grad_pair;  // [total pair bins], accumulated
 	double* grad_bond;  // [total bond bins], accumulated
 };

@@ -484,9 +484,15 @@ __global__ void __launch_bounds__(256) pack_kernel(const float4* __restrict__ po
 												   const int* __restrict__ type_ids,
 												   const uint32_t* __restrict__ s2o, uint32_t n,
 												   float4* __restrict__ sorted_pos,
-												   unsigned long long* nonfinite) {
+												   unsigned long long* nonfinite,
+												   float4* __restrict__ clear_a,
+												   float4* __restrict__ clear_b) {
 	const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
 	if (s >= n) return;
+	// Accumulators of the step that follows, cleared here instead of by
+	// separate memsets (one launch less each on short steps).
+	if (clear_a) clear_a[s] = make_float4(0.f, 0.f, 0.f, 0.f);
+	if (clear_b) clear_b[s] = make_float4(0.f, 0.f, 0.f, 0.f);
 	const uint32_t o = s2o[s];
 	float4 p = pos[o];
 	if (nonfinite && !(isfinite(p.x) && isfinite(p.y) && isfinite(p.z))) atomicAdd(nonfinite, 1ull);
@@ -563,10 +569,10 @@ void max_displacement_sq(const float4* cur, const float4* prev, uint32_t n, cons
 
 void pack_sorted_positions(const float4* pos, const int* type_ids, const uint32_t* s2o,
 						   uint32_t n, float4* sorted_pos, cudaStream_t st,
-						   unsigned long long* nonfinite) {
+						   unsigned long long* nonfinite, float4* clear_a, float4* clear_b) {
 	if (n == 0) return;
 	MB2_LAUNCH pack_kernel<<<(n + 255) / 256, 256, 0, st>>>(pos, type_ids, s2o, n, sorted_pos,
-															 nonfinite);
+															 nonfinite, clear_a, clear_b);
 }
 
 }  // namespace mb2
