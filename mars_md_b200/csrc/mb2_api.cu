@@ -30,6 +30,12 @@ struct mb2_context {
 	// Z-order state of the last build
 	DevBuf<uint32_t> keys, s2o, inv, row_len, row_off, nbr, cell_begin, cell_end, row_far;
 	DevBuf<float4> sorted_pos, ref_pos, force_sorted;
+	// Displacement since the last build, tracked by the step's pack (the
+	// pair kernel's inner rows): the build's Z-ordered positions, the squared
+	// maximum as float bits, and the build's list radius (0: not tracked).
+	DevBuf<float4> ref_sorted;
+	DevBuf<unsigned int> d2max;
+	float track_rc = 0.0f;
 	DevBuf<StencilEntry> stencil;
 	DevBuf<float> bbox;  // 6 floats, ordered-int min/max
 	DevBuf<unsigned int> disp;
@@ -411,6 +417,20 @@ void build(mb2_context* ctx, const float4* pos, const int* type_ids, uint32_t n,
 	ctx->ref_pos.ensure(n);
 	MB2_CUDA(cudaMemcpyAsync(ctx->ref_pos.ptr, pos, static_cast<size_t>(n) * sizeof(float4),
 							 cudaMemcpyDeviceToDevice, st));
+	// and, in Z order, the origin of the displacement the packs track. Only
+	// above kRowWalkMaxN particles: the inner rows save the pair kernel
+	// 2.6 % at 2,097,152 beads, while on a 65,536-bead step the pack's extra
+	// read and reduction cost more (1-2 us) than they save.
+	ctx->track_rc = 0.0f;
+	if (n > kRowWalkMaxN) {
+		ctx->ref_sorted.ensure(n);
+		ctx->d2max.ensure(1);
+		MB2_CUDA(cudaMemcpyAsync(ctx->ref_sorted.ptr, ctx->sorted_pos.ptr,
+								 static_cast<size_t>(n) * sizeof(float4), cudaMemcpyDeviceToDevice,
+								 st));
+		MB2_CUDA(cudaMemsetAsync(ctx->d2max.ptr, 0, sizeof(unsigned int), st));
+		ctx->track_rc = rc_list;
+	}
 	ctx->num_pairs = stats.first;
 	ctx->max_row = stats.second;
 	ctx->built = true;
@@ -422,6 +442,13 @@ bool matrix_has_analytical(const mb2_context* ctx) {
 	for (uint32_t tag : ctx->term_matrix_h)
 		if (tag & kTermAnalytical) return true;
 	return false;
+}
+
+// The displacement track of the last build, for the step's pack (none
+// before a build or after the box changed).
+DisplacementTrack track_of(mb2_context* ctx) {
+	if (!(ctx->track_rc > 0.0f)) return DisplacementTrack{};
+	return displacement_track(ctx->box, ctx->ref_sorted.ptr, ctx->d2max.ptr);
 }
 
 // Pair kernel over the sorted positions into the zeroed sorted accumulator.
@@ -447,8 +474,11 @@ void pair_kernel(mb2_context* ctx, uint32_t n, float cutoff, int get_energy, cud
 								 st));
 	const float cutoff_sq = cutoff > 0.0f ? cutoff * cutoff : 0.0f;
 	StageScope scope(ctx, MB2_STAGE_PAIR_FORCE, st);
+	// Every caller packs with track_of (or builds) just before: the track
+	// covers the positions the kernel reads.
 	pair_forces(ctx->sorted_pos.ptr, ctx->nbr.ptr, ctx->row_len.ptr, n, ctx->cap, ctx->lanes, ctx->pt,
-				ctx->box, cutoff_sq, get_energy, ctx->force_sorted.ptr, ctx->energy.ptr, st);
+				ctx->box, cutoff_sq, get_energy, ctx->force_sorted.ptr, ctx->energy.ptr, st,
+				ctx->track_rc > 0.0f ? ctx->d2max.ptr : nullptr, ctx->track_rc);
 }
 
 void pair_forces_impl(mb2_context* ctx, const float4* pos, const int* type_ids, float4* fe,
@@ -456,7 +486,7 @@ void pair_forces_impl(mb2_context* ctx, const float4* pos, const int* type_ids, 
 	require(ctx->built, MB2_ERR_STATE, "mb2_pair_forces: no pairlist; call mb2_build_pairlist");
 	if (n == 0) return;
 	pack_sorted_positions(pos, type_ids, ctx->s2o.ptr, n, ctx->sorted_pos.ptr, st, nullptr,
-						  sorted_forces(ctx, n));
+						  sorted_forces(ctx, n), nullptr, track_of(ctx));
 	pair_kernel(ctx, n, cutoff, get_energy, st, true);
 	scatter_add_forces(ctx->force_sorted.ptr, ctx->s2o.ptr, n, fe, get_energy, st);
 }
@@ -565,7 +595,7 @@ void window_step(mb2_context* ctx, float4* pos, float4* fe, const int* type_ids,
 				 uint64_t step, const mb2_step_params* prm, cudaStream_t st) {
 	const bool bonded = prm->num_bonds != 0 || prm->num_angles != 0;
 	pack_sorted_positions(pos, type_ids, ctx->s2o.ptr, n, ctx->sorted_pos.ptr, st, nullptr,
-						  sorted_forces(ctx, n), bonded ? fe : nullptr);
+						  sorted_forces(ctx, n), bonded ? fe : nullptr, track_of(ctx));
 	pair_kernel(ctx, n, prm->cutoff, 0, st, true);
 	if (bonded)
 		bond_angle_forces(reinterpret_cast<const int2*>(prm->bonds2), prm->bond_table_idx,
@@ -645,6 +675,7 @@ int mb2_set_box(mb2_context* ctx, const float origin[3], const float size[3],
 		}
 		ctx->box_set = true;
 		ctx->grid_valid = false;
+		ctx->track_rc = 0.0f;  // the tracked displacement belongs to the old box
 	});
 }
 
@@ -1208,7 +1239,7 @@ void step_once(mb2_context* ctx, float4* pos, float4* fe, const int* type_ids,
 		// The pack also clears the pair-force accumulator and, when bonded
 		// terms run, ForceEnergy.
 		pack_sorted_positions(pos, type_ids, ctx->s2o.ptr, n, ctx->sorted_pos.ptr, st, nullptr,
-							  sorted_forces(ctx, n), bonded ? fe : nullptr);
+							  sorted_forces(ctx, n), bonded ? fe : nullptr, track_of(ctx));
 	}
 	if (n == 0) return;
 	pair_kernel(ctx, n, prm->cutoff, prm->get_energy, st, !rebuild);
@@ -1238,7 +1269,7 @@ void step_body_replayable(mb2_context* ctx, float4* pos, float4* fe, const int* 
 						  cudaStream_t st) {
 	const bool bonded = step_has_bonded(prm);
 	pack_sorted_positions(pos, type_ids, ctx->s2o.ptr, n, ctx->sorted_pos.ptr, st, nullptr,
-						  sorted_forces(ctx, n), bonded ? fe : nullptr);
+						  sorted_forces(ctx, n), bonded ? fe : nullptr, track_of(ctx));
 	pair_kernel(ctx, n, prm->cutoff, prm->get_energy, st, true);
 	bonded_stage(ctx, pos, fe, prm, prm->get_energy, st);
 	BdParams p{prm->dt, prm->kT, 0u, 0u, 0u, {prm->efield[0], prm->efield[1], prm->efield[2]}};
@@ -1285,7 +1316,8 @@ std::vector<uint64_t> run_graph_key(const mb2_context* ctx, const float4* pos, c
 		static_cast<uint64_t>(ctx->types.num_types), P(ctx->types.charge), P(ctx->types.diffusion),
 		P(ctx->types.pmf_offset), P(ctx->types.pmf_count), P(ctx->types.terms),
 		P(ctx->types.force_grid_id), P(ctx->types.force_grid_scale), P(ctx->types.grids),
-		static_cast<uint64_t>(ctx->types.num_grids)};
+		static_cast<uint64_t>(ctx->types.num_grids), P(ctx->ref_sorted.ptr), P(ctx->d2max.ptr),
+		fbits(ctx->track_rc)};
 	push_words(k, ctx->pt.solvent);
 	push_words(k, ctx->box);
 	return k;

@@ -75,6 +75,18 @@ __device__ __forceinline__ float wrap1(float x, float l, float inv, float half) 
 	return x >= half ? __fsub_rn(x, l) : x;
 }
 
+// wrap1 for a component known to lie in [-l/2, l/2] (rows inside the box,
+// below): the reference's image floor(RN(x / l)) is 0 for x >= 0 and -1 for
+// x < 0, so its result is x, or RN(RN(x + l) - l) (which is >= l/2 before the
+// second rounding, so the reference takes that branch too), picked by the
+// sign bit. -0 takes the second form: RN(RN(-0 + l) - l) = +0, as the
+// reference's floor(-0) = -0 gives. (A negative x so small that x / l
+// underflows, |x| < 2^-149 l, would keep x where this gives +0.)
+__device__ __forceinline__ float wrap_inner(float x, float l, float negl) {
+	const float w = __fadd_rn(__fadd_rn(x, l), negl);
+	return __float_as_int(x) < 0 ? w : x;
+}
+
 // math::sinh_minus_x / x_cosh_minus_sinh (src/Types/Math.h:199-216): the
 // reference's series below |x| = 1, the direct difference above.
 __device__ __forceinline__ float sinh_minus_x(float x) {
@@ -202,7 +214,7 @@ struct TableRow {
 // -pi.y); a - b is computed as a + (-b) and b * l as -(b * (-l)), both exact
 // rewrites. The i-force is accumulated negated (nxy, nz): -(a - h) = (-a) + h
 // in round-to-nearest, so the caller's negation at the end gives the same sum.
-template <bool kEnergy, bool kAllPeriodic, bool kTerms, class TRow>
+template <bool kEnergy, bool kAllPeriodic, bool kTerms, bool kInner, class TRow>
 __device__ __forceinline__ void pair_scalar(const float4& pi, float2 npi, const float4& pj,
 											uint32_t j, uint32_t flip,
 											const TRow& trow, const float* bin_f,
@@ -216,7 +228,14 @@ __device__ __forceinline__ void pair_scalar(const float4& pi, float2 npi, const 
 	const float sgn = __uint_as_float(flip | 0x3F800000u);  // +1, or -1 when flipped
 	float2 dxy = __fmul2_rn(__fadd2_rn(make_float2(pj.x, pj.y), npi), make_float2(sgn, sgn));
 	float dz = __fmul_rn(__fsub_rn(pj.z, pi.z), sgn);
-	if (kAllPeriodic) {
+	if (kInner) {
+		// the row lies inside the box: |d| <= l/2 on every axis
+		const float2 l = make_float2(box.size[0], box.size[1]);
+		const float2 w = __fadd2_rn(__fadd2_rn(dxy, l), make_float2(-l.x, -l.y));
+		dxy.x = __float_as_int(dxy.x) < 0 ? w.x : dxy.x;
+		dxy.y = __float_as_int(dxy.y) < 0 ? w.y : dxy.y;
+		dz = wrap_inner(dz, box.size[2], -box.size[2]);
+	} else if (kAllPeriodic) {
 		// wrap1 on x and y: image = floor(d / l); d -= image * l; d >= l/2 -> d - l.
 		const float2 negl = make_float2(-box.size[0], -box.size[1]);
 		float2 img = __fmul2_rn(dxy, make_float2(box.inv[0], box.inv[1]));
@@ -293,8 +312,14 @@ __device__ __forceinline__ void pair_scalar(const float4& pi, float2 npi, const 
 // (batched replicas: system id in the top bits of the sorted key).
 struct OneBox {
 	Box b;
+	// Displacement track (may be null) and list_rc (1 + 2^-20) + kInnerSafety.
+	const unsigned int* d2max;
+	float margin;
 	__device__ __forceinline__ const Box& row(uint32_t) const { return b; }
 };
+// Added to the list radius in the inner-row test: covers kTrackBand and the
+// rounding of the displacement and of the walk's radius test.
+constexpr float kInnerSafety = 1.0f;
 struct SystemBoxes {
 	const Box* __restrict__ boxes;
 	const uint32_t* __restrict__ keys;
@@ -373,28 +398,57 @@ __global__ void __launch_bounds__(
 	float2 nxy = make_float2(0.0f, 0.0f);  // minus the i-force, x and y
 	float nz = 0.0f, fe = 0.0f;
 	double e_acc = 0.0, w_acc = 0.0;
+	// A row inside the box (all-periodic box, displacement tracked): every
+	// neighbour's minimum image is its plain difference, |d| <= list radius +
+	// twice the largest displacement since the build < l/2, so the pairs take
+	// wrap_inner's shorter sequence (same result). Decided per warp.
+	constexpr bool kCanInner = kAllPeriodic && std::is_same<BoxSrc, OneBox>::value;
+	bool inner = false;
+	if constexpr (kCanInner) {
+		if (boxes.d2max != nullptr) {
+			const float m = boxes.margin + 2.0f * sqrtf(__uint_as_float(__ldg(boxes.d2max)));
+			const float c[3] = {pi.x, pi.y, pi.z};
+			inner = true;
+#pragma unroll
+			for (int a = 0; a < 3; ++a)
+				inner = inner && c[a] >= box.origin[a] + m &&
+						c[a] <= box.origin[a] + box.size[a] - m;
+			inner = inner || !valid;
+		}
+		inner = __all_sync(0xFFFFFFFFu, inner);
+	}
 	// Two entries per lane per iteration: both neighbour gathers are in flight
 	// before either pair's arithmetic (the kernel is bound by gather latency).
-	uint32_t t = sub;
-	for (; t + G < cnt; t += 2 * G) {
-		const uint32_t e0 = __ldcs(col + static_cast<size_t>(t) * H);
-		const uint32_t e1 = __ldcs(col + static_cast<size_t>(t + G) * H);
-		const uint32_t j0 = e0 & ~kOrientBit, j1 = e1 & ~kOrientBit;
-		const float4 p0 = sorted_pos[j0];
-		const float4 p1 = sorted_pos[j1];
-		pair_scalar<kEnergy, kAllPeriodic, kTerms>(pi, npi, p0, j0, e0 & kOrientBit, trow, bin_f,
-												   bin_e, arow, sv, box, win, force, nxy, nz,
-												   fe, e_acc, w_acc);
-		pair_scalar<kEnergy, kAllPeriodic, kTerms>(pi, npi, p1, j1, e1 & kOrientBit, trow, bin_f,
-												   bin_e, arow, sv, box, win, force, nxy, nz,
-												   fe, e_acc, w_acc);
-	}
-	if (t < cnt) {
-		const uint32_t entry = __ldcs(col + static_cast<size_t>(t) * H);
-		const uint32_t j = entry & ~kOrientBit;
-		pair_scalar<kEnergy, kAllPeriodic, kTerms>(pi, npi, sorted_pos[j], j, entry & kOrientBit,
-												   trow, bin_f, bin_e, arow, sv, box, win, force,
-												   nxy, nz, fe, e_acc, w_acc);
+	auto walk = [&](auto inner_tag) {
+		constexpr bool kIn = decltype(inner_tag)::value;
+		uint32_t t = sub;
+		for (; t + G < cnt; t += 2 * G) {
+			const uint32_t e0 = __ldcs(col + static_cast<size_t>(t) * H);
+			const uint32_t e1 = __ldcs(col + static_cast<size_t>(t + G) * H);
+			const uint32_t j0 = e0 & ~kOrientBit, j1 = e1 & ~kOrientBit;
+			const float4 p0 = sorted_pos[j0];
+			const float4 p1 = sorted_pos[j1];
+			pair_scalar<kEnergy, kAllPeriodic, kTerms, kIn>(pi, npi, p0, j0, e0 & kOrientBit,
+															trow, bin_f, bin_e, arow, sv, box,
+															win, force, nxy, nz, fe, e_acc, w_acc);
+			pair_scalar<kEnergy, kAllPeriodic, kTerms, kIn>(pi, npi, p1, j1, e1 & kOrientBit,
+															trow, bin_f, bin_e, arow, sv, box,
+															win, force, nxy, nz, fe, e_acc, w_acc);
+		}
+		if (t < cnt) {
+			const uint32_t entry = __ldcs(col + static_cast<size_t>(t) * H);
+			const uint32_t j = entry & ~kOrientBit;
+			pair_scalar<kEnergy, kAllPeriodic, kTerms, kIn>(pi, npi, sorted_pos[j], j,
+															entry & kOrientBit, trow, bin_f,
+															bin_e, arow, sv, box, win, force, nxy,
+															nz, fe, e_acc, w_acc);
+		}
+	};
+	if constexpr (kCanInner) {
+		if (inner) walk(std::true_type{});
+		else walk(std::false_type{});
+	} else {
+		walk(std::false_type{});
 	}
 	// The lanes' sums of minus the i-force, then negated (exact).
 	float fx = nxy.x, fy = nxy.y, fz = nz;
@@ -864,11 +918,14 @@ bool uniform_tables(const std::vector<PairTableRef>& refs, std::vector<int>& off
 void pair_forces(const float4* sorted_pos, const uint32_t* nbr, const uint32_t* row_len,
 				 uint32_t n, uint32_t cap, int lanes_per_row, const PairTables& t, const Box& box,
 				 float cutoff_sq, int get_energy, float4* force_sorted, double* ev,
-				 cudaStream_t st) {
+				 cudaStream_t st, const unsigned int* d2max, float list_rc) {
 	if (n == 0) return;
 	const bool all_periodic = box.periodic[0] && box.periodic[1] && box.periodic[2];
-	launch_pair_lanes(sorted_pos, nbr, row_len, n, cap, lanes_per_row, t, OneBox{box},
-					  all_periodic, cutoff_sq, get_energy, force_sorted, ev, st);
+	const bool track = d2max != nullptr && list_rc > 0.0f && std::isfinite(list_rc);
+	const OneBox one{box, track ? d2max : nullptr,
+					 track ? list_rc * (1.0f + 0x1p-20f) + kInnerSafety : 0.0f};
+	launch_pair_lanes(sorted_pos, nbr, row_len, n, cap, lanes_per_row, t, one, all_periodic,
+					  cutoff_sq, get_energy, force_sorted, ev, st);
 }
 
 void pair_forces_systems(const float4* sorted_pos, const uint32_t* nbr, const uint32_t* row_len,

@@ -178,13 +178,31 @@ void export_pairs(const uint32_t* nbr, const uint32_t* row_len, const uint32_t* 
 				  cudaStream_t st);
 void max_displacement_sq(const float4* cur, const float4* prev, uint32_t n, const Box& box,
 						 unsigned int* out_bits, cudaStream_t st);
+// The largest displacement of any particle since the last pairlist build,
+// kept by the step's pack: d2max (a device word) holds its square as float
+// bits, raised with atomicMax and cleared at each build; +inf when a position
+// is not finite or lies outside a periodic axis of the box by more than
+// kTrackBand. ref_sorted: the Z-ordered positions the list was built from.
+// d2max == nullptr: not tracked.
+constexpr float kTrackBand = 0.5f;
+struct DisplacementTrack {
+	const float4* ref_sorted = nullptr;
+	unsigned int* d2max = nullptr;
+	float len[3] = {0.0f, 0.0f, 0.0f};  // periodic lengths (0: open axis)
+	float lo[3] = {0.0f, 0.0f, 0.0f};   // box bounds widened by kTrackBand
+	float hi[3] = {0.0f, 0.0f, 0.0f};
+};
+DisplacementTrack displacement_track(const Box& box, const float4* ref_sorted,
+									 unsigned int* d2max);
 // nonfinite (optional): incremented once per particle with a NaN or infinite
 // coordinate.
 // clear_a / clear_b (may be null): float4[n] arrays zeroed by the same launch.
+// track (optional): raises track.d2max to this step's largest displacement.
 void pack_sorted_positions(const float4* pos, const int* type_ids, const uint32_t* s2o,
 						   uint32_t n, float4* sorted_pos, cudaStream_t st,
 						   unsigned long long* nonfinite = nullptr, float4* clear_a = nullptr,
-						   float4* clear_b = nullptr);
+						   float4* clear_b = nullptr,
+						   const DisplacementTrack& track = DisplacementTrack{});
 
 // forces.cu
 // Per type pair: the tabulated table's lookup constants and offset into the
@@ -226,10 +244,14 @@ struct PairTables {
 	bool uniform = false;
 	PairTableRef uniform_ref{0.0f, 0.0f, 0, -1};
 };
+// d2max / list_rc (optional): the displacement track of the list's build and
+// its list radius. With them, rows of an all-periodic box that lie deeper
+// inside the box than list_rc + 2 * sqrt(*d2max) (plus a safety band) take a
+// shorter minimum-image sequence with the same result.
 void pair_forces(const float4* sorted_pos, const uint32_t* nbr, const uint32_t* row_len,
 				 uint32_t n, uint32_t cap, int lanes_per_row, const PairTables& t, const Box& box,
 				 float cutoff_sq, int get_energy, float4* force_sorted, double* energy_virial,
-				 cudaStream_t st);
+				 cudaStream_t st, const unsigned int* d2max = nullptr, float list_rc = 0.0f);
 // Host: per-type-pair lookup constants and per-bin force / (U0, dU) arrays of
 // a set of tabulated pair tables; returns the total number of bins.
 size_t pair_table_arrays(int num_types, const uint32_t* term_matrix, int num_tables,

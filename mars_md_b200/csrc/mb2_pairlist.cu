@@ -30,6 +30,7 @@
 #include "mb2_walk.cuh"
 
 #include <algorithm>
+#include <cfloat>
 #include <cmath>
 
 namespace mb2 {
@@ -486,18 +487,43 @@ __global__ void __launch_bounds__(256) pack_kernel(const float4* __restrict__ po
 												   float4* __restrict__ sorted_pos,
 												   unsigned long long* nonfinite,
 												   float4* __restrict__ clear_a,
-												   float4* __restrict__ clear_b) {
+												   float4* __restrict__ clear_b,
+												   DisplacementTrack track) {
 	const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
-	if (s >= n) return;
-	// Accumulators of the step that follows, cleared here instead of by
-	// separate memsets (one launch less each on short steps).
-	if (clear_a) clear_a[s] = make_float4(0.f, 0.f, 0.f, 0.f);
-	if (clear_b) clear_b[s] = make_float4(0.f, 0.f, 0.f, 0.f);
-	const uint32_t o = s2o[s];
-	float4 p = pos[o];
-	if (nonfinite && !(isfinite(p.x) && isfinite(p.y) && isfinite(p.z))) atomicAdd(nonfinite, 1ull);
-	p.w = __int_as_float(type_ids ? type_ids[o] : 0);
-	sorted_pos[s] = p;
+	float d2 = 0.0f;
+	if (s < n) {
+		// Accumulators of the step that follows, cleared here instead of by
+		// separate memsets (one launch less each on short steps).
+		if (clear_a) clear_a[s] = make_float4(0.f, 0.f, 0.f, 0.f);
+		if (clear_b) clear_b[s] = make_float4(0.f, 0.f, 0.f, 0.f);
+		const uint32_t o = s2o[s];
+		float4 p = pos[o];
+		if (nonfinite && !(isfinite(p.x) && isfinite(p.y) && isfinite(p.z)))
+			atomicAdd(nonfinite, 1ull);
+		if (track.d2max) {
+			const float4 r = track.ref_sorted[s];
+			d2 = len2(min_image(__fsub_rn(p.x, r.x), track.len[0]),
+					  min_image(__fsub_rn(p.y, r.y), track.len[1]),
+					  min_image(__fsub_rn(p.z, r.z), track.len[2]));
+			const float c[3] = {p.x, p.y, p.z};
+			bool inside = d2 <= FLT_MAX;  // false for NaN
+#pragma unroll
+			for (int a = 0; a < 3; ++a)
+				inside = inside && (track.len[a] == 0.0f || (c[a] >= track.lo[a] && c[a] <= track.hi[a]));
+			if (!inside) d2 = INFINITY;
+		}
+		p.w = __int_as_float(type_ids ? type_ids[o] : 0);
+		sorted_pos[s] = p;
+	}
+	if (track.d2max) {
+#pragma unroll
+		for (int k = 16; k > 0; k >>= 1) d2 = fmaxf(d2, __shfl_xor_sync(0xFFFFFFFFu, d2, k));
+		// Non-negative floats order like their bit patterns; the word only
+		// grows between builds, so most warps find nothing to raise.
+		const unsigned int bits = __float_as_uint(d2);
+		if ((threadIdx.x & 31) == 0 && bits > *reinterpret_cast<volatile unsigned int*>(track.d2max))
+			atomicMax(track.d2max, bits);
+	}
 }
 
 }  // namespace
@@ -567,12 +593,26 @@ void max_displacement_sq(const float4* cur, const float4* prev, uint32_t n, cons
 	MB2_LAUNCH displacement_kernel<<<(n + 255) / 256, 256, 0, st>>>(cur, prev, n, len, out_bits);
 }
 
+DisplacementTrack displacement_track(const Box& box, const float4* ref_sorted,
+									 unsigned int* d2max) {
+	DisplacementTrack t;
+	t.ref_sorted = ref_sorted;
+	t.d2max = d2max;
+	for (int a = 0; a < 3; ++a) {
+		t.len[a] = box.periodic[a] ? box.size[a] : 0.0f;
+		t.lo[a] = box.origin[a] - kTrackBand;
+		t.hi[a] = box.origin[a] + box.size[a] + kTrackBand;
+	}
+	return t;
+}
+
 void pack_sorted_positions(const float4* pos, const int* type_ids, const uint32_t* s2o,
 						   uint32_t n, float4* sorted_pos, cudaStream_t st,
-						   unsigned long long* nonfinite, float4* clear_a, float4* clear_b) {
+						   unsigned long long* nonfinite, float4* clear_a, float4* clear_b,
+						   const DisplacementTrack& track) {
 	if (n == 0) return;
 	MB2_LAUNCH pack_kernel<<<(n + 255) / 256, 256, 0, st>>>(pos, type_ids, s2o, n, sorted_pos,
-															 nonfinite, clear_a, clear_b);
+															 nonfinite, clear_a, clear_b, track);
 }
 
 }  // namespace mb2

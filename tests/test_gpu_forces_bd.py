@@ -27,7 +27,7 @@ import torch
 import pyoracle
 from conftest import box_of, force_errors, tableset, u32
 from mars_md_b200 import workloads as W
-from mars_md_b200.engine import setup_workload
+from mars_md_b200.engine import setup_workload, step_params
 
 pytestmark = pytest.mark.gpu
 
@@ -129,6 +129,46 @@ def test_pair_forces_large_plain_full_size_sample(ctx_factory, oracle):
     scaled, plain = force_errors(fe[sample], f64[sample], fabs[sample])
     print(f"large_plain full size, {len(sample)} particles, {len(sub)} pairs: worst {plain:.3e} "
           f"(scaled {scaled:.3e})")
+    assert plain <= 1e-5, (plain, scaled)
+    assert scaled <= 1e-5, (scaled, plain)
+
+
+def test_pair_forces_inner_rows_after_steps(ctx_factory, oracle):
+    """Above 131,072 particles the packs track the largest displacement since
+    the build, and rows deeper inside the box than the list radius plus twice
+    that displacement take the shorter minimum image. After nine BD steps on
+    the list of the first (no rebuild; the displacement is then a few
+    angstrom), the forces on the current positions from that list must still
+    be the oracle's: 16,384 strided particles at the bar above."""
+    w = W.large_plain(n=262144)
+    ctx = ctx_factory(w.n)
+    dev = setup_workload(ctx, w)
+    prm = step_params(w)
+    prm.rebuild_period = 1000  # step 1 builds; steps 2-10 keep its list
+    for s in range(1, 11):
+        ctx.step(dev["pos"], dev["fe"], dev["type"], None, s, prm)
+    dev["fe"].zero_()
+    ctx.pair_forces(dev["pos"], dev["type"], dev["fe"], w.cutoff, get_energy=False)
+    fe = dev["fe"].cpu().numpy()
+    pos = dev["pos"].cpu().numpy()
+    pos[:, 3] = w.pos[:, 3]
+    start = w.pos[:, :3].astype(np.float64)
+    moved = np.abs(pos[:, :3] - start)
+    moved = np.minimum(moved, np.array(w.box_size) - moved)
+    dmax = float(np.sqrt((moved ** 2).sum(1)).max())
+    assert dmax > 0.5, dmax
+    sample = np.arange(0, w.n, 16)
+    mask = torch.zeros(w.n, dtype=torch.bool, device="cuda")
+    mask[torch.from_numpy(sample).cuda()] = True
+    pairs = ctx.export_pairs()
+    keep = mask[pairs[:, 0].long()] | mask[pairs[:, 1].long()]
+    sub = pairs[keep].cpu().numpy()
+    tags = oracle.resolve_tags(sub, w.type_ids, w.term_matrix, w.num_types)
+    _, f64, fabs = oracle.pair_forces(sub, pos, tags, tableset(w), box_of(w),
+                                      np.float32(w.cutoff) ** 2)
+    scaled, plain = force_errors(fe[sample], f64[sample], fabs[sample])
+    print(f"large_plain 262,144 after 9 steps (max displacement {dmax:.2f} A): "
+          f"worst {plain:.3e} (scaled {scaled:.3e})")
     assert plain <= 1e-5, (plain, scaled)
     assert scaled <= 1e-5, (scaled, plain)
 

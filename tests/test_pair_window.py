@@ -55,3 +55,36 @@ def test_window_is_the_reference_test(cutoff):
 def test_window_rejects_null_outputs():
     lib = L.load()
     assert lib.mb2_pair_distance_window(f32(30.0), None, None) == L.MB2_ERR_ARG
+
+
+def _wrap_reference(x, l):
+    """PeriodicBox::wrap_diff_scalar (src/System/PeriodicBox.h:453-461) in
+    float32: image = floor(x * (1/l)); x -= image * l; x >= l/2 -> x - l."""
+    f = np.float32
+    inv, half = f(1) / l, f(0.5) * l
+    img = np.floor((x * inv).astype(f)).astype(f)
+    y = (x - (img * l).astype(f)).astype(f)
+    return np.where(y >= half, (y - l).astype(f), y).astype(f)
+
+
+@pytest.mark.parametrize("l", [1015.9, 127.0, 253.98427, 600.0, 33.3])
+def test_inner_row_minimum_image(l):
+    """The pair kernel's rows inside the box (every neighbour's difference in
+    [-l/2, l/2)) take x, or RN(RN(x + l) - l) for a set sign bit, in place of
+    the reference's floor sequence: the same float on every such x, signed
+    zeros and tiny magnitudes included (+l/2 itself is outside the rows'
+    bound and is the one value where the two differ)."""
+    f = np.float32
+    l = f(l)
+    half = f(0.5) * l
+    rng = np.random.default_rng(7)
+    x = np.concatenate([
+        rng.uniform(-half, half, 1_000_000).astype(f),
+        (rng.uniform(-1, 1, 100_000) * 1e-3).astype(f),
+        (rng.uniform(-1, 1, 100_000) * 1e-30).astype(f),
+        np.array([0.0, -0.0, -half, np.nextafter(half, f(0)), -np.nextafter(half, f(0))], f)])
+    w = ((x + l).astype(f) + (-l)).astype(f)
+    inner = np.where(x.view(np.int32) < 0, w, x).astype(f)
+    ref = _wrap_reference(x, l)
+    assert np.array_equal(inner.view(np.uint32), ref.view(np.uint32))
+    assert _wrap_reference(np.array([half], f), l)[0] != half  # the excluded end
