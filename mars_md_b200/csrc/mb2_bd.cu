@@ -112,13 +112,16 @@ __device__ __forceinline__ void grid_sample(const GridView& g, float px, float p
 	grad.z = __fadd_rn(__fadd_rn(__fmul_rn(gx, m[6]), __fmul_rn(gy, m[7])), __fmul_rn(gz, m[8]));
 }
 
-// compute_position_dependent_force (Pmf.h:68-124).
+// compute_position_dependent_force (Pmf.h:68-124). kGrids false: the caller
+// knows that no grid is loaded (ty.num_grids == 0), and the grid code is not
+// compiled in.
+template <bool kGrids = true>
 __device__ __forceinline__ float4 position_force(const TypeTable& ty, int type, float px, float py,
 												 float pz, const float* efield) {
 	const float q = ty.charge[type];
 	float4 f = make_float4(__fmul_rn(q, efield[0]), __fmul_rn(q, efield[1]),
 						   __fmul_rn(q, efield[2]), 0.0f);
-	if (ty.num_grids == 0) return f;
+	if (!kGrids || ty.num_grids == 0) return f;
 	const int begin = ty.pmf_offset[type];
 	const int end = begin + ty.pmf_count[type];
 	for (int k = begin; k < end; ++k) {
@@ -217,7 +220,9 @@ __device__ __forceinline__ uint64_t mix_seed(uint64_t seed, uint64_t patch, uint
 // after integrate_motion; then the grid force, noise and update as bd_kernel.
 // step_ptr (graph replay): the step number comes from device memory and the
 // Philox key is mixed here from (seed, patch_id, step), as the host does for
-// bp.base_seed otherwise.
+// bp.base_seed otherwise. kGrids false (no grid loaded): without the grid
+// code the kernel takes fewer registers and more warps fit on an SM.
+template <bool kGrids>
 __global__ void __launch_bounds__(256) bd_gather_kernel(
 	float4* __restrict__ pos, float4* __restrict__ fe, const float4* __restrict__ fs,
 	const uint32_t* __restrict__ inv, const int* __restrict__ type_ids,
@@ -245,7 +250,7 @@ __global__ void __launch_bounds__(256) bd_gather_kernel(
 	}
 	const float4 p = pos[i];
 	const int type = type_ids[i];
-	const float4 pmf = position_force(ty, type, p.x, p.y, p.z, bp.efield);
+	const float4 pmf = position_force<kGrids>(ty, type, p.x, p.y, p.z, bp.efield);
 	const float3 xi = bd_noise(bp.base_seed, bp.base_ctr + i, bp.step);
 	if (pmf.w != 0.0f) f.w = __fadd_rn(f.w, pmf.w);
 	fe[i] = f;
@@ -365,7 +370,8 @@ __global__ void __launch_bounds__(256) baoab_last_kernel(float4* __restrict__ mo
 // Batched replicas: particle i of system s = sys_of[i] integrates as a plain
 // step of system s with seed (seed + s) would (counter = index in the
 // system, its own box); the step number comes from device memory so that a
-// captured graph can be replayed step after step.
+// captured graph can be replayed step after step. kGrids as bd_gather_kernel.
+template <bool kGrids>
 __global__ void __launch_bounds__(256) bd_systems_kernel(
 	float4* __restrict__ pos, float4* __restrict__ fe, const float4* __restrict__ fs,
 	const uint32_t* __restrict__ inv, const int* __restrict__ type_ids,
@@ -382,7 +388,7 @@ __global__ void __launch_bounds__(256) bd_systems_kernel(
 	const int type = type_ids[i];
 	const BdParams bp{dt, kT, static_cast<uint32_t>(step), mix_seed(seed + s, patch_id, step), 0u,
 					  {0.0f, 0.0f, 0.0f}};
-	const float4 pmf = position_force(ty, type, p.x, p.y, p.z, bp.efield);
+	const float4 pmf = position_force<kGrids>(ty, type, p.x, p.y, p.z, bp.efield);
 	const float3 xi = bd_noise(bp.base_seed, i - offsets[s], bp.step);
 	if (pmf.w != 0.0f) f.w = __fadd_rn(f.w, pmf.w);
 	fe[i] = f;
@@ -419,9 +425,10 @@ void bd_integrate_gather(float4* pos, float4* fe, const float4* force_sorted, co
 						 cudaStream_t st, const unsigned long long* step_ptr, uint64_t seed,
 						 uint64_t patch_id) {
 	if (n == 0) return;
-	MB2_LAUNCH bd_gather_kernel<<<(n + 255) / 256, 256, 0, st>>>(pos, fe, force_sorted, inv, type_ids,
-																 flags, n, types, box, p, read_fe,
-																 step_ptr, seed, patch_id);
+	auto kern = types.num_grids == 0 ? bd_gather_kernel<false> : bd_gather_kernel<true>;
+	MB2_LAUNCH kern<<<(n + 255) / 256, 256, 0, st>>>(pos, fe, force_sorted, inv, type_ids, flags, n,
+													 types, box, p, read_fe, step_ptr, seed,
+													 patch_id);
 }
 
 void baoab_integrate(float4* pos, float4* mom, float4* fe, const int* type_ids,
@@ -457,9 +464,10 @@ void bd_integrate_systems(float4* pos, float4* fe, const float4* force_sorted,
 						  const TypeTable& types, float dt, float kT, uint64_t seed,
 						  uint64_t patch_id, const unsigned long long* step_ptr, cudaStream_t st) {
 	if (n == 0) return;
-	MB2_LAUNCH bd_systems_kernel<<<(n + 255) / 256, 256, 0, st>>>(
-		pos, fe, force_sorted, inv, type_ids, sys_of, offsets, boxes, n, types, dt, kT, seed,
-		patch_id, step_ptr);
+	auto kern = types.num_grids == 0 ? bd_systems_kernel<false> : bd_systems_kernel<true>;
+	MB2_LAUNCH kern<<<(n + 255) / 256, 256, 0, st>>>(pos, fe, force_sorted, inv, type_ids, sys_of,
+													 offsets, boxes, n, types, dt, kT, seed,
+													 patch_id, step_ptr);
 }
 
 void step_counter_set(unsigned long long* ptr, uint64_t value, cudaStream_t st) {
