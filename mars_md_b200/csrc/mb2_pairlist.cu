@@ -467,6 +467,9 @@ __global__ void __launch_bounds__(256) displacement_kernel(const float4* __restr
 														   uint32_t n, float3 len,
 														   unsigned int* __restrict__ out) {
 	const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+	// The word so far, read before the loads so its latency overlaps theirs:
+	// a warp whose maximum is not above it has nothing to raise.
+	const unsigned int seen = (threadIdx.x & 31) == 0 ? *reinterpret_cast<volatile unsigned int*>(out) : 0u;
 	float d2 = 0.0f;
 	if (i < n) {
 		const float4 c = cur[i], p = prev[i];
@@ -474,11 +477,11 @@ __global__ void __launch_bounds__(256) displacement_kernel(const float4* __restr
 		const float dy = min_image(__fsub_rn(c.y, p.y), len.y);
 		const float dz = min_image(__fsub_rn(c.z, p.z), len.z);
 		d2 = len2(dx, dy, dz);
+		if (isnan(d2)) d2 = 0.0f;  // a NaN coordinate does not trip the skin check
 	}
-#pragma unroll
-	for (int o = 16; o > 0; o >>= 1) d2 = fmaxf(d2, __shfl_xor_sync(0xFFFFFFFFu, d2, o));
 	// Non-negative floats order like their bit patterns.
-	if ((threadIdx.x & 31) == 0) atomicMax(out, __float_as_uint(d2));
+	const unsigned int bits = __reduce_max_sync(0xFFFFFFFFu, __float_as_uint(d2));
+	if ((threadIdx.x & 31) == 0 && bits > seen) atomicMax(out, bits);
 }
 
 __global__ void __launch_bounds__(256) pack_kernel(const float4* __restrict__ pos,
@@ -490,6 +493,10 @@ __global__ void __launch_bounds__(256) pack_kernel(const float4* __restrict__ po
 												   float4* __restrict__ clear_b,
 												   DisplacementTrack track) {
 	const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
+	// The tracked word so far, read before the loads (see displacement_kernel).
+	const unsigned int seen = track.d2max && (threadIdx.x & 31) == 0
+								  ? *reinterpret_cast<volatile unsigned int*>(track.d2max)
+								  : 0u;
 	float d2 = 0.0f;
 	if (s < n) {
 		// Accumulators of the step that follows, cleared here instead of by
@@ -516,13 +523,10 @@ __global__ void __launch_bounds__(256) pack_kernel(const float4* __restrict__ po
 		sorted_pos[s] = p;
 	}
 	if (track.d2max) {
-#pragma unroll
-		for (int k = 16; k > 0; k >>= 1) d2 = fmaxf(d2, __shfl_xor_sync(0xFFFFFFFFu, d2, k));
 		// Non-negative floats order like their bit patterns; the word only
 		// grows between builds, so most warps find nothing to raise.
-		const unsigned int bits = __float_as_uint(d2);
-		if ((threadIdx.x & 31) == 0 && bits > *reinterpret_cast<volatile unsigned int*>(track.d2max))
-			atomicMax(track.d2max, bits);
+		const unsigned int bits = __reduce_max_sync(0xFFFFFFFFu, __float_as_uint(d2));
+		if ((threadIdx.x & 31) == 0 && bits > seen) atomicMax(track.d2max, bits);
 	}
 }
 

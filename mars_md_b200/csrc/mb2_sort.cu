@@ -134,8 +134,64 @@ __global__ void __launch_bounds__(256) remap_kernel(int* __restrict__ idx, size_
 
 }  // namespace
 
+namespace {
+
+// Up to this many pairs the sort runs in one CTA: the passes above take
+// twenty launches, which at a few thousand elements is launch latency.
+constexpr uint32_t kOneBlockSortMax = 8192;
+
+// One-CTA sort of up to kOneBlockSortMax (key, value) pairs, stable: a
+// bitonic network in shared memory over (key << 32 | position), whose
+// composites are distinct, so their order is the stable order by key; each
+// value then follows its position. p2: n rounded up to a power of two
+// (padding sorts last).
+__global__ void __launch_bounds__(1024) sort_one_block_kernel(uint32_t* __restrict__ keys,
+															  uint32_t* __restrict__ vals,
+															  uint32_t n, uint32_t p2) {
+	extern __shared__ unsigned long long comp[];
+	uint32_t* vsh = reinterpret_cast<uint32_t*>(comp + p2);
+	for (uint32_t i = threadIdx.x; i < p2; i += blockDim.x) {
+		comp[i] = i < n ? (static_cast<unsigned long long>(keys[i]) << 32) | i : ~0ull;
+		if (i < n) vsh[i] = vals[i];
+	}
+	__syncthreads();
+	for (uint32_t k = 2; k <= p2; k <<= 1) {
+		for (uint32_t j = k >> 1; j > 0; j >>= 1) {
+			for (uint32_t t = threadIdx.x; t < p2 / 2; t += blockDim.x) {
+				const uint32_t lo = 2 * t - (t & (j - 1));  // bit j of lo clear
+				const uint32_t hi = lo + j;
+				const unsigned long long a = comp[lo], b = comp[hi];
+				const bool ascending = (lo & k) == 0;
+				if ((a > b) == ascending) {
+					comp[lo] = b;
+					comp[hi] = a;
+				}
+			}
+			__syncthreads();
+		}
+	}
+	for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) {
+		const unsigned long long c = comp[i];
+		keys[i] = static_cast<uint32_t>(c >> 32);
+		vals[i] = vsh[static_cast<uint32_t>(c)];
+	}
+}
+
+}  // namespace
+
 void radix_sort_pairs(Scratch& s, uint32_t* keys, uint32_t* vals, uint32_t n, cudaStream_t st) {
 	if (n <= 1) return;
+	if (n <= kOneBlockSortMax) {
+		uint32_t p2 = 2;
+		while (p2 < n) p2 <<= 1;
+		const size_t smem = static_cast<size_t>(p2) * (sizeof(unsigned long long) + sizeof(uint32_t));
+		if (smem > 48 * 1024)
+			MB2_CUDA(cudaFuncSetAttribute(sort_one_block_kernel,
+										  cudaFuncAttributeMaxDynamicSharedMemorySize,
+										  static_cast<int>(smem)));
+		MB2_LAUNCH sort_one_block_kernel<<<1, 1024, smem, st>>>(keys, vals, n, p2);
+		return;
+	}
 	const uint32_t tiles = (n + kTile - 1) / kTile;
 	s.ensure_sort(n, tiles * 256u);
 	uint32_t *ks = keys, *vs = vals, *kd = s.sort_keys_alt, *vd = s.sort_vals_alt;

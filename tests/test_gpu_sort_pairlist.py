@@ -63,6 +63,25 @@ def test_radix_sort_large_sortedness(ctx_factory):
     assert np.array_equal(ref_keys.cpu().numpy().view(np.uint32)[v], k.astype(np.uint32))
 
 
+@pytest.mark.parametrize("n", [2, 3, 1000, 4097, 8192, 8193, 20000])
+def test_radix_sort_small_stable(ctx_factory, n):
+    """Up to 8,192 pairs one CTA sorts (a bitonic network over key and
+    position), above that the radix passes: both must give a host stable
+    argsort's permutation, here with many equal keys (16 distinct values) and
+    payloads that are not in ascending order, on both sides of the switch."""
+    rng = np.random.default_rng(n)
+    keys_np = rng.integers(0, 16, n).astype(np.uint32) * np.uint32(0x10001001)
+    vals_np = rng.permutation(n).astype(np.uint32)
+    keys = torch.from_numpy(keys_np.view(np.int32)).cuda()
+    vals = torch.from_numpy(vals_np.view(np.int32)).cuda()
+    ctx = ctx_factory(16)
+    ctx.radix_sort_pairs(keys, vals)
+    torch.cuda.synchronize()
+    order = np.argsort(keys_np, kind="stable")
+    assert np.array_equal(u32(keys), keys_np[order])
+    assert np.array_equal(u32(vals), vals_np[order])
+
+
 def _build_and_compare(ctx, oracle, w, rc_list, excl=None, excl_np=None):
     d = torch.from_numpy(w.pos).cuda()
     t = torch.from_numpy(w.type_ids).cuda()
